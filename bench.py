@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark: zone-updates/s of the explicit FV step on B200 (and the CPU reference arm).
+
+Default workload: 3D stratified convection box, Helmholtz EoS, well-balanced LHLLC + PLM + RK3,
+256^3 cells (the configuration the headline metric is quoted on).  A "step" is one full
+hydro step (3 RK stages) plus the CFL dt reduction, i.e. one iteration of time_loop without
+output; zone-updates/s = steps * cells / time (the reference's own "updated cells/s",
+source/source.F90:6834-6835).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--n SIZE] [--impl ours|reference]
+
+One process per GPU; for N > 1 (torchrun) every rank advances an independent replica of the
+workload (the single-GPU path has no data-path collective) and rank 0 prints the aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200: FP32+learned-EoS vs FP64 plain vs CPU, at stated L1 err"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return dict(PEAKS_FALLBACK), "fallback"
+
+
+def build_problem(name, n):
+    from phlegethon_b200 import helm_table, problems
+    table = None
+    if name == "stratified":
+        cfg, h = problems.stratified_3d(n)
+        table = helm_table.generate()
+    elif name == "stratified_mhd":
+        cfg, h = problems.stratified_3d(n, mhd=True)
+        table = helm_table.generate()
+    elif name == "hot_bubble":
+        cfg, h = problems.hot_bubble_2d(n)
+    elif name == "orszag_tang":
+        cfg, h = problems.orszag_tang_2d(n)
+    else:
+        raise SystemExit("unknown config " + name)
+    return cfg, h, table
+
+
+def default_size(name):
+    return {"stratified": 256, "stratified_mhd": 256, "hot_bubble": 256, "orszag_tang": 1024}[name]
+
+
+def step_bytes_per_cell(cfg):
+    """Algorithmic HBM bytes per zone-update of the fused stage kernel (minimum traffic).
+
+    Stage 1 reads W (nv) and eint and writes U0, U, W; middle stages read W, U0, U and write U,
+    W; the last stage reads W, U0, U and writes W and eint.  Helmholtz adds temp (read+write per
+    stage) and the two gamma fields (read+write per stage).  MHD adds the face fields: per stage
+    b read, b0 read (b0 written in stage 1), b written, plus the face EMFs and signs written and
+    read once (2D: 1 EMF + 1 sign per face direction; 3D: 2 + 1).
+    """
+    nv = cfg.nvars
+    s = cfg.rk_stages
+    doubles = (nv + 1 + 3 * nv) + (s - 2) * (5 * nv) + (3 * nv + nv + 1)
+    if cfg.helmholtz:
+        doubles += s * (2 + 4)
+    if cfg.mhd:
+        nd = cfg.sdims
+        emf = 1 if nd == 2 else 2
+        doubles += s * nd * (3 + 2 * (emf + 1)) + nd
+        doubles += s * nd  # b_cc write
+    return 8 * doubles
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = []
+        for k, nm in enumerate(names):
+            if any(r[5 + k].lower().startswith("active") for r in rows):
+                reasons.append(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_rate(name, steps, nthreads=0, slab=None):
+    """Oracle (CPU restatement) zone-updates/s on a bounded slab of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from phlegethon_b200 import helm_table, problems
+    if name in ("stratified", "stratified_mhd"):
+        n = default_size(name)
+        nz = slab or 32
+        cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"))
+        tab, dpdr = helm_table.generate()
+        helm = pyoracle.Helm.for_config(cfg, tab, dpdr)
+        sample = "%dx%dx%d slab of the %d^3 workload" % (cfg.nx1, cfg.nx2, cfg.nx3, n)
+    else:
+        n = default_size(name)
+        cfg, h, _ = build_problem(name, n)
+        helm = None
+        sample = "%dx%d full workload" % (cfg.nx1, cfg.nx2)
+    o = pyoracle.OracleGrid(h, helm, nthreads=nthreads)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(1)  # warm-up: first-touch allocations
+    t0 = time.perf_counter()
+    o.time_loop(steps)
+    dt = time.perf_counter() - t0
+    cores = nthreads or os.cpu_count()
+    return steps * cfg.n_cells / dt, cores, sample + ", %d steps" % steps
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    rate, cores, sample = cpu_rate(args.config, steps)
+    cfgname = args.config
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "zone-updates/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfgname, "n": args.n or default_size(cfgname)},
+            "cpu_baseline": {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of the reference routines (oracle/), OpenMP over all host cores; "
+                    "the reference's Fortran build is unavailable (no gfortran/mpifort)"}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_like(a):
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    v = t.numpy().reshape(a.shape, order="F")
+    v[...] = a
+    return t, v
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from phlegethon_b200 import abi
+    from phlegethon_b200.grid import HostGrid
+
+    name = args.config
+    n = args.n or default_size(name)
+    cfg, h, table = build_problem(name, n)
+    cfg.device = local
+    peaks, peak_kind = load_peaks()
+
+    sim = abi.Simulation(cfg, table)
+    sim.upload(h)
+    sim.init_thermo()
+    sim.compute_hyperbolic_dt()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=torch.device("cuda", local))
+
+    # ---------------------------------------------------------------- device-resident timing
+    sim.time_loop(args.warmup)
+    sim.reset_status()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done, _ = sim.time_loop(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    status = sim.status()
+    cells = cfg.n_cells
+    value = world * done * cells / (ms * 1e-3)
+
+    # ---------------------------------------------------------------- dominant kernel timing
+    # hydro_step launches the RK stage kernels back to back without a graph; their average
+    # duration is measured with events on the library's stream
+    reps = max(2, min(args.steps, 5))
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(reps):
+        sim.hydro_step()
+    k1.record(stream)
+    torch.cuda.synchronize()
+    launches = reps * cfg.rk_stages
+    launch_ms = k0.elapsed_time(k1) / launches
+    bytes_per_cell = step_bytes_per_cell(cfg)
+    achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "kernel": "k_stage (fused flux + RK + cons->prim + EoS)", "peak_kind": peak_kind,
+            "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
+
+    # ---------------------------------------------------------------- end-to-end through the ABI
+    # host-owned state in pinned memory: every step uploads the dynamic state, advances one
+    # step and downloads it again (prim, temp, eint [, gammaf, b_cc, b faces])
+    dyn = HostGrid.__new__(HostGrid)
+    dyn.__dict__.update(h.__dict__)
+    keep = []
+    for nm in ("prim", "temp", "eint", "gammaf", "b_cc"):
+        a = getattr(h, nm)
+        if a is not None:
+            t_, v_ = pinned_like(a)
+            keep.append(t_)
+            setattr(dyn, nm, v_)
+    bx = []
+    for d in range(3):
+        a = h.b_x[d]
+        if a is not None:
+            t_, v_ = pinned_like(a)
+            keep.append(t_)
+            bx.append(v_)
+        else:
+            bx.append(None)
+    dyn.b_x = bx
+    for nm in ("grav", "phi_cc", "eq_prim_cc", "eq_gammae_cc"):
+        setattr(dyn, nm, None)
+    dyn.phi_x = [None] * 3
+    dyn.eq_prim_x = [None] * 3
+    dyn.eq_gammae_x = [None] * 3
+    sim.download(dyn)
+    e2e_steps = max(1, min(args.steps, 5))
+    h2d = sum(a.nbytes for a in [dyn.prim, dyn.temp, dyn.eint, dyn.gammaf, dyn.b_cc] + bx if a is not None)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    x0 = torch.cuda.Event(enable_timing=True)
+    x1 = torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload(dyn)
+        sim.time_loop(1)
+        sim.download(dyn)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = x0.elapsed_time(x1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * e2e_steps * cells / (e2e_ms * 1e-3)
+    sim.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample = cpu_rate(name, steps=1)
+        cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / max(done, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": name, "n": n, "cells": cells, "form": "fp64 plain",
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(h2d)},
+                "gpu_launches": int(done * (cfg.rk_stages + 2)), "clocks": clocks,
+                "newton": {k: status[k] for k in ("newton_calls", "newton_iterations", "newton_nonconverged")},
+                "nonfinite": status["nonfinite"]}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="stratified",
+                    choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang"])
+    ap.add_argument("--n", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,708 @@
+// phl_kernels.cuh -- stage kernels of the explicit FV step on the device-resident SoA domain.
+//
+// Device layout (no ghost cells are stored; ghost values are produced by index mapping):
+//   W[iv][c]   primitive variables (full values), c = i + nx*(j + ny*k), ping-ponged per stage
+//   U0, U      conserved state at the step start and the running RK state
+//   eint, temp internal energy density and temperature (in place, own cell only)
+//   gam[2][c]  (gammae, gammac) for USE_FASTEOS, ping-ponged with W
+//   background fields (eq_prim, eq_gammae, phi, grav) either full arrays or profiles along x2
+//   MHD: face fields bf[d] (interior faces only), b0f, face EMFs/signs, corner EMFs, bcc[3][c]
+//
+// The kernels take `Prm` by value.  Arithmetic follows source/source.F90 operation by operation
+// so that the FP64 instantiation (compiled with --fmad=false) reproduces the reference.
+#pragma once
+#include "phl_device.cuh"
+
+namespace phl {
+
+template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_>
+struct Cfg {
+  static constexpr int DIM = DIM_, NV = NV_, RIEM = RIEM_;
+  static constexpr bool MHD = MHD_, HELM = HELM_, WB = WB_, ETOT = ETOT_, GRAV = GRAV_;
+  static constexpr int IP = 1 + DIM, IAS = 2 + DIM;
+  static_assert(!HELM || NV >= IAS + 2, "Helmholtz needs ADVECT_YE_IABAR scalars");
+};
+
+struct Prm {
+  Geo g;
+  const double *__restrict__ Win;
+  double *Wout;
+  double *U, *U0, *eint, *temp;
+  const double *__restrict__ gin;
+  double *gout;
+  // background (cell-centred: full N or profile ny; faces: full or profile)
+  const double *eq_rho_cc, *eq_p_cc, *eq_ge_cc, *phi_cc, *grav;
+  const double *eq_rho_f[3], *eq_p_f[3], *eq_ge_f[3], *phi_f[3];
+  // MHD
+  const double *bcc_in;
+  double *bcc_out;
+  double *bf[3], *b0f[3], *emf[3], *sgnf[3], *cor[3];
+  // device scalars: [0] time, [1] dt, [2] smax, [3] tmax
+  double *scal;
+  unsigned long long *smax_bits;
+  int *active;
+  unsigned long long *stat;  // see STAT_* below
+  HelmTable helm;
+  double a1, a2, c3;
+  int first_stage, last_stage;
+};
+
+enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,
+       STAT_MLP_ACC, STAT_MLP_REJ, STAT_NONFINITE, STAT_COUNT };
+
+__device__ __forceinline__ long long bg_cc(const Geo &g, int i, int j, int k) {
+  return g.bg_profile ? (long long)j : lin(g, i, j, k);
+}
+// face index along d: (i,j,k) with the d coordinate in 0..nx[d]
+__device__ __forceinline__ long long face_lin(const Geo &g, int d, int i, int j, int k) {
+  long long n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  return (long long)i + n0 * ((long long)j + n1 * (long long)k);
+}
+__device__ __forceinline__ long long bg_face(const Geo &g, int d, int i, int j, int k) {
+  return g.bg_profile ? (long long)j : face_lin(g, d, i, j, k);
+}
+__device__ __forceinline__ long long nfaces(const Geo &g, int d) {
+  return (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
+}
+
+// warp/block max of a non-negative double, then one atomic per block (bit patterns of
+// non-negative doubles order like the values)
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *dst) {
+  __shared__ double red[32];
+  unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
+    if (lane == 0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+__device__ __forceinline__ void block_sum_atomic(unsigned long long v, unsigned long long *dst) {
+  unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// --------------------------------------------------------------------- cell loads
+// Deviation primitive state of a (possibly ghost) cell: (W - eq) for rho and p under WB,
+// velocity component d negated for each mirrored dimension d.
+template <class C>
+__device__ __forceinline__ void load_wdev(const Prm &P, int i, int j, int k, double w[C::NV]) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
+  long long c = lin(g, si, sj, sk);
+#pragma unroll
+  for (int iv = 0; iv < C::NV; ++iv) w[iv] = __ldg(P.Win + (long long)iv * g.N + c);
+  if (C::WB) {
+    long long b = bg_cc(g, si, sj, sk);
+    w[0] = w[0] - __ldg(P.eq_rho_cc + b);
+    w[C::IP] = w[C::IP] - __ldg(P.eq_p_cc + b);
+  }
+  if (f0) w[1] = -1.0 * w[1];
+  if (f1) w[2] = -1.0 * w[2];
+  if (C::DIM == 3 && f2) w[3] = -1.0 * w[3];
+}
+
+template <class C>
+__device__ __forceinline__ void load_gdev(const Prm &P, int i, int j, int k, double gm_[2]) {
+  const Geo &g = P.g;
+  bool f = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f) : 0;
+  long long c = lin(g, si, sj, sk);
+  gm_[0] = __ldg(P.gin + c);
+  gm_[1] = __ldg(P.gin + g.N + c);
+  if (C::WB) gm_[0] = gm_[0] - __ldg(P.eq_ge_cc + bg_cc(g, si, sj, sk));
+}
+
+template <class C>
+__device__ __forceinline__ void load_bcc(const Prm &P, int i, int j, int k, double b[3]) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
+  long long c = lin(g, si, sj, sk);
+  b[0] = __ldg(P.bcc_in + c);
+  b[1] = __ldg(P.bcc_in + g.N + c);
+  b[2] = C::DIM == 3 ? __ldg(P.bcc_in + 2 * g.N + c) : 0.0;
+  if (f0) b[0] = -1.0 * b[0];
+  if (f1) b[1] = -1.0 * b[1];
+  if (C::DIM == 3 && f2) b[2] = -1.0 * b[2];
+}
+
+// --------------------------------------------------------------------- face flux
+// Flux through the low face of cell `m` along d, given the deviation states of cells
+// m-2..m+1 (wl2, wl1, wr1, wr2 = cells m-2, m-1, m, m+1).  Implements, for one face, the body
+// of the x1/x2/x3 sweeps (source.F90:8138-9105, 9107-10301, 10303-11364).
+template <class C>
+__device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, int fk,
+                                          const double *wl2, const double *wl1, const double *wr1,
+                                          const double *wr2, const double *gl2, const double *gl1,
+                                          const double *gr1, const double *gr2, const double *bcl2,
+                                          const double *bcl1, const double *bcr1, const double *bcr2,
+                                          double F[C::NV], double Fb[3], double &rho_face_sum) {
+  constexpr int NV = C::NV, IP = C::IP;
+  const Geo &g = P.g;
+  double qL[NV], qR[NV], lo, hi;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    plm(wl2[iv], wl1[iv], wr1[iv], lo, hi);
+    qL[iv] = hi;
+    plm(wl1[iv], wr1[iv], wr2[iv], lo, hi);
+    qR[iv] = lo;
+  }
+  double bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
+  if (C::MHD) {
+#pragma unroll
+    for (int iv = 0; iv < C::DIM; ++iv) {
+      if (iv == d) continue;
+      plm(bcl2[iv], bcl1[iv], bcr1[iv], lo, hi);
+      bL[iv] = hi;
+      plm(bcl1[iv], bcr1[iv], bcr2[iv], lo, hi);
+      bR[iv] = lo;
+    }
+    double bn = P.bf[d][face_lin(g, d, fi, fj, fk)];
+    bL[d] = bn;
+    bR[d] = bn;
+  }
+  // rotation into the normal frame: x2 (v1,v2) <- (v2,-v1); x3 (v1,v2,v3) <- (v3,v1,v2)
+  if (d == 1) {
+    double a = qL[1], b = qL[2]; qL[1] = b; qL[2] = -a;
+    a = qR[1]; b = qR[2]; qR[1] = b; qR[2] = -a;
+    if (C::MHD) {
+      a = bL[0]; b = bL[1]; bL[0] = b; bL[1] = -a;
+      a = bR[0]; b = bR[1]; bR[0] = b; bR[1] = -a;
+    }
+  } else if (C::DIM == 3 && d == 2) {
+    double a = qL[1], b = qL[2], c = qL[3]; qL[1] = c; qL[2] = a; qL[3] = b;
+    a = qR[1]; b = qR[2]; c = qR[3]; qR[1] = c; qR[2] = a; qR[3] = b;
+    if (C::MHD) {
+      a = bL[0]; b = bL[1]; c = bL[2]; bL[0] = c; bL[1] = a; bL[2] = b;
+      a = bR[0]; b = bR[1]; c = bR[2]; bR[0] = c; bR[1] = a; bR[2] = b;
+    }
+  }
+  long long fb = 0;
+  if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
+  if (C::WB) {
+    double rho_eq = __ldg(P.eq_rho_f[d] + fb), p_eq = __ldg(P.eq_p_f[d] + fb);
+    qL[0] = qL[0] + rho_eq;
+    qR[0] = qR[0] + rho_eq;
+    qL[IP] = qL[IP] + p_eq;
+    qR[IP] = qR[IP] + p_eq;
+  }
+  double gL[2] = {0, 0}, gR[2] = {0, 0};
+  if (C::HELM) {
+#pragma unroll
+    for (int iv = 0; iv < 2; ++iv) {
+      plm(gl2[iv], gl1[iv], gr1[iv], lo, hi);
+      gL[iv] = hi;
+      plm(gl1[iv], gr1[iv], gr2[iv], lo, hi);
+      gR[iv] = lo;
+    }
+    if (C::WB) {
+      double ge = __ldg(P.eq_ge_f[d] + fb);
+      gL[0] = gL[0] + ge;
+      gR[0] = gR[0] + ge;
+    }
+  }
+  const double gm = P.g.gm, mc = P.g.mach_cutoff;
+  if (C::MHD) {
+    riemann_mhd<double, C::DIM, NV, C::HELM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb);
+  } else {
+    riemann_hydro<double, C::DIM, NV, C::HELM, C::RIEM>(qL, qR, gL, gR, gm, mc, F);
+  }
+  // back to the lab frame
+  if (d == 1) {
+    double a = F[1], b = F[2]; F[1] = -b; F[2] = a;
+    if (C::MHD) { a = Fb[0]; b = Fb[1]; Fb[0] = -b; Fb[1] = a; }
+  } else if (C::DIM == 3 && d == 2) {
+    double a = F[1], b = F[2], c = F[3]; F[1] = b; F[2] = c; F[3] = a;
+    if (C::MHD) { a = Fb[0]; b = Fb[1]; c = Fb[2]; Fb[0] = b; Fb[1] = c; Fb[2] = a; }
+  }
+  rho_face_sum = qL[0] + qR[0];
+  // MHD: the EMF/sign are taken before the WB momentum fix (source.F90:8926-8959)
+  if (C::WB) F[1 + d] = F[1 + d] - __ldg(P.eq_p_f[d] + fb);
+  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.phi_f[d] + fb);
+}
+
+// EMF components of a face flux and the mass-flux sign (source.F90:8926-8951)
+template <class C>
+__device__ __forceinline__ void store_face_emf(const Prm &P, int d, long long fidx, const double Fb[3],
+                                               double frho, double rho_face_sum, double smax) {
+  const Geo &g = P.g;
+  long long nf = nfaces(g, d);
+  double *e = P.emf[d];
+  if (d == 0) { if (C::DIM == 3) e[1 * nf + fidx] = Fb[2]; e[2 * nf + fidx] = -Fb[1]; }
+  if (d == 1) { if (C::DIM == 3) e[0 * nf + fidx] = -Fb[2]; e[2 * nf + fidx] = Fb[0]; }
+  if (d == 2) { e[0 * nf + fidx] = Fb[1]; e[1 * nf + fidx] = -Fb[0]; }
+  double tmp = 0.5 * rho_face_sum * smax;
+  double mach = frho / tmp, sgn = 0.0;
+  if (mach > g.mach_ct) sgn = 1.0;
+  if (mach < -g.mach_ct) sgn = -1.0;
+  P.sgnf[d][fidx] = sgn;
+}
+
+// --------------------------------------------------------------------- stage kernel
+// One thread per cell: both faces in every direction, flux divergence, gravity source, RK
+// combine; for hydro also cons->prim + EoS and (last stage) the CFL max.  For MHD the kernel
+// stops after the RK combine of U and stores face EMFs; ct/face-B/cons->prim follow.
+template <class C>
+__global__ void __launch_bounds__(128) k_stage(Prm P) {
+  if (!*P.active) return;
+  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool valid = c < g.N;
+  double smax_loc = 0.0;
+  unsigned long long n_calls = 0, n_iters = 0, n_nonconv = 0, n_clamp = 0, n_bad = 0;
+  if (valid) {
+    const int i = (int)(c % g.nx[0]);
+    const int j = (int)((c / g.nx[0]) % g.nx[1]);
+    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    const double dt = P.scal[1];
+    const double smax_prev = P.scal[2];
+    double res[NV];
+    double wc[NV];
+    load_wdev<C>(P, i, j, k, wc);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      // cells c-2..c+2 along d
+      double w[5][NV], gmv[5][2], bc[5][3];
+#pragma unroll
+      for (int s = 0; s < 5; ++s) {
+        int ii = i + (d == 0 ? s - 2 : 0), jj = j + (d == 1 ? s - 2 : 0), kk = k + (d == 2 ? s - 2 : 0);
+        load_wdev<C>(P, ii, jj, kk, w[s]);
+        if (C::HELM) load_gdev<C>(P, ii, jj, kk, gmv[s]);
+        if (C::MHD) load_bcc<C>(P, ii, jj, kk, bc[s]);
+      }
+      double Flo[NV], Fhi[NV], Fb[3], rs;
+      face_flux<C>(P, d, i, j, k, w[0], w[1], w[2], w[3], gmv[0], gmv[1], gmv[2], gmv[3], bc[0], bc[1],
+                   bc[2], bc[3], Flo, Fb, rs);
+      if (C::MHD) store_face_emf<C>(P, d, face_lin(g, d, i, j, k), Fb, Flo[0], rs, smax_prev);
+      int hi_i = i + (d == 0), hi_j = j + (d == 1), hi_k = k + (d == 2);
+      face_flux<C>(P, d, hi_i, hi_j, hi_k, w[1], w[2], w[3], w[4], gmv[1], gmv[2], gmv[3], gmv[4], bc[1],
+                   bc[2], bc[3], bc[4], Fhi, Fb, rs);
+      if (C::MHD) {
+        int hc = d == 0 ? i : (d == 1 ? j : k);
+        if (hc == g.nx[d] - 1) store_face_emf<C>(P, d, face_lin(g, d, hi_i, hi_j, hi_k), Fb, Fhi[0], rs, smax_prev);
+      }
+      const double inv_dl = g.inv_dx[d];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        double dd = (Fhi[iv] - Flo[iv]) * inv_dl;
+        res[iv] = d == 0 ? dd : res[iv] + dd;
+      }
+    }
+    if (C::GRAV) {
+      long long b = bg_cc(g, i, j, k);
+      double rho = wc[0];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) res[1 + d] = res[1 + d] - rho * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + b);
+    }
+    // state0 / state
+    double u0[NV], u[NV];
+    if (P.first_stage) {
+      double w[NV];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) w[iv] = P.Win[(long long)iv * g.N + c];
+      double rho = w[0], vx1 = w[1], vx2 = w[2], vx3 = DIM == 3 ? w[3] : 0.0;
+      u0[0] = rho;
+      u0[1] = rho * vx1;
+      u0[2] = rho * vx2;
+      if (DIM == 3) u0[3] = rho * vx3;
+      double eint = P.eint[c];
+      double rhoe = eint + 0.5 * rho * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+      if (C::MHD) {
+        double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
+        rhoe = rhoe + 0.5 * (b0 * b0 + b1 * b1 + b2 * b2);
+      }
+      if (C::ETOT) rhoe = rhoe + rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
+      u0[IP] = rhoe;
+#pragma unroll
+      for (int iv = IAS; iv < NV; ++iv) u0[iv] = rho * w[iv];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) { u[iv] = u0[iv]; P.U0[(long long)iv * g.N + c] = u0[iv]; }
+    } else {
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        u0[iv] = P.U0[(long long)iv * g.N + c];
+        u[iv] = P.U[(long long)iv * g.N + c];
+      }
+    }
+    const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      u[iv] = a1 * u0[iv] + a2 * u[iv] + a3 * res[iv];
+      P.U[(long long)iv * g.N + c] = u[iv];
+    }
+    if (!C::MHD) {
+      // cons -> prim + EoS (source.F90:13533-13686)
+      double rho = u[0], rhovx1 = u[1], rhovx2 = u[2], rhovx3 = DIM == 3 ? u[3] : 0.0, rhoe = u[IP];
+      double inv_rho = 1.0 / rho;
+      double eint = rhoe - 0.5 * (rhovx1 * rhovx1 + rhovx2 * rhovx2 + rhovx3 * rhovx3) * inv_rho;
+      if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
+      double wn[NV];
+      wn[0] = rho;
+      wn[1] = rhovx1 * inv_rho;
+      wn[2] = rhovx2 * inv_rho;
+      if (DIM == 3) wn[3] = rhovx3 * inv_rho;
+      double p, T, sound = 0.0;
+      if (C::HELM) {
+        double ye = u[IAS] * inv_rho;
+        double abar = rho / u[IAS + 1];
+        double zbar = ye * abar;
+        T = P.temp[c];
+        int clamped = 0;
+        int it = helm_rhoe_newton(P.helm, rho, eint * inv_rho, abar, zbar, T, 100, clamped);
+        n_calls += 1; n_iters += it; n_nonconv += (it == 100); n_clamp += clamped;
+        double E, cv;
+        helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
+        P.gout[c] = p / eint + 1.0;
+        P.gout[g.N + c] = sound * sound * rho / p;
+      } else {
+        p = (g.gm - 1.0) * eint;
+        T = p / (rho * CONST_RGAS * (1.0 / g.mu));
+      }
+      wn[IP] = p;
+#pragma unroll
+      for (int iv = IAS; iv < NV; ++iv) wn[iv] = u[iv] * inv_rho;
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) P.Wout[(long long)iv * g.N + c] = wn[iv];
+      P.temp[c] = T;
+      P.eint[c] = eint;
+      if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) n_bad += 1;
+      if (P.last_stage) {
+        // compute_hyperbolic_dt on the new state (source.F90:13707-13960)
+        double cs;
+        if (C::HELM) {
+          double ye = wn[IAS], abar = 1.0 / wn[IAS + 1], zbar = ye * abar, pp, ei, cv;
+          helm_given_full(P.helm, rho, T, abar, zbar, pp, ei, cs, cv);
+        } else {
+          cs = sqrt(g.gm * p / rho);
+        }
+        double sx1 = (fabs(wn[1]) + cs) * g.inv_dx[0];
+        double sx2 = (fabs(wn[2]) + cs) * g.inv_dx[1];
+        if (DIM == 3) {
+          double sx3 = (fabs(wn[3]) + cs) * g.inv_dx[2];
+          smax_loc = sx3 + sx1 + sx2;
+        } else {
+          smax_loc = sx1 + sx2;
+        }
+      }
+    }
+  }
+  if (!C::MHD) {
+    if (P.last_stage) block_max_atomic(smax_loc, P.smax_bits);
+    if (C::HELM) {
+      block_sum_atomic(n_calls, P.stat + STAT_NEWTON_CALLS);
+      block_sum_atomic(n_iters, P.stat + STAT_NEWTON_ITERS);
+      block_sum_atomic(n_nonconv, P.stat + STAT_NEWTON_NONCONV);
+      block_sum_atomic(n_clamp, P.stat + STAT_NEWTON_CLAMP);
+    }
+    block_sum_atomic(n_bad, P.stat + STAT_NONFINITE);
+  }
+}
+
+// --------------------------------------------------------------------- MHD: corner EMFs
+// Face EMF / sign of a face array along `d` at a possibly-ghost transverse index
+// (periodic wrap, or the reflective EMF BC: component == wall normal keeps its sign, the
+// others flip; source.F90:11374-11964).
+template <class C>
+__device__ __forceinline__ void face_emf_at(const Prm &P, int d, int comp, int i, int j, int k, double &e,
+                                            double &sgn) {
+  const Geo &g = P.g;
+  int c[3] = {i, j, k};
+  double fac = 1.0;
+#pragma unroll
+  for (int d2 = 0; d2 < C::DIM; ++d2) {
+    if (d2 == d) continue;
+    int n = g.nx[d2];
+    if (c[d2] < 0) {
+      if (g.bc[d2][0] == BC_PERIODIC) c[d2] += n;
+      else { c[d2] = 0; if (comp != d2) fac = -1.0 * fac; }
+    } else if (c[d2] >= n) {
+      if (g.bc[d2][1] == BC_PERIODIC) c[d2] -= n;
+      else { c[d2] = n - 1; if (comp != d2) fac = -1.0 * fac; }
+    }
+  }
+  long long f = face_lin(g, d, c[0], c[1], c[2]);
+  e = fac * P.emf[d][(long long)comp * nfaces(g, d) + f];
+  sgn = P.sgnf[d][f];
+}
+
+template <class C>
+__device__ __forceinline__ double emf_cell(const Prm &P, int a, int i, int j, int k) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
+  long long c = lin(g, si, sj, sk);
+  double v[3], b[3];
+  v[0] = P.Win[g.N + c];
+  v[1] = P.Win[2 * g.N + c];
+  v[2] = C::DIM == 3 ? P.Win[3 * g.N + c] : 0.0;
+  b[0] = P.bcc_in[c];
+  b[1] = P.bcc_in[g.N + c];
+  b[2] = C::DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
+  if (f0) { v[0] = -1.0 * v[0]; b[0] = -1.0 * b[0]; }
+  if (f1) { v[1] = -1.0 * v[1]; b[1] = -1.0 * b[1]; }
+  if (f2) { v[2] = -1.0 * v[2]; b[2] = -1.0 * b[2]; }
+  if (a == 2) return -v[0] * b[1] + v[1] * b[0];
+  if (a == 0) return v[2] * b[1] - v[1] * b[2];
+  return v[0] * b[2] - v[2] * b[0];
+}
+
+// corner EMF along axis a (source.F90:11966-12206); one thread per corner
+template <class C>
+__global__ void __launch_bounds__(256) k_corner(Prm P, int a) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  int pa, qa;
+  if (a == 2) { pa = 0; qa = 1; } else if (a == 0) { pa = 1; qa = 2; } else { pa = 2; qa = 0; }
+  int n0 = g.nx[0] + (a != 0), n1 = g.nx[1] + (a != 1), n2 = C::DIM == 3 ? g.nx[2] + (a != 2) : 1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n0 * n1 * n2) return;
+  int c[3];
+  c[0] = (int)(t % n0);
+  c[1] = (int)((t / n0) % n1);
+  c[2] = (int)(t / ((long long)n0 * n1));
+  int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
+  int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
+  int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
+  double emf_N, emf_E, emf_S, emf_W, s_dummy;
+  double sgS, sgN, sgW, sgE;
+  face_emf_at<C>(P, pa, a, c[0], c[1], c[2], emf_N, sgN);
+  face_emf_at<C>(P, qa, a, c[0], c[1], c[2], emf_E, sgE);
+  face_emf_at<C>(P, pa, a, cqm[0], cqm[1], cqm[2], emf_S, sgS);
+  face_emf_at<C>(P, qa, a, cpm[0], cpm[1], cpm[2], emf_W, sgW);
+  (void)s_dummy;
+  double emf_SW = emf_cell<C>(P, a, cpq[0], cpq[1], cpq[2]);
+  double emf_NW = emf_cell<C>(P, a, cpm[0], cpm[1], cpm[2]);
+  double emf_NE = emf_cell<C>(P, a, c[0], c[1], c[2]);
+  double emf_SE = emf_cell<C>(P, a, cqm[0], cqm[1], cqm[2]);
+  double sgn = sgS;
+  double demf_S = 0.5 * (1.0 + sgn) * (emf_W - emf_SW) + 0.5 * (1.0 - sgn) * (emf_E - emf_SE);
+  sgn = sgN;
+  double demf_N = 0.5 * (1.0 + sgn) * (emf_NW - emf_W) + 0.5 * (1.0 - sgn) * (emf_NE - emf_E);
+  sgn = sgW;
+  double demf_W = 0.5 * (1.0 + sgn) * (emf_S - emf_SW) + 0.5 * (1.0 - sgn) * (emf_N - emf_NW);
+  sgn = sgE;
+  double demf_E = 0.5 * (1.0 + sgn) * (emf_SE - emf_S) + 0.5 * (1.0 - sgn) * (emf_NE - emf_N);
+  P.cor[a][t] = 0.25 * (emf_S + emf_W + emf_N + emf_E + demf_S - demf_N + demf_W - demf_E);
+}
+
+__device__ __forceinline__ long long cor_lin(const Geo &g, int a, int i, int j, int k) {
+  long long n0 = g.nx[0] + (a != 0), n1 = g.nx[1] + (a != 1);
+  return (long long)i + n0 * ((long long)j + n1 * (long long)k);
+}
+
+// face-B update (source.F90:12208-12437); one thread per face of direction d
+template <class C>
+__global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  long long nf = nfaces(g, d);
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  int i = (int)(t % n0), j = (int)((t / n0) % n1), k = (int)(t / ((long long)n0 * n1));
+  const double dt = P.scal[1];
+  const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+  const double *E1 = P.cor[0], *E2 = P.cor[1], *E3 = P.cor[2];
+  double tmp;
+  if (d == 0) {
+    if (C::DIM == 2) tmp = (E3[cor_lin(g, 2, i, j + 1, k)] - E3[cor_lin(g, 2, i, j, k)]) * g.inv_dx[1];
+    else tmp = -(E2[cor_lin(g, 1, i, j, k + 1)] - E2[cor_lin(g, 1, i, j, k)]) * g.inv_dx[2] +
+               (E3[cor_lin(g, 2, i, j + 1, k)] - E3[cor_lin(g, 2, i, j, k)]) * g.inv_dx[1];
+  } else if (d == 1) {
+    if (C::DIM == 2) tmp = (E3[cor_lin(g, 2, i, j, k)] - E3[cor_lin(g, 2, i + 1, j, k)]) * g.inv_dx[0];
+    else tmp = (E1[cor_lin(g, 0, i, j, k + 1)] - E1[cor_lin(g, 0, i, j, k)]) * g.inv_dx[2] +
+               (E3[cor_lin(g, 2, i, j, k)] - E3[cor_lin(g, 2, i + 1, j, k)]) * g.inv_dx[0];
+  } else {
+    tmp = (E2[cor_lin(g, 1, i + 1, j, k)] - E2[cor_lin(g, 1, i, j, k)]) * g.inv_dx[0] -
+          (E1[cor_lin(g, 0, i, j + 1, k)] - E1[cor_lin(g, 0, i, j, k)]) * g.inv_dx[1];
+  }
+  double b = P.bf[d][t];
+  double b0;
+  if (P.first_stage) { b0 = b; P.b0f[d][t] = b; } else { b0 = P.b0f[d][t]; }
+  P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
+}
+
+// MHD cons->prim: b_cc from the updated faces, then the EoS (source.F90:12439-12487,
+// 13533-13686), last stage also the CFL max
+template <class C>
+__global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
+  if (!*P.active) return;
+  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double smax_loc = 0.0;
+  unsigned long long n_calls = 0, n_iters = 0, n_nonconv = 0, n_clamp = 0, n_bad = 0;
+  if (c < g.N) {
+    const int i = (int)(c % g.nx[0]);
+    const int j = (int)((c / g.nx[0]) % g.nx[1]);
+    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    double bcc[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
+      bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+      P.bcc_out[(long long)d * g.N + c] = bcc[d];
+    }
+    double u[NV];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) u[iv] = P.U[(long long)iv * g.N + c];
+    double rho = u[0], rhovx1 = u[1], rhovx2 = u[2], rhovx3 = DIM == 3 ? u[3] : 0.0, rhoe = u[IP];
+    double inv_rho = 1.0 / rho;
+    double eint = rhoe - 0.5 * (rhovx1 * rhovx1 + rhovx2 * rhovx2 + rhovx3 * rhovx3) * inv_rho;
+    eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
+    if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
+    double wn[NV];
+    wn[0] = rho;
+    wn[1] = rhovx1 * inv_rho;
+    wn[2] = rhovx2 * inv_rho;
+    if (DIM == 3) wn[3] = rhovx3 * inv_rho;
+    double p, T, sound = 0.0;
+    if (C::HELM) {
+      double ye = u[IAS] * inv_rho;
+      double abar = rho / u[IAS + 1];
+      double zbar = ye * abar;
+      T = P.temp[c];
+      int clamped = 0;
+      int it = helm_rhoe_newton(P.helm, rho, eint * inv_rho, abar, zbar, T, 100, clamped);
+      n_calls += 1; n_iters += it; n_nonconv += (it == 100); n_clamp += clamped;
+      double E, cv;
+      helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
+      P.gout[c] = p / eint + 1.0;
+      P.gout[g.N + c] = sound * sound * rho / p;
+    } else {
+      p = (g.gm - 1.0) * eint;
+      T = p / (rho * CONST_RGAS * (1.0 / g.mu));
+    }
+    wn[IP] = p;
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) wn[iv] = u[iv] * inv_rho;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) P.Wout[(long long)iv * g.N + c] = wn[iv];
+    P.temp[c] = T;
+    P.eint[c] = eint;
+    if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) n_bad += 1;
+    if (P.last_stage) {
+      double cs;
+      if (C::HELM) {
+        double ye = wn[IAS], abar = 1.0 / wn[IAS + 1], zbar = ye * abar, pp, ei, cv;
+        helm_given_full(P.helm, rho, T, abar, zbar, pp, ei, cs, cv);
+      } else {
+        cs = sqrt(g.gm * p / rho);
+      }
+      double ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
+      cs = sqrt(cs * cs + ca2 / rho);
+      double sx1 = (fabs(wn[1]) + cs) * g.inv_dx[0];
+      double sx2 = (fabs(wn[2]) + cs) * g.inv_dx[1];
+      if (DIM == 3) {
+        double sx3 = (fabs(wn[3]) + cs) * g.inv_dx[2];
+        smax_loc = sx3 + sx1 + sx2;
+      } else {
+        smax_loc = sx1 + sx2;
+      }
+    }
+  }
+  if (P.last_stage) block_max_atomic(smax_loc, P.smax_bits);
+  if (C::HELM) {
+    block_sum_atomic(n_calls, P.stat + STAT_NEWTON_CALLS);
+    block_sum_atomic(n_iters, P.stat + STAT_NEWTON_ITERS);
+    block_sum_atomic(n_nonconv, P.stat + STAT_NEWTON_NONCONV);
+    block_sum_atomic(n_clamp, P.stat + STAT_NEWTON_CLAMP);
+  }
+  block_sum_atomic(n_bad, P.stat + STAT_NONFINITE);
+}
+
+// --------------------------------------------------------------------- dt (step 0)
+template <class C>
+__global__ void __launch_bounds__(256) k_dt(Prm P) {
+  constexpr int IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (c < g.N) {
+    const double *W = P.Win;
+    double rho = W[c], vx1 = W[g.N + c], vx2 = W[2 * g.N + c], vx3 = DIM == 3 ? W[3 * g.N + c] : 0.0;
+    double p = W[(long long)IP * g.N + c], cs;
+    if (C::HELM) {
+      double ye = W[(long long)IAS * g.N + c], abar = 1.0 / W[(long long)(IAS + 1) * g.N + c];
+      double zbar = ye * abar, T = P.temp[c], ei, cv;
+      helm_given_full(P.helm, rho, T, abar, zbar, p, ei, cs, cv);
+    } else {
+      cs = sqrt(g.gm * p / rho);
+    }
+    if (C::MHD) {
+      double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
+      double ca2 = b0 * b0 + b1 * b1 + b2 * b2;
+      cs = sqrt(cs * cs + ca2 / rho);
+    }
+    double sx1 = (fabs(vx1) + cs) * g.inv_dx[0];
+    double sx2 = (fabs(vx2) + cs) * g.inv_dx[1];
+    if (DIM == 3) {
+      double sx3 = (fabs(vx3) + cs) * g.inv_dx[2];
+      s = sx3 + sx1 + sx2;
+    } else {
+      s = sx1 + sx2;
+    }
+  }
+  block_max_atomic(s, P.smax_bits);
+}
+
+// step-0 thermodynamics (source.F90:6271-6383) and b_cc from faces (source.F90:6012-6062)
+template <class C>
+__global__ void __launch_bounds__(128) k_init_thermo(Prm P) {
+  constexpr int IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.N) return;
+  const int i = (int)(c % g.nx[0]);
+  const int j = (int)((c / g.nx[0]) % g.nx[1]);
+  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+  if (C::MHD) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
+      P.bcc_out[(long long)d * g.N + c] =
+          0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+    }
+  }
+  const double *W = P.Win;
+  double rho = W[c], p = W[(long long)IP * g.N + c], eint, T;
+  if (C::HELM) {
+    double abar = 1.0 / W[(long long)(IAS + 1) * g.N + c];
+    double ye = W[(long long)IAS * g.N + c];
+    double zbar = abar * ye, sound, cv, Pdummy;
+    T = P.temp[c];
+    int clamped = 0;
+    helm_rhoP_newton(P.helm, rho, p, abar, zbar, T, clamped);
+    helm_given_full(P.helm, rho, T, abar, zbar, Pdummy, eint, sound, cv);
+    eint = rho * eint;
+    P.gout[c] = p / eint + 1.0;
+    P.gout[g.N + c] = sound * sound * rho / p;
+  } else {
+    T = p / (CONST_RGAS * rho * (1.0 / g.mu));
+    eint = p * (1.0 / (g.gm - 1.0));
+  }
+  P.eint[c] = eint;
+  P.temp[c] = T;
+}
+
+}  // namespace phl

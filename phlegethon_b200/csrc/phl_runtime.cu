@@ -1,0 +1,844 @@
+// phl_runtime.cu -- host runtime and C ABI (include/phl_gpu.h) of the B200 explicit FV step.
+//
+// One context = one device-resident domain on one stream.  The reference-layout host arrays
+// (Fortran order, ghosts included) are staged to the device in one copy each and transposed
+// by kernels into the SoA layout of phl_kernels.cuh.  Steps run as CUDA graphs with dt, time and
+// the CFL maximum kept on the device (time_loop body, source/source.F90:6525-6748).
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/phl_gpu.h"
+#include "phl_kernels.cuh"
+#include "phl_eos_batch.cuh"
+
+using namespace phl;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+      return PHL_E_CUDA;                                                              \
+    }                                                                                 \
+  } while (0)
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ----------------------------------------------------------------------------- runners
+struct Runner {
+  virtual ~Runner() {}
+  virtual void stage(const Prm &P, cudaStream_t s) = 0;
+  virtual void dt(const Prm &P, cudaStream_t s) = 0;
+  virtual void init_thermo(const Prm &P, cudaStream_t s) = 0;
+};
+
+template <class C>
+struct RunnerT : Runner {
+  void stage(const Prm &P, cudaStream_t s) override {
+    const Geo &g = P.g;
+    k_stage<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+    if (C::MHD) {
+      for (int a = 0; a < 3; ++a) {
+        if (C::DIM == 2 && a != 2) continue;
+        long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) *
+                      (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
+        k_corner<C><<<nblk(n, 256), 256, 0, s>>>(P, a);
+      }
+      for (int d = 0; d < C::DIM; ++d) k_bface<C><<<nblk(nfaces_host(g, d), 256), 256, 0, s>>>(P, d);
+      k_c2p_mhd<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+    }
+  }
+  void dt(const Prm &P, cudaStream_t s) override { k_dt<C><<<nblk(P.g.N, 256), 256, 0, s>>>(P); }
+  void init_thermo(const Prm &P, cudaStream_t s) override {
+    k_init_thermo<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P);
+  }
+  static long long nfaces_host(const Geo &g, int d) {
+    return (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
+  }
+};
+
+// Instantiated option sets: (dims, nvars, MHD, Helmholtz+FASTEOS, stratified = WB+ETOT+gravity,
+// Riemann solver).  Other combinations return PHL_E_UNSUPPORTED.
+#define PHL_RUNNER_LIST(X)                 \
+  X(2, 4, false, false, false, R_LHLLC)    \
+  X(2, 4, false, false, false, R_HLLC)     \
+  X(2, 4, false, false, true, R_LHLLC)     \
+  X(2, 4, false, false, true, R_HLLC)      \
+  X(2, 4, true, false, false, R_HLLD)      \
+  X(2, 4, true, false, false, R_LHLLD)     \
+  X(2, 6, false, true, true, R_LHLLC)      \
+  X(2, 6, true, true, true, R_LHLLD)       \
+  X(3, 5, false, false, false, R_LHLLC)    \
+  X(3, 5, false, false, false, R_HLLC)     \
+  X(3, 5, true, false, false, R_HLLD)      \
+  X(3, 5, true, false, false, R_LHLLD)     \
+  X(3, 7, false, true, true, R_LHLLC)      \
+  X(3, 7, false, true, true, R_HLLC)       \
+  X(3, 7, true, true, true, R_LHLLD)       \
+  X(3, 7, true, true, true, R_HLLD)
+
+Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem) {
+#define X(D, N, M, H, S, R)                                                              \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R)           \
+    return new RunnerT<Cfg<D, N, M, H, S, S, S, R>>();
+  PHL_RUNNER_LIST(X)
+#undef X
+  return nullptr;
+}
+
+// ----------------------------------------------------------------------------- transposes
+// host reference layout (nv, n1g, n2g, n3g) with ghost offsets -> SoA interior [nv][N]
+__global__ void k_unpack(const double *src, double *dst, int nv, int nx, int ny, int nz, int n1, int n2,
+                         int o1, int o2, int o3, int ncomp, long long dst_stride) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long N = (long long)nx * ny * nz;
+  if (c >= N) return;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+  long long s = (long long)nv * ((long long)(i + o1) + (long long)n1 * ((long long)(j + o2) + (long long)n2 * (k + o3)));
+  for (int iv = 0; iv < ncomp; ++iv) dst[(long long)iv * dst_stride + c] = src[s + iv];
+}
+__global__ void k_pack(const double *src, double *dst, int nv, int nx, int ny, int nz, int n1, int n2, int o1,
+                       int o2, int o3, int ncomp, long long src_stride) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long N = (long long)nx * ny * nz;
+  if (c >= N) return;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+  long long s = (long long)nv * ((long long)(i + o1) + (long long)n1 * ((long long)(j + o2) + (long long)n2 * (k + o3)));
+  for (int iv = 0; iv < ncomp; ++iv) dst[s + iv] = src[(long long)iv * src_stride + c];
+}
+
+// per-step scalar bookkeeping (time_loop, source.F90:6662-6664, 6710, 6716)
+__global__ void k_pre_step(double *scal, int *active, unsigned long long *smax_bits, long long *step,
+                           long long step_limit) {
+  double time = scal[0], dt = scal[1], tmax = scal[3];
+  int a = (time < tmax) && (*step < step_limit);
+  *active = a;
+  if (!a) return;
+  if ((time + dt) > tmax) scal[1] = tmax - time;
+  *smax_bits = 0ull;
+}
+__global__ void k_post_step(double *scal, const int *active, const unsigned long long *smax_bits,
+                            long long *step, double cfl) {
+  if (!*active) return;
+  scal[0] = scal[0] + scal[1];
+  double smax = __longlong_as_double((long long)*smax_bits);
+  scal[2] = smax;
+  scal[1] = cfl / smax;
+  *step = *step + 1;
+}
+__global__ void k_set_active(int *active, unsigned long long *smax_bits) {
+  *active = 1;
+  *smax_bits = 0ull;
+}
+__global__ void k_finish_dt(double *scal, const unsigned long long *smax_bits, double cfl) {
+  double smax = __longlong_as_double((long long)*smax_bits);
+  scal[2] = smax;
+  scal[1] = cfl / smax;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------- context
+struct phl_ctx {
+  phl_config cfg;
+  Geo geo;
+  std::unique_ptr<Runner> runner;
+  cudaStream_t stream = nullptr;
+  int dim = 2, nv = 0;
+  long long N = 0;
+  // dynamic
+  double *W[2] = {nullptr, nullptr}, *gam[2] = {nullptr, nullptr};
+  int cur = 0;
+  double *U = nullptr, *U0 = nullptr, *eint = nullptr, *temp = nullptr;
+  double *bcc = nullptr;
+  double *bf[3] = {}, *b0f[3] = {}, *emf[3] = {}, *sgnf[3] = {}, *cor[3] = {};
+  // background
+  int bg_profile = 0;
+  double *eq_rho_cc = nullptr, *eq_p_cc = nullptr, *eq_ge_cc = nullptr, *phi_cc = nullptr, *grav = nullptr;
+  double *eq_rho_f[3] = {}, *eq_p_f[3] = {}, *eq_ge_f[3] = {}, *phi_f[3] = {};
+  // scalars
+  double *scal = nullptr;
+  unsigned long long *smax_bits = nullptr;
+  int *active = nullptr;
+  long long *step = nullptr;
+  unsigned long long *stat = nullptr;
+  // table
+  double *htab = nullptr, *hdpd = nullptr, *hrho = nullptr, *hT = nullptr;
+  HelmTable helm{};
+  bool table_loaded = false, uploaded = false, bg_uploaded = false;
+  // staging
+  double *stage_buf = nullptr;
+  size_t stage_bytes = 0;
+  // graphs: one per parity of the W ping-pong
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // EoS batch scratch and MLP
+  EosBatch eos;
+  std::vector<void *> allocs;
+
+  ~phl_ctx() {
+    for (int p = 0; p < 2; ++p)
+      if (graph[p]) cudaGraphExecDestroy(graph[p]);
+    eos.release();
+    for (void *a : allocs) cudaFree(a);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  template <class T>
+  int alloc(T **p, size_t count) {
+    void *q = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+      g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return PHL_E_CUDA;
+    }
+    cudaMemsetAsync(q, 0, count * sizeof(T), stream);
+    allocs.push_back(q);
+    *p = (T *)q;
+    return PHL_OK;
+  }
+  long long nfaces(int d) const {
+    return (long long)(geo.nx[0] + (d == 0)) * (geo.nx[1] + (d == 1)) * (geo.nx[2] + (d == 2));
+  }
+  long long ncor(int a) const {
+    return (long long)(geo.nx[0] + (a != 0)) * (geo.nx[1] + (a != 1)) * (dim == 3 ? geo.nx[2] + (a != 2) : 1);
+  }
+  int ensure_stage(size_t bytes) {
+    if (bytes <= stage_bytes) return PHL_OK;
+    if (stage_buf) cudaFree(stage_buf);
+    stage_buf = nullptr;
+    CK(cudaMalloc(&stage_buf, bytes));
+    stage_bytes = bytes;
+    return PHL_OK;
+  }
+  Prm prm(int stage_idx) const {
+    Prm P;
+    memset(&P, 0, sizeof(P));
+    P.g = geo;
+    int in = (cur + stage_idx) & 1;
+    P.Win = W[in];
+    P.Wout = W[in ^ 1];
+    P.gin = gam[in];
+    P.gout = gam[in ^ 1];
+    P.U = U;
+    P.U0 = U0;
+    P.eint = eint;
+    P.temp = temp;
+    P.eq_rho_cc = eq_rho_cc; P.eq_p_cc = eq_p_cc; P.eq_ge_cc = eq_ge_cc; P.phi_cc = phi_cc; P.grav = grav;
+    for (int d = 0; d < 3; ++d) {
+      P.eq_rho_f[d] = eq_rho_f[d]; P.eq_p_f[d] = eq_p_f[d]; P.eq_ge_f[d] = eq_ge_f[d]; P.phi_f[d] = phi_f[d];
+      P.bf[d] = bf[d]; P.b0f[d] = b0f[d]; P.emf[d] = emf[d]; P.sgnf[d] = sgnf[d]; P.cor[d] = cor[d];
+    }
+    P.bcc_in = bcc;
+    P.bcc_out = bcc;
+    P.scal = scal;
+    P.smax_bits = smax_bits;
+    P.active = active;
+    P.stat = stat;
+    P.helm = helm;
+    double rk[3][3] = {{1.0, 0.0, -1.0}, {0.75, 0.25, -0.25}, {1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0)}};
+    if (cfg.rk_stages == 2) {
+      rk[1][0] = 0.5; rk[1][1] = 0.5; rk[1][2] = -0.5;
+    }
+    P.a1 = rk[stage_idx][0];
+    P.a2 = rk[stage_idx][1];
+    P.c3 = rk[stage_idx][2];
+    P.first_stage = stage_idx == 0;
+    P.last_stage = stage_idx == cfg.rk_stages - 1;
+    return P;
+  }
+  // hydro_step: all RK stages starting from W[cur]
+  void launch_stages() {
+    for (int s = 0; s < cfg.rk_stages; ++s) runner->stage(prm(s), stream);
+  }
+};
+
+namespace {
+
+int check_cfg(const phl_config *c) {
+  if (!c || c->abi_version != PHL_ABI_VERSION) return PHL_E_INVALID;
+  if (c->sdims != 2 && c->sdims != 3) return PHL_E_INVALID;
+  if (c->nx1 < 4 || c->nx2 < 4 || c->nx3 < 1) return PHL_E_INVALID;
+  if (c->sdims == 2 && c->nx3 != 1) return PHL_E_INVALID;
+  if (c->sdims == 3 && c->nx3 < 4) return PHL_E_INVALID;
+  if (c->ngc < 2) return PHL_E_INVALID;
+  if (c->nvars != 2 + c->sdims + c->nas) return PHL_E_INVALID;
+  if (c->rk_stages != 2 && c->rk_stages != 3) return PHL_E_INVALID;
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s)
+      if (c->bc[d][s] != PHL_BC_PERIODIC && c->bc[d][s] != PHL_BC_REFLECTIVE) return PHL_E_INVALID;
+  for (int d = 0; d < c->sdims; ++d)
+    if ((c->bc[d][0] == PHL_BC_PERIODIC) != (c->bc[d][1] == PHL_BC_PERIODIC)) return PHL_E_INVALID;
+  bool mhd = c->flags & PHL_MHD, helm = c->flags & PHL_HELMHOLTZ;
+  if (mhd && (c->riemann != PHL_HLLD && c->riemann != PHL_LHLLD)) return PHL_E_INVALID;
+  if (!mhd && (c->riemann != PHL_LHLLC && c->riemann != PHL_HLLC)) return PHL_E_INVALID;
+  if (helm && !((c->flags & PHL_FASTEOS) && (c->flags & PHL_ADVECT_YE_IABAR) && c->nas >= 2))
+    return PHL_E_UNSUPPORTED;
+  if (c->precision != PHL_FP64 && c->precision != PHL_FP32_SPLIT) return PHL_E_INVALID;
+  return PHL_OK;
+}
+
+// A background array (nv comps with a component index `comp`) is a profile along x2 when all
+// its interior values agree along x1 and x3 for every x2 index.  On success fills prof[0..n2).
+bool extract_profile(const double *a, int nv, int comp, int n1, int n2, int n3, int o1, int o2, int o3,
+                     int ld1, int ld2, int nj, std::vector<double> &prof) {
+  prof.assign(nj, 0.0);
+  for (int j = 0; j < nj; ++j) {
+    double ref = a[(size_t)nv * ((size_t)(0 + o1) + (size_t)ld1 * ((size_t)(j + o2) + (size_t)ld2 * (0 + o3))) + comp];
+    for (int k = 0; k < n3; ++k)
+      for (int i = 0; i < n1; ++i) {
+        double v = a[(size_t)nv * ((size_t)(i + o1) + (size_t)ld1 * ((size_t)(j + o2) + (size_t)ld2 * (k + o3))) + comp];
+        if (!(v == ref) && !(std::isnan(v) && std::isnan(ref))) return false;
+      }
+    prof[j] = ref;
+  }
+  (void)n2;
+  return true;
+}
+
+}  // namespace
+
+// =============================================================================== C ABI
+extern "C" {
+
+int phl_abi_version(void) { return PHL_ABI_VERSION; }
+
+const char *phl_error_string(int code) {
+  if (!g_last_error.empty() && code == PHL_E_CUDA) return g_last_error.c_str();
+  switch (code) {
+    case PHL_OK: return "ok";
+    case PHL_E_INVALID: return "invalid argument or option combination";
+    case PHL_E_CUDA: return "CUDA error";
+    case PHL_E_NO_TABLE: return "Helmholtz table not loaded";
+    case PHL_E_STATE: return "call out of order";
+    case PHL_E_NO_DEVICE: return "no usable CUDA device";
+    case PHL_E_UNSUPPORTED: return "option combination not built";
+    case PHL_E_TOO_LARGE: return "size beyond capacity";
+  }
+  return "unknown error";
+}
+
+int phl_init(const phl_config *cfg, phl_ctx **out) {
+  if (!out) return PHL_E_INVALID;
+  *out = nullptr;
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) {
+    g_last_error = "no CUDA device";
+    return PHL_E_NO_DEVICE;
+  }
+  CK(cudaSetDevice(cfg->device));
+  std::unique_ptr<phl_ctx> c(new phl_ctx());
+  c->cfg = *cfg;
+  c->dim = cfg->sdims;
+  c->nv = cfg->nvars;
+  bool mhd = cfg->flags & PHL_MHD, helm = cfg->flags & PHL_HELMHOLTZ;
+  bool wb = cfg->flags & PHL_WB, etot = cfg->flags & PHL_EVOLVE_ETOT, grav = cfg->flags & PHL_GRAVITY;
+  if (!(wb == etot && etot == grav)) return PHL_E_UNSUPPORTED;
+  if (cfg->precision != PHL_FP64) return PHL_E_UNSUPPORTED;
+  c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+  if (!c->runner) return PHL_E_UNSUPPORTED;
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  Geo &g = c->geo;
+  memset(&g, 0, sizeof(g));
+  g.sdims = cfg->sdims;
+  g.nx[0] = cfg->nx1; g.nx[1] = cfg->nx2; g.nx[2] = cfg->nx3;
+  g.N = (long long)cfg->nx1 * cfg->nx2 * cfg->nx3;
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s) g.bc[d][s] = cfg->bc[d][s];
+  // dx as initialize_simulation (source.F90:1717-1735)
+  double dx1 = (cfg->x1u - cfg->x1l) / (double)cfg->nx1;
+  double dx2 = (cfg->x2u - cfg->x2l) / (double)cfg->nx2;
+  double dx3 = (cfg->x3u - cfg->x3l) / (double)cfg->nx3;
+  g.inv_dx[0] = 1.0 / dx1; g.inv_dx[1] = 1.0 / dx2; g.inv_dx[2] = cfg->sdims == 3 ? 1.0 / dx3 : 0.0;
+  g.gm = cfg->gamma_ad; g.mu = cfg->mu; g.cfl = cfg->cfl;
+  g.mach_cutoff = cfg->mach_cutoff; g.mach_ct = cfg->mach_ct;
+  c->N = g.N;
+  long long N = g.N;
+  int nv = cfg->nvars;
+  if ((rc = c->alloc(&c->W[0], (size_t)nv * N))) return rc;
+  if ((rc = c->alloc(&c->W[1], (size_t)nv * N))) return rc;
+  if ((rc = c->alloc(&c->U, (size_t)nv * N))) return rc;
+  if ((rc = c->alloc(&c->U0, (size_t)nv * N))) return rc;
+  if ((rc = c->alloc(&c->eint, (size_t)N))) return rc;
+  if ((rc = c->alloc(&c->temp, (size_t)N))) return rc;
+  if (helm) {
+    if ((rc = c->alloc(&c->gam[0], (size_t)2 * N))) return rc;
+    if ((rc = c->alloc(&c->gam[1], (size_t)2 * N))) return rc;
+  }
+  if (mhd) {
+    if ((rc = c->alloc(&c->bcc, (size_t)3 * N))) return rc;
+    for (int d = 0; d < cfg->sdims; ++d) {
+      long long nf = c->nfaces(d);
+      if ((rc = c->alloc(&c->bf[d], (size_t)nf))) return rc;
+      if ((rc = c->alloc(&c->b0f[d], (size_t)nf))) return rc;
+      if ((rc = c->alloc(&c->emf[d], (size_t)3 * nf))) return rc;
+      if ((rc = c->alloc(&c->sgnf[d], (size_t)nf))) return rc;
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (cfg->sdims == 2 && a != 2) continue;
+      if ((rc = c->alloc(&c->cor[a], (size_t)c->ncor(a)))) return rc;
+    }
+  }
+  if ((rc = c->alloc(&c->scal, 8))) return rc;
+  if ((rc = c->alloc(&c->smax_bits, 1))) return rc;
+  if ((rc = c->alloc(&c->active, 1))) return rc;
+  if ((rc = c->alloc(&c->step, 1))) return rc;
+  if ((rc = c->alloc(&c->stat, STAT_COUNT))) return rc;
+  k_set_active<<<1, 1, 0, c->stream>>>(c->active, c->smax_bits);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  *out = c.release();
+  return PHL_OK;
+}
+
+void phl_finalize(phl_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->cfg.device);
+  cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+}
+
+int phl_load_helm_table(phl_ctx *ctx, const double *tab, const double *dpdr) {
+  if (!ctx || !tab || !dpdr) return PHL_E_INVALID;
+  const phl_config &c = ctx->cfg;
+  int nr = c.helm_nrho, nT = c.helm_nT;
+  if (nr < 2 || nT < 2) return PHL_E_INVALID;
+  CK(cudaSetDevice(c.device));
+  int rc;
+  if (!ctx->htab) {
+    if ((rc = ctx->alloc(&ctx->htab, (size_t)9 * nr * nT))) return rc;
+    if ((rc = ctx->alloc(&ctx->hdpd, (size_t)4 * nr * nT))) return rc;
+    if ((rc = ctx->alloc(&ctx->hrho, (size_t)nr))) return rc;
+    if ((rc = ctx->alloc(&ctx->hT, (size_t)nT))) return rc;
+  }
+  // nodes as load_helm_table builds them (source.F90:23091-23104)
+  double dT = (c.helm_lthi - c.helm_ltlo) / (double)(nT - 1);
+  double drho = (c.helm_ldhi - c.helm_ldlo) / (double)(nr - 1);
+  std::vector<double> T(nT), rho(nr);
+  for (int j = 0; j < nT; ++j) T[j] = std::pow(10.0, c.helm_ltlo + (double)j * dT);
+  for (int i = 0; i < nr; ++i) rho[i] = std::pow(10.0, c.helm_ldlo + (double)i * drho);
+  CK(cudaMemcpyAsync(ctx->htab, tab, sizeof(double) * 9 * nr * nT, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hdpd, dpdr, sizeof(double) * 4 * nr * nT, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hrho, rho.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hT, T.data(), sizeof(double) * nT, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  HelmTable &h = ctx->helm;
+  h.tab = ctx->htab; h.dpdr = ctx->hdpd; h.rho = ctx->hrho; h.T = ctx->hT;
+  h.nrho = nr; h.nT = nT; h.drho = drho; h.dT = dT;
+  h.log10_rho1 = std::log10(rho[0]);
+  h.log10_T1 = std::log10(T[0]);
+  h.Tl = std::pow(10.0, c.helm_ltlo);
+  h.Th = std::pow(10.0, c.helm_lthi);
+  ctx->table_loaded = true;
+  return PHL_OK;
+}
+
+int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
+  if (!ctx || !f || !f->prim) return PHL_E_INVALID;
+  const phl_config &c = ctx->cfg;
+  CK(cudaSetDevice(c.device));
+  cudaStream_t s = ctx->stream;
+  const int G = c.ngc, G3 = c.sdims == 3 ? c.ngc : 0, sd = c.sdims, nv = c.nvars;
+  const int nx = c.nx1, ny = c.nx2, nz = c.nx3;
+  const int n1 = nx + 2 * G, n2 = ny + 2 * G, n3 = nz + 2 * G3;
+  const long long Ng = (long long)n1 * n2 * n3, N = ctx->N;
+  bool mhd = c.flags & PHL_MHD, helm = c.flags & PHL_HELMHOLTZ, strat = c.flags & PHL_WB;
+  int rc;
+  if ((rc = ctx->ensure_stage(sizeof(double) * (size_t)std::max<long long>(Ng * std::max(nv, 3), 1)))) return rc;
+  auto unpack_cell = [&](const double *h, int ncomp_host, int ncomp, double *dst) -> int {
+    CK(cudaMemcpyAsync(ctx->stage_buf, h, sizeof(double) * (size_t)ncomp_host * Ng, cudaMemcpyHostToDevice, s));
+    k_unpack<<<nblk(N, 256), 256, 0, s>>>(ctx->stage_buf, dst, ncomp_host, nx, ny, nz, n1, n2, G, G, G3, ncomp, N);
+    CK(cudaGetLastError());
+    return PHL_OK;
+  };
+  ctx->cur = 0;
+  if ((rc = unpack_cell(f->prim, nv, nv, ctx->W[0]))) return rc;
+  if (f->temp && (rc = unpack_cell(f->temp, 1, 1, ctx->temp))) return rc;
+  if (f->eint && (rc = unpack_cell(f->eint, 1, 1, ctx->eint))) return rc;
+  if (helm && f->gammaf && (rc = unpack_cell(f->gammaf, 2, 2, ctx->gam[0]))) return rc;
+  if (mhd && f->b_cc && (rc = unpack_cell(f->b_cc, sd, sd, ctx->bcc))) return rc;
+  if (mhd) {
+    // interior faces of b_x1(lx1-1:ux1+2, lx2-1:ux2+1, lx3-1:ux3+1), ...
+    for (int d = 0; d < sd; ++d) {
+      if (!f->b_x[d]) return PHL_E_INVALID;
+      int b1 = nx + 2 + (d == 0), b2 = ny + 2 + (d == 1), b3 = sd == 3 ? nz + 2 + (d == 2) : 1;
+      int o3 = sd == 3 ? 1 : 0;
+      long long nb = (long long)b1 * b2 * b3;
+      CK(cudaMemcpyAsync(ctx->stage_buf, f->b_x[d], sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+      k_unpack<<<nblk(ctx->nfaces(d), 256), 256, 0, s>>>(ctx->stage_buf, ctx->bf[d], 1, nx + (d == 0), ny + (d == 1),
+                                                         nz + (d == 2), b1, b2, 1, 1, o3, 1, ctx->nfaces(d));
+      CK(cudaGetLastError());
+    }
+  }
+  if (strat && !f->eq_prim_cc && !ctx->bg_uploaded) return PHL_E_INVALID;
+  if (strat && f->eq_prim_cc) {
+    // background: profiles along x2 when uniform in x1/x3, otherwise full arrays.  A later
+    // upload without background pointers refreshes only the dynamic state.
+    if (!f->phi_cc || !f->grav) return PHL_E_INVALID;
+    for (int d = 0; d < sd; ++d)
+      if (!f->eq_prim_x[d] || !f->phi_x[d]) return PHL_E_INVALID;
+    if (helm && (!f->eq_gammae_cc)) return PHL_E_INVALID;
+    for (int d = 0; d < sd && helm; ++d)
+      if (!f->eq_gammae_x[d]) return PHL_E_INVALID;
+    std::vector<std::vector<double>> prof;
+    bool ok = true;
+    auto cellprof = [&](const double *a, int nvh, int comp) {
+      std::vector<double> p;
+      ok = ok && extract_profile(a, nvh, comp, nx, ny, nz, G, G, G3, n1, n2, ny, p);
+      prof.push_back(p);
+    };
+    auto faceprof = [&](const double *a, int nvh, int comp, int d) {
+      std::vector<double> p;
+      int fx = nx + (d == 0), fy = ny + (d == 1), fz = nz + (d == 2);
+      ok = ok && extract_profile(a, nvh, comp, fx, fy, fz, 0, 0, 0, fx, fy, fy, p);
+      prof.push_back(p);
+    };
+    cellprof(f->eq_prim_cc, 3, 0);
+    cellprof(f->eq_prim_cc, 3, 1);
+    cellprof(f->phi_cc, 1, 0);
+    for (int d = 0; d < sd; ++d) cellprof(f->grav, sd, d);
+    if (helm) cellprof(f->eq_gammae_cc, 1, 0);
+    for (int d = 0; d < sd; ++d) {
+      faceprof(f->eq_prim_x[d], 3, 0, d);
+      faceprof(f->eq_prim_x[d], 3, 1, d);
+      faceprof(f->phi_x[d], 1, 0, d);
+      if (helm) faceprof(f->eq_gammae_x[d], 1, 0, d);
+    }
+    ctx->bg_profile = ok ? 1 : 0;
+    ctx->geo.bg_profile = ctx->bg_profile;
+    auto need = [&](double **p, size_t n) -> int {
+      if (!*p) return ctx->alloc(p, n);
+      return PHL_OK;
+    };
+    size_t ncc = ok ? (size_t)ny : (size_t)N;
+    if ((rc = need(&ctx->eq_rho_cc, ncc)) || (rc = need(&ctx->eq_p_cc, ncc)) || (rc = need(&ctx->phi_cc, ncc)) ||
+        (rc = need(&ctx->grav, (size_t)sd * ncc)))
+      return rc;
+    if (helm && (rc = need(&ctx->eq_ge_cc, ncc))) return rc;
+    for (int d = 0; d < sd; ++d) {
+      size_t nf = ok ? (size_t)(ny + (d == 1)) : (size_t)ctx->nfaces(d);
+      if ((rc = need(&ctx->eq_rho_f[d], nf)) || (rc = need(&ctx->eq_p_f[d], nf)) || (rc = need(&ctx->phi_f[d], nf)))
+        return rc;
+      if (helm && (rc = need(&ctx->eq_ge_f[d], nf))) return rc;
+    }
+    if (ok) {
+      size_t q = 0;
+      auto put = [&](double *dst) -> int {
+        CK(cudaMemcpyAsync(dst, prof[q].data(), sizeof(double) * prof[q].size(), cudaMemcpyHostToDevice, s));
+        ++q;
+        return PHL_OK;
+      };
+      if ((rc = put(ctx->eq_rho_cc)) || (rc = put(ctx->eq_p_cc)) || (rc = put(ctx->phi_cc))) return rc;
+      for (int d = 0; d < sd; ++d)
+        if ((rc = put(ctx->grav + (size_t)d * ny))) return rc;
+      if (helm && (rc = put(ctx->eq_ge_cc))) return rc;
+      for (int d = 0; d < sd; ++d) {
+        if ((rc = put(ctx->eq_rho_f[d])) || (rc = put(ctx->eq_p_f[d])) || (rc = put(ctx->phi_f[d]))) return rc;
+        if (helm && (rc = put(ctx->eq_ge_f[d]))) return rc;
+      }
+      CK(cudaStreamSynchronize(s));  // host vectors go out of scope
+    } else {
+      if ((rc = unpack_cell(f->eq_prim_cc, 3, 1, ctx->eq_rho_cc))) return rc;
+      // second component: unpack with a shifted base
+      CK(cudaMemcpyAsync(ctx->stage_buf, f->eq_prim_cc, sizeof(double) * 3 * Ng, cudaMemcpyHostToDevice, s));
+      k_unpack<<<nblk(N, 256), 256, 0, s>>>(ctx->stage_buf + 1, ctx->eq_p_cc, 3, nx, ny, nz, n1, n2, G, G, G3, 1, N);
+      if ((rc = unpack_cell(f->phi_cc, 1, 1, ctx->phi_cc))) return rc;
+      if ((rc = unpack_cell(f->grav, sd, sd, ctx->grav))) return rc;
+      if (helm && (rc = unpack_cell(f->eq_gammae_cc, 1, 1, ctx->eq_ge_cc))) return rc;
+      for (int d = 0; d < sd; ++d) {
+        long long nf = ctx->nfaces(d);
+        int fx = nx + (d == 0), fy = ny + (d == 1), fz = nz + (d == 2);
+        CK(cudaMemcpyAsync(ctx->stage_buf, f->eq_prim_x[d], sizeof(double) * 3 * nf, cudaMemcpyHostToDevice, s));
+        k_unpack<<<nblk(nf, 256), 256, 0, s>>>(ctx->stage_buf, ctx->eq_rho_f[d], 3, fx, fy, fz, fx, fy, 0, 0, 0, 1, nf);
+        k_unpack<<<nblk(nf, 256), 256, 0, s>>>(ctx->stage_buf + 1, ctx->eq_p_f[d], 3, fx, fy, fz, fx, fy, 0, 0, 0, 1, nf);
+        CK(cudaMemcpyAsync(ctx->phi_f[d], f->phi_x[d], sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+        if (helm) CK(cudaMemcpyAsync(ctx->eq_ge_f[d], f->eq_gammae_x[d], sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(s));
+  if (strat && f->eq_prim_cc) {
+    ctx->bg_uploaded = true;
+    // graphs bake the background layout into their kernel arguments
+    for (int p = 0; p < 2; ++p)
+      if (ctx->graph[p]) { cudaGraphExecDestroy(ctx->graph[p]); ctx->graph[p] = nullptr; }
+  }
+  ctx->uploaded = true;
+  return PHL_OK;
+}
+
+int phl_download_state(phl_ctx *ctx, phl_fields *f) {
+  if (!ctx || !f) return PHL_E_INVALID;
+  const phl_config &c = ctx->cfg;
+  CK(cudaSetDevice(c.device));
+  cudaStream_t s = ctx->stream;
+  const int G = c.ngc, G3 = c.sdims == 3 ? c.ngc : 0, sd = c.sdims, nv = c.nvars;
+  const int nx = c.nx1, ny = c.nx2, nz = c.nx3;
+  const int n1 = nx + 2 * G, n2 = ny + 2 * G, n3 = nz + 2 * G3;
+  const long long Ng = (long long)n1 * n2 * n3, N = ctx->N;
+  bool mhd = c.flags & PHL_MHD, helm = c.flags & PHL_HELMHOLTZ;
+  int rc;
+  if ((rc = ctx->ensure_stage(sizeof(double) * (size_t)Ng * std::max(nv, 3)))) return rc;
+  // pack into a staging copy of the host array so its ghost cells are preserved
+  auto pack_cell = [&](double *h, int ncomp, const double *src) -> int {
+    CK(cudaMemcpyAsync(ctx->stage_buf, h, sizeof(double) * (size_t)ncomp * Ng, cudaMemcpyHostToDevice, s));
+    k_pack<<<nblk(N, 256), 256, 0, s>>>(src, ctx->stage_buf, ncomp, nx, ny, nz, n1, n2, G, G, G3, ncomp, N);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h, ctx->stage_buf, sizeof(double) * (size_t)ncomp * Ng, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PHL_OK;
+  };
+  if (f->prim && (rc = pack_cell(f->prim, nv, ctx->W[ctx->cur]))) return rc;
+  if (f->temp && (rc = pack_cell(f->temp, 1, ctx->temp))) return rc;
+  if (f->eint && (rc = pack_cell(f->eint, 1, ctx->eint))) return rc;
+  if (helm && f->gammaf && (rc = pack_cell(f->gammaf, 2, ctx->gam[ctx->cur]))) return rc;
+  if (mhd && f->b_cc && (rc = pack_cell(f->b_cc, sd, ctx->bcc))) return rc;
+  if (mhd) {
+    for (int d = 0; d < sd; ++d) {
+      if (!f->b_x[d]) continue;
+      int b1 = nx + 2 + (d == 0), b2 = ny + 2 + (d == 1), b3 = sd == 3 ? nz + 2 + (d == 2) : 1;
+      int o3 = sd == 3 ? 1 : 0;
+      long long nb = (long long)b1 * b2 * b3;
+      CK(cudaMemcpyAsync(ctx->stage_buf, f->b_x[d], sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+      k_pack<<<nblk(ctx->nfaces(d), 256), 256, 0, s>>>(ctx->bf[d], ctx->stage_buf, 1, nx + (d == 0), ny + (d == 1),
+                                                       nz + (d == 2), b1, b2, 1, 1, o3, 1, ctx->nfaces(d));
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(f->b_x[d], ctx->stage_buf, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+  }
+  return PHL_OK;
+}
+
+static int ready(phl_ctx *ctx) {
+  if (!ctx) return PHL_E_INVALID;
+  if (!ctx->uploaded) return PHL_E_STATE;
+  if ((ctx->cfg.flags & PHL_HELMHOLTZ) && !ctx->table_loaded) return PHL_E_NO_TABLE;
+  return PHL_OK;
+}
+
+int phl_init_thermo(phl_ctx *ctx) {
+  int rc = ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->cfg.device));
+  Prm P = ctx->prm(0);
+  // write gammaf into the current buffer: gout must alias gin here
+  P.Win = ctx->W[ctx->cur];
+  P.gout = ctx->gam[ctx->cur];
+  ctx->runner->init_thermo(P, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PHL_OK;
+}
+
+int phl_compute_hyperbolic_dt(phl_ctx *ctx, double *dt, double *smax) {
+  int rc = ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->cfg.device));
+  Prm P = ctx->prm(0);
+  CK(cudaMemsetAsync(ctx->smax_bits, 0, sizeof(unsigned long long), ctx->stream));
+  ctx->runner->dt(P, ctx->stream);
+  k_finish_dt<<<1, 1, 0, ctx->stream>>>(ctx->scal, ctx->smax_bits, ctx->cfg.cfl);
+  CK(cudaGetLastError());
+  double sc[3];
+  CK(cudaMemcpyAsync(sc, ctx->scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (dt) *dt = sc[1];
+  if (smax) *smax = sc[2];
+  return PHL_OK;
+}
+
+int phl_hydro_step(phl_ctx *ctx) {
+  int rc = ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->cfg.device));
+  k_set_active<<<1, 1, 0, ctx->stream>>>(ctx->active, ctx->smax_bits);
+  ctx->launch_stages();
+  CK(cudaGetLastError());
+  ctx->cur = (ctx->cur + ctx->cfg.rk_stages) & 1;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PHL_OK;
+}
+
+int phl_set_time(phl_ctx *ctx, double time, double dt, double smax) {
+  if (!ctx) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  double sc[3] = {time, dt, smax};
+  CK(cudaMemcpyAsync(ctx->scal, sc, sizeof(sc), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PHL_OK;
+}
+
+int phl_get_time(phl_ctx *ctx, double *time, double *dt, double *smax) {
+  if (!ctx) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  double sc[3];
+  CK(cudaMemcpyAsync(sc, ctx->scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (time) *time = sc[0];
+  if (dt) *dt = sc[1];
+  if (smax) *smax = sc[2];
+  return PHL_OK;
+}
+
+int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double *time) {
+  int rc = ready(ctx);
+  if (rc) return rc;
+  if (nsteps < 0) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t s = ctx->stream;
+  long long step0 = 0;
+  CK(cudaMemcpyAsync(&step0, ctx->step, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ctx->scal + 3, &tmax, sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  // graphs run with no device-side step limit: the host launches exactly nsteps of them and
+  // the device stops by itself once time >= tmax.
+  for (int n = 0; n < nsteps; ++n) {
+    int p = ctx->cur;
+    if (!ctx->graph[p]) {
+      cudaGraph_t gph;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      k_pre_step<<<1, 1, 0, s>>>(ctx->scal, ctx->active, ctx->smax_bits, ctx->step, (long long)1 << 62);
+      ctx->launch_stages();
+      k_post_step<<<1, 1, 0, s>>>(ctx->scal, ctx->active, ctx->smax_bits, ctx->step, ctx->cfg.cfl);
+      CK(cudaStreamEndCapture(s, &gph));
+      cudaError_t e = cudaGraphInstantiate(&ctx->graph[p], gph, 0);
+      cudaGraphDestroy(gph);
+      if (e != cudaSuccess) {
+        g_last_error = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        return PHL_E_CUDA;
+      }
+    }
+    CK(cudaGraphLaunch(ctx->graph[p], s));
+    ctx->cur = (ctx->cur + ctx->cfg.rk_stages) & 1;
+  }
+  long long step1 = 0;
+  double t = 0;
+  CK(cudaMemcpyAsync(&step1, ctx->step, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&t, ctx->scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  // steps skipped by the device (time >= tmax) did not swap the W buffers: recover parity
+  long long skipped = (long long)nsteps - (step1 - step0);
+  if (skipped > 0 && (ctx->cfg.rk_stages & 1)) ctx->cur = (int)((ctx->cur + skipped) & 1);
+  if (steps_done) *steps_done = (int)(step1 - step0);
+  if (time) *time = t;
+  return PHL_OK;
+}
+
+int phl_get_status(phl_ctx *ctx, phl_status *st) {
+  if (!ctx || !st) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  unsigned long long h[STAT_COUNT];
+  long long step = 0;
+  double sc[3];
+  CK(cudaMemcpyAsync(h, ctx->stat, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&step, ctx->step, sizeof(step), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(sc, ctx->scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  memset(st, 0, sizeof(*st));
+  st->newton_calls = (long long)h[STAT_NEWTON_CALLS];
+  st->newton_iterations = (long long)h[STAT_NEWTON_ITERS];
+  st->newton_nonconverged = (long long)h[STAT_NEWTON_NONCONV];
+  st->newton_clamped = (long long)h[STAT_NEWTON_CLAMP];
+  st->mlp_accepted = (long long)h[STAT_MLP_ACC];
+  st->mlp_rejected = (long long)h[STAT_MLP_REJ];
+  st->nonfinite = (long long)h[STAT_NONFINITE];
+  st->steps = step;
+  st->time = sc[0];
+  st->dt = sc[1];
+  st->smax = sc[2];
+  return PHL_OK;
+}
+
+int phl_reset_status(phl_ctx *ctx) {
+  if (!ctx) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaMemsetAsync(ctx->stat, 0, sizeof(unsigned long long) * STAT_COUNT, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PHL_OK;
+}
+
+void *phl_device_field(phl_ctx *ctx, const char *name) {
+  if (!ctx || !name) return nullptr;
+  std::string n(name);
+  if (n == "prim") return ctx->W[ctx->cur];
+  if (n == "U") return ctx->U;
+  if (n == "U0") return ctx->U0;
+  if (n == "eint") return ctx->eint;
+  if (n == "temp") return ctx->temp;
+  if (n == "gammaf") return ctx->gam[ctx->cur];
+  if (n == "b_cc") return ctx->bcc;
+  if (n == "b_x1") return ctx->bf[0];
+  if (n == "b_x2") return ctx->bf[1];
+  if (n == "b_x3") return ctx->bf[2];
+  return nullptr;
+}
+
+void *phl_stream(phl_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+// ---- EoS batch (config 4) and MLP live in phl_eos_batch.cuh / phl_mlp.cu
+int phl_eos_invert_batch_device(phl_ctx *ctx, long long n, const double *rho, const double *e,
+                                const double *abar, const double *zbar, double *T_inout, double *p,
+                                double *cs, int *iters, int guess) {
+  if (!ctx || n < 0 || !rho || !e || !abar || !zbar || !T_inout) return PHL_E_INVALID;
+  if (!ctx->table_loaded) return PHL_E_NO_TABLE;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.invert(ctx->helm, ctx->stream, n, rho, e, abar, zbar, T_inout, p, cs, iters, guess, ctx->stat);
+}
+
+int phl_eos_energy_device(phl_ctx *ctx, long long n, const double *rho, const double *T, const double *abar,
+                          const double *zbar, double *e) {
+  if (!ctx || n < 0 || !rho || !T || !abar || !zbar || !e) return PHL_E_INVALID;
+  if (!ctx->table_loaded) return PHL_E_NO_TABLE;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.energy(ctx->helm, ctx->stream, n, rho, T, abar, zbar, e);
+}
+
+int phl_eos_invert_batch(phl_ctx *ctx, long long n, const double *rho, const double *e, const double *abar,
+                         const double *zbar, double *T_inout, double *p, double *cs, int *iters, int guess) {
+  if (!ctx || n < 0 || !rho || !e || !abar || !zbar || !T_inout) return PHL_E_INVALID;
+  if (!ctx->table_loaded) return PHL_E_NO_TABLE;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.invert_host(ctx->helm, ctx->stream, n, rho, e, abar, zbar, T_inout, p, cs, iters, guess, ctx->stat);
+}
+
+int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs, int batch, double lr,
+                  double *final_loss) {
+  if (!ctx || n <= 0 || epochs < 0 || batch <= 0) return PHL_E_INVALID;
+  if (!ctx->table_loaded) return PHL_E_NO_TABLE;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.mlp_train(ctx->helm, ctx->stream, n, seed, epochs, batch, lr, final_loss);
+}
+
+int phl_mlp_get_params(phl_ctx *ctx, float *params) {
+  if (!ctx || !params) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.mlp_get(ctx->stream, params);
+}
+
+int phl_mlp_set_params(phl_ctx *ctx, const float *params) {
+  if (!ctx || !params) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.mlp_set(ctx->stream, params);
+}
+
+int phl_mlp_infer_device(phl_ctx *ctx, long long n, const float *features, float *out) {
+  if (!ctx || n < 0 || !features || !out) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.mlp_infer(ctx->stream, n, features, out);
+}
+
+}  // extern "C"
