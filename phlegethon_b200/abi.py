@@ -34,7 +34,7 @@ EXPORTS = [
     "phl_hydro_step", "phl_set_time", "phl_get_time", "phl_run_steps", "phl_get_status",
     "phl_reset_status", "phl_eos_invert_batch_device", "phl_eos_invert_batch",
     "phl_eos_energy_device", "phl_mlp_train", "phl_mlp_get_params", "phl_mlp_set_params",
-    "phl_mlp_infer_device", "phl_device_field", "phl_stream",
+    "phl_mlp_infer_device", "phl_device_field", "phl_stream"
 ]
 
 
