@@ -170,6 +170,20 @@ int phl_eos_invert_batch_device(phl_ctx *ctx, long long n, const double *rho, co
 int phl_eos_invert_batch(phl_ctx *ctx, long long n, const double *rho, const double *e,
                          const double *abar, const double *zbar, double *T_inout, double *p,
                          double *cs, int *iters, int guess);
+/* Same as phl_eos_invert_batch, but allocates no device memory: the device copies of the
+ * inputs and outputs live in one fixed array compiled into the library.  No counterpart in the
+ * reference.  For callers that must not allocate GPU memory during the call: a driver whose
+ * device memory is already claimed by its own pool allocator, or code that runs while a CUDA
+ * stream capture is open (cudaMalloc is not allowed there and would break the capture).
+ * At most PHL_NOALLOC_MAX_SAMPLES samples per call; larger n returns PHL_E_TOO_LARGE.
+ * The first call on each device looks up the array's device address: make that first call
+ * before any stream capture.  The array is shared by every call and every context on a device
+ * (it stays allocated until the process exits), so calls that overlap on the GPU race; issue
+ * them one after another.  Host pointers; copies in and out are included. */
+#define PHL_NOALLOC_MAX_SAMPLES 65536
+int phl_eos_invert_batch_noalloc(phl_ctx *ctx, long long n, const double *rho, const double *e,
+                                 const double *abar, const double *zbar, double *T_inout, double *p,
+                                 double *cs, int *iters, int guess);
 /* Forward EoS e(rho, T) on device pointers (helm_rhoT_given2 without dE/dT). */
 int phl_eos_energy_device(phl_ctx *ctx, long long n, const double *rho, const double *T,
                           const double *abar, const double *zbar, double *e);

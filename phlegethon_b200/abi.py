@@ -34,7 +34,7 @@ EXPORTS = [
     "phl_hydro_step", "phl_set_time", "phl_get_time", "phl_run_steps", "phl_get_status",
     "phl_reset_status", "phl_eos_invert_batch_device", "phl_eos_invert_batch",
     "phl_eos_energy_device", "phl_mlp_train", "phl_mlp_get_params", "phl_mlp_set_params",
-    "phl_mlp_infer_device", "phl_device_field", "phl_stream"
+    "phl_mlp_infer_device", "phl_device_field", "phl_stream", "phl_eos_invert_batch_noalloc",
 ]
 
 
@@ -115,6 +115,7 @@ def load_library(path: str = LIB_PATH):
         "phl_reset_status": ([vp], C.c_int),
         "phl_eos_invert_batch_device": ([vp, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int], C.c_int),
         "phl_eos_invert_batch": ([vp, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int], C.c_int),
+        "phl_eos_invert_batch_noalloc": ([vp, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int], C.c_int),
         "phl_eos_energy_device": ([vp, C.c_longlong, vp, vp, vp, vp, vp], C.c_int),
         "phl_mlp_train": ([vp, C.c_longlong, C.c_ulonglong, C.c_int, C.c_int, C.c_double, _P], C.c_int),
         "phl_mlp_get_params": ([vp, C.POINTER(C.c_float)], C.c_int),

@@ -815,6 +815,87 @@ int phl_eos_invert_batch(phl_ctx *ctx, long long n, const double *rho, const dou
   return ctx->eos.invert_host(ctx->helm, ctx->stream, n, rho, e, abar, zbar, T_inout, p, cs, iters, guess, ctx->stat);
 }
 
+}  // extern "C"
+
+// ---- allocation-free EoS batch inversion.  Device copies of inputs and outputs live in one
+// file-scope array per device image.  Host code must never hand `g_noalloc_scratch` to a kernel
+// or a copy: in host code the name is only a stand-in for the symbol, and its device address is
+// obtained once per device with cudaGetSymbolAddress.
+namespace {
+constexpr int NOALLOC_FIELDS = 7;  // rho, e, abar, zbar, T, p, cs
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_FIELDS * PHL_NOALLOC_MAX_SAMPLES];
+static __device__ __align__(256) int g_noalloc_iters[PHL_NOALLOC_MAX_SAMPLES];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_noalloc_dev[NOALLOC_MAX_DEVICES] = {};
+int *g_noalloc_idev[NOALLOC_MAX_DEVICES] = {};
+
+// once per device, with that device current
+int noalloc_setup(int device, double **buf, int **ibuf) {
+  if (device < 0 || device >= NOALLOC_MAX_DEVICES) return PHL_E_INVALID;
+  if (!g_noalloc_dev[device]) {
+    double *p = nullptr;
+    int *q = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+      return PHL_E_CUDA;
+    }
+    e = cudaGetSymbolAddress((void **)&q, g_noalloc_iters);
+    if (e != cudaSuccess) {
+      g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_iters): ") + cudaGetErrorString(e);
+      return PHL_E_CUDA;
+    }
+    g_noalloc_dev[device] = p;
+    g_noalloc_idev[device] = q;
+  }
+  *buf = g_noalloc_dev[device];
+  *ibuf = g_noalloc_idev[device];
+  return PHL_OK;
+}
+}  // namespace
+
+extern "C" int phl_eos_invert_batch_noalloc(phl_ctx *ctx, long long n, const double *rho, const double *e,
+                                            const double *abar, const double *zbar, double *T_inout,
+                                            double *p, double *cs, int *iters, int guess) {
+  if (!ctx || n < 0 || !rho || !e || !abar || !zbar || !T_inout) return PHL_E_INVALID;
+  if (n > PHL_NOALLOC_MAX_SAMPLES) {
+    g_last_error = "phl_eos_invert_batch_noalloc: n exceeds PHL_NOALLOC_MAX_SAMPLES";
+    return PHL_E_TOO_LARGE;
+  }
+  if (!ctx->table_loaded) return PHL_E_NO_TABLE;
+  if (guess < 0 || guess > 2) return PHL_E_INVALID;
+  if (guess == 1 && !ctx->eos.mlp.ready) return PHL_E_STATE;
+  if (n == 0) return PHL_OK;
+  CK(cudaSetDevice(ctx->cfg.device));
+  double *buf = nullptr;
+  int *ibuf = nullptr;
+  int rc = noalloc_setup(ctx->cfg.device, &buf, &ibuf);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const size_t M = PHL_NOALLOC_MAX_SAMPLES, b = sizeof(double) * (size_t)n;
+  double *d_rho = buf, *d_e = buf + M, *d_a = buf + 2 * M, *d_z = buf + 3 * M, *d_T = buf + 4 * M;
+  double *d_p = buf + 5 * M, *d_c = buf + 6 * M;
+  // every element the kernel reads is copied in first; it writes every output it is asked for,
+  // so nothing left in the array by an earlier call is ever read
+  CK(cudaMemcpyAsync(d_rho, rho, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_e, e, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_a, abar, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_z, zbar, b, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_T, T_inout, b, cudaMemcpyHostToDevice, s));
+  k_eos_invert<<<nblk(n, 128), 128, 0, s>>>(ctx->helm, n, d_rho, d_e, d_a, d_z, d_T, p ? d_p : nullptr,
+                                            cs ? d_c : nullptr, iters ? ibuf : nullptr, guess,
+                                            ctx->eos.mlp.weights(), ctx->stat);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(T_inout, d_T, b, cudaMemcpyDeviceToHost, s));
+  if (p) CK(cudaMemcpyAsync(p, d_p, b, cudaMemcpyDeviceToHost, s));
+  if (cs) CK(cudaMemcpyAsync(cs, d_c, b, cudaMemcpyDeviceToHost, s));
+  if (iters) CK(cudaMemcpyAsync(iters, ibuf, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PHL_OK;
+}
+
+extern "C" {
+
 int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs, int batch, double lr,
                   double *final_loss) {
   if (!ctx || n <= 0 || epochs < 0 || batch <= 0) return PHL_E_INVALID;
