@@ -74,6 +74,13 @@ def step_bytes_per_cell(cfg):
     """
     nv = cfg.nvars
     s = cfg.rk_stages
+    if cfg.precision == "fp32_split":
+        # per stage: FP32 deviations W' read + written (nv), FP64 U read + written, U0 written in
+        # stage 1 and read in later stages; temp read + written, eint written in the last stage
+        b = s * (4 * nv + 4 * nv + 8 * nv + 8 * nv) + 8 * nv + (s - 1) * 8 * nv + 8
+        if cfg.helmholtz:
+            b += s * (16 + 16)  # temp (r+w, FP64) and the two FP32 gammas (r+w)
+        return b
     doubles = (nv + 1 + 3 * nv) + (s - 2) * (5 * nv) + (3 * nv + nv + 1)
     if cfg.helmholtz:
         doubles += s * (2 + 4)
@@ -189,35 +196,18 @@ def pinned_like(a):
     return t, v
 
 
-def run_ours(args):
+def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind, want_e2e):
+    """Time one arithmetic form on the workload; returns timings and the final host state."""
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    torch.cuda.set_device(local)
     from phlegethon_b200 import abi
     from phlegethon_b200.grid import HostGrid
 
-    name = args.config
-    n = args.n or default_size(name)
-    cfg, h, table = build_problem(name, n)
-    cfg.device = local
-    peaks, peak_kind = load_peaks()
-
-    sim = abi.Simulation(cfg, table)
+    c = cfg.replace(precision=form, device=local)
+    sim = abi.Simulation(c, table)
     sim.upload(h)
     sim.init_thermo()
     sim.compute_hyperbolic_dt()
     stream = torch.cuda.ExternalStream(sim.stream(), device=torch.device("cuda", local))
-
-    # ---------------------------------------------------------------- device-resident timing
     sim.time_loop(args.warmup)
     sim.reset_status()
     if dist is not None:
@@ -238,12 +228,12 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     status = sim.status()
-    cells = cfg.n_cells
-    value = world * done * cells / (ms * 1e-3)
+    out = h.copy()
+    sim.download(out)
+    res = {"form": form, "ms": ms, "done": done, "clocks": clocks, "status": status, "state": out}
 
-    # ---------------------------------------------------------------- dominant kernel timing
-    # hydro_step launches the RK stage kernels back to back without a graph; their average
-    # duration is measured with events on the library's stream
+    # dominant kernel: hydro_step launches the RK stage kernels back to back (no graph); their
+    # average duration is measured with events on the library's stream
     reps = max(2, min(args.steps, 5))
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
@@ -252,64 +242,103 @@ def run_ours(args):
         sim.hydro_step()
     k1.record(stream)
     torch.cuda.synchronize()
-    launches = reps * cfg.rk_stages
-    launch_ms = k0.elapsed_time(k1) / launches
-    bytes_per_cell = step_bytes_per_cell(cfg)
-    achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-            "kernel": "k_stage (fused flux + RK + cons->prim + EoS)", "peak_kind": peak_kind,
-            "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
+    res["launch_ms"] = k0.elapsed_time(k1) / (reps * c.rk_stages)
 
-    # ---------------------------------------------------------------- end-to-end through the ABI
-    # host-owned state in pinned memory: every step uploads the dynamic state, advances one
-    # step and downloads it again (prim, temp, eint [, gammaf, b_cc, b faces])
-    dyn = HostGrid.__new__(HostGrid)
-    dyn.__dict__.update(h.__dict__)
-    keep = []
-    for nm in ("prim", "temp", "eint", "gammaf", "b_cc"):
-        a = getattr(h, nm)
-        if a is not None:
-            t_, v_ = pinned_like(a)
-            keep.append(t_)
-            setattr(dyn, nm, v_)
-    bx = []
-    for d in range(3):
-        a = h.b_x[d]
-        if a is not None:
-            t_, v_ = pinned_like(a)
-            keep.append(t_)
-            bx.append(v_)
-        else:
-            bx.append(None)
-    dyn.b_x = bx
-    for nm in ("grav", "phi_cc", "eq_prim_cc", "eq_gammae_cc"):
-        setattr(dyn, nm, None)
-    dyn.phi_x = [None] * 3
-    dyn.eq_prim_x = [None] * 3
-    dyn.eq_gammae_x = [None] * 3
-    sim.download(dyn)
-    e2e_steps = max(1, min(args.steps, 5))
-    h2d = sum(a.nbytes for a in [dyn.prim, dyn.temp, dyn.eint, dyn.gammaf, dyn.b_cc] + bx if a is not None)
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    x0 = torch.cuda.Event(enable_timing=True)
-    x1 = torch.cuda.Event(enable_timing=True)
-    x0.record(stream)
-    for _ in range(e2e_steps):
-        sim.upload(dyn)
-        sim.time_loop(1)
+    if want_e2e:
+        # host-owned state in pinned memory: every step uploads the dynamic state, advances one
+        # step and downloads it again (prim, temp, eint [, gammaf, b_cc, b faces])
+        dyn = HostGrid.__new__(HostGrid)
+        dyn.__dict__.update(h.__dict__)
+        keep = []
+        for nm in ("prim", "temp", "eint", "gammaf", "b_cc"):
+            a = getattr(h, nm)
+            if a is not None:
+                t_, v_ = pinned_like(a)
+                keep.append(t_)
+                setattr(dyn, nm, v_)
+        bx = []
+        for d in range(3):
+            a = h.b_x[d]
+            if a is not None:
+                t_, v_ = pinned_like(a)
+                keep.append(t_)
+                bx.append(v_)
+            else:
+                bx.append(None)
+        dyn.b_x = bx
+        for nm in ("grav", "phi_cc", "eq_prim_cc", "eq_gammae_cc"):
+            setattr(dyn, nm, None)
+        dyn.phi_x = [None] * 3
+        dyn.eq_prim_x = [None] * 3
+        dyn.eq_gammae_x = [None] * 3
         sim.download(dyn)
-    x1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = x0.elapsed_time(x1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * e2e_steps * cells / (e2e_ms * 1e-3)
+        e2e_steps = max(1, min(args.steps, 5))
+        h2d = sum(a.nbytes for a in [dyn.prim, dyn.temp, dyn.eint, dyn.gammaf, dyn.b_cc] + bx if a is not None)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        x0 = torch.cuda.Event(enable_timing=True)
+        x1 = torch.cuda.Event(enable_timing=True)
+        x0.record(stream)
+        for _ in range(e2e_steps):
+            sim.upload(dyn)
+            sim.time_loop(1)
+            sim.download(dyn)
+        x1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = x0.elapsed_time(x1)
+        if dist is not None:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        res["e2e_ms_per_step"] = e2e_ms / e2e_steps
+        res["h2d"] = int(h2d)
     sim.close()
+    return res
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+    name = args.config
+    n = args.n or default_size(name)
+    cfg, h, table = build_problem(name, n)
+    peaks, peak_kind = load_peaks()
+    cells = cfg.n_cells
+    head_form = args.form
+    forms = [head_form] + [f for f in ("fp64",) if f != head_form]
+    results = {}
+    for form in forms:
+        results[form] = measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
+                                     want_e2e=(form == head_form))
+    head = results[head_form]
+    value = world * head["done"] * cells / (head["ms"] * 1e-3)
+    fp64 = results["fp64"]
+    fp64_value = world * fp64["done"] * cells / (fp64["ms"] * 1e-3)
+    errors = None
+    if head_form != "fp64":
+        from util import field_errors
+        errors = field_errors(head["state"], fp64["state"])
+
+    bytes_per_cell = step_bytes_per_cell(cfg.replace(precision=head_form))
+    launch_ms = head["launch_ms"]
+    achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
+    kname = "k_stage_split (FP32 fluxes, FP64 state/EoS)" if head_form == "fp32_split" else "k_stage (FP64)"
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": kname, "peak_kind": peak_kind,
+            "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -317,16 +346,23 @@ def run_ours(args):
         cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
+        e2e_value = world * cells / (head["e2e_ms_per_step"] * 1e-3)
+        status = head["status"]
         line = {"metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / max(done, 1), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": name, "n": n, "cells": cells, "form": "fp64 plain",
+                "warmup": args.warmup, "ms_per_step": head["ms"] / max(head["done"], 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 fluxes / f64 state+EoS" if head_form == "fp32_split" else "f64",
+                "data": "synthetic",
+                "config": {"workload": name, "n": n, "cells": cells, "form": head_form,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
+                "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
+                               "speedup_of_form": value / fp64_value},
+                "l1_vs_fp64": errors,
                 "roofline": roof, "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": int(h2d)},
-                "gpu_launches": int(done * (cfg.rk_stages + 2)), "clocks": clocks,
+                "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": head["h2d"],
+                        "d2h_bytes_per_step": head["h2d"]},
+                "gpu_launches": int(head["done"] * (cfg.rk_stages + 2)), "clocks": head["clocks"],
                 "newton": {k: status[k] for k in ("newton_calls", "newton_iterations", "newton_nonconverged")},
                 "nonfinite": status["nonfinite"]}
         print(json.dumps(line), flush=True)
@@ -345,6 +381,7 @@ def main():
                     choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang"])
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

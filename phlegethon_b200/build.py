@@ -22,6 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (source, extra flags)
 UNITS = [
     ("phl_runtime.cu", ["--fmad=false"]),
+    ("phl_split.cu", ["--fmad=false"]),
 ]
 
 

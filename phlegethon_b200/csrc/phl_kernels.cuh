@@ -45,6 +45,14 @@ struct Prm {
   HelmTable helm;
   double a1, a2, c3;
   int first_stage, last_stage;
+  // FP32 split-precision path: primitive deviations and FASTEOS gammas, ping-ponged
+  const float *__restrict__ Wf_in;
+  float *Wf_out;
+  const float *__restrict__ gf_in;
+  float *gf_out;
+  // reference scales of the FP32 split path: the FP32 deviations and fluxes are kept in units
+  // of rho_ref, p_ref and v_ref = sqrt(p_ref / rho_ref) so that no product leaves FP32 range
+  double rho_ref, p_ref, v_ref;
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,

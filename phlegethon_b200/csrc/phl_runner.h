@@ -1,0 +1,26 @@
+// phl_runner.h -- interface between the runtime (phl_runtime.cu) and the per-configuration
+// kernel launchers, which live in two translation units: the FP64 path (compiled without FMA
+// contraction, reference rounding) and the FP32 split-precision path (phl_split.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "phl_kernels.cuh"
+
+namespace phl {
+
+struct Runner {
+  virtual ~Runner() {}
+  // one RK stage (all kernels of the stage)
+  virtual void stage(const Prm &P, cudaStream_t s) = 0;
+  // standalone CFL maximum over the FP64 primitive state
+  virtual void dt(const Prm &P, cudaStream_t s) = 0;
+  // step-0 thermodynamics
+  virtual void init_thermo(const Prm &P, cudaStream_t s) = 0;
+  // split path only: FP64 primitives -> (U, FP32 deviations) and back
+  virtual void split_from_prim(const Prm &, cudaStream_t) {}
+  virtual void split_to_prim(const Prm &, cudaStream_t) {}
+};
+
+// factory of the FP32 split-precision runners (phl_split.cu); nullptr when not built
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem);
+
+}  // namespace phl

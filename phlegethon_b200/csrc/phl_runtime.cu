@@ -15,6 +15,7 @@
 
 #include "../../include/phl_gpu.h"
 #include "phl_kernels.cuh"
+#include "phl_runner.h"
 #include "phl_eos_batch.cuh"
 
 using namespace phl;
@@ -35,19 +36,12 @@ thread_local std::string g_last_error;
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // ----------------------------------------------------------------------------- runners
-struct Runner {
-  virtual ~Runner() {}
-  virtual void stage(const Prm &P, cudaStream_t s) = 0;
-  virtual void dt(const Prm &P, cudaStream_t s) = 0;
-  virtual void init_thermo(const Prm &P, cudaStream_t s) = 0;
-};
-
 template <class C>
 struct RunnerT : Runner {
   void stage(const Prm &P, cudaStream_t s) override {
     const Geo &g = P.g;
     k_stage<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
-    if (C::MHD) {
+    if constexpr (C::MHD) {
       for (int a = 0; a < 3; ++a) {
         if (C::DIM == 2 && a != 2) continue;
         long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) *
@@ -158,6 +152,10 @@ struct phl_ctx {
   long long N = 0;
   // dynamic
   double *W[2] = {nullptr, nullptr}, *gam[2] = {nullptr, nullptr};
+  float *Wf[2] = {nullptr, nullptr}, *gf[2] = {nullptr, nullptr};  // FP32 split path
+  bool split = false;
+  double rho_ref = 1.0, p_ref = 1.0, v_ref = 1.0;  // FP32 split-path scales
+  bool refs_set = false;
   int cur = 0;
   double *U = nullptr, *U0 = nullptr, *eint = nullptr, *temp = nullptr;
   double *bcc = nullptr;
@@ -229,6 +227,13 @@ struct phl_ctx {
     P.Wout = W[in ^ 1];
     P.gin = gam[in];
     P.gout = gam[in ^ 1];
+    P.Wf_in = Wf[in];
+    P.Wf_out = Wf[in ^ 1];
+    P.gf_in = gf[in];
+    P.gf_out = gf[in ^ 1];
+    P.rho_ref = rho_ref;
+    P.p_ref = p_ref;
+    P.v_ref = v_ref;
     P.U = U;
     P.U0 = U0;
     P.eint = eint;
@@ -255,6 +260,22 @@ struct phl_ctx {
     P.first_stage = stage_idx == 0;
     P.last_stage = stage_idx == cfg.rk_stages - 1;
     return P;
+  }
+  // split path: FP64 primitives of W[cur] -> U and the FP32 deviations of Wf[cur]
+  void split_from_prim() {
+    Prm P = prm(0);
+    P.Win = W[cur];
+    P.gin = gam[cur];
+    P.Wf_out = Wf[cur];
+    P.gf_out = gf[cur];
+    runner->split_from_prim(P, stream);
+  }
+  // split path: U (+temp, eint) -> FP64 primitives and gammaf in W[cur], gam[cur]
+  void split_to_prim() {
+    Prm P = prm(0);
+    P.Wout = W[cur];
+    P.gout = gam[cur];
+    runner->split_to_prim(P, stream);
   }
   // hydro_step: all RK stages starting from W[cur]
   void launch_stages() {
@@ -345,8 +366,11 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   bool mhd = cfg->flags & PHL_MHD, helm = cfg->flags & PHL_HELMHOLTZ;
   bool wb = cfg->flags & PHL_WB, etot = cfg->flags & PHL_EVOLVE_ETOT, grav = cfg->flags & PHL_GRAVITY;
   if (!(wb == etot && etot == grav)) return PHL_E_UNSUPPORTED;
-  if (cfg->precision != PHL_FP64) return PHL_E_UNSUPPORTED;
-  c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+  c->split = cfg->precision == PHL_FP32_SPLIT;
+  if (c->split)
+    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+  else
+    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
   if (!c->runner) return PHL_E_UNSUPPORTED;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   Geo &g = c->geo;
@@ -375,6 +399,12 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   if (helm) {
     if ((rc = c->alloc(&c->gam[0], (size_t)2 * N))) return rc;
     if ((rc = c->alloc(&c->gam[1], (size_t)2 * N))) return rc;
+  }
+  if (c->split) {
+    for (int q = 0; q < 2; ++q) {
+      if ((rc = c->alloc(&c->Wf[q], (size_t)nv * N))) return rc;
+      if (helm && (rc = c->alloc(&c->gf[q], (size_t)2 * N))) return rc;
+    }
   }
   if (mhd) {
     if ((rc = c->alloc(&c->bcc, (size_t)3 * N))) return rc;
@@ -463,6 +493,20 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
     return PHL_OK;
   };
   ctx->cur = 0;
+  if (ctx->split && !ctx->refs_set) {
+    // scales of the FP32 split path: largest density and pressure of the first uploaded state
+    double rmax = 0.0, pmax = 0.0;
+    const int ip = 1 + sd;
+    for (long long q = 0; q < Ng; ++q) {
+      double r = std::fabs(f->prim[(size_t)nv * q]), pp = std::fabs(f->prim[(size_t)nv * q + ip]);
+      if (std::isfinite(r) && r > rmax) rmax = r;
+      if (std::isfinite(pp) && pp > pmax) pmax = pp;
+    }
+    ctx->rho_ref = rmax > 0.0 ? rmax : 1.0;
+    ctx->p_ref = pmax > 0.0 ? pmax : 1.0;
+    ctx->v_ref = std::sqrt(ctx->p_ref / ctx->rho_ref);
+    ctx->refs_set = true;
+  }
   if ((rc = unpack_cell(f->prim, nv, nv, ctx->W[0]))) return rc;
   if (f->temp && (rc = unpack_cell(f->temp, 1, 1, ctx->temp))) return rc;
   if (f->eint && (rc = unpack_cell(f->eint, 1, 1, ctx->eint))) return rc;
@@ -568,6 +612,10 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
       }
     }
   }
+  if (ctx->split && f->eint && (!strat || ctx->bg_uploaded || f->eq_prim_cc)) {
+    ctx->split_from_prim();
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(s));
   if (strat && f->eq_prim_cc) {
     ctx->bg_uploaded = true;
@@ -591,6 +639,10 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
   bool mhd = c.flags & PHL_MHD, helm = c.flags & PHL_HELMHOLTZ;
   int rc;
   if ((rc = ctx->ensure_stage(sizeof(double) * (size_t)Ng * std::max(nv, 3)))) return rc;
+  if (ctx->split) {
+    ctx->split_to_prim();
+    CK(cudaGetLastError());
+  }
   // pack into a staging copy of the host array so its ghost cells are preserved
   auto pack_cell = [&](double *h, int ncomp, const double *src) -> int {
     CK(cudaMemcpyAsync(ctx->stage_buf, h, sizeof(double) * (size_t)ncomp * Ng, cudaMemcpyHostToDevice, s));
@@ -639,6 +691,10 @@ int phl_init_thermo(phl_ctx *ctx) {
   P.gout = ctx->gam[ctx->cur];
   ctx->runner->init_thermo(P, ctx->stream);
   CK(cudaGetLastError());
+  if (ctx->split) {
+    ctx->split_from_prim();
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   return PHL_OK;
 }
@@ -647,7 +703,9 @@ int phl_compute_hyperbolic_dt(phl_ctx *ctx, double *dt, double *smax) {
   int rc = ready(ctx);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->split) ctx->split_to_prim();
   Prm P = ctx->prm(0);
+  P.Win = ctx->W[ctx->cur];
   CK(cudaMemsetAsync(ctx->smax_bits, 0, sizeof(unsigned long long), ctx->stream));
   ctx->runner->dt(P, ctx->stream);
   k_finish_dt<<<1, 1, 0, ctx->stream>>>(ctx->scal, ctx->smax_bits, ctx->cfg.cfl);
@@ -784,6 +842,8 @@ void *phl_device_field(phl_ctx *ctx, const char *name) {
   if (n == "b_x1") return ctx->bf[0];
   if (n == "b_x2") return ctx->bf[1];
   if (n == "b_x3") return ctx->bf[2];
+  if (n == "prim_dev32") return ctx->Wf[ctx->cur];
+  if (n == "gammaf_dev32") return ctx->gf[ctx->cur];
   return nullptr;
 }
 
