@@ -188,6 +188,21 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms, dist, device="cuda"):
+    """Largest elapsed time over all ranks (the job is as slow as its slowest replica)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, steps, cells, ms):
+    """Whole-job zone-updates/s of `world` replicas that each advanced `steps` steps."""
+    return world * steps * cells / (ms * 1e-3)
+
+
 def pinned_like(a):
     import torch
     t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
@@ -222,11 +237,7 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     status = sim.status()
     out = h.copy()
     sim.download(out)
@@ -286,11 +297,7 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
             sim.download(dyn)
         x1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = x0.elapsed_time(x1)
-        if dist is not None:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(x0.elapsed_time(x1), dist)
         res["e2e_ms_per_step"] = e2e_ms / e2e_steps
         res["h2d"] = int(h2d)
     sim.close()
@@ -324,9 +331,9 @@ def run_ours(args):
         results[form] = measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
                                      want_e2e=(form == head_form))
     head = results[head_form]
-    value = world * head["done"] * cells / (head["ms"] * 1e-3)
+    value = aggregate_rate(world, head["done"], cells, head["ms"])
     fp64 = results["fp64"]
-    fp64_value = world * fp64["done"] * cells / (fp64["ms"] * 1e-3)
+    fp64_value = aggregate_rate(world, fp64["done"], cells, fp64["ms"])
     errors = None
     if head_form != "fp64":
         from util import field_errors

@@ -118,9 +118,10 @@ def write_text(path, tab, dpdr):
 
 def read_text(path, nrho, nT):
     """Inverse of :func:`write_text` (the parse of load_helm_table)."""
-    raw = np.loadtxt(path)
-    a = raw[: nrho * nT].reshape(nT, nrho, 9)
-    b = raw[nrho * nT: 2 * nrho * nT].reshape(nT, nrho, 4)
+    with open(path) as fh:
+        lines = fh.read().split("\n")
+    a = np.array([[float(x) for x in ln.split()] for ln in lines[: nrho * nT]]).reshape(nT, nrho, 9)
+    b = np.array([[float(x) for x in ln.split()] for ln in lines[nrho * nT: 2 * nrho * nT]]).reshape(nT, nrho, 4)
     tab = np.zeros((9, nrho, nT), order="F")
     dpdr = np.zeros((4, nrho, nT), order="F")
     order = [0, 3, 1, 4, 2, 5, 6, 7, 8]

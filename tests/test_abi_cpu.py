@@ -1,0 +1,64 @@
+"""CPU checks of the C-ABI library: it loads, exports every declared entry point, and refuses
+to run without a CUDA device (no CPU fallback)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "phl_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:int|void|const char|void \*)\s*\*?\s*(phl_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib_path():
+    import importlib
+    return importlib.import_module("phlegethon_b200.build").build(force=False)
+
+
+def test_library_exports_every_declared_symbol(lib_path):
+    lib = C.CDLL(lib_path)
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    from phlegethon_b200 import abi
+    assert sorted(abi.EXPORTS) == names
+
+
+def test_abi_version_and_errors(lib_path):
+    from phlegethon_b200 import abi
+    lib = abi.load_library(lib_path)
+    assert lib.phl_abi_version() == abi.ABI_VERSION
+    assert lib.phl_error_string(-1).decode().startswith("invalid")
+
+
+def test_no_cpu_fallback(lib_path):
+    """Without a GPU, phl_init reports PHL_E_NO_DEVICE instead of running anything on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from phlegethon_b200 import abi, problems
+    cfg, _ = problems.hot_bubble_2d(16)
+    with pytest.raises(abi.PhlError) as e:
+        abi.Simulation(cfg)
+    assert e.value.code == -5
+
+
+def test_invalid_config_rejected_before_device_use(lib_path):
+    from phlegethon_b200 import abi, problems
+    lib = abi.load_library(lib_path)
+    cfg, _ = problems.hot_bubble_2d(16)
+    s = abi.make_config_struct(cfg)
+    s.nvars = 99
+    ctx = C.c_void_p()
+    assert lib.phl_init(C.byref(s), C.byref(ctx)) == -1
+    s = abi.make_config_struct(cfg)
+    s.abi_version = 12345
+    assert lib.phl_init(C.byref(s), C.byref(ctx)) == -1
