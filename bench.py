@@ -378,6 +378,140 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+EOS_METRIC = "(rho,e)->T inversions/s on 1 B200: learned vs bracket guess, T identical to 1e-10"
+EOS_BYTES_PER_SAMPLE = 44  # rho, e, Abar, Zbar in (FP64), T out (FP64), iteration count out (int32)
+
+
+def run_eos(args):
+    """EoS inversion batch: 2^24 samples over the full table range, bracket vs learned guess.
+
+    A step is one inversion of the whole batch (inputs resident in HBM, 2^24 x 44 B > L2).
+    """
+    import torch
+    from phlegethon_b200 import helm_table, problems
+    from phlegethon_b200.abi import Simulation
+    n = args.n or (1 << 24)
+    cfg, _ = problems.stratified_3d(8)
+    table = helm_table.generate()
+    peaks, peak_kind = load_peaks()
+    import ctypes as C
+    with Simulation(cfg, table) as sim:
+        lib = sim.lib
+        stream = torch.cuda.ExternalStream(sim.stream())
+        t0 = time.perf_counter()
+        loss = C.c_double()
+        rc = lib.phl_mlp_train(sim.ctx, 1 << 22, 12345, 256, 8192, C.c_double(3e-3), C.byref(loss))
+        train_s = time.perf_counter() - t0
+        assert rc == 0, rc
+        rho, T, abar, zbar = problems.eos_samples(n, seed=99)
+        d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+             dict(rho=rho, T=T, abar=abar, zbar=zbar).items()}
+        e = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert lib.phl_eos_energy_device(sim.ctx, n, d["rho"].data_ptr(), d["T"].data_ptr(), d["abar"].data_ptr(),
+                                         d["zbar"].data_ptr(), e.data_ptr()) == 0
+        out = {}
+        for guess, gname in ((2, "bracket"), (1, "mlp")):
+            Tout = torch.zeros(n, dtype=torch.float64, device="cuda")
+            its = torch.zeros(n, dtype=torch.int32, device="cuda")
+
+            def step():
+                return lib.phl_eos_invert_batch_device(sim.ctx, n, d["rho"].data_ptr(), e.data_ptr(),
+                                                       d["abar"].data_ptr(), d["zbar"].data_ptr(), Tout.data_ptr(),
+                                                       None, None, its.data_ptr(), guess)
+            for _ in range(args.warmup):
+                assert step() == 0
+            sim.reset_status()
+            torch.cuda.synchronize()
+            clk = ClockSampler(0)
+            clk.start()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                assert step() == 0
+            e1.record(stream)
+            torch.cuda.synchronize()
+            clocks = clk.stop()
+            ms = e0.elapsed_time(e1) / args.steps
+            st = sim.status()
+            out[gname] = dict(ms=ms, rate=n / (ms * 1e-3), T=Tout.clone(), iters=its.double().mean().item(),
+                              evals=(st["guess_evaluations"] + st["newton_iterations"]) / (n * args.steps),
+                              accepted=st["mlp_accepted"] / (n * args.steps), clocks=clocks,
+                              nonconv=st["newton_nonconverged"])
+        # host-buffer end to end through the public host-pointer entry point
+        e_host = e.cpu().numpy()
+        h_in = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for v in (rho, e_host, abar, zbar)]
+        h_T = torch.zeros(n, dtype=torch.float64).pin_memory()
+        h_it = torch.zeros(n, dtype=torch.int32).pin_memory()
+        x0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            assert lib.phl_eos_invert_batch(sim.ctx, n, *[a.data_ptr() for a in h_in], h_T.data_ptr(), None, None,
+                                            h_it.data_ptr(), 1) == 0
+        e2e_ms = (time.perf_counter() - x0) * 1e3 / e2e_steps
+        # agreement of the two answers, judged by the conditioning kappa = |E / (T dE/dT)|
+        Tb = out["bracket"]["T"]
+        hh = 1e-6
+        ep = torch.zeros_like(e)
+        em = torch.zeros_like(e)
+        tp = Tb * (1 + hh)
+        tm = Tb * (1 - hh)
+        lib.phl_eos_energy_device(sim.ctx, n, d["rho"].data_ptr(), tp.data_ptr(), d["abar"].data_ptr(),
+                                  d["zbar"].data_ptr(), ep.data_ptr())
+        lib.phl_eos_energy_device(sim.ctx, n, d["rho"].data_ptr(), tm.data_ptr(), d["abar"].data_ptr(),
+                                  d["zbar"].data_ptr(), em.data_ptr())
+        kappa = (e / ((ep - em) / (2 * hh))).abs()
+        rel = (out["mlp"]["T"] - Tb).abs() / Tb
+        good = kappa < 10
+        agree = {"frac_kappa_lt_10": good.double().mean().item(),
+                 "max_rel_T_diff_kappa_lt_10": rel[good].max().item(),
+                 "frac_within_1e-10_plus_4e-11_kappa": (rel <= 1e-10 + 4e-11 * kappa).double().mean().item()}
+    m, b = out["mlp"], out["bracket"]
+    cpu = None
+    if not args.no_cpu:
+        k = min(n, 1 << 20)
+        cpu = eos_cpu_rate(rho[:k], e_host[:k], abar[:k], zbar[:k])
+    achieved = EOS_BYTES_PER_SAMPLE * m["rate"] / 1e9
+    line = {"metric": EOS_METRIC, "value": m["rate"], "unit": "inversions/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (EoS/Newton), bf16/f32 (MLP)", "data": "synthetic",
+            "config": {"workload": "eos_batch", "n": n, "l2": "inputs larger than L2 (%.0f MB)" % (n * 44 / 1e6),
+                       "train": {"samples": 1 << 22, "epochs": 256, "seconds": train_s, "loss": loss.value}},
+            "bracket": {"value": b["rate"], "ms_per_step": b["ms"], "newton_iters_per_sample": b["iters"],
+                        "eos_evals_per_sample": b["evals"]},
+            "mlp": {"newton_iters_per_sample": m["iters"], "eos_evals_per_sample": m["evals"],
+                    "accepted": m["accepted"], "speedup_vs_bracket": m["rate"] / b["rate"]},
+            "agreement": agree,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_eos_invert + k_eos_fallback",
+                         "note": "FP64-compute bound (EoS evaluations); HBM fraction stated for completeness"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "inversions/s", "h2d_bytes_per_step": 40 * n,
+                    "d2h_bytes_per_step": 12 * n},
+            "gpu_launches": 2 * args.steps, "clocks": m["clocks"]}
+    print(json.dumps(line), flush=True)
+
+
+def eos_cpu_rate(rho, e, abar, zbar, seconds=10.0):
+    """Oracle bracket-guess inversions/s on all host cores, repeating a bounded slice of the batch."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from phlegethon_b200 import helm_table, problems
+    cfg, _ = problems.stratified_3d(8)
+    helm = pyoracle.Helm.for_config(cfg, *helm_table.generate())
+    done = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        helm.invert_batch(rho, e, abar, zbar, guess=2)
+        done += rho.size
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "inversions/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "%d inversions (first %d samples of the batch, repeated; oracle bracket guess + "
+                      "helm_rhoe_given Newton, OpenMP)" % (done, rho.size)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,7 +519,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="stratified",
-                    choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang"])
+                    choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang", "eos"])
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
@@ -394,6 +528,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "eos":
+        run_eos(args)
     else:
         run_ours(args)
 

@@ -62,7 +62,8 @@ extern "C" {
 
 /* initial temperature guess for the (rho, e) -> T Newton inversion */
 #define PHL_GUESS_WARM 0  /* previous-stage temperature, as the reference (source.F90:13649) */
-#define PHL_GUESS_MLP 1   /* learned 4-64-64-1 guess, judged by <=3 Newton steps, else warm */
+#define PHL_GUESS_MLP 1   /* learned 4-64-64-1 guess, judged by <=3 Newton steps, else the
+                                     warm guess (hydro step) or the bracket guess (EoS batch) */
 
 typedef struct phl_config {
   int abi_version;                 /* must be PHL_ABI_VERSION */
@@ -110,6 +111,8 @@ typedef struct phl_status {
   long long mlp_accepted;         /* MLP guesses that converged within 3 iterations */
   long long mlp_rejected;         /* MLP guesses that fell back to the warm/bracket guess */
   long long nonfinite;            /* non-finite or non-positive rho/p/T produced */
+  long long guess_evaluations;    /* EoS evaluations spent building initial guesses (bracket
+                                     search, cold energy of the learned guess's input) */
   long long steps;                /* steps taken by this context */
   double time, dt, smax;
 } phl_status;
@@ -196,6 +199,11 @@ int phl_eos_energy_device(phl_ctx *ctx, long long n, const double *rho, const do
  * NULL.  Everything runs on the device with the project's own kernels. */
 int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs, int batch,
                   double lr, double *final_loss);
+/* One gradient evaluation of the mean-squared loss on n training pairs (host pointers:
+ * features n x 4 FP32, targets n FP32 as (log10 T - 7)/3), with the current parameters; n must
+ * be a multiple of 64.  grad receives PHL_MLP_NPARAMS floats; loss may be NULL. */
+int phl_mlp_gradient(phl_ctx *ctx, long long n, const float *features, const float *targets, float *grad,
+                     double *loss);
 /* FP32 master weights in the order W1(64x4), b1(64), W2(64x64), b2(64), W3(1x64), b3(1). */
 int phl_mlp_get_params(phl_ctx *ctx, float *params);
 int phl_mlp_set_params(phl_ctx *ctx, const float *params);

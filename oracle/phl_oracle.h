@@ -88,6 +88,17 @@ int phlo_helm_rhoP_given(const phlo_helm *h, double rho, double P0, double abar,
 int phlo_helm_rhoe_given(const phlo_helm *h, double rho, double E0, double abar, double zbar,
                          double *T, double *P, double *sound, int return_sound);
 
+/* Cold initial guess for the (rho, e) -> T inversion of independent samples (no reference
+ * counterpart; the reference always has a warm start): bisection over the table's T nodes for
+ * E(rho, T_j) <= e, then linear interpolation of E between the bracketing nodes.  Returns the
+ * EoS evaluations used. */
+int phlo_eos_bracket_guess(const phlo_helm *h, double rho, double e, double abar, double zbar, double *T);
+/* Batch inversion with helm_rhoe_given's Newton (guess 0: T holds the warm start; guess 2: the
+ * bracket guess); T receives the result, iters (may be NULL) the Newton iterations.  OpenMP over
+ * nthreads (0 = all). */
+void phlo_eos_invert_batch(const phlo_helm *h, long n, const double *rho, const double *e, const double *abar,
+                           const double *zbar, double *T, int *iters, int guess, int nthreads);
+
 /* ---- Riemann solvers for one face, in the normal frame (source/source.F90:13969-16260) ----
  * q*: nvars primitive face states; g*: (gammae, gammac) face values for USE_FASTEOS (NULL
  * otherwise); b*: 3 components (normal first), MHD only. */

@@ -13,6 +13,7 @@
  * contraction (-ffp-contract=off) to reproduce the reference bit for bit.
  */
 #include <math.h>
+#include <omp.h>
 #include "phl_oracle.h"
 
 /* physical constants (source/source.F90:612-629) */
@@ -340,4 +341,49 @@ int phlo_helm_rhoe_given(const phlo_helm *h, double rho, double E0, double abar,
     phlo_helm_rhoT_given1(h, rho, *T, abar, zbar, P, &dP, 0);
   }
   return used;
+}
+
+int phlo_eos_bracket_guess(const phlo_helm *h, double rho, double e, double abar, double zbar, double *T) {
+  int lo = 0, hi = h->nT - 1, evals = 2;
+  double elo, ehi, dd, em, w;
+  phlo_helm_rhoT_given2(h, rho, h->T[lo], abar, zbar, &elo, &dd, 0);
+  if (e <= elo) {
+    *T = h->T[lo];
+    return 1;
+  }
+  phlo_helm_rhoT_given2(h, rho, h->T[hi] * 0.999999, abar, zbar, &ehi, &dd, 0);
+  if (e >= ehi) {
+    *T = h->T[hi] * 0.999999;
+    return 2;
+  }
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    phlo_helm_rhoT_given2(h, rho, h->T[mid], abar, zbar, &em, &dd, 0);
+    ++evals;
+    if (em <= e) {
+      lo = mid;
+      elo = em;
+    } else {
+      hi = mid;
+      ehi = em;
+    }
+  }
+  w = (e - elo) / (ehi - elo);
+  *T = h->T[lo] + w * (h->T[hi] - h->T[lo]);
+  return evals;
+}
+
+void phlo_eos_invert_batch(const phlo_helm *h, long n, const double *rho, const double *e, const double *abar,
+                           const double *zbar, double *T, int *iters, int guess, int nthreads) {
+  long i;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (i = 0; i < n; ++i) {
+    double t = T[i], P, snd;
+    int it;
+    if (guess == 2) phlo_eos_bracket_guess(h, rho[i], e[i], abar[i], zbar[i], &t);
+    it = phlo_helm_rhoe_given(h, rho[i], e[i], abar[i], zbar[i], &t, &P, &snd, 0);
+    T[i] = t;
+    if (iters) iters[i] = it;
+  }
 }

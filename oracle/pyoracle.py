@@ -72,6 +72,12 @@ def load():
         lib.phlo_helm_rhoP_given.argtypes = [C.POINTER(_Helm), C.c_double, C.c_double, C.c_double,
                                              C.c_double, _P, _P, _P, C.c_int]
         lib.phlo_helm_rhoP_given.restype = C.c_int
+        lib.phlo_eos_invert_batch.argtypes = [C.POINTER(_Helm), C.c_long, _P, _P, _P, _P, _P,
+                                              C.POINTER(C.c_int), C.c_int, C.c_int]
+        lib.phlo_eos_invert_batch.restype = None
+        lib.phlo_eos_bracket_guess.argtypes = [C.POINTER(_Helm), C.c_double, C.c_double, C.c_double, C.c_double,
+                                               _P]
+        lib.phlo_eos_bracket_guess.restype = C.c_int
         lib.phlo_riemann_hydro.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P]
         lib.phlo_riemann_hydro.restype = None
         lib.phlo_riemann_mhd.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P, _P, _P, _P]
@@ -126,6 +132,16 @@ class Helm:
         T, P, s = C.c_double(T0), C.c_double(), C.c_double()
         it = load().phlo_helm_rhoe_given(C.byref(self.s), rho, E0, abar, zbar, C.byref(T), C.byref(P), C.byref(s), 1)
         return T.value, P.value, s.value, it
+
+    def invert_batch(self, rho, e, abar, zbar, T0=None, guess=2, nthreads=0):
+        """(rho, e) -> T for arrays of samples; guess 2 = bracket guess, 0 = warm start T0."""
+        n = len(rho)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, e, abar, zbar)]
+        T = np.zeros(n) if T0 is None else np.array(T0, dtype=np.float64)
+        it = np.zeros(n, dtype=np.int32)
+        load().phlo_eos_invert_batch(C.byref(self.s), n, *[a.ctypes.data_as(_P) for a in arrs],
+                                     T.ctypes.data_as(_P), it.ctypes.data_as(C.POINTER(C.c_int)), guess, nthreads)
+        return T, it
 
     def rhoP_given(self, rho, P0, abar, zbar, T0):
         T, E, s = C.c_double(T0), C.c_double(), C.c_double()

@@ -34,7 +34,7 @@ EXPORTS = [
     "phl_hydro_step", "phl_set_time", "phl_get_time", "phl_run_steps", "phl_get_status",
     "phl_reset_status", "phl_eos_invert_batch_device", "phl_eos_invert_batch",
     "phl_eos_energy_device", "phl_mlp_train", "phl_mlp_get_params", "phl_mlp_set_params",
-    "phl_mlp_infer_device", "phl_device_field", "phl_stream", "phl_eos_invert_batch_noalloc",
+    "phl_mlp_infer_device", "phl_mlp_gradient", "phl_device_field", "phl_stream", "phl_eos_invert_batch_noalloc",
 ]
 
 
@@ -69,7 +69,8 @@ class PhlStatus(C.Structure):
         ("newton_calls", C.c_longlong), ("newton_iterations", C.c_longlong),
         ("newton_nonconverged", C.c_longlong), ("newton_clamped", C.c_longlong),
         ("mlp_accepted", C.c_longlong), ("mlp_rejected", C.c_longlong),
-        ("nonfinite", C.c_longlong), ("steps", C.c_longlong), ("time", C.c_double),
+        ("nonfinite", C.c_longlong), ("guess_evaluations", C.c_longlong), ("steps", C.c_longlong),
+        ("time", C.c_double),
         ("dt", C.c_double), ("smax", C.c_double),
     ]
 
@@ -121,6 +122,7 @@ def load_library(path: str = LIB_PATH):
         "phl_mlp_get_params": ([vp, C.POINTER(C.c_float)], C.c_int),
         "phl_mlp_set_params": ([vp, C.POINTER(C.c_float)], C.c_int),
         "phl_mlp_infer_device": ([vp, C.c_longlong, vp, vp], C.c_int),
+        "phl_mlp_gradient": ([vp, C.c_longlong, vp, vp, vp, _P], C.c_int),
         "phl_device_field": ([vp, C.c_char_p], vp),
         "phl_stream": ([vp], vp),
     }

@@ -1,9 +1,9 @@
 """Build the sm_100a shared library ``phlegethon_b200/_lib/libphl_b200.so`` in-tree.
 
-FP64 translation units are compiled with ``--fmad=false``: the reference's CPU build targets
-baseline x86-64 (no FMA, Make.local/Make.pkgconfig:91-93), and keeping every multiply and add
-separately rounded lets the FP64 path reproduce it bit for bit.  The FP32 split-precision unit
-is compiled with contraction on.
+The FP64 unit is compiled with ``--fmad=false``: the reference's CPU build targets baseline
+x86-64 (no FMA, Make.local/Make.pkgconfig:91-93), and keeping every multiply and add separately
+rounded lets the FP64 path reproduce it bit for bit.  The FP32 split-precision unit is compiled
+with contraction on and approximate FP32 division/square root.
 """
 from __future__ import annotations
 
@@ -22,7 +22,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (source, extra flags)
 UNITS = [
     ("phl_runtime.cu", ["--fmad=false"]),
-    ("phl_split.cu", ["--fmad=false"]),
+    # FP32 flux arithmetic of the split form: approximate (2 ulp) division and square root,
+    # FP32 denormals flushed; the FP64 EoS/state arithmetic in this unit is unaffected
+    ("phl_split.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
 ]
 
 

@@ -1,0 +1,186 @@
+// phl_eos_fast.cuh -- Helmholtz (rho, e) -> T inversion for the split-precision form.
+//
+// Same mathematics as helm_rhoe_given / helm_rhoT_given2 / helm_rhoT_given_full
+// (source/source.F90:23686-25019): biquintic Hermite interpolation of the free energy, Newton on
+// E(T) = e with the reference's tolerance, iteration cap and out-of-table reset.  The evaluation
+// order differs: the density is fixed during a solve, so for the current table cell the 36
+// coefficients are contracted once with the density basis into A[ot][jt] (value) and B[ot][jt]
+// (d/drho), ot = T-derivative order of the table variable, jt = lower/upper T node.  An
+// iteration then needs the T basis and 3 x 6 products; the contraction is redone only when T
+// leaves the cell.  Results agree with the reference evaluation to rounding.
+#pragma once
+#include "phl_device.cuh"
+
+namespace phl {
+
+// table node index (1-based like the reference) of x in the log-spaced nodes, from a single
+// precision log and exact comparisons against the node values
+__device__ __forceinline__ int helm_node_index(const double *nodes, int n, double log10_first, double dlog,
+                                               double x) {
+  float lx = __log2f((float)x) * 0.30102999566398120f;
+  int i = (int)(((double)lx - log10_first) / dlog) + 1;
+  i = max(1, min(i, n - 1));
+  if (i < n - 1 && __ldg(nodes + i) <= x) ++i;
+  if (i > 1 && __ldg(nodes + i - 1) > x) --i;
+  return i;
+}
+
+struct HelmCell {
+  int ih, jh;
+  double Ye, rhos, x, drho;
+  double r0[3], r1[3], dr0[3], dr1[3];  // density bases (value, d/drho) at the lower/upper node
+  double A[3][2], B[3][2];              // contracted coefficients of the current T cell
+  double T0, dT;                        // lower T node and spacing of the current T cell
+};
+
+__device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell &c, int jh) {
+  c.jh = jh;
+  c.T0 = __ldg(h.T + jh - 1);
+  c.dT = __ldg(h.T + jh) - c.T0;
+  // variables grouped by T order: ot 0 -> (f, f_d, f_dd), 1 -> (f_T, f_dT, f_ddT), 2 -> (f_TT, ...)
+  const int var[3][3] = {{0, 3, 4}, {1, 5, 6}, {2, 7, 8}};
+#pragma unroll
+  for (int jt = 0; jt < 2; ++jt) {
+    const double *lo = h.tab + 9 * ((long long)(c.ih - 1) + (long long)h.nrho * (jh - 1 + jt));
+    const double *hi = lo + 9;
+#pragma unroll
+    for (int ot = 0; ot < 3; ++ot) {
+      double a = 0.0, b = 0.0;
+#pragma unroll
+      for (int orr = 0; orr < 3; ++orr) {
+        double cl = __ldg(lo + var[ot][orr]), ch = __ldg(hi + var[ot][orr]);
+        a = fma(cl, c.r0[orr], fma(ch, c.r1[orr], a));
+        b = fma(cl, c.dr0[orr], fma(ch, c.dr1[orr], b));
+      }
+      c.A[ot][jt] = a;
+      c.B[ot][jt] = b;
+    }
+  }
+}
+
+__device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, double rho, double abar,
+                                               double zbar, double T) {
+  c.Ye = zbar / abar;
+  c.rhos = rho * c.Ye;
+  c.ih = helm_node_index(h.rho, h.nrho, h.log10_rho1, h.drho, c.rhos);
+  double r_lo = __ldg(h.rho + c.ih - 1);
+  c.drho = __ldg(h.rho + c.ih) - r_lo;
+  double idrho = 1.0 / c.drho;
+  c.x = (c.rhos - r_lo) * idrho;
+  double omx = 1.0 - c.x;
+  hb0(c.x, c.drho, c.drho * c.drho, c.r0);
+  hb0m(omx, c.drho, c.drho * c.drho, c.r1);
+  hb1(c.x, idrho, c.drho, c.dr0);
+  hb1m(omx, idrho, c.drho, c.dr1);
+  helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
+}
+
+// f, f_T, f_TT at T (T inside the current cell)
+__device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, double &f, double &fT, double &fTT) {
+  double idT = 1.0 / c.dT;
+  double y = (T - c.T0) * idT, omy = 1.0 - y;
+  double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
+  hb0(y, c.dT, c.dT * c.dT, t0);
+  hb0m(omy, c.dT, c.dT * c.dT, t1);
+  hb1(y, idT, c.dT, d0);
+  hb1m(omy, idT, c.dT, d1);
+  hb2(y, idT * idT, idT, e0);
+  hb2m(omy, idT * idT, idT, e1);
+  f = fT = fTT = 0.0;
+#pragma unroll
+  for (int ot = 0; ot < 3; ++ot) {
+    f = fma(c.A[ot][0], t0[ot], fma(c.A[ot][1], t1[ot], f));
+    fT = fma(c.A[ot][0], d0[ot], fma(c.A[ot][1], d1[ot], fT));
+    fTT = fma(c.A[ot][0], e0[ot], fma(c.A[ot][1], e1[ot], fTT));
+  }
+}
+
+// Newton on E(rho, T) = E0 from the warm start T (helm_rhoe_given's loop and exit rules);
+// returns iterations, sets converged / clamped.  On return `c` holds the cell of the final T.
+__device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, double rho, double E0,
+                                              double inv_abar, double &T, int max_iter, int &clamped,
+                                              bool &converged) {
+  const double Told = T;
+  const double irho = 1.0 / rho;
+  converged = false;
+  int used = 0;
+  for (int iter = 1; iter <= max_iter; ++iter) {
+    used = iter;
+    if (T < c.T0 || T >= c.T0 + c.dT) helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
+    double f, fT, fTT;
+    helm_cell_eval(c, T, f, fT, fTT);
+    double T3 = T * T * T;
+    double E = c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T3 * T * irho;
+    double dE = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
+    double res = E - E0;
+    T = T - res / dE;
+    double error = fabs(res / E0);
+    if ((T < h.Tl) || (T > h.Th)) {
+      T = Told;
+      error = EM15;
+      ++clamped;
+    }
+    if (error < HELM_TOL) { converged = true; break; }
+  }
+  if (T < c.T0 || T >= c.T0 + c.dT) helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
+  return used;
+}
+
+// pressure and relativistic sound speed at (rho, T) from the prepared cell (given_full's output)
+__device__ __forceinline__ void helm_cell_p_sound(const HelmTable &h, const HelmCell &c, double rho, double T,
+                                                  double inv_abar, double &P, double &sound) {
+  double idT = 1.0 / c.dT;
+  double y = (T - c.T0) * idT, omy = 1.0 - y;
+  double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
+  hb0(y, c.dT, c.dT * c.dT, t0);
+  hb0m(omy, c.dT, c.dT * c.dT, t1);
+  hb1(y, idT, c.dT, d0);
+  hb1m(omy, idT, c.dT, d1);
+  hb2(y, idT * idT, idT, e0);
+  hb2m(omy, idT * idT, idT, e1);
+  double f = 0, fT = 0, fTT = 0, fd = 0, fdT = 0;
+#pragma unroll
+  for (int ot = 0; ot < 3; ++ot) {
+    f = fma(c.A[ot][0], t0[ot], fma(c.A[ot][1], t1[ot], f));
+    fT = fma(c.A[ot][0], d0[ot], fma(c.A[ot][1], d1[ot], fT));
+    fTT = fma(c.A[ot][0], e0[ot], fma(c.A[ot][1], e1[ot], fTT));
+    fd = fma(c.B[ot][0], t0[ot], fma(c.B[ot][1], t1[ot], fd));
+    fdT = fma(c.B[ot][0], d0[ot], fma(c.B[ot][1], d1[ot], fdT));
+  }
+  // bicubic dP/d(rho Ye) (source.F90:24082-24118)
+  double x = c.x, omx = 1.0 - x;
+  double p0r = (2.0 * x - 3.0) * x * x + 1.0, p1r = ((x - 2.0) * x + 1.0) * x * c.drho;
+  double p0mr = (2.0 * omx - 3.0) * omx * omx + 1.0, p1mr = -((omx - 2.0) * omx + 1.0) * omx * c.drho;
+  double p0t = (2.0 * y - 3.0) * y * y + 1.0, p1t = ((y - 2.0) * y + 1.0) * y * c.dT;
+  double p0mt = (2.0 * omy - 3.0) * omy * omy + 1.0, p1mt = -((omy - 2.0) * omy + 1.0) * omy * c.dT;
+  const double *q00 = h.dpdr + 4 * ((long long)(c.ih - 1) + (long long)h.nrho * (c.jh - 1));
+  const double *q10 = q00 + 4, *q01 = q00 + 4 * (long long)h.nrho, *q11 = q01 + 4;
+  double rb[2][2] = {{p0r, p0mr}, {p1r, p1mr}}, tb[2][2] = {{p0t, p0mt}, {p1t, p1mt}};
+  const int ordr[4] = {0, 0, 1, 1}, ordt[4] = {0, 1, 0, 1};  // c, c_T, c_rho, c_rhoT
+  double dpd = 0.0;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    dpd = fma(__ldg(q00 + v) * rb[ordr[v]][0], tb[ordt[v]][0], dpd);
+    dpd = fma(__ldg(q10 + v) * rb[ordr[v]][1], tb[ordt[v]][0], dpd);
+    dpd = fma(__ldg(q01 + v) * rb[ordr[v]][0], tb[ordt[v]][1], dpd);
+    dpd = fma(__ldg(q11 + v) * rb[ordr[v]][1], tb[ordt[v]][1], dpd);
+  }
+  double dP_drho = c.Ye * dpd;
+  double r2 = c.rhos * c.rhos;
+  double T3 = T * T * T, T4 = T3 * T;
+  double irho = 1.0 / rho;
+  P = r2 * fd + CONST_RGAS * rho * T * inv_abar + CONST_RAD * T4 * (1.0 / 3.0);
+  double dP_dT = r2 * fdT + CONST_RGAS * rho * inv_abar + (4.0 / 3.0) * CONST_RAD * T3;
+  dP_drho = dP_drho + CONST_RGAS * T * inv_abar;
+  double E = c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T4 * irho;
+  double cv = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
+  double zz = P * irho;
+  double chiT = T / P * dP_dT;
+  double chirho = dP_drho / zz;
+  double xx = zz * chiT / (T * cv);
+  double gam1 = chiT * xx + chirho;
+  double z = 1.0 + (E + CONST_C2) / zz;
+  sound = CONST_C * sqrt(gam1 / z);
+}
+
+}  // namespace phl

@@ -1,68 +1,415 @@
 // phl_mlp.cuh -- learned initial temperature guess for the (rho, e) -> T Newton inversion.
-// No reference counterpart.  A 4-64-64-1 MLP maps (log10 rho, log10 e, Abar, Zbar), normalised,
-// to log10 T.  Parameters live in FP32 (master copy for Adam) and BF16 (tensor-core operands).
+// No reference counterpart.  A 4-64-64-1 MLP maps normalised (log10 rho, log10 e, Abar, Zbar)
+// to log10 T.  Parameters: FP32 master copy (Adam) plus a BF16 copy of the 64x64 hidden layer,
+// which runs on the tensor cores (BF16 operands, FP32 accumulate) in training and inference;
+// the 4->64 input layer and the 64->1 output layer are FP32 on the CUDA cores.
+//
+// Training (all on the device): samples are drawn with a counter-based hash over the EoS
+// benchmark ranges and labelled by the forward EoS (helm_rhoT_given2); each step a CTA takes 64
+// samples through forward and backward passes (three 64x64x64 tensor-core products: layer-2
+// forward, dH1 = dH2 W2, dW2 = dH2^T H1), writes its partial gradient, a second kernel sums the
+// partials in a fixed order (deterministic), and a third applies Adam.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <mma.h>
+#include "phl_device.cuh"
 
 namespace phl {
 
 constexpr int MLP_IN = 4, MLP_H = 64;
-constexpr int MLP_NPARAM = MLP_IN * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1;
+// parameter layout: W1[64][4], b1[64], W2[64][64] (out, in), b2[64], W3[64], b3
+constexpr int MLP_OFF_W1 = 0, MLP_OFF_B1 = 256, MLP_OFF_W2 = 320, MLP_OFF_B2 = 4416, MLP_OFF_W3 = 4480,
+              MLP_OFF_B3 = 4544, MLP_NPARAM = 4545;
+constexpr int MLP_TILE = 64;  // samples per CTA in training
 
-// fixed input/output normalisation over config-4 style ranges
-__device__ __forceinline__ void mlp_features(double rho, double e, double abar, double zbar, float f[4]) {
+// Inputs: log10 rho, log10 of the thermal part of the specific energy e_th = e - E(rho, T_lo)
+// (T_lo the table's lowest temperature), Abar, Zbar, each mapped to about [-1, 1] over the EoS
+// benchmark ranges.  Subtracting the cold energy removes the T-independent degenerate part, so
+// log T stays a smooth function of the inputs where the electrons are degenerate.
+__host__ __device__ __forceinline__ void mlp_features(double rho, double e_th, double abar, double zbar,
+                                                      float f[4]) {
   f[0] = (float)((log10(rho) - 3.5) / 5.5);
-  f[1] = (float)((log10(fabs(e) + 1e-300) - 16.0) / 6.0);
+  f[1] = (float)((log10(fmax(e_th, 1e-300)) - 19.5) / 8.5);
   f[2] = (float)((abar - 28.5) / 27.5);
   f[3] = (float)((zbar - 14.0) / 14.0);
 }
-__host__ __device__ __forceinline__ float mlp_out_scale() { return 3.0f; }
-__host__ __device__ __forceinline__ float mlp_out_shift() { return 7.0f; }
+// cold (lowest-table-temperature) specific energy of the mixture at rho
+__device__ __forceinline__ double mlp_cold_energy(const HelmTable &h, double rho, double abar, double zbar) {
+  double E, dE;
+  helm_given2(h, rho, __ldg(h.T), abar, zbar, E, dE, false);
+  return E;
+}
+// Fixed (non-trained) skip connection: log10 of the temperature at which ideal ions plus
+// radiation alone would hold e_th, (T_ion^-4 + T_rad^-4)^(-1/4) with T_ion = e_th Abar / (3/2 R)
+// and T_rad = (e_th rho / a)^(1/4); both parts are the analytic terms the reference adds outside
+// the table.  It is computed from the features, so the network maps features -> log10 T as
+//   log10 T = prior(features) + MLP_OUT_SCALE * y + MLP_OUT_SHIFT,
+// and the trained part only learns what the electron table contributes.
+__host__ __device__ __forceinline__ float mlp_prior(const float f[4]) {
+  const float lrho = 5.5f * f[0] + 3.5f, le = 8.5f * f[1] + 19.5f, abar = 27.5f * f[2] + 28.5f;
+  const float l_ion = le + log10f(abar) - 8.095925f;        // log10(3/2 R)
+  const float l_rad = 0.25f * (le + lrho + 14.121147f);     // -log10(a)
+  const float m = fminf(l_ion, l_rad);
+  return m - 0.25f * log10f(1.0f + exp10f(-4.0f * fabsf(l_ion - l_rad)));
+}
+constexpr float MLP_OUT_SCALE = 0.5f, MLP_OUT_SHIFT = -0.75f;
 
 struct MlpWeights {
-  const float *w;  // FP32 params: W1[64][4], b1[64], W2[64][64], b2[64], W3[64], b3
+  const float *w;               // FP32 master parameters
+  const __nv_bfloat16 *w2bf;    // BF16 copy of W2 (row-major [out][in])
 };
 
-// scalar FP32 forward pass of one sample (used where one thread owns one sample)
-__device__ __forceinline__ float mlp_forward_scalar(const MlpWeights &m, const float x[4]) {
-  const float *W1 = m.w, *b1 = W1 + MLP_H * MLP_IN, *W2 = b1 + MLP_H, *b2 = W2 + MLP_H * MLP_H;
-  const float *W3 = b2 + MLP_H, *b3 = W3 + MLP_H;
-  float h1[MLP_H];
-#pragma unroll
-  for (int o = 0; o < MLP_H; ++o) {
-    float a = __ldg(b1 + o);
-#pragma unroll
-    for (int i = 0; i < MLP_IN; ++i) a += __ldg(W1 + o * MLP_IN + i) * x[i];
-    h1[o] = a > 0.f ? a : 0.f;
+// counter-based sample of the EoS benchmark distribution: log10 rho ~ U[-2,9],
+// log10 T ~ U[4,10], Abar ~ U[1,56], Zbar ~ U[1, max(Abar/2,1)]
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ double u01(unsigned long long seed, long long i, int c) {
+  unsigned long long h = mix64(mix64(seed ^ (unsigned long long)i * 0x100000001B3ull) + (unsigned long long)c);
+  return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void k_mlp_make_samples(HelmTable h, long long n, unsigned long long seed, float *feat, float *target) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double lrho = -2.0 + 11.0 * u01(seed, i, 0);
+  double lT = 4.0 + 6.0 * u01(seed, i, 1);
+  double abar = 1.0 + 55.0 * u01(seed, i, 2);
+  double zbar = 1.0 + fmax(abar * 0.5 - 1.0, 0.0) * u01(seed, i, 3);
+  double rho = exp10(lrho), T = exp10(lT), E, dE;
+  helm_given2(h, rho, T, abar, zbar, E, dE, false);
+  float f[4];
+  mlp_features(rho, E - mlp_cold_energy(h, rho, abar, zbar), abar, zbar, f);
+  for (int k = 0; k < 4; ++k) feat[i * 4 + k] = f[k];
+  target[i] = (float)((lT - (double)mlp_prior(f) - MLP_OUT_SHIFT) / MLP_OUT_SCALE);
+}
+
+// ------------------------------------------------------------------ training step (one CTA = 64 samples)
+// shared layout (bytes): X 64x4 f32 | T 64 f32 | H1 64x64 f32 | H1b 64x64 bf16 | W2b 64x64 bf16 |
+// Z 64x64 f32 (Z2, later dH1) | G 64x64 bf16 (dH2) | Gf 64x64 f32 (dH2) | y 64 f32
+struct MlpTrainSmem {
+  float X[MLP_TILE][4];
+  float T[MLP_TILE];
+  float y[MLP_TILE];
+  float H1[MLP_TILE][MLP_H];
+  float Z[MLP_TILE][MLP_H];
+  float Gf[MLP_TILE][MLP_H];
+  alignas(32) __nv_bfloat16 H1b[MLP_TILE][MLP_H];
+  alignas(32) __nv_bfloat16 W2b[MLP_H][MLP_H];
+  alignas(32) __nv_bfloat16 Gb[MLP_TILE][MLP_H];
+  alignas(32) float dW2[MLP_H][MLP_H];
+};
+
+__global__ void __launch_bounds__(128) k_mlp_train_step(const float *params, const __nv_bfloat16 *w2bf,
+                                                        const float *feat, const float *target, long long n,
+                                                        long long offset, int batch, float *partial,
+                                                        float *loss_partial) {
+  using namespace nvcuda;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  MlpTrainSmem &S = *reinterpret_cast<MlpTrainSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const float *W1 = params + MLP_OFF_W1, *b1 = params + MLP_OFF_B1, *b2 = params + MLP_OFF_B2;
+  const float *W3 = params + MLP_OFF_W3, b3 = params[MLP_OFF_B3];
+  const long long base = offset + (long long)blockIdx.x * MLP_TILE;
+  // samples (wrapping around the training set)
+  for (int q = tid; q < MLP_TILE * 4; q += blockDim.x) {
+    long long s = (base + q / 4) % n;
+    S.X[q / 4][q % 4] = feat[s * 4 + q % 4];
   }
-  float out = __ldg(b3);
-  for (int o = 0; o < MLP_H; ++o) {
-    float a = __ldg(b2 + o);
+  for (int q = tid; q < MLP_TILE; q += blockDim.x) S.T[q] = target[(base + q) % n];
+  for (int q = tid; q < MLP_H * MLP_H; q += blockDim.x) S.W2b[q / MLP_H][q % MLP_H] = w2bf[q];
+  __syncthreads();
+  // layer 1 (FP32)
+  for (int q = tid; q < MLP_TILE * MLP_H; q += blockDim.x) {
+    int s = q / MLP_H, o = q % MLP_H;
+    float a = b1[o];
 #pragma unroll
-    for (int i = 0; i < MLP_H; ++i) a += __ldg(W2 + o * MLP_H + i) * h1[i];
-    out += __ldg(W3 + o) * (a > 0.f ? a : 0.f);
+    for (int k = 0; k < 4; ++k) a = fmaf(W1[o * 4 + k], S.X[s][k], a);
+    a = fmaxf(a, 0.0f);
+    S.H1[s][o] = a;
+    S.H1b[s][o] = __float2bfloat16(a);
   }
-  return out * mlp_out_scale() + mlp_out_shift();
+  __syncthreads();
+  // layer 2 on the tensor cores: Z[s][o] = sum_i H1[s][i] W2[o][i]; warp w owns rows 16w..16w+15
+  {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::col_major> b;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      wmma::fill_fragment(acc, 0.0f);
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+        wmma::load_matrix_sync(a, &S.H1b[16 * warp][16 * kt], MLP_H);
+        wmma::load_matrix_sync(b, &S.W2b[16 * nt][16 * kt], MLP_H);  // B(k=i, n=o) = W2[o][i]
+        wmma::mma_sync(acc, a, b, acc);
+      }
+      wmma::store_matrix_sync(&S.Z[16 * warp][16 * nt], acc, MLP_H, wmma::mem_row_major);
+    }
+  }
+  __syncthreads();
+  // bias + ReLU -> H2 (kept in Z), output layer, loss gradient
+  for (int q = tid; q < MLP_TILE * MLP_H; q += blockDim.x) {
+    int s = q / MLP_H, o = q % MLP_H;
+    S.Z[s][o] = fmaxf(S.Z[s][o] + b2[o], 0.0f);
+  }
+  __syncthreads();
+  if (tid < MLP_TILE) {
+    float a = b3;
+    for (int o = 0; o < MLP_H; ++o) a = fmaf(W3[o], S.Z[tid][o], a);
+    float d = a - S.T[tid];
+    S.y[tid] = 2.0f * d / (float)batch;  // dL/dy for L = mean (y - t)^2
+    loss_partial[blockIdx.x * MLP_TILE + tid] = d * d;
+  }
+  __syncthreads();
+  // dH2 = dy W3 * relu'(H2)
+  for (int q = tid; q < MLP_TILE * MLP_H; q += blockDim.x) {
+    int s = q / MLP_H, o = q % MLP_H;
+    float g = S.Z[s][o] > 0.0f ? S.y[s] * W3[o] : 0.0f;
+    S.Gf[s][o] = g;
+    S.Gb[s][o] = __float2bfloat16(g);
+  }
+  __syncthreads();
+  float *P = partial + (long long)blockIdx.x * MLP_NPARAM;
+  // dW3, b3, b2 from FP32 H2 / dH2
+  for (int o = tid; o < MLP_H; o += blockDim.x) {
+    float gw3 = 0.0f, gb2 = 0.0f;
+    for (int s = 0; s < MLP_TILE; ++s) {
+      gw3 = fmaf(S.y[s], S.Z[s][o], gw3);
+      gb2 += S.Gf[s][o];
+    }
+    P[MLP_OFF_W3 + o] = gw3;
+    P[MLP_OFF_B2 + o] = gb2;
+  }
+  if (tid == 0) {
+    float g = 0.0f;
+    for (int s = 0; s < MLP_TILE; ++s) g += S.y[s];
+    P[MLP_OFF_B3] = g;
+  }
+  __syncthreads();
+  // tensor cores: dH1pre[s][i] = sum_o dH2[s][o] W2[o][i] (into Z) and
+  // dW2[o][i] = sum_s dH2[s][o] H1[s][i]
+  {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::col_major> at;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      wmma::fill_fragment(acc, 0.0f);
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+        wmma::load_matrix_sync(a, &S.Gb[16 * warp][16 * kt], MLP_H);     // A(s, o) = dH2[s][o]
+        wmma::load_matrix_sync(b, &S.W2b[16 * kt][16 * nt], MLP_H);      // B(k=o, n=i) = W2[o][i]
+        wmma::mma_sync(acc, a, b, acc);
+      }
+      wmma::store_matrix_sync(&S.Z[16 * warp][16 * nt], acc, MLP_H, wmma::mem_row_major);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      wmma::fill_fragment(acc, 0.0f);
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+        wmma::load_matrix_sync(at, &S.Gb[16 * kt][16 * warp], MLP_H);    // A(o, s) = dH2[s][o]
+        wmma::load_matrix_sync(b, &S.H1b[16 * kt][16 * nt], MLP_H);      // B(k=s, n=i) = H1[s][i]
+        wmma::mma_sync(acc, at, b, acc);
+      }
+      wmma::store_matrix_sync(&S.dW2[16 * warp][16 * nt], acc, MLP_H, wmma::mem_row_major);
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < MLP_H * MLP_H; q += blockDim.x) P[MLP_OFF_W2 + q] = S.dW2[q / MLP_H][q % MLP_H];
+  // dH1 = dH1pre * relu'(H1); dW1, db1 (FP32)
+  for (int q = tid; q < MLP_TILE * MLP_H; q += blockDim.x) {
+    int s = q / MLP_H, i = q % MLP_H;
+    S.Z[s][i] = S.H1[s][i] > 0.0f ? S.Z[s][i] : 0.0f;
+  }
+  __syncthreads();
+  for (int o = tid; o < MLP_H; o += blockDim.x) {
+    float g[4] = {0, 0, 0, 0}, gb = 0.0f;
+    for (int s = 0; s < MLP_TILE; ++s) {
+      float d = S.Z[s][o];
+      gb += d;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) g[k] = fmaf(d, S.X[s][k], g[k]);
+    }
+    for (int k = 0; k < 4; ++k) P[MLP_OFF_W1 + o * 4 + k] = g[k];
+    P[MLP_OFF_B1 + o] = gb;
+  }
+}
+
+// fixed-order sum of the per-CTA partial gradients
+__global__ void k_mlp_reduce(const float *partial, int nblocks, float *grad) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= MLP_NPARAM) return;
+  float s = 0.0f;
+  for (int b = 0; b < nblocks; ++b) s += partial[(long long)b * MLP_NPARAM + p];
+  grad[p] = s;
+}
+
+__global__ void k_mlp_adam(float *params, const float *grad, float *m, float *v, float lr, float b1, float b2,
+                           float eps, int step, __nv_bfloat16 *w2bf) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= MLP_NPARAM) return;
+  float g = grad[p];
+  float mm = b1 * m[p] + (1.0f - b1) * g;
+  float vv = b2 * v[p] + (1.0f - b2) * g * g;
+  m[p] = mm;
+  v[p] = vv;
+  float mh = mm / (1.0f - powf(b1, (float)step)), vh = vv / (1.0f - powf(b2, (float)step));
+  float w = params[p] - lr * mh / (sqrtf(vh) + eps);
+  params[p] = w;
+  if (p >= MLP_OFF_W2 && p < MLP_OFF_B2) w2bf[p - MLP_OFF_W2] = __float2bfloat16(w);
+}
+
+__global__ void k_mlp_to_bf16(const float *params, __nv_bfloat16 *w2bf) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < MLP_H * MLP_H) w2bf[q] = __float2bfloat16(params[MLP_OFF_W2 + q]);
+}
+
+__global__ void k_mlp_init(float *params, unsigned long long seed) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= MLP_NPARAM) return;
+  double u = u01(seed, p, 7) * 2.0 - 1.0;
+  float w = 0.0f;
+  if (p < MLP_OFF_B1) w = (float)(u * 0.5 * 1.7320508);                 // fan-in 4
+  else if (p >= MLP_OFF_W2 && p < MLP_OFF_B2) w = (float)(u * 0.125 * 1.7320508 * 1.414);  // fan-in 64
+  else if (p >= MLP_OFF_W3 && p < MLP_OFF_B3) w = (float)(u * 0.125 * 1.7320508);
+  else if (p >= MLP_OFF_B1 && p < MLP_OFF_W2) w = 0.01f;
+  else if (p >= MLP_OFF_B2 && p < MLP_OFF_W3) w = 0.01f;
+  params[p] = w;
+}
+
+// ------------------------------------------------------------------ warp-cooperative inference
+// 32 samples per warp (one per lane): layer 1 per lane, layer 2 as a 32x64x64 tensor-core
+// product through shared memory, layer 3 per lane.  Shared rows are padded (72 bf16, 68 f32) and
+// each lane moves its row in 16-byte pieces, so the per-lane row accesses are free of bank
+// conflicts (the 8 lanes of a 16-byte access phase land on disjoint 4-bank groups).
+constexpr int MLP_LDB = 72;  // padded bf16 row (activations and the W2 copy)
+constexpr int MLP_LDZ = 68;  // padded f32 row (layer-2 products)
+
+__device__ __forceinline__ void mlp_stage_w2(__nv_bfloat16 *w2s, const __nv_bfloat16 *w2bf) {
+  // 64 rows x 8 pieces of 16 bytes
+  for (int q = threadIdx.x; q < MLP_H * 8; q += blockDim.x) {
+    int r = q >> 3, c = q & 7;
+    *reinterpret_cast<uint4 *>(w2s + r * MLP_LDB + 8 * c) = __ldg(reinterpret_cast<const uint4 *>(w2bf + r * MLP_H) + c);
+  }
+}
+
+__device__ __forceinline__ float mlp_forward_warp(const MlpWeights &m, const float x[4], __nv_bfloat16 *hb,
+                                                  float *z, const __nv_bfloat16 *w2s) {
+  using namespace nvcuda;
+  const int lane = threadIdx.x & 31;
+  const float *W1 = m.w + MLP_OFF_W1, *b1 = m.w + MLP_OFF_B1, *b2 = m.w + MLP_OFF_B2, *W3 = m.w + MLP_OFF_W3;
+#pragma unroll 2
+  for (int c = 0; c < MLP_H / 8; ++c) {
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int o = 8 * c + j;
+      float a = __ldg(b1 + o);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a = fmaf(__ldg(W1 + o * 4 + k), x[k], a);
+      v[j] = __float2bfloat16(fmaxf(a, 0.0f));
+    }
+    *reinterpret_cast<uint4 *>(hb + lane * MLP_LDB + 8 * c) = *reinterpret_cast<const uint4 *>(v);
+  }
+  __syncwarp();
+  wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+  wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::col_major> b;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      wmma::fill_fragment(acc, 0.0f);
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) {
+        wmma::load_matrix_sync(a, hb + (16 * mt) * MLP_LDB + 16 * kt, MLP_LDB);
+        wmma::load_matrix_sync(b, w2s + (16 * nt) * MLP_LDB + 16 * kt, MLP_LDB);
+        wmma::mma_sync(acc, a, b, acc);
+      }
+      wmma::store_matrix_sync(z + (16 * mt) * MLP_LDZ + 16 * nt, acc, MLP_LDZ, wmma::mem_row_major);
+    }
+  }
+  __syncwarp();
+  float out = __ldg(m.w + MLP_OFF_B3);
+#pragma unroll 4
+  for (int c = 0; c < MLP_H / 4; ++c) {
+    float4 q = *reinterpret_cast<const float4 *>(z + lane * MLP_LDZ + 4 * c);
+    out = fmaf(__ldg(W3 + 4 * c + 0), fmaxf(q.x + __ldg(b2 + 4 * c + 0), 0.0f), out);
+    out = fmaf(__ldg(W3 + 4 * c + 1), fmaxf(q.y + __ldg(b2 + 4 * c + 1), 0.0f), out);
+    out = fmaf(__ldg(W3 + 4 * c + 2), fmaxf(q.z + __ldg(b2 + 4 * c + 2), 0.0f), out);
+    out = fmaf(__ldg(W3 + 4 * c + 3), fmaxf(q.w + __ldg(b2 + 4 * c + 3), 0.0f), out);
+  }
+  __syncwarp();
+  return mlp_prior(x) + out * MLP_OUT_SCALE + MLP_OUT_SHIFT;
+}
+
+// dynamic shared memory of a block of `warps` warps running mlp_forward_warp
+__host__ __device__ constexpr size_t mlp_warp_smem(int warps) {
+  return sizeof(__nv_bfloat16) * MLP_H * MLP_LDB +
+         (size_t)warps * 32 * (MLP_LDB * sizeof(__nv_bfloat16) + MLP_LDZ * sizeof(float));
+}
+// carve the block's shared memory: W2 copy, then per-warp activations (all pieces 32-byte aligned)
+__device__ __forceinline__ void mlp_smem_carve(unsigned char *sm, int warps, int warp, __nv_bfloat16 *&w2s,
+                                               __nv_bfloat16 *&hb, float *&z) {
+  w2s = reinterpret_cast<__nv_bfloat16 *>(sm);
+  hb = w2s + MLP_H * MLP_LDB + (size_t)warp * 32 * MLP_LDB;
+  z = reinterpret_cast<float *>(sm + sizeof(__nv_bfloat16) * MLP_H * MLP_LDB +
+                                (size_t)warps * 32 * MLP_LDB * sizeof(__nv_bfloat16)) +
+      (size_t)warp * 32 * MLP_LDZ;
+}
+
+// per-sample inference kernel (features n x 4 -> log10 T), 128 threads per block
+__global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __nv_bfloat16 *w2s, *hb;
+  float *z;
+  mlp_smem_carve(sm, 4, threadIdx.x >> 5, w2s, hb, z);
+  mlp_stage_w2(w2s, m.w2bf);
+  __syncthreads();
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float x[4] = {0, 0, 0, 0};
+  if (t < n)
+    for (int k = 0; k < 4; ++k) x[k] = feat[t * 4 + k];
+  float y = mlp_forward_warp(m, x, hb, z, w2s);
+  if (t < n) out[t] = y;
 }
 
 struct Mlp {
   bool ready = false;
-  float *params = nullptr;
+  float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *partial = nullptr, *lossp = nullptr;
+  float *feat = nullptr, *target = nullptr;
+  __nv_bfloat16 *w2bf = nullptr;
+  long long nsamp = 0;
+  int npart = 0;
+
   void release() {
-    if (params) cudaFree(params);
-    params = nullptr;
+    for (void *p : {(void *)params, (void *)grad, (void *)m, (void *)v, (void *)partial, (void *)lossp,
+                    (void *)feat, (void *)target, (void *)w2bf})
+      if (p) cudaFree(p);
+    params = grad = m = v = partial = lossp = feat = target = nullptr;
+    w2bf = nullptr;
     ready = false;
   }
-  MlpWeights weights() const { return MlpWeights{params}; }
+  MlpWeights weights() const { return MlpWeights{params, w2bf}; }
   int alloc() {
     if (params) return 0;
-    if (cudaMalloc(&params, sizeof(float) * MLP_NPARAM) != cudaSuccess) return -2;
+    if (cudaMalloc(&params, sizeof(float) * MLP_NPARAM) || cudaMalloc(&grad, sizeof(float) * MLP_NPARAM) ||
+        cudaMalloc(&m, sizeof(float) * MLP_NPARAM) || cudaMalloc(&v, sizeof(float) * MLP_NPARAM) ||
+        cudaMalloc(&w2bf, sizeof(__nv_bfloat16) * MLP_H * MLP_H))
+      return -2;
     return 0;
   }
   int set(cudaStream_t s, const float *h) {
     if (alloc()) return -2;
     if (cudaMemcpyAsync(params, h, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, s) != cudaSuccess) return -2;
+    k_mlp_to_bf16<<<(MLP_H * MLP_H + 255) / 256, 256, 0, s>>>(params, w2bf);
     if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
     ready = true;
     return 0;
@@ -73,8 +420,117 @@ struct Mlp {
     if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
     return 0;
   }
-  int train(const HelmTable &, cudaStream_t, long long, unsigned long long, int, int, double, double *) { return -6; }
-  int infer(cudaStream_t, long long, const float *, float *) { return -6; }
+  // one gradient evaluation on `batch` samples starting at `offset` (grad -> this->grad);
+  // returns the mean squared loss through *loss when non-null
+  int gradient(cudaStream_t s, long long offset, int batch, double *loss) {
+    int nb = batch / MLP_TILE;
+    size_t sm = sizeof(MlpTrainSmem);
+    k_mlp_train_step<<<nb, 128, sm, s>>>(params, w2bf, feat, target, nsamp, offset, batch, partial, lossp);
+    k_mlp_reduce<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(partial, nb, grad);
+    if (cudaGetLastError() != cudaSuccess) return -2;
+    if (loss) {
+      float *h = new float[batch];
+      cudaMemcpyAsync(h, lossp, sizeof(float) * batch, cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) { delete[] h; return -2; }
+      double acc = 0;
+      for (int i = 0; i < batch; ++i) acc += h[i];
+      *loss = acc / batch;
+      delete[] h;
+    }
+    return 0;
+  }
+  int train(const HelmTable &h, cudaStream_t s, long long n, unsigned long long seed, int epochs, int batch,
+            double lr, double *final_loss) {
+    if (batch % MLP_TILE || batch <= 0 || n < batch) return -1;
+    if (alloc()) return -2;
+    if (n != nsamp) {
+      if (feat) cudaFree(feat);
+      if (target) cudaFree(target);
+      feat = target = nullptr;
+      if (cudaMalloc(&feat, sizeof(float) * 4 * n) || cudaMalloc(&target, sizeof(float) * n)) return -2;
+      nsamp = n;
+    }
+    int nb = batch / MLP_TILE;
+    if (nb > npart) {
+      if (partial) cudaFree(partial);
+      if (lossp) cudaFree(lossp);
+      partial = lossp = nullptr;
+      if (cudaMalloc(&partial, sizeof(float) * (size_t)nb * MLP_NPARAM) || cudaMalloc(&lossp, sizeof(float) * batch))
+        return -2;
+      npart = nb;
+    }
+    if (cudaFuncSetAttribute(k_mlp_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MlpTrainSmem)) != cudaSuccess)
+      return -2;
+    k_mlp_make_samples<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h, n, seed, feat, target);
+    if (!ready) {
+      k_mlp_init<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(params, seed ^ 0xABCDEFull);
+      k_mlp_to_bf16<<<(MLP_H * MLP_H + 255) / 256, 256, 0, s>>>(params, w2bf);
+    }
+    cudaMemsetAsync(m, 0, sizeof(float) * MLP_NPARAM, s);
+    cudaMemsetAsync(v, 0, sizeof(float) * MLP_NPARAM, s);
+    long long steps_per_epoch = n / batch;
+    int step = 0;
+    for (int ep = 0; ep < epochs; ++ep) {
+      // cosine-free schedule: constant lr for the first half, then linear decay to lr/20
+      for (long long k = 0; k < steps_per_epoch; ++k) {
+        ++step;
+        double frac = (double)(ep * steps_per_epoch + k) / (double)(epochs * steps_per_epoch);
+        float lr_t = (float)(frac < 0.5 ? lr : lr * (1.0 - 1.9 * (frac - 0.5)));
+        if (gradient(s, k * batch, batch, nullptr)) return -2;
+        k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(params, grad, m, v, lr_t, 0.9f, 0.999f, 1e-8f, step,
+                                                           w2bf);
+      }
+    }
+    if (cudaGetLastError() != cudaSuccess) return -2;
+    if (final_loss) {
+      if (gradient(s, 0, batch, final_loss)) return -2;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+    ready = true;
+    return 0;
+  }
+  // gradient on caller-provided pairs (host arrays), for checking against a CPU reference
+  int gradient_host(cudaStream_t s, long long n, const float *hf, const float *ht, float *hg, double *loss) {
+    if (!ready || n <= 0 || n % MLP_TILE) return -1;
+    if (n != nsamp) {
+      if (feat) cudaFree(feat);
+      if (target) cudaFree(target);
+      feat = target = nullptr;
+      if (cudaMalloc(&feat, sizeof(float) * 4 * n) || cudaMalloc(&target, sizeof(float) * n)) return -2;
+      nsamp = n;
+    }
+    int nb = (int)(n / MLP_TILE);
+    if (nb > npart) {
+      if (partial) cudaFree(partial);
+      if (lossp) cudaFree(lossp);
+      partial = lossp = nullptr;
+      if (cudaMalloc(&partial, sizeof(float) * (size_t)nb * MLP_NPARAM) || cudaMalloc(&lossp, sizeof(float) * n))
+        return -2;
+      npart = nb;
+    }
+    if (cudaFuncSetAttribute(k_mlp_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MlpTrainSmem)) != cudaSuccess)
+      return -2;
+    if (cudaMemcpyAsync(feat, hf, sizeof(float) * 4 * n, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(target, ht, sizeof(float) * n, cudaMemcpyHostToDevice, s))
+      return -2;
+    if (gradient(s, 0, (int)n, loss)) return -2;
+    if (cudaMemcpyAsync(hg, grad, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, s)) return -2;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+    return 0;
+  }
+  int infer(cudaStream_t s, long long n, const float *f, float *o) {
+    if (!ready) return -4;
+    if (n == 0) return 0;
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_warp_smem(4)) !=
+        cudaSuccess)
+      return -2;
+    k_mlp_infer<<<(unsigned)((n + 127) / 128), 128, mlp_warp_smem(4), s>>>(weights(), n, f, o);
+    if (cudaGetLastError() != cudaSuccess) return -2;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+    return 0;
+  }
 };
 
 }  // namespace phl

@@ -814,6 +814,7 @@ int phl_get_status(phl_ctx *ctx, phl_status *st) {
   st->mlp_accepted = (long long)h[STAT_MLP_ACC];
   st->mlp_rejected = (long long)h[STAT_MLP_REJ];
   st->nonfinite = (long long)h[STAT_NONFINITE];
+  st->guess_evaluations = (long long)h[STAT_GUESS_EVALS];
   st->steps = step;
   st->time = sc[0];
   st->dt = sc[1];
@@ -885,31 +886,36 @@ namespace {
 constexpr int NOALLOC_FIELDS = 7;  // rho, e, abar, zbar, T, p, cs
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_FIELDS * PHL_NOALLOC_MAX_SAMPLES];
 static __device__ __align__(256) int g_noalloc_iters[PHL_NOALLOC_MAX_SAMPLES];
+// queue of rejected learned guesses: count, then one entry per sample
+static __device__ __align__(256) unsigned long long g_noalloc_queue[PHL_NOALLOC_MAX_SAMPLES + 1];
 constexpr int NOALLOC_MAX_DEVICES = 64;
 double *g_noalloc_dev[NOALLOC_MAX_DEVICES] = {};
 int *g_noalloc_idev[NOALLOC_MAX_DEVICES] = {};
+unsigned long long *g_noalloc_qdev[NOALLOC_MAX_DEVICES] = {};
+
+int noalloc_symbol(void **dst, const void *symbol, const char *name) {
+  cudaError_t e = cudaGetSymbolAddress(dst, symbol);
+  if (e == cudaSuccess) return PHL_OK;
+  g_last_error = std::string("cudaGetSymbolAddress(") + name + "): " + cudaGetErrorString(e);
+  return PHL_E_CUDA;
+}
 
 // once per device, with that device current
-int noalloc_setup(int device, double **buf, int **ibuf) {
+int noalloc_setup(int device, double **buf, int **ibuf, unsigned long long **queue) {
   if (device < 0 || device >= NOALLOC_MAX_DEVICES) return PHL_E_INVALID;
   if (!g_noalloc_dev[device]) {
-    double *p = nullptr;
-    int *q = nullptr;
-    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
-      return PHL_E_CUDA;
-    }
-    e = cudaGetSymbolAddress((void **)&q, g_noalloc_iters);
-    if (e != cudaSuccess) {
-      g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_iters): ") + cudaGetErrorString(e);
-      return PHL_E_CUDA;
-    }
-    g_noalloc_dev[device] = p;
-    g_noalloc_idev[device] = q;
+    void *p = nullptr, *q = nullptr, *r = nullptr;
+    int rc;
+    if ((rc = noalloc_symbol(&p, g_noalloc_scratch, "g_noalloc_scratch"))) return rc;
+    if ((rc = noalloc_symbol(&q, g_noalloc_iters, "g_noalloc_iters"))) return rc;
+    if ((rc = noalloc_symbol(&r, g_noalloc_queue, "g_noalloc_queue"))) return rc;
+    g_noalloc_idev[device] = static_cast<int *>(q);
+    g_noalloc_qdev[device] = static_cast<unsigned long long *>(r);
+    g_noalloc_dev[device] = static_cast<double *>(p);
   }
   *buf = g_noalloc_dev[device];
   *ibuf = g_noalloc_idev[device];
+  *queue = g_noalloc_qdev[device];
   return PHL_OK;
 }
 }  // namespace
@@ -929,7 +935,8 @@ extern "C" int phl_eos_invert_batch_noalloc(phl_ctx *ctx, long long n, const dou
   CK(cudaSetDevice(ctx->cfg.device));
   double *buf = nullptr;
   int *ibuf = nullptr;
-  int rc = noalloc_setup(ctx->cfg.device, &buf, &ibuf);
+  unsigned long long *queue = nullptr;
+  int rc = noalloc_setup(ctx->cfg.device, &buf, &ibuf, &queue);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
   const size_t M = PHL_NOALLOC_MAX_SAMPLES, b = sizeof(double) * (size_t)n;
@@ -942,10 +949,9 @@ extern "C" int phl_eos_invert_batch_noalloc(phl_ctx *ctx, long long n, const dou
   CK(cudaMemcpyAsync(d_a, abar, b, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_z, zbar, b, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_T, T_inout, b, cudaMemcpyHostToDevice, s));
-  k_eos_invert<<<nblk(n, 128), 128, 0, s>>>(ctx->helm, n, d_rho, d_e, d_a, d_z, d_T, p ? d_p : nullptr,
-                                            cs ? d_c : nullptr, iters ? ibuf : nullptr, guess,
-                                            ctx->eos.mlp.weights(), ctx->stat);
-  CK(cudaGetLastError());
+  CK((cudaError_t)eos_launch(ctx->helm, s, n, d_rho, d_e, d_a, d_z, d_T, p ? d_p : nullptr, cs ? d_c : nullptr,
+                             iters ? ibuf : nullptr, guess, ctx->eos.mlp.weights(), ctx->stat, queue,
+                             ctx->eos.sm_count()));
   CK(cudaMemcpyAsync(T_inout, d_T, b, cudaMemcpyDeviceToHost, s));
   if (p) CK(cudaMemcpyAsync(p, d_p, b, cudaMemcpyDeviceToHost, s));
   if (cs) CK(cudaMemcpyAsync(cs, d_c, b, cudaMemcpyDeviceToHost, s));
@@ -962,6 +968,13 @@ int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs
   if (!ctx->table_loaded) return PHL_E_NO_TABLE;
   CK(cudaSetDevice(ctx->cfg.device));
   return ctx->eos.mlp_train(ctx->helm, ctx->stream, n, seed, epochs, batch, lr, final_loss);
+}
+
+int phl_mlp_gradient(phl_ctx *ctx, long long n, const float *features, const float *targets, float *grad,
+                     double *loss) {
+  if (!ctx || n <= 0 || !features || !targets || !grad) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  return ctx->eos.mlp_gradient(ctx->stream, n, features, targets, grad, loss);
 }
 
 int phl_mlp_get_params(phl_ctx *ctx, float *params) {

@@ -11,6 +11,7 @@
 // (rho / rho_ref, p / p_ref, v / v_ref with v_ref^2 = p_ref / rho_ref, phi / v_ref^2), fixed per run,
 // so products of deviations never leave FP32 range whatever the problem's cgs magnitudes.
 #include <cuda_runtime.h>
+#include "phl_eos_fast.cuh"
 #include "phl_runner.h"
 
 namespace phl {
@@ -264,14 +265,16 @@ __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
     if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
     double p, T, sound = 0.0;
     if (C::HELM) {
-      double ye = u[IAS] * inv_rho, abar = rho / u[IAS + 1], zbar = ye * abar;
+      double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
+      double abar = 1.0 / inv_abar, zbar = ye * abar;
       T = P.temp[c];
       int clamped = 0;
       bool conv = false;
-      int it = helm_rhoe_newton(P.helm, rho, eint * inv_rho, abar, zbar, T, 100, clamped, &conv);
+      HelmCell hc;
+      helm_cell_init(P.helm, hc, rho, abar, zbar, T);
+      int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
       n_calls += 1; n_iters += it; n_nonconv += !conv; n_clamp += clamped;
-      double E, cv;
-      helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
+      helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
       double ge = p / eint + 1.0, gc = sound * sound * rho / p;
       if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
       P.gf_out[c] = (float)ge;

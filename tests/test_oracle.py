@@ -9,6 +9,7 @@ known answers of the scheme and by an independent numpy restatement of the same 
   * the Helmholtz Newton inversions round-trip T -> e(rho,T) -> T and P(rho,T) -> T,
   * LIM2ND/LHLLC/HLLD of the oracle equal a vectorised numpy restatement bit for bit.
 """
+import ctypes as C
 import math
 
 import numpy as np
@@ -185,3 +186,22 @@ def test_table_thermodynamic_consistency():
     c = 2 * rho[i] * tab[3, i, j] + rho[i] ** 2 * tab[4, i, j]
     assert abs(c - dpdr[0, i, j]) / abs(dpdr[0, i, j]) < 1e-12
     del h
+
+
+def test_bracket_guess_batch_round_trip(oracle, table):
+    """Cold bracket guess + helm_rhoe_given Newton recovers T over the EoS benchmark ranges."""
+    cfg, _ = problems.stratified_3d(8)
+    helm = oracle.Helm.for_config(cfg, *table)
+    rho, T, abar, zbar = problems.eos_samples(2000, seed=31)
+    e = np.array([helm.given2(rho[i], T[i], abar[i], zbar[i])[0] for i in range(rho.size)])
+    Tb, it = helm.invert_batch(rho, e, abar, zbar, guess=2, nthreads=2)
+    assert it.max() < 100
+    E2 = np.array([helm.given2(rho[i], Tb[i], abar[i], zbar[i])[0] for i in range(rho.size)])
+    assert np.max(np.abs(E2 - e) / np.abs(e)) < 1e-11
+    # the guess itself lands between two table nodes: at most one node spacing (0.05 dex) off
+    Tg = np.zeros(1)
+    for i in range(0, rho.size, 97):
+        nev = oracle.load().phlo_eos_bracket_guess(C.byref(helm.s), rho[i], e[i], abar[i], zbar[i],
+                                                    Tg.ctypes.data_as(C.POINTER(C.c_double)))
+        assert 1 <= nev <= 2 + 8
+        assert abs(math.log10(Tg[0] / Tb[i])) < 0.06

@@ -17,14 +17,14 @@ from phlegethon_b200 import problems
 pytestmark = pytest.mark.gpu
 
 
-def _invert(sim, fn, rho, e, abar, zbar, T0):
+def _invert(sim, fn, rho, e, abar, zbar, T0, guess):
     n = rho.size
     T = T0.copy()
     p = np.zeros(n)
     cs = np.zeros(n)
     it = np.zeros(n, dtype=np.int32)
     rc = fn(sim.ctx, n, rho.ctypes.data, e.ctypes.data, abar.ctypes.data, zbar.ctypes.data, T.ctypes.data,
-            p.ctypes.data, cs.ctypes.data, it.ctypes.data, 0)
+            p.ctypes.data, cs.ctypes.data, it.ctypes.data, guess)
     return rc, T, p, cs, it
 
 
@@ -33,6 +33,7 @@ def test_noalloc_matches_allocating_entry_point(gpu_lib, table):
     cfg, _ = problems.stratified_3d(8)
     with Simulation(cfg, table) as sim:
         lib = sim.lib
+        assert lib.phl_mlp_train(sim.ctx, 1 << 16, 7, 4, 4096, C.c_double(3e-3), None) == 0
         for call, (n, seed) in enumerate([(5000, 11), (3000, 12)]):
             rho, T, abar, zbar = problems.eos_samples(n, seed=seed)
             e = np.zeros(n)
@@ -46,14 +47,17 @@ def test_noalloc_matches_allocating_entry_point(gpu_lib, table):
                                              d["abar"].data_ptr(), d["zbar"].data_ptr(), de.data_ptr()) == 0
             e = de.cpu().numpy()
             T0 = T * np.exp(0.2 * np.cos(np.arange(n) + call))
-            rc_a, Ta, pa, csa, ita = _invert(sim, lib.phl_eos_invert_batch, rho, e, abar, zbar, T0)
-            rc_b, Tb, pb, csb, itb = _invert(sim, lib.phl_eos_invert_batch_noalloc, rho, e, abar, zbar, T0)
-            assert rc_a == 0 and rc_b == 0
-            # same kernel on the same inputs: identical results (tolerance of the EoS tests)
-            np.testing.assert_allclose(Tb, Ta, rtol=1e-12, atol=0)
-            np.testing.assert_allclose(pb, pa, rtol=1e-12, atol=0)
-            np.testing.assert_allclose(csb, csa, rtol=1e-12, atol=0)
-            assert np.array_equal(itb, ita)
+            # warm, bracket and learned guesses (the learned one also uses the rejection queue)
+            for guess in (0, 2, 1):
+                rc_a, Ta, pa, csa, ita = _invert(sim, lib.phl_eos_invert_batch, rho, e, abar, zbar, T0, guess)
+                rc_b, Tb, pb, csb, itb = _invert(sim, lib.phl_eos_invert_batch_noalloc, rho, e, abar, zbar, T0,
+                                                 guess)
+                assert rc_a == 0 and rc_b == 0
+                # same kernels on the same inputs: identical results (tolerance of the EoS tests)
+                np.testing.assert_allclose(Tb, Ta, rtol=1e-12, atol=0)
+                np.testing.assert_allclose(pb, pa, rtol=1e-12, atol=0)
+                np.testing.assert_allclose(csb, csa, rtol=1e-12, atol=0)
+                assert np.array_equal(itb, ita)
 
 
 def test_noalloc_rejects_oversize(gpu_lib, table):
