@@ -63,6 +63,13 @@ def default_size(name):
     return {"stratified": 256, "stratified_mhd": 256, "hot_bubble": 256, "orszag_tang": 1024}[name]
 
 
+# DRAM bytes per cell of one stage-kernel launch, from ncu captures of the 128^3 stratified box
+# (dram__bytes_read.sum + dram__bytes_write.sum over 2,097,152 cells); the kernel streams the
+# domain once per launch, so the per-launch traffic scales with the cell count
+TRAFFIC_PER_CELL = {("stratified", "fp32_split"): 499.604224e6 / 2097152,
+                    ("stratified", "fp64"): 557.258496e6 / 2097152}
+
+
 def step_bytes_per_cell(cfg):
     """Algorithmic HBM bytes per zone-update of the fused stage kernel (minimum traffic).
 
@@ -342,9 +349,14 @@ def run_ours(args):
     bytes_per_cell = step_bytes_per_cell(cfg.replace(precision=head_form))
     launch_ms = head["launch_ms"]
     achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
-    kname = "k_stage_split (FP32 fluxes, FP64 state/EoS)" if head_form == "fp32_split" else "k_stage (FP64)"
+    tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
+    kname = ("k_stage_split_tiled" if tiled else "k_stage_split") + " (FP32 fluxes, FP64 state/EoS)" \
+        if head_form == "fp32_split" else "k_stage (FP64)"
+    tpc = TRAFFIC_PER_CELL.get((name, head_form))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": kname, "peak_kind": peak_kind,
+            "frac": achieved / peaks["hbm_gbs"], "traffic": tpc * cells if tpc else None,
+            "traffic_source": "ncu DRAM bytes of one launch at 128^3, scaled by cells" if tpc else None,
+            "kernel": kname, "peak_kind": peak_kind,
             "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
 
     cpu = None
@@ -400,7 +412,7 @@ def run_eos(args):
         stream = torch.cuda.ExternalStream(sim.stream())
         t0 = time.perf_counter()
         loss = C.c_double()
-        rc = lib.phl_mlp_train(sim.ctx, 1 << 22, 12345, 256, 8192, C.c_double(3e-3), C.byref(loss))
+        rc = lib.phl_mlp_train(sim.ctx, 1 << 22, 12345, args.train_epochs, 8192, C.c_double(3e-3), C.byref(loss))
         train_s = time.perf_counter() - t0
         assert rc == 0, rc
         rho, T, abar, zbar = problems.eos_samples(n, seed=99)
@@ -477,7 +489,8 @@ def run_eos(args):
             "warmup": args.warmup, "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (EoS/Newton), bf16/f32 (MLP)", "data": "synthetic",
             "config": {"workload": "eos_batch", "n": n, "l2": "inputs larger than L2 (%.0f MB)" % (n * 44 / 1e6),
-                       "train": {"samples": 1 << 22, "epochs": 256, "seconds": train_s, "loss": loss.value}},
+                       "train": {"samples": 1 << 22, "epochs": args.train_epochs, "seconds": train_s,
+                                 "loss": loss.value}},
             "bracket": {"value": b["rate"], "ms_per_step": b["ms"], "newton_iters_per_sample": b["iters"],
                         "eos_evals_per_sample": b["evals"]},
             "mlp": {"newton_iters_per_sample": m["iters"], "eos_evals_per_sample": m["evals"],
@@ -522,6 +535,7 @@ def main():
                     choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang", "eos"])
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--train-epochs", type=int, default=256, help="MLP training epochs (eos workload)")
     ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
     args = ap.parse_args()
     if args.warmup < 3:

@@ -30,13 +30,14 @@ struct HelmCell {
   double Ye, rhos, x, drho;
   double r0[3], r1[3], dr0[3], dr1[3];  // density bases (value, d/drho) at the lower/upper node
   double A[3][2], B[3][2];              // contracted coefficients of the current T cell
-  double T0, dT;                        // lower T node and spacing of the current T cell
+  double T0, dT, idT;                   // lower T node, spacing and its inverse, current T cell
 };
 
 __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell &c, int jh) {
   c.jh = jh;
   c.T0 = __ldg(h.T + jh - 1);
   c.dT = __ldg(h.T + jh) - c.T0;
+  c.idT = 1.0 / c.dT;
   // variables grouped by T order: ot 0 -> (f, f_d, f_dd), 1 -> (f_T, f_dT, f_ddT), 2 -> (f_TT, ...)
   const int var[3][3] = {{0, 3, 4}, {1, 5, 6}, {2, 7, 8}};
 #pragma unroll
@@ -77,7 +78,7 @@ __device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, 
 
 // f, f_T, f_TT at T (T inside the current cell)
 __device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, double &f, double &fT, double &fTT) {
-  double idT = 1.0 / c.dT;
+  const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
   hb0(y, c.dT, c.dT * c.dT, t0);
@@ -101,7 +102,7 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
                                               double inv_abar, double &T, int max_iter, int &clamped,
                                               bool &converged) {
   const double Told = T;
-  const double irho = 1.0 / rho;
+  const double irho = 1.0 / rho, inv_E0 = 1.0 / E0;
   converged = false;
   int used = 0;
   for (int iter = 1; iter <= max_iter; ++iter) {
@@ -114,7 +115,7 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
     double dE = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
     double res = E - E0;
     T = T - res / dE;
-    double error = fabs(res / E0);
+    double error = fabs(res * inv_E0);
     if ((T < h.Tl) || (T > h.Th)) {
       T = Told;
       error = EM15;
@@ -129,7 +130,7 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
 // pressure and relativistic sound speed at (rho, T) from the prepared cell (given_full's output)
 __device__ __forceinline__ void helm_cell_p_sound(const HelmTable &h, const HelmCell &c, double rho, double T,
                                                   double inv_abar, double &P, double &sound) {
-  double idT = 1.0 / c.dT;
+  const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
   hb0(y, c.dT, c.dT * c.dT, t0);

@@ -53,6 +53,9 @@ struct Prm {
   // reference scales of the FP32 split path: the FP32 deviations and fluxes are kept in units
   // of rho_ref, p_ref and v_ref = sqrt(p_ref / rho_ref) so that no product leaves FP32 range
   double rho_ref, p_ref, v_ref;
+  double inv_rho_ref, inv_p_ref, inv_v_ref;
+  // face background of the split path in those units, FP32 (x / ref rounded once at upload)
+  const float *sf_rho_f[3], *sf_p_f[3], *sf_ge_f[3], *sf_phi_f[3];
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,

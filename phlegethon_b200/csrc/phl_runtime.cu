@@ -90,6 +90,12 @@ Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem) 
   return nullptr;
 }
 
+// dst = (float)(src / ref): the split path's FP32 copy of a background array
+__global__ void k_scale_f32(const double *src, float *dst, long long n, double ref) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)(src[i] / ref);
+}
+
 // ----------------------------------------------------------------------------- transposes
 // host reference layout (nv, n1g, n2g, n3g) with ghost offsets -> SoA interior [nv][N]
 __global__ void k_unpack(const double *src, double *dst, int nv, int nx, int ny, int nz, int n1, int n2,
@@ -164,6 +170,7 @@ struct phl_ctx {
   int bg_profile = 0;
   double *eq_rho_cc = nullptr, *eq_p_cc = nullptr, *eq_ge_cc = nullptr, *phi_cc = nullptr, *grav = nullptr;
   double *eq_rho_f[3] = {}, *eq_p_f[3] = {}, *eq_ge_f[3] = {}, *phi_f[3] = {};
+  float *sf_rho_f[3] = {}, *sf_p_f[3] = {}, *sf_ge_f[3] = {}, *sf_phi_f[3] = {};  // split path
   // scalars
   double *scal = nullptr;
   unsigned long long *smax_bits = nullptr;
@@ -234,6 +241,9 @@ struct phl_ctx {
     P.rho_ref = rho_ref;
     P.p_ref = p_ref;
     P.v_ref = v_ref;
+    P.inv_rho_ref = 1.0 / rho_ref;
+    P.inv_p_ref = 1.0 / p_ref;
+    P.inv_v_ref = 1.0 / v_ref;
     P.U = U;
     P.U0 = U0;
     P.eint = eint;
@@ -241,6 +251,7 @@ struct phl_ctx {
     P.eq_rho_cc = eq_rho_cc; P.eq_p_cc = eq_p_cc; P.eq_ge_cc = eq_ge_cc; P.phi_cc = phi_cc; P.grav = grav;
     for (int d = 0; d < 3; ++d) {
       P.eq_rho_f[d] = eq_rho_f[d]; P.eq_p_f[d] = eq_p_f[d]; P.eq_ge_f[d] = eq_ge_f[d]; P.phi_f[d] = phi_f[d];
+      P.sf_rho_f[d] = sf_rho_f[d]; P.sf_p_f[d] = sf_p_f[d]; P.sf_ge_f[d] = sf_ge_f[d]; P.sf_phi_f[d] = sf_phi_f[d];
       P.bf[d] = bf[d]; P.b0f[d] = b0f[d]; P.emf[d] = emf[d]; P.sgnf[d] = sgnf[d]; P.cor[d] = cor[d];
     }
     P.bcc_in = bcc;
@@ -262,6 +273,22 @@ struct phl_ctx {
     return P;
   }
   // split path: FP64 primitives of W[cur] -> U and the FP32 deviations of Wf[cur]
+  // FP32 copies of the face background in the split path's units
+  int scale_background(bool helm) {
+    for (int d = 0; d < dim; ++d) {
+      long long nf = geo.bg_profile ? (long long)(geo.nx[1] + (d == 1)) : nfaces(d);
+      int rc;
+      if (!sf_rho_f[d] && ((rc = alloc(&sf_rho_f[d], nf)) || (rc = alloc(&sf_p_f[d], nf)) ||
+                           (rc = alloc(&sf_phi_f[d], nf)) || (rc = alloc(&sf_ge_f[d], nf))))
+        return rc;
+      k_scale_f32<<<nblk(nf, 256), 256, 0, stream>>>(eq_rho_f[d], sf_rho_f[d], nf, rho_ref);
+      k_scale_f32<<<nblk(nf, 256), 256, 0, stream>>>(eq_p_f[d], sf_p_f[d], nf, p_ref);
+      k_scale_f32<<<nblk(nf, 256), 256, 0, stream>>>(phi_f[d], sf_phi_f[d], nf, v_ref * v_ref);
+      if (helm) k_scale_f32<<<nblk(nf, 256), 256, 0, stream>>>(eq_ge_f[d], sf_ge_f[d], nf, 1.0);
+    }
+    CK(cudaGetLastError());
+    return PHL_OK;
+  }
   void split_from_prim() {
     Prm P = prm(0);
     P.Win = W[cur];
@@ -305,6 +332,13 @@ int check_cfg(const phl_config *c) {
   if (helm && !((c->flags & PHL_FASTEOS) && (c->flags & PHL_ADVECT_YE_IABAR) && c->nas >= 2))
     return PHL_E_UNSUPPORTED;
   if (c->precision != PHL_FP64 && c->precision != PHL_FP32_SPLIT) return PHL_E_INVALID;
+  // the step's Newton starts from the previous stage's temperature (the reference's warm start);
+  // the learned guess is offered by the batch inversion entry points only
+  if (c->eos_guess == PHL_GUESS_MLP) {
+    g_last_error = "eos_guess = PHL_GUESS_MLP: the step uses the warm start; use the batch inversion";
+    return PHL_E_UNSUPPORTED;
+  }
+  if (c->eos_guess != PHL_GUESS_WARM) return PHL_E_INVALID;
   return PHL_OK;
 }
 
@@ -612,6 +646,7 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
       }
     }
   }
+  if (ctx->split && strat && f->eq_prim_cc && (rc = ctx->scale_background(helm))) return rc;
   if (ctx->split && f->eint && (!strat || ctx->bg_uploaded || f->eq_prim_cc)) {
     ctx->split_from_prim();
     CK(cudaGetLastError());

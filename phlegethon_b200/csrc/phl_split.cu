@@ -11,6 +11,8 @@
 // (rho / rho_ref, p / p_ref, v / v_ref with v_ref^2 = p_ref / rho_ref, phi / v_ref^2), fixed per run,
 // so products of deviations never leave FP32 range whatever the problem's cgs magnitudes.
 #include <cuda_runtime.h>
+#include <cstdlib>
+#include <cstring>
 #include "phl_eos_fast.cuh"
 #include "phl_runner.h"
 
@@ -125,20 +127,36 @@ __device__ __forceinline__ void load_wf(const Prm &P, int i, int j, int k, float
   }
 }
 
+// States of the four cells m-2..m+1 around the low face of cell m: variable iv of cell s is
+// w(s, iv), FASTEOS gamma q is g(s, q).
+template <int NV>
+struct RegCells {
+  const float *w_[4], *g_[4];
+  __device__ __forceinline__ float w(int s, int iv) const { return w_[s][iv]; }
+  __device__ __forceinline__ float g(int s, int q) const { return g_[s][q]; }
+};
+// cells in a shared-memory array: variable iv of cell s at base[off[s] + iv * vs]
+template <int NV>
+struct SmemCells {
+  const float *base;
+  int off[4], vs;
+  __device__ __forceinline__ float w(int s, int iv) const { return base[off[s] + iv * vs]; }
+  __device__ __forceinline__ float g(int s, int q) const { return base[off[s] + (NV + q) * vs]; }
+};
+
 // flux through the low face of cell m along d from the FP32 deviation states of cells m-2..m+1
-template <class C>
-__device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int fj, int fk, const float *wl2,
-                                                const float *wl1, const float *wr1, const float *wr2,
-                                                const float *gl2, const float *gl1, const float *gr1,
-                                                const float *gr2, float F[C::NV]) {
+template <class C, class Cells>
+__device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int fj, int fk, const Cells &cl,
+                                                float F[C::NV]) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
   float qL[NV], qR[NV], lo, hi;
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
-    plm_f32(wl2[iv], wl1[iv], wr1[iv], lo, hi);
+    const float w0 = cl.w(0, iv), w1 = cl.w(1, iv), w2 = cl.w(2, iv), w3 = cl.w(3, iv);
+    plm_f32(w0, w1, w2, lo, hi);
     qL[iv] = hi;
-    plm_f32(wl1[iv], wr1[iv], wr2[iv], lo, hi);
+    plm_f32(w1, w2, w3, lo, hi);
     qR[iv] = lo;
   }
   if (d == 1) {
@@ -152,22 +170,23 @@ __device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int
   long long fb = 0;
   if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
   if (C::WB) {
-    float rho_eq = (float)(__ldg(P.eq_rho_f[d] + fb) / P.rho_ref);
+    float rho_eq = __ldg(P.sf_rho_f[d] + fb);
     qL[0] = rho_eq + qL[0];
     qR[0] = rho_eq + qR[0];
-    pe = (float)(__ldg(P.eq_p_f[d] + fb) / P.p_ref);
+    pe = __ldg(P.sf_p_f[d] + fb);
   }
   float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
   if (C::HELM) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      plm_f32(gl2[iv], gl1[iv], gr1[iv], lo, hi);
+      const float g0 = cl.g(0, iv), g1 = cl.g(1, iv), g2 = cl.g(2, iv), g3 = cl.g(3, iv);
+      plm_f32(g0, g1, g2, lo, hi);
       gL[iv] = hi;
-      plm_f32(gl1[iv], gr1[iv], gr2[iv], lo, hi);
+      plm_f32(g1, g2, g3, lo, hi);
       gR[iv] = lo;
     }
     if (C::WB) {
-      float ge = (float)__ldg(P.eq_ge_f[d] + fb);
+      float ge = __ldg(P.sf_ge_f[d] + fb);
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
     }
@@ -179,25 +198,147 @@ __device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int
     float a = F[1], b = F[2], c = F[3]; F[1] = b; F[2] = c; F[3] = a;
   }
   if (C::ETOT) {
-    phi_f = (float)(__ldg(P.phi_f[d] + fb) / (P.v_ref * P.v_ref));
+    phi_f = __ldg(P.sf_phi_f[d] + fb);
     F[IP] = F[IP] + F[0] * phi_f;
   }
 }
 
-// --------------------------------------------------------------------- split stage kernel
+template <class C>
+__device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int fj, int fk, const float *wl2,
+                                                const float *wl1, const float *wr1, const float *wr2,
+                                                const float *gl2, const float *gl1, const float *gr1,
+                                                const float *gr2, float F[C::NV]) {
+  RegCells<C::NV> cl{{wl2, wl1, wr1, wr2}, {gl2, gl1, gr1, gr2}};
+  face_flux_cells<C>(P, d, fi, fj, fk, cl, F);
+}
+
+// --------------------------------------------------------------------- split stage kernels
+// Per-cell statistics of a stage, reduced once per block.
+struct SplitStat {
+  double smax = 0.0;
+  unsigned long long calls = 0, iters = 0, nonconv = 0, clamp = 0, bad = 0;
+};
+
+// Everything of a stage after the flux divergence, for one cell: flux divergence to physical
+// units, gravity, RK combine (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
+// deviations out, and the cell's CFL speed in the last stage.  res: divergence in scaled units.
+template <class C>
+__device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int i, int j, int k,
+                                                  const float res[C::NV], float rho_dev, SplitStat &st) {
+  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  const double dt = P.scal[1];
+  // back to physical units: mass and scalar fluxes scale with rho_ref v_ref, momentum with
+  // p_ref, energy with p_ref v_ref
+  const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
+  double rd[NV];
+  rd[0] = (double)res[0] * fm;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) rd[1 + d] = (double)res[1 + d] * P.p_ref;
+  rd[IP] = (double)res[IP] * fe;
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) rd[iv] = (double)res[iv] * fm;
+  const long long bc = bg_cc(g, i, j, k);
+  if (C::GRAV) {
+    const double rho_dev_phys = (double)rho_dev * P.rho_ref;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
+  }
+  double u0[NV], u[NV];
+  if (P.first_stage) {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      u0[iv] = P.U[(long long)iv * g.N + c];
+      u[iv] = u0[iv];
+      P.U0[(long long)iv * g.N + c] = u0[iv];
+    }
+  } else {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      u0[iv] = P.U0[(long long)iv * g.N + c];
+      u[iv] = P.U[(long long)iv * g.N + c];
+    }
+  }
+  const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    u[iv] = a1 * u0[iv] + a2 * u[iv] + a3 * rd[iv];
+    P.U[(long long)iv * g.N + c] = u[iv];
+  }
+  // cons -> prim + EoS in FP64
+  double rho = u[0], inv_rho = 1.0 / rho;
+  double ke = u[1] * u[1] + u[2] * u[2] + (DIM == 3 ? u[3] * u[3] : 0.0);
+  double eint = u[IP] - 0.5 * ke * inv_rho;
+  if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
+  double p, T, sound = 0.0;
+  if (C::HELM) {
+    double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
+    double abar = 1.0 / inv_abar, zbar = ye * abar;
+    T = P.temp[c];
+    int clamped = 0;
+    bool conv = false;
+    HelmCell hc;
+    helm_cell_init(P.helm, hc, rho, abar, zbar, T);
+    int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+    st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
+    helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
+    double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+    if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
+    P.gf_out[c] = (float)ge;
+    P.gf_out[g.N + c] = (float)gc;
+  } else {
+    p = (g.gm - 1.0) * eint;
+    T = p / (rho * CONST_RGAS * (1.0 / g.mu));
+    sound = sqrt(g.gm * p / rho);
+  }
+  double rdev = rho, pdev = p;
+  if (C::WB) {
+    rdev = rho - __ldg(P.eq_rho_cc + bc);
+    pdev = p - __ldg(P.eq_p_cc + bc);
+  }
+  P.Wf_out[c] = (float)(rdev * P.inv_rho_ref);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) P.Wf_out[(long long)(1 + d) * g.N + c] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
+  P.Wf_out[(long long)IP * g.N + c] = (float)(pdev * P.inv_p_ref);
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
+  P.temp[c] = T;
+  P.eint[c] = eint;
+  if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) st.bad += 1;
+  if (P.last_stage) {
+    double sx1 = (fabs(u[1] * inv_rho) + sound) * g.inv_dx[0];
+    double sx2 = (fabs(u[2] * inv_rho) + sound) * g.inv_dx[1];
+    double sm = sx1 + sx2;
+    if (DIM == 3) sm = (fabs(u[3] * inv_rho) + sound) * g.inv_dx[2] + sm;
+    st.smax = fmax(st.smax, sm);
+  }
+}
+
+template <class C>
+__device__ __forceinline__ void split_stat_flush(const Prm &P, const SplitStat &st) {
+  if (P.last_stage) block_max_atomic(st.smax, P.smax_bits);
+  if (C::HELM) {
+    block_sum_atomic(st.calls, P.stat + STAT_NEWTON_CALLS);
+    block_sum_atomic(st.iters, P.stat + STAT_NEWTON_ITERS);
+    block_sum_atomic(st.nonconv, P.stat + STAT_NEWTON_NONCONV);
+    block_sum_atomic(st.clamp, P.stat + STAT_NEWTON_CLAMP);
+  }
+  block_sum_atomic(st.bad, P.stat + STAT_NONFINITE);
+}
+
+// One thread per cell; every face is solved by both of its cells.  Any grid size.
 template <class C>
 __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
   if (!*P.active) return;
-  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  constexpr int NV = C::NV, DIM = C::DIM;
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double smax_loc = 0.0;
-  unsigned long long n_calls = 0, n_iters = 0, n_nonconv = 0, n_clamp = 0, n_bad = 0;
+  SplitStat st;
   if (c < g.N) {
     const int i = (int)(c % g.nx[0]);
     const int j = (int)((c / g.nx[0]) % g.nx[1]);
     const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
-    const double dt = P.scal[1];
     float res[NV];
     float rho_dev = 0.0f;
 #pragma unroll
@@ -220,99 +361,140 @@ __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
         res[iv] = d == 0 ? dd : res[iv] + dd;
       }
     }
-    // back to physical units: mass and scalar fluxes scale with rho_ref v_ref, momentum with
-    // p_ref, energy with p_ref v_ref
-    const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
-    double rd[NV];
-    rd[0] = (double)res[0] * fm;
+    split_cell_update<C>(P, c, i, j, k, res, rho_dev, st);
+  }
+  split_stat_flush<C>(P, st);
+}
+
+// 3D, face reuse: a block owns TX x TY columns of cells in (x1, x2) and marches KZ planes along
+// x3.  Deviation states live in a shared-memory ring of four planes (k-1 .. k+2), the current
+// plane k with a 2-cell halo in x1 and x2; each x1 and x2 face of the plane is solved once into
+// shared memory and each x3 face once per column (the upper face of plane k is the lower face of
+// plane k+1, kept in registers): 3.16 solves per cell against 6 in k_stage_split.  The divergence
+// sums the three directions in the same order as k_stage_split.
+// Requires nx1 % TX == nx2 % TY == nx3 % KZ == 0, blockDim.x == TX * TY and
+// split_tiled_smem<C, TX, TY>() bytes of dynamic shared memory.
+template <class C, int TX, int TY>
+struct SplitTile {
+  static constexpr int NQ = C::NV + (C::HELM ? 2 : 0);  // stored values per cell
+  static constexpr int SX = TX + 4, SY = TY + 4, PL = SX * SY;
+  static constexpr int RING = 4 * NQ * PL;               // floats: [slot][q][y][x]
+  static constexpr int FX = C::NV * TY * (TX + 1), FY = C::NV * (TY + 1) * TX;
+  static constexpr size_t bytes() { return sizeof(float) * (size_t)(RING + FX + FY); }
+};
+
+template <class C, int TX, int TY, int KZ>
+__global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
+  if (!*P.active) return;
+  using T = SplitTile<C, TX, TY>;
+  constexpr int NV = C::NV, NQ = T::NQ, SX = T::SX, PL = T::PL, VS = PL;
+  static_assert(C::DIM == 3, "tiled stage is 3D");
+  constexpr int NHALO = 4 * TX + 4 * TY;  // halo cells the x1 and x2 faces read (no corners)
+  extern __shared__ __align__(16) float smem[];
+  float *ring = smem;                      // [4][NQ][SY][SX]
+  float *fx = smem + T::RING;              // [NV][TY][TX+1]
+  float *fy = fx + T::FX;                  // [NV][TY+1][TX]
+  const Geo &g = P.g;
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+  const int i = i0 + tx, j = j0 + ty;
+  const float idx = (float)g.inv_dx[0], idy = (float)g.inv_dx[1], idz = (float)g.inv_dx[2];
+  const int own = (ty + 2) * SX + (tx + 2);  // own cell inside a plane
+  auto slot = [&](int k) { return ((k - k0 + 2) & 3) * NQ * PL; };
+  auto put = [&](int base, int cell, const float *w, const float *g2) {
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) rd[1 + d] = (double)res[1 + d] * P.p_ref;
-    rd[IP] = (double)res[IP] * fe;
-#pragma unroll
-    for (int iv = IAS; iv < NV; ++iv) rd[iv] = (double)res[iv] * fm;
-    const long long bc = bg_cc(g, i, j, k);
-    if (C::GRAV) {
-      const double rho_dev_phys = (double)rho_dev * P.rho_ref;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
+    for (int q = 0; q < NV; ++q) ring[base + q * VS + cell] = w[q];
+    if (NQ > NV) {
+      ring[base + NV * VS + cell] = g2[0];
+      ring[base + (NV + 1) * VS + cell] = g2[1];
     }
-    double u0[NV], u[NV];
-    if (P.first_stage) {
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) {
-        u0[iv] = P.U[(long long)iv * g.N + c];
-        u[iv] = u0[iv];
-        P.U0[(long long)iv * g.N + c] = u0[iv];
-      }
-    } else {
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) {
-        u0[iv] = P.U0[(long long)iv * g.N + c];
-        u[iv] = P.U[(long long)iv * g.N + c];
-      }
-    }
-    const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-      u[iv] = a1 * u0[iv] + a2 * u[iv] + a3 * rd[iv];
-      P.U[(long long)iv * g.N + c] = u[iv];
-    }
-    // cons -> prim + EoS in FP64
-    double rho = u[0], inv_rho = 1.0 / rho;
-    double ke = u[1] * u[1] + u[2] * u[2] + (DIM == 3 ? u[3] * u[3] : 0.0);
-    double eint = u[IP] - 0.5 * ke * inv_rho;
-    if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
-    double p, T, sound = 0.0;
-    if (C::HELM) {
-      double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
-      double abar = 1.0 / inv_abar, zbar = ye * abar;
-      T = P.temp[c];
-      int clamped = 0;
-      bool conv = false;
-      HelmCell hc;
-      helm_cell_init(P.helm, hc, rho, abar, zbar, T);
-      int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
-      n_calls += 1; n_iters += it; n_nonconv += !conv; n_clamp += clamped;
-      helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
-      double ge = p / eint + 1.0, gc = sound * sound * rho / p;
-      if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
-      P.gf_out[c] = (float)ge;
-      P.gf_out[g.N + c] = (float)gc;
-    } else {
-      p = (g.gm - 1.0) * eint;
-      T = p / (rho * CONST_RGAS * (1.0 / g.mu));
-      sound = sqrt(g.gm * p / rho);
-    }
-    double rdev = rho, pdev = p;
-    if (C::WB) {
-      rdev = rho - __ldg(P.eq_rho_cc + bc);
-      pdev = p - __ldg(P.eq_p_cc + bc);
-    }
-    P.Wf_out[c] = (float)(rdev / P.rho_ref);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) P.Wf_out[(long long)(1 + d) * g.N + c] = (float)(u[1 + d] * inv_rho / P.v_ref);
-    P.Wf_out[(long long)IP * g.N + c] = (float)(pdev / P.p_ref);
-#pragma unroll
-    for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
-    P.temp[c] = T;
-    P.eint[c] = eint;
-    if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) n_bad += 1;
-    if (P.last_stage) {
-      double sx1 = (fabs(u[1] * inv_rho) + sound) * g.inv_dx[0];
-      double sx2 = (fabs(u[2] * inv_rho) + sound) * g.inv_dx[1];
-      smax_loc = sx1 + sx2;
-      if (DIM == 3) smax_loc = (fabs(u[3] * inv_rho) + sound) * g.inv_dx[2] + smax_loc;
+  };
+  SplitStat st;
+  // prologue: planes k0-2 .. k0+1 of the own column, the x3 face below plane k0
+  {
+    float w[NV], g2[2] = {0, 0};
+#pragma unroll 1
+    for (int k = k0 - 2; k <= k0 + 1; ++k) {
+      load_wf<C>(P, i, j, k, w, g2);
+      put(slot(k), own, w, g2);
     }
   }
-  if (P.last_stage) block_max_atomic(smax_loc, P.smax_bits);
-  if (C::HELM) {
-    block_sum_atomic(n_calls, P.stat + STAT_NEWTON_CALLS);
-    block_sum_atomic(n_iters, P.stat + STAT_NEWTON_ITERS);
-    block_sum_atomic(n_nonconv, P.stat + STAT_NEWTON_NONCONV);
-    block_sum_atomic(n_clamp, P.stat + STAT_NEWTON_CLAMP);
+  __syncthreads();
+  float fz_lo[NV], fz_hi[NV];
+  {
+    SmemCells<NV> cl{ring, {slot(k0 - 2) + own, slot(k0 - 1) + own, slot(k0) + own, slot(k0 + 1) + own}, VS};
+    face_flux_cells<C>(P, 2, i, j, k0, cl, fz_lo);
   }
-  block_sum_atomic(n_bad, P.stat + STAT_NONFINITE);
+  float nw[NV], ng[2] = {0, 0};
+  load_wf<C>(P, i, j, k0 + 2, nw, ng);
+  __syncthreads();
+
+#pragma unroll 1
+  for (int kk = 0; kk < KZ; ++kk) {
+    const int k = k0 + kk;
+    const int sk = slot(k);
+    // plane k+2 of the own column (prefetched), halo of plane k
+    put(slot(k + 2), own, nw, ng);
+    for (int h = threadIdx.x; h < NHALO; h += TX * TY) {
+      int hx, hy;
+      if (h < 4 * TX) {
+        const int r = h / TX;
+        hx = 2 + h % TX;
+        hy = r < 2 ? r : TY + r;
+      } else {
+        const int h3 = h - 4 * TX, cc = h3 / TY;
+        hy = 2 + h3 % TY;
+        hx = cc < 2 ? cc : TX + cc;
+      }
+      float w[NV], g2[2] = {0, 0};
+      load_wf<C>(P, i0 + hx - 2, j0 + hy - 2, k, w, g2);
+      put(sk, hy * SX + hx, w, g2);
+    }
+    if (kk + 1 < KZ) load_wf<C>(P, i, j, k + 3, nw, ng);
+    __syncthreads();
+    {
+      float F[NV];
+      // low x1 face of the own cell
+      SmemCells<NV> cx{ring, {sk + own - 2, sk + own - 1, sk + own, sk + own + 1}, VS};
+      face_flux_cells<C>(P, 0, i, j, k, cx, F);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) fx[(q * TY + ty) * (TX + 1) + tx] = F[q];
+      // low x2 face of the own cell
+      SmemCells<NV> cy{ring, {sk + own - 2 * SX, sk + own - SX, sk + own, sk + own + SX}, VS};
+      face_flux_cells<C>(P, 1, i, j, k, cy, F);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) fy[(q * (TY + 1) + ty) * TX + tx] = F[q];
+      if (ty == 0) {
+        // upper x2 face of the tile, column tx
+        const int c = (TY + 2) * SX + tx + 2;
+        SmemCells<NV> cu{ring, {sk + c - 2 * SX, sk + c - SX, sk + c, sk + c + SX}, VS};
+        face_flux_cells<C>(P, 1, i, j0 + TY, k, cu, F);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) fy[(q * (TY + 1) + TY) * TX + tx] = F[q];
+      } else if (ty == 1 && tx < TY) {
+        // upper x1 face of the tile, row tx
+        const int c = (tx + 2) * SX + TX + 2;
+        SmemCells<NV> cr{ring, {sk + c - 2, sk + c - 1, sk + c, sk + c + 1}, VS};
+        face_flux_cells<C>(P, 0, i0 + TX, j0 + tx, k, cr, F);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) fx[(q * TY + tx) * (TX + 1) + TX] = F[q];
+      }
+      // upper x3 face of the own cell
+      SmemCells<NV> cz{ring, {slot(k - 1) + own, sk + own, slot(k + 1) + own, slot(k + 2) + own}, VS};
+      face_flux_cells<C>(P, 2, i, j, k + 1, cz, fz_hi);
+    }
+    __syncthreads();
+    float res[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      float dd = (fx[(q * TY + ty) * (TX + 1) + tx + 1] - fx[(q * TY + ty) * (TX + 1) + tx]) * idx;
+      dd = dd + (fy[(q * (TY + 1) + ty + 1) * TX + tx] - fy[(q * (TY + 1) + ty) * TX + tx]) * idy;
+      res[q] = dd + (fz_hi[q] - fz_lo[q]) * idz;
+      fz_lo[q] = fz_hi[q];
+    }
+    split_cell_update<C>(P, lin(g, i, j, k), i, j, k, res, ring[sk + own], st);
+  }
+  split_stat_flush<C>(P, st);
 }
 
 // FP64 primitives (+eint, gammaf) -> U (FP64) and FP32 deviations (prim->cons of
@@ -399,7 +581,32 @@ inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 template <class C>
 struct SplitRunnerT : Runner {
-  void stage(const Prm &P, cudaStream_t s) override { k_stage_split<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P); }
+  static constexpr int TX = 32, TY = 8, KZ = 16;
+  bool attr_set = false;
+  // PHL_STAGE_KERNEL=cell selects the per-cell kernel on any grid (comparison of the two)
+  const bool allow_tiled = [] {
+    const char *e = getenv("PHL_STAGE_KERNEL");
+    return !(e && strcmp(e, "cell") == 0);
+  }();
+  bool tiled(const Geo &g) const {
+    return allow_tiled && C::DIM == 3 && g.nx[0] % TX == 0 && g.nx[1] % TY == 0 && g.nx[2] % KZ == 0;
+  }
+  void stage(const Prm &P, cudaStream_t s) override {
+    if constexpr (C::DIM == 3) {
+      if (tiled(P.g)) {
+        constexpr size_t sm = SplitTile<C, TX, TY>::bytes();
+        if (!attr_set) {
+          cudaFuncSetAttribute(k_stage_split_tiled<C, TX, TY, KZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sm);
+          attr_set = true;
+        }
+        dim3 grid(P.g.nx[0] / TX, P.g.nx[1] / TY, P.g.nx[2] / KZ);
+        k_stage_split_tiled<C, TX, TY, KZ><<<grid, TX * TY, sm, s>>>(P);
+        return;
+      }
+    }
+    k_stage_split<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P);
+  }
   void dt(const Prm &P, cudaStream_t s) override { k_dt<C><<<nblk(P.g.N, 256), 256, 0, s>>>(P); }
   void init_thermo(const Prm &P, cudaStream_t s) override {
     k_init_thermo<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P);

@@ -81,6 +81,7 @@ def test_hot_bubble_many_steps(gpu_lib, oracle):
     hg, ho, _ = run_pair(cfg, h, 100, oracle=oracle)
     err = field_errors(hg, ho)
     assert max(err.values()) <= 1e-9, err
+    assert max_abs_diff(hg, ho) == 0.0  # same operation order: bit for bit
 
 
 def test_hydrostatic_balance_kept(gpu_lib):
@@ -109,6 +110,7 @@ def test_orszag_tang(gpu_lib, oracle, riemann):
     hg, ho, _ = run_pair(cfg, h, 30, oracle=oracle)
     err = field_errors(hg, ho)
     assert max(err.values()) <= 1e-9, err
+    assert max_abs_diff(hg, ho) == 0.0
     assert div_b_max(hg) <= 1e-13
 
 
@@ -119,6 +121,7 @@ def test_periodic_3d(gpu_lib, oracle, mhd, riemann):
     hg, ho, _ = run_pair(cfg, h, 5, oracle=oracle)
     err = field_errors(hg, ho)
     assert max(err.values()) <= 1e-12, err
+    assert max_abs_diff(hg, ho) == 0.0
     if mhd:
         assert div_b_max(hg) <= 1e-13
 
@@ -130,6 +133,7 @@ def test_stratified_helmholtz(gpu_lib, oracle, table, mhd):
     hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
     err = field_errors(hg, ho)
     assert max(err.values()) <= 1e-12, err
+    assert max_abs_diff(hg, ho) == 0.0
     assert st["newton_nonconverged"] == 0
     assert st["nonfinite"] == 0
     if mhd:

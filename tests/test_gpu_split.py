@@ -59,3 +59,25 @@ def test_split_keeps_hydrostatic_balance(gpu_lib, table):
     v = np.abs(h32.interior(h32.prim)[1:4]).max()
     cs = np.sqrt(5.0 / 3.0 * h32.interior(h32.prim)[4] / h32.interior(h32.prim)[0]).min()
     assert v / cs < 1e-9
+
+
+@pytest.mark.parametrize("riemann", ["lhllc", "hllc"])
+def test_tiled_stage_equals_per_cell_stage(gpu_lib, table, riemann, monkeypatch):
+    """The face-reuse tiled stage kernel (grids divisible by its 32 x 8 x 16 tile) against the
+    per-cell kernel, which solves every face twice (once per neighbour, so its two copies of a
+    face flux can differ in the last FP32 bits where the compiler contracts differently).  Both
+    sit at the same FP32 rounding distance from the FP64 form."""
+    cfg, h = problems.stratified_3d(32, ny=16, nz=32, riemann=riemann)
+    monkeypatch.setenv("PHL_STAGE_KERNEL", "cell")
+    hc, stc = run_form(cfg, h, 6, table, "fp32_split")
+    monkeypatch.setenv("PHL_STAGE_KERNEL", "auto")
+    ht, stt = run_form(cfg, h, 6, table, "fp32_split")
+    h64, _ = run_form(cfg, h, 6, table, "fp64")
+    assert stt["nonfinite"] == 0 and stt["newton_nonconverged"] == 0
+    e_t = field_errors(ht, h64)
+    e_c = field_errors(hc, h64)
+    diff = field_errors(ht, hc)
+    for f in e_c:
+        # no further from FP64 than the per-cell kernel, and apart by FP32 rounding noise only
+        assert e_t[f] <= 1.5 * e_c[f] + 1e-12, (f, e_t, e_c)
+        assert diff[f] <= 2.0 * e_c[f] + 1e-12, (f, diff, e_c)
