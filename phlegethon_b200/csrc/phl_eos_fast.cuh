@@ -28,17 +28,14 @@ __device__ __forceinline__ int helm_node_index(const double *nodes, int n, doubl
 struct HelmCell {
   int ih, jh;
   double Ye, rhos, x, drho;
-  double r0[3], r1[3], dr0[3], dr1[3];  // density bases (value, d/drho) at the lower/upper node
-  double A[3][2], B[3][2];              // contracted coefficients of the current T cell
+  double A[3][2];                       // contracted coefficients of the current T cell
   double T0, dT, idT;                   // lower T node, spacing and its inverse, current T cell
 };
 
-__device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell &c, int jh) {
-  c.jh = jh;
-  c.T0 = __ldg(h.T + jh - 1);
-  c.dT = __ldg(h.T + jh) - c.T0;
-  c.idT = 1.0 / c.dT;
-  // variables grouped by T order: ot 0 -> (f, f_d, f_dd), 1 -> (f_T, f_dT, f_ddT), 2 -> (f_TT, ...)
+// coefficients of T order ot (variables {0,3,4}, {1,5,6}, {2,7,8}: value, d/drho, d2/drho2 of
+// f, f_T, f_TT) at the lower/upper T node jt, contracted with a density basis (r0, r1)
+__device__ __forceinline__ void helm_cell_contract_with(const HelmTable &h, const HelmCell &c, int jh,
+                                                        const double r0[3], const double r1[3], double out[3][2]) {
   const int var[3][3] = {{0, 3, 4}, {1, 5, 6}, {2, 7, 8}};
 #pragma unroll
   for (int jt = 0; jt < 2; ++jt) {
@@ -46,17 +43,29 @@ __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell 
     const double *hi = lo + 9;
 #pragma unroll
     for (int ot = 0; ot < 3; ++ot) {
-      double a = 0.0, b = 0.0;
+      double a = 0.0;
 #pragma unroll
-      for (int orr = 0; orr < 3; ++orr) {
-        double cl = __ldg(lo + var[ot][orr]), ch = __ldg(hi + var[ot][orr]);
-        a = fma(cl, c.r0[orr], fma(ch, c.r1[orr], a));
-        b = fma(cl, c.dr0[orr], fma(ch, c.dr1[orr], b));
-      }
-      c.A[ot][jt] = a;
-      c.B[ot][jt] = b;
+      for (int orr = 0; orr < 3; ++orr)
+        a = fma(__ldg(lo + var[ot][orr]), r0[orr], fma(__ldg(hi + var[ot][orr]), r1[orr], a));
+      out[ot][jt] = a;
     }
   }
+}
+
+// density basis (value) of the cell, recomputed where needed instead of kept in registers
+__device__ __forceinline__ void helm_cell_rbasis(const HelmCell &c, double r0[3], double r1[3]) {
+  hb0(c.x, c.drho, c.drho * c.drho, r0);
+  hb0m(1.0 - c.x, c.drho, c.drho * c.drho, r1);
+}
+
+__device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell &c, int jh) {
+  c.jh = jh;
+  c.T0 = __ldg(h.T + jh - 1);
+  c.dT = __ldg(h.T + jh) - c.T0;
+  c.idT = 1.0 / c.dT;
+  double r0[3], r1[3];
+  helm_cell_rbasis(c, r0, r1);
+  helm_cell_contract_with(h, c, jh, r0, r1, c.A);
 }
 
 __device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, double rho, double abar,
@@ -66,13 +75,7 @@ __device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, 
   c.ih = helm_node_index(h.rho, h.nrho, h.log10_rho1, h.drho, c.rhos);
   double r_lo = __ldg(h.rho + c.ih - 1);
   c.drho = __ldg(h.rho + c.ih) - r_lo;
-  double idrho = 1.0 / c.drho;
-  c.x = (c.rhos - r_lo) * idrho;
-  double omx = 1.0 - c.x;
-  hb0(c.x, c.drho, c.drho * c.drho, c.r0);
-  hb0m(omx, c.drho, c.drho * c.drho, c.r1);
-  hb1(c.x, idrho, c.drho, c.dr0);
-  hb1m(omx, idrho, c.drho, c.dr1);
+  c.x = (c.rhos - r_lo) * (1.0 / c.drho);
   helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
 }
 
@@ -139,14 +142,23 @@ __device__ __forceinline__ void helm_cell_p_sound(const HelmTable &h, const Helm
   hb1m(omy, idT, c.dT, d1);
   hb2(y, idT * idT, idT, e0);
   hb2m(omy, idT * idT, idT, e1);
+  // d/drho contraction of the final cell
+  double B[3][2];
+  {
+    const double idrho = 1.0 / c.drho;
+    double dr0[3], dr1[3];
+    hb1(c.x, idrho, c.drho, dr0);
+    hb1m(1.0 - c.x, idrho, c.drho, dr1);
+    helm_cell_contract_with(h, c, c.jh, dr0, dr1, B);
+  }
   double f = 0, fT = 0, fTT = 0, fd = 0, fdT = 0;
 #pragma unroll
   for (int ot = 0; ot < 3; ++ot) {
     f = fma(c.A[ot][0], t0[ot], fma(c.A[ot][1], t1[ot], f));
     fT = fma(c.A[ot][0], d0[ot], fma(c.A[ot][1], d1[ot], fT));
     fTT = fma(c.A[ot][0], e0[ot], fma(c.A[ot][1], e1[ot], fTT));
-    fd = fma(c.B[ot][0], t0[ot], fma(c.B[ot][1], t1[ot], fd));
-    fdT = fma(c.B[ot][0], d0[ot], fma(c.B[ot][1], d1[ot], fdT));
+    fd = fma(B[ot][0], t0[ot], fma(B[ot][1], t1[ot], fd));
+    fdT = fma(B[ot][0], d0[ot], fma(B[ot][1], d1[ot], fdT));
   }
   // bicubic dP/d(rho Ye) (source.F90:24082-24118)
   double x = c.x, omx = 1.0 - x;

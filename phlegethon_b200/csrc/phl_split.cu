@@ -366,19 +366,58 @@ __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
   split_stat_flush<C>(P, st);
 }
 
+// 4-byte asynchronous global -> shared copy (cp.async, completes at the next wait)
+__device__ __forceinline__ void cp_async4(float *smem_dst, const float *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Start the copy of the FP32 state of a (possibly ghost) cell into shared memory (variable q at
+// dst[q * vs]); returns the velocity components to negate once the copy has landed (bit d for
+// a mirrored dimension d, as load_wf does).
+template <class C>
+__device__ __forceinline__ void load_wf_async(const Prm &P, int i, int j, int k, float *dst, int vs) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2);
+  long long c = lin(g, si, sj, sk);
+#pragma unroll
+  for (int iv = 0; iv < C::NV; ++iv) cp_async4(dst + iv * vs, P.Wf_in + (long long)iv * g.N + c);
+  if (C::HELM) {
+    cp_async4(dst + C::NV * vs, P.gf_in + c);
+    cp_async4(dst + (C::NV + 1) * vs, P.gf_in + g.N + c);
+  }
+}
+// after the copy of cell (i, j, k) has landed: negate the velocity components of its mirrored
+// dimensions (what load_wf does on load)
+__device__ __forceinline__ void fix_mirrored(const Geo &g, int i, int j, int k, float *dst, int vs) {
+  bool f[3] = {false, false, false};
+  map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f[0]);
+  map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f[1]);
+  map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f[2]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (f[d]) dst[(1 + d) * vs] = -dst[(1 + d) * vs];
+}
+
 // 3D, face reuse: a block owns TX x TY columns of cells in (x1, x2) and marches KZ planes along
-// x3.  Deviation states live in a shared-memory ring of four planes (k-1 .. k+2), the current
-// plane k with a 2-cell halo in x1 and x2; each x1 and x2 face of the plane is solved once into
-// shared memory and each x3 face once per column (the upper face of plane k is the lower face of
-// plane k+1, kept in registers): 3.16 solves per cell against 6 in k_stage_split.  The divergence
-// sums the three directions in the same order as k_stage_split.
-// Requires nx1 % TX == nx2 % TY == nx3 % KZ == 0, blockDim.x == TX * TY and
-// split_tiled_smem<C, TX, TY>() bytes of dynamic shared memory.
+// x3.  Deviation states live in a shared-memory ring of five planes (k-1 .. k+3), each with a
+// 2-cell halo in x1 and x2, filled by asynchronous copies one plane ahead of use.  Each x1 and
+// x2 face of plane k is solved once into shared memory and each x3 face once per column (the
+// upper face of plane k is the lower face of plane k+1, kept in registers): 3.16 solves per cell
+// against 6 in k_stage_split.  The divergence sums the three directions in the same order as
+// k_stage_split.  Requires nx1 % TX == nx2 % TY == nx3 % KZ == 0, blockDim.x == TX * TY and
+// SplitTile<C, TX, TY>::bytes() of dynamic shared memory.
 template <class C, int TX, int TY>
 struct SplitTile {
   static constexpr int NQ = C::NV + (C::HELM ? 2 : 0);  // stored values per cell
   static constexpr int SX = TX + 4, SY = TY + 4, PL = SX * SY;
-  static constexpr int RING = 4 * NQ * PL;               // floats: [slot][q][y][x]
+  static constexpr int NSLOT = 5;
+  static constexpr int RING = NSLOT * NQ * PL;           // floats: [slot][q][y][x]
   static constexpr int FX = C::NV * TY * (TX + 1), FY = C::NV * (TY + 1) * TX;
   static constexpr size_t bytes() { return sizeof(float) * (size_t)(RING + FX + FY); }
 };
@@ -390,8 +429,9 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
   constexpr int NV = C::NV, NQ = T::NQ, SX = T::SX, PL = T::PL, VS = PL;
   static_assert(C::DIM == 3, "tiled stage is 3D");
   constexpr int NHALO = 4 * TX + 4 * TY;  // halo cells the x1 and x2 faces read (no corners)
+  static_assert(NHALO <= TX * TY, "one halo cell per thread");
   extern __shared__ __align__(16) float smem[];
-  float *ring = smem;                      // [4][NQ][SY][SX]
+  float *ring = smem;                      // [5][NQ][SY][SX]
   float *fx = smem + T::RING;              // [NV][TY][TX+1]
   float *fy = fx + T::FX;                  // [NV][TY+1][TX]
   const Geo &g = P.g;
@@ -400,58 +440,46 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
   const int i = i0 + tx, j = j0 + ty;
   const float idx = (float)g.inv_dx[0], idy = (float)g.inv_dx[1], idz = (float)g.inv_dx[2];
   const int own = (ty + 2) * SX + (tx + 2);  // own cell inside a plane
-  auto slot = [&](int k) { return ((k - k0 + 2) & 3) * NQ * PL; };
-  auto put = [&](int base, int cell, const float *w, const float *g2) {
-#pragma unroll
-    for (int q = 0; q < NV; ++q) ring[base + q * VS + cell] = w[q];
-    if (NQ > NV) {
-      ring[base + NV * VS + cell] = g2[0];
-      ring[base + (NV + 1) * VS + cell] = g2[1];
+  auto slot = [&](int k) { return ((k - k0 + 2) % T::NSLOT) * NQ * PL; };
+  // this thread's halo cell (x1/x2 halo of every plane), if any
+  int hcell = -1, hx = 0, hy = 0;
+  if ((int)threadIdx.x < NHALO) {
+    const int h = threadIdx.x;
+    if (h < 4 * TX) {
+      const int r = h / TX;
+      hx = 2 + h % TX;
+      hy = r < 2 ? r : TY + r;
+    } else {
+      const int h3 = h - 4 * TX, cc = h3 / TY;
+      hy = 2 + h3 % TY;
+      hx = cc < 2 ? cc : TX + cc;
     }
-  };
-  SplitStat st;
-  // prologue: planes k0-2 .. k0+1 of the own column, the x3 face below plane k0
-  {
-    float w[NV], g2[2] = {0, 0};
-#pragma unroll 1
-    for (int k = k0 - 2; k <= k0 + 1; ++k) {
-      load_wf<C>(P, i, j, k, w, g2);
-      put(slot(k), own, w, g2);
-    }
+    hcell = hy * SX + hx;
   }
+  SplitStat st;
+  // prologue: planes k0-2 .. k0+2 of the own column, halo of plane k0
+  for (int k = k0 - 2; k <= k0 + 2; ++k) load_wf_async<C>(P, i, j, k, ring + slot(k) + own, VS);
+  if (hcell >= 0) load_wf_async<C>(P, i0 + hx - 2, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
+  cp_async_commit();
+  cp_async_wait_all();
+  for (int k = k0 - 2; k <= k0 + 2; ++k) fix_mirrored(g, i, j, k, ring + slot(k) + own, VS);
+  if (hcell >= 0) fix_mirrored(g, i0 + hx - 2, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
   __syncthreads();
   float fz_lo[NV], fz_hi[NV];
   {
     SmemCells<NV> cl{ring, {slot(k0 - 2) + own, slot(k0 - 1) + own, slot(k0) + own, slot(k0 + 1) + own}, VS};
     face_flux_cells<C>(P, 2, i, j, k0, cl, fz_lo);
   }
-  float nw[NV], ng[2] = {0, 0};
-  load_wf<C>(P, i, j, k0 + 2, nw, ng);
-  __syncthreads();
 
 #pragma unroll 1
   for (int kk = 0; kk < KZ; ++kk) {
     const int k = k0 + kk;
     const int sk = slot(k);
-    // plane k+2 of the own column (prefetched), halo of plane k
-    put(slot(k + 2), own, nw, ng);
-    for (int h = threadIdx.x; h < NHALO; h += TX * TY) {
-      int hx, hy;
-      if (h < 4 * TX) {
-        const int r = h / TX;
-        hx = 2 + h % TX;
-        hy = r < 2 ? r : TY + r;
-      } else {
-        const int h3 = h - 4 * TX, cc = h3 / TY;
-        hy = 2 + h3 % TY;
-        hx = cc < 2 ? cc : TX + cc;
-      }
-      float w[NV], g2[2] = {0, 0};
-      load_wf<C>(P, i0 + hx - 2, j0 + hy - 2, k, w, g2);
-      put(sk, hy * SX + hx, w, g2);
-    }
-    if (kk + 1 < KZ) load_wf<C>(P, i, j, k + 3, nw, ng);
-    __syncthreads();
+    // next copies: own column plane k+3, halo of plane k+1 (both unread during this plane)
+    const bool next_own = kk + 3 <= KZ + 1, next_halo = kk + 1 < KZ && hcell >= 0;
+    if (next_own) load_wf_async<C>(P, i, j, k + 3, ring + slot(k + 3) + own, VS);
+    if (next_halo) load_wf_async<C>(P, i0 + hx - 2, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
+    cp_async_commit();
     {
       float F[NV];
       // low x1 face of the own cell
@@ -493,6 +521,10 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
       fz_lo[q] = fz_hi[q];
     }
     split_cell_update<C>(P, lin(g, i, j, k), i, j, k, res, ring[sk + own], st);
+    cp_async_wait_all();
+    if (next_own) fix_mirrored(g, i, j, k + 3, ring + slot(k + 3) + own, VS);
+    if (next_halo) fix_mirrored(g, i0 + hx - 2, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
+    __syncthreads();
   }
   split_stat_flush<C>(P, st);
 }
