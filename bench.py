@@ -1,11 +1,12 @@
 #!/usr/bin/env python
 """Benchmark: zone-updates/s of the explicit FV step on B200 (and the CPU reference arm).
 
-Default workload: 3D stratified convection box, Helmholtz EoS, well-balanced LHLLC + PLM + RK3,
-256^3 cells (the configuration the headline metric is quoted on).  A "step" is one full
-hydro step (3 RK stages) plus the CFL dt reduction, i.e. one iteration of time_loop without
-output; zone-updates/s = steps * cells / time (the reference's own "updated cells/s",
-source/source.F90:6834-6835).
+Default workload: 3D magnetised stratified box (Helmholtz EoS, well-balanced LHLLD + PLM + RK3,
+constrained transport, uniform horizontal B at plasma beta 1e4), 256^3 cells: the 3D Helmholtz
+MHD configuration the headline target is quoted on; --config stratified runs the hydro box.
+A "step" is one full hydro step (3 RK stages) plus the CFL dt reduction, i.e. one iteration of
+time_loop without output; zone-updates/s = steps * cells / time (the reference's own "updated
+cells/s", source/source.F90:6834-6835).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--n SIZE] [--impl ours|reference]
 
@@ -63,6 +64,21 @@ def default_size(name):
     return {"stratified": 256, "stratified_mhd": 256, "hot_bubble": 256, "orszag_tang": 1024}[name]
 
 
+def stage_kernels(cfg, form):
+    """Name of what the per-stage timing covers, and the kernel launches of one step."""
+    s = cfg.rk_stages
+    if cfg.mhd:
+        nax = 3 if cfg.sdims == 3 else 1
+        per = 1 + nax + cfg.sdims + 1
+        names = ("k_stage_split_mhd + k_corner_split + k_bface_split + k_c2p_mhd_split" if form == "fp32_split"
+                 else "k_stage + k_corner + k_bface + k_c2p_mhd")
+        return names + " (one MHD stage)", s * per + 2
+    if form == "fp32_split":
+        tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
+        return ("k_stage_split_tiled" if tiled else "k_stage_split") + " (FP32 fluxes, FP64 state/EoS)", s + 2
+    return "k_stage (FP64)", s + 2
+
+
 # DRAM bytes per cell of one stage-kernel launch, from ncu captures of the 128^3 stratified box
 # (dram__bytes_read.sum + dram__bytes_write.sum over 2,097,152 cells); the kernel streams the
 # domain once per launch, so the per-launch traffic scales with the cell count
@@ -87,6 +103,20 @@ def step_bytes_per_cell(cfg):
         b = s * (4 * nv + 4 * nv + 8 * nv + 8 * nv) + 8 * nv + (s - 1) * 8 * nv + 8
         if cfg.helmholtz:
             b += s * (16 + 16)  # temp (r+w, FP64) and the two FP32 gammas (r+w)
+        if cfg.mhd:
+            # per stage and cell, nd face directions: flux kernel reads the normal face B (FP64)
+            # and b_cc (FP32), writes 2 EMF components + 1 sign per face (FP32; 1 + 1 in 2D);
+            # corner kernel reads those, the FP32 velocities and b_cc, writes one corner EMF per
+            # axis; face update reads corner EMFs, B and B0, writes B; cons->prim reads B and U
+            # again and writes b_cc
+            nd = cfg.sdims
+            ne = 2 if nd == 3 else 1
+            nax = 3 if nd == 3 else 1
+            flux = 8 * nd + 4 * nd + 4 * nd * (ne + 1)
+            corner = 4 * nd * (ne + 1) + 4 * nd + 4 * nd + 4 * nax
+            face = 4 * nax + 8 * nd * 3
+            c2p = 8 * nd + 8 * nv + 4 * nd
+            b += s * (flux + corner + face + c2p)
         return b
     doubles = (nv + 1 + 3 * nv) + (s - 2) * (5 * nv) + (3 * nv + nv + 1)
     if cfg.helmholtz:
@@ -311,6 +341,24 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
     return res
 
 
+def long_run_errors(cfg, h, table, form, steps, local):
+    """Per-field relative L1 of `form` against the FP64 form after `steps` steps from h."""
+    from phlegethon_b200 import abi
+    from util import field_errors
+    out = {}
+    for f in (form, "fp64"):
+        hh = h.copy()
+        with abi.Simulation(cfg.replace(precision=f, device=local), table) as sim:
+            sim.upload(hh)
+            sim.init_thermo()
+            sim.compute_hyperbolic_dt()
+            done, _ = sim.time_loop(steps)
+            assert done == steps
+            sim.download(hh)
+        out[f] = hh
+    return field_errors(out[form], out["fp64"])
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -338,6 +386,9 @@ def run_ours(args):
         results[form] = measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
                                      want_e2e=(form == head_form))
     head = results[head_form]
+    l1_long = None
+    if args.l1_steps and head_form != "fp64":
+        l1_long = {"steps": args.l1_steps, "errors": long_run_errors(cfg, h, table, head_form, args.l1_steps, local)}
     value = aggregate_rate(world, head["done"], cells, head["ms"])
     fp64 = results["fp64"]
     fp64_value = aggregate_rate(world, fp64["done"], cells, fp64["ms"])
@@ -349,9 +400,7 @@ def run_ours(args):
     bytes_per_cell = step_bytes_per_cell(cfg.replace(precision=head_form))
     launch_ms = head["launch_ms"]
     achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
-    tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
-    kname = ("k_stage_split_tiled" if tiled else "k_stage_split") + " (FP32 fluxes, FP64 state/EoS)" \
-        if head_form == "fp32_split" else "k_stage (FP64)"
+    kname, launches_per_step = stage_kernels(cfg, head_form)
     tpc = TRAFFIC_PER_CELL.get((name, head_form))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": tpc * cells if tpc else None,
@@ -377,11 +426,11 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
                 "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
                                "speedup_of_form": value / fp64_value},
-                "l1_vs_fp64": errors,
+                "l1_vs_fp64": errors, "l1_vs_fp64_long": l1_long,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": head["h2d"],
                         "d2h_bytes_per_step": head["h2d"]},
-                "gpu_launches": int(head["done"] * (cfg.rk_stages + 2)), "clocks": head["clocks"],
+                "gpu_launches": int(head["done"] * launches_per_step), "clocks": head["clocks"],
                 "newton": {k: status[k] for k in ("newton_calls", "newton_iterations", "newton_nonconverged")},
                 "nonfinite": status["nonfinite"]}
         print(json.dumps(line), flush=True)
@@ -531,8 +580,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="stratified",
+    ap.add_argument("--config", default="stratified_mhd",
                     choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang", "eos"])
+    ap.add_argument("--l1-steps", type=int, default=0,
+                    help="also run both forms this many steps from the initial state and report the "
+                         "per-field relative L1 difference (untimed)")
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--train-epochs", type=int, default=256, help="MLP training epochs (eos workload)")

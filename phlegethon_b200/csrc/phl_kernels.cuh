@@ -56,6 +56,11 @@ struct Prm {
   double inv_rho_ref, inv_p_ref, inv_v_ref;
   // face background of the split path in those units, FP32 (x / ref rounded once at upload)
   const float *sf_rho_f[3], *sf_p_f[3], *sf_ge_f[3], *sf_phi_f[3];
+  // MHD in the split path: B in units of b_ref = sqrt(p_ref) (magnetic pressure B^2/2 in p_ref),
+  // EMFs in v_ref b_ref; cell-centred B, face EMFs, mass-flux signs and corner EMFs in FP32
+  double b_ref, inv_b_ref;
+  float *bccf;
+  float *femf[3], *fsgn[3], *fcor[3];
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,

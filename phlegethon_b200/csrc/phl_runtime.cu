@@ -171,6 +171,7 @@ struct phl_ctx {
   double *eq_rho_cc = nullptr, *eq_p_cc = nullptr, *eq_ge_cc = nullptr, *phi_cc = nullptr, *grav = nullptr;
   double *eq_rho_f[3] = {}, *eq_p_f[3] = {}, *eq_ge_f[3] = {}, *phi_f[3] = {};
   float *sf_rho_f[3] = {}, *sf_p_f[3] = {}, *sf_ge_f[3] = {}, *sf_phi_f[3] = {};  // split path
+  float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
   // scalars
   double *scal = nullptr;
   unsigned long long *smax_bits = nullptr;
@@ -244,6 +245,10 @@ struct phl_ctx {
     P.inv_rho_ref = 1.0 / rho_ref;
     P.inv_p_ref = 1.0 / p_ref;
     P.inv_v_ref = 1.0 / v_ref;
+    P.b_ref = sqrt(p_ref);
+    P.inv_b_ref = 1.0 / P.b_ref;
+    P.bccf = bccf;
+    for (int d = 0; d < 3; ++d) { P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; }
     P.U = U;
     P.U0 = U0;
     P.eint = eint;
@@ -452,6 +457,18 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
     for (int a = 0; a < 3; ++a) {
       if (cfg->sdims == 2 && a != 2) continue;
       if ((rc = c->alloc(&c->cor[a], (size_t)c->ncor(a)))) return rc;
+    }
+    if (c->split) {
+      if ((rc = c->alloc(&c->bccf, (size_t)3 * N))) return rc;
+      for (int d = 0; d < cfg->sdims; ++d) {
+        long long nf = c->nfaces(d);
+        if ((rc = c->alloc(&c->femf[d], (size_t)3 * nf))) return rc;
+        if ((rc = c->alloc(&c->fsgn[d], (size_t)nf))) return rc;
+      }
+      for (int a = 0; a < 3; ++a) {
+        if (cfg->sdims == 2 && a != 2) continue;
+        if ((rc = c->alloc(&c->fcor[a], (size_t)c->ncor(a)))) return rc;
+      }
     }
   }
   if ((rc = c->alloc(&c->scal, 8))) return rc;
@@ -880,6 +897,18 @@ void *phl_device_field(phl_ctx *ctx, const char *name) {
   if (n == "b_x3") return ctx->bf[2];
   if (n == "prim_dev32") return ctx->Wf[ctx->cur];
   if (n == "gammaf_dev32") return ctx->gf[ctx->cur];
+  if (n == "b_cc32") return ctx->bccf;
+  // CT scratch of the last stage: face EMFs [3][faces] and mass-flux signs per face direction,
+  // corner EMFs per axis (FP64 form, and the FP32 arrays of the split form with suffix 32)
+  static const char *dn[3] = {"1", "2", "3"};
+  for (int d = 0; d < 3; ++d) {
+    if (n == std::string("emf_x") + dn[d]) return ctx->emf[d];
+    if (n == std::string("sign_x") + dn[d]) return ctx->sgnf[d];
+    if (n == std::string("emf_corner") + dn[d]) return ctx->cor[d];
+    if (n == std::string("emf_x") + dn[d] + "_32") return ctx->femf[d];
+    if (n == std::string("sign_x") + dn[d] + "_32") return ctx->fsgn[d];
+    if (n == std::string("emf_corner") + dn[d] + "_32") return ctx->fcor[d];
+  }
   return nullptr;
 }
 

@@ -107,6 +107,191 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
   }
 }
 
+// --------------------------------------------------------------------- FP32 Riemann (MHD)
+// HLLD / LHLLD (source.F90:13969-15024) on the split variables: qL/qR as for
+// riemann_hydro_split, bL/bR the face B in the normal frame (units sqrt(p_ref)), pe the face
+// equilibrium pressure.  Every difference of total pressures is formed from the deviations
+// (pT' = p' + B^2/2), the star pressure as pe + pT*' with the weights of the reference, and the
+// normal momentum flux is returned with pe removed (the reference's WB fix).  fluxb is the
+// induction flux (0, v1 B2 - B1 v2, v1 B3 - B1 v3).
+template <int DIM, int NV, bool FAST, int RIEM>
+__device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *qR, const float *bL,
+                                                  const float *bR, const float *gL, const float *gR, float pe,
+                                                  float gm, float mach_cutoff, float *flux, float *fluxb) {
+  constexpr int IP = 1 + DIM, IAS = 2 + DIM;
+  const float igmm1 = 1.0f / (gm - 1.0f);
+  float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
+  float v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
+  float pLd = qL[IP], pL = pe + pLd, eint, c2L, c2R;
+  if (FAST) { eint = pL / (gL[0] - 1.0f); c2L = gL[1] * pL * inv_rhoL; }
+  else { eint = pL * igmm1; c2L = gm * pL * inv_rhoL; }
+  float rhoeL = eint + 0.5f * rhoL * v2L;
+  float bx1L = bL[0], bx2L = bL[1], bx3L = DIM == 3 ? bL[2] : 0.0f;
+  float rhoR = qR[0], inv_rhoR = 1.0f / rhoR, vx1R = qR[1], vx2R = qR[2], vx3R = DIM == 3 ? qR[3] : 0.0f;
+  float v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
+  float pRd = qR[IP], pR = pe + pRd;
+  if (FAST) { eint = pR / (gR[0] - 1.0f); c2R = gR[1] * pR * inv_rhoR; }
+  else { eint = pR * igmm1; c2R = gm * pR * inv_rhoR; }
+  float rhoeR = eint + 0.5f * rhoR * v2R;
+  float bx1R = bR[0], bx2R = bR[1], bx3R = DIM == 3 ? bR[2] : 0.0f;
+
+  float bx1 = 0.5f * (bx1L + bx1R), bx1_2 = bx1 * bx1;
+  float pbL = 0.5f * (bx1_2 + bx2L * bx2L + bx3L * bx3L);
+  float pbR = 0.5f * (bx1_2 + bx2R * bx2R + bx3R * bx3R);
+  rhoeL = rhoeL + pbL;
+  rhoeR = rhoeR + pbR;
+  float ptLd = pLd + pbL, ptRd = pRd + pbR;  // total pressure deviations
+  float ptL = pe + ptLd, ptR = pe + ptRd;
+  float a2L = 2.0f * pbL * inv_rhoL, a2R = 2.0f * pbR * inv_rhoR;
+  float an2L = bx1_2 * inv_rhoL, an2R = bx1_2 * inv_rhoR;
+  float dummy = c2L + a2L;
+  float cL = sqrtf(0.5f * (c2L + a2L + sqrtf(fmaxf(dummy * dummy - 4.0f * c2L * an2L, 0.0f))));
+  dummy = c2R + a2R;
+  float cR = sqrtf(0.5f * (c2R + a2R + sqrtf(fmaxf(dummy * dummy - 4.0f * c2R * an2R, 0.0f))));
+  float max_c = fmaxf(cL, cR);
+  float sL = fminf(vx1L, vx1R) - max_c;
+  float sR = fmaxf(vx1L, vx1R) + max_c;
+  float dsuL = sL - vx1L, dsuR = sR - vx1R;
+  float inv_temp1 = 1.0f / (dsuR * rhoR - dsuL * rhoL);
+  float ustar = (dsuR * rhoR * vx1R - dsuL * rhoL * vx1L - (ptRd - ptLd)) * inv_temp1;
+  float dsumL = sL - ustar, dsumR = sR - ustar;
+  float phi = 1.0f;
+  if (RIEM == R_LHLLD) {
+    dummy = v2L + a2L;
+    float cu2L = 0.5f * (v2L + a2L + sqrtf(fmaxf(dummy * dummy - 4.0f * v2L * an2L, 0.0f)));
+    dummy = v2R + a2R;
+    float cu2R = 0.5f * (v2R + a2R + sqrtf(fmaxf(dummy * dummy - 4.0f * v2R * an2R, 0.0f)));
+    float machL = sqrtf(cu2L) / cL, machR = sqrtf(cu2R) / cR;
+    float mm = fmaxf(machL, machR);
+    if (mm < 0.6f) {
+      float chi = fminf(1.0f, fmaxf(machL, machR));
+      chi = fmaxf(mach_cutoff, chi);
+      phi = chi * (2.0f - chi);
+    }
+  }
+  // star total pressure: the weights sum to one, so pe factors out
+  float pstar_d = (dsuR * rhoR * ptLd - dsuL * rhoL * ptRd - phi * rhoL * rhoR * dsuR * dsuL * (vx1L - vx1R)) *
+                  inv_temp1;
+  float rhostarL = rhoL * dsuL / dsumL, rhostarR = rhoR * dsuR / dsumR;
+  float a1_inv = 1.0f / (rhoL * dsuL * dsumL - bx1_2);
+  float vx2starL = vx2L - bx1 * bx2L * (ustar - vx1L) * a1_inv;
+  float bx2starL = bx2L * (rhoL * dsuL * dsuL - bx1_2) * a1_inv;
+  float vx3starL = vx3L - bx1 * bx3L * (ustar - vx1L) * a1_inv;
+  float bx3starL = bx3L * (rhoL * dsuL * dsuL - bx1_2) * a1_inv;
+  float a2_inv = 1.0f / (rhoR * dsuR * dsumR - bx1_2);
+  float vx2starR = vx2R - bx1 * bx2R * (ustar - vx1R) * a2_inv;
+  float bx2starR = bx2R * (rhoR * dsuR * dsuR - bx1_2) * a2_inv;
+  float vx3starR = vx3R - bx1 * bx3R * (ustar - vx1R) * a2_inv;
+  float bx3starR = bx3R * (rhoR * dsuR * dsuR - bx1_2) * a2_inv;
+  float vdotbL = vx1L * bx1 + vx2L * bx2L + vx3L * bx3L;
+  float vdotbR = vx1R * bx1 + vx2R * bx2R + vx3R * bx3R;
+  float vdotbstarL = ustar * bx1 + vx2starL * bx2starL + vx3starL * bx3starL;
+  float vdotbstarR = ustar * bx1 + vx2starR * bx2starR + vx3starR * bx3starR;
+  // -pT u + pT* u* with pe factored: pe (u* - u) + (pT*' u* - pT' u)
+  float rhoestarL = (dsuL * rhoeL + pe * (ustar - vx1L) + (pstar_d * ustar - ptLd * vx1L) +
+                     bx1 * (vdotbL - vdotbstarL)) / dsumL;
+  float rhoestarR = (dsuR * rhoeR + pe * (ustar - vx1R) + (pstar_d * ustar - ptRd * vx1R) +
+                     bx1 * (vdotbR - vdotbstarR)) / dsumR;
+  float sqrt_rhostarL = sqrtf(rhostarL), sqrt_rhostarR = sqrtf(rhostarR);
+  float abs_bx1 = fabsf(bx1);
+  float sstarL = ustar - abs_bx1 / sqrt_rhostarL;
+  float sstarR = ustar + abs_bx1 / sqrt_rhostarR;
+  float inv_sqr_bar = 1.0f / (sqrt_rhostarL + sqrt_rhostarR);
+  float sgn = copysignf(1.0f, bx1);
+  float vx22star = (sqrt_rhostarL * vx2starL + sqrt_rhostarR * vx2starR + (bx2starR - bx2starL) * sgn) * inv_sqr_bar;
+  float bx22star = (sqrt_rhostarL * bx2starR + sqrt_rhostarR * bx2starL +
+                    sqrt_rhostarL * sqrt_rhostarR * (vx2starR - vx2starL) * sgn) * inv_sqr_bar;
+  float vx32star = (sqrt_rhostarL * vx3starL + sqrt_rhostarR * vx3starR + (bx3starR - bx3starL) * sgn) * inv_sqr_bar;
+  float bx32star = (sqrt_rhostarL * bx3starR + sqrt_rhostarR * bx3starL +
+                    sqrt_rhostarL * sqrt_rhostarR * (vx3starR - vx3starL) * sgn) * inv_sqr_bar;
+  float vdotb2star = ustar * bx1 + vx22star * bx22star + vx32star * bx32star;
+  float rhoe2starL = rhoestarL - sqrt_rhostarL * (vdotbstarL - vdotb2star) * sgn;
+  float rhoe2starR = rhoestarR + sqrt_rhostarR * (vdotbstarR - vdotb2star) * sgn;
+
+  fluxb[0] = 0.0f;
+  if (RIEM == R_LHLLD) {
+    float rho, vx1, vx2, vx3, rhoe, bx2, bx3;
+    if (sstarL > 0.0f) {
+      rho = rhostarL; vx1 = ustar; vx2 = vx2starL; vx3 = vx3starL; rhoe = rhoestarL; bx2 = bx2starL; bx3 = bx3starL;
+    } else if (ustar > 0.0f) {
+      rho = rhostarL; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starL; bx2 = bx22star; bx3 = bx32star;
+    } else if (sstarR > 0.0f) {
+      rho = rhostarR; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starR; bx2 = bx22star; bx3 = bx32star;
+    } else {
+      rho = rhostarR; vx1 = ustar; vx2 = vx2starR; vx3 = vx3starR; rhoe = rhoestarR; bx2 = bx2starR; bx3 = bx3starR;
+    }
+    flux[0] = rho * vx1;
+    flux[1] = rho * vx1 * vx1 + pstar_d - bx1_2;
+    flux[2] = rho * vx1 * vx2 - bx1 * bx2;
+    if (DIM == 3) flux[3] = rho * vx1 * vx3 - bx1 * bx3;
+    flux[IP] = (rhoe + (pe + pstar_d)) * vx1 - bx1 * (bx1 * vx1 + vx2 * bx2 + vx3 * bx3);
+    float sg = copysignf(1.0f, vx1), hp = 0.5f * (1.0f + sg), hm = 0.5f * (1.0f - sg);
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) flux[iv] = rho * vx1 * (hp * qL[iv] + hm * qR[iv]);
+    fluxb[1] = vx1 * bx2 - bx1 * vx2;
+    if (DIM == 3) fluxb[2] = vx1 * bx3 - bx1 * vx3;
+    return;
+  }
+  const bool left = ustar > 0.0f;
+  const float *q = left ? qL : qR;
+  float rho = left ? rhoL : rhoR, vx1 = left ? vx1L : vx1R, vx2 = left ? vx2L : vx2R, vx3 = left ? vx3L : vx3R;
+  float rhoe = left ? rhoeL : rhoeR, pt = left ? ptL : ptR, ptd = left ? ptLd : ptRd;
+  float bx2 = left ? bx2L : bx2R, bx3 = left ? bx3L : bx3R;
+  float vdotb = left ? vdotbL : vdotbR, rhostar = left ? rhostarL : rhostarR;
+  float vx2s = left ? vx2starL : vx2starR, vx3s = left ? vx3starL : vx3starR;
+  float bx2s = left ? bx2starL : bx2starR, bx3s = left ? bx3starL : bx3starR;
+  float rhoes = left ? rhoestarL : rhoestarR, rhoe2s = left ? rhoe2starL : rhoe2starR;
+  float s = left ? sL : sR, sst = left ? sstarL : sstarR;
+  const bool outer = left ? (sL > 0.0f) : (sR < 0.0f);
+  const bool single = left ? (sstarL > 0.0f) : (sstarR < 0.0f);
+  constexpr int NB = DIM == 3 ? 3 : 2;
+  float U[NV], f[NV], Ub[3], fb[3];
+  U[0] = rho; U[1] = rho * vx1; U[2] = rho * vx2; if (DIM == 3) U[3] = rho * vx3; U[IP] = rhoe;
+  f[0] = rho * vx1; f[1] = rho * vx1 * vx1 + ptd - bx1_2; f[2] = rho * vx1 * vx2 - bx1 * bx2;
+  if (DIM == 3) f[3] = rho * vx1 * vx3 - bx1 * bx3;
+  f[IP] = (rhoe + pt) * vx1 - bx1 * vdotb;
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) { U[iv] = rho * q[iv]; f[iv] = rho * vx1 * q[iv]; }
+  Ub[0] = bx1; Ub[1] = bx2; Ub[2] = bx3;
+  fb[0] = 0.0f; fb[1] = vx1 * bx2 - bx1 * vx2; fb[2] = vx1 * bx3 - bx1 * vx3;
+  if (outer) {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = f[iv];
+#pragma unroll
+    for (int iv = 0; iv < NB; ++iv) fluxb[iv] = fb[iv];
+    return;
+  }
+  float Us[NV], Ubs[3];
+  Us[0] = rhostar; Us[1] = rhostar * ustar; Us[2] = rhostar * vx2s; if (DIM == 3) Us[3] = rhostar * vx3s;
+  Us[IP] = rhoes;
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) Us[iv] = rhostar * q[iv];
+  Ubs[0] = bx1; Ubs[1] = bx2s; Ubs[2] = bx3s;
+  if (single) {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = f[iv] + s * (Us[iv] - U[iv]);
+#pragma unroll
+    for (int iv = 0; iv < NB; ++iv) fluxb[iv] = fb[iv] + s * (Ubs[iv] - Ub[iv]);
+    return;
+  }
+  float Uss[NV], Ubss[3];
+  Uss[0] = rhostar; Uss[1] = rhostar * ustar; Uss[2] = rhostar * vx22star; if (DIM == 3) Uss[3] = rhostar * vx32star;
+  Uss[IP] = rhoe2s;
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) Uss[iv] = rhostar * q[iv];
+  Ubss[0] = bx1; Ubss[1] = bx22star; Ubss[2] = bx32star;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    float d0 = Us[iv];
+    flux[iv] = f[iv] + s * (d0 - U[iv]) + sst * (Uss[iv] - d0);
+  }
+#pragma unroll
+  for (int iv = 0; iv < NB; ++iv) {
+    float d0 = Ubs[iv];
+    fluxb[iv] = fb[iv] + s * (d0 - Ub[iv]) + sst * (Ubss[iv] - d0);
+  }
+}
+
 // --------------------------------------------------------------------- FP32 loads
 template <class C>
 __device__ __forceinline__ void load_wf(const Prm &P, int i, int j, int k, float w[C::NV], float g2[2]) {
@@ -529,6 +714,406 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
   split_stat_flush<C>(P, st);
 }
 
+// --------------------------------------------------------------------- split MHD
+// Cell-centred B of a (possibly ghost) cell in units of b_ref, component d negated for each
+// mirrored dimension d.
+template <class C>
+__device__ __forceinline__ void load_bccf(const Prm &P, int i, int j, int k, float b[3]) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
+  long long c = lin(g, si, sj, sk);
+  b[0] = __ldg(P.bccf + c);
+  b[1] = __ldg(P.bccf + g.N + c);
+  b[2] = C::DIM == 3 ? __ldg(P.bccf + 2 * g.N + c) : 0.0f;
+  if (f0) b[0] = -b[0];
+  if (f1) b[1] = -b[1];
+  if (C::DIM == 3 && f2) b[2] = -b[2];
+}
+
+// MHD flux through the low face of cell m along d (cells m-2..m+1); also the induction flux
+// Fb (lab frame) and rho_L + rho_R at the face for the CT upwinding sign (source.F90:8138-9105
+// with the MHD parts 8327-8469, 8926-8959)
+template <class C>
+__device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi, int fj, int fk, const float *const w[4],
+                                                    const float *const gm[4], const float *const b[4], float F[C::NV],
+                                                    float Fb[3], float &rho_sum) {
+  constexpr int NV = C::NV, IP = C::IP;
+  const Geo &g = P.g;
+  float qL[NV], qR[NV], lo, hi;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    plm_f32(w[0][iv], w[1][iv], w[2][iv], lo, hi);
+    qL[iv] = hi;
+    plm_f32(w[1][iv], w[2][iv], w[3][iv], lo, hi);
+    qR[iv] = lo;
+  }
+  float bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
+#pragma unroll
+  for (int iv = 0; iv < C::DIM; ++iv) {
+    if (iv == d) continue;
+    plm_f32(b[0][iv], b[1][iv], b[2][iv], lo, hi);
+    bL[iv] = hi;
+    plm_f32(b[1][iv], b[2][iv], b[3][iv], lo, hi);
+    bR[iv] = lo;
+  }
+  const float bn = (float)(P.bf[d][face_lin(g, d, fi, fj, fk)] * P.inv_b_ref);
+  bL[d] = bn;
+  bR[d] = bn;
+  if (d == 1) {
+    float a = qL[1], c = qL[2]; qL[1] = c; qL[2] = -a;
+    a = qR[1]; c = qR[2]; qR[1] = c; qR[2] = -a;
+    a = bL[0]; c = bL[1]; bL[0] = c; bL[1] = -a;
+    a = bR[0]; c = bR[1]; bR[0] = c; bR[1] = -a;
+  } else if (C::DIM == 3 && d == 2) {
+    float a = qL[1], c = qL[2], e = qL[3]; qL[1] = e; qL[2] = a; qL[3] = c;
+    a = qR[1]; c = qR[2]; e = qR[3]; qR[1] = e; qR[2] = a; qR[3] = c;
+    a = bL[0]; c = bL[1]; e = bL[2]; bL[0] = e; bL[1] = a; bL[2] = c;
+    a = bR[0]; c = bR[1]; e = bR[2]; bR[0] = e; bR[1] = a; bR[2] = c;
+  }
+  float pe = 0.0f;
+  long long fb = 0;
+  if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
+  if (C::WB) {
+    float rho_eq = __ldg(P.sf_rho_f[d] + fb);
+    qL[0] = rho_eq + qL[0];
+    qR[0] = rho_eq + qR[0];
+    pe = __ldg(P.sf_p_f[d] + fb);
+  }
+  float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
+  if (C::HELM) {
+#pragma unroll
+    for (int iv = 0; iv < 2; ++iv) {
+      plm_f32(gm[0][iv], gm[1][iv], gm[2][iv], lo, hi);
+      gL[iv] = hi;
+      plm_f32(gm[1][iv], gm[2][iv], gm[3][iv], lo, hi);
+      gR[iv] = lo;
+    }
+    if (C::WB) {
+      float ge = __ldg(P.sf_ge_f[d] + fb);
+      gL[0] = gL[0] + ge;
+      gR[0] = gR[0] + ge;
+    }
+  }
+  riemann_mhd_split<C::DIM, NV, C::HELM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
+                                                   Fb);
+  if (d == 1) {
+    float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
+    a = Fb[0]; c = Fb[1]; Fb[0] = -c; Fb[1] = a;
+  } else if (C::DIM == 3 && d == 2) {
+    float a = F[1], c = F[2], e = F[3]; F[1] = c; F[2] = e; F[3] = a;
+    a = Fb[0]; c = Fb[1]; e = Fb[2]; Fb[0] = c; Fb[1] = e; Fb[2] = a;
+  }
+  rho_sum = qL[0] + qR[0];
+  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.sf_phi_f[d] + fb);
+}
+
+// FP32 face EMF components (units v_ref b_ref) and the CT mass-flux sign (source.F90:8926-8951)
+template <class C>
+__device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long long fidx, const float Fb[3], float frho,
+                                                     float rho_sum, float smax_s) {
+  const Geo &g = P.g;
+  long long nf = nfaces(g, d);
+  float *e = P.femf[d];
+  if (d == 0) { if (C::DIM == 3) e[1 * nf + fidx] = Fb[2]; e[2 * nf + fidx] = -Fb[1]; }
+  if (d == 1) { if (C::DIM == 3) e[0 * nf + fidx] = -Fb[2]; e[2 * nf + fidx] = Fb[0]; }
+  if (d == 2) { e[0 * nf + fidx] = Fb[1]; e[1 * nf + fidx] = -Fb[0]; }
+  // the reference's dead-band ratio f_rho / (rho_bar smax) in physical units: with f_rho and
+  // rho in scaled units it carries one factor v_ref, folded into smax_s = smax / v_ref
+  float mach = frho / (0.5f * rho_sum * smax_s), sgn = 0.0f;
+  if (mach > (float)g.mach_ct) sgn = 1.0f;
+  if (mach < -(float)g.mach_ct) sgn = -1.0f;
+  // a reflective wall face has mirror-image states and no mass flux: the reference (no FMA) gets
+  // exactly zero there, while FP32 with contracted products leaves a rounding residue whose sign
+  // would select an upwind side; the wall's dead-band value is restored explicitly
+  const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  const long long q = d == 0 ? fidx % n0 : (d == 1 ? (fidx / n0) % n1 : fidx / ((long long)n0 * n1));
+  if ((q == 0 && g.bc[d][0] != BC_PERIODIC) || (q == g.nx[d] && g.bc[d][1] != BC_PERIODIC)) sgn = 0.0f;
+  P.fsgn[d][fidx] = sgn;
+}
+
+// MHD stage, part 1: fluxes, face EMFs and the RK combine of U (one thread per cell)
+template <class C>
+__global__ void __launch_bounds__(128) k_stage_split_mhd(Prm P) {
+  if (!*P.active) return;
+  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.N) return;
+  const int i = (int)(c % g.nx[0]);
+  const int j = (int)((c / g.nx[0]) % g.nx[1]);
+  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+  const double dt = P.scal[1];
+  const float smax_s = (float)(P.scal[2] * P.inv_v_ref);
+  float res[NV];
+  float rho_dev = 0.0f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    float w[5][NV], gm5[5][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}}, b5[5][3];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      int ii = i + (d == 0 ? s - 2 : 0), jj = j + (d == 1 ? s - 2 : 0), kk = k + (d == 2 ? s - 2 : 0);
+      load_wf<C>(P, ii, jj, kk, w[s], gm5[s]);
+      load_bccf<C>(P, ii, jj, kk, b5[s]);
+    }
+    if (d == 0) rho_dev = w[2][0];
+    float Flo[NV], Fhi[NV], Fb[3], rs;
+    {
+      const float *const wv[4] = {w[0], w[1], w[2], w[3]}, *const gv[4] = {gm5[0], gm5[1], gm5[2], gm5[3]},
+                         *const bv[4] = {b5[0], b5[1], b5[2], b5[3]};
+      face_flux_split_mhd<C>(P, d, i, j, k, wv, gv, bv, Flo, Fb, rs);
+      store_face_emf_split<C>(P, d, face_lin(g, d, i, j, k), Fb, Flo[0], rs, smax_s);
+    }
+    {
+      const int hi_i = i + (d == 0), hi_j = j + (d == 1), hi_k = k + (d == 2);
+      const float *const wv[4] = {w[1], w[2], w[3], w[4]}, *const gv[4] = {gm5[1], gm5[2], gm5[3], gm5[4]},
+                         *const bv[4] = {b5[1], b5[2], b5[3], b5[4]};
+      face_flux_split_mhd<C>(P, d, hi_i, hi_j, hi_k, wv, gv, bv, Fhi, Fb, rs);
+      const int hc = d == 0 ? i : (d == 1 ? j : k);
+      if (hc == g.nx[d] - 1) store_face_emf_split<C>(P, d, face_lin(g, d, hi_i, hi_j, hi_k), Fb, Fhi[0], rs, smax_s);
+    }
+    const float inv_dl = (float)g.inv_dx[d];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      float dd = (Fhi[iv] - Flo[iv]) * inv_dl;
+      res[iv] = d == 0 ? dd : res[iv] + dd;
+    }
+  }
+  const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
+  double rd[NV];
+  rd[0] = (double)res[0] * fm;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) rd[1 + d] = (double)res[1 + d] * P.p_ref;
+  rd[IP] = (double)res[IP] * fe;
+#pragma unroll
+  for (int iv = IAS; iv < NV; ++iv) rd[iv] = (double)res[iv] * fm;
+  if (C::GRAV) {
+    const long long bc = bg_cc(g, i, j, k);
+    const double rho_dev_phys = (double)rho_dev * P.rho_ref;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
+  }
+  double u0[NV], u[NV];
+  if (P.first_stage) {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      u0[iv] = P.U[(long long)iv * g.N + c];
+      u[iv] = u0[iv];
+      P.U0[(long long)iv * g.N + c] = u0[iv];
+    }
+  } else {
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      u0[iv] = P.U0[(long long)iv * g.N + c];
+      u[iv] = P.U[(long long)iv * g.N + c];
+    }
+  }
+  const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) P.U[(long long)iv * g.N + c] = a1 * u0[iv] + a2 * u[iv] + a3 * rd[iv];
+}
+
+// FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
+// EMF BC: the wall-normal component keeps its sign, the others flip; source.F90:11374-11964)
+template <class C>
+__device__ __forceinline__ void face_emf_split_at(const Prm &P, int d, int comp, int i, int j, int k, float &e,
+                                                  float &sgn) {
+  const Geo &g = P.g;
+  int c[3] = {i, j, k};
+  float fac = 1.0f;
+#pragma unroll
+  for (int d2 = 0; d2 < C::DIM; ++d2) {
+    if (d2 == d) continue;
+    int n = g.nx[d2];
+    if (c[d2] < 0) {
+      if (g.bc[d2][0] == BC_PERIODIC) c[d2] += n;
+      else { c[d2] = 0; if (comp != d2) fac = -fac; }
+    } else if (c[d2] >= n) {
+      if (g.bc[d2][1] == BC_PERIODIC) c[d2] -= n;
+      else { c[d2] = n - 1; if (comp != d2) fac = -fac; }
+    }
+  }
+  long long f = face_lin(g, d, c[0], c[1], c[2]);
+  e = fac * P.femf[d][(long long)comp * nfaces(g, d) + f];
+  sgn = P.fsgn[d][f];
+}
+
+// cell-centred -v x B component a from the stage's input state (scaled units)
+template <class C>
+__device__ __forceinline__ float emf_cell_split(const Prm &P, int a, int i, int j, int k) {
+  const Geo &g = P.g;
+  bool f0 = false, f1 = false, f2 = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
+  long long c = lin(g, si, sj, sk);
+  float v[3], b[3];
+  v[0] = P.Wf_in[g.N + c];
+  v[1] = P.Wf_in[2 * g.N + c];
+  v[2] = C::DIM == 3 ? P.Wf_in[3 * g.N + c] : 0.0f;
+  b[0] = P.bccf[c];
+  b[1] = P.bccf[g.N + c];
+  b[2] = C::DIM == 3 ? P.bccf[2 * g.N + c] : 0.0f;
+  if (f0) { v[0] = -v[0]; b[0] = -b[0]; }
+  if (f1) { v[1] = -v[1]; b[1] = -b[1]; }
+  if (f2) { v[2] = -v[2]; b[2] = -b[2]; }
+  if (a == 2) return -v[0] * b[1] + v[1] * b[0];
+  if (a == 0) return v[2] * b[1] - v[1] * b[2];
+  return v[0] * b[2] - v[2] * b[0];
+}
+
+// corner EMF along axis a (source.F90:11966-12206), FP32; one thread per corner
+template <class C>
+__global__ void __launch_bounds__(256) k_corner_split(Prm P, int a) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  int pa, qa;
+  if (a == 2) { pa = 0; qa = 1; } else if (a == 0) { pa = 1; qa = 2; } else { pa = 2; qa = 0; }
+  int n0 = g.nx[0] + (a != 0), n1 = g.nx[1] + (a != 1), n2 = C::DIM == 3 ? g.nx[2] + (a != 2) : 1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n0 * n1 * n2) return;
+  int c[3];
+  c[0] = (int)(t % n0);
+  c[1] = (int)((t / n0) % n1);
+  c[2] = (int)(t / ((long long)n0 * n1));
+  int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
+  int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
+  int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
+  float emf_N, emf_E, emf_S, emf_W, sgS, sgN, sgW, sgE;
+  face_emf_split_at<C>(P, pa, a, c[0], c[1], c[2], emf_N, sgN);
+  face_emf_split_at<C>(P, qa, a, c[0], c[1], c[2], emf_E, sgE);
+  face_emf_split_at<C>(P, pa, a, cqm[0], cqm[1], cqm[2], emf_S, sgS);
+  face_emf_split_at<C>(P, qa, a, cpm[0], cpm[1], cpm[2], emf_W, sgW);
+  float emf_SW = emf_cell_split<C>(P, a, cpq[0], cpq[1], cpq[2]);
+  float emf_NW = emf_cell_split<C>(P, a, cpm[0], cpm[1], cpm[2]);
+  float emf_NE = emf_cell_split<C>(P, a, c[0], c[1], c[2]);
+  float emf_SE = emf_cell_split<C>(P, a, cqm[0], cqm[1], cqm[2]);
+  float sgn = sgS;
+  float demf_S = 0.5f * (1.0f + sgn) * (emf_W - emf_SW) + 0.5f * (1.0f - sgn) * (emf_E - emf_SE);
+  sgn = sgN;
+  float demf_N = 0.5f * (1.0f + sgn) * (emf_NW - emf_W) + 0.5f * (1.0f - sgn) * (emf_NE - emf_E);
+  sgn = sgW;
+  float demf_W = 0.5f * (1.0f + sgn) * (emf_S - emf_SW) + 0.5f * (1.0f - sgn) * (emf_N - emf_NW);
+  sgn = sgE;
+  float demf_E = 0.5f * (1.0f + sgn) * (emf_SE - emf_S) + 0.5f * (1.0f - sgn) * (emf_NE - emf_N);
+  P.fcor[a][t] = 0.25f * (emf_S + emf_W + emf_N + emf_E + demf_S - demf_N + demf_W - demf_E);
+}
+
+// face-B update (source.F90:12208-12437) in FP64 from the FP32 corner EMFs; one thread per face
+template <class C>
+__global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  long long nf = nfaces(g, d);
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  int i = (int)(t % n0), j = (int)((t / n0) % n1), k = (int)(t / ((long long)n0 * n1));
+  const double dt = P.scal[1];
+  const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt * (P.v_ref * P.b_ref);
+  const float *E1 = P.fcor[0], *E2 = P.fcor[1], *E3 = P.fcor[2];
+  // differences of the FP32 corner EMFs are formed in FP64 (exact), so the discrete divergence
+  // of the update cancels to FP64 rounding as in the FP64 form
+  auto e = [](const float *E, long long q) { return (double)E[q]; };
+  double tmp;
+  if (d == 0) {
+    if (C::DIM == 2) tmp = (e(E3, cor_lin(g, 2, i, j + 1, k)) - e(E3, cor_lin(g, 2, i, j, k))) * g.inv_dx[1];
+    else tmp = -(e(E2, cor_lin(g, 1, i, j, k + 1)) - e(E2, cor_lin(g, 1, i, j, k))) * g.inv_dx[2] +
+               (e(E3, cor_lin(g, 2, i, j + 1, k)) - e(E3, cor_lin(g, 2, i, j, k))) * g.inv_dx[1];
+  } else if (d == 1) {
+    if (C::DIM == 2) tmp = (e(E3, cor_lin(g, 2, i, j, k)) - e(E3, cor_lin(g, 2, i + 1, j, k))) * g.inv_dx[0];
+    else tmp = (e(E1, cor_lin(g, 0, i, j, k + 1)) - e(E1, cor_lin(g, 0, i, j, k))) * g.inv_dx[2] +
+               (e(E3, cor_lin(g, 2, i, j, k)) - e(E3, cor_lin(g, 2, i + 1, j, k))) * g.inv_dx[0];
+  } else {
+    tmp = (e(E2, cor_lin(g, 1, i + 1, j, k)) - e(E2, cor_lin(g, 1, i, j, k))) * g.inv_dx[0] -
+          (e(E1, cor_lin(g, 0, i, j + 1, k)) - e(E1, cor_lin(g, 0, i, j, k))) * g.inv_dx[1];
+  }
+  double b = P.bf[d][t];
+  double b0;
+  if (P.first_stage) { b0 = b; P.b0f[d][t] = b; } else { b0 = P.b0f[d][t]; }
+  P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
+}
+
+// MHD stage, part 3: b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton
+// (FP64), FP32 deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
+template <class C>
+__global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
+  if (!*P.active) return;
+  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  const Geo &g = P.g;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  SplitStat st;
+  if (c < g.N) {
+    const int i = (int)(c % g.nx[0]);
+    const int j = (int)((c / g.nx[0]) % g.nx[1]);
+    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    const long long bc = bg_cc(g, i, j, k);
+    double bcc[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
+      bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+      P.bccf[(long long)d * g.N + c] = (float)(bcc[d] * P.inv_b_ref);
+    }
+    double u[NV];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) u[iv] = P.U[(long long)iv * g.N + c];
+    double rho = u[0], inv_rho = 1.0 / rho;
+    double ke = u[1] * u[1] + u[2] * u[2] + (DIM == 3 ? u[3] * u[3] : 0.0);
+    double eint = u[IP] - 0.5 * ke * inv_rho;
+    eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
+    if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
+    double p, T, sound;
+    if (C::HELM) {
+      double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
+      double abar = 1.0 / inv_abar, zbar = ye * abar;
+      T = P.temp[c];
+      int clamped = 0;
+      bool conv = false;
+      HelmCell hc;
+      helm_cell_init(P.helm, hc, rho, abar, zbar, T);
+      int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+      st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
+      helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
+      double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+      if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
+      P.gf_out[c] = (float)ge;
+      P.gf_out[g.N + c] = (float)gc;
+    } else {
+      p = (g.gm - 1.0) * eint;
+      T = p / (rho * CONST_RGAS * (1.0 / g.mu));
+      sound = sqrt(g.gm * p / rho);
+    }
+    double rdev = rho, pdev = p;
+    if (C::WB) {
+      rdev = rho - __ldg(P.eq_rho_cc + bc);
+      pdev = p - __ldg(P.eq_p_cc + bc);
+    }
+    P.Wf_out[c] = (float)(rdev * P.inv_rho_ref);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) P.Wf_out[(long long)(1 + d) * g.N + c] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
+    P.Wf_out[(long long)IP * g.N + c] = (float)(pdev * P.inv_p_ref);
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
+    P.temp[c] = T;
+    P.eint[c] = eint;
+    if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) st.bad += 1;
+    if (P.last_stage) {
+      double ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
+      double cs = sqrt(sound * sound + ca2 * inv_rho);
+      double sx1 = (fabs(u[1] * inv_rho) + cs) * g.inv_dx[0];
+      double sx2 = (fabs(u[2] * inv_rho) + cs) * g.inv_dx[1];
+      double sm = sx1 + sx2;
+      if (DIM == 3) sm = (fabs(u[3] * inv_rho) + cs) * g.inv_dx[2] + sm;
+      st.smax = sm;
+    }
+  }
+  split_stat_flush<C>(P, st);
+}
+
 // FP64 primitives (+eint, gammaf) -> U (FP64) and FP32 deviations (prim->cons of
 // source.F90:7057-7117)
 template <class C>
@@ -548,6 +1133,13 @@ __global__ void k_split_from_prim(Prm P) {
   double u[NV];
   u[0] = rho; u[1] = rho * vx1; u[2] = rho * vx2; if (DIM == 3) u[3] = rho * vx3;
   double rhoe = P.eint[c] + 0.5 * rho * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+  if (C::MHD) {
+    double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
+    rhoe = rhoe + 0.5 * (b0 * b0 + b1 * b1 + b2 * b2);
+    P.bccf[c] = (float)(b0 * P.inv_b_ref);
+    P.bccf[g.N + c] = (float)(b1 * P.inv_b_ref);
+    if (DIM == 3) P.bccf[2 * g.N + c] = (float)(b2 * P.inv_b_ref);
+  }
   if (C::ETOT) rhoe = rhoe + rho * __ldg(P.phi_cc + bc);
   u[IP] = rhoe;
 #pragma unroll
@@ -598,6 +1190,13 @@ __global__ void k_split_to_prim(Prm P) {
   } else {
     p = (g.gm - 1.0) * eint;
   }
+  if (C::MHD) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
+      P.bcc_out[(long long)d * g.N + c] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+    }
+  }
   P.Wout[c] = rho;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) P.Wout[(long long)(1 + d) * g.N + c] = u[1 + d] * inv_rho;
@@ -624,7 +1223,21 @@ struct SplitRunnerT : Runner {
     return allow_tiled && C::DIM == 3 && g.nx[0] % TX == 0 && g.nx[1] % TY == 0 && g.nx[2] % KZ == 0;
   }
   void stage(const Prm &P, cudaStream_t s) override {
-    if constexpr (C::DIM == 3) {
+    if constexpr (C::MHD) {
+      const Geo &g = P.g;
+      k_stage_split_mhd<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      for (int a = 0; a < 3; ++a) {
+        if (C::DIM == 2 && a != 2) continue;
+        long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
+        k_corner_split<C><<<nblk(n, 256), 256, 0, s>>>(P, a);
+      }
+      for (int d = 0; d < C::DIM; ++d) {
+        long long nf = (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
+        k_bface_split<C><<<nblk(nf, 256), 256, 0, s>>>(P, d);
+      }
+      k_c2p_mhd_split<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      return;
+    } else if constexpr (C::DIM == 3) {
       if (tiled(P.g)) {
         constexpr size_t sm = SplitTile<C, TX, TY>::bytes();
         if (!attr_set) {
@@ -652,6 +1265,12 @@ struct SplitRunnerT : Runner {
 };
 
 #define PHL_SPLIT_LIST(X)                 \
+  X(2, 4, true, false, false, R_HLLD)     \
+  X(2, 4, true, false, false, R_LHLLD)    \
+  X(3, 5, true, false, false, R_HLLD)     \
+  X(3, 5, true, false, false, R_LHLLD)    \
+  X(3, 7, true, true, true, R_LHLLD)      \
+  X(3, 7, true, true, true, R_HLLD)       \
   X(2, 4, false, false, false, R_LHLLC)   \
   X(2, 4, false, false, false, R_HLLC)    \
   X(2, 4, false, false, true, R_LHLLC)    \

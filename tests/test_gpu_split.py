@@ -81,3 +81,43 @@ def test_tiled_stage_equals_per_cell_stage(gpu_lib, table, riemann, monkeypatch)
         # no further from FP64 than the per-cell kernel, and apart by FP32 rounding noise only
         assert e_t[f] <= 1.5 * e_c[f] + 1e-12, (f, e_t, e_c)
         assert diff[f] <= 2.0 * e_c[f] + 1e-12, (f, diff, e_c)
+
+
+# ------------------------------------------------------------------------------ MHD
+@pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
+def test_split_orszag_tang(gpu_lib, riemann):
+    """Split MHD (FP32 HLLD/LHLLD, FP32 EMFs, FP64 face-B update) against the FP64 form."""
+    from util import div_b_max
+    cfg, h = problems.orszag_tang_2d(64, riemann=riemann)
+    h64, _ = run_form(cfg, h, 30, None, "fp64")
+    h32, st = run_form(cfg, h, 30, None, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0
+    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
+        assert err[f] <= lim, (f, err)
+    assert div_b_max(h32) <= 1e-13
+
+
+# LHLLD (the low-dissipation solver the low-Mach box is run with) keeps FP32 rounding-level
+# errors; HLLD's dissipative flux f + s (U* - U) cancels O(Mach) differences of O(1) states, so
+# its FP32 velocity and induction fluxes carry relative errors ~ eps / Mach
+MHD_LIMITS = {"lhlld": {"thermo": 1e-8, "v": 1e-5, "b": 1e-6},
+              "hlld": {"thermo": 1e-6, "v": 2e-3, "b": 1e-3}}
+
+
+@pytest.mark.parametrize("riemann", ["lhlld", "hlld"])
+def test_split_stratified_helmholtz_mhd(gpu_lib, table, riemann):
+    from util import div_b_max
+    cfg, h = problems.stratified_3d(16, ny=24, nz=12, mhd=True, riemann=riemann)
+    h64, _ = run_form(cfg, h, 30, table, "fp64")
+    h32, st = run_form(cfg, h, 30, table, "fp32_split")
+    err = field_errors(h32, h64)
+    lim = MHD_LIMITS[riemann]
+    assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    for f in ("rho", "p", "e", "T"):
+        assert err[f] <= lim["thermo"], (f, err)
+    for f in ("v1", "v2", "v3"):
+        assert err[f] <= lim["v"], (f, err)
+    for f in ("b1", "b2", "b3"):
+        assert err[f] <= lim["b"], (f, err)
+    assert div_b_max(h32) <= 1e-13
