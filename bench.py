@@ -69,9 +69,12 @@ def stage_kernels(cfg, form):
     s = cfg.rk_stages
     if cfg.mhd:
         nax = 3 if cfg.sdims == 3 else 1
-        per = 1 + nax + cfg.sdims + 1
-        names = ("k_stage_split_mhd + k_corner_split + k_bface_split + k_c2p_mhd_split" if form == "fp32_split"
-                 else "k_stage + k_corner + k_bface + k_c2p_mhd")
+        if form == "fp32_split":
+            per = cfg.sdims + nax + cfg.sdims + 1
+            names = "k_face_split_mhd + k_corner_split + k_bface_split + k_c2p_mhd_split"
+        else:
+            per = 1 + nax + cfg.sdims + 1
+            names = "k_stage + k_corner + k_bface + k_c2p_mhd"
         return names + " (one MHD stage)", s * per + 2
     if form == "fp32_split":
         tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
@@ -104,18 +107,20 @@ def step_bytes_per_cell(cfg):
         if cfg.helmholtz:
             b += s * (16 + 16)  # temp (r+w, FP64) and the two FP32 gammas (r+w)
         if cfg.mhd:
-            # per stage and cell, nd face directions: flux kernel reads the normal face B (FP64)
+            # per stage and cell, nd face directions: face kernel reads the normal face B (FP64)
             # and b_cc (FP32), writes 2 EMF components + 1 sign per face (FP32; 1 + 1 in 2D);
             # corner kernel reads those, the FP32 velocities and b_cc, writes one corner EMF per
-            # axis; face update reads corner EMFs, B and B0, writes B; cons->prim reads B and U
-            # again and writes b_cc
+            # axis; face update reads corner EMFs, B and B0, writes B; cons->prim reads B and
+            # writes b_cc
             nd = cfg.sdims
             ne = 2 if nd == 3 else 1
             nax = 3 if nd == 3 else 1
-            flux = 8 * nd + 4 * nd + 4 * nd * (ne + 1)
+            # the flux divergence moves into cons->prim: face fluxes (FP32, nv per face) are
+            # written once and read once per cell-face direction
+            flux = 8 * nd + 4 * nd + 4 * nd * (ne + 1) + 4 * nv * nd
             corner = 4 * nd * (ne + 1) + 4 * nd + 4 * nd + 4 * nax
             face = 4 * nax + 8 * nd * 3
-            c2p = 8 * nd + 8 * nv + 4 * nd
+            c2p = 8 * nd + 4 * nv * nd + 4 * nd
             b += s * (flux + corner + face + c2p)
         return b
     doubles = (nv + 1 + 3 * nv) + (s - 2) * (5 * nv) + (3 * nv + nv + 1)

@@ -61,6 +61,7 @@ struct Prm {
   double b_ref, inv_b_ref;
   float *bccf;
   float *femf[3], *fsgn[3], *fcor[3];
+  float *fflux[3];  // FP32 face fluxes [NV][faces] per direction
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,

@@ -172,6 +172,7 @@ struct phl_ctx {
   double *eq_rho_f[3] = {}, *eq_p_f[3] = {}, *eq_ge_f[3] = {}, *phi_f[3] = {};
   float *sf_rho_f[3] = {}, *sf_p_f[3] = {}, *sf_ge_f[3] = {}, *sf_phi_f[3] = {};  // split path
   float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
+  float *fflux[3] = {};
   // scalars
   double *scal = nullptr;
   unsigned long long *smax_bits = nullptr;
@@ -248,7 +249,9 @@ struct phl_ctx {
     P.b_ref = sqrt(p_ref);
     P.inv_b_ref = 1.0 / P.b_ref;
     P.bccf = bccf;
-    for (int d = 0; d < 3; ++d) { P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; }
+    for (int d = 0; d < 3; ++d) {
+      P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; P.fflux[d] = fflux[d];
+    }
     P.U = U;
     P.U0 = U0;
     P.eint = eint;
@@ -464,6 +467,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
         long long nf = c->nfaces(d);
         if ((rc = c->alloc(&c->femf[d], (size_t)3 * nf))) return rc;
         if ((rc = c->alloc(&c->fsgn[d], (size_t)nf))) return rc;
+        if ((rc = c->alloc(&c->fflux[d], (size_t)nv * nf))) return rc;
       }
       for (int a = 0; a < 3; ++a) {
         if (cfg->sdims == 2 && a != 2) continue;

@@ -834,86 +834,32 @@ __device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long l
   P.fsgn[d][fidx] = sgn;
 }
 
-// MHD stage, part 1: fluxes, face EMFs and the RK combine of U (one thread per cell)
+// MHD stage, part 1: one thread per face of direction d solves it once: the FP32 flux goes to
+// P.fflux[d] ([NV][faces]), the face EMF and the CT sign to their arrays
 template <class C>
-__global__ void __launch_bounds__(128) k_stage_split_mhd(Prm P) {
+__global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
   if (!*P.active) return;
-  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
+  constexpr int NV = C::NV;
   const Geo &g = P.g;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.N) return;
-  const int i = (int)(c % g.nx[0]);
-  const int j = (int)((c / g.nx[0]) % g.nx[1]);
-  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
-  const double dt = P.scal[1];
-  const float smax_s = (float)(P.scal[2] * P.inv_v_ref);
-  float res[NV];
-  float rho_dev = 0.0f;
+  const long long nf = nfaces(g, d);
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
+  float w[4][NV], gm4[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, b4[4][3];
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) {
-    float w[5][NV], gm5[5][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}}, b5[5][3];
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-      int ii = i + (d == 0 ? s - 2 : 0), jj = j + (d == 1 ? s - 2 : 0), kk = k + (d == 2 ? s - 2 : 0);
-      load_wf<C>(P, ii, jj, kk, w[s], gm5[s]);
-      load_bccf<C>(P, ii, jj, kk, b5[s]);
-    }
-    if (d == 0) rho_dev = w[2][0];
-    float Flo[NV], Fhi[NV], Fb[3], rs;
-    {
-      const float *const wv[4] = {w[0], w[1], w[2], w[3]}, *const gv[4] = {gm5[0], gm5[1], gm5[2], gm5[3]},
-                         *const bv[4] = {b5[0], b5[1], b5[2], b5[3]};
-      face_flux_split_mhd<C>(P, d, i, j, k, wv, gv, bv, Flo, Fb, rs);
-      store_face_emf_split<C>(P, d, face_lin(g, d, i, j, k), Fb, Flo[0], rs, smax_s);
-    }
-    {
-      const int hi_i = i + (d == 0), hi_j = j + (d == 1), hi_k = k + (d == 2);
-      const float *const wv[4] = {w[1], w[2], w[3], w[4]}, *const gv[4] = {gm5[1], gm5[2], gm5[3], gm5[4]},
-                         *const bv[4] = {b5[1], b5[2], b5[3], b5[4]};
-      face_flux_split_mhd<C>(P, d, hi_i, hi_j, hi_k, wv, gv, bv, Fhi, Fb, rs);
-      const int hc = d == 0 ? i : (d == 1 ? j : k);
-      if (hc == g.nx[d] - 1) store_face_emf_split<C>(P, d, face_lin(g, d, hi_i, hi_j, hi_k), Fb, Fhi[0], rs, smax_s);
-    }
-    const float inv_dl = (float)g.inv_dx[d];
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-      float dd = (Fhi[iv] - Flo[iv]) * inv_dl;
-      res[iv] = d == 0 ? dd : res[iv] + dd;
-    }
+  for (int s = 0; s < 4; ++s) {
+    const int ii = fi + (d == 0 ? s - 2 : 0), jj = fj + (d == 1 ? s - 2 : 0), kk = fk + (d == 2 ? s - 2 : 0);
+    load_wf<C>(P, ii, jj, kk, w[s], gm4[s]);
+    load_bccf<C>(P, ii, jj, kk, b4[s]);
   }
-  const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
-  double rd[NV];
-  rd[0] = (double)res[0] * fm;
+  const float *const wv[4] = {w[0], w[1], w[2], w[3]}, *const gv[4] = {gm4[0], gm4[1], gm4[2], gm4[3]},
+                     *const bv[4] = {b4[0], b4[1], b4[2], b4[3]};
+  float F[NV], Fb[3], rs;
+  face_flux_split_mhd<C>(P, d, fi, fj, fk, wv, gv, bv, F, Fb, rs);
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) rd[1 + d] = (double)res[1 + d] * P.p_ref;
-  rd[IP] = (double)res[IP] * fe;
-#pragma unroll
-  for (int iv = IAS; iv < NV; ++iv) rd[iv] = (double)res[iv] * fm;
-  if (C::GRAV) {
-    const long long bc = bg_cc(g, i, j, k);
-    const double rho_dev_phys = (double)rho_dev * P.rho_ref;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
-  }
-  double u0[NV], u[NV];
-  if (P.first_stage) {
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-      u0[iv] = P.U[(long long)iv * g.N + c];
-      u[iv] = u0[iv];
-      P.U0[(long long)iv * g.N + c] = u0[iv];
-    }
-  } else {
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-      u0[iv] = P.U0[(long long)iv * g.N + c];
-      u[iv] = P.U[(long long)iv * g.N + c];
-    }
-  }
-  const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
-#pragma unroll
-  for (int iv = 0; iv < NV; ++iv) P.U[(long long)iv * g.N + c] = a1 * u0[iv] + a2 * u[iv] + a3 * rd[iv];
+  for (int iv = 0; iv < NV; ++iv) P.fflux[d][(long long)iv * nf + f] = F[iv];
+  store_face_emf_split<C>(P, d, f, Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
 }
 
 // FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
@@ -1037,8 +983,9 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
   P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
 }
 
-// MHD stage, part 3: b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton
-// (FP64), FP32 deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
+// MHD stage, part 3: flux divergence from the face fluxes, gravity and the RK combine of U (FP64),
+// b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
+// deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
 template <class C>
 __global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
@@ -1058,9 +1005,50 @@ __global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
       bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
       P.bccf[(long long)d * g.N + c] = (float)(bcc[d] * P.inv_b_ref);
     }
-    double u[NV];
+    // flux divergence (directions in the order of the hydro stage), gravity, RK combine
+    float res[NV];
 #pragma unroll
-    for (int iv = 0; iv < NV; ++iv) u[iv] = P.U[(long long)iv * g.N + c];
+    for (int d = 0; d < DIM; ++d) {
+      const long long nf = nfaces(g, d);
+      const long long flo = face_lin(g, d, i, j, k), fhi = face_lin(g, d, i + (d == 0), j + (d == 1), k + (d == 2));
+      const float inv_dl = (float)g.inv_dx[d];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        float dd = (P.fflux[d][(long long)iv * nf + fhi] - P.fflux[d][(long long)iv * nf + flo]) * inv_dl;
+        res[iv] = d == 0 ? dd : res[iv] + dd;
+      }
+    }
+    const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
+    double rd[NV];
+    rd[0] = (double)res[0] * fm;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) rd[1 + d] = (double)res[1 + d] * P.p_ref;
+    rd[IP] = (double)res[IP] * fe;
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) rd[iv] = (double)res[iv] * fm;
+    if (C::GRAV) {
+      const double rho_dev_phys = (double)P.Wf_in[c] * P.rho_ref;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
+    }
+    double u[NV];
+    {
+      const double dt = P.scal[1], a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        const double un = P.U[(long long)iv * g.N + c];
+        double u0;
+        if (P.first_stage) {
+          u0 = un;
+          P.U0[(long long)iv * g.N + c] = un;
+        } else {
+          u0 = P.U0[(long long)iv * g.N + c];
+        }
+        u[iv] = a1 * u0 + a2 * un + a3 * rd[iv];
+        P.U[(long long)iv * g.N + c] = u[iv];
+      }
+    }
     double rho = u[0], inv_rho = 1.0 / rho;
     double ke = u[1] * u[1] + u[2] * u[2] + (DIM == 3 ? u[3] * u[3] : 0.0);
     double eint = u[IP] - 0.5 * ke * inv_rho;
@@ -1225,7 +1213,10 @@ struct SplitRunnerT : Runner {
   void stage(const Prm &P, cudaStream_t s) override {
     if constexpr (C::MHD) {
       const Geo &g = P.g;
-      k_stage_split_mhd<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      for (int d = 0; d < C::DIM; ++d) {
+        long long nf = (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
+        k_face_split_mhd<C><<<nblk(nf, 128), 128, 0, s>>>(P, d);
+      }
       for (int a = 0; a < 3; ++a) {
         if (C::DIM == 2 && a != 2) continue;
         long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
