@@ -69,7 +69,8 @@ class PhlStatus(C.Structure):
         ("newton_calls", C.c_longlong), ("newton_iterations", C.c_longlong),
         ("newton_nonconverged", C.c_longlong), ("newton_clamped", C.c_longlong),
         ("mlp_accepted", C.c_longlong), ("mlp_rejected", C.c_longlong),
-        ("nonfinite", C.c_longlong), ("guess_evaluations", C.c_longlong), ("steps", C.c_longlong),
+        ("nonfinite", C.c_longlong), ("guess_evaluations", C.c_longlong),
+        ("tensor_core_stalls", C.c_longlong), ("steps", C.c_longlong),
         ("time", C.c_double),
         ("dt", C.c_double), ("smax", C.c_double),
     ]

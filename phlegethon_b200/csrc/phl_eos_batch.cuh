@@ -83,10 +83,12 @@ __device__ __forceinline__ void eos_finish(const HelmTable &h, long long t, doub
 }
 
 // Phase 1.  guess 0 / 2: warm or bracket guess and the full Newton.  guess 1: the learned guess
-// (computed warp-cooperatively on the tensor cores for all lanes), judged by at most 3 reference
+// (computed per block of 128 samples on the tensor cores), judged by at most 3 reference
 // Newton iterations; a sample whose guess did not converge within them without a reset is
 // appended to `queue` (queue[0] = count, then index | judged iterations << 56) for phase 2, so
 // that the fallback runs in converged warps instead of stalling the accepted lanes.
+// LEARNED selects the learned-guess instantiation (guess 1); the other carries no tensor-core code.
+template <bool LEARNED>
 __global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, const double *rho, const double *e,
                                                     const double *abar, const double *zbar, double *T,
                                                     double *p, double *cs, int *iters, int guess, MlpWeights mw,
@@ -95,20 +97,16 @@ __global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, co
   EosStat st;
   float lT_mlp = 0.0f;
   double ecold = 0.0;
-  if (guess == PHL_GUESS_MLP) {
+  if constexpr (LEARNED) {
     extern __shared__ __align__(128) unsigned char sm[];
-    __nv_bfloat16 *w2s, *hb;
-    float *z;
-    mlp_smem_carve(sm, blockDim.x >> 5, threadIdx.x >> 5, w2s, hb, z);
-    mlp_stage_w2(w2s, mw.w2bf);
-    __syncthreads();
+    MlpUmmaSmem &S = *reinterpret_cast<MlpUmmaSmem *>(sm);
     float feat[4] = {0, 0, 0, 0};
     if (t < n) {
       ecold = mlp_cold_energy(h, rho[t], abar[t], zbar[t]);
       st.v[6] = 1;
       mlp_features(rho[t], e[t] - ecold, abar[t], zbar[t], feat);
     }
-    lT_mlp = mlp_forward_warp(mw, feat, hb, z, w2s);
+    lT_mlp = mlp_forward_cta(mw, feat, S, stat + STAT_TC_STALLED);
   }
   bool reject = false;
   int judged = 0;
@@ -117,7 +115,7 @@ __global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, co
     double Tg;
     int used = 0, clamped = 0;
     bool conv = false;
-    if (guess == PHL_GUESS_MLP) {
+    if constexpr (LEARNED) {
       Tg = fmin(fmax(exp10((double)lT_mlp), h.Tl * 1.000001), h.Th * 0.999999);
       used = helm_rhoe_newton(h, r, ee, ab, zb, Tg, 3, clamped, &conv);
       st.v[3] = clamped;
@@ -142,7 +140,7 @@ __global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, co
       eos_finish(h, t, r, ab, zb, Tg, used, T, p, cs, iters);
     }
   }
-  if (guess == PHL_GUESS_MLP) {
+  if constexpr (LEARNED) {
     // warp-aggregated append of the rejected samples
     const unsigned mask = __ballot_sync(0xffffffffu, reject);
     if (mask) {
@@ -199,14 +197,14 @@ inline int eos_launch(const HelmTable &h, cudaStream_t s, long long n, const dou
                       int guess, MlpWeights mw, unsigned long long *stat, unsigned long long *queue, int nsm) {
   const unsigned blocks = (unsigned)((n + 127) / 128);
   if (guess != PHL_GUESS_MLP) {
-    k_eos_invert<<<blocks, 128, 0, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, nullptr);
+    k_eos_invert<false><<<blocks, 128, 0, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, nullptr);
     return (int)cudaGetLastError();
   }
-  const size_t sm = mlp_warp_smem(4);
-  cudaError_t err = cudaFuncSetAttribute(k_eos_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const size_t sm = sizeof(MlpUmmaSmem);
+  cudaError_t err = cudaFuncSetAttribute(k_eos_invert<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
   if (err != cudaSuccess) return (int)err;
-  k_eos_invert<<<blocks, 128, sm, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue);
+  k_eos_invert<true><<<blocks, 128, sm, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue);
   // enough resident blocks to cover every SM several times; the loop covers any queue length
   const unsigned fb = (unsigned)std::min<long long>((long long)nsm * 8, (long long)blocks);
   k_eos_fallback<<<fb, 128, 0, s>>>(h, queue, rho, e, abar, zbar, T, p, cs, iters, stat);
@@ -311,7 +309,9 @@ struct EosBatch {
   }
   int mlp_get(cudaStream_t s, float *p) { return mlp.get(s, p); }
   int mlp_set(cudaStream_t s, const float *p) { return mlp.set(s, p); }
-  int mlp_infer(cudaStream_t s, long long n, const float *f, float *o) { return mlp.infer(s, n, f, o); }
+  int mlp_infer(cudaStream_t s, long long n, const float *f, float *o, unsigned long long *stalled) {
+    return mlp.infer(s, n, f, o, stalled);
+  }
 };
 
 }  // namespace phl

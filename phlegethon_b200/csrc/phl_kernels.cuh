@@ -65,7 +65,7 @@ struct Prm {
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,
-       STAT_MLP_ACC, STAT_MLP_REJ, STAT_NONFINITE, STAT_GUESS_EVALS, STAT_COUNT };
+       STAT_MLP_ACC, STAT_MLP_REJ, STAT_NONFINITE, STAT_GUESS_EVALS, STAT_TC_STALLED, STAT_COUNT };
 
 __device__ __forceinline__ long long bg_cc(const Geo &g, int i, int j, int k) {
   return g.bg_profile ? (long long)j : lin(g, i, j, k);

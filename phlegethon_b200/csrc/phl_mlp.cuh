@@ -1,7 +1,8 @@
 // phl_mlp.cuh -- learned initial temperature guess for the (rho, e) -> T Newton inversion.
 // No reference counterpart.  A 4-64-64-1 MLP maps normalised (log10 rho, log10 e, Abar, Zbar)
 // to log10 T.  Parameters: FP32 master copy (Adam) plus a BF16 copy of the 64x64 hidden layer,
-// which runs on the tensor cores (BF16 operands, FP32 accumulate) in training and inference;
+// which runs on the tensor cores (BF16 operands, FP32 accumulate): tcgen05 MMAs with the
+// accumulator in tensor memory for inference, warp-level MMAs for the 64-sample training tiles;
 // the 4->64 input layer and the 64->1 output layer are FP32 on the CUDA cores.
 //
 // Training (all on the device): samples are drawn with a counter-based hash over the EoS
@@ -14,6 +15,7 @@
 #include <cuda_bf16.h>
 #include <mma.h>
 #include "phl_device.cuh"
+#include "phl_umma.cuh"
 
 namespace phl {
 
@@ -284,27 +286,38 @@ __global__ void k_mlp_init(float *params, unsigned long long seed) {
   params[p] = w;
 }
 
-// ------------------------------------------------------------------ warp-cooperative inference
-// 32 samples per warp (one per lane): layer 1 per lane, layer 2 as a 32x64x64 tensor-core
-// product through shared memory, layer 3 per lane.  Shared rows are padded (72 bf16, 68 f32) and
-// each lane moves its row in 16-byte pieces, so the per-lane row accesses are free of bank
-// conflicts (the 8 lanes of a 16-byte access phase land on disjoint 4-bank groups).
-constexpr int MLP_LDB = 72;  // padded bf16 row (activations and the W2 copy)
-constexpr int MLP_LDZ = 68;  // padded f32 row (layer-2 products)
+// ------------------------------------------------------------------ inference on tcgen05
+// 128 samples per CTA of 128 threads (thread = sample): layer 1 per thread in FP32, written as
+// BF16 row `tid` of A (128 x 64) in shared memory; one thread issues the layer-2 product
+// D = A W2^T (M = 128, N = 64, K = 64 as four K = 16 MMAs) into 64 tensor-memory columns; each
+// warp reads its 32 rows of D back (thread = row = sample) and finishes layer 3 in FP32.
+struct MlpUmmaSmem {
+  alignas(128) unsigned char A[128 * MLP_H * 2];  // hidden activations, core-matrix layout
+  alignas(128) unsigned char B[MLP_H * MLP_H * 2];  // W2 [out][in], core-matrix layout
+  uint64_t mbar;
+  uint32_t tmem;
+};
+constexpr int MLP_UMMA_COLS = 64;         // FP32 accumulator columns (N)
+constexpr int MLP_UMMA_POLLS = 1 << 22;   // mbarrier polls before a stalled MMA is reported
 
-__device__ __forceinline__ void mlp_stage_w2(__nv_bfloat16 *w2s, const __nv_bfloat16 *w2bf) {
-  // 64 rows x 8 pieces of 16 bytes
-  for (int q = threadIdx.x; q < MLP_H * 8; q += blockDim.x) {
-    int r = q >> 3, c = q & 7;
-    *reinterpret_cast<uint4 *>(w2s + r * MLP_LDB + 8 * c) = __ldg(reinterpret_cast<const uint4 *>(w2bf + r * MLP_H) + c);
+// All 128 threads of the block call this with uniform control flow.  A product that does not
+// complete within the poll limit increments *stalled (once per warp) and leaves layer 2 at zero.
+__device__ __forceinline__ float mlp_forward_cta(const MlpWeights &m, const float x[4], MlpUmmaSmem &S,
+                                                 unsigned long long *stalled) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    tmem_alloc(&S.tmem, MLP_UMMA_COLS);
+    tmem_relinquish();
   }
-}
-
-__device__ __forceinline__ float mlp_forward_warp(const MlpWeights &m, const float x[4], __nv_bfloat16 *hb,
-                                                  float *z, const __nv_bfloat16 *w2s) {
-  using namespace nvcuda;
-  const int lane = threadIdx.x & 31;
-  const float *W1 = m.w + MLP_OFF_W1, *b1 = m.w + MLP_OFF_B1, *b2 = m.w + MLP_OFF_B2, *W3 = m.w + MLP_OFF_W3;
+  if (tid == 0) mbar_init(&S.mbar, 1);
+  // W2 (row-major bf16 [out][in]) into the core-matrix layout, 16-byte pieces
+  for (int q = tid; q < MLP_H * 8; q += blockDim.x) {
+    const int n = q >> 3, c = q & 7;
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(m.w2bf + n * MLP_H) + c);
+    *reinterpret_cast<uint4 *>(S.B + umma_kmajor_offset(n, 8 * c)) = v;
+  }
+  // layer 1 (FP32) -> BF16 row tid of A
+  const float *W1 = m.w + MLP_OFF_W1, *b1 = m.w + MLP_OFF_B1;
 #pragma unroll 2
   for (int c = 0; c < MLP_H / 8; ++c) {
     __align__(16) __nv_bfloat16 v[8];
@@ -316,68 +329,56 @@ __device__ __forceinline__ float mlp_forward_warp(const MlpWeights &m, const flo
       for (int k = 0; k < 4; ++k) a = fmaf(__ldg(W1 + o * 4 + k), x[k], a);
       v[j] = __float2bfloat16(fmaxf(a, 0.0f));
     }
-    *reinterpret_cast<uint4 *>(hb + lane * MLP_LDB + 8 * c) = *reinterpret_cast<const uint4 *>(v);
+    *reinterpret_cast<uint4 *>(S.A + umma_kmajor_offset(tid, 8 * c)) = *reinterpret_cast<const uint4 *>(v);
   }
-  __syncwarp();
-  wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
-  wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::col_major> b;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+  fence_proxy_async_smem();
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+  const uint32_t tbase = S.tmem;
+  if (tid == 0) {
+    const uint32_t a0 = smem_u32(S.A), b0 = smem_u32(S.B);
+    constexpr uint32_t idesc = umma_idesc_bf16(128, MLP_H);
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      wmma::fill_fragment(acc, 0.0f);
-#pragma unroll
-      for (int kt = 0; kt < 4; ++kt) {
-        wmma::load_matrix_sync(a, hb + (16 * mt) * MLP_LDB + 16 * kt, MLP_LDB);
-        wmma::load_matrix_sync(b, w2s + (16 * nt) * MLP_LDB + 16 * kt, MLP_LDB);
-        wmma::mma_sync(acc, a, b, acc);
-      }
-      wmma::store_matrix_sync(z + (16 * mt) * MLP_LDZ + 16 * nt, acc, MLP_LDZ, wmma::mem_row_major);
-    }
+    for (int kk = 0; kk < MLP_H / 16; ++kk)
+      umma_bf16_f32(tbase, umma_desc(a0 + kk * UMMA_KSTEP_BYTES, UMMA_KCORE_BYTES, UMMA_ROW_GROUP_BYTES),
+                    umma_desc(b0 + kk * UMMA_KSTEP_BYTES, UMMA_KCORE_BYTES, UMMA_ROW_GROUP_BYTES), idesc, kk > 0);
+    umma_commit(&S.mbar);
   }
-  __syncwarp();
+  // a phase seen complete by any lane is complete for the whole warp
+  const bool done = __any_sync(0xffffffffu, mbar_wait_bounded(&S.mbar, 0, MLP_UMMA_POLLS));
+  tc_fence_after_sync();
   float out = __ldg(m.w + MLP_OFF_B3);
-#pragma unroll 4
-  for (int c = 0; c < MLP_H / 4; ++c) {
-    float4 q = *reinterpret_cast<const float4 *>(z + lane * MLP_LDZ + 4 * c);
-    out = fmaf(__ldg(W3 + 4 * c + 0), fmaxf(q.x + __ldg(b2 + 4 * c + 0), 0.0f), out);
-    out = fmaf(__ldg(W3 + 4 * c + 1), fmaxf(q.y + __ldg(b2 + 4 * c + 1), 0.0f), out);
-    out = fmaf(__ldg(W3 + 4 * c + 2), fmaxf(q.z + __ldg(b2 + 4 * c + 2), 0.0f), out);
-    out = fmaf(__ldg(W3 + 4 * c + 3), fmaxf(q.w + __ldg(b2 + 4 * c + 3), 0.0f), out);
+  if (done) {
+    const float *W3 = m.w + MLP_OFF_W3, *b2 = m.w + MLP_OFF_B2;
+    const uint32_t row_addr = tbase + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c = 0; c < MLP_H / 16; ++c) {
+      float z[16];
+      tmem_ld16(row_addr + 16 * c, z);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) out = fmaf(__ldg(W3 + 16 * c + q), fmaxf(z[q] + __ldg(b2 + 16 * c + q), 0.0f), out);
+    }
+  } else {
+    if (lane == 0 && stalled) atomicAdd(stalled, 1ull);
+    // give the product a second bounded chance to land before its columns are released
+    mbar_wait_bounded(&S.mbar, 0, MLP_UMMA_POLLS);
   }
-  __syncwarp();
+  tc_fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tbase, MLP_UMMA_COLS);
   return mlp_prior(x) + out * MLP_OUT_SCALE + MLP_OUT_SHIFT;
 }
 
-// dynamic shared memory of a block of `warps` warps running mlp_forward_warp
-__host__ __device__ constexpr size_t mlp_warp_smem(int warps) {
-  return sizeof(__nv_bfloat16) * MLP_H * MLP_LDB +
-         (size_t)warps * 32 * (MLP_LDB * sizeof(__nv_bfloat16) + MLP_LDZ * sizeof(float));
-}
-// carve the block's shared memory: W2 copy, then per-warp activations (all pieces 32-byte aligned)
-__device__ __forceinline__ void mlp_smem_carve(unsigned char *sm, int warps, int warp, __nv_bfloat16 *&w2s,
-                                               __nv_bfloat16 *&hb, float *&z) {
-  w2s = reinterpret_cast<__nv_bfloat16 *>(sm);
-  hb = w2s + MLP_H * MLP_LDB + (size_t)warp * 32 * MLP_LDB;
-  z = reinterpret_cast<float *>(sm + sizeof(__nv_bfloat16) * MLP_H * MLP_LDB +
-                                (size_t)warps * 32 * MLP_LDB * sizeof(__nv_bfloat16)) +
-      (size_t)warp * 32 * MLP_LDZ;
-}
-
 // per-sample inference kernel (features n x 4 -> log10 T), 128 threads per block
-__global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out) {
-  extern __shared__ __align__(128) unsigned char sm[];
-  __nv_bfloat16 *w2s, *hb;
-  float *z;
-  mlp_smem_carve(sm, 4, threadIdx.x >> 5, w2s, hb, z);
-  mlp_stage_w2(w2s, m.w2bf);
-  __syncthreads();
+__global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out,
+                                                   unsigned long long *stalled) {
+  __shared__ MlpUmmaSmem S;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float x[4] = {0, 0, 0, 0};
   if (t < n)
     for (int k = 0; k < 4; ++k) x[k] = feat[t * 4 + k];
-  float y = mlp_forward_warp(m, x, hb, z, w2s);
+  float y = mlp_forward_cta(m, x, S, stalled);
   if (t < n) out[t] = y;
 }
 
@@ -520,13 +521,10 @@ struct Mlp {
     if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
     return 0;
   }
-  int infer(cudaStream_t s, long long n, const float *f, float *o) {
+  int infer(cudaStream_t s, long long n, const float *f, float *o, unsigned long long *stalled) {
     if (!ready) return -4;
     if (n == 0) return 0;
-    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_warp_smem(4)) !=
-        cudaSuccess)
-      return -2;
-    k_mlp_infer<<<(unsigned)((n + 127) / 128), 128, mlp_warp_smem(4), s>>>(weights(), n, f, o);
+    k_mlp_infer<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(weights(), n, f, o, stalled);
     if (cudaGetLastError() != cudaSuccess) return -2;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
     return 0;

@@ -871,6 +871,7 @@ int phl_get_status(phl_ctx *ctx, phl_status *st) {
   st->mlp_rejected = (long long)h[STAT_MLP_REJ];
   st->nonfinite = (long long)h[STAT_NONFINITE];
   st->guess_evaluations = (long long)h[STAT_GUESS_EVALS];
+  st->tensor_core_stalls = (long long)h[STAT_TC_STALLED];
   st->steps = step;
   st->time = sc[0];
   st->dt = sc[1];
@@ -1060,7 +1061,7 @@ int phl_mlp_set_params(phl_ctx *ctx, const float *params) {
 int phl_mlp_infer_device(phl_ctx *ctx, long long n, const float *features, float *out) {
   if (!ctx || n < 0 || !features || !out) return PHL_E_INVALID;
   CK(cudaSetDevice(ctx->cfg.device));
-  return ctx->eos.mlp_infer(ctx->stream, n, features, out);
+  return ctx->eos.mlp_infer(ctx->stream, n, features, out, ctx->stat + STAT_TC_STALLED);
 }
 
 }  // extern "C"

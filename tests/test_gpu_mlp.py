@@ -96,6 +96,7 @@ def test_mlp_training_gains_over_bracket_guess(gpu_lib, table):
         for Tx in (Tb, Tm):
             assert np.max(np.abs(_energy(sim, rho, Tx, abar, zbar) - e) / np.abs(e)) < 1e-11
     assert stb["newton_nonconverged"] == 0 and stm["newton_nonconverged"] == 0
+    assert stm["tensor_core_stalls"] == 0 and st0["tensor_core_stalls"] == 0
     assert stm["newton_calls"] == n and stb["newton_calls"] == n
     # same temperature: to 1e-10 where the inversion is well conditioned, and everywhere within
     # what the 1e-11 energy tolerance allows
