@@ -114,8 +114,8 @@ typedef struct phl_status {
   long long nonfinite;            /* non-finite or non-positive rho/p/T produced */
   long long guess_evaluations;    /* EoS evaluations spent building initial guesses (bracket
                                      search, cold energy of the learned guess's input) */
-  long long tensor_core_stalls;   /* warps whose tensor-core product did not complete within the
-                                     poll limit (the learned guess then falls back) */
+  long long tensor_core_stalls;   /* asynchronous operations (tensor-core products, bulk tensor
+                                     copies) that did not complete within the poll limit */
   long long steps;                /* steps taken by this context */
   double time, dt, smax;
 } phl_status;

@@ -11,9 +11,11 @@
 // (rho / rho_ref, p / p_ref, v / v_ref with v_ref^2 = p_ref / rho_ref, phi / v_ref^2), fixed per run,
 // so products of deviations never leave FP32 range whatever the problem's cgs magnitudes.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <cstdlib>
 #include <cstring>
 #include "phl_eos_fast.cuh"
+#include "phl_umma.cuh"
 #include "phl_runner.h"
 
 namespace phl {
@@ -600,55 +602,99 @@ __device__ __forceinline__ void fix_mirrored(const Geo &g, int i, int j, int k, 
 template <class C, int TX, int TY>
 struct SplitTile {
   static constexpr int NQ = C::NV + (C::HELM ? 2 : 0);  // stored values per cell
-  static constexpr int SX = TX + 4, SY = TY + 4, PL = SX * SY;
+  // plane rows are TX + 8 wide with the tile at x offset XO = 4: a tensor copy of the plane
+  // starts at x = i0 - 4, a multiple of 4 floats (16 bytes) as bulk tensor copies require;
+  // the faces read x offsets 2 .. TX + 5
+  static constexpr int XO = 4, SX = TX + 8, SY = TY + 4, PL = SX * SY;
   static constexpr int NSLOT = 5;
   static constexpr int RING = NSLOT * NQ * PL;           // floats: [slot][q][y][x]
   static constexpr int FX = C::NV * TY * (TX + 1), FY = C::NV * (TY + 1) * TX;
-  static constexpr size_t bytes() { return sizeof(float) * (size_t)(RING + FX + FY); }
+  static constexpr int PLANE_BYTES = NQ * PL * 4;        // one staged plane, all fields
+  static_assert(PLANE_BYTES % 128 == 0, "slots stay 128-byte aligned");
+  static constexpr size_t MBAR_OFFSET = sizeof(float) * (size_t)(RING + FX + FY);  // 8-byte aligned
+  static constexpr size_t bytes() { return MBAR_OFFSET + 8 * NSLOT; }
 };
 
+// Tensor maps of the stage's FP32 input for the bulk tensor copies: W' as a 4D tensor
+// (x1, x2, x3, variable) and the two FASTEOS gammas likewise; box = one plane of the tile with
+// its halo, all variables.
+struct SplitMaps {
+  CUtensorMap w, g;
+};
+constexpr int SPLIT_TMA_POLLS = 1 << 22;  // mbarrier polls before a stalled copy is reported
+
 template <class C, int TX, int TY, int KZ>
-__global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
+__global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P, const __grid_constant__ SplitMaps maps,
+                                                                  int use_tma) {
   if (!*P.active) return;
   using T = SplitTile<C, TX, TY>;
-  constexpr int NV = C::NV, NQ = T::NQ, SX = T::SX, PL = T::PL, VS = PL;
+  constexpr int NV = C::NV, NQ = T::NQ, SX = T::SX, PL = T::PL, VS = PL, XO = T::XO;
   static_assert(C::DIM == 3, "tiled stage is 3D");
   constexpr int NHALO = 4 * TX + 4 * TY;  // halo cells the x1 and x2 faces read (no corners)
   static_assert(NHALO <= TX * TY, "one halo cell per thread");
-  extern __shared__ __align__(16) float smem[];
+  extern __shared__ __align__(128) float smem[];
   float *ring = smem;                      // [5][NQ][SY][SX]
   float *fx = smem + T::RING;              // [NV][TY][TX+1]
   float *fy = fx + T::FX;                  // [NV][TY+1][TX]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(smem) + T::MBAR_OFFSET);
   const Geo &g = P.g;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
   const int i = i0 + tx, j = j0 + ty;
   const float idx = (float)g.inv_dx[0], idy = (float)g.inv_dx[1], idz = (float)g.inv_dx[2];
-  const int own = (ty + 2) * SX + (tx + 2);  // own cell inside a plane
+  const int own = (ty + 2) * SX + (tx + XO);  // own cell inside a plane
   auto slot = [&](int k) { return ((k - k0 + 2) % T::NSLOT) * NQ * PL; };
-  // this thread's halo cell (x1/x2 halo of every plane), if any
+  SplitStat st;
+  // Interior tiles (the plane with its halo lies inside the domain in x1 and x2, x3 periodic)
+  // stage whole planes with bulk tensor copies; the others copy cell by cell with cp.async,
+  // mapping ghost indices and mirroring velocities.
+  const bool tma = use_tma && blockIdx.x >= 1 && blockIdx.x + 2 <= gridDim.x && blockIdx.y >= 1 &&
+                   blockIdx.y + 2 <= gridDim.y;
+  auto plane_copy = [&](int k) {
+    // one thread: arm the slot's barrier and copy plane k (x3 wrapped) with all variables
+    const int s = (k - k0 + 2) % T::NSLOT;
+    int kz = k % g.nx[2];
+    if (kz < 0) kz += g.nx[2];
+    mbar_arrive_expect_tx(mbar + s, T::PLANE_BYTES);
+    tma_load_4d(ring + s * NQ * PL, &maps.w, mbar + s, i0 - XO, j0 - 2, kz, 0);
+    if (NQ > NV) tma_load_4d(ring + s * NQ * PL + NV * PL, &maps.g, mbar + s, i0 - XO, j0 - 2, kz, 0);
+  };
+  auto plane_wait = [&](int k) {
+    // all threads: the n-th use of a slot completes phase n
+    const int u = k - k0 + 2, s = u % T::NSLOT;
+    if (!mbar_wait_bounded(mbar + s, (uint32_t)((u / T::NSLOT) & 1), SPLIT_TMA_POLLS) && threadIdx.x == 0)
+      atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
+  };
+  // this thread's halo cell (x1/x2 halo of every plane) for the cell-by-cell path, if any
   int hcell = -1, hx = 0, hy = 0;
   if ((int)threadIdx.x < NHALO) {
     const int h = threadIdx.x;
     if (h < 4 * TX) {
       const int r = h / TX;
-      hx = 2 + h % TX;
+      hx = XO + h % TX;
       hy = r < 2 ? r : TY + r;
     } else {
       const int h3 = h - 4 * TX, cc = h3 / TY;
       hy = 2 + h3 % TY;
-      hx = cc < 2 ? cc : TX + cc;
+      hx = cc < 2 ? XO - 2 + cc : XO + TX + cc - 2;
     }
     hcell = hy * SX + hx;
   }
-  SplitStat st;
-  // prologue: planes k0-2 .. k0+2 of the own column, halo of plane k0
-  for (int k = k0 - 2; k <= k0 + 2; ++k) load_wf_async<C>(P, i, j, k, ring + slot(k) + own, VS);
-  if (hcell >= 0) load_wf_async<C>(P, i0 + hx - 2, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
-  cp_async_commit();
-  cp_async_wait_all();
-  for (int k = k0 - 2; k <= k0 + 2; ++k) fix_mirrored(g, i, j, k, ring + slot(k) + own, VS);
-  if (hcell >= 0) fix_mirrored(g, i0 + hx - 2, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
+  if (tma) {
+    if (threadIdx.x < T::NSLOT) mbar_init(mbar + threadIdx.x, 1);
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int k = k0 - 2; k <= k0 + 2; ++k) plane_copy(k);
+    for (int k = k0 - 2; k <= k0 + 2; ++k) plane_wait(k);
+  } else {
+    // prologue: planes k0-2 .. k0+2 of the own column, halo of plane k0
+    for (int k = k0 - 2; k <= k0 + 2; ++k) load_wf_async<C>(P, i, j, k, ring + slot(k) + own, VS);
+    if (hcell >= 0) load_wf_async<C>(P, i0 + hx - XO, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
+    cp_async_commit();
+    cp_async_wait_all();
+    for (int k = k0 - 2; k <= k0 + 2; ++k) fix_mirrored(g, i, j, k, ring + slot(k) + own, VS);
+    if (hcell >= 0) fix_mirrored(g, i0 + hx - XO, j0 + hy - 2, k0, ring + slot(k0) + hcell, VS);
+  }
   __syncthreads();
   float fz_lo[NV], fz_hi[NV];
   {
@@ -660,11 +706,16 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
   for (int kk = 0; kk < KZ; ++kk) {
     const int k = k0 + kk;
     const int sk = slot(k);
-    // next copies: own column plane k+3, halo of plane k+1 (both unread during this plane)
-    const bool next_own = kk + 3 <= KZ + 1, next_halo = kk + 1 < KZ && hcell >= 0;
-    if (next_own) load_wf_async<C>(P, i, j, k + 3, ring + slot(k + 3) + own, VS);
-    if (next_halo) load_wf_async<C>(P, i0 + hx - 2, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
-    cp_async_commit();
+    // next copies: plane k+3 (tensor copy of the whole plane, or the own column) and the halo
+    // of plane k+1 (cell-by-cell path); neither is read during this plane
+    const bool next_own = kk + 3 <= KZ + 1, next_halo = !tma && kk + 1 < KZ && hcell >= 0;
+    if (tma) {
+      if (next_own && threadIdx.x == 0) plane_copy(k + 3);
+    } else {
+      if (next_own) load_wf_async<C>(P, i, j, k + 3, ring + slot(k + 3) + own, VS);
+      if (next_halo) load_wf_async<C>(P, i0 + hx - XO, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
+      cp_async_commit();
+    }
     {
       float F[NV];
       // low x1 face of the own cell
@@ -679,14 +730,14 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
       for (int q = 0; q < NV; ++q) fy[(q * (TY + 1) + ty) * TX + tx] = F[q];
       if (ty == 0) {
         // upper x2 face of the tile, column tx
-        const int c = (TY + 2) * SX + tx + 2;
+        const int c = (TY + 2) * SX + tx + XO;
         SmemCells<NV> cu{ring, {sk + c - 2 * SX, sk + c - SX, sk + c, sk + c + SX}, VS};
         face_flux_cells<C>(P, 1, i, j0 + TY, k, cu, F);
 #pragma unroll
         for (int q = 0; q < NV; ++q) fy[(q * (TY + 1) + TY) * TX + tx] = F[q];
       } else if (ty == 1 && tx < TY) {
         // upper x1 face of the tile, row tx
-        const int c = (tx + 2) * SX + TX + 2;
+        const int c = (tx + 2) * SX + TX + XO;
         SmemCells<NV> cr{ring, {sk + c - 2, sk + c - 1, sk + c, sk + c + 1}, VS};
         face_flux_cells<C>(P, 0, i0 + TX, j0 + tx, k, cr, F);
 #pragma unroll
@@ -706,9 +757,13 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P) {
       fz_lo[q] = fz_hi[q];
     }
     split_cell_update<C>(P, lin(g, i, j, k), i, j, k, res, ring[sk + own], st);
-    cp_async_wait_all();
-    if (next_own) fix_mirrored(g, i, j, k + 3, ring + slot(k + 3) + own, VS);
-    if (next_halo) fix_mirrored(g, i0 + hx - 2, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
+    if (tma) {
+      if (next_own) plane_wait(k + 3);
+    } else {
+      cp_async_wait_all();
+      if (next_own) fix_mirrored(g, i, j, k + 3, ring + slot(k + 3) + own, VS);
+      if (next_halo) fix_mirrored(g, i0 + hx - XO, j0 + hy - 2, k + 1, ring + slot(k + 1) + hcell, VS);
+    }
     __syncthreads();
   }
   split_stat_flush<C>(P, st);
@@ -1196,16 +1251,74 @@ __global__ void k_split_to_prim(Prm P) {
 
 namespace {
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime (no link to libcuda)
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 4D map (x1, x2, x3, variable) over an FP32 SoA field block, box = (bx, by, 1, nvar)
+bool encode_plane_map(CUtensorMap *m, const float *base, int nvar, const Geo &g, int bx, int by) {
+  PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+  if (!enc || !base) return false;
+  const cuuint64_t nx = (cuuint64_t)g.nx[0], ny = (cuuint64_t)g.nx[1], nz = (cuuint64_t)g.nx[2];
+  const cuuint64_t dims[4] = {nx, ny, nz, (cuuint64_t)nvar};
+  const cuuint64_t strides[3] = {nx * 4, nx * ny * 4, (cuuint64_t)g.N * 4};
+  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)nvar};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 }
 
 template <class C>
 struct SplitRunnerT : Runner {
   static constexpr int TX = 32, TY = 8, KZ = 16;
   bool attr_set = false;
-  // PHL_STAGE_KERNEL=cell selects the per-cell kernel on any grid (comparison of the two)
+  // tensor maps of the two FP32 state buffers (the stage input alternates between them)
+  struct MapEntry {
+    const float *w = nullptr;
+    SplitMaps maps;
+    bool ok = false;
+  } map_cache[2];
+  // maps of this stage's input, or false when interior tiles must also copy cell by cell
+  bool stage_maps(const Prm &P, SplitMaps &out) {
+    using T = SplitTile<C, TX, TY>;
+    const Geo &g = P.g;
+    // bulk copies need a periodic x3 (the plane index wraps) and interior tiles in x1 and x2
+    if (g.bc[2][0] != BC_PERIODIC || g.nx[0] < 3 * TX || g.nx[1] < 3 * TY) return false;
+    for (auto &e : map_cache)
+      if (e.w == P.Wf_in) {
+        out = e.maps;
+        return e.ok;
+      }
+    MapEntry &e = map_cache[map_cache[0].w ? 1 : 0];
+    e.w = P.Wf_in;
+    e.ok = encode_plane_map(&e.maps.w, P.Wf_in, C::NV, g, T::SX, T::SY);
+    if (e.ok && C::HELM) e.ok = encode_plane_map(&e.maps.g, P.gf_in, 2, g, T::SX, T::SY);
+    out = e.maps;
+    return e.ok;
+  }
+  // PHL_STAGE_KERNEL=cell selects the per-cell kernel on any grid, =tiled_cpasync the tiled
+  // kernel with cell-by-cell copies only (comparisons of the three)
   const bool allow_tiled = [] {
     const char *e = getenv("PHL_STAGE_KERNEL");
     return !(e && strcmp(e, "cell") == 0);
+  }();
+  const bool allow_tma = [] {
+    const char *e = getenv("PHL_STAGE_KERNEL");
+    return !(e && strcmp(e, "tiled_cpasync") == 0);
   }();
   bool tiled(const Geo &g) const {
     return allow_tiled && C::DIM == 3 && g.nx[0] % TX == 0 && g.nx[1] % TY == 0 && g.nx[2] % KZ == 0;
@@ -1237,7 +1350,10 @@ struct SplitRunnerT : Runner {
           attr_set = true;
         }
         dim3 grid(P.g.nx[0] / TX, P.g.nx[1] / TY, P.g.nx[2] / KZ);
-        k_stage_split_tiled<C, TX, TY, KZ><<<grid, TX * TY, sm, s>>>(P);
+        SplitMaps maps;
+        memset(&maps, 0, sizeof(maps));
+        const int use_tma = allow_tma && stage_maps(P, maps) ? 1 : 0;
+        k_stage_split_tiled<C, TX, TY, KZ><<<grid, TX * TY, sm, s>>>(P, maps, use_tma);
         return;
       }
     }

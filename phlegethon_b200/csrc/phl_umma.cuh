@@ -116,3 +116,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
 }
 
 }  // namespace phl
+
+// ------------------------------------------------------------------ TMA (bulk tensor copies)
+#include <cuda.h>
+namespace phl {
+// arm an mbarrier for `bytes` of asynchronous copies (one arrival)
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+// 4D tiled tensor copy global -> shared, completion counted on `mbar` (no multicast)
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *mbar, int c0, int c1, int c2,
+                                            int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(mbar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+}  // namespace phl
