@@ -73,8 +73,8 @@ def stage_kernels(cfg, form):
             per = cfg.sdims + nax + cfg.sdims + 1
             names = "k_face_split_mhd + k_corner_split + k_bface_split + k_c2p_mhd_split"
         else:
-            per = 1 + nax + cfg.sdims + 1
-            names = "k_stage + k_corner + k_bface + k_c2p_mhd"
+            per = cfg.sdims + nax + cfg.sdims + 1
+            names = "k_face_mhd + k_corner + k_bface + k_c2p_mhd"
         return names + " (one MHD stage)", s * per + 2
     if form == "fp32_split":
         tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
@@ -131,6 +131,7 @@ def step_bytes_per_cell(cfg):
         emf = 1 if nd == 2 else 2
         doubles += s * nd * (3 + 2 * (emf + 1)) + nd
         doubles += s * nd  # b_cc write
+        doubles += s * 2 * cfg.nvars * nd  # face fluxes written once and read back per direction
     return 8 * doubles
 
 

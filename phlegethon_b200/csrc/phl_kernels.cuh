@@ -62,6 +62,7 @@ struct Prm {
   float *bccf;
   float *femf[3], *fsgn[3], *fcor[3];
   float *fflux[3];  // FP32 face fluxes [NV][faces] per direction
+  double *dflux[3]; // FP64 MHD face fluxes [NV][faces] per direction
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,
@@ -433,6 +434,36 @@ __global__ void __launch_bounds__(128) k_stage(Prm P) {
   }
 }
 
+// --------------------------------------------------------------------- MHD: face fluxes
+// One thread per face of direction d: the face flux of the x1/x2/x3 sweeps (same inputs and
+// operations as the per-cell k_stage, which solves every face twice), stored in P.dflux[d],
+// plus the face EMF and CT sign
+template <class C>
+__global__ void __launch_bounds__(128) k_face_mhd(Prm P, int d) {
+  if (!*P.active) return;
+  constexpr int NV = C::NV;
+  const Geo &g = P.g;
+  const long long nf = nfaces(g, d);
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
+  const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
+  double w[4][NV], gmv[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, bc[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const int ii = fi + (d == 0 ? s - 2 : 0), jj = fj + (d == 1 ? s - 2 : 0), kk = fk + (d == 2 ? s - 2 : 0);
+    load_wdev<C>(P, ii, jj, kk, w[s]);
+    if (C::HELM) load_gdev<C>(P, ii, jj, kk, gmv[s]);
+    load_bcc<C>(P, ii, jj, kk, bc[s]);
+  }
+  double F[NV], Fb[3], rs;
+  face_flux<C>(P, d, fi, fj, fk, w[0], w[1], w[2], w[3], gmv[0], gmv[1], gmv[2], gmv[3], bc[0], bc[1], bc[2], bc[3],
+               F, Fb, rs);
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) P.dflux[d][(long long)iv * nf + f] = F[iv];
+  store_face_emf<C>(P, d, f, Fb, F[0], rs, P.scal[2]);
+}
+
 // --------------------------------------------------------------------- MHD: corner EMFs
 // Face EMF / sign of a face array along `d` at a possibly-ghost transverse index
 // (periodic wrap, or the reflective EMF BC: component == wall normal keeps its sign, the
@@ -559,8 +590,9 @@ __global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
   P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
 }
 
-// MHD cons->prim: b_cc from the updated faces, then the EoS (source.F90:12439-12487,
-// 13533-13686), last stage also the CFL max
+// MHD stage end: flux divergence of the face fluxes, gravity and the RK combine of U
+// (source.F90:9057-9102, 12606-12644, 13518-13531), b_cc from the updated faces, then
+// cons->prim with the EoS (source.F90:12439-12487, 13533-13686), last stage also the CFL max
 template <class C>
 __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
   if (!*P.active) return;
@@ -578,11 +610,67 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
     for (int d = 0; d < DIM; ++d) {
       int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
       bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
-      P.bcc_out[(long long)d * g.N + c] = bcc[d];
     }
-    double u[NV];
+    // flux divergence of the face fluxes, gravity and the RK combine, in the order of k_stage
+    double res[NV];
 #pragma unroll
-    for (int iv = 0; iv < NV; ++iv) u[iv] = P.U[(long long)iv * g.N + c];
+    for (int d = 0; d < DIM; ++d) {
+      const long long nf = nfaces(g, d);
+      const long long flo = face_lin(g, d, i, j, k), fhi = face_lin(g, d, i + (d == 0), j + (d == 1), k + (d == 2));
+      const double inv_dl = g.inv_dx[d];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        double dd = (P.dflux[d][(long long)iv * nf + fhi] - P.dflux[d][(long long)iv * nf + flo]) * inv_dl;
+        res[iv] = d == 0 ? dd : res[iv] + dd;
+      }
+    }
+    double w[NV];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) w[iv] = P.Win[(long long)iv * g.N + c];
+    if (C::GRAV) {
+      const long long b = bg_cc(g, i, j, k);
+      const double rho_dev = C::WB ? w[0] - __ldg(P.eq_rho_cc + b) : w[0];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        res[1 + d] = res[1 + d] - rho_dev * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + b);
+    }
+    double u0[NV], u[NV];
+    if (P.first_stage) {
+      double rho0 = w[0], vx1 = w[1], vx2 = w[2], vx3 = DIM == 3 ? w[3] : 0.0;
+      u0[0] = rho0;
+      u0[1] = rho0 * vx1;
+      u0[2] = rho0 * vx2;
+      if (DIM == 3) u0[3] = rho0 * vx3;
+      double rhoe0 = P.eint[c] + 0.5 * rho0 * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
+      {
+        // magnetic energy of the stage input (b_cc before this stage's face update)
+        double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
+        rhoe0 = rhoe0 + 0.5 * (b0 * b0 + b1 * b1 + b2 * b2);
+      }
+      if (C::ETOT) rhoe0 = rhoe0 + rho0 * __ldg(P.phi_cc + bg_cc(g, i, j, k));
+      u0[IP] = rhoe0;
+#pragma unroll
+      for (int iv = IAS; iv < NV; ++iv) u0[iv] = rho0 * w[iv];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) { u[iv] = u0[iv]; P.U0[(long long)iv * g.N + c] = u0[iv]; }
+    } else {
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        u0[iv] = P.U0[(long long)iv * g.N + c];
+        u[iv] = P.U[(long long)iv * g.N + c];
+      }
+    }
+    {
+      const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * P.scal[1];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) {
+        u[iv] = a1 * u0[iv] + a2 * u[iv] + a3 * res[iv];
+        P.U[(long long)iv * g.N + c] = u[iv];
+      }
+    }
+    // the stage input's b_cc has been read: store the new one
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) P.bcc_out[(long long)d * g.N + c] = bcc[d];
     double rho = u[0], rhovx1 = u[1], rhovx2 = u[2], rhovx3 = DIM == 3 ? u[3] : 0.0, rhoe = u[IP];
     double inv_rho = 1.0 / rho;
     double eint = rhoe - 0.5 * (rhovx1 * rhovx1 + rhovx2 * rhovx2 + rhovx3 * rhovx3) * inv_rho;

@@ -40,8 +40,11 @@ template <class C>
 struct RunnerT : Runner {
   void stage(const Prm &P, cudaStream_t s) override {
     const Geo &g = P.g;
-    k_stage<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
-    if constexpr (C::MHD) {
+    if constexpr (!C::MHD) {
+      k_stage<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+    } else {
+      // each face once, then corners, face B and (divergence + RK + cons->prim) per cell
+      for (int d = 0; d < C::DIM; ++d) k_face_mhd<C><<<nblk(nfaces_host(g, d), 128), 128, 0, s>>>(P, d);
       for (int a = 0; a < 3; ++a) {
         if (C::DIM == 2 && a != 2) continue;
         long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) *
@@ -173,6 +176,7 @@ struct phl_ctx {
   float *sf_rho_f[3] = {}, *sf_p_f[3] = {}, *sf_ge_f[3] = {}, *sf_phi_f[3] = {};  // split path
   float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
   float *fflux[3] = {};
+  double *dflux[3] = {};                                                               // FP64 MHD
   // scalars
   double *scal = nullptr;
   unsigned long long *smax_bits = nullptr;
@@ -251,6 +255,7 @@ struct phl_ctx {
     P.bccf = bccf;
     for (int d = 0; d < 3; ++d) {
       P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; P.fflux[d] = fflux[d];
+      P.dflux[d] = dflux[d];
     }
     P.U = U;
     P.U0 = U0;
@@ -461,6 +466,9 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
       if (cfg->sdims == 2 && a != 2) continue;
       if ((rc = c->alloc(&c->cor[a], (size_t)c->ncor(a)))) return rc;
     }
+    if (!c->split)
+      for (int d = 0; d < cfg->sdims; ++d)
+        if ((rc = c->alloc(&c->dflux[d], (size_t)nv * c->nfaces(d)))) return rc;
     if (c->split) {
       if ((rc = c->alloc(&c->bccf, (size_t)3 * N))) return rc;
       for (int d = 0; d < cfg->sdims; ++d) {
