@@ -62,3 +62,20 @@ def test_invalid_config_rejected_before_device_use(lib_path):
     s = abi.make_config_struct(cfg)
     s.abi_version = 12345
     assert lib.phl_init(C.byref(s), C.byref(ctx)) == -1
+
+
+def test_bench_algorithmic_bytes():
+    """Algorithmic HBM bytes per zone-update used for the roofline (derivations in bench.py)."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(os.path.dirname(__file__), "..", "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    from phlegethon_b200 import problems
+    cfg, _ = problems.stratified_3d(8)
+    assert bench.step_bytes_per_cell(cfg.replace(precision="fp64")) == 888
+    assert bench.step_bytes_per_cell(cfg.replace(precision="fp32_split")) == 776
+    cfgm, _ = problems.stratified_3d(8, mhd=True)
+    assert bench.step_bytes_per_cell(cfgm.replace(precision="fp32_split")) == 2072
+    name, launches = bench.stage_kernels(cfgm.replace(precision="fp32_split"), "fp32_split")
+    assert "k_face_split_mhd" in name and launches == 3 * (3 + 3 + 3 + 1) + 2
