@@ -149,6 +149,11 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
   if (g->fasteos) {
     eint = pL / (gL[0] - 1.0);
     cL = sqrt(gL[1] * pL * inv_rhoL);
+  } else if (g->helm) {
+    /* helm_rhoP_given from the face temperature guess (source.F90:15705-15720, 15777-15781) */
+    double ye = qL[ias], abar = 1.0 / qL[ias + 1], zbar = ye * abar, T = gL[0];
+    phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &cL, 1);
+    eint = eint * rhoL;
   } else {
     eint = igmm1 * pL;
     cL = sqrt(gm * pL * inv_rhoL);
@@ -160,6 +165,10 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
   if (g->fasteos) {
     eint = pR / (gR[0] - 1.0);
     cR = sqrt(gR[1] * pR * inv_rhoR);
+  } else if (g->helm) {
+    double ye = qR[ias], abar = 1.0 / qR[ias + 1], zbar = ye * abar, T = gR[0];
+    phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &cR, 1);
+    eint = eint * rhoR;
   } else {
     eint = igmm1 * pR;
     cR = sqrt(gm * pR * inv_rhoR);
@@ -233,6 +242,13 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
   double v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
   double pL = qL[ip], eint, c2L, c2R;
   if (g->fasteos) { eint = pL / (gL[0] - 1.0); c2L = gL[1] * pL * inv_rhoL; }
+  else if (g->helm) {
+    /* helm_rhoP_given from the face temperature guess (source.F90:14266-14275) */
+    double ye = qL[ias], abar = 1.0 / qL[ias + 1], zbar = ye * abar, T = gL[0], sound;
+    phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &sound, 1);
+    eint = eint * rhoL;
+    c2L = sound * sound;
+  }
   else { eint = pL * igmm1; c2L = gm * pL * inv_rhoL; }
   double rhoeL = eint + 0.5 * rhoL * v2L;
   double bx1L = bL[0], bx2L = bL[1], bx3L = three ? bL[2] : 0.0;
@@ -240,6 +256,12 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
   double v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
   double pR = qR[ip];
   if (g->fasteos) { eint = pR / (gR[0] - 1.0); c2R = gR[1] * pR * inv_rhoR; }
+  else if (g->helm) {
+    double ye = qR[ias], abar = 1.0 / qR[ias + 1], zbar = ye * abar, T = gR[0], sound;
+    phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &sound, 1);
+    eint = eint * rhoR;
+    c2R = sound * sound;
+  }
   else { eint = pR * igmm1; c2R = gm * pR * inv_rhoR; }
   double rhoeR = eint + 0.5 * rhoR * v2R;
   double bx1R = bR[0], bx2R = bR[1], bx3R = three ? bR[2] : 0.0;
@@ -469,6 +491,8 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
   shp sc = cellg(g, nv), sb = cellg(g, sd), s1 = cellg(g, 1), s2 = cellg(g, 2), s3 = cellg(g, 3);
   shp sin_ = interior(g, nv), sf3 = face(g, 3, dir), sf1 = face(g, 1, dir);
   shp sbf = bface(g, 1, dir), se = bface(g, 3, dir);
+  shp st1 = cellg(g, 1);
+  const int helm_nf = g->helm && !g->fasteos; /* Helmholtz without USE_FASTEOS */
   (void)s3; (void)G;
   int ta = dir == 0 ? 1 : 0, tb = dir == 2 ? 1 : 2; /* transverse axes */
   int nl = n[dir];
@@ -499,6 +523,7 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
         for (int iv = 0; iv < nv; ++iv) W[(m + 1) * nv + iv] = g->prim[OFF(&sc, iv, c[0], c[1], c[2])];
         if (g->mhd) for (int iv = 0; iv < sd; ++iv) Bc[(m + 1) * 3 + iv] = g->b_cc[OFF(&sb, iv, c[0], c[1], c[2])];
         if (g->fasteos) for (int iv = 0; iv < 2; ++iv) Gf[(m + 1) * 2 + iv] = g->gammaf[OFF(&s2, iv, c[0], c[1], c[2])];
+        if (helm_nf) Gf[(m + 1) * 2] = g->temp[OFF(&st1, 0, c[0], c[1], c[2])];
       }
 #define WC(m) (W + ((m) + 1) * nv)
       /* PLM over cells 0..n+1: face f=m is the low face of cell m */
@@ -578,9 +603,17 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
           }
         }
       }
+      /* without FASTEOS: the face temperature guess 1/2 (T(i-1) + T(i)) (source.F90:8488-8495) */
+      if (helm_nf)
+        for (int f = 1; f <= nl + 1; ++f) {
+          double tf = 0.5 * (Gf[f * 2] + Gf[(f + 1) * 2]);
+          gL[f * 2] = tf;
+          gR[f * 2] = tf;
+        }
       /* Riemann solver per face */
       for (int f = 1; f <= nl + 1; ++f) {
-        const double *gl = g->fasteos ? gL + f * 2 : NULL, *gr = g->fasteos ? gR + f * 2 : NULL;
+        const int thermo = g->fasteos || helm_nf;
+        const double *gl = thermo ? gL + f * 2 : NULL, *gr = thermo ? gR + f * 2 : NULL;
         if (g->mhd)
           phlo_riemann_mhd(g, qL + f * nv, qR + f * nv, bL + f * 3, bR + f * 3, gl, gr, fx + f * nv, fb + f * 3);
         else
@@ -960,6 +993,7 @@ void phlo_hydro_step(phlo_grid *g) {
     fill_ghosts(g, g->prim, nv, 1);
     if (g->mhd) fill_ghosts(g, g->b_cc, sd, 2);
     if (g->fasteos) fill_ghosts(g, g->gammaf, 2, 0);
+    if (g->helm && !g->fasteos) fill_ghosts(g, g->temp, 1, 0);
 
     for (int dir = 0; dir < sd; ++dir) sweep(g, &S, dir);
 

@@ -100,8 +100,9 @@ void phlo_eos_invert_batch(const phlo_helm *h, long n, const double *rho, const 
                            const double *zbar, double *T, int *iters, int guess, int nthreads);
 
 /* ---- Riemann solvers for one face, in the normal frame (source/source.F90:13969-16260) ----
- * q*: nvars primitive face states; g*: (gammae, gammac) face values for USE_FASTEOS (NULL
- * otherwise); b*: 3 components (normal first), MHD only. */
+ * q*: nvars primitive face states; g*: (gammae, gammac) face values for USE_FASTEOS, the face
+ * temperature guess in g*[0] for the Helmholtz EoS without USE_FASTEOS (helm_rhoP_given per
+ * side), NULL otherwise; b*: 3 components (normal first), MHD only. */
 void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
                         const double *gL, const double *gR, double *flux);
 void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,

@@ -164,7 +164,7 @@ class OracleGrid:
         g.sdims, g.nx1, g.nx2, g.nx3, g.ngc, g.nas, g.nvars = c.sdims, c.nx1, c.nx2, c.nx3, c.ngc, c.nas, c.nvars
         g.mhd, g.wb, g.gravity, g.etot = int(c.mhd), int(c.wb), int(c.gravity), int(c.etot)
         g.helm = int(c.helmholtz)
-        g.fasteos = int(c.helmholtz)
+        g.fasteos = int(c.helmholtz and c.fasteos)
         g.riemann = self.RIEM[c.riemann]
         g.rk_stages = c.rk_stages
         for d in range(3):

@@ -71,10 +71,13 @@ template <typename R>
 __device__ __forceinline__ R sgn1(R x) { return copysign(R(1), x); }
 
 // ------------------------------------------------------------------ hydro Riemann
-// qL/qR: [rho, v1, v2, (v3), p, scalars...] in the normal frame; gL/gR = (gammae, gammac) for
-// FASTEOS.  LHLLC source.F90:15681-16122 (Minoshima & Miyoshi low-dissipation pressure),
-// HLLC source.F90:16124-16252.
-template <typename R, int DIM, int NV, bool FAST, int RIEM>
+// qL/qR: [rho, v1, v2, (v3), p, scalars...] in the normal frame.  Side thermodynamics by EOSM:
+// EOS_IDEAL gamma-law; EOS_FAST gL/gR = (gammae, gammac) (USE_FASTEOS); EOS_GIVEN gL/gR =
+// (rho*e, sound speed) already evaluated by helm_rhoP_given (Helmholtz without USE_FASTEOS,
+// source.F90:15777-15781).  LHLLC source.F90:15681-16122 (Minoshima & Miyoshi low-dissipation
+// pressure), HLLC source.F90:16124-16252.
+enum { EOS_IDEAL = 0, EOS_FAST = 1, EOS_GIVEN = 2 };
+template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R *gL, const R *gR,
                                               R gm, R mach_cutoff, R *flux) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
@@ -82,13 +85,15 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
   R v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
   R pL = qL[IP], eint, cL, cR;
-  if (FAST) { eint = pL / (gL[0] - R(1)); cL = sqrt(gL[1] * pL * inv_rhoL); }
+  if (EOSM == EOS_FAST) { eint = pL / (gL[0] - R(1)); cL = sqrt(gL[1] * pL * inv_rhoL); }
+  else if (EOSM == EOS_GIVEN) { eint = gL[0]; cL = gL[1]; }
   else { eint = igmm1 * pL; cL = sqrt(gm * pL * inv_rhoL); }
   R rhoeL = eint + R(0.5) * rhoL * v2L;
   R rhoR = qR[0], inv_rhoR = R(1) / rhoR, vx1R = qR[1], vx2R = qR[2], vx3R = DIM == 3 ? qR[3] : R(0);
   R v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
   R pR = qR[IP];
-  if (FAST) { eint = pR / (gR[0] - R(1)); cR = sqrt(gR[1] * pR * inv_rhoR); }
+  if (EOSM == EOS_FAST) { eint = pR / (gR[0] - R(1)); cR = sqrt(gR[1] * pR * inv_rhoR); }
+  else if (EOSM == EOS_GIVEN) { eint = gR[0]; cR = gR[1]; }
   else { eint = igmm1 * pR; cR = sqrt(gm * pR * inv_rhoR); }
   R rhoeR = eint + R(0.5) * rhoR * v2R;
   R max_c = fmax(cL, cR);
@@ -149,7 +154,7 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
 // ------------------------------------------------------------------ MHD Riemann
 // HLLD (Miyoshi & Kusano) source.F90:13969-15016, LHLLD source.F90:14364-14384, 14663-14732.
 // b*: [Bn, Bt1, Bt2]; fluxb receives [0, Ft1, Ft2].
-template <typename R, int DIM, int NV, bool FAST, int RIEM>
+template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *bL, const R *bR,
                                             const R *gL, const R *gR, R gm, R mach_cutoff,
                                             R *flux, R *fluxb) {
@@ -158,14 +163,16 @@ __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *b
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
   R v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
   R pL = qL[IP], eint, c2L, c2R;
-  if (FAST) { eint = pL / (gL[0] - R(1)); c2L = gL[1] * pL * inv_rhoL; }
+  if (EOSM == EOS_FAST) { eint = pL / (gL[0] - R(1)); c2L = gL[1] * pL * inv_rhoL; }
+  else if (EOSM == EOS_GIVEN) { eint = gL[0]; c2L = gL[1] * gL[1]; }
   else { eint = pL * igmm1; c2L = gm * pL * inv_rhoL; }
   R rhoeL = eint + R(0.5) * rhoL * v2L;
   R bx1L = bL[0], bx2L = bL[1], bx3L = DIM == 3 ? bL[2] : R(0);
   R rhoR = qR[0], inv_rhoR = R(1) / rhoR, vx1R = qR[1], vx2R = qR[2], vx3R = DIM == 3 ? qR[3] : R(0);
   R v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
   R pR = qR[IP];
-  if (FAST) { eint = pR / (gR[0] - R(1)); c2R = gR[1] * pR * inv_rhoR; }
+  if (EOSM == EOS_FAST) { eint = pR / (gR[0] - R(1)); c2R = gR[1] * pR * inv_rhoR; }
+  else if (EOSM == EOS_GIVEN) { eint = gR[0]; c2R = gR[1] * gR[1]; }
   else { eint = pR * igmm1; c2R = gm * pR * inv_rhoR; }
   R rhoeR = eint + R(0.5) * rhoR * v2R;
   R bx1R = bR[0], bx2R = bR[1], bx3R = DIM == 3 ? bR[2] : R(0);

@@ -15,10 +15,13 @@
 
 namespace phl {
 
-template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_>
+// FAST_: USE_FASTEOS (gamma_e, gamma_c reconstructed to the faces); without it the Helmholtz
+// configurations evaluate helm_rhoP_given per Riemann side from the face temperature guess
+template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_, bool FAST_ = HELM_>
 struct Cfg {
   static constexpr int DIM = DIM_, NV = NV_, RIEM = RIEM_;
-  static constexpr bool MHD = MHD_, HELM = HELM_, WB = WB_, ETOT = ETOT_, GRAV = GRAV_;
+  static constexpr bool MHD = MHD_, HELM = HELM_, WB = WB_, ETOT = ETOT_, GRAV = GRAV_, FAST = HELM_ && FAST_;
+  static constexpr int EOSM = !HELM_ ? EOS_IDEAL : (FAST_ ? EOS_FAST : EOS_GIVEN);
   static constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   static_assert(!HELM || NV >= IAS + 2, "Helmholtz needs ADVECT_YE_IABAR scalars");
 };
@@ -140,6 +143,13 @@ __device__ __forceinline__ void load_gdev(const Prm &P, int i, int j, int k, dou
   int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f);
   int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f) : 0;
   long long c = lin(g, si, sj, sk);
+  if (!C::FAST) {
+    // without USE_FASTEOS the faces need the stage input's cell temperatures (the guess of
+    // helm_rhoP_given); they ride in the first gamma slot, which is ping-ponged per stage
+    gm_[0] = __ldg(P.gin + c);
+    gm_[1] = 0.0;
+    return;
+  }
   gm_[0] = __ldg(P.gin + c);
   gm_[1] = __ldg(P.gin + g.N + c);
   if (C::WB) gm_[0] = gm_[0] - __ldg(P.eq_ge_cc + bg_cc(g, si, sj, sk));
@@ -222,7 +232,7 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
     qR[IP] = qR[IP] + p_eq;
   }
   double gL[2] = {0, 0}, gR[2] = {0, 0};
-  if (C::HELM) {
+  if (C::FAST) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
       plm(gl2[iv], gl1[iv], gr1[iv], lo, hi);
@@ -235,12 +245,29 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
     }
+  } else if (C::HELM) {
+    // Helmholtz without USE_FASTEOS: helm_rhoP_given on each side of the face from the guess
+    // 1/2 (T(m-1) + T(m)) (source.F90:8488-8495, 15705-15720, 15777-15781); passes rho*e and c
+    const double tface = 0.5 * (gl1[0] + gr1[0]);
+    double *gs[2] = {gL, gR};
+    const double *qs[2] = {qL, qR};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const double *q = qs[side];
+      const double ye = q[C::IAS], abar = 1.0 / q[C::IAS + 1], zbar = ye * abar;
+      double T = tface, Pd, E, snd, cv;
+      int clamped = 0;
+      helm_rhoP_newton(P.helm, q[0], q[IP], abar, zbar, T, clamped);
+      helm_given_full(P.helm, q[0], T, abar, zbar, Pd, E, snd, cv);
+      gs[side][0] = E * q[0];
+      gs[side][1] = snd;
+    }
   }
   const double gm = P.g.gm, mc = P.g.mach_cutoff;
   if (C::MHD) {
-    riemann_mhd<double, C::DIM, NV, C::HELM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb);
+    riemann_mhd<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb);
   } else {
-    riemann_hydro<double, C::DIM, NV, C::HELM, C::RIEM>(qL, qR, gL, gR, gm, mc, F);
+    riemann_hydro<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, gm, mc, F);
   }
   // back to the lab frame
   if (d == 1) {
@@ -388,8 +415,12 @@ __global__ void __launch_bounds__(128) k_stage(Prm P) {
         n_calls += 1; n_iters += it; n_nonconv += (it == 100); n_clamp += clamped;
         double E, cv;
         helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
-        P.gout[c] = p / eint + 1.0;
-        P.gout[g.N + c] = sound * sound * rho / p;
+        if (C::FAST) {
+          P.gout[c] = p / eint + 1.0;
+          P.gout[g.N + c] = sound * sound * rho / p;
+        } else {
+          P.gout[c] = T;
+        }
       } else {
         p = (g.gm - 1.0) * eint;
         T = p / (rho * CONST_RGAS * (1.0 / g.mu));
@@ -692,8 +723,12 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
       n_calls += 1; n_iters += it; n_nonconv += (it == 100); n_clamp += clamped;
       double E, cv;
       helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
-      P.gout[c] = p / eint + 1.0;
-      P.gout[g.N + c] = sound * sound * rho / p;
+      if (C::FAST) {
+        P.gout[c] = p / eint + 1.0;
+        P.gout[g.N + c] = sound * sound * rho / p;
+      } else {
+        P.gout[c] = T;
+      }
     } else {
       p = (g.gm - 1.0) * eint;
       T = p / (rho * CONST_RGAS * (1.0 / g.mu));
@@ -800,8 +835,12 @@ __global__ void __launch_bounds__(128) k_init_thermo(Prm P) {
     helm_rhoP_newton(P.helm, rho, p, abar, zbar, T, clamped);
     helm_given_full(P.helm, rho, T, abar, zbar, Pdummy, eint, sound, cv);
     eint = rho * eint;
-    P.gout[c] = p / eint + 1.0;
-    P.gout[g.N + c] = sound * sound * rho / p;
+    if (C::FAST) {
+      P.gout[c] = p / eint + 1.0;
+      P.gout[g.N + c] = sound * sound * rho / p;
+    } else {
+      P.gout[c] = T;
+    }
   } else {
     T = p / (CONST_RGAS * rho * (1.0 / g.mu));
     eint = p * (1.0 / (g.gm - 1.0));

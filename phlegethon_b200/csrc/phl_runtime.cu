@@ -64,30 +64,33 @@ struct RunnerT : Runner {
   }
 };
 
-// Instantiated option sets: (dims, nvars, MHD, Helmholtz+FASTEOS, stratified = WB+ETOT+gravity,
-// Riemann solver).  Other combinations return PHL_E_UNSUPPORTED.
-#define PHL_RUNNER_LIST(X)                 \
-  X(2, 4, false, false, false, R_LHLLC)    \
-  X(2, 4, false, false, false, R_HLLC)     \
-  X(2, 4, false, false, true, R_LHLLC)     \
-  X(2, 4, false, false, true, R_HLLC)      \
-  X(2, 4, true, false, false, R_HLLD)      \
-  X(2, 4, true, false, false, R_LHLLD)     \
-  X(2, 6, false, true, true, R_LHLLC)      \
-  X(2, 6, true, true, true, R_LHLLD)       \
-  X(3, 5, false, false, false, R_LHLLC)    \
-  X(3, 5, false, false, false, R_HLLC)     \
-  X(3, 5, true, false, false, R_HLLD)      \
-  X(3, 5, true, false, false, R_LHLLD)     \
-  X(3, 7, false, true, true, R_LHLLC)      \
-  X(3, 7, false, true, true, R_HLLC)       \
-  X(3, 7, true, true, true, R_LHLLD)       \
-  X(3, 7, true, true, true, R_HLLD)
+// Instantiated option sets: (dims, nvars, MHD, Helmholtz, stratified = WB+ETOT+gravity, Riemann
+// solver, USE_FASTEOS).  Other combinations return PHL_E_UNSUPPORTED.
+#define PHL_RUNNER_LIST(X)                       \
+  X(2, 4, false, false, false, R_LHLLC, false)   \
+  X(2, 4, false, false, false, R_HLLC, false)    \
+  X(2, 4, false, false, true, R_LHLLC, false)    \
+  X(2, 4, false, false, true, R_HLLC, false)     \
+  X(2, 4, true, false, false, R_HLLD, false)     \
+  X(2, 4, true, false, false, R_LHLLD, false)    \
+  X(2, 6, false, true, true, R_LHLLC, true)      \
+  X(2, 6, true, true, true, R_LHLLD, true)       \
+  X(3, 5, false, false, false, R_LHLLC, false)   \
+  X(3, 5, false, false, false, R_HLLC, false)    \
+  X(3, 5, true, false, false, R_HLLD, false)     \
+  X(3, 5, true, false, false, R_LHLLD, false)    \
+  X(3, 7, false, true, true, R_LHLLC, true)      \
+  X(3, 7, false, true, true, R_HLLC, true)       \
+  X(3, 7, true, true, true, R_LHLLD, true)       \
+  X(3, 7, true, true, true, R_HLLD, true)        \
+  X(3, 7, false, true, true, R_LHLLC, false)     \
+  X(3, 7, false, true, true, R_HLLC, false)      \
+  X(3, 7, true, true, true, R_LHLLD, false)
 
-Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem) {
-#define X(D, N, M, H, S, R)                                                              \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R)           \
-    return new RunnerT<Cfg<D, N, M, H, S, S, S, R>>();
+Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast) {
+#define X(D, N, M, H, S, R, F)                                                                  \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F)) \
+    return new RunnerT<Cfg<D, N, M, H, S, S, S, R, F>>();
   PHL_RUNNER_LIST(X)
 #undef X
   return nullptr;
@@ -342,8 +345,7 @@ int check_cfg(const phl_config *c) {
   bool mhd = c->flags & PHL_MHD, helm = c->flags & PHL_HELMHOLTZ;
   if (mhd && (c->riemann != PHL_HLLD && c->riemann != PHL_LHLLD)) return PHL_E_INVALID;
   if (!mhd && (c->riemann != PHL_LHLLC && c->riemann != PHL_HLLC)) return PHL_E_INVALID;
-  if (helm && !((c->flags & PHL_FASTEOS) && (c->flags & PHL_ADVECT_YE_IABAR) && c->nas >= 2))
-    return PHL_E_UNSUPPORTED;
+  if (helm && !((c->flags & PHL_ADVECT_YE_IABAR) && c->nas >= 2)) return PHL_E_UNSUPPORTED;
   if (c->precision != PHL_FP64 && c->precision != PHL_FP32_SPLIT) return PHL_E_INVALID;
   // the step's Newton starts from the previous stage's temperature (the reference's warm start);
   // the learned guess is offered by the batch inversion entry points only
@@ -414,10 +416,11 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   bool wb = cfg->flags & PHL_WB, etot = cfg->flags & PHL_EVOLVE_ETOT, grav = cfg->flags & PHL_GRAVITY;
   if (!(wb == etot && etot == grav)) return PHL_E_UNSUPPORTED;
   c->split = cfg->precision == PHL_FP32_SPLIT;
+  const bool fast = cfg->flags & PHL_FASTEOS;
   if (c->split)
-    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+    c->runner.reset(helm && !fast ? nullptr : make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
   else
-    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast));
   if (!c->runner) return PHL_E_UNSUPPORTED;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   Geo &g = c->geo;
@@ -573,7 +576,11 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
   if ((rc = unpack_cell(f->prim, nv, nv, ctx->W[0]))) return rc;
   if (f->temp && (rc = unpack_cell(f->temp, 1, 1, ctx->temp))) return rc;
   if (f->eint && (rc = unpack_cell(f->eint, 1, 1, ctx->eint))) return rc;
-  if (helm && f->gammaf && (rc = unpack_cell(f->gammaf, 2, 2, ctx->gam[0]))) return rc;
+  const bool fast = c.flags & PHL_FASTEOS;
+  if (helm && fast && f->gammaf && (rc = unpack_cell(f->gammaf, 2, 2, ctx->gam[0]))) return rc;
+  // without USE_FASTEOS the first gamma slot carries the stage input's temperature
+  if (helm && !fast && f->temp)
+    CK(cudaMemcpyAsync(ctx->gam[0], ctx->temp, sizeof(double) * (size_t)N, cudaMemcpyDeviceToDevice, s));
   if (mhd && f->b_cc && (rc = unpack_cell(f->b_cc, sd, sd, ctx->bcc))) return rc;
   if (mhd) {
     // interior faces of b_x1(lx1-1:ux1+2, lx2-1:ux2+1, lx3-1:ux3+1), ...
@@ -719,7 +726,7 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
   if (f->prim && (rc = pack_cell(f->prim, nv, ctx->W[ctx->cur]))) return rc;
   if (f->temp && (rc = pack_cell(f->temp, 1, ctx->temp))) return rc;
   if (f->eint && (rc = pack_cell(f->eint, 1, ctx->eint))) return rc;
-  if (helm && f->gammaf && (rc = pack_cell(f->gammaf, 2, ctx->gam[ctx->cur]))) return rc;
+  if (helm && (c.flags & PHL_FASTEOS) && f->gammaf && (rc = pack_cell(f->gammaf, 2, ctx->gam[ctx->cur]))) return rc;
   if (mhd && f->b_cc && (rc = pack_cell(f->b_cc, sd, ctx->bcc))) return rc;
   if (mhd) {
     for (int d = 0; d < sd; ++d) {

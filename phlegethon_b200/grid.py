@@ -41,7 +41,9 @@ class Config:
     wb: bool = False
     gravity: bool = False
     etot: bool = False
-    helmholtz: bool = False          # HELMHOLTZ_EOS with USE_FASTEOS and ADVECT_YE_IABAR
+    helmholtz: bool = False          # HELMHOLTZ_EOS with ADVECT_YE_IABAR
+    fasteos: bool = True             # USE_FASTEOS (with helmholtz): gamma_e/gamma_c at the faces
+                                     # instead of helm_rhoP_given per Riemann side
     riemann: str = "lhllc"
     rk_stages: int = 3
     bc: list = field(default_factory=lambda: [["periodic", "periodic"]] * 3)
@@ -82,7 +84,9 @@ class Config:
         if self.etot:
             f |= FLAG_EVOLVE_ETOT
         if self.helmholtz:
-            f |= FLAG_HELMHOLTZ | FLAG_FASTEOS | FLAG_ADVECT_YE_IABAR
+            f |= FLAG_HELMHOLTZ | FLAG_ADVECT_YE_IABAR
+            if self.fasteos:
+                f |= FLAG_FASTEOS
         return f
 
     @property

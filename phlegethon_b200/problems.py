@@ -147,7 +147,7 @@ STRAT_ZBAR = 6.9
 
 
 def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, seed=12345,
-                  riemann=None, table=X2_TABLE):
+                  riemann=None, table=X2_TABLE, fasteos=True):
     """3D stratified convection box with the Helmholtz EoS.
 
     x2 is vertical (reflecting walls), x1 and x3 periodic.  rho_eq(y) falls exponentially from
@@ -155,7 +155,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     chosen so that T_eq spans ~1e8 (top) to ~3e8 K (bottom).  Abar = 13.7 and Zbar = 6.9 are
     advected as Ye and 1/Abar.  Velocities are mach * c_s * U[-1,1] per component from a
     counter-based hash (seed).  With mhd=True a uniform horizontal B_x1 of plasma beta `beta` at
-    mid-height is added and the LHLLD solver with constrained transport is used.
+    mid-height is added and the LHLLD solver with constrained transport is used.  fasteos=False
+    selects the Helmholtz path without USE_FASTEOS (helm_rhoP_given per Riemann side).
     """
     ny = n if ny is None else ny
     nz = n if nz is None else nz
@@ -169,7 +170,7 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     p_bot = float(analytic_pressure(rho_bot, 3.0e8, abar, zbar))
     g = (p_bot - p_top) / (rho_bot * Hrho * (1.0 - rho_top / rho_bot))
     cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=2, nas=2, mhd=mhd, wb=True, gravity=True, etot=True,
-                 helmholtz=True, riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
+                 helmholtz=True, fasteos=fasteos, riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
                  bc=[["periodic", "periodic"], ["reflective", "reflective"], ["periodic", "periodic"]],
                  x1l=0.0, x1u=Lx * n / ny, x2l=0.0, x2u=L, x3l=0.0, x3u=Lx * nz / ny,
                  gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8, mach_cutoff=1e-4, mach_ct=1e-6,

@@ -166,3 +166,22 @@ def test_eos_inversion_matches_oracle(gpu_lib, oracle, table):
         if Tg[i] != To or it[i] != ito:
             mism += 1
     assert mism == 0
+
+
+# ------------------------------------------------------------------------------ Helmholtz without USE_FASTEOS
+@pytest.mark.parametrize("mhd,riemann", [(False, "lhllc"), (False, "hllc"), (True, "lhlld")])
+def test_stratified_helmholtz_without_fasteos(gpu_lib, oracle, table, mhd, riemann):
+    """helm_rhoP_given on each Riemann side from the face temperature guess, bit for bit."""
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd, riemann=riemann, fasteos=False)
+    hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["newton_nonconverged"] == 0 and st["nonfinite"] == 0
+    if mhd:
+        assert div_b_max(hg) <= 1e-13
+
+
+def test_split_form_needs_fasteos(gpu_lib, table):
+    from phlegethon_b200.abi import PhlError, Simulation
+    cfg, _ = problems.stratified_3d(8, fasteos=False)
+    with pytest.raises(PhlError):
+        Simulation(cfg.replace(precision="fp32_split"), table)
