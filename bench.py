@@ -42,14 +42,14 @@ def load_peaks():
     return dict(PEAKS_FALLBACK), "fallback"
 
 
-def build_problem(name, n):
+def build_problem(name, n, fasteos=True):
     from phlegethon_b200 import helm_table, problems
     table = None
     if name == "stratified":
-        cfg, h = problems.stratified_3d(n)
+        cfg, h = problems.stratified_3d(n, fasteos=fasteos)
         table = helm_table.generate()
     elif name == "stratified_mhd":
-        cfg, h = problems.stratified_3d(n, mhd=True)
+        cfg, h = problems.stratified_3d(n, mhd=True, fasteos=fasteos)
         table = helm_table.generate()
     elif name == "hot_bubble":
         cfg, h = problems.hot_bubble_2d(n)
@@ -74,12 +74,12 @@ def stage_kernels(cfg, form):
             names = "k_face_split_mhd + k_corner_split + k_bface_split + k_c2p_mhd_split"
         else:
             per = cfg.sdims + nax + cfg.sdims + 1
-            names = "k_face_mhd + k_corner + k_bface + k_c2p_mhd"
+            names = "k_face + k_corner + k_bface + k_c2p"
         return names + " (one MHD stage)", s * per + 2
     if form == "fp32_split":
         tiled = cfg.sdims == 3 and cfg.nx1 % 32 == 0 and cfg.nx2 % 8 == 0 and cfg.nx3 % 16 == 0
         return ("k_stage_split_tiled" if tiled else "k_stage_split") + " (FP32 fluxes, FP64 state/EoS)", s + 2
-    return "k_stage (FP64)", s + 2
+    return "k_face + k_c2p (FP64)", s * (cfg.sdims + 1) + 2
 
 
 # DRAM bytes per cell of one stage-kernel launch, from ncu captures of the 128^3 stratified box
@@ -126,12 +126,13 @@ def step_bytes_per_cell(cfg):
     doubles = (nv + 1 + 3 * nv) + (s - 2) * (5 * nv) + (3 * nv + nv + 1)
     if cfg.helmholtz:
         doubles += s * (2 + 4)
+    # face fluxes (FP64, nv per face) written once and read back per direction
+    doubles += s * 2 * nv * cfg.sdims
     if cfg.mhd:
         nd = cfg.sdims
         emf = 1 if nd == 2 else 2
         doubles += s * nd * (3 + 2 * (emf + 1)) + nd
         doubles += s * nd  # b_cc write
-        doubles += s * 2 * cfg.nvars * nd  # face fluxes written once and read back per direction
     return 8 * doubles
 
 
@@ -184,7 +185,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_rate(name, steps, nthreads=0, slab=None):
+def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True):
     """Oracle (CPU restatement) zone-updates/s on a bounded slab of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
@@ -192,7 +193,7 @@ def cpu_rate(name, steps, nthreads=0, slab=None):
     if name in ("stratified", "stratified_mhd"):
         n = default_size(name)
         nz = slab or 32
-        cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"))
+        cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"), fasteos=fasteos)
         tab, dpdr = helm_table.generate()
         helm = pyoracle.Helm.for_config(cfg, tab, dpdr)
         sample = "%dx%dx%d slab of the %d^3 workload" % (cfg.nx1, cfg.nx2, cfg.nx3, n)
@@ -217,7 +218,7 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, args.steps)
-    rate, cores, sample = cpu_rate(args.config, steps)
+    rate, cores, sample = cpu_rate(args.config, steps, fasteos=not args.no_fasteos)
     cfgname = args.config
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "zone-updates/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
@@ -382,7 +383,7 @@ def run_ours(args):
 
     name = args.config
     n = args.n or default_size(name)
-    cfg, h, table = build_problem(name, n)
+    cfg, h, table = build_problem(name, n, fasteos=not args.no_fasteos)
     peaks, peak_kind = load_peaks()
     cells = cfg.n_cells
     head_form = args.form
@@ -416,7 +417,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, cores, sample = cpu_rate(name, steps=1)
+        rate, cores, sample = cpu_rate(name, steps=1, fasteos=not args.no_fasteos)
         cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -427,7 +428,8 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 fluxes / f64 state+EoS" if head_form == "fp32_split" else "f64",
                 "data": "synthetic",
-                "config": {"workload": name, "n": n, "cells": cells, "form": head_form,
+                "config": {"workload": name + ("_no_fasteos" if args.no_fasteos else ""), "n": n, "cells": cells,
+                           "form": head_form,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
                 "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
@@ -594,6 +596,8 @@ def main():
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--train-epochs", type=int, default=256, help="MLP training epochs (eos workload)")
+    ap.add_argument("--no-fasteos", action="store_true",
+                    help="Helmholtz boxes without USE_FASTEOS (helm_rhoP_given per Riemann side)")
     ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
     args = ap.parse_args()
     if args.warmup < 3:

@@ -641,4 +641,15 @@ __device__ __forceinline__ int helm_rhoP_newton(const HelmTable &h, double rho, 
   return used;
 }
 
+// helm_rhoP_given with return_sound (source.F90:24943-24980) for one Riemann side: returns
+// rho * e and the sound speed
+__device__ __forceinline__ void helm_side_eos_inl(const HelmTable &h, double rho, double p, double abar,
+                                                  double zbar, double T, double &rhoe, double &sound) {
+  int clamped = 0;
+  helm_rhoP_newton(h, rho, p, abar, zbar, T, clamped);
+  double Pd, E, cv;
+  helm_given_full(h, rho, T, abar, zbar, Pd, E, sound, cv);
+  rhoe = E * rho;
+}
+
 }  // namespace phl

@@ -255,12 +255,7 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
     for (int side = 0; side < 2; ++side) {
       const double *q = qs[side];
       const double ye = q[C::IAS], abar = 1.0 / q[C::IAS + 1], zbar = ye * abar;
-      double T = tface, Pd, E, snd, cv;
-      int clamped = 0;
-      helm_rhoP_newton(P.helm, q[0], q[IP], abar, zbar, T, clamped);
-      helm_given_full(P.helm, q[0], T, abar, zbar, Pd, E, snd, cv);
-      gs[side][0] = E * q[0];
-      gs[side][1] = snd;
+      helm_side_eos_inl(P.helm, q[0], q[IP], abar, zbar, tface, gs[side][0], gs[side][1]);
     }
   }
   const double gm = P.g.gm, mc = P.g.mach_cutoff;
@@ -300,177 +295,13 @@ __device__ __forceinline__ void store_face_emf(const Prm &P, int d, long long fi
   P.sgnf[d][fidx] = sgn;
 }
 
-// --------------------------------------------------------------------- stage kernel
-// One thread per cell: both faces in every direction, flux divergence, gravity source, RK
-// combine; for hydro also cons->prim + EoS and (last stage) the CFL max.  For MHD the kernel
-// stops after the RK combine of U and stores face EMFs; ct/face-B/cons->prim follow.
+// --------------------------------------------------------------------- face fluxes
+// One thread per face of direction d: the face flux of the x1/x2/x3 sweeps (source.F90:8138-9105,
+// 9107-10301, 10303-11364), stored in P.dflux[d] for the divergence of k_c2p; for MHD also the
+// face EMF and CT sign.  Each face is solved once; with --fmad=false the result equals what a
+// per-cell loop over both faces of every cell computes.
 template <class C>
-__global__ void __launch_bounds__(128) k_stage(Prm P) {
-  if (!*P.active) return;
-  constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
-  const Geo &g = P.g;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = c < g.N;
-  double smax_loc = 0.0;
-  unsigned long long n_calls = 0, n_iters = 0, n_nonconv = 0, n_clamp = 0, n_bad = 0;
-  if (valid) {
-    const int i = (int)(c % g.nx[0]);
-    const int j = (int)((c / g.nx[0]) % g.nx[1]);
-    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
-    const double dt = P.scal[1];
-    const double smax_prev = P.scal[2];
-    double res[NV];
-    double wc[NV];
-    load_wdev<C>(P, i, j, k, wc);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      // cells c-2..c+2 along d
-      double w[5][NV], gmv[5][2], bc[5][3];
-#pragma unroll
-      for (int s = 0; s < 5; ++s) {
-        int ii = i + (d == 0 ? s - 2 : 0), jj = j + (d == 1 ? s - 2 : 0), kk = k + (d == 2 ? s - 2 : 0);
-        load_wdev<C>(P, ii, jj, kk, w[s]);
-        if (C::HELM) load_gdev<C>(P, ii, jj, kk, gmv[s]);
-        if (C::MHD) load_bcc<C>(P, ii, jj, kk, bc[s]);
-      }
-      double Flo[NV], Fhi[NV], Fb[3], rs;
-      face_flux<C>(P, d, i, j, k, w[0], w[1], w[2], w[3], gmv[0], gmv[1], gmv[2], gmv[3], bc[0], bc[1],
-                   bc[2], bc[3], Flo, Fb, rs);
-      if (C::MHD) store_face_emf<C>(P, d, face_lin(g, d, i, j, k), Fb, Flo[0], rs, smax_prev);
-      int hi_i = i + (d == 0), hi_j = j + (d == 1), hi_k = k + (d == 2);
-      face_flux<C>(P, d, hi_i, hi_j, hi_k, w[1], w[2], w[3], w[4], gmv[1], gmv[2], gmv[3], gmv[4], bc[1],
-                   bc[2], bc[3], bc[4], Fhi, Fb, rs);
-      if (C::MHD) {
-        int hc = d == 0 ? i : (d == 1 ? j : k);
-        if (hc == g.nx[d] - 1) store_face_emf<C>(P, d, face_lin(g, d, hi_i, hi_j, hi_k), Fb, Fhi[0], rs, smax_prev);
-      }
-      const double inv_dl = g.inv_dx[d];
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) {
-        double dd = (Fhi[iv] - Flo[iv]) * inv_dl;
-        res[iv] = d == 0 ? dd : res[iv] + dd;
-      }
-    }
-    if (C::GRAV) {
-      long long b = bg_cc(g, i, j, k);
-      double rho = wc[0];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) res[1 + d] = res[1 + d] - rho * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + b);
-    }
-    // state0 / state
-    double u0[NV], u[NV];
-    if (P.first_stage) {
-      double w[NV];
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) w[iv] = P.Win[(long long)iv * g.N + c];
-      double rho = w[0], vx1 = w[1], vx2 = w[2], vx3 = DIM == 3 ? w[3] : 0.0;
-      u0[0] = rho;
-      u0[1] = rho * vx1;
-      u0[2] = rho * vx2;
-      if (DIM == 3) u0[3] = rho * vx3;
-      double eint = P.eint[c];
-      double rhoe = eint + 0.5 * rho * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
-      if (C::MHD) {
-        double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
-        rhoe = rhoe + 0.5 * (b0 * b0 + b1 * b1 + b2 * b2);
-      }
-      if (C::ETOT) rhoe = rhoe + rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
-      u0[IP] = rhoe;
-#pragma unroll
-      for (int iv = IAS; iv < NV; ++iv) u0[iv] = rho * w[iv];
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) { u[iv] = u0[iv]; P.U0[(long long)iv * g.N + c] = u0[iv]; }
-    } else {
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) {
-        u0[iv] = P.U0[(long long)iv * g.N + c];
-        u[iv] = P.U[(long long)iv * g.N + c];
-      }
-    }
-    const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-      u[iv] = a1 * u0[iv] + a2 * u[iv] + a3 * res[iv];
-      P.U[(long long)iv * g.N + c] = u[iv];
-    }
-    if (!C::MHD) {
-      // cons -> prim + EoS (source.F90:13533-13686)
-      double rho = u[0], rhovx1 = u[1], rhovx2 = u[2], rhovx3 = DIM == 3 ? u[3] : 0.0, rhoe = u[IP];
-      double inv_rho = 1.0 / rho;
-      double eint = rhoe - 0.5 * (rhovx1 * rhovx1 + rhovx2 * rhovx2 + rhovx3 * rhovx3) * inv_rho;
-      if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
-      double wn[NV];
-      wn[0] = rho;
-      wn[1] = rhovx1 * inv_rho;
-      wn[2] = rhovx2 * inv_rho;
-      if (DIM == 3) wn[3] = rhovx3 * inv_rho;
-      double p, T, sound = 0.0;
-      if (C::HELM) {
-        double ye = u[IAS] * inv_rho;
-        double abar = rho / u[IAS + 1];
-        double zbar = ye * abar;
-        T = P.temp[c];
-        int clamped = 0;
-        int it = helm_rhoe_newton(P.helm, rho, eint * inv_rho, abar, zbar, T, 100, clamped);
-        n_calls += 1; n_iters += it; n_nonconv += (it == 100); n_clamp += clamped;
-        double E, cv;
-        helm_given_full(P.helm, rho, T, abar, zbar, p, E, sound, cv);
-        if (C::FAST) {
-          P.gout[c] = p / eint + 1.0;
-          P.gout[g.N + c] = sound * sound * rho / p;
-        } else {
-          P.gout[c] = T;
-        }
-      } else {
-        p = (g.gm - 1.0) * eint;
-        T = p / (rho * CONST_RGAS * (1.0 / g.mu));
-      }
-      wn[IP] = p;
-#pragma unroll
-      for (int iv = IAS; iv < NV; ++iv) wn[iv] = u[iv] * inv_rho;
-#pragma unroll
-      for (int iv = 0; iv < NV; ++iv) P.Wout[(long long)iv * g.N + c] = wn[iv];
-      P.temp[c] = T;
-      P.eint[c] = eint;
-      if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) n_bad += 1;
-      if (P.last_stage) {
-        // compute_hyperbolic_dt on the new state (source.F90:13707-13960)
-        double cs;
-        if (C::HELM) {
-          double ye = wn[IAS], abar = 1.0 / wn[IAS + 1], zbar = ye * abar, pp, ei, cv;
-          helm_given_full(P.helm, rho, T, abar, zbar, pp, ei, cs, cv);
-        } else {
-          cs = sqrt(g.gm * p / rho);
-        }
-        double sx1 = (fabs(wn[1]) + cs) * g.inv_dx[0];
-        double sx2 = (fabs(wn[2]) + cs) * g.inv_dx[1];
-        if (DIM == 3) {
-          double sx3 = (fabs(wn[3]) + cs) * g.inv_dx[2];
-          smax_loc = sx3 + sx1 + sx2;
-        } else {
-          smax_loc = sx1 + sx2;
-        }
-      }
-    }
-  }
-  if (!C::MHD) {
-    if (P.last_stage) block_max_atomic(smax_loc, P.smax_bits);
-    if (C::HELM) {
-      block_sum_atomic(n_calls, P.stat + STAT_NEWTON_CALLS);
-      block_sum_atomic(n_iters, P.stat + STAT_NEWTON_ITERS);
-      block_sum_atomic(n_nonconv, P.stat + STAT_NEWTON_NONCONV);
-      block_sum_atomic(n_clamp, P.stat + STAT_NEWTON_CLAMP);
-    }
-    block_sum_atomic(n_bad, P.stat + STAT_NONFINITE);
-  }
-}
-
-// --------------------------------------------------------------------- MHD: face fluxes
-// One thread per face of direction d: the face flux of the x1/x2/x3 sweeps (same inputs and
-// operations as the per-cell k_stage, which solves every face twice), stored in P.dflux[d],
-// plus the face EMF and CT sign
-template <class C>
-__global__ void __launch_bounds__(128) k_face_mhd(Prm P, int d) {
+__global__ void __launch_bounds__(128) k_face(Prm P, int d) {
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -479,20 +310,20 @@ __global__ void __launch_bounds__(128) k_face_mhd(Prm P, int d) {
   if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
   const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
-  double w[4][NV], gmv[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, bc[4][3];
+  double w[4][NV], gmv[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, bc[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     const int ii = fi + (d == 0 ? s - 2 : 0), jj = fj + (d == 1 ? s - 2 : 0), kk = fk + (d == 2 ? s - 2 : 0);
     load_wdev<C>(P, ii, jj, kk, w[s]);
     if (C::HELM) load_gdev<C>(P, ii, jj, kk, gmv[s]);
-    load_bcc<C>(P, ii, jj, kk, bc[s]);
+    if (C::MHD) load_bcc<C>(P, ii, jj, kk, bc[s]);
   }
   double F[NV], Fb[3], rs;
   face_flux<C>(P, d, fi, fj, fk, w[0], w[1], w[2], w[3], gmv[0], gmv[1], gmv[2], gmv[3], bc[0], bc[1], bc[2], bc[3],
                F, Fb, rs);
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.dflux[d][(long long)iv * nf + f] = F[iv];
-  store_face_emf<C>(P, d, f, Fb, F[0], rs, P.scal[2]);
+  if (C::MHD) store_face_emf<C>(P, d, f, Fb, F[0], rs, P.scal[2]);
 }
 
 // --------------------------------------------------------------------- MHD: corner EMFs
@@ -621,11 +452,11 @@ __global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
   P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
 }
 
-// MHD stage end: flux divergence of the face fluxes, gravity and the RK combine of U
+// Stage end: flux divergence of the face fluxes, gravity and the RK combine of U
 // (source.F90:9057-9102, 12606-12644, 13518-13531), b_cc from the updated faces, then
 // cons->prim with the EoS (source.F90:12439-12487, 13533-13686), last stage also the CFL max
 template <class C>
-__global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
+__global__ void __launch_bounds__(128) k_c2p(Prm P) {
   if (!*P.active) return;
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
@@ -637,12 +468,14 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
     const int j = (int)((c / g.nx[0]) % g.nx[1]);
     const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
     double bcc[3] = {0, 0, 0};
+    if (C::MHD) {
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
-      bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+      for (int d = 0; d < DIM; ++d) {
+        int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
+        bcc[d] = 0.5 * (P.bf[d][face_lin(g, d, ui, uj, uk)] + P.bf[d][face_lin(g, d, i, j, k)]);
+      }
     }
-    // flux divergence of the face fluxes, gravity and the RK combine, in the order of k_stage
+    // flux divergence of the face fluxes (directions in order), gravity and the RK combine
     double res[NV];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -673,7 +506,7 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
       u0[2] = rho0 * vx2;
       if (DIM == 3) u0[3] = rho0 * vx3;
       double rhoe0 = P.eint[c] + 0.5 * rho0 * (vx1 * vx1 + vx2 * vx2 + vx3 * vx3);
-      {
+      if (C::MHD) {
         // magnetic energy of the stage input (b_cc before this stage's face update)
         double b0 = P.bcc_in[c], b1 = P.bcc_in[g.N + c], b2 = DIM == 3 ? P.bcc_in[2 * g.N + c] : 0.0;
         rhoe0 = rhoe0 + 0.5 * (b0 * b0 + b1 * b1 + b2 * b2);
@@ -700,12 +533,13 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
       }
     }
     // the stage input's b_cc has been read: store the new one
+    if (C::MHD)
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) P.bcc_out[(long long)d * g.N + c] = bcc[d];
+      for (int d = 0; d < DIM; ++d) P.bcc_out[(long long)d * g.N + c] = bcc[d];
     double rho = u[0], rhovx1 = u[1], rhovx2 = u[2], rhovx3 = DIM == 3 ? u[3] : 0.0, rhoe = u[IP];
     double inv_rho = 1.0 / rho;
     double eint = rhoe - 0.5 * (rhovx1 * rhovx1 + rhovx2 * rhovx2 + rhovx3 * rhovx3) * inv_rho;
-    eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
+    if (C::MHD) eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
     if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bg_cc(g, i, j, k));
     double wn[NV];
     wn[0] = rho;
@@ -749,8 +583,10 @@ __global__ void __launch_bounds__(128) k_c2p_mhd(Prm P) {
       } else {
         cs = sqrt(g.gm * p / rho);
       }
-      double ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
-      cs = sqrt(cs * cs + ca2 / rho);
+      if (C::MHD) {
+        double ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
+        cs = sqrt(cs * cs + ca2 / rho);
+      }
       double sx1 = (fabs(wn[1]) + cs) * g.inv_dx[0];
       double sx2 = (fabs(wn[2]) + cs) * g.inv_dx[1];
       if (DIM == 3) {

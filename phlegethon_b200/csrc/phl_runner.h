@@ -20,8 +20,7 @@ struct Runner {
   virtual void split_to_prim(const Prm &, cudaStream_t) {}
 };
 
-// factory of the FP32 split-precision runners (phl_split.cu; Helmholtz with USE_FASTEOS only);
-// nullptr when not built
-Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem);
+// factory of the FP32 split-precision runners (phl_split.cu); nullptr when not built
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast);
 
 }  // namespace phl

@@ -40,11 +40,9 @@ template <class C>
 struct RunnerT : Runner {
   void stage(const Prm &P, cudaStream_t s) override {
     const Geo &g = P.g;
-    if constexpr (!C::MHD) {
-      k_stage<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
-    } else {
-      // each face once, then corners, face B and (divergence + RK + cons->prim) per cell
-      for (int d = 0; d < C::DIM; ++d) k_face_mhd<C><<<nblk(nfaces_host(g, d), 128), 128, 0, s>>>(P, d);
+    // each face once, then (MHD) corners and face B, then divergence + RK + cons->prim per cell
+    for (int d = 0; d < C::DIM; ++d) k_face<C><<<nblk(nfaces_host(g, d), 128), 128, 0, s>>>(P, d);
+    if constexpr (C::MHD) {
       for (int a = 0; a < 3; ++a) {
         if (C::DIM == 2 && a != 2) continue;
         long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) *
@@ -52,8 +50,8 @@ struct RunnerT : Runner {
         k_corner<C><<<nblk(n, 256), 256, 0, s>>>(P, a);
       }
       for (int d = 0; d < C::DIM; ++d) k_bface<C><<<nblk(nfaces_host(g, d), 256), 256, 0, s>>>(P, d);
-      k_c2p_mhd<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
     }
+    k_c2p<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
   }
   void dt(const Prm &P, cudaStream_t s) override { k_dt<C><<<nblk(P.g.N, 256), 256, 0, s>>>(P); }
   void init_thermo(const Prm &P, cudaStream_t s) override {
@@ -418,7 +416,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   c->split = cfg->precision == PHL_FP32_SPLIT;
   const bool fast = cfg->flags & PHL_FASTEOS;
   if (c->split)
-    c->runner.reset(helm && !fast ? nullptr : make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann));
+    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast));
   else
     c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast));
   if (!c->runner) return PHL_E_UNSUPPORTED;
@@ -469,9 +467,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
       if (cfg->sdims == 2 && a != 2) continue;
       if ((rc = c->alloc(&c->cor[a], (size_t)c->ncor(a)))) return rc;
     }
-    if (!c->split)
-      for (int d = 0; d < cfg->sdims; ++d)
-        if ((rc = c->alloc(&c->dflux[d], (size_t)nv * c->nfaces(d)))) return rc;
+
     if (c->split) {
       if ((rc = c->alloc(&c->bccf, (size_t)3 * N))) return rc;
       for (int d = 0; d < cfg->sdims; ++d) {
@@ -486,6 +482,9 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
       }
     }
   }
+  if (!c->split)
+    for (int d = 0; d < cfg->sdims; ++d)
+      if ((rc = c->alloc(&c->dflux[d], (size_t)nv * c->nfaces(d)))) return rc;
   if ((rc = c->alloc(&c->scal, 8))) return rc;
   if ((rc = c->alloc(&c->smax_bits, 1))) return rc;
   if ((rc = c->alloc(&c->active, 1))) return rc;

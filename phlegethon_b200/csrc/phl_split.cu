@@ -35,7 +35,7 @@ __device__ __forceinline__ void plm_f32(float qm, float qc, float qp, float &lo,
 // qL/qR: [rho (full), v1, v2, (v3), p' (deviation), scalars...] in the normal frame, pe the face
 // equilibrium pressure.  Returns the flux with the momentum flux already reduced by pe (the
 // reference's WB fix).  Same solver as riemann_hydro (source.F90:15681-16252).
-template <int DIM, int NV, bool FAST, int RIEM>
+template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float *qR, const float *gL,
                                                     const float *gR, float pe, float gm, float mach_cutoff,
                                                     float *flux) {
@@ -44,13 +44,15 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
   float v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
   float pLd = qL[IP], pL = pe + pLd, eint, cL, cR;
-  if (FAST) { eint = pL / (gL[0] - 1.0f); cL = sqrtf(gL[1] * pL * inv_rhoL); }
+  if (EOSM == EOS_FAST) { eint = pL / (gL[0] - 1.0f); cL = sqrtf(gL[1] * pL * inv_rhoL); }
+  else if (EOSM == EOS_GIVEN) { eint = gL[0]; cL = gL[1]; }
   else { eint = igmm1 * pL; cL = sqrtf(gm * pL * inv_rhoL); }
   float rhoeL = eint + 0.5f * rhoL * v2L;
   float rhoR = qR[0], inv_rhoR = 1.0f / rhoR, vx1R = qR[1], vx2R = qR[2], vx3R = DIM == 3 ? qR[3] : 0.0f;
   float v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
   float pRd = qR[IP], pR = pe + pRd;
-  if (FAST) { eint = pR / (gR[0] - 1.0f); cR = sqrtf(gR[1] * pR * inv_rhoR); }
+  if (EOSM == EOS_FAST) { eint = pR / (gR[0] - 1.0f); cR = sqrtf(gR[1] * pR * inv_rhoR); }
+  else if (EOSM == EOS_GIVEN) { eint = gR[0]; cR = gR[1]; }
   else { eint = igmm1 * pR; cR = sqrtf(gm * pR * inv_rhoR); }
   float rhoeR = eint + 0.5f * rhoR * v2R;
   float max_c = fmaxf(cL, cR);
@@ -116,7 +118,7 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
 // (pT' = p' + B^2/2), the star pressure as pe + pT*' with the weights of the reference, and the
 // normal momentum flux is returned with pe removed (the reference's WB fix).  fluxb is the
 // induction flux (0, v1 B2 - B1 v2, v1 B3 - B1 v3).
-template <int DIM, int NV, bool FAST, int RIEM>
+template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *qR, const float *bL,
                                                   const float *bR, const float *gL, const float *gR, float pe,
                                                   float gm, float mach_cutoff, float *flux, float *fluxb) {
@@ -125,14 +127,16 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
   float v2L = vx1L * vx1L + vx2L * vx2L + vx3L * vx3L;
   float pLd = qL[IP], pL = pe + pLd, eint, c2L, c2R;
-  if (FAST) { eint = pL / (gL[0] - 1.0f); c2L = gL[1] * pL * inv_rhoL; }
+  if (EOSM == EOS_FAST) { eint = pL / (gL[0] - 1.0f); c2L = gL[1] * pL * inv_rhoL; }
+  else if (EOSM == EOS_GIVEN) { eint = gL[0]; c2L = gL[1] * gL[1]; }
   else { eint = pL * igmm1; c2L = gm * pL * inv_rhoL; }
   float rhoeL = eint + 0.5f * rhoL * v2L;
   float bx1L = bL[0], bx2L = bL[1], bx3L = DIM == 3 ? bL[2] : 0.0f;
   float rhoR = qR[0], inv_rhoR = 1.0f / rhoR, vx1R = qR[1], vx2R = qR[2], vx3R = DIM == 3 ? qR[3] : 0.0f;
   float v2R = vx1R * vx1R + vx2R * vx2R + vx3R * vx3R;
   float pRd = qR[IP], pR = pe + pRd;
-  if (FAST) { eint = pR / (gR[0] - 1.0f); c2R = gR[1] * pR * inv_rhoR; }
+  if (EOSM == EOS_FAST) { eint = pR / (gR[0] - 1.0f); c2R = gR[1] * pR * inv_rhoR; }
+  else if (EOSM == EOS_GIVEN) { eint = gR[0]; c2R = gR[1] * gR[1]; }
   else { eint = pR * igmm1; c2R = gm * pR * inv_rhoR; }
   float rhoeR = eint + 0.5f * rhoR * v2R;
   float bx1R = bR[0], bx2R = bR[1], bx3R = DIM == 3 ? bR[2] : 0.0f;
@@ -331,6 +335,26 @@ struct SmemCells {
   __device__ __forceinline__ float g(int s, int q) const { return base[off[s] + (NV + q) * vs]; }
 };
 
+// helm_side_eos_inl out of line: the split stage kernels call it twice per face, and an inlined
+// full Helmholtz evaluation at each site costs them their registers
+static __device__ __noinline__ void helm_side_eos(const HelmTable &h, double rho, double p, double abar,
+                                                  double zbar, double T, double &rhoe, double &sound) {
+  helm_side_eos_inl(h, rho, p, abar, zbar, T, rhoe, sound);
+}
+
+// Helmholtz without USE_FASTEOS, split form: helm_rhoP_given (FP64) for one side of a face from
+// the scaled FP32 face state and temperature guess; returns rho*e and the sound speed, scaled
+template <class C>
+__device__ __forceinline__ void split_side_eos(const Prm &P, const float *q, float pe, float tguess, float &rhoe_s,
+                                               float &c_s) {
+  const double rho = (double)q[0] * P.rho_ref, p = ((double)pe + (double)q[C::IP]) * P.p_ref;
+  const double ye = q[C::IAS], abar = 1.0 / (double)q[C::IAS + 1], zbar = ye * abar;
+  double rhoe, snd;
+  helm_side_eos(P.helm, rho, p, abar, zbar, (double)tguess, rhoe, snd);
+  rhoe_s = (float)(rhoe * P.inv_p_ref);
+  c_s = (float)(snd * P.inv_v_ref);
+}
+
 // flux through the low face of cell m along d from the FP32 deviation states of cells m-2..m+1
 template <class C, class Cells>
 __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int fj, int fk, const Cells &cl,
@@ -363,7 +387,7 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     pe = __ldg(P.sf_p_f[d] + fb);
   }
   float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
-  if (C::HELM) {
+  if (C::FAST) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
       const float g0 = cl.g(0, iv), g1 = cl.g(1, iv), g2 = cl.g(2, iv), g3 = cl.g(3, iv);
@@ -377,8 +401,13 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
     }
+  } else if (C::HELM) {
+    // without USE_FASTEOS the first gamma slot holds the stage input's temperature
+    const float tface = 0.5f * (cl.g(1, 0) + cl.g(2, 0));
+    split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
+    split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
-  riemann_hydro_split<C::DIM, NV, C::HELM, C::RIEM>(qL, qR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F);
+  riemann_hydro_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F);
   if (d == 1) {
     float a = F[1], b = F[2]; F[1] = -b; F[2] = a;
   } else if (C::DIM == 3 && d == 2) {
@@ -470,10 +499,14 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
     int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
     st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
     helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
-    double ge = p / eint + 1.0, gc = sound * sound * rho / p;
-    if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
-    P.gf_out[c] = (float)ge;
-    P.gf_out[g.N + c] = (float)gc;
+    if (C::FAST) {
+      double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+      if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
+      P.gf_out[c] = (float)ge;
+      P.gf_out[g.N + c] = (float)gc;
+    } else {
+      P.gf_out[c] = (float)T;
+    }
   } else {
     p = (g.gm - 1.0) * eint;
     T = p / (rho * CONST_RGAS * (1.0 / g.mu));
@@ -624,7 +657,7 @@ struct SplitMaps {
 constexpr int SPLIT_TMA_POLLS = 1 << 22;  // mbarrier polls before a stalled copy is reported
 
 template <class C, int TX, int TY, int KZ>
-__global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P, const __grid_constant__ SplitMaps maps,
+__global__ void __launch_bounds__(TX * TY, C::FAST || !C::HELM ? 2 : 1) k_stage_split_tiled(Prm P, const __grid_constant__ SplitMaps maps,
                                                                   int use_tma) {
   if (!*P.active) return;
   using T = SplitTile<C, TX, TY>;
@@ -838,7 +871,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     pe = __ldg(P.sf_p_f[d] + fb);
   }
   float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
-  if (C::HELM) {
+  if (C::FAST) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
       plm_f32(gm[0][iv], gm[1][iv], gm[2][iv], lo, hi);
@@ -851,8 +884,12 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
     }
+  } else if (C::HELM) {
+    const float tface = 0.5f * (gm[1][0] + gm[2][0]);
+    split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
+    split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
-  riemann_mhd_split<C::DIM, NV, C::HELM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
+  riemann_mhd_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
                                                    Fb);
   if (d == 1) {
     float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
@@ -1121,10 +1158,14 @@ __global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
       int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
       st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
       helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
-      double ge = p / eint + 1.0, gc = sound * sound * rho / p;
-      if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
-      P.gf_out[c] = (float)ge;
-      P.gf_out[g.N + c] = (float)gc;
+      if (C::FAST) {
+        double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+        if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
+        P.gf_out[c] = (float)ge;
+        P.gf_out[g.N + c] = (float)gc;
+      } else {
+        P.gf_out[c] = (float)T;
+      }
     } else {
       p = (g.gm - 1.0) * eint;
       T = p / (rho * CONST_RGAS * (1.0 / g.mu));
@@ -1200,11 +1241,13 @@ __global__ void k_split_from_prim(Prm P) {
   P.Wf_out[(long long)IP * g.N + c] = (float)(pdev / P.p_ref);
 #pragma unroll
   for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)w[iv];
-  if (C::HELM) {
+  if (C::FAST) {
     double ge = P.gin[c];
     if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
     P.gf_out[c] = (float)ge;
     P.gf_out[g.N + c] = (float)P.gin[g.N + c];
+  } else if (C::HELM) {
+    P.gf_out[c] = (float)P.temp[c];
   }
 }
 
@@ -1228,8 +1271,12 @@ __global__ void k_split_to_prim(Prm P) {
   if (C::HELM) {
     double ye = u[IAS] * inv_rho, abar = rho / u[IAS + 1], zbar = ye * abar, E, s, cv;
     helm_given_full(P.helm, rho, P.temp[c], abar, zbar, p, E, s, cv);
-    P.gout[c] = p / eint + 1.0;
-    P.gout[g.N + c] = s * s * rho / p;
+    if (C::FAST) {
+      P.gout[c] = p / eint + 1.0;
+      P.gout[g.N + c] = s * s * rho / p;
+    } else {
+      P.gout[c] = P.temp[c];
+    }
   } else {
     p = (g.gm - 1.0) * eint;
   }
@@ -1371,26 +1418,29 @@ struct SplitRunnerT : Runner {
   }
 };
 
-#define PHL_SPLIT_LIST(X)                 \
-  X(2, 4, true, false, false, R_HLLD)     \
-  X(2, 4, true, false, false, R_LHLLD)    \
-  X(3, 5, true, false, false, R_HLLD)     \
-  X(3, 5, true, false, false, R_LHLLD)    \
-  X(3, 7, true, true, true, R_LHLLD)      \
-  X(3, 7, true, true, true, R_HLLD)       \
-  X(2, 4, false, false, false, R_LHLLC)   \
-  X(2, 4, false, false, false, R_HLLC)    \
-  X(2, 4, false, false, true, R_LHLLC)    \
-  X(2, 6, false, true, true, R_LHLLC)     \
-  X(3, 5, false, false, false, R_LHLLC)   \
-  X(3, 5, false, false, false, R_HLLC)    \
-  X(3, 7, false, true, true, R_LHLLC)     \
-  X(3, 7, false, true, true, R_HLLC)
+#define PHL_SPLIT_LIST(X)                       \
+  X(2, 4, true, false, false, R_HLLD, false)     \
+  X(2, 4, true, false, false, R_LHLLD, false)    \
+  X(3, 5, true, false, false, R_HLLD, false)     \
+  X(3, 5, true, false, false, R_LHLLD, false)    \
+  X(3, 7, true, true, true, R_LHLLD, true)       \
+  X(3, 7, true, true, true, R_HLLD, true)        \
+  X(3, 7, true, true, true, R_LHLLD, false)      \
+  X(2, 4, false, false, false, R_LHLLC, false)   \
+  X(2, 4, false, false, false, R_HLLC, false)    \
+  X(2, 4, false, false, true, R_LHLLC, false)    \
+  X(2, 6, false, true, true, R_LHLLC, true)      \
+  X(3, 5, false, false, false, R_LHLLC, false)   \
+  X(3, 5, false, false, false, R_HLLC, false)    \
+  X(3, 7, false, true, true, R_LHLLC, true)      \
+  X(3, 7, false, true, true, R_HLLC, true)       \
+  X(3, 7, false, true, true, R_LHLLC, false)     \
+  X(3, 7, false, true, true, R_HLLC, false)
 
-Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem) {
-#define X(D, N, M, H, S, R)                                                              \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R)           \
-    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R>>();
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast) {
+#define X(D, N, M, H, S, R, F)                                                                  \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F)) \
+    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R, F>>();
   PHL_SPLIT_LIST(X)
 #undef X
   return nullptr;

@@ -73,7 +73,7 @@ def test_bench_algorithmic_bytes():
     spec.loader.exec_module(bench)
     from phlegethon_b200 import problems
     cfg, _ = problems.stratified_3d(8)
-    assert bench.step_bytes_per_cell(cfg.replace(precision="fp64")) == 888
+    assert bench.step_bytes_per_cell(cfg.replace(precision="fp64")) == 888 + 8 * 3 * 2 * 7 * 3
     assert bench.step_bytes_per_cell(cfg.replace(precision="fp32_split")) == 776
     cfgm, _ = problems.stratified_3d(8, mhd=True)
     assert bench.step_bytes_per_cell(cfgm.replace(precision="fp32_split")) == 2072

@@ -179,9 +179,3 @@ def test_stratified_helmholtz_without_fasteos(gpu_lib, oracle, table, mhd, riema
     if mhd:
         assert div_b_max(hg) <= 1e-13
 
-
-def test_split_form_needs_fasteos(gpu_lib, table):
-    from phlegethon_b200.abi import PhlError, Simulation
-    cfg, _ = problems.stratified_3d(8, fasteos=False)
-    with pytest.raises(PhlError):
-        Simulation(cfg.replace(precision="fp32_split"), table)

@@ -135,3 +135,19 @@ def test_split_stratified_helmholtz_mhd(gpu_lib, table, riemann):
     for f in ("b1", "b2", "b3"):
         assert err[f] <= lim["b"], (f, err)
     assert div_b_max(h32) <= 1e-13
+
+
+@pytest.mark.parametrize("mhd,riemann", [(False, "lhllc"), (True, "lhlld")])
+def test_split_helmholtz_without_fasteos(gpu_lib, table, mhd, riemann):
+    """Split form of the Helmholtz path without FASTEOS: helm_rhoP_given (FP64) per Riemann side
+    from the FP32 face state, tiled and per-cell grids."""
+    for n, ny, nz in ((16, 24, 12), (32, 16, 16)):
+        cfg, h = problems.stratified_3d(n, ny=ny, nz=nz, mhd=mhd, riemann=riemann, fasteos=False)
+        h64, _ = run_form(cfg, h, 20, table, "fp64")
+        h32, st = run_form(cfg, h, 20, table, "fp32_split")
+        err = field_errors(h32, h64)
+        assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+        for f in ("rho", "p", "e", "T"):
+            assert err[f] <= 1e-8, (f, err)
+        for f in ("v1", "v2", "v3"):
+            assert err[f] <= 1e-5, (f, err)
