@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PHL_ABI_VERSION 1
+#define PHL_ABI_VERSION 2
 
 /* return codes */
 #define PHL_OK 0
@@ -61,6 +61,9 @@ extern "C" {
 #define PHL_FP32_SPLIT 1  /* FP32 reconstruction/Riemann/EMF on WB deviations, FP64 state + EoS */
 
 /* initial temperature guess for the (rho, e) -> T Newton inversion */
+#define PHL_REC_LIM2ND 0  /* LIM2ND_REC: van Leer PLM (source.F90:8141-8181) */
+#define PHL_REC_PPH 1     /* PPH_REC: third order, scalars limited (source.F90:8183-8259) */
+#define PHL_REC_LIM5TH 2  /* LIM5TH_REC: limited fifth order (source.F90:8261-8323) */
 #define PHL_GUESS_WARM 0  /* previous-stage temperature, as the reference (source.F90:13649) */
 #define PHL_GUESS_MLP 1   /* learned 4-64-64-1 guess, judged by <=3 Newton steps, else the
                                      warm guess (hydro step) or the bracket guess (EoS batch) */
@@ -85,6 +88,8 @@ typedef struct phl_config {
   double cfl, mach_cutoff, mach_ct;/* cfl_make, Mach_cutoff_make, Mach_ct_make */
   int helm_nT, helm_nrho;          /* helm_nT_make, helm_nrho_make */
   double helm_ltlo, helm_lthi, helm_ldlo, helm_ldhi;
+  int reconstruction;              /* PHL_REC_LIM2ND (LIM2ND_REC), PHL_REC_PPH, PHL_REC_LIM5TH
+                                      (ngc >= 3) */
 } phl_config;
 
 /* Host arrays, laid out exactly as the locgrid members of the same name

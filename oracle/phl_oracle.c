@@ -459,17 +459,54 @@ static void fill_ghosts(const phlo_grid *g, double *a, int nv, int vec_kind) {
 }
 
 /* ---------------------------------------------------------------- helpers */
-static void plm(const double *qm, const double *qc, const double *qp, int n, double *lo, double *hi) {
-  /* LIM2ND_REC (source.F90:8141-8181): slope = df*db/(df+db) if df*db>0, faces qc -/+ slope/2 */
-  for (int iv = 0; iv < n; ++iv) {
-    double slopef = qp[iv] - qc[iv], slopeb = qc[iv] - qm[iv];
-    double prod = slopef * slopeb, slope = 0.0;
+/* Face values (lo = left edge, hi = right edge) of the centre cell qc from its neighbours, by the
+ * reference's reconstructions: LIM2ND_REC (source.F90:8141-8181), PPH_REC (8183-8259: third
+ * order, limited only when `limited`), LIM5TH_REC (8261-8323: fifth order, always limited). */
+static void rec_cell(int rec, int limited, double qmm, double qm, double qc, double qp, double qpp,
+                     double *lo, double *hi) {
+  if (rec == 0) {
+    double slopef = qp - qc, slopeb = qc - qm, prod = slopef * slopeb, slope = 0.0;
     if (prod > 0.0) slope = prod / (slopef + slopeb);
     double tmp = 0.5 * slope;
-    lo[iv] = qc[iv] - tmp;
-    hi[iv] = qc[iv] + tmp;
+    *lo = qc - tmp;
+    *hi = qc + tmp;
+    return;
   }
+  double am, ap;
+  if (rec == 1) {
+    double tmp = (5.0 / 6.0) * qc;
+    am = (1.0 / 3.0) * qm + tmp - (1.0 / 6.0) * qp;
+    ap = -(1.0 / 6.0) * qm + tmp + (1.0 / 3.0) * qp;
+    if (!limited) {
+      *lo = am;
+      *hi = ap;
+      return;
+    }
+  } else {
+    double tmp = 329.0 * qc;
+    am = (-21.0 * qmm + 189.0 * qm + tmp - 91.0 * qp + 14.0 * qpp) * (1.0 / 420.0);
+    ap = (14.0 * qmm - 91.0 * qm + tmp + 189.0 * qp - 21.0 * qpp) * (1.0 / 420.0);
+  }
+  double mn = fmin(qm, qc), mx = fmax(qm, qc);
+  if (am < mn) am = mn;
+  if (am > mx) am = mx;
+  mn = fmin(qc, qp);
+  mx = fmax(qc, qp);
+  if (ap < mn) ap = mn;
+  if (ap > mx) ap = mx;
+  am = am - qc;
+  ap = ap - qc;
+  if (ap * am >= 0.0) {
+    ap = 0.0;
+    am = 0.0;
+  } else {
+    if (fabs(ap) >= 2.0 * fabs(am)) ap = -2.0 * am;
+    if (fabs(am) >= 2.0 * fabs(ap)) am = -2.0 * ap;
+  }
+  *lo = am + qc;
+  *hi = ap + qc;
 }
+
 
 static void rk_coeffs(int stages, double c[3][3]) {
   memset(c, 0, sizeof(double) * 9);
@@ -500,9 +537,9 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
 
 #pragma omp parallel num_threads(g->nthreads > 0 ? g->nthreads : omp_get_max_threads())
   {
-    double *W = (double *)malloc(sizeof(double) * (size_t)nv * (nl + 4));
-    double *Bc = (double *)malloc(sizeof(double) * 3 * (size_t)(nl + 4));
-    double *Gf = (double *)malloc(sizeof(double) * 2 * (size_t)(nl + 4));
+    double *W = (double *)malloc(sizeof(double) * (size_t)nv * (nl + 6));
+    double *Bc = (double *)malloc(sizeof(double) * 3 * (size_t)(nl + 6));
+    double *Gf = (double *)malloc(sizeof(double) * 2 * (size_t)(nl + 6));
     double *qL = (double *)malloc(sizeof(double) * (size_t)nv * (nl + 2));
     double *qR = (double *)malloc(sizeof(double) * (size_t)nv * (nl + 2));
     double *fx = (double *)malloc(sizeof(double) * (size_t)nv * (nl + 2));
@@ -517,33 +554,38 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       int c[3];
       c[ta] = t0; c[tb] = t1;
       if (sd == 2) c[2] = 1;
-      /* gather the line: cells 1-2 .. n+2 -> W[(m+2)*nv], m = cell-1 .. */
-      for (int m = -1; m <= nl + 2; ++m) {
+      /* gather the line: cells 1-ng .. n+ng (ng = 3 for LIM5TH, 2 otherwise) -> W[(m+2)*nv] */
+      const int ngl = g->rec == 2 ? 3 : 2;
+      for (int m = 1 - ngl; m <= nl + ngl; ++m) {
         c[dir] = m;
-        for (int iv = 0; iv < nv; ++iv) W[(m + 1) * nv + iv] = g->prim[OFF(&sc, iv, c[0], c[1], c[2])];
-        if (g->mhd) for (int iv = 0; iv < sd; ++iv) Bc[(m + 1) * 3 + iv] = g->b_cc[OFF(&sb, iv, c[0], c[1], c[2])];
-        if (g->fasteos) for (int iv = 0; iv < 2; ++iv) Gf[(m + 1) * 2 + iv] = g->gammaf[OFF(&s2, iv, c[0], c[1], c[2])];
-        if (helm_nf) Gf[(m + 1) * 2] = g->temp[OFF(&st1, 0, c[0], c[1], c[2])];
+        for (int iv = 0; iv < nv; ++iv) W[(m + 2) * nv + iv] = g->prim[OFF(&sc, iv, c[0], c[1], c[2])];
+        if (g->mhd) for (int iv = 0; iv < sd; ++iv) Bc[(m + 2) * 3 + iv] = g->b_cc[OFF(&sb, iv, c[0], c[1], c[2])];
+        if (g->fasteos) for (int iv = 0; iv < 2; ++iv) Gf[(m + 2) * 2 + iv] = g->gammaf[OFF(&s2, iv, c[0], c[1], c[2])];
+        if (helm_nf) Gf[(m + 2) * 2] = g->temp[OFF(&st1, 0, c[0], c[1], c[2])];
       }
-#define WC(m) (W + ((m) + 1) * nv)
-      /* PLM over cells 0..n+1: face f=m is the low face of cell m */
-      double lo[16], hi[16];
+#define WC(m) (W + ((m) + 2) * nv)
+      /* reconstruction over cells 0..n+1: face f=m is the low face of cell m */
       for (int m = 0; m <= nl + 1; ++m) {
-        plm(WC(m - 1), WC(m), WC(m + 1), nv, lo, hi);
-        if (m >= 1) memcpy(qR + m * nv, lo, sizeof(double) * nv);
-        if (m <= nl) memcpy(qL + (m + 1) * nv, hi, sizeof(double) * nv);
+        for (int iv = 0; iv < nv; ++iv) {
+          const int limited = g->rec == 2 || (g->rec == 1 && iv >= IAS1(g));
+          double lo, hi;
+          rec_cell(g->rec, limited, g->rec == 2 ? WC(m - 2)[iv] : 0.0, WC(m - 1)[iv], WC(m)[iv], WC(m + 1)[iv],
+                   g->rec == 2 ? WC(m + 2)[iv] : 0.0, &lo, &hi);
+          if (m >= 1) qR[m * nv + iv] = lo;
+          if (m <= nl) qL[(m + 1) * nv + iv] = hi;
+        }
       }
+#define BC(m, iv) Bc[((m) + 2) * 3 + (iv)]
       if (g->mhd) {
-        /* transverse B from b_cc, normal B = face value */
+        /* transverse B from b_cc (PPH unlimited), normal B = face value */
         for (int m = 0; m <= nl + 1; ++m) {
           for (int iv = 0; iv < sd; ++iv) {
             if (iv == dir) continue;
-            double qm = Bc[m * 3 + iv], qc = Bc[(m + 1) * 3 + iv], qp = Bc[(m + 2) * 3 + iv];
-            double slopef = qp - qc, slopeb = qc - qm, prod = slopef * slopeb, slope = 0.0;
-            if (prod > 0.0) slope = prod / (slopef + slopeb);
-            double tmp = 0.5 * slope;
-            if (m >= 1) bR[m * 3 + iv] = qc - tmp;
-            if (m <= nl) bL[(m + 1) * 3 + iv] = qc + tmp;
+            double lo, hi;
+            rec_cell(g->rec, g->rec == 2, g->rec == 2 ? BC(m - 2, iv) : 0.0, BC(m - 1, iv), BC(m, iv), BC(m + 1, iv),
+                     g->rec == 2 ? BC(m + 2, iv) : 0.0, &lo, &hi);
+            if (m >= 1) bR[m * 3 + iv] = lo;
+            if (m <= nl) bL[(m + 1) * 3 + iv] = hi;
           }
         }
         for (int f = 1; f <= nl + 1; ++f) {
@@ -584,14 +626,14 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       }
       /* FASTEOS gamma_e, gamma_c reconstruction + WB add-back (source.F90:8497-8729) */
       if (g->fasteos) {
+#define GF(m, iv) Gf[((m) + 2) * 2 + (iv)]
         for (int iv = 0; iv < 2; ++iv) {
           for (int m = 0; m <= nl + 1; ++m) {
-            double qm = Gf[m * 2 + iv], qc = Gf[(m + 1) * 2 + iv], qp = Gf[(m + 2) * 2 + iv];
-            double slopef = qp - qc, slopeb = qc - qm, prod = slopef * slopeb, slope = 0.0;
-            if (prod > 0.0) slope = prod / (slopef + slopeb);
-            double tmp = 0.5 * slope;
-            if (m >= 1) gR[m * 2 + iv] = qc - tmp;
-            if (m <= nl) gL[(m + 1) * 2 + iv] = qc + tmp;
+            double lo, hi;
+            rec_cell(g->rec, g->rec == 2, g->rec == 2 ? GF(m - 2, iv) : 0.0, GF(m - 1, iv), GF(m, iv), GF(m + 1, iv),
+                     g->rec == 2 ? GF(m + 2, iv) : 0.0, &lo, &hi);
+            if (m >= 1) gR[m * 2 + iv] = lo;
+            if (m <= nl) gL[(m + 1) * 2 + iv] = hi;
           }
         }
         if (g->wb) {
@@ -606,7 +648,7 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       /* without FASTEOS: the face temperature guess 1/2 (T(i-1) + T(i)) (source.F90:8488-8495) */
       if (helm_nf)
         for (int f = 1; f <= nl + 1; ++f) {
-          double tf = 0.5 * (Gf[f * 2] + Gf[(f + 1) * 2]);
+          double tf = 0.5 * (Gf[(f + 1) * 2] + Gf[(f + 2) * 2]);
           gL[f * 2] = tf;
           gR[f * 2] = tf;
         }

@@ -47,6 +47,7 @@ typedef struct phlo_grid {
   /* compile-time options of the reference, as run-time fields */
   int sdims, nx1, nx2, nx3, ngc, nas, nvars;
   int mhd, wb, gravity, etot, helm, fasteos;
+  int rec;                /* reconstruction: 0 LIM2ND_REC, 1 PPH_REC, 2 LIM5TH_REC (ngc >= 3) */
   int riemann, rk_stages;
   int bc[3][2];           /* [dim][lower/upper] */
   double gm, mu, cfl, mach_cutoff, mach_ct;

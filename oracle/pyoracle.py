@@ -30,7 +30,7 @@ class _Grid(C.Structure):
     _fields_ = [
         ("sdims", C.c_int), ("nx1", C.c_int), ("nx2", C.c_int), ("nx3", C.c_int), ("ngc", C.c_int),
         ("nas", C.c_int), ("nvars", C.c_int), ("mhd", C.c_int), ("wb", C.c_int), ("gravity", C.c_int),
-        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("riemann", C.c_int),
+        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("rec", C.c_int), ("riemann", C.c_int),
         ("rk_stages", C.c_int), ("bc", (C.c_int * 2) * 3), ("gm", C.c_double), ("mu", C.c_double),
         ("cfl", C.c_double), ("mach_cutoff", C.c_double), ("mach_ct", C.c_double), ("dx1", C.c_double),
         ("dx2", C.c_double), ("dx3", C.c_double), ("inv_dx1", C.c_double), ("inv_dx2", C.c_double),
@@ -165,6 +165,7 @@ class OracleGrid:
         g.mhd, g.wb, g.gravity, g.etot = int(c.mhd), int(c.wb), int(c.gravity), int(c.etot)
         g.helm = int(c.helmholtz)
         g.fasteos = int(c.helmholtz and c.fasteos)
+        g.rec = {"lim2nd": 0, "pph": 1, "lim5th": 2}[c.rec]
         g.riemann = self.RIEM[c.riemann]
         g.rk_stages = c.rk_stages
         for d in range(3):

@@ -54,6 +54,49 @@ __device__ __forceinline__ long long lin(const Geo &g, int i, int j, int k) {
   return (long long)i + (long long)g.nx[0] * ((long long)j + (long long)g.nx[1] * k);
 }
 
+// ------------------------------------------------------------------ reconstructions
+enum { REC_LIM2ND = 0, REC_PPH = 1, REC_LIM5TH = 2 };
+// Edge values of the centre cell qc (lo = left edge, hi = right edge) from its neighbours:
+// PPH_REC (source.F90:8183-8259; third order, limited only when `limited`, i.e. for the
+// advected scalars) and LIM5TH_REC (source.F90:8261-8323; fifth order, always limited), with
+// the reference's limiter and operation order.  LIM2ND_REC is plm below.
+template <typename R, int REC>
+__device__ __forceinline__ void rec_edges(bool limited, R qmm, R qm, R qc, R qp, R qpp, R &lo, R &hi) {
+  R am, ap;
+  if (REC == REC_PPH) {
+    R tmp = R(5.0 / 6.0) * qc;
+    am = R(1.0 / 3.0) * qm + tmp - R(1.0 / 6.0) * qp;
+    ap = -R(1.0 / 6.0) * qm + tmp + R(1.0 / 3.0) * qp;
+    if (!limited) {
+      lo = am;
+      hi = ap;
+      return;
+    }
+  } else {
+    R tmp = R(329) * qc;
+    am = (-R(21) * qmm + R(189) * qm + tmp - R(91) * qp + R(14) * qpp) * R(1.0 / 420.0);
+    ap = (R(14) * qmm - R(91) * qm + tmp + R(189) * qp - R(21) * qpp) * R(1.0 / 420.0);
+  }
+  R mn = fmin(qm, qc), mx = fmax(qm, qc);
+  if (am < mn) am = mn;
+  if (am > mx) am = mx;
+  mn = fmin(qc, qp);
+  mx = fmax(qc, qp);
+  if (ap < mn) ap = mn;
+  if (ap > mx) ap = mx;
+  am = am - qc;
+  ap = ap - qc;
+  if (ap * am >= R(0)) {
+    ap = R(0);
+    am = R(0);
+  } else {
+    if (fabs(ap) >= R(2) * fabs(am)) ap = -R(2) * am;
+    if (fabs(am) >= R(2) * fabs(ap)) am = -R(2) * ap;
+  }
+  lo = am + qc;
+  hi = ap + qc;
+}
+
 // ------------------------------------------------------------------ LIM2ND reconstruction
 // source.F90:8141-8181: slope = df*db/(df+db) if df*db > 0 else 0; faces at qc -/+ slope/2.
 template <typename R>

@@ -17,9 +17,12 @@ namespace phl {
 
 // FAST_: USE_FASTEOS (gamma_e, gamma_c reconstructed to the faces); without it the Helmholtz
 // configurations evaluate helm_rhoP_given per Riemann side from the face temperature guess
-template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_, bool FAST_ = HELM_>
+template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_, bool FAST_ = HELM_,
+          int REC_ = REC_LIM2ND>
 struct Cfg {
-  static constexpr int DIM = DIM_, NV = NV_, RIEM = RIEM_;
+  static constexpr int DIM = DIM_, NV = NV_, RIEM = RIEM_, REC = REC_;
+  // cells on each side of a face the reconstruction reads (3 for LIM5TH, 2 otherwise)
+  static constexpr int SW = REC_ == REC_LIM5TH ? 3 : 2;
   static constexpr bool MHD = MHD_, HELM = HELM_, WB = WB_, ETOT = ETOT_, GRAV = GRAV_, FAST = HELM_ && FAST_;
   static constexpr int EOSM = !HELM_ ? EOS_IDEAL : (FAST_ ? EOS_FAST : EOS_GIVEN);
   static constexpr int IP = 1 + DIM, IAS = 2 + DIM;
@@ -175,32 +178,40 @@ __device__ __forceinline__ void load_bcc(const Prm &P, int i, int j, int k, doub
 // Flux through the low face of cell `m` along d, given the deviation states of cells
 // m-2..m+1 (wl2, wl1, wr1, wr2 = cells m-2, m-1, m, m+1).  Implements, for one face, the body
 // of the x1/x2/x3 sweeps (source.F90:8138-9105, 9107-10301, 10303-11364).
+// Left/right face values of variable iv: the right edge of cell m-1 and the left edge of cell m,
+// from the cells m-3 .. m+2 (c[0] .. c[5]; the outer pair is read by LIM5TH only)
+template <class C, typename R>
+__device__ __forceinline__ void rec_face(const R *const c[6], int iv, bool limited, R &qL, R &qR) {
+  R lo, hi;
+  if (C::REC == REC_LIM2ND) {
+    plm(c[1][iv], c[2][iv], c[3][iv], lo, hi);
+    qL = hi;
+    plm(c[2][iv], c[3][iv], c[4][iv], lo, hi);
+    qR = lo;
+  } else {
+    const bool w5 = C::REC == REC_LIM5TH;
+    rec_edges<R, C::REC>(limited, w5 ? c[0][iv] : R(0), c[1][iv], c[2][iv], c[3][iv], w5 ? c[4][iv] : R(0), lo, hi);
+    qL = hi;
+    rec_edges<R, C::REC>(limited, w5 ? c[1][iv] : R(0), c[2][iv], c[3][iv], c[4][iv], w5 ? c[5][iv] : R(0), lo, hi);
+    qR = lo;
+  }
+}
+
 template <class C>
-__device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, int fk,
-                                          const double *wl2, const double *wl1, const double *wr1,
-                                          const double *wr2, const double *gl2, const double *gl1,
-                                          const double *gr1, const double *gr2, const double *bcl2,
-                                          const double *bcl1, const double *bcr1, const double *bcr2,
-                                          double F[C::NV], double Fb[3], double &rho_face_sum) {
+__device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, int fk, const double *const w[6],
+                                          const double *const gmv[6], const double *const bc[6], double F[C::NV],
+                                          double Fb[3], double &rho_face_sum) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
-  double qL[NV], qR[NV], lo, hi;
+  double qL[NV], qR[NV];
 #pragma unroll
-  for (int iv = 0; iv < NV; ++iv) {
-    plm(wl2[iv], wl1[iv], wr1[iv], lo, hi);
-    qL[iv] = hi;
-    plm(wl1[iv], wr1[iv], wr2[iv], lo, hi);
-    qR[iv] = lo;
-  }
+  for (int iv = 0; iv < NV; ++iv) rec_face<C>(w, iv, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
   double bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
   if (C::MHD) {
 #pragma unroll
     for (int iv = 0; iv < C::DIM; ++iv) {
       if (iv == d) continue;
-      plm(bcl2[iv], bcl1[iv], bcr1[iv], lo, hi);
-      bL[iv] = hi;
-      plm(bcl1[iv], bcr1[iv], bcr2[iv], lo, hi);
-      bR[iv] = lo;
+      rec_face<C>(bc, iv, C::REC == REC_LIM5TH, bL[iv], bR[iv]);
     }
     double bn = P.bf[d][face_lin(g, d, fi, fj, fk)];
     bL[d] = bn;
@@ -234,12 +245,7 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   double gL[2] = {0, 0}, gR[2] = {0, 0};
   if (C::FAST) {
 #pragma unroll
-    for (int iv = 0; iv < 2; ++iv) {
-      plm(gl2[iv], gl1[iv], gr1[iv], lo, hi);
-      gL[iv] = hi;
-      plm(gl1[iv], gr1[iv], gr2[iv], lo, hi);
-      gR[iv] = lo;
-    }
+    for (int iv = 0; iv < 2; ++iv) rec_face<C>(gmv, iv, C::REC == REC_LIM5TH, gL[iv], gR[iv]);
     if (C::WB) {
       double ge = __ldg(P.eq_ge_f[d] + fb);
       gL[0] = gL[0] + ge;
@@ -248,7 +254,7 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   } else if (C::HELM) {
     // Helmholtz without USE_FASTEOS: helm_rhoP_given on each side of the face from the guess
     // 1/2 (T(m-1) + T(m)) (source.F90:8488-8495, 15705-15720, 15777-15781); passes rho*e and c
-    const double tface = 0.5 * (gl1[0] + gr1[0]);
+    const double tface = 0.5 * (gmv[2][0] + gmv[3][0]);
     double *gs[2] = {gL, gR};
     const double *qs[2] = {qL, qR};
 #pragma unroll
@@ -310,17 +316,27 @@ __global__ void __launch_bounds__(128) k_face(Prm P, int d) {
   if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
   const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
-  double w[4][NV], gmv[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, bc[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  // cells m-3 .. m+2 around the face (the reconstruction reads m-SW .. m+SW-1)
+  double w[6][NV], gmv[6][2], bc[6][3];
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    const int ii = fi + (d == 0 ? s - 2 : 0), jj = fj + (d == 1 ? s - 2 : 0), kk = fk + (d == 2 ? s - 2 : 0);
+  for (int s = 0; s < 6; ++s) {
+    gmv[s][0] = gmv[s][1] = 0.0;
+    bc[s][0] = bc[s][1] = bc[s][2] = 0.0;
+    if (s < 3 - C::SW || s >= 3 + C::SW) {
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) w[s][iv] = 0.0;
+      continue;
+    }
+    const int ii = fi + (d == 0 ? s - 3 : 0), jj = fj + (d == 1 ? s - 3 : 0), kk = fk + (d == 2 ? s - 3 : 0);
     load_wdev<C>(P, ii, jj, kk, w[s]);
     if (C::HELM) load_gdev<C>(P, ii, jj, kk, gmv[s]);
     if (C::MHD) load_bcc<C>(P, ii, jj, kk, bc[s]);
   }
+  const double *const wp[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
+  const double *const gp[6] = {gmv[0], gmv[1], gmv[2], gmv[3], gmv[4], gmv[5]};
+  const double *const bp[6] = {bc[0], bc[1], bc[2], bc[3], bc[4], bc[5]};
   double F[NV], Fb[3], rs;
-  face_flux<C>(P, d, fi, fj, fk, w[0], w[1], w[2], w[3], gmv[0], gmv[1], gmv[2], gmv[3], bc[0], bc[1], bc[2], bc[3],
-               F, Fb, rs);
+  face_flux<C>(P, d, fi, fj, fk, wp, gp, bp, F, Fb, rs);
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.dflux[d][(long long)iv * nf + f] = F[iv];
   if (C::MHD) store_face_emf<C>(P, d, f, Fb, F[0], rs, P.scal[2]);

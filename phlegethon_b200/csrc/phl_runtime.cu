@@ -63,32 +63,38 @@ struct RunnerT : Runner {
 };
 
 // Instantiated option sets: (dims, nvars, MHD, Helmholtz, stratified = WB+ETOT+gravity, Riemann
-// solver, USE_FASTEOS).  Other combinations return PHL_E_UNSUPPORTED.
-#define PHL_RUNNER_LIST(X)                       \
-  X(2, 4, false, false, false, R_LHLLC, false)   \
-  X(2, 4, false, false, false, R_HLLC, false)    \
-  X(2, 4, false, false, true, R_LHLLC, false)    \
-  X(2, 4, false, false, true, R_HLLC, false)     \
-  X(2, 4, true, false, false, R_HLLD, false)     \
-  X(2, 4, true, false, false, R_LHLLD, false)    \
-  X(2, 6, false, true, true, R_LHLLC, true)      \
-  X(2, 6, true, true, true, R_LHLLD, true)       \
-  X(3, 5, false, false, false, R_LHLLC, false)   \
-  X(3, 5, false, false, false, R_HLLC, false)    \
-  X(3, 5, true, false, false, R_HLLD, false)     \
-  X(3, 5, true, false, false, R_LHLLD, false)    \
-  X(3, 7, false, true, true, R_LHLLC, true)      \
-  X(3, 7, false, true, true, R_HLLC, true)       \
-  X(3, 7, true, true, true, R_LHLLD, true)       \
-  X(3, 7, true, true, true, R_HLLD, true)        \
-  X(3, 7, false, true, true, R_LHLLC, false)     \
-  X(3, 7, false, true, true, R_HLLC, false)      \
-  X(3, 7, true, true, true, R_LHLLD, false)
+// solver, USE_FASTEOS, reconstruction).  Other combinations return PHL_E_UNSUPPORTED.
+#define PHL_RUNNER_LIST(X)                                  \
+  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
+  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND)   \
+  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND)   \
+  X(2, 4, false, false, true, R_HLLC, false, REC_LIM2ND)    \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND)    \
+  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
+  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
+  X(2, 6, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
+  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
+  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND)   \
+  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND)    \
+  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
+  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND)      \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
+  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND)       \
+  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND)    \
+  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND)     \
+  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND)     \
+  X(2, 4, true, false, false, R_HLLD, false, REC_PPH)       \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH)    \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH)        \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM5TH)     \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH)         \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH)      
 
-Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast) {
-#define X(D, N, M, H, S, R, F)                                                                  \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F)) \
-    return new RunnerT<Cfg<D, N, M, H, S, S, S, R, F>>();
+Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec) {
+#define X(D, N, M, H, S, R, F, REC)                                                                           \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) && rec == REC) \
+    return new RunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC>>();
   PHL_RUNNER_LIST(X)
 #undef X
   return nullptr;
@@ -345,6 +351,8 @@ int check_cfg(const phl_config *c) {
   if (!mhd && (c->riemann != PHL_LHLLC && c->riemann != PHL_HLLC)) return PHL_E_INVALID;
   if (helm && !((c->flags & PHL_ADVECT_YE_IABAR) && c->nas >= 2)) return PHL_E_UNSUPPORTED;
   if (c->precision != PHL_FP64 && c->precision != PHL_FP32_SPLIT) return PHL_E_INVALID;
+  if (c->reconstruction < PHL_REC_LIM2ND || c->reconstruction > PHL_REC_LIM5TH) return PHL_E_INVALID;
+  if (c->reconstruction == PHL_REC_LIM5TH && c->ngc < 3) return PHL_E_INVALID;
   // the step's Newton starts from the previous stage's temperature (the reference's warm start);
   // the learned guess is offered by the batch inversion entry points only
   if (c->eos_guess == PHL_GUESS_MLP) {
@@ -416,9 +424,9 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   c->split = cfg->precision == PHL_FP32_SPLIT;
   const bool fast = cfg->flags & PHL_FASTEOS;
   if (c->split)
-    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast));
+    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction));
   else
-    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast));
+    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction));
   if (!c->runner) return PHL_E_UNSUPPORTED;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   Geo &g = c->geo;

@@ -355,20 +355,36 @@ __device__ __forceinline__ void split_side_eos(const Prm &P, const float *q, flo
   c_s = (float)(snd * P.inv_v_ref);
 }
 
+// FP32 face values of one variable from the values of cells m-3 .. m+2 (v[0] .. v[5]; LIM2ND and
+// PPH read v[1] .. v[4])
+template <class C>
+__device__ __forceinline__ void rec_face_f32(const float v[6], bool limited, float &qL, float &qR) {
+  float lo, hi;
+  if (C::REC == REC_LIM2ND) {
+    plm_f32(v[1], v[2], v[3], lo, hi);
+    qL = hi;
+    plm_f32(v[2], v[3], v[4], lo, hi);
+    qR = lo;
+  } else {
+    rec_edges<float, C::REC>(limited, v[0], v[1], v[2], v[3], v[4], lo, hi);
+    qL = hi;
+    rec_edges<float, C::REC>(limited, v[1], v[2], v[3], v[4], v[5], lo, hi);
+    qR = lo;
+  }
+}
+
 // flux through the low face of cell m along d from the FP32 deviation states of cells m-2..m+1
 template <class C, class Cells>
 __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int fj, int fk, const Cells &cl,
                                                 float F[C::NV]) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
-  float qL[NV], qR[NV], lo, hi;
+  static_assert(C::SW == 2, "cell-accessor faces read two cells per side");
+  float qL[NV], qR[NV];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
-    const float w0 = cl.w(0, iv), w1 = cl.w(1, iv), w2 = cl.w(2, iv), w3 = cl.w(3, iv);
-    plm_f32(w0, w1, w2, lo, hi);
-    qL[iv] = hi;
-    plm_f32(w1, w2, w3, lo, hi);
-    qR[iv] = lo;
+    const float v[6] = {0.0f, cl.w(0, iv), cl.w(1, iv), cl.w(2, iv), cl.w(3, iv), 0.0f};
+    rec_face_f32<C>(v, iv >= C::IAS, qL[iv], qR[iv]);
   }
   if (d == 1) {
     float a = qL[1], b = qL[2]; qL[1] = b; qL[2] = -a;
@@ -390,11 +406,8 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
   if (C::FAST) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      const float g0 = cl.g(0, iv), g1 = cl.g(1, iv), g2 = cl.g(2, iv), g3 = cl.g(3, iv);
-      plm_f32(g0, g1, g2, lo, hi);
-      gL[iv] = hi;
-      plm_f32(g1, g2, g3, lo, hi);
-      gR[iv] = lo;
+      const float v[6] = {0.0f, cl.g(0, iv), cl.g(1, iv), cl.g(2, iv), cl.g(3, iv), 0.0f};
+      rec_face_f32<C>(v, false, gL[iv], gR[iv]);
     }
     if (C::WB) {
       float ge = __ldg(P.sf_ge_f[d] + fb);
@@ -825,27 +838,23 @@ __device__ __forceinline__ void load_bccf(const Prm &P, int i, int j, int k, flo
 // Fb (lab frame) and rho_L + rho_R at the face for the CT upwinding sign (source.F90:8138-9105
 // with the MHD parts 8327-8469, 8926-8959)
 template <class C>
-__device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi, int fj, int fk, const float *const w[4],
-                                                    const float *const gm[4], const float *const b[4], float F[C::NV],
+__device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi, int fj, int fk, const float *const w[6],
+                                                    const float *const gm[6], const float *const b[6], float F[C::NV],
                                                     float Fb[3], float &rho_sum) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
-  float qL[NV], qR[NV], lo, hi;
+  float qL[NV], qR[NV];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
-    plm_f32(w[0][iv], w[1][iv], w[2][iv], lo, hi);
-    qL[iv] = hi;
-    plm_f32(w[1][iv], w[2][iv], w[3][iv], lo, hi);
-    qR[iv] = lo;
+    const float v[6] = {w[0][iv], w[1][iv], w[2][iv], w[3][iv], w[4][iv], w[5][iv]};
+    rec_face_f32<C>(v, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
   }
   float bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
 #pragma unroll
   for (int iv = 0; iv < C::DIM; ++iv) {
     if (iv == d) continue;
-    plm_f32(b[0][iv], b[1][iv], b[2][iv], lo, hi);
-    bL[iv] = hi;
-    plm_f32(b[1][iv], b[2][iv], b[3][iv], lo, hi);
-    bR[iv] = lo;
+    const float v[6] = {b[0][iv], b[1][iv], b[2][iv], b[3][iv], b[4][iv], b[5][iv]};
+    rec_face_f32<C>(v, C::REC == REC_LIM5TH, bL[iv], bR[iv]);
   }
   const float bn = (float)(P.bf[d][face_lin(g, d, fi, fj, fk)] * P.inv_b_ref);
   bL[d] = bn;
@@ -874,10 +883,8 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
   if (C::FAST) {
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      plm_f32(gm[0][iv], gm[1][iv], gm[2][iv], lo, hi);
-      gL[iv] = hi;
-      plm_f32(gm[1][iv], gm[2][iv], gm[3][iv], lo, hi);
-      gR[iv] = lo;
+      const float v[6] = {gm[0][iv], gm[1][iv], gm[2][iv], gm[3][iv], gm[4][iv], gm[5][iv]};
+      rec_face_f32<C>(v, C::REC == REC_LIM5TH, gL[iv], gR[iv]);
     }
     if (C::WB) {
       float ge = __ldg(P.sf_ge_f[d] + fb);
@@ -885,7 +892,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
       gR[0] = gR[0] + ge;
     }
   } else if (C::HELM) {
-    const float tface = 0.5f * (gm[1][0] + gm[2][0]);
+    const float tface = 0.5f * (gm[2][0] + gm[3][0]);
     split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
@@ -938,15 +945,24 @@ __global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
   if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
   const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
-  float w[4][NV], gm4[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, b4[4][3];
+  // cells m-3 .. m+2 (the reconstruction reads m-SW .. m+SW-1)
+  float w[6][NV], gm4[6][2], b4[6][3];
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    const int ii = fi + (d == 0 ? s - 2 : 0), jj = fj + (d == 1 ? s - 2 : 0), kk = fk + (d == 2 ? s - 2 : 0);
+  for (int s = 0; s < 6; ++s) {
+    gm4[s][0] = gm4[s][1] = 0.0f;
+    b4[s][0] = b4[s][1] = b4[s][2] = 0.0f;
+    if (s < 3 - C::SW || s >= 3 + C::SW) {
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) w[s][iv] = 0.0f;
+      continue;
+    }
+    const int ii = fi + (d == 0 ? s - 3 : 0), jj = fj + (d == 1 ? s - 3 : 0), kk = fk + (d == 2 ? s - 3 : 0);
     load_wf<C>(P, ii, jj, kk, w[s], gm4[s]);
     load_bccf<C>(P, ii, jj, kk, b4[s]);
   }
-  const float *const wv[4] = {w[0], w[1], w[2], w[3]}, *const gv[4] = {gm4[0], gm4[1], gm4[2], gm4[3]},
-                     *const bv[4] = {b4[0], b4[1], b4[2], b4[3]};
+  const float *const wv[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
+  const float *const gv[6] = {gm4[0], gm4[1], gm4[2], gm4[3], gm4[4], gm4[5]};
+  const float *const bv[6] = {b4[0], b4[1], b4[2], b4[3], b4[4], b4[5]};
   float F[NV], Fb[3], rs;
   face_flux_split_mhd<C>(P, d, fi, fj, fk, wv, gv, bv, F, Fb, rs);
 #pragma unroll
@@ -1387,8 +1403,12 @@ struct SplitRunnerT : Runner {
         k_bface_split<C><<<nblk(nf, 256), 256, 0, s>>>(P, d);
       }
       k_c2p_mhd_split<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
-      return;
-    } else if constexpr (C::DIM == 3) {
+    } else {
+      hydro_stage(P, s);
+    }
+  }
+  void hydro_stage(const Prm &P, cudaStream_t s) {
+    if constexpr (C::DIM == 3) {
       if (tiled(P.g)) {
         constexpr size_t sm = SplitTile<C, TX, TY>::bytes();
         if (!attr_set) {
@@ -1418,29 +1438,33 @@ struct SplitRunnerT : Runner {
   }
 };
 
-#define PHL_SPLIT_LIST(X)                       \
-  X(2, 4, true, false, false, R_HLLD, false)     \
-  X(2, 4, true, false, false, R_LHLLD, false)    \
-  X(3, 5, true, false, false, R_HLLD, false)     \
-  X(3, 5, true, false, false, R_LHLLD, false)    \
-  X(3, 7, true, true, true, R_LHLLD, true)       \
-  X(3, 7, true, true, true, R_HLLD, true)        \
-  X(3, 7, true, true, true, R_LHLLD, false)      \
-  X(2, 4, false, false, false, R_LHLLC, false)   \
-  X(2, 4, false, false, false, R_HLLC, false)    \
-  X(2, 4, false, false, true, R_LHLLC, false)    \
-  X(2, 6, false, true, true, R_LHLLC, true)      \
-  X(3, 5, false, false, false, R_LHLLC, false)   \
-  X(3, 5, false, false, false, R_HLLC, false)    \
-  X(3, 7, false, true, true, R_LHLLC, true)      \
-  X(3, 7, false, true, true, R_HLLC, true)       \
-  X(3, 7, false, true, true, R_LHLLC, false)     \
-  X(3, 7, false, true, true, R_HLLC, false)
+#define PHL_SPLIT_LIST(X)                                   \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND)    \
+  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
+  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND)    \
+  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
+  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND)       \
+  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND)     \
+  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
+  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND)   \
+  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND)   \
+  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
+  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
+  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND)   \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
+  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND)      \
+  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND)    \
+  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND)     \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH)    \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH)         \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH)      \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH)        
 
-Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast) {
-#define X(D, N, M, H, S, R, F)                                                                  \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F)) \
-    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R, F>>();
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec) {
+#define X(D, N, M, H, S, R, F, REC)                                                                           \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) && rec == REC) \
+    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC>>();
   PHL_SPLIT_LIST(X)
 #undef X
   return nullptr;

@@ -45,6 +45,7 @@ class Config:
     fasteos: bool = True             # USE_FASTEOS (with helmholtz): gamma_e/gamma_c at the faces
                                      # instead of helm_rhoP_given per Riemann side
     riemann: str = "lhllc"
+    rec: str = "lim2nd"              # LIM2ND_REC, PPH_REC or LIM5TH_REC (needs ngc >= 3)
     rk_stages: int = 3
     bc: list = field(default_factory=lambda: [["periodic", "periodic"]] * 3)
     precision: str = "fp64"

@@ -116,9 +116,11 @@ def hot_bubble_2d(n=256, riemann="lhllc", seed=None):
 
 
 # ------------------------------------------------------------------------------ config 2
-def orszag_tang_2d(n=1024, riemann="hlld"):
-    """Orszag-Tang vortex on the periodic unit square (tests/orszag-tang/app.F90:13-79)."""
-    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=2, nas=0, mhd=True, riemann=riemann, rk_stages=3,
+def orszag_tang_2d(n=1024, riemann="hlld", rec="lim2nd"):
+    """Orszag-Tang vortex on the periodic unit square (tests/orszag-tang/app.F90:13-79; the
+    reference's test runs it with LIM5TH_REC, tests/orszag-tang/Makefile:29)."""
+    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=3 if rec == "lim5th" else 2, nas=0, mhd=True, riemann=riemann,
+                 rec=rec, rk_stages=3,
                  bc=[["periodic", "periodic"]] * 3, gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8,
                  mach_cutoff=1e-4, mach_ct=1e-6)
     h = HostGrid(cfg)
@@ -147,7 +149,7 @@ STRAT_ZBAR = 6.9
 
 
 def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, seed=12345,
-                  riemann=None, table=X2_TABLE, fasteos=True):
+                  riemann=None, table=X2_TABLE, fasteos=True, rec="lim2nd"):
     """3D stratified convection box with the Helmholtz EoS.
 
     x2 is vertical (reflecting walls), x1 and x3 periodic.  rho_eq(y) falls exponentially from
@@ -156,7 +158,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     advected as Ye and 1/Abar.  Velocities are mach * c_s * U[-1,1] per component from a
     counter-based hash (seed).  With mhd=True a uniform horizontal B_x1 of plasma beta `beta` at
     mid-height is added and the LHLLD solver with constrained transport is used.  fasteos=False
-    selects the Helmholtz path without USE_FASTEOS (helm_rhoP_given per Riemann side).
+    selects the Helmholtz path without USE_FASTEOS (helm_rhoP_given per Riemann side); rec picks
+    the reconstruction (lim2nd, pph, lim5th; lim5th uses 3 ghost layers).
     """
     ny = n if ny is None else ny
     nz = n if nz is None else nz
@@ -169,8 +172,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     p_top = float(analytic_pressure(rho_top, 1.0e8, abar, zbar))
     p_bot = float(analytic_pressure(rho_bot, 3.0e8, abar, zbar))
     g = (p_bot - p_top) / (rho_bot * Hrho * (1.0 - rho_top / rho_bot))
-    cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=2, nas=2, mhd=mhd, wb=True, gravity=True, etot=True,
-                 helmholtz=True, fasteos=fasteos, riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
+    cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=3 if rec == "lim5th" else 2, nas=2, mhd=mhd, wb=True,
+                 gravity=True, etot=True, rec=rec, helmholtz=True, fasteos=fasteos, riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
                  bc=[["periodic", "periodic"], ["reflective", "reflective"], ["periodic", "periodic"]],
                  x1l=0.0, x1u=Lx * n / ny, x2l=0.0, x2u=L, x3l=0.0, x3u=Lx * nz / ny,
                  gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8, mach_cutoff=1e-4, mach_ct=1e-6,

@@ -179,3 +179,21 @@ def test_stratified_helmholtz_without_fasteos(gpu_lib, oracle, table, mhd, riema
     if mhd:
         assert div_b_max(hg) <= 1e-13
 
+
+
+# ------------------------------------------------------------------------------ PPH_REC / LIM5TH_REC
+@pytest.mark.parametrize("rec", ["pph", "lim5th"])
+def test_orszag_tang_higher_order(gpu_lib, oracle, rec):
+    cfg, h = problems.orszag_tang_2d(48, rec=rec)
+    hg, ho, _ = run_pair(cfg, h, 10, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert div_b_max(hg) <= 1e-13
+
+
+@pytest.mark.parametrize("mhd,riemann,rec", [(False, "lhllc", "pph"), (False, "lhllc", "lim5th"),
+                                             (True, "lhlld", "pph"), (True, "lhlld", "lim5th")])
+def test_stratified_helmholtz_higher_order(gpu_lib, oracle, table, mhd, riemann, rec):
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd, riemann=riemann, rec=rec)
+    hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["newton_nonconverged"] == 0 and st["nonfinite"] == 0

@@ -151,3 +151,30 @@ def test_split_helmholtz_without_fasteos(gpu_lib, table, mhd, riemann):
             assert err[f] <= 1e-8, (f, err)
         for f in ("v1", "v2", "v3"):
             assert err[f] <= 1e-5, (f, err)
+
+
+def test_split_orszag_tang_lim5th(gpu_lib):
+    from util import div_b_max
+    cfg, h = problems.orszag_tang_2d(64, rec="lim5th")
+    h64, _ = run_form(cfg, h, 30, None, "fp64")
+    h32, st = run_form(cfg, h, 30, None, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0
+    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
+        assert err[f] <= lim, (f, err)
+    assert div_b_max(h32) <= 1e-13
+
+
+@pytest.mark.parametrize("mhd,riemann,rec,dims", [(True, "lhlld", "pph", (16, 24, 12)), (True, "lhlld", "lim5th", (16, 24, 12)),
+                                                  (False, "lhllc", "pph", (32, 16, 16))])
+def test_split_stratified_higher_order(gpu_lib, table, mhd, riemann, rec, dims):
+    n, ny, nz = dims
+    cfg, h = problems.stratified_3d(n, ny=ny, nz=nz, mhd=mhd, riemann=riemann, rec=rec)
+    h64, _ = run_form(cfg, h, 20, table, "fp64")
+    h32, st = run_form(cfg, h, 20, table, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    for f in ("rho", "p", "e", "T"):
+        assert err[f] <= 1e-8, (f, err)
+    for f in ("v1", "v2", "v3"):
+        assert err[f] <= 1e-5, (f, err)

@@ -205,3 +205,35 @@ def test_bracket_guess_batch_round_trip(oracle, table):
                                                     Tg.ctypes.data_as(C.POINTER(C.c_double)))
         assert 1 <= nev <= 2 + 8
         assert abs(math.log10(Tg[0] / Tb[i])) < 0.06
+
+
+@pytest.mark.parametrize("rec", ["pph", "lim5th"])
+def test_higher_order_uniform_and_div_b(oracle, rec):
+    """PPH_REC / LIM5TH_REC: a uniform state stays uniform; constrained transport keeps div B."""
+    cfg = Config(sdims=2, nx1=16, nx2=12, riemann="hllc", rec=rec, ngc=3 if rec == "lim5th" else 2,
+                 bc=[["periodic", "periodic"]] * 3)
+    h = HostGrid(cfg)
+    h.prim[0] = 1.3
+    h.prim[1] = 0.2
+    h.prim[2] = -0.1
+    h.prim[3] = 0.7
+    _run(oracle, h, steps=4)
+    out = h.interior(h.prim)
+    assert np.all(out == out[:, :1, :1, :1])
+    cfg, h = problems.orszag_tang_2d(32, rec=rec)
+    _run(oracle, h, steps=10)
+    assert div_b_max(h) <= 1e-13
+
+
+def test_lim5th_edges_reproduce_smooth_data():
+    """The fifth-order edge formula of LIM5TH_REC is exact for quartic data (away from extrema)."""
+    x = np.arange(-2, 3, dtype=float)
+    f = lambda t: 1.0 + 0.1 * t + 0.01 * t ** 2 + 0.001 * t ** 3 + 0.0001 * t ** 4
+    # cell averages of f over [i-1/2, i+1/2]
+    from numpy.polynomial import polynomial as Pn
+    coef = [1.0, 0.1, 0.01, 0.001, 0.0001]
+    integ = Pn.polyint(coef)
+    avg = np.array([Pn.polyval(i + 0.5, integ) - Pn.polyval(i - 0.5, integ) for i in x])
+    am = (-21 * avg[0] + 189 * avg[1] + 329 * avg[2] - 91 * avg[3] + 14 * avg[4]) / 420.0
+    ap = (14 * avg[0] - 91 * avg[1] + 329 * avg[2] + 189 * avg[3] - 21 * avg[4]) / 420.0
+    assert abs(am - f(-0.5)) < 1e-12 and abs(ap - f(0.5)) < 1e-12
