@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PHL_ABI_VERSION 2
+#define PHL_ABI_VERSION 3
 
 /* return codes */
 #define PHL_OK 0
@@ -55,6 +55,7 @@ extern "C" {
 #define PHL_HELMHOLTZ (1 << 4)        /* HELMHOLTZ_EOS */
 #define PHL_FASTEOS (1 << 5)          /* USE_FASTEOS */
 #define PHL_ADVECT_YE_IABAR (1 << 6)  /* ADVECT_YE_IABAR */
+#define PHL_SHOCK_FLATTENING (1 << 7) /* USE_SHOCK_FLATTENING (ngc >= 3; PHL_FP64 only) */
 
 /* arithmetic of the flux path */
 #define PHL_FP64 0        /* FP64 throughout, bit-compatible with the reference order */
@@ -90,6 +91,9 @@ typedef struct phl_config {
   double helm_ltlo, helm_lthi, helm_ldlo, helm_ldhi;
   int reconstruction;              /* PHL_REC_LIM2ND (LIM2ND_REC), PHL_REC_PPH, PHL_REC_LIM5TH
                                       (ngc >= 3) */
+  double eps_sf;                   /* eps_sf_make (reference default 0.25): a cell whose summed
+                                      central pressure jumps exceed eps_sf * p flags itself and
+                                      its neighbours; read with PHL_SHOCK_FLATTENING */
 } phl_config;
 
 /* Host arrays, laid out exactly as the locgrid members of the same name

@@ -9,8 +9,10 @@
  *   WB deviation (rho', p', gammae')         7151-7168
  *   periodic self-copy of ghosts             2293-2306 / 2431-2444 (communicate_*)
  *   reflective physical BCs                  7532-7958 (bc_fac / bc_facb)
+ *   shock detector (USE_SHOCK_FLATTENING)   8073-8136
  *   x1 sweep: LIM2ND PLM, B recon, WB add,   8138-9105
- *             FASTEOS gamma recon, riemann, EMF + sign_frho, WB flux fix, ETOT, res
+ *             FASTEOS gamma recon, flattening 8731-8878, riemann, EMF + sign_frho,
+ *             WB flux fix, ETOT, res
  *   x2 sweep (rotation v,B / flux back)      9107-10301
  *   x3 sweep (cyclic rotation)               10303-11364
  *   EMF ghosts + reflective EMF BCs          11374-11964
@@ -85,6 +87,7 @@ typedef struct {
   double *state, *state0, *res;
   double *b0[3];
   double *emf[3], *sgn[3], *cor[3];
+  double *flat;   /* is_flattened(cells), 0/1 (USE_SHOCK_FLATTENING) */
 } scr_t;
 
 long phlo_scratch_doubles(const phlo_grid *g) {
@@ -100,6 +103,10 @@ long phlo_scratch_doubles(const phlo_grid *g) {
       shp c = corner(g, a);
       n += ssize(&c);
     }
+  }
+  if (g->sf) {
+    shp c = cellg(g, 1);
+    n += ssize(&c);
   }
   return n;
 }
@@ -126,6 +133,10 @@ static scr_t carve(phlo_grid *g) {
       s.cor[a] = p; p += ssize(&c);
     }
   }
+  if (g->sf) {
+    shp c = cellg(g, 1);
+    s.flat = p; p += ssize(&c);
+  }
   return s;
 }
 
@@ -140,7 +151,7 @@ static inline double sgnf(double x) { return copysign(1.0, x); }
 
 /* ---------------------------------------------------------------- Riemann: hydro */
 void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
-                        const double *gL, const double *gR, double *flux) {
+                        const double *gL, const double *gR, double *flux, int flat) {
   const int three = g->sdims == 3, ip = IP(g), ias = IAS1(g), nv = g->nvars;
   const double gm = g->gm, gmm1 = gm - 1.0, igmm1 = 1.0 / gmm1;
   double rhoL = qL[IRHO], inv_rhoL = 1.0 / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = three ? qL[3] : 0.0;
@@ -183,6 +194,28 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
   double rhoestarL = rhostarL * (rhoeL * inv_rhoL + (ustar - vx1L) * (ustar + pL * inv_rhoL / dsuL));
   double rhostarR = rhoR * (dsuR / (sR - ustar));
   double rhoestarR = rhostarR * (rhoeR * inv_rhoR + (ustar - vx1R) * (ustar + pR * inv_rhoR / dsuR));
+
+  if (flat) {
+    /* HLL flux on a flattened face (source.F90:15929-16010) */
+    double UL[16], UR[16], fL[16], fR[16];
+    sL = fmin(0.0, sL);
+    sR = fmax(0.0, sR);
+    UL[IRHO] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (three) UL[3] = rhoL * vx3L; UL[ip] = rhoeL;
+    for (int iv = ias; iv < nv; ++iv) UL[iv] = rhoL * qL[iv];
+    UR[IRHO] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (three) UR[3] = rhoR * vx3R; UR[ip] = rhoeR;
+    for (int iv = ias; iv < nv; ++iv) UR[iv] = rhoR * qR[iv];
+    fL[IRHO] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + pL; fL[2] = rhoL * vx1L * vx2L;
+    if (three) fL[3] = rhoL * vx1L * vx3L;
+    fL[ip] = (rhoeL + pL) * vx1L;
+    for (int iv = ias; iv < nv; ++iv) fL[iv] = UL[iv] * vx1L;
+    fR[IRHO] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + pR; fR[2] = rhoR * vx1R * vx2R;
+    if (three) fR[3] = rhoR * vx1R * vx3R;
+    fR[ip] = (rhoeR + pR) * vx1R;
+    for (int iv = ias; iv < nv; ++iv) fR[iv] = UR[iv] * vx1R;
+    double dummy = 1.0 / (sR - sL), phi = sL * sR;
+    for (int iv = 0; iv < nv; ++iv) flux[iv] = dummy * (sR * fL[iv] - sL * fR[iv] + phi * (UR[iv] - UL[iv]));
+    return;
+  }
 
   if (g->riemann == PHLO_LHLLC) {
     /* low-dissipation HLLC (source.F90:16012-16122, FLUX_IS_ALL_MACH off) */
@@ -235,7 +268,7 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
 /* ---------------------------------------------------------------- Riemann: MHD */
 void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
                       const double *bL, const double *bR, const double *gL, const double *gR,
-                      double *flux, double *fluxb) {
+                      double *flux, double *fluxb, int flat) {
   const int three = g->sdims == 3, ip = IP(g), ias = IAS1(g), nv = g->nvars;
   const double gm = g->gm, gmm1 = gm - 1.0, igmm1 = 1.0 / gmm1;
   double rhoL = qL[IRHO], inv_rhoL = 1.0 / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = three ? qL[3] : 0.0;
@@ -301,6 +334,33 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
     } else {
       phi = 1.0;
     }
+  }
+  if (flat) {
+    /* HLL flux on a flattened face (source.F90:14386-14495) */
+    double UL[16], UR[16], fL[16], fR[16], UbL[3], UbR[3], fbL[3], fbR[3];
+    sL = fmin(0.0, sL);
+    sR = fmax(0.0, sR);
+    UL[IRHO] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (three) UL[3] = rhoL * vx3L; UL[ip] = rhoeL;
+    for (int iv = ias; iv < nv; ++iv) UL[iv] = rhoL * qL[iv];
+    UbL[0] = bx1; UbL[1] = bx2L; UbL[2] = bx3L;
+    UR[IRHO] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (three) UR[3] = rhoR * vx3R; UR[ip] = rhoeR;
+    for (int iv = ias; iv < nv; ++iv) UR[iv] = rhoR * qR[iv];
+    UbR[0] = bx1; UbR[1] = bx2R; UbR[2] = bx3R;
+    fL[IRHO] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + ptL - bx1_2; fL[2] = rhoL * vx1L * vx2L - bx1 * bx2L;
+    if (three) fL[3] = rhoL * vx1L * vx3L - bx1 * bx3L;
+    fL[ip] = (rhoeL + ptL) * vx1L - bx1 * (bx1 * vx1L + bx2L * vx2L + bx3L * vx3L);
+    for (int iv = ias; iv < nv; ++iv) fL[iv] = UL[iv] * vx1L;
+    fbL[0] = 0.0; fbL[1] = vx1L * bx2L - vx2L * bx1; fbL[2] = vx1L * bx3L - vx3L * bx1;
+    fR[IRHO] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + ptR - bx1_2; fR[2] = rhoR * vx1R * vx2R - bx1 * bx2R;
+    if (three) fR[3] = rhoR * vx1R * vx3R - bx1 * bx3R;
+    fR[ip] = (rhoeR + ptR) * vx1R - bx1 * (bx1 * vx1R + bx2R * vx2R + bx3R * vx3R);
+    for (int iv = ias; iv < nv; ++iv) fR[iv] = UR[iv] * vx1R;
+    fbR[0] = 0.0; fbR[1] = vx1R * bx2R - vx2R * bx1; fbR[2] = vx1R * bx3R - vx3R * bx1;
+    double dummy_h = 1.0 / (sR - sL), phi_h = sL * sR;
+    for (int iv = 0; iv < nv; ++iv) flux[iv] = dummy_h * (sR * fL[iv] - sL * fR[iv] + phi_h * (UR[iv] - UL[iv]));
+    for (int iv = 0; iv < (three ? 3 : 2); ++iv)
+      fluxb[iv] = dummy_h * (sR * fbL[iv] - sL * fbR[iv] + phi_h * (UbR[iv] - UbL[iv]));
+    return;
   }
   double pstar = (dsuR * rhoR * ptL - dsuL * rhoL * ptR - phi * rhoL * rhoR * dsuR * dsuL * (vx1L - vx1R)) * inv_temp1;
   double rhostarL = rhoL * dsuL / dsumL, rhostarR = rhoR * dsuR / dsumR;
@@ -520,6 +580,37 @@ static void rk_coeffs(int stages, double c[3][3]) {
   }
 }
 
+/* ---------------------------------------------------------------- shock detector */
+/* USE_SHOCK_FLATTENING (source.F90:8073-8136): a cell whose summed central pressure jumps
+ * |p(+1) - p(-1)| over all directions exceed eps_sf times its own pressure flags itself and its
+ * 3x3(x3) neighbours.  Pressures are full values (deviation + equilibrium under WB), ghosts
+ * included; cells lx-2..ux+2 are tested, so the test reads 3 ghost layers.  The flags of cells
+ * lx-1..ux+1 are what the sweeps read; every flag is recomputed here, each stage. */
+static void detect_shocks(phlo_grid *g, scr_t *S) {
+  const int ip = IP(g), three = g->sdims == 3;
+  shp sc = cellg(g, g->nvars), s1 = cellg(g, 1), s3c = cellg(g, 3);
+  const int kl = three ? -1 : 1, ku = three ? g->nx3 + 2 : g->nx3;
+  memset(S->flat, 0, sizeof(double) * (size_t)ssize(&s1));
+#define PF(i, j, k) (g->wb ? g->prim[OFF(&sc, ip, i, j, k)] + g->eq_prim_cc[OFF(&s3c, 1, i, j, k)] \
+                           : g->prim[OFF(&sc, ip, i, j, k)])
+  for (int k = kl; k <= ku; ++k)
+    for (int j = -1; j <= g->nx2 + 2; ++j)
+      for (int i = -1; i <= g->nx1 + 2; ++i) {
+        double tmp;
+        if (three)
+          tmp = (fabs(PF(i, j, k + 1) - PF(i, j, k - 1)) + fabs(PF(i, j + 1, k) - PF(i, j - 1, k)) +
+                 fabs(PF(i + 1, j, k) - PF(i - 1, j, k))) / PF(i, j, k);
+        else
+          tmp = (fabs(PF(i, j + 1, k) - PF(i, j - 1, k)) + fabs(PF(i + 1, j, k) - PF(i - 1, j, k))) / PF(i, j, k);
+        if (tmp > g->eps_sf) {
+          for (int c = three ? -1 : 0; c <= (three ? 1 : 0); ++c)
+            for (int b = -1; b <= 1; ++b)
+              for (int a = -1; a <= 1; ++a) S->flat[OFF(&s1, 0, i + a, j + b, k + c)] = 1.0;
+        }
+      }
+#undef PF
+}
+
 /* ---------------------------------------------------------------- one directional sweep */
 static void sweep(phlo_grid *g, scr_t *S, int dir) {
   const int nv = g->nvars, ip = IP(g), sd = g->sdims, G = g->ngc;
@@ -548,6 +639,7 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
     double *fb = (double *)malloc(sizeof(double) * 3 * (size_t)(nl + 2));
     double *gL = (double *)malloc(sizeof(double) * 2 * (size_t)(nl + 2));
     double *gR = (double *)malloc(sizeof(double) * 2 * (size_t)(nl + 2));
+    int *Fl = (int *)malloc(sizeof(int) * (size_t)(nl + 2));
 #pragma omp for schedule(static)
     for (long line = 0; line < nlines; ++line) {
       int t0 = 1 + (int)(line % n[ta]), t1 = 1 + (int)(line / n[ta]);
@@ -564,6 +656,11 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
         if (helm_nf) Gf[(m + 2) * 2] = g->temp[OFF(&st1, 0, c[0], c[1], c[2])];
       }
 #define WC(m) (W + ((m) + 2) * nv)
+      /* is_flattened of cells 0..n+1 of the line (USE_SHOCK_FLATTENING) */
+      for (int m = 0; m <= nl + 1; ++m) {
+        c[dir] = m;
+        Fl[m] = g->sf ? (int)S->flat[OFF(&st1, 0, c[0], c[1], c[2])] : 0;
+      }
       /* reconstruction over cells 0..n+1: face f=m is the low face of cell m */
       for (int m = 0; m <= nl + 1; ++m) {
         for (int iv = 0; iv < nv; ++iv) {
@@ -571,6 +668,8 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
           double lo, hi;
           rec_cell(g->rec, limited, g->rec == 2 ? WC(m - 2)[iv] : 0.0, WC(m - 1)[iv], WC(m)[iv], WC(m + 1)[iv],
                    g->rec == 2 ? WC(m + 2)[iv] : 0.0, &lo, &hi);
+          /* a flagged cell falls back to LIM2ND PLM (source.F90:8743-8789, 9635-9668) */
+          if (Fl[m]) rec_cell(0, 1, 0.0, WC(m - 1)[iv], WC(m)[iv], WC(m + 1)[iv], 0.0, &lo, &hi);
           if (m >= 1) qR[m * nv + iv] = lo;
           if (m <= nl) qL[(m + 1) * nv + iv] = hi;
         }
@@ -584,6 +683,7 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
             double lo, hi;
             rec_cell(g->rec, g->rec == 2, g->rec == 2 ? BC(m - 2, iv) : 0.0, BC(m - 1, iv), BC(m, iv), BC(m + 1, iv),
                      g->rec == 2 ? BC(m + 2, iv) : 0.0, &lo, &hi);
+            if (Fl[m]) rec_cell(0, 1, 0.0, BC(m - 1, iv), BC(m, iv), BC(m + 1, iv), 0.0, &lo, &hi);
             if (m >= 1) bR[m * 3 + iv] = lo;
             if (m <= nl) bL[(m + 1) * 3 + iv] = hi;
           }
@@ -627,11 +727,15 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       /* FASTEOS gamma_e, gamma_c reconstruction + WB add-back (source.F90:8497-8729) */
       if (g->fasteos) {
 #define GF(m, iv) Gf[((m) + 2) * 2 + (iv)]
+        /* the x1 sweep flattens its gammas after the WB add-back (below); x2 and x3 before it
+         * (source.F90:9993-10031, 11135-11173) */
+        const int sf_late = g->sf && g->wb && dir == 0;
         for (int iv = 0; iv < 2; ++iv) {
           for (int m = 0; m <= nl + 1; ++m) {
             double lo, hi;
             rec_cell(g->rec, g->rec == 2, g->rec == 2 ? GF(m - 2, iv) : 0.0, GF(m - 1, iv), GF(m, iv), GF(m + 1, iv),
                      g->rec == 2 ? GF(m + 2, iv) : 0.0, &lo, &hi);
+            if (Fl[m] && !sf_late) rec_cell(0, 1, 0.0, GF(m - 1, iv), GF(m, iv), GF(m + 1, iv), 0.0, &lo, &hi);
             if (m >= 1) gR[m * 2 + iv] = lo;
             if (m <= nl) gL[(m + 1) * 2 + iv] = hi;
           }
@@ -642,6 +746,26 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
             double p_eq = g->eq_gammae_x[dir][OFF(&sf1, 0, c[0], c[1], c[2])];
             gL[f * 2] = gL[f * 2] + p_eq;
             gR[f * 2] = gR[f * 2] + p_eq;
+          }
+        }
+        if (sf_late) {
+          /* x1 sweep (source.F90:8829-8872): a flagged cell's PLM gammas replace its edge values
+           * without the equilibrium gamma_e, and eq_gammae_x1 of that face is added once more to
+           * the value on the OTHER side of the face; cells in ascending order */
+          for (int m = 0; m <= nl + 1; ++m) {
+            if (!Fl[m]) continue;
+            double lo[2], hi[2];
+            for (int iv = 0; iv < 2; ++iv) rec_cell(0, 1, 0.0, GF(m - 1, iv), GF(m, iv), GF(m + 1, iv), 0.0, &lo[iv], &hi[iv]);
+            if (m >= 1) {
+              for (int iv = 0; iv < 2; ++iv) gR[m * 2 + iv] = lo[iv];
+              c[dir] = m;
+              gL[m * 2] = gL[m * 2] + g->eq_gammae_x[dir][OFF(&sf1, 0, c[0], c[1], c[2])];
+            }
+            if (m <= nl) {
+              for (int iv = 0; iv < 2; ++iv) gL[(m + 1) * 2 + iv] = hi[iv];
+              c[dir] = m + 1;
+              gR[(m + 1) * 2] = gR[(m + 1) * 2] + g->eq_gammae_x[dir][OFF(&sf1, 0, c[0], c[1], c[2])];
+            }
           }
         }
       }
@@ -656,10 +780,12 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       for (int f = 1; f <= nl + 1; ++f) {
         const int thermo = g->fasteos || helm_nf;
         const double *gl = thermo ? gL + f * 2 : NULL, *gr = thermo ? gR + f * 2 : NULL;
+        const int flat = Fl[f - 1] || Fl[f]; /* source.F90:8732-8739 */
         if (g->mhd)
-          phlo_riemann_mhd(g, qL + f * nv, qR + f * nv, bL + f * 3, bR + f * 3, gl, gr, fx + f * nv, fb + f * 3);
+          phlo_riemann_mhd(g, qL + f * nv, qR + f * nv, bL + f * 3, bR + f * 3, gl, gr, fx + f * nv, fb + f * 3,
+                           flat);
         else
-          phlo_riemann_hydro(g, qL + f * nv, qR + f * nv, gl, gr, fx + f * nv);
+          phlo_riemann_hydro(g, qL + f * nv, qR + f * nv, gl, gr, fx + f * nv, flat);
       }
       /* rotate fluxes back */
       for (int f = 1; f <= nl + 1; ++f) {
@@ -710,7 +836,7 @@ static void sweep(phlo_grid *g, scr_t *S, int dir) {
       }
 #undef WC
     }
-    free(W); free(Bc); free(Gf); free(qL); free(qR); free(fx); free(bL); free(bR); free(fb); free(gL); free(gR);
+    free(W); free(Bc); free(Gf); free(qL); free(qR); free(fx); free(bL); free(bR); free(fb); free(gL); free(gR); free(Fl);
   }
   (void)s1;
 }
@@ -1037,6 +1163,7 @@ void phlo_hydro_step(phlo_grid *g) {
     if (g->fasteos) fill_ghosts(g, g->gammaf, 2, 0);
     if (g->helm && !g->fasteos) fill_ghosts(g, g->temp, 1, 0);
 
+    if (g->sf) detect_shocks(g, &S);
     for (int dir = 0; dir < sd; ++dir) sweep(g, &S, dir);
 
     double a1 = rkc[irk][0], a2 = rkc[irk][1], a3 = rkc[irk][2] * g->dt;

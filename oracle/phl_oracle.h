@@ -48,9 +48,11 @@ typedef struct phlo_grid {
   int sdims, nx1, nx2, nx3, ngc, nas, nvars;
   int mhd, wb, gravity, etot, helm, fasteos;
   int rec;                /* reconstruction: 0 LIM2ND_REC, 1 PPH_REC, 2 LIM5TH_REC (ngc >= 3) */
+  int sf;                 /* USE_SHOCK_FLATTENING (ngc >= 3) */
   int riemann, rk_stages;
   int bc[3][2];           /* [dim][lower/upper] */
   double gm, mu, cfl, mach_cutoff, mach_ct;
+  double eps_sf;          /* eps_sf_make: pressure-jump threshold of the shock detector */
   double dx1, dx2, dx3, inv_dx1, inv_dx2, inv_dx3;
   double dt, smax, time;
   const phlo_helm *eos;
@@ -103,12 +105,13 @@ void phlo_eos_invert_batch(const phlo_helm *h, long n, const double *rho, const 
 /* ---- Riemann solvers for one face, in the normal frame (source/source.F90:13969-16260) ----
  * q*: nvars primitive face states; g*: (gammae, gammac) face values for USE_FASTEOS, the face
  * temperature guess in g*[0] for the Helmholtz EoS without USE_FASTEOS (helm_rhoP_given per
- * side), NULL otherwise; b*: 3 components (normal first), MHD only. */
+ * side), NULL otherwise; b*: 3 components (normal first), MHD only.  flat: the face is
+ * flattened (USE_SHOCK_FLATTENING): HLL flux instead of the selected solver. */
 void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
-                        const double *gL, const double *gR, double *flux);
+                        const double *gL, const double *gR, double *flux, int flat);
 void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
                       const double *bL, const double *bR, const double *gL, const double *gR,
-                      double *flux, double *fluxb);
+                      double *flux, double *fluxb, int flat);
 
 /* ---- step-level routines ---- */
 long phlo_scratch_doubles(const phlo_grid *g);

@@ -30,9 +30,10 @@ class _Grid(C.Structure):
     _fields_ = [
         ("sdims", C.c_int), ("nx1", C.c_int), ("nx2", C.c_int), ("nx3", C.c_int), ("ngc", C.c_int),
         ("nas", C.c_int), ("nvars", C.c_int), ("mhd", C.c_int), ("wb", C.c_int), ("gravity", C.c_int),
-        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("rec", C.c_int), ("riemann", C.c_int),
-        ("rk_stages", C.c_int), ("bc", (C.c_int * 2) * 3), ("gm", C.c_double), ("mu", C.c_double),
-        ("cfl", C.c_double), ("mach_cutoff", C.c_double), ("mach_ct", C.c_double), ("dx1", C.c_double),
+        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("rec", C.c_int), ("sf", C.c_int),
+        ("riemann", C.c_int), ("rk_stages", C.c_int), ("bc", (C.c_int * 2) * 3), ("gm", C.c_double), ("mu", C.c_double),
+        ("cfl", C.c_double), ("mach_cutoff", C.c_double), ("mach_ct", C.c_double), ("eps_sf", C.c_double),
+        ("dx1", C.c_double),
         ("dx2", C.c_double), ("dx3", C.c_double), ("inv_dx1", C.c_double), ("inv_dx2", C.c_double),
         ("inv_dx3", C.c_double), ("dt", C.c_double), ("smax", C.c_double), ("time", C.c_double),
         ("eos", C.POINTER(_Helm)), ("nthreads", C.c_int),
@@ -78,9 +79,9 @@ def load():
         lib.phlo_eos_bracket_guess.argtypes = [C.POINTER(_Helm), C.c_double, C.c_double, C.c_double, C.c_double,
                                                _P]
         lib.phlo_eos_bracket_guess.restype = C.c_int
-        lib.phlo_riemann_hydro.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P]
+        lib.phlo_riemann_hydro.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P, C.c_int]
         lib.phlo_riemann_hydro.restype = None
-        lib.phlo_riemann_mhd.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P, _P, _P, _P]
+        lib.phlo_riemann_mhd.argtypes = [C.POINTER(_Grid), _P, _P, _P, _P, _P, _P, _P, _P, C.c_int]
         lib.phlo_riemann_mhd.restype = None
         _lib = lib
     return _lib
@@ -166,6 +167,10 @@ class OracleGrid:
         g.helm = int(c.helmholtz)
         g.fasteos = int(c.helmholtz and c.fasteos)
         g.rec = {"lim2nd": 0, "pph": 1, "lim5th": 2}[c.rec]
+        g.sf = int(c.shock_flattening)
+        g.eps_sf = c.eps_sf
+        if c.shock_flattening and c.ngc < 3:
+            raise ValueError("USE_SHOCK_FLATTENING reads 3 ghost layers: ngc >= 3")
         g.riemann = self.RIEM[c.riemann]
         g.rk_stages = c.rk_stages
         for d in range(3):

@@ -122,7 +122,7 @@ __device__ __forceinline__ R sgn1(R x) { return copysign(R(1), x); }
 enum { EOS_IDEAL = 0, EOS_FAST = 1, EOS_GIVEN = 2 };
 template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R *gL, const R *gR,
-                                              R gm, R mach_cutoff, R *flux) {
+                                              R gm, R mach_cutoff, R *flux, bool flat = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const R gmm1 = gm - R(1), igmm1 = R(1) / gmm1;
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
@@ -148,6 +148,32 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
   R rhoestarL = rhostarL * (rhoeL * inv_rhoL + (ustar - vx1L) * (ustar + pL * inv_rhoL / dsuL));
   R rhostarR = rhoR * (dsuR / (sR - ustar));
   R rhoestarR = rhostarR * (rhoeR * inv_rhoR + (ustar - vx1R) * (ustar + pR * inv_rhoR / dsuR));
+  if (flat) {
+    // two-wave HLL flux on a face next to a detected shock (USE_SHOCK_FLATTENING,
+    // source.F90:15929-16010)
+    sL = fmin(R(0), sL);
+    sR = fmax(R(0), sR);
+    R UL[NV], UR[NV], fL[NV], fR[NV];
+    UL[0] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (DIM == 3) UL[3] = rhoL * vx3L; UL[IP] = rhoeL;
+    UR[0] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (DIM == 3) UR[3] = rhoR * vx3R; UR[IP] = rhoeR;
+    fL[0] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + pL; fL[2] = rhoL * vx1L * vx2L;
+    if (DIM == 3) fL[3] = rhoL * vx1L * vx3L;
+    fL[IP] = (rhoeL + pL) * vx1L;
+    fR[0] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + pR; fR[2] = rhoR * vx1R * vx2R;
+    if (DIM == 3) fR[3] = rhoR * vx1R * vx3R;
+    fR[IP] = (rhoeR + pR) * vx1R;
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) {
+      UL[iv] = rhoL * qL[iv];
+      UR[iv] = rhoR * qR[iv];
+      fL[iv] = UL[iv] * vx1L;
+      fR[iv] = UR[iv] * vx1R;
+    }
+    const R dummy = R(1) / (sR - sL), phi = sL * sR;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = dummy * (sR * fL[iv] - sL * fR[iv] + phi * (UR[iv] - UL[iv]));
+    return;
+  }
   if (RIEM == R_LHLLC) {
     R machL = sqrt(v2L) / cL, machR = sqrt(v2R) / cR;
     R chi = fmin(R(1), fmax(machL, machR));
@@ -200,7 +226,7 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
 template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *bL, const R *bR,
                                             const R *gL, const R *gR, R gm, R mach_cutoff,
-                                            R *flux, R *fluxb) {
+                                            R *flux, R *fluxb, bool flat = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const R gmm1 = gm - R(1), igmm1 = R(1) / gmm1;
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
@@ -254,6 +280,36 @@ __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *b
     } else {
       phi = R(1);
     }
+  }
+  if (flat) {
+    // HLL flux on a flattened face (USE_SHOCK_FLATTENING, source.F90:14386-14495)
+    sL = fmin(R(0), sL);
+    sR = fmax(R(0), sR);
+    R UL[NV], UR[NV], fL[NV], fR[NV];
+    UL[0] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (DIM == 3) UL[3] = rhoL * vx3L; UL[IP] = rhoeL;
+    UR[0] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (DIM == 3) UR[3] = rhoR * vx3R; UR[IP] = rhoeR;
+    fL[0] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + ptL - bx1_2; fL[2] = rhoL * vx1L * vx2L - bx1 * bx2L;
+    if (DIM == 3) fL[3] = rhoL * vx1L * vx3L - bx1 * bx3L;
+    fL[IP] = (rhoeL + ptL) * vx1L - bx1 * (bx1 * vx1L + bx2L * vx2L + bx3L * vx3L);
+    fR[0] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + ptR - bx1_2; fR[2] = rhoR * vx1R * vx2R - bx1 * bx2R;
+    if (DIM == 3) fR[3] = rhoR * vx1R * vx3R - bx1 * bx3R;
+    fR[IP] = (rhoeR + ptR) * vx1R - bx1 * (bx1 * vx1R + bx2R * vx2R + bx3R * vx3R);
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) {
+      UL[iv] = rhoL * qL[iv];
+      UR[iv] = rhoR * qR[iv];
+      fL[iv] = UL[iv] * vx1L;
+      fR[iv] = UR[iv] * vx1R;
+    }
+    const R UbL[3] = {bx1, bx2L, bx3L}, UbR[3] = {bx1, bx2R, bx3R};
+    const R fbL[3] = {R(0), vx1L * bx2L - vx2L * bx1, vx1L * bx3L - vx3L * bx1};
+    const R fbR[3] = {R(0), vx1R * bx2R - vx2R * bx1, vx1R * bx3R - vx3R * bx1};
+    const R dh = R(1) / (sR - sL), ph = sL * sR;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = dh * (sR * fL[iv] - sL * fR[iv] + ph * (UR[iv] - UL[iv]));
+#pragma unroll
+    for (int iv = 0; iv < DIM; ++iv) fluxb[iv] = dh * (sR * fbL[iv] - sL * fbR[iv] + ph * (UbR[iv] - UbL[iv]));
+    return;
   }
   R pstar = (dsuR * rhoR * ptL - dsuL * rhoL * ptR - phi * rhoL * rhoR * dsuR * dsuL * (vx1L - vx1R)) * inv_temp1;
   R rhostarL = rhoL * dsuL / dsumL, rhostarR = rhoR * dsuR / dsumR;

@@ -17,10 +17,12 @@ namespace phl {
 
 // FAST_: USE_FASTEOS (gamma_e, gamma_c reconstructed to the faces); without it the Helmholtz
 // configurations evaluate helm_rhoP_given per Riemann side from the face temperature guess
+// SF_: USE_SHOCK_FLATTENING (shock detector, LIM2ND PLM in flagged cells, HLL on their faces)
 template <int DIM_, int NV_, bool MHD_, bool HELM_, bool WB_, bool ETOT_, bool GRAV_, int RIEM_, bool FAST_ = HELM_,
-          int REC_ = REC_LIM2ND>
+          int REC_ = REC_LIM2ND, bool SF_ = false>
 struct Cfg {
   static constexpr int DIM = DIM_, NV = NV_, RIEM = RIEM_, REC = REC_;
+  static constexpr bool SF = SF_;
   // cells on each side of a face the reconstruction reads (3 for LIM5TH, 2 otherwise)
   static constexpr int SW = REC_ == REC_LIM5TH ? 3 : 2;
   static constexpr bool MHD = MHD_, HELM = HELM_, WB = WB_, ETOT = ETOT_, GRAV = GRAV_, FAST = HELM_ && FAST_;
@@ -69,6 +71,13 @@ struct Prm {
   float *femf[3], *fsgn[3], *fcor[3];
   float *fflux[3];  // FP32 face fluxes [NV][faces] per direction
   double *dflux[3]; // FP64 MHD face fluxes [NV][faces] per direction
+  // USE_SHOCK_FLATTENING: is_flattened of the cells -1..n per dimension (index + 1, bytes),
+  // the detector's marks of cells -2..n+1 (index + 2), the pressure equilibrium with its ghost
+  // layers (profile along x2 or full ghosted array, ghost offset sf_G), and eps_sf
+  unsigned char *sf_flag, *sf_mark;
+  const double *sf_eq_p;
+  int sf_G, sf_eq_profile;
+  double eps_sf;
 };
 
 enum { STAT_NEWTON_CALLS = 0, STAT_NEWTON_ITERS, STAT_NEWTON_NONCONV, STAT_NEWTON_CLAMP,
@@ -197,21 +206,44 @@ __device__ __forceinline__ void rec_face(const R *const c[6], int iv, bool limit
   }
 }
 
+// USE_SHOCK_FLATTENING: the left state of the face comes from the right edge of cell m-1
+// (c[1..3]), the right state from the left edge of cell m (c[2..4]); a flagged cell gives both
+// by LIM2ND PLM instead of the selected reconstruction (source.F90:8743-8827, 9635-9700,
+// 10765-10830).  With LIM2ND selected nothing changes.
+template <class C, typename R>
+__device__ __forceinline__ void flatten_face(const R *const c[6], int iv, bool fa, bool fb, R &qL, R &qR) {
+  if (C::REC == REC_LIM2ND) return;
+  R lo, hi;
+  if (fa) {
+    plm(c[1][iv], c[2][iv], c[3][iv], lo, hi);
+    qL = hi;
+  }
+  if (fb) {
+    plm(c[2][iv], c[3][iv], c[4][iv], lo, hi);
+    qR = lo;
+  }
+}
+
+// fa, fb: is_flattened of cells m-1 and m (always false without USE_SHOCK_FLATTENING)
 template <class C>
 __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, int fk, const double *const w[6],
                                           const double *const gmv[6], const double *const bc[6], double F[C::NV],
-                                          double Fb[3], double &rho_face_sum) {
+                                          double Fb[3], double &rho_face_sum, bool fa = false, bool fb = false) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
   double qL[NV], qR[NV];
 #pragma unroll
-  for (int iv = 0; iv < NV; ++iv) rec_face<C>(w, iv, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
+  for (int iv = 0; iv < NV; ++iv) {
+    rec_face<C>(w, iv, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
+    if (C::SF) flatten_face<C>(w, iv, fa, fb, qL[iv], qR[iv]);
+  }
   double bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
   if (C::MHD) {
 #pragma unroll
     for (int iv = 0; iv < C::DIM; ++iv) {
       if (iv == d) continue;
       rec_face<C>(bc, iv, C::REC == REC_LIM5TH, bL[iv], bR[iv]);
+      if (C::SF) flatten_face<C>(bc, iv, fa, fb, bL[iv], bR[iv]);
     }
     double bn = P.bf[d][face_lin(g, d, fi, fj, fk)];
     bL[d] = bn;
@@ -233,10 +265,10 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
       a = bR[0]; b = bR[1]; c = bR[2]; bR[0] = c; bR[1] = a; bR[2] = b;
     }
   }
-  long long fb = 0;
-  if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
+  long long fbg = 0;
+  if (C::WB || C::ETOT) fbg = bg_face(g, d, fi, fj, fk);
   if (C::WB) {
-    double rho_eq = __ldg(P.eq_rho_f[d] + fb), p_eq = __ldg(P.eq_p_f[d] + fb);
+    double rho_eq = __ldg(P.eq_rho_f[d] + fbg), p_eq = __ldg(P.eq_p_f[d] + fbg);
     qL[0] = qL[0] + rho_eq;
     qR[0] = qR[0] + rho_eq;
     qL[IP] = qL[IP] + p_eq;
@@ -244,12 +276,39 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   }
   double gL[2] = {0, 0}, gR[2] = {0, 0};
   if (C::FAST) {
+    // the x1 sweep flattens the gammas after the WB add-back, x2 and x3 before it
+    const bool late = C::SF && C::WB && d == 0;
 #pragma unroll
-    for (int iv = 0; iv < 2; ++iv) rec_face<C>(gmv, iv, C::REC == REC_LIM5TH, gL[iv], gR[iv]);
+    for (int iv = 0; iv < 2; ++iv) {
+      rec_face<C>(gmv, iv, C::REC == REC_LIM5TH, gL[iv], gR[iv]);
+      if (C::SF && !late) flatten_face<C>(gmv, iv, fa, fb, gL[iv], gR[iv]);
+    }
     if (C::WB) {
-      double ge = __ldg(P.eq_ge_f[d] + fb);
+      double ge = __ldg(P.eq_ge_f[d] + fbg);
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
+      if (late) {
+        // x1 sweep (source.F90:8829-8872), reproduced as written: a flagged cell's PLM gammas
+        // replace its edge values without the equilibrium gamma_e, and eq_gammae_x1 of the
+        // face is added once more to the value on the other side; cell m-1 before cell m
+        double lo, hi;
+        if (fa) {
+#pragma unroll
+          for (int iv = 0; iv < 2; ++iv) {
+            plm(gmv[1][iv], gmv[2][iv], gmv[3][iv], lo, hi);
+            gL[iv] = hi;
+          }
+          gR[0] = gR[0] + ge;
+        }
+        if (fb) {
+#pragma unroll
+          for (int iv = 0; iv < 2; ++iv) {
+            plm(gmv[2][iv], gmv[3][iv], gmv[4][iv], lo, hi);
+            gR[iv] = lo;
+          }
+          gL[0] = gL[0] + ge;
+        }
+      }
     }
   } else if (C::HELM) {
     // Helmholtz without USE_FASTEOS: helm_rhoP_given on each side of the face from the guess
@@ -266,9 +325,9 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   }
   const double gm = P.g.gm, mc = P.g.mach_cutoff;
   if (C::MHD) {
-    riemann_mhd<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb);
+    riemann_mhd<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb, C::SF && (fa || fb));
   } else {
-    riemann_hydro<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, gm, mc, F);
+    riemann_hydro<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, gm, mc, F, C::SF && (fa || fb));
   }
   // back to the lab frame
   if (d == 1) {
@@ -280,8 +339,8 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   }
   rho_face_sum = qL[0] + qR[0];
   // MHD: the EMF/sign are taken before the WB momentum fix (source.F90:8926-8959)
-  if (C::WB) F[1 + d] = F[1 + d] - __ldg(P.eq_p_f[d] + fb);
-  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.phi_f[d] + fb);
+  if (C::WB) F[1 + d] = F[1 + d] - __ldg(P.eq_p_f[d] + fbg);
+  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.phi_f[d] + fbg);
 }
 
 // EMF components of a face flux and the mass-flux sign (source.F90:8926-8951)
@@ -299,6 +358,90 @@ __device__ __forceinline__ void store_face_emf(const Prm &P, int d, long long fi
   if (mach > g.mach_ct) sgn = 1.0;
   if (mach < -g.mach_ct) sgn = -1.0;
   P.sgnf[d][fidx] = sgn;
+}
+
+// --------------------------------------------------------------------- shock detector
+// USE_SHOCK_FLATTENING (source.F90:8073-8136).  is_flattened is kept for cells -1..n of every
+// dimension (the cells whose edges the faces read), the detector's marks for cells -2..n+1.
+template <class C>
+__device__ __forceinline__ long long sf_flag_index(const Geo &g, int i, int j, int k) {
+  return (long long)(i + 1) + (long long)(g.nx[0] + 2) * ((long long)(j + 1) + (long long)(g.nx[1] + 2) * (C::DIM == 3 ? k + 1 : 0));
+}
+template <class C>
+__host__ __device__ __forceinline__ long long sf_flag_cells(const Geo &g) {
+  return (long long)(g.nx[0] + 2) * (g.nx[1] + 2) * (C::DIM == 3 ? g.nx[2] + 2 : 1);
+}
+template <class C>
+__host__ __device__ __forceinline__ long long sf_mark_cells(const Geo &g) {
+  return (long long)(g.nx[0] + 4) * (g.nx[1] + 4) * (C::DIM == 3 ? g.nx[2] + 4 : 1);
+}
+
+// full pressure of a (possibly ghost) cell as the reference forms it: the communicated
+// deviation plus the equilibrium stored for that ghost cell under WB
+template <class C>
+__device__ __forceinline__ double sf_pressure(const Prm &P, int i, int j, int k) {
+  const Geo &g = P.g;
+  bool f = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f) : 0;
+  double p = __ldg(P.Win + (long long)C::IP * g.N + lin(g, si, sj, sk));
+  if (C::WB) {
+    p = p - __ldg(P.eq_p_cc + bg_cc(g, si, sj, sk));
+    const int G = P.sf_G, G3 = C::DIM == 3 ? P.sf_G : 0;
+    long long e = P.sf_eq_profile ? (long long)(j + G)
+                                  : (long long)(i + G) + (long long)(g.nx[0] + 2 * G) *
+                                        ((long long)(j + G) + (long long)(g.nx[1] + 2 * G) * (k + G3));
+    p = p + __ldg(P.sf_eq_p + e);
+  }
+  return p;
+}
+
+// marks: summed central pressure jumps over all directions > eps_sf * p, cells -2..n+1
+template <class C>
+__global__ void __launch_bounds__(256) k_sf_mark(Prm P) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  const long long n = sf_mark_cells<C>(g);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int m0 = g.nx[0] + 4, m1 = g.nx[1] + 4;
+  const int i = (int)(t % m0) - 2, j = (int)((t / m0) % m1) - 2;
+  const int k = C::DIM == 3 ? (int)(t / ((long long)m0 * m1)) - 2 : 0;
+  double tmp;
+  if (C::DIM == 3)
+    tmp = (fabs(sf_pressure<C>(P, i, j, k + 1) - sf_pressure<C>(P, i, j, k - 1)) +
+           fabs(sf_pressure<C>(P, i, j + 1, k) - sf_pressure<C>(P, i, j - 1, k)) +
+           fabs(sf_pressure<C>(P, i + 1, j, k) - sf_pressure<C>(P, i - 1, j, k))) /
+          sf_pressure<C>(P, i, j, k);
+  else
+    tmp = (fabs(sf_pressure<C>(P, i, j + 1, k) - sf_pressure<C>(P, i, j - 1, k)) +
+           fabs(sf_pressure<C>(P, i + 1, j, k) - sf_pressure<C>(P, i - 1, j, k))) /
+          sf_pressure<C>(P, i, j, k);
+  P.sf_mark[t] = tmp > P.eps_sf ? 1 : 0;
+}
+
+// is_flattened of cells -1..n: a mark anywhere in the 3x3(x3) neighbourhood
+template <class C>
+__global__ void __launch_bounds__(256) k_sf_flag(Prm P) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  const long long n = sf_flag_cells<C>(g);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int f0 = g.nx[0] + 2, f1 = g.nx[1] + 2, m0 = g.nx[0] + 4, m1 = g.nx[1] + 4;
+  const int i = (int)(t % f0) - 1, j = (int)((t / f0) % f1) - 1;
+  const int k = C::DIM == 3 ? (int)(t / ((long long)f0 * f1)) - 1 : 0;
+  unsigned char any = 0;
+#pragma unroll
+  for (int c = (C::DIM == 3 ? -1 : 0); c <= (C::DIM == 3 ? 1 : 0); ++c)
+#pragma unroll
+    for (int b = -1; b <= 1; ++b)
+#pragma unroll
+      for (int a = -1; a <= 1; ++a)
+        any |= P.sf_mark[(long long)(i + a + 2) + (long long)m0 * ((long long)(j + b + 2) +
+                                                                   (long long)m1 * (C::DIM == 3 ? k + c + 2 : 0))];
+  P.sf_flag[t] = any;
 }
 
 // --------------------------------------------------------------------- face fluxes
@@ -335,8 +478,13 @@ __global__ void __launch_bounds__(128) k_face(Prm P, int d) {
   const double *const wp[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
   const double *const gp[6] = {gmv[0], gmv[1], gmv[2], gmv[3], gmv[4], gmv[5]};
   const double *const bp[6] = {bc[0], bc[1], bc[2], bc[3], bc[4], bc[5]};
+  bool fa = false, fb = false;
+  if (C::SF) {
+    fa = P.sf_flag[sf_flag_index<C>(g, fi - (d == 0), fj - (d == 1), fk - (d == 2))] != 0;
+    fb = P.sf_flag[sf_flag_index<C>(g, fi, fj, fk)] != 0;
+  }
   double F[NV], Fb[3], rs;
-  face_flux<C>(P, d, fi, fj, fk, wp, gp, bp, F, Fb, rs);
+  face_flux<C>(P, d, fi, fj, fk, wp, gp, bp, F, Fb, rs, fa, fb);
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.dflux[d][(long long)iv * nf + f] = F[iv];
   if (C::MHD) store_face_emf<C>(P, d, f, Fb, F[0], rs, P.scal[2]);

@@ -41,6 +41,10 @@ struct RunnerT : Runner {
   void stage(const Prm &P, cudaStream_t s) override {
     const Geo &g = P.g;
     // each face once, then (MHD) corners and face B, then divergence + RK + cons->prim per cell
+    if constexpr (C::SF) {
+      k_sf_mark<C><<<nblk(sf_mark_cells<C>(g), 256), 256, 0, s>>>(P);
+      k_sf_flag<C><<<nblk(sf_flag_cells<C>(g), 256), 256, 0, s>>>(P);
+    }
     for (int d = 0; d < C::DIM; ++d) k_face<C><<<nblk(nfaces_host(g, d), 128), 128, 0, s>>>(P, d);
     if constexpr (C::MHD) {
       for (int a = 0; a < 3; ++a) {
@@ -63,38 +67,51 @@ struct RunnerT : Runner {
 };
 
 // Instantiated option sets: (dims, nvars, MHD, Helmholtz, stratified = WB+ETOT+gravity, Riemann
-// solver, USE_FASTEOS, reconstruction).  Other combinations return PHL_E_UNSUPPORTED.
-#define PHL_RUNNER_LIST(X)                                  \
-  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
-  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND)   \
-  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND)   \
-  X(2, 4, false, false, true, R_HLLC, false, REC_LIM2ND)    \
-  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND)    \
-  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
-  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
-  X(2, 6, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
-  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
-  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND)   \
-  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND)    \
-  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
-  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
-  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND)      \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
-  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND)       \
-  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND)    \
-  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND)     \
-  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND)     \
-  X(2, 4, true, false, false, R_HLLD, false, REC_PPH)       \
-  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH)    \
-  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH)        \
-  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM5TH)     \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH)         \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH)      
+// solver, USE_FASTEOS, reconstruction, USE_SHOCK_FLATTENING).  Other combinations return
+// PHL_E_UNSUPPORTED.
+#define PHL_RUNNER_LIST(X)                                         \
+  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND, false)  \
+  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND, false)   \
+  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND, false)   \
+  X(2, 4, false, false, true, R_HLLC, false, REC_LIM2ND, false)    \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND, false)    \
+  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND, false)   \
+  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND, false)     \
+  X(2, 6, true, true, true, R_LHLLD, true, REC_LIM2ND, false)      \
+  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND, false)  \
+  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND, false)   \
+  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND, false)    \
+  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND, false)   \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND, false)     \
+  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND, false)      \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND, false)      \
+  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND, false)       \
+  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND, false)    \
+  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND, false)     \
+  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND, false)     \
+  X(2, 4, true, false, false, R_HLLD, false, REC_PPH, false)       \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH, false)    \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH, false)        \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM5TH, false)     \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH, false)         \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH, false)      \
+  X(2, 5, false, false, false, R_HLLC, false, REC_LIM2ND, true)    \
+  X(2, 5, false, false, false, R_LHLLC, false, REC_LIM2ND, true)   \
+  X(2, 5, false, false, false, R_HLLC, false, REC_PPH, true)       \
+  X(2, 5, false, false, false, R_HLLC, false, REC_LIM5TH, true)    \
+  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND, true)    \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND, true)     \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH, true)     \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND, true)      \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH, true)         \
+  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND, true)     \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND, true)
 
-Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec) {
-#define X(D, N, M, H, S, R, F, REC)                                                                           \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) && rec == REC) \
-    return new RunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC>>();
+Runner *make_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec, bool sf) {
+#define X(D, N, M, H, S, R, F, REC, SF)                                                                      \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) &&         \
+      rec == REC && sf == SF)                                                                                 \
+    return new RunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC, SF>>();
   PHL_RUNNER_LIST(X)
 #undef X
   return nullptr;
@@ -184,6 +201,10 @@ struct phl_ctx {
   float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
   float *fflux[3] = {};
   double *dflux[3] = {};                                                               // FP64 MHD
+  // USE_SHOCK_FLATTENING: flags, detector marks, ghosted pressure equilibrium (see Prm)
+  unsigned char *sf_flag = nullptr, *sf_mark = nullptr;
+  double *sf_eq_p = nullptr;
+  int sf_eq_profile = 0;
   // scalars
   double *scal = nullptr;
   unsigned long long *smax_bits = nullptr;
@@ -276,6 +297,12 @@ struct phl_ctx {
     }
     P.bcc_in = bcc;
     P.bcc_out = bcc;
+    P.sf_flag = sf_flag;
+    P.sf_mark = sf_mark;
+    P.sf_eq_p = sf_eq_p;
+    P.sf_G = cfg.ngc;
+    P.sf_eq_profile = sf_eq_profile;
+    P.eps_sf = cfg.eps_sf;
     P.scal = scal;
     P.smax_bits = smax_bits;
     P.active = active;
@@ -353,6 +380,14 @@ int check_cfg(const phl_config *c) {
   if (c->precision != PHL_FP64 && c->precision != PHL_FP32_SPLIT) return PHL_E_INVALID;
   if (c->reconstruction < PHL_REC_LIM2ND || c->reconstruction > PHL_REC_LIM5TH) return PHL_E_INVALID;
   if (c->reconstruction == PHL_REC_LIM5TH && c->ngc < 3) return PHL_E_INVALID;
+  if (c->flags & PHL_SHOCK_FLATTENING) {
+    // the detector tests cells lx-2..ux+2 with central differences: 3 ghost layers
+    if (c->ngc < 3 || !(c->eps_sf == c->eps_sf)) return PHL_E_INVALID;
+    if (c->precision != PHL_FP64) {
+      g_last_error = "USE_SHOCK_FLATTENING is built for PHL_FP64";
+      return PHL_E_UNSUPPORTED;
+    }
+  }
   // the step's Newton starts from the previous stage's temperature (the reference's warm start);
   // the learned guess is offered by the batch inversion entry points only
   if (c->eos_guess == PHL_GUESS_MLP) {
@@ -426,7 +461,8 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   if (c->split)
     c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction));
   else
-    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction));
+    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction,
+                                (cfg->flags & PHL_SHOCK_FLATTENING) != 0));
   if (!c->runner) return PHL_E_UNSUPPORTED;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   Geo &g = c->geo;
@@ -461,6 +497,13 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
       if ((rc = c->alloc(&c->Wf[q], (size_t)nv * N))) return rc;
       if (helm && (rc = c->alloc(&c->gf[q], (size_t)2 * N))) return rc;
     }
+  }
+  if (cfg->flags & PHL_SHOCK_FLATTENING) {
+    const long long nz2 = cfg->sdims == 3 ? 1 : 0;
+    long long nflag = (long long)(cfg->nx1 + 2) * (cfg->nx2 + 2) * (cfg->nx3 + 2 * nz2);
+    long long nmark = (long long)(cfg->nx1 + 4) * (cfg->nx2 + 4) * (cfg->nx3 + 4 * nz2);
+    if ((rc = c->alloc(&c->sf_flag, (size_t)nflag))) return rc;
+    if ((rc = c->alloc(&c->sf_mark, (size_t)nmark))) return rc;
   }
   if (mhd) {
     if ((rc = c->alloc(&c->bcc, (size_t)3 * N))) return rc;
@@ -688,6 +731,22 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
         CK(cudaStreamSynchronize(s));
       }
     }
+  }
+  if ((c.flags & PHL_SHOCK_FLATTENING) && strat && f->eq_prim_cc) {
+    // the shock detector reads the pressure equilibrium of 3 ghost layers as the caller set
+    // them: kept as a profile along x2 when it is one over the ghosted array, else in full
+    std::vector<double> prof;
+    bool pr = extract_profile(f->eq_prim_cc, 3, 1, n1, n2, n3, 0, 0, 0, n1, n2, n2, prof);
+    size_t ne = pr ? (size_t)n2 : (size_t)Ng;
+    if (!ctx->sf_eq_p && (rc = ctx->alloc(&ctx->sf_eq_p, (size_t)Ng))) return rc;
+    std::vector<double> full;
+    if (!pr) {
+      full.resize(ne);
+      for (size_t q = 0; q < ne; ++q) full[q] = f->eq_prim_cc[3 * q + 1];
+    }
+    CK(cudaMemcpyAsync(ctx->sf_eq_p, pr ? prof.data() : full.data(), sizeof(double) * ne, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // host vectors go out of scope
+    ctx->sf_eq_profile = pr ? 1 : 0;
   }
   if (ctx->split && strat && f->eq_prim_cc && (rc = ctx->scale_background(helm))) return rc;
   if (ctx->split && f->eint && (!strat || ctx->bg_uploaded || f->eq_prim_cc)) {

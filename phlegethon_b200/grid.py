@@ -24,6 +24,7 @@ FLAG_EVOLVE_ETOT = 1 << 3
 FLAG_HELMHOLTZ = 1 << 4
 FLAG_FASTEOS = 1 << 5
 FLAG_ADVECT_YE_IABAR = 1 << 6
+FLAG_SHOCK_FLATTENING = 1 << 7
 
 PRECISION = {"fp64": 0, "fp32_split": 1}
 GUESS = {"warm": 0, "mlp": 1, "bracket": 2}
@@ -46,6 +47,8 @@ class Config:
                                      # instead of helm_rhoP_given per Riemann side
     riemann: str = "lhllc"
     rec: str = "lim2nd"              # LIM2ND_REC, PPH_REC or LIM5TH_REC (needs ngc >= 3)
+    shock_flattening: bool = False   # USE_SHOCK_FLATTENING (needs ngc >= 3)
+    eps_sf: float = 0.25             # eps_sf_make
     rk_stages: int = 3
     bc: list = field(default_factory=lambda: [["periodic", "periodic"]] * 3)
     precision: str = "fp64"
@@ -88,6 +91,8 @@ class Config:
             f |= FLAG_HELMHOLTZ | FLAG_ADVECT_YE_IABAR
             if self.fasteos:
                 f |= FLAG_FASTEOS
+        if self.shock_flattening:
+            f |= FLAG_SHOCK_FLATTENING
         return f
 
     @property

@@ -79,12 +79,12 @@ def analytic_temperature(rho, p, abar, zbar, T0=1e8):
 
 
 # ------------------------------------------------------------------------------ config 1
-def hot_bubble_2d(n=256, riemann="lhllc", seed=None):
+def hot_bubble_2d(n=256, riemann="lhllc", seed=None, shock_flattening=False, eps_sf=0.25):
     """2D hot bubble: [0,1]^2, periodic x / reflecting y, g = -1 in y, isothermal atmosphere
     rho = exp(-y/H), H = 0.5, p = rho*H*|g|, Gaussian temperature bump
     dT/T = 0.05 exp(-r^2/0.1^2) at (0.5, 0.25) in pressure equilibrium; ideal gas gamma = 5/3."""
-    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=2, nas=0, wb=True, gravity=True, etot=True,
-                 riemann=riemann, rk_stages=3,
+    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=3 if shock_flattening else 2, nas=0, wb=True, gravity=True,
+                 etot=True, riemann=riemann, rk_stages=3, shock_flattening=shock_flattening, eps_sf=eps_sf,
                  bc=[["periodic", "periodic"], ["reflective", "reflective"], ["periodic", "periodic"]],
                  x1l=0.0, x1u=1.0, x2l=0.0, x2u=1.0, x3l=0.0, x3u=1.0, gamma_ad=5.0 / 3.0, mu=1.0,
                  cfl=0.8, mach_cutoff=1e-4)
@@ -116,11 +116,11 @@ def hot_bubble_2d(n=256, riemann="lhllc", seed=None):
 
 
 # ------------------------------------------------------------------------------ config 2
-def orszag_tang_2d(n=1024, riemann="hlld", rec="lim2nd"):
+def orszag_tang_2d(n=1024, riemann="hlld", rec="lim2nd", shock_flattening=False, eps_sf=0.25):
     """Orszag-Tang vortex on the periodic unit square (tests/orszag-tang/app.F90:13-79; the
     reference's test runs it with LIM5TH_REC, tests/orszag-tang/Makefile:29)."""
-    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=3 if rec == "lim5th" else 2, nas=0, mhd=True, riemann=riemann,
-                 rec=rec, rk_stages=3,
+    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=3 if (rec == "lim5th" or shock_flattening) else 2, nas=0,
+                 mhd=True, riemann=riemann, rec=rec, shock_flattening=shock_flattening, eps_sf=eps_sf, rk_stages=3,
                  bc=[["periodic", "periodic"]] * 3, gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8,
                  mach_cutoff=1e-4, mach_ct=1e-6)
     h = HostGrid(cfg)
@@ -143,13 +143,35 @@ def orszag_tang_2d(n=1024, riemann="hlld", rec="lim2nd"):
     return cfg, h
 
 
+def blast_2d(n=128, riemann="hllc", rec="lim2nd", shock_flattening=True, eps_sf=0.25, p_in=10.0, p_out=0.1,
+             nas=1):
+    """Cylindrical blast wave on the periodic unit square: rho = 1, v = 0, p = p_in inside
+    r < 0.1 of the centre and p_out outside, one passive scalar marking the hot gas; ideal gas
+    gamma = 5/3.  A strong shock for the shock flattener (USE_SHOCK_FLATTENING)."""
+    cfg = Config(sdims=2, nx1=n, nx2=n, nx3=1, ngc=3, nas=nas, riemann=riemann, rec=rec,
+                 shock_flattening=shock_flattening, eps_sf=eps_sf, rk_stages=3,
+                 bc=[["periodic", "periodic"]] * 3, gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8, mach_cutoff=1e-4)
+    h = HostGrid(cfg)
+    x, y, _ = h.coords()
+    r2 = (x - 0.5) ** 2 + (y - 0.5) ** 2
+    inside = r2 < 0.01
+    h.prim[0] = 1.0
+    h.prim[1] = 0.0
+    h.prim[2] = 0.0
+    h.prim[3] = np.where(inside, p_in, p_out)
+    for iv in range(nas):
+        h.prim[4 + iv] = np.where(inside, 1.0, 0.0)
+    h.temp[...] = h.prim[3] / (CONST_RGAS * h.prim[0])
+    return cfg, h
+
+
 # ------------------------------------------------------------------------------ configs 3 / 5
 STRAT_ABAR = 13.7
 STRAT_ZBAR = 6.9
 
 
 def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, seed=12345,
-                  riemann=None, table=X2_TABLE, fasteos=True, rec="lim2nd"):
+                  riemann=None, table=X2_TABLE, fasteos=True, rec="lim2nd", shock_flattening=False, eps_sf=0.25):
     """3D stratified convection box with the Helmholtz EoS.
 
     x2 is vertical (reflecting walls), x1 and x3 periodic.  rho_eq(y) falls exponentially from
@@ -159,7 +181,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     counter-based hash (seed).  With mhd=True a uniform horizontal B_x1 of plasma beta `beta` at
     mid-height is added and the LHLLD solver with constrained transport is used.  fasteos=False
     selects the Helmholtz path without USE_FASTEOS (helm_rhoP_given per Riemann side); rec picks
-    the reconstruction (lim2nd, pph, lim5th; lim5th uses 3 ghost layers).
+    the reconstruction (lim2nd, pph, lim5th; lim5th uses 3 ghost layers); shock_flattening
+    enables USE_SHOCK_FLATTENING with threshold eps_sf (3 ghost layers).
     """
     ny = n if ny is None else ny
     nz = n if nz is None else nz
@@ -172,8 +195,10 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     p_top = float(analytic_pressure(rho_top, 1.0e8, abar, zbar))
     p_bot = float(analytic_pressure(rho_bot, 3.0e8, abar, zbar))
     g = (p_bot - p_top) / (rho_bot * Hrho * (1.0 - rho_top / rho_bot))
-    cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=3 if rec == "lim5th" else 2, nas=2, mhd=mhd, wb=True,
-                 gravity=True, etot=True, rec=rec, helmholtz=True, fasteos=fasteos, riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
+    cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=3 if (rec == "lim5th" or shock_flattening) else 2, nas=2,
+                 mhd=mhd, wb=True, gravity=True, etot=True, rec=rec, helmholtz=True, fasteos=fasteos,
+                 shock_flattening=shock_flattening, eps_sf=eps_sf,
+                 riemann=riemann or ("lhlld" if mhd else "lhllc"), rk_stages=3,
                  bc=[["periodic", "periodic"], ["reflective", "reflective"], ["periodic", "periodic"]],
                  x1l=0.0, x1u=Lx * n / ny, x2l=0.0, x2u=L, x3l=0.0, x3u=Lx * nz / ny,
                  gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8, mach_cutoff=1e-4, mach_ct=1e-6,

@@ -7,6 +7,8 @@ reflective mirror, S:2293-2306 / S:7532-7958), well-balanced deviations (S:7151-
 LIM2ND PLM (S:8141-8181), x2 rotation (S:9715-9747, S:10101-10111), LHLLC (S:15681-16122),
 WB momentum fix and EVOLVE_ETOT potential flux (S:8953-8966), gravity (S:12606-12644), RK3
 (S:7018-7048, S:13518-13531), cons->prim (S:13533-13686) and the CFL dt (S:13707-13960).
+With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073-8136) and
+the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
 Test infrastructure only.
 """
 import numpy as np
@@ -57,6 +59,41 @@ def _lhllc(qL, qR, gm, mach_cutoff):
     return [rs * us, rs * us * us + pstar, rs * us * (hp * v2L + hm * v2R), (hp * resL + hm * resR + pstar) * us]
 
 
+def _hll(qL, qR, gm):
+    """Two-wave HLL flux of the ideal-gas hydro solver on flattened faces."""
+    igmm1 = 1.0 / (gm - 1.0)
+    rhoL, v1L, v2L, pL = qL
+    rhoR, v1R, v2R, pR = qR
+    cL = np.sqrt(gm * pL * (1.0 / rhoL))
+    cR = np.sqrt(gm * pR * (1.0 / rhoR))
+    rhoeL = igmm1 * pL + 0.5 * rhoL * (v1L * v1L + v2L * v2L + 0.0 * 0.0)
+    rhoeR = igmm1 * pR + 0.5 * rhoR * (v1R * v1R + v2R * v2R + 0.0 * 0.0)
+    mc = np.maximum(cL, cR)
+    sL = np.minimum(0.0, np.minimum(v1L, v1R) - mc)
+    sR = np.maximum(0.0, np.maximum(v1L, v1R) + mc)
+    UL = [rhoL, rhoL * v1L, rhoL * v2L, rhoeL]
+    UR = [rhoR, rhoR * v1R, rhoR * v2R, rhoeR]
+    fL = [rhoL * v1L, rhoL * v1L * v1L + pL, rhoL * v1L * v2L, (rhoeL + pL) * v1L]
+    fR = [rhoR * v1R, rhoR * v1R * v1R + pR, rhoR * v1R * v2R, (rhoeR + pR) * v1R]
+    d = 1.0 / (sR - sL)
+    ph = sL * sR
+    return [d * (sR * a - sL * b + ph * (ur - ul)) for a, b, ul, ur in zip(fL, fR, UL, UR)]
+
+
+def _flags(p_full, G, nx, ny, eps_sf):
+    """is_flattened of the padded cells G-1..G+n (2D): cells G-2..G+n+1 whose summed central
+    pressure jumps exceed eps_sf * p mark their 3x3 neighbourhood."""
+    c = p_full[G - 2:G + nx + 2, G - 2:G + ny + 2]
+    tmp = (np.abs(p_full[G - 2:G + nx + 2, G - 1:G + ny + 3] - p_full[G - 2:G + nx + 2, G - 3:G + ny + 1]) +
+           np.abs(p_full[G - 1:G + nx + 3, G - 2:G + ny + 2] - p_full[G - 3:G + nx + 1, G - 2:G + ny + 2])) / c
+    mark = tmp > eps_sf
+    f = np.zeros((nx + 2, ny + 2), dtype=bool)
+    for a in range(3):
+        for b in range(3):
+            f |= mark[a:a + nx + 2, b:b + ny + 2]
+    return f   # f[i, j] is padded cell (G - 1 + i, G - 1 + j)
+
+
 def _fill(a, flip_y, G):
     """Ghosts of a (nx+2G, ny+2G) array: periodic in x, reflective in y (component flips)."""
     nx = a.shape[0] - 2 * G
@@ -68,8 +105,9 @@ def _fill(a, flip_y, G):
         a[:, ny + G - 1 + g] = (-1.0 if flip_y else 1.0) * a[:, ny + G - g]
 
 
-def hot_bubble_steps(h, nsteps, dt=None):
-    """Advance the hot-bubble HostGrid `h` (2D, ideal, WB+ETOT+gravity, LHLLC, RK3) in place."""
+def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
+    """Advance the hot-bubble HostGrid `h` (2D, ideal, WB+ETOT+gravity, LHLLC, RK3) in place;
+    eps_sf: USE_SHOCK_FLATTENING with that threshold (ngc >= 3)."""
     c = h.cfg
     G = c.ngc
     gm = c.gamma_ad
@@ -113,6 +151,8 @@ def hot_bubble_steps(h, nsteps, dt=None):
             Wd[3][I] = W[3][I] - eq_p
             for v in range(4):
                 _fill(Wd[v], v == 2, G)
+            if eps_sf is not None:
+                fl = _flags(Wd[3] + h.eq_prim_cc[1, :, :, 0], G, nx, ny, eps_sf)
             # x1 sweep: faces i = 0..nx (index of the low face of interior cell i)
             lo, hi = zip(*[_plm(w[G - 2:G + nx, G:G + ny], w[G - 1:G + nx + 1, G:G + ny], w[G:G + nx + 2, G:G + ny])
                            for w in Wd])
@@ -123,6 +163,9 @@ def hot_bubble_steps(h, nsteps, dt=None):
             qL[3] = qL[3] + epx
             qR[3] = qR[3] + epx
             F = _lhllc(qL, qR, gm, c.mach_cutoff)
+            if eps_sf is not None:
+                flat = fl[0:nx + 1, 1:ny + 1] | fl[1:nx + 2, 1:ny + 1]
+                F = [np.where(flat, a, b) for a, b in zip(_hll(qL, qR, gm), F)]
             F[1] = F[1] - epx
             F[3] = F[3] + F[0] * phx
             res = [(f[1:] - f[:-1]) * idx1 for f in F]
@@ -138,6 +181,9 @@ def hot_bubble_steps(h, nsteps, dt=None):
             qL[3] = qL[3] + epy
             qR[3] = qR[3] + epy
             F = _lhllc(qL, qR, gm, c.mach_cutoff)
+            if eps_sf is not None:
+                flat = fl[1:nx + 1, 0:ny + 1] | fl[1:nx + 1, 1:ny + 2]
+                F = [np.where(flat, a, b) for a, b in zip(_hll(qL, qR, gm), F)]
             F = [F[0], -F[2], F[1], F[3]]
             F[2] = F[2] - epy
             F[3] = F[3] + F[0] * phy

@@ -197,3 +197,43 @@ def test_stratified_helmholtz_higher_order(gpu_lib, oracle, table, mhd, riemann,
     hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
     assert max_abs_diff(hg, ho) == 0.0
     assert st["newton_nonconverged"] == 0 and st["nonfinite"] == 0
+
+
+# ------------------------------------------------------------------------------ USE_SHOCK_FLATTENING
+@pytest.mark.parametrize("riemann,rec", [("hllc", "lim2nd"), ("lhllc", "lim2nd"), ("hllc", "pph"),
+                                         ("hllc", "lim5th")])
+def test_blast_shock_flattening(gpu_lib, oracle, riemann, rec):
+    """Detector, PLM fallback in flagged cells and HLL on their faces, bit for bit."""
+    cfg, h = problems.blast_2d(48, riemann=riemann, rec=rec)
+    hg, ho, st = run_pair(cfg, h, 12, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["nonfinite"] == 0
+
+
+@pytest.mark.parametrize("rec", ["lim2nd", "lim5th"])
+def test_orszag_tang_shock_flattening(gpu_lib, oracle, rec):
+    cfg, h = problems.orszag_tang_2d(48, rec=rec, shock_flattening=True)
+    hg, ho, _ = run_pair(cfg, h, 10, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert div_b_max(hg) <= 1e-13
+
+
+def test_hot_bubble_shock_flattening(gpu_lib, oracle):
+    """WB ideal gas: the detector adds the cell equilibrium of the ghost layers to the pressure."""
+    cfg, h = problems.hot_bubble_2d(32, shock_flattening=True, eps_sf=0.12)
+    hg, ho, _ = run_pair(cfg, h, 3, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+
+
+@pytest.mark.parametrize("mhd,rec,fasteos", [(False, "lim2nd", True), (False, "pph", True), (True, "lim2nd", True),
+                                             (False, "lim2nd", False)])
+def test_stratified_shock_flattening(gpu_lib, oracle, table, mhd, rec, fasteos):
+    """eps_sf = 0.4 flags the upper half of the box (the pressure scale height shrinks upwards);
+    with WB and USE_FASTEOS this includes the x1 sweep's handling of gamma_e on flagged faces."""
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd, rec=rec, fasteos=fasteos, shock_flattening=True,
+                                    eps_sf=0.4)
+    hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["nonfinite"] == 0
+    if mhd:
+        assert div_b_max(hg) <= 1e-13

@@ -54,8 +54,9 @@ def test_hydrostatic_equilibrium_at_rest(oracle):
     assert float(np.abs(h.interior(h.prim)[3] - p0).max() / p0.max()) < 1e-14
 
 
+@pytest.mark.parametrize("flat", [0, 1])
 @pytest.mark.parametrize("riemann", ["lhllc", "hllc"])
-def test_hydro_riemann_mirror_symmetry(oracle, riemann):
+def test_hydro_riemann_mirror_symmetry(oracle, riemann, flat):
     import ctypes as C
     cfg = Config(sdims=3, nx1=8, nx2=8, nx3=8, nas=2, riemann=riemann, mach_cutoff=1e-4,
                  bc=[["periodic", "periodic"]] * 3)
@@ -71,20 +72,21 @@ def test_hydro_riemann_mirror_symmetry(oracle, riemann):
         fm = np.zeros(7)
         P = C.POINTER(C.c_double)
         oracle.load().phlo_riemann_hydro(C.byref(og.g), qL.ctypes.data_as(P), qR.ctypes.data_as(P), None, None,
-                                         f.ctypes.data_as(P))
+                                         f.ctypes.data_as(P), flat)
         mL = qR.copy()
         mR = qL.copy()
         mL[1] = -mL[1]
         mR[1] = -mR[1]
         oracle.load().phlo_riemann_hydro(C.byref(og.g), mL.ctypes.data_as(P), mR.ctypes.data_as(P), None, None,
-                                         fm.ctypes.data_as(P))
+                                         fm.ctypes.data_as(P), flat)
         # mirrored problem: mass, transverse momenta, energy, scalars flip sign; normal momentum not
         sgn = np.array([-1, 1, -1, -1, -1, -1, -1])
         np.testing.assert_allclose(fm, sgn * f, rtol=1e-12, atol=1e-12)
 
 
+@pytest.mark.parametrize("flat", [0, 1])
 @pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
-def test_mhd_riemann_mirror_symmetry(oracle, riemann):
+def test_mhd_riemann_mirror_symmetry(oracle, riemann, flat):
     import ctypes as C
     cfg = Config(sdims=3, nx1=8, nx2=8, nx3=8, mhd=True, riemann=riemann, mach_cutoff=1e-4,
                  bc=[["periodic", "periodic"]] * 3)
@@ -101,7 +103,7 @@ def test_mhd_riemann_mirror_symmetry(oracle, riemann):
         f, fb, fm, fbm = np.zeros(5), np.zeros(3), np.zeros(5), np.zeros(3)
         oracle.load().phlo_riemann_mhd(C.byref(og.g), qL.ctypes.data_as(P), qR.ctypes.data_as(P),
                                        bL.ctypes.data_as(P), bR.ctypes.data_as(P), None, None,
-                                       f.ctypes.data_as(P), fb.ctypes.data_as(P))
+                                       f.ctypes.data_as(P), fb.ctypes.data_as(P), flat)
         mL, mR, bmL, bmR = qR.copy(), qL.copy(), bR.copy(), bL.copy()
         mL[1] = -mL[1]
         mR[1] = -mR[1]
@@ -109,7 +111,7 @@ def test_mhd_riemann_mirror_symmetry(oracle, riemann):
         bmR[0] = -bmR[0]
         oracle.load().phlo_riemann_mhd(C.byref(og.g), mL.ctypes.data_as(P), mR.ctypes.data_as(P),
                                        bmL.ctypes.data_as(P), bmR.ctypes.data_as(P), None, None,
-                                       fm.ctypes.data_as(P), fbm.ctypes.data_as(P))
+                                       fm.ctypes.data_as(P), fbm.ctypes.data_as(P), flat)
         np.testing.assert_allclose(fm, np.array([-1, 1, -1, -1, -1]) * f, rtol=1e-9, atol=1e-10)
         # induction flux v_n B_t - B_n v_t changes sign with v_n and B_n
         np.testing.assert_allclose(fbm[1:], -fb[1:], rtol=1e-9, atol=1e-10)
@@ -237,3 +239,65 @@ def test_lim5th_edges_reproduce_smooth_data():
     am = (-21 * avg[0] + 189 * avg[1] + 329 * avg[2] - 91 * avg[3] + 14 * avg[4]) / 420.0
     ap = (14 * avg[0] - 91 * avg[1] + 329 * avg[2] + 189 * avg[3] - 21 * avg[4]) / 420.0
     assert abs(am - f(-0.5)) < 1e-12 and abs(ap - f(0.5)) < 1e-12
+
+
+# ------------------------------------------------------------------------------ USE_SHOCK_FLATTENING
+def _interior_state(h):
+    return h.interior(h.prim).copy()
+
+
+@pytest.mark.parametrize("rec", ["pph", "lim5th"])
+def test_flattening_threshold_out_of_reach_changes_nothing(oracle, rec):
+    """No cell reaches eps_sf = 1e300: the step equals the one without the option, bit for bit."""
+    cfg, h = problems.blast_2d(32, rec=rec, shock_flattening=True, eps_sf=1e300)
+    cfg0, h0 = problems.blast_2d(32, rec=rec, shock_flattening=False)
+    _run(oracle, h, steps=8)
+    _run(oracle, h0, steps=8)
+    assert np.array_equal(_interior_state(h), _interior_state(h0))
+
+
+@pytest.mark.parametrize("maker", ["blast", "orszag_tang"])
+def test_flattening_everywhere_is_lim2nd(oracle, maker):
+    """eps_sf < 0 flags every cell: every reconstruction falls back to LIM2ND PLM, so PPH and
+    LIM5TH give exactly the LIM2ND result (hydro and MHD, including transverse B)."""
+    out = {}
+    for rec in ("lim2nd", "pph", "lim5th"):
+        if maker == "blast":
+            cfg, h = problems.blast_2d(32, rec=rec, shock_flattening=True, eps_sf=-1.0)
+        else:
+            cfg, h = problems.orszag_tang_2d(32, rec=rec, shock_flattening=True, eps_sf=-1.0)
+        _run(oracle, h, steps=6)
+        out[rec] = (_interior_state(h), None if h.b_cc is None else h.interior(h.b_cc).copy())
+    for rec in ("pph", "lim5th"):
+        assert np.array_equal(out[rec][0], out["lim2nd"][0])
+        if out[rec][1] is not None:
+            assert np.array_equal(out[rec][1], out["lim2nd"][1])
+
+
+def test_flattening_removes_pph_overshoots(oracle):
+    """Unlimited PPH rings at the blast front (p and rho undershoot their initial minima);
+    with the shock flattener the flagged cells fall back to PLM + HLL and stay bounded."""
+    res = {}
+    for sf in (False, True):
+        cfg, h = problems.blast_2d(64, rec="pph", shock_flattening=sf)
+        _run(oracle, h, steps=20)
+        s = _interior_state(h)
+        res[sf] = (s[0].min(), s[3].min())
+    assert res[False][0] < 0.3 and res[False][1] < 0.095   # ringing without the flattener
+    assert res[True][0] > 0.4 and res[True][1] > 0.0999     # bounded with it
+
+
+def test_flattening_conserves_mass_and_energy(oracle):
+    cfg, h = problems.blast_2d(48, rec="lim5th", shock_flattening=True)
+    dv = np.prod(cfg.dx()[:2])
+
+    def totals():
+        s = _interior_state(h)
+        rho, v1, v2, p = s[0], s[1], s[2], s[3]
+        return (rho.sum() * dv, (p / (cfg.gamma_ad - 1.0) + 0.5 * rho * (v1 * v1 + v2 * v2)).sum() * dv)
+
+    m0, e0 = totals()
+    _run(oracle, h, steps=15)
+    m1, e1 = totals()
+    assert abs(m1 - m0) <= 1e-13 * m0
+    assert abs(e1 - e0) <= 1e-12 * e0

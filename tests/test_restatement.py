@@ -1,5 +1,6 @@
 """The C oracle against the independent numpy restatement (bit for bit)."""
 import numpy as np
+import pytest
 
 from phlegethon_b200 import problems
 from numpy_restatement import hot_bubble_steps
@@ -19,4 +20,25 @@ def test_oracle_matches_numpy_restatement(oracle):
         np.testing.assert_array_equal(h.prim[v, :, :, 0][I], W[v][I])
     np.testing.assert_array_equal(h.interior(h.eint)[:, :, 0], eint)
     np.testing.assert_array_equal(h.interior(h.temp)[:, :, 0], temp)
+    assert o.g.dt == dt
+
+
+@pytest.mark.parametrize("eps_sf", [0.1, 0.1251])
+def test_oracle_shock_flattening_matches_numpy_restatement(oracle, eps_sf):
+    """Detector over 3 ghost layers (deviation + ghost equilibrium) and HLL on flagged faces.
+    For the 32^2 bubble the background jump 2 sinh(dy/H) = 0.12508 sits between the two
+    thresholds: every cell is flagged at 0.1, only cells next to the bubble's disturbance at
+    0.1251 once it has moved the pressure."""
+    cfg, h = problems.hot_bubble_2d(32, shock_flattening=True, eps_sf=eps_sf)
+    hn = h.copy()
+    o = oracle.OracleGrid(h, nthreads=2)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(6)
+    W, eint, temp, dt = hot_bubble_steps(hn, 6, eps_sf=eps_sf)
+    G = cfg.ngc
+    I = (slice(G, G + cfg.nx1), slice(G, G + cfg.nx2))
+    for v in range(4):
+        np.testing.assert_array_equal(h.prim[v, :, :, 0][I], W[v][I])
+    np.testing.assert_array_equal(h.interior(h.eint)[:, :, 0], eint)
     assert o.g.dt == dt
