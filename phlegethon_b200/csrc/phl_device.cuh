@@ -50,6 +50,15 @@ __device__ __forceinline__ int map_index(int i, int n, int bcl, int bcu, bool &f
   return i;
 }
 
+// (i, j, k) of a linear index t = i + n0 * (j + n1 * k) with 32-bit unsigned division (index
+// spaces stay below 2^32, checked at phl_init; 64-bit division is a long software sequence)
+__device__ __forceinline__ void unflatten3(long long t, int n0, int n1, int &i, int &j, int &k) {
+  const unsigned u = (unsigned)t, q = u / (unsigned)n0, r = q / (unsigned)n1;
+  i = (int)(u - q * (unsigned)n0);
+  j = (int)(q - r * (unsigned)n1);
+  k = (int)r;
+}
+
 __device__ __forceinline__ long long lin(const Geo &g, int i, int j, int k) {
   return (long long)i + (long long)g.nx[0] * ((long long)j + (long long)g.nx[1] * k);
 }

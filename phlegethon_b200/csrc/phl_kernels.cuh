@@ -70,6 +70,7 @@ struct Prm {
   float *bccf;
   float *femf[3], *fsgn[3], *fcor[3];
   float *fflux[3];  // FP32 face fluxes [NV][faces] per direction
+  float *fecell;    // FP32 cell-centred -v x B [3][cells] of the stage input (split MHD)
   double *dflux[3]; // FP64 MHD face fluxes [NV][faces] per direction
   // USE_SHOCK_FLATTENING: is_flattened of the cells -1..n per dimension (index + 1, bytes),
   // the detector's marks of cells -2..n+1 (index + 2), the pressure equilibrium with its ghost
@@ -181,6 +182,31 @@ __device__ __forceinline__ void load_bcc(const Prm &P, int i, int j, int k, doub
   if (f0) b[0] = -1.0 * b[0];
   if (f1) b[1] = -1.0 * b[1];
   if (C::DIM == 3 && f2) b[2] = -1.0 * b[2];
+}
+
+// The three loads above for an interior cell given by its linear index c and x2 index j (no
+// mapping, no mirror)
+template <class C>
+__device__ __forceinline__ void load_cell_at(const Prm &P, long long c, int j, double w[C::NV], double gm_[2],
+                                             double b[3]) {
+  const Geo &g = P.g;
+#pragma unroll
+  for (int iv = 0; iv < C::NV; ++iv) w[iv] = __ldg(P.Win + (long long)iv * g.N + c);
+  const long long bg = g.bg_profile ? (long long)j : c;
+  if (C::WB) {
+    w[0] = w[0] - __ldg(P.eq_rho_cc + bg);
+    w[C::IP] = w[C::IP] - __ldg(P.eq_p_cc + bg);
+  }
+  if (C::HELM) {
+    gm_[0] = __ldg(P.gin + c);
+    gm_[1] = C::FAST ? __ldg(P.gin + g.N + c) : 0.0;
+    if (C::FAST && C::WB) gm_[0] = gm_[0] - __ldg(P.eq_ge_cc + bg);
+  }
+  if (C::MHD) {
+    b[0] = __ldg(P.bcc_in + c);
+    b[1] = __ldg(P.bcc_in + g.N + c);
+    b[2] = C::DIM == 3 ? __ldg(P.bcc_in + 2 * g.N + c) : 0.0;
+  }
 }
 
 // --------------------------------------------------------------------- face flux
@@ -406,8 +432,11 @@ __global__ void __launch_bounds__(256) k_sf_mark(Prm P) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const int m0 = g.nx[0] + 4, m1 = g.nx[1] + 4;
-  const int i = (int)(t % m0) - 2, j = (int)((t / m0) % m1) - 2;
-  const int k = C::DIM == 3 ? (int)(t / ((long long)m0 * m1)) - 2 : 0;
+  int i, j, k;
+  unflatten3(t, m0, m1, i, j, k);
+  i -= 2;
+  j -= 2;
+  k = C::DIM == 3 ? k - 2 : 0;
   double tmp;
   if (C::DIM == 3)
     tmp = (fabs(sf_pressure<C>(P, i, j, k + 1) - sf_pressure<C>(P, i, j, k - 1)) +
@@ -430,8 +459,11 @@ __global__ void __launch_bounds__(256) k_sf_flag(Prm P) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const int f0 = g.nx[0] + 2, f1 = g.nx[1] + 2, m0 = g.nx[0] + 4, m1 = g.nx[1] + 4;
-  const int i = (int)(t % f0) - 1, j = (int)((t / f0) % f1) - 1;
-  const int k = C::DIM == 3 ? (int)(t / ((long long)f0 * f1)) - 1 : 0;
+  int i, j, k;
+  unflatten3(t, f0, f1, i, j, k);
+  i -= 1;
+  j -= 1;
+  k = C::DIM == 3 ? k - 1 : 0;
   unsigned char any = 0;
 #pragma unroll
   for (int c = (C::DIM == 3 ? -1 : 0); c <= (C::DIM == 3 ? 1 : 0); ++c)
@@ -458,9 +490,15 @@ __global__ void __launch_bounds__(128) k_face(Prm P, int d) {
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
-  const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
-  // cells m-3 .. m+2 around the face (the reconstruction reads m-SW .. m+SW-1)
+  int fi, fj, fk;
+  unflatten3(f, n0, n1, fi, fj, fk);
+  // cells m-3 .. m+2 around the face (the reconstruction reads m-SW .. m+SW-1); a stencil inside
+  // the domain is read by linear index, one at a boundary maps each ghost index
   double w[6][NV], gmv[6][2], bc[6][3];
+  const int fd = d == 0 ? fi : (d == 1 ? fj : fk);
+  const bool inside = fd >= C::SW && fd + C::SW <= g.nx[d];
+  const long long base = lin(g, fi, fj, fk);
+  const long long stride = d == 0 ? 1 : (d == 1 ? (long long)g.nx[0] : (long long)g.nx[0] * g.nx[1]);
 #pragma unroll
   for (int s = 0; s < 6; ++s) {
     gmv[s][0] = gmv[s][1] = 0.0;
@@ -468,6 +506,10 @@ __global__ void __launch_bounds__(128) k_face(Prm P, int d) {
     if (s < 3 - C::SW || s >= 3 + C::SW) {
 #pragma unroll
       for (int iv = 0; iv < NV; ++iv) w[s][iv] = 0.0;
+      continue;
+    }
+    if (inside) {
+      load_cell_at<C>(P, base + (s - 3) * stride, fj + (d == 1 ? s - 3 : 0), w[s], gmv[s], bc[s]);
       continue;
     }
     const int ii = fi + (d == 0 ? s - 3 : 0), jj = fj + (d == 1 ? s - 3 : 0), kk = fk + (d == 2 ? s - 3 : 0);
@@ -551,9 +593,7 @@ __global__ void __launch_bounds__(256) k_corner(Prm P, int a) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)n0 * n1 * n2) return;
   int c[3];
-  c[0] = (int)(t % n0);
-  c[1] = (int)((t / n0) % n1);
-  c[2] = (int)(t / ((long long)n0 * n1));
+  unflatten3(t, n0, n1, c[0], c[1], c[2]);
   int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
   int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
   int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
@@ -593,7 +633,8 @@ __global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nf) return;
   int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
-  int i = (int)(t % n0), j = (int)((t / n0) % n1), k = (int)(t / ((long long)n0 * n1));
+  int i, j, k;
+  unflatten3(t, n0, n1, i, j, k);
   const double dt = P.scal[1];
   const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
   const double *E1 = P.cor[0], *E2 = P.cor[1], *E3 = P.cor[2];
@@ -628,9 +669,8 @@ __global__ void __launch_bounds__(128) k_c2p(Prm P) {
   double smax_loc = 0.0;
   unsigned long long n_calls = 0, n_iters = 0, n_nonconv = 0, n_clamp = 0, n_bad = 0;
   if (c < g.N) {
-    const int i = (int)(c % g.nx[0]);
-    const int j = (int)((c / g.nx[0]) % g.nx[1]);
-    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    int i, j, k;
+    unflatten3(c, g.nx[0], g.nx[1], i, j, k);
     double bcc[3] = {0, 0, 0};
     if (C::MHD) {
 #pragma unroll
@@ -813,9 +853,8 @@ __global__ void __launch_bounds__(128) k_init_thermo(Prm P) {
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.N) return;
-  const int i = (int)(c % g.nx[0]);
-  const int j = (int)((c / g.nx[0]) % g.nx[1]);
-  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+  int i, j, k;
+  unflatten3(c, g.nx[0], g.nx[1], i, j, k);
   if (C::MHD) {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {

@@ -200,6 +200,7 @@ struct phl_ctx {
   float *sf_rho_f[3] = {}, *sf_p_f[3] = {}, *sf_ge_f[3] = {}, *sf_phi_f[3] = {};  // split path
   float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
   float *fflux[3] = {};
+  float *fecell = nullptr;                                                             // split MHD
   double *dflux[3] = {};                                                               // FP64 MHD
   // USE_SHOCK_FLATTENING: flags, detector marks, ghosted pressure equilibrium (see Prm)
   unsigned char *sf_flag = nullptr, *sf_mark = nullptr;
@@ -281,6 +282,7 @@ struct phl_ctx {
     P.b_ref = sqrt(p_ref);
     P.inv_b_ref = 1.0 / P.b_ref;
     P.bccf = bccf;
+    P.fecell = fecell;
     for (int d = 0; d < 3; ++d) {
       P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; P.fflux[d] = fflux[d];
       P.dflux[d] = dflux[d];
@@ -366,6 +368,8 @@ int check_cfg(const phl_config *c) {
   if (c->sdims == 2 && c->nx3 != 1) return PHL_E_INVALID;
   if (c->sdims == 3 && c->nx3 < 4) return PHL_E_INVALID;
   if (c->ngc < 2) return PHL_E_INVALID;
+  // kernels decompose linear cell / face / corner indices with 32-bit arithmetic
+  if ((double)(c->nx1 + 4) * (double)(c->nx2 + 4) * (double)(c->nx3 + 4) >= 4294967296.0) return PHL_E_TOO_LARGE;
   if (c->nvars != 2 + c->sdims + c->nas) return PHL_E_INVALID;
   if (c->rk_stages != 2 && c->rk_stages != 3) return PHL_E_INVALID;
   for (int d = 0; d < 3; ++d)
@@ -521,6 +525,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
 
     if (c->split) {
       if ((rc = c->alloc(&c->bccf, (size_t)3 * N))) return rc;
+      if ((rc = c->alloc(&c->fecell, (size_t)3 * N))) return rc;
       for (int d = 0; d < cfg->sdims; ++d) {
         long long nf = c->nfaces(d);
         if ((rc = c->alloc(&c->femf[d], (size_t)3 * nf))) return rc;

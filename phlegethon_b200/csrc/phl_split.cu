@@ -318,6 +318,23 @@ __device__ __forceinline__ void load_wf(const Prm &P, int i, int j, int k, float
   }
 }
 
+// the same for an interior cell given by its linear index (no mapping, no mirror)
+template <class C>
+__device__ __forceinline__ void load_wf_at(const Prm &P, long long c, float w[C::NV], float g2[2]) {
+  const long long N = P.g.N;
+#pragma unroll
+  for (int iv = 0; iv < C::NV; ++iv) w[iv] = __ldg(P.Wf_in + iv * N + c);
+  if (C::HELM) {
+    g2[0] = __ldg(P.gf_in + c);
+    g2[1] = __ldg(P.gf_in + N + c);
+  }
+}
+
+// linear-index step between neighbours along d
+__device__ __forceinline__ long long dir_stride(const Geo &g, int d) {
+  return d == 0 ? 1 : (d == 1 ? (long long)g.nx[0] : (long long)g.nx[0] * g.nx[1]);
+}
+
 // States of the four cells m-2..m+1 around the low face of cell m: variable iv of cell s is
 // w(s, iv), FASTEOS gamma q is g(s, q).
 template <int NV>
@@ -569,9 +586,8 @@ __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   SplitStat st;
   if (c < g.N) {
-    const int i = (int)(c % g.nx[0]);
-    const int j = (int)((c / g.nx[0]) % g.nx[1]);
-    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    int i, j, k;
+    unflatten3(c, g.nx[0], g.nx[1], i, j, k);
     float res[NV];
     float rho_dev = 0.0f;
 #pragma unroll
@@ -834,6 +850,13 @@ __device__ __forceinline__ void load_bccf(const Prm &P, int i, int j, int k, flo
   if (C::DIM == 3 && f2) b[2] = -b[2];
 }
 
+template <class C>
+__device__ __forceinline__ void load_bccf_at(const Prm &P, long long c, float b[3]) {
+  b[0] = __ldg(P.bccf + c);
+  b[1] = __ldg(P.bccf + P.g.N + c);
+  b[2] = C::DIM == 3 ? __ldg(P.bccf + 2 * P.g.N + c) : 0.0f;
+}
+
 // MHD flux through the low face of cell m along d (cells m-2..m+1); also the induction flux
 // Fb (lab frame) and rho_L + rho_R at the face for the CT upwinding sign (source.F90:8138-9105
 // with the MHD parts 8327-8469, 8926-8959)
@@ -911,8 +934,8 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
 
 // FP32 face EMF components (units v_ref b_ref) and the CT mass-flux sign (source.F90:8926-8951)
 template <class C>
-__device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long long fidx, const float Fb[3], float frho,
-                                                     float rho_sum, float smax_s) {
+__device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long long fidx, int q, const float Fb[3],
+                                                     float frho, float rho_sum, float smax_s) {
   const Geo &g = P.g;
   long long nf = nfaces(g, d);
   float *e = P.femf[d];
@@ -927,16 +950,20 @@ __device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long l
   // a reflective wall face has mirror-image states and no mass flux: the reference (no FMA) gets
   // exactly zero there, while FP32 with contracted products leaves a rounding residue whose sign
   // would select an upwind side; the wall's dead-band value is restored explicitly
-  const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
-  const long long q = d == 0 ? fidx % n0 : (d == 1 ? (fidx / n0) % n1 : fidx / ((long long)n0 * n1));
+  // q: the face's index along d
   if ((q == 0 && g.bc[d][0] != BC_PERIODIC) || (q == g.nx[d] && g.bc[d][1] != BC_PERIODIC)) sgn = 0.0f;
   P.fsgn[d][fidx] = sgn;
 }
 
 // MHD stage, part 1: one thread per face of direction d solves it once: the FP32 flux goes to
 // P.fflux[d] ([NV][faces]), the face EMF and the CT sign to their arrays
+// 8 resident blocks (64 registers) per SM for the face kernel: measured faster than the 80
+// registers it takes unconstrained
+#ifndef PHL_FACE_MIN_BLOCKS
+#define PHL_FACE_MIN_BLOCKS 8
+#endif
 template <class C>
-__global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
+__global__ void __launch_bounds__(128, PHL_FACE_MIN_BLOCKS) k_face_split_mhd(Prm P, int d) {
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -944,9 +971,14 @@ __global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
-  const int fi = (int)(f % n0), fj = (int)((f / n0) % n1), fk = (int)(f / ((long long)n0 * n1));
-  // cells m-3 .. m+2 (the reconstruction reads m-SW .. m+SW-1)
+  int fi, fj, fk;
+  unflatten3(f, n0, n1, fi, fj, fk);
+  // cells m-3 .. m+2 (the reconstruction reads m-SW .. m+SW-1); a stencil inside the domain
+  // is read by linear index, one at a boundary maps each ghost index
   float w[6][NV], gm4[6][2], b4[6][3];
+  const int fd = d == 0 ? fi : (d == 1 ? fj : fk);
+  const bool inside = fd >= C::SW && fd + C::SW <= g.nx[d];
+  const long long base = lin(g, fi, fj, fk), stride = dir_stride(g, d);
 #pragma unroll
   for (int s = 0; s < 6; ++s) {
     gm4[s][0] = gm4[s][1] = 0.0f;
@@ -956,9 +988,15 @@ __global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
       for (int iv = 0; iv < NV; ++iv) w[s][iv] = 0.0f;
       continue;
     }
-    const int ii = fi + (d == 0 ? s - 3 : 0), jj = fj + (d == 1 ? s - 3 : 0), kk = fk + (d == 2 ? s - 3 : 0);
-    load_wf<C>(P, ii, jj, kk, w[s], gm4[s]);
-    load_bccf<C>(P, ii, jj, kk, b4[s]);
+    if (inside) {
+      const long long c = base + (s - 3) * stride;
+      load_wf_at<C>(P, c, w[s], gm4[s]);
+      load_bccf_at<C>(P, c, b4[s]);
+    } else {
+      const int ii = fi + (d == 0 ? s - 3 : 0), jj = fj + (d == 1 ? s - 3 : 0), kk = fk + (d == 2 ? s - 3 : 0);
+      load_wf<C>(P, ii, jj, kk, w[s], gm4[s]);
+      load_bccf<C>(P, ii, jj, kk, b4[s]);
+    }
   }
   const float *const wv[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
   const float *const gv[6] = {gm4[0], gm4[1], gm4[2], gm4[3], gm4[4], gm4[5]};
@@ -967,7 +1005,7 @@ __global__ void __launch_bounds__(128) k_face_split_mhd(Prm P, int d) {
   face_flux_split_mhd<C>(P, d, fi, fj, fk, wv, gv, bv, F, Fb, rs);
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.fflux[d][(long long)iv * nf + f] = F[iv];
-  store_face_emf_split<C>(P, d, f, Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
+  store_face_emf_split<C>(P, d, f, d == 0 ? fi : (d == 1 ? fj : fk), Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
 }
 
 // FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
@@ -995,7 +1033,22 @@ __device__ __forceinline__ void face_emf_split_at(const Prm &P, int d, int comp,
   sgn = P.fsgn[d][f];
 }
 
-// cell-centred -v x B component a from the stage's input state (scaled units)
+// cell-centred -v x B (components 0..2) of FP32 velocity v and cell B b (scaled units)
+__device__ __forceinline__ void cell_emf3(const float v[3], const float b[3], float e[3]) {
+  e[2] = -v[0] * b[1] + v[1] * b[0];
+  e[0] = v[2] * b[1] - v[1] * b[2];
+  e[1] = v[0] * b[2] - v[2] * b[0];
+}
+// the stage input's cell EMFs, written by the kernel that produced its FP32 state
+__device__ __forceinline__ void store_cell_emf(const Prm &P, long long c, const float v[3], const float b[3]) {
+  float e[3];
+  cell_emf3(v, b, e);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) P.fecell[(long long)a * P.g.N + c] = e[a];
+}
+
+// cell-centred -v x B component a of a (possibly ghost) cell from the stored cell EMFs: a mirror
+// in dimension d != a flips one factor of each product of component a
 template <class C>
 __device__ __forceinline__ float emf_cell_split(const Prm &P, int a, int i, int j, int k) {
   const Geo &g = P.g;
@@ -1003,20 +1056,9 @@ __device__ __forceinline__ float emf_cell_split(const Prm &P, int a, int i, int 
   int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f0);
   int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f1);
   int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f2) : 0;
-  long long c = lin(g, si, sj, sk);
-  float v[3], b[3];
-  v[0] = P.Wf_in[g.N + c];
-  v[1] = P.Wf_in[2 * g.N + c];
-  v[2] = C::DIM == 3 ? P.Wf_in[3 * g.N + c] : 0.0f;
-  b[0] = P.bccf[c];
-  b[1] = P.bccf[g.N + c];
-  b[2] = C::DIM == 3 ? P.bccf[2 * g.N + c] : 0.0f;
-  if (f0) { v[0] = -v[0]; b[0] = -b[0]; }
-  if (f1) { v[1] = -v[1]; b[1] = -b[1]; }
-  if (f2) { v[2] = -v[2]; b[2] = -b[2]; }
-  if (a == 2) return -v[0] * b[1] + v[1] * b[0];
-  if (a == 0) return v[2] * b[1] - v[1] * b[2];
-  return v[0] * b[2] - v[2] * b[0];
+  float e = __ldg(P.fecell + (long long)a * g.N + lin(g, si, sj, sk));
+  const bool flip = (a != 0 && f0) != ((a != 1 && f1) != (a != 2 && f2));
+  return flip ? -e : e;
 }
 
 // corner EMF along axis a (source.F90:11966-12206), FP32; one thread per corner
@@ -1030,9 +1072,7 @@ __global__ void __launch_bounds__(256) k_corner_split(Prm P, int a) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)n0 * n1 * n2) return;
   int c[3];
-  c[0] = (int)(t % n0);
-  c[1] = (int)((t / n0) % n1);
-  c[2] = (int)(t / ((long long)n0 * n1));
+  unflatten3(t, n0, n1, c[0], c[1], c[2]);
   int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
   int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
   int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
@@ -1065,7 +1105,8 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nf) return;
   int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
-  int i = (int)(t % n0), j = (int)((t / n0) % n1), k = (int)(t / ((long long)n0 * n1));
+  int i, j, k;
+  unflatten3(t, n0, n1, i, j, k);
   const double dt = P.scal[1];
   const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt * (P.v_ref * P.b_ref);
   const float *E1 = P.fcor[0], *E2 = P.fcor[1], *E3 = P.fcor[2];
@@ -1094,17 +1135,23 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
 // MHD stage, part 3: flux divergence from the face fluxes, gravity and the RK combine of U (FP64),
 // b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
 // deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
+// Blocks of 128 threads per SM that the register budget of k_c2p_mhd_split is sized for.  The
+// cons->prim kernel waits mostly on table gathers and FP64 dependency chains, so it runs
+// faster at 6 resident blocks (80 registers, a few spilled to L1) than with the 230 registers
+// the compiler would otherwise take (2 blocks).
+#ifndef PHL_C2P_MIN_BLOCKS
+#define PHL_C2P_MIN_BLOCKS 6
+#endif
 template <class C>
-__global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
+__global__ void __launch_bounds__(128, PHL_C2P_MIN_BLOCKS) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   SplitStat st;
   if (c < g.N) {
-    const int i = (int)(c % g.nx[0]);
-    const int j = (int)((c / g.nx[0]) % g.nx[1]);
-    const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+    int i, j, k;
+    unflatten3(c, g.nx[0], g.nx[1], i, j, k);
     const long long bc = bg_cc(g, i, j, k);
     double bcc[3] = {0, 0, 0};
 #pragma unroll
@@ -1193,8 +1240,17 @@ __global__ void __launch_bounds__(128) k_c2p_mhd_split(Prm P) {
       pdev = p - __ldg(P.eq_p_cc + bc);
     }
     P.Wf_out[c] = (float)(rdev * P.inv_rho_ref);
+    float vf[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) P.Wf_out[(long long)(1 + d) * g.N + c] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
+    for (int d = 0; d < DIM; ++d) {
+      vf[d] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
+      P.Wf_out[(long long)(1 + d) * g.N + c] = vf[d];
+    }
+    {
+      const float bf3[3] = {(float)(bcc[0] * P.inv_b_ref), (float)(bcc[1] * P.inv_b_ref),
+                            DIM == 3 ? (float)(bcc[2] * P.inv_b_ref) : 0.0f};
+      store_cell_emf(P, c, vf, bf3);
+    }
     P.Wf_out[(long long)IP * g.N + c] = (float)(pdev * P.inv_p_ref);
 #pragma unroll
     for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
@@ -1222,9 +1278,8 @@ __global__ void k_split_from_prim(Prm P) {
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.N) return;
-  const int i = (int)(c % g.nx[0]);
-  const int j = (int)((c / g.nx[0]) % g.nx[1]);
-  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+  int i, j, k;
+  unflatten3(c, g.nx[0], g.nx[1], i, j, k);
   const long long bc = bg_cc(g, i, j, k);
   double w[NV];
 #pragma unroll
@@ -1254,6 +1309,11 @@ __global__ void k_split_from_prim(Prm P) {
   P.Wf_out[c] = (float)(rdev / P.rho_ref);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) P.Wf_out[(long long)(1 + d) * g.N + c] = (float)(w[1 + d] / P.v_ref);
+  if (C::MHD) {
+    const float vf[3] = {(float)(w[1] / P.v_ref), (float)(w[2] / P.v_ref), DIM == 3 ? (float)(w[3] / P.v_ref) : 0.0f};
+    const float bf3[3] = {P.bccf[c], P.bccf[g.N + c], DIM == 3 ? P.bccf[2 * g.N + c] : 0.0f};
+    store_cell_emf(P, c, vf, bf3);
+  }
   P.Wf_out[(long long)IP * g.N + c] = (float)(pdev / P.p_ref);
 #pragma unroll
   for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)w[iv];
@@ -1274,9 +1334,8 @@ __global__ void k_split_to_prim(Prm P) {
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.N) return;
-  const int i = (int)(c % g.nx[0]);
-  const int j = (int)((c / g.nx[0]) % g.nx[1]);
-  const int k = (int)(c / ((long long)g.nx[0] * g.nx[1]));
+  int i, j, k;
+  unflatten3(c, g.nx[0], g.nx[1], i, j, k);
   const long long bc = bg_cc(g, i, j, k);
   double u[NV];
 #pragma unroll
