@@ -29,6 +29,15 @@ struct Cfg {
   static constexpr int EOSM = !HELM_ ? EOS_IDEAL : (FAST_ ? EOS_FAST : EOS_GIVEN);
   static constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   static_assert(!HELM || NV >= IAS + 2, "Helmholtz needs ADVECT_YE_IABAR scalars");
+  // Resident blocks of 128 threads per SM that the register budgets of the face and cons->prim
+  // kernels are sized for.  These kernels wait mostly on gathers and FP64 dependency chains and
+  // run faster with more warps resident, even with a few registers spilled to L1 (measured on
+  // B200 for the Helmholtz boxes); the variants whose inlined EoS or fifth-order stencil would
+  // spill kilobytes keep the compiler's own budget (1).
+  static constexpr int MINB_FACE64 = (EOSM == EOS_GIVEN || REC_ == REC_LIM5TH) ? 1 : 6;
+  static constexpr int MINB_C2P64 = HELM_ ? 4 : 1;
+  static constexpr int MINB_FACE32 = (EOSM == EOS_GIVEN || REC_ == REC_LIM5TH) ? 1 : 8;
+  static constexpr int MINB_C2P32 = HELM_ ? 6 : 1;
 };
 
 struct Prm {
@@ -482,7 +491,7 @@ __global__ void __launch_bounds__(256) k_sf_flag(Prm P) {
 // face EMF and CT sign.  Each face is solved once; with --fmad=false the result equals what a
 // per-cell loop over both faces of every cell computes.
 template <class C>
-__global__ void __launch_bounds__(128) k_face(Prm P, int d) {
+__global__ void __launch_bounds__(128, C::MINB_FACE64) k_face(Prm P, int d) {
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -661,7 +670,7 @@ __global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
 // (source.F90:9057-9102, 12606-12644, 13518-13531), b_cc from the updated faces, then
 // cons->prim with the EoS (source.F90:12439-12487, 13533-13686), last stage also the CFL max
 template <class C>
-__global__ void __launch_bounds__(128) k_c2p(Prm P) {
+__global__ void __launch_bounds__(128, C::MINB_C2P64) k_c2p(Prm P) {
   if (!*P.active) return;
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;

@@ -949,21 +949,16 @@ __device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long l
   if (mach < -(float)g.mach_ct) sgn = -1.0f;
   // a reflective wall face has mirror-image states and no mass flux: the reference (no FMA) gets
   // exactly zero there, while FP32 with contracted products leaves a rounding residue whose sign
-  // would select an upwind side; the wall's dead-band value is restored explicitly
-  // q: the face's index along d
+  // would select an upwind side; the wall's dead-band value is restored explicitly (q is the
+  // face's index along d)
   if ((q == 0 && g.bc[d][0] != BC_PERIODIC) || (q == g.nx[d] && g.bc[d][1] != BC_PERIODIC)) sgn = 0.0f;
   P.fsgn[d][fidx] = sgn;
 }
 
 // MHD stage, part 1: one thread per face of direction d solves it once: the FP32 flux goes to
 // P.fflux[d] ([NV][faces]), the face EMF and the CT sign to their arrays
-// 8 resident blocks (64 registers) per SM for the face kernel: measured faster than the 80
-// registers it takes unconstrained
-#ifndef PHL_FACE_MIN_BLOCKS
-#define PHL_FACE_MIN_BLOCKS 8
-#endif
 template <class C>
-__global__ void __launch_bounds__(128, PHL_FACE_MIN_BLOCKS) k_face_split_mhd(Prm P, int d) {
+__global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P, int d) {
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -1076,15 +1071,37 @@ __global__ void __launch_bounds__(256) k_corner_split(Prm P, int a) {
   int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
   int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
   int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
-  float emf_N, emf_E, emf_S, emf_W, sgS, sgN, sgW, sgE;
-  face_emf_split_at<C>(P, pa, a, c[0], c[1], c[2], emf_N, sgN);
-  face_emf_split_at<C>(P, qa, a, c[0], c[1], c[2], emf_E, sgE);
-  face_emf_split_at<C>(P, pa, a, cqm[0], cqm[1], cqm[2], emf_S, sgS);
-  face_emf_split_at<C>(P, qa, a, cpm[0], cpm[1], cpm[2], emf_W, sgW);
-  float emf_SW = emf_cell_split<C>(P, a, cpq[0], cpq[1], cpq[2]);
-  float emf_NW = emf_cell_split<C>(P, a, cpm[0], cpm[1], cpm[2]);
-  float emf_NE = emf_cell_split<C>(P, a, c[0], c[1], c[2]);
-  float emf_SE = emf_cell_split<C>(P, a, cqm[0], cqm[1], cqm[2]);
+  float emf_N, emf_E, emf_S, emf_W, sgS, sgN, sgW, sgE, emf_SW, emf_NW, emf_NE, emf_SE;
+  if (c[pa] >= 1 && c[pa] < g.nx[pa] && c[qa] >= 1 && c[qa] < g.nx[qa]) {
+    // all four faces and cells inside the domain: linear indices, no wrap or mirror
+    const long long fp = face_lin(g, pa, c[0], c[1], c[2]), fq = face_lin(g, qa, c[0], c[1], c[2]);
+    const int p0 = g.nx[0] + (pa == 0), p1 = g.nx[1] + (pa == 1);  // face array of pa
+    const int q0 = g.nx[0] + (qa == 0), q1 = g.nx[1] + (qa == 1);  // face array of qa
+    const long long sp_q = qa == 0 ? 1 : (qa == 1 ? (long long)p0 : (long long)p0 * p1);  // step along qa
+    const long long sq_p = pa == 0 ? 1 : (pa == 1 ? (long long)q0 : (long long)q0 * q1);  // step along pa
+    const float *ep = P.femf[pa] + (long long)a * nfaces(g, pa), *eq = P.femf[qa] + (long long)a * nfaces(g, qa);
+    emf_N = __ldg(ep + fp); sgN = __ldg(P.fsgn[pa] + fp);
+    emf_S = __ldg(ep + fp - sp_q); sgS = __ldg(P.fsgn[pa] + fp - sp_q);
+    emf_E = __ldg(eq + fq); sgE = __ldg(P.fsgn[qa] + fq);
+    emf_W = __ldg(eq + fq - sq_p); sgW = __ldg(P.fsgn[qa] + fq - sq_p);
+    const long long cc = lin(g, c[0], c[1], c[2]);
+    const long long cp = pa == 0 ? 1 : (pa == 1 ? (long long)g.nx[0] : (long long)g.nx[0] * g.nx[1]);
+    const long long cq = qa == 0 ? 1 : (qa == 1 ? (long long)g.nx[0] : (long long)g.nx[0] * g.nx[1]);
+    const float *ec = P.fecell + (long long)a * g.N;
+    emf_NE = __ldg(ec + cc);
+    emf_NW = __ldg(ec + cc - cp);
+    emf_SE = __ldg(ec + cc - cq);
+    emf_SW = __ldg(ec + cc - cp - cq);
+  } else {
+    face_emf_split_at<C>(P, pa, a, c[0], c[1], c[2], emf_N, sgN);
+    face_emf_split_at<C>(P, qa, a, c[0], c[1], c[2], emf_E, sgE);
+    face_emf_split_at<C>(P, pa, a, cqm[0], cqm[1], cqm[2], emf_S, sgS);
+    face_emf_split_at<C>(P, qa, a, cpm[0], cpm[1], cpm[2], emf_W, sgW);
+    emf_SW = emf_cell_split<C>(P, a, cpq[0], cpq[1], cpq[2]);
+    emf_NW = emf_cell_split<C>(P, a, cpm[0], cpm[1], cpm[2]);
+    emf_NE = emf_cell_split<C>(P, a, c[0], c[1], c[2]);
+    emf_SE = emf_cell_split<C>(P, a, cqm[0], cqm[1], cqm[2]);
+  }
   float sgn = sgS;
   float demf_S = 0.5f * (1.0f + sgn) * (emf_W - emf_SW) + 0.5f * (1.0f - sgn) * (emf_E - emf_SE);
   sgn = sgN;
@@ -1135,15 +1152,8 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
 // MHD stage, part 3: flux divergence from the face fluxes, gravity and the RK combine of U (FP64),
 // b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
 // deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
-// Blocks of 128 threads per SM that the register budget of k_c2p_mhd_split is sized for.  The
-// cons->prim kernel waits mostly on table gathers and FP64 dependency chains, so it runs
-// faster at 6 resident blocks (80 registers, a few spilled to L1) than with the 230 registers
-// the compiler would otherwise take (2 blocks).
-#ifndef PHL_C2P_MIN_BLOCKS
-#define PHL_C2P_MIN_BLOCKS 6
-#endif
 template <class C>
-__global__ void __launch_bounds__(128, PHL_C2P_MIN_BLOCKS) k_c2p_mhd_split(Prm P) {
+__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
