@@ -42,15 +42,15 @@ def load_peaks():
     return dict(PEAKS_FALLBACK), "fallback"
 
 
-def build_problem(name, n, fasteos=True):
+def build_problem(name, n, fasteos=True, eos_table="fermi"):
     from phlegethon_b200 import helm_table, problems
     table = None
     if name == "stratified":
-        cfg, h = problems.stratified_3d(n, fasteos=fasteos)
-        table = helm_table.generate()
+        cfg, h = problems.stratified_3d(n, fasteos=fasteos, eos_model=eos_table)
+        table = helm_table.make(eos_table)
     elif name == "stratified_mhd":
-        cfg, h = problems.stratified_3d(n, mhd=True, fasteos=fasteos)
-        table = helm_table.generate()
+        cfg, h = problems.stratified_3d(n, mhd=True, fasteos=fasteos, eos_model=eos_table)
+        table = helm_table.make(eos_table)
     elif name == "hot_bubble":
         cfg, h = problems.hot_bubble_2d(n)
     elif name == "orszag_tang":
@@ -185,7 +185,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True):
+def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True, eos_table="fermi"):
     """Oracle (CPU restatement) zone-updates/s on a bounded slab of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
@@ -193,8 +193,9 @@ def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True):
     if name in ("stratified", "stratified_mhd"):
         n = default_size(name)
         nz = slab or 32
-        cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"), fasteos=fasteos)
-        tab, dpdr = helm_table.generate()
+        cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"), fasteos=fasteos,
+                                        eos_model=eos_table)
+        tab, dpdr = helm_table.make(eos_table)
         helm = pyoracle.Helm.for_config(cfg, tab, dpdr)
         sample = "%dx%dx%d slab of the %d^3 workload" % (cfg.nx1, cfg.nx2, cfg.nx3, n)
     else:
@@ -218,12 +219,12 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, args.steps)
-    rate, cores, sample = cpu_rate(args.config, steps, fasteos=not args.no_fasteos)
+    rate, cores, sample = cpu_rate(args.config, steps, fasteos=not args.no_fasteos, eos_table=args.eos_table)
     cfgname = args.config
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "zone-updates/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfgname, "n": args.n or default_size(cfgname)},
+            "config": {"workload": cfgname, "n": args.n or default_size(cfgname), "eos_table": args.eos_table},
             "cpu_baseline": {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -383,7 +384,7 @@ def run_ours(args):
 
     name = args.config
     n = args.n or default_size(name)
-    cfg, h, table = build_problem(name, n, fasteos=not args.no_fasteos)
+    cfg, h, table = build_problem(name, n, fasteos=not args.no_fasteos, eos_table=args.eos_table)
     peaks, peak_kind = load_peaks()
     cells = cfg.n_cells
     head_form = args.form
@@ -417,7 +418,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, cores, sample = cpu_rate(name, steps=1, fasteos=not args.no_fasteos)
+        rate, cores, sample = cpu_rate(name, steps=1, fasteos=not args.no_fasteos, eos_table=args.eos_table)
         cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -429,6 +430,7 @@ def run_ours(args):
                 "dtype": "f32 fluxes / f64 state+EoS" if head_form == "fp32_split" else "f64",
                 "data": "synthetic",
                 "config": {"workload": name + ("_no_fasteos" if args.no_fasteos else ""), "n": n, "cells": cells,
+                           "eos_table": args.eos_table,
                            "form": head_form,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
@@ -461,7 +463,7 @@ def run_eos(args):
     from phlegethon_b200.abi import Simulation
     n = args.n or (1 << 24)
     cfg, _ = problems.stratified_3d(8)
-    table = helm_table.generate()
+    table = helm_table.make(args.eos_table)
     peaks, peak_kind = load_peaks()
     import ctypes as C
     with Simulation(cfg, table) as sim:
@@ -540,12 +542,12 @@ def run_eos(args):
     cpu = None
     if not args.no_cpu:
         k = min(n, 1 << 20)
-        cpu = eos_cpu_rate(rho[:k], e_host[:k], abar[:k], zbar[:k])
+        cpu = eos_cpu_rate(rho[:k], e_host[:k], abar[:k], zbar[:k], eos_table=args.eos_table)
     achieved = EOS_BYTES_PER_SAMPLE * m["rate"] / 1e9
     line = {"metric": EOS_METRIC, "value": m["rate"], "unit": "inversions/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (EoS/Newton), bf16/f32 (MLP)", "data": "synthetic",
-            "config": {"workload": "eos_batch", "n": n, "l2": "inputs larger than L2 (%.0f MB)" % (n * 44 / 1e6),
+            "config": {"workload": "eos_batch", "n": n, "eos_table": args.eos_table, "l2": "inputs larger than L2 (%.0f MB)" % (n * 44 / 1e6),
                        "train": {"samples": 1 << 22, "epochs": args.train_epochs, "seconds": train_s,
                                  "loss": loss.value}},
             "bracket": {"value": b["rate"], "ms_per_step": b["ms"], "newton_iters_per_sample": b["iters"],
@@ -564,13 +566,13 @@ def run_eos(args):
     print(json.dumps(line), flush=True)
 
 
-def eos_cpu_rate(rho, e, abar, zbar, seconds=10.0):
+def eos_cpu_rate(rho, e, abar, zbar, seconds=10.0, eos_table="fermi"):
     """Oracle bracket-guess inversions/s on all host cores, repeating a bounded slice of the batch."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from phlegethon_b200 import helm_table, problems
     cfg, _ = problems.stratified_3d(8)
-    helm = pyoracle.Helm.for_config(cfg, *helm_table.generate())
+    helm = pyoracle.Helm.for_config(cfg, *helm_table.make(eos_table))
     done = 0
     t0 = time.perf_counter()
     while time.perf_counter() - t0 < seconds:
@@ -599,6 +601,9 @@ def main():
     ap.add_argument("--no-fasteos", action="store_true",
                     help="Helmholtz boxes without USE_FASTEOS (helm_rhoP_given per Riemann side)")
     ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
+    ap.add_argument("--eos-table", default="fermi", choices=["fermi", "synthetic"],
+                    help="electron free-energy table of the Helmholtz workloads: the electron-positron "
+                         "Fermi gas (helm_fermi) or the closed-form synthetic model (helm_table.generate)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

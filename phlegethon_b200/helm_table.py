@@ -21,7 +21,9 @@ thermodynamically consistent electron free energy:
 a non-relativistic zero-temperature degenerate term plus a classical ideal electron gas
 (``R`` = CONST_RGAS, ``C0`` from the thermal de Broglie wavelength).  Every derivative in the
 table is exact, so the biquintic Hermite interpolation of the reference reproduces the model to
-interpolation accuracy.  Physically faithful Fermi-Dirac tables are outside this module.
+interpolation accuracy.  The physically faithful table (electron-positron Fermi gas from
+Fermi-Dirac integrals) is built by :mod:`phlegethon_b200.helm_fermi`; :func:`make` returns
+either, cached per process.
 """
 from __future__ import annotations
 
@@ -131,3 +133,25 @@ def read_text(path, nrho, nT):
     for col, v in enumerate(corder):
         dpdr[v] = b[:, :, col].T
     return tab, dpdr
+
+
+_CACHE = {}
+
+
+def make(model="synthetic", ranges=None, workers=None):
+    """``(tab, dpdr)`` of the named electron free-energy model over ``ranges`` (a dict like
+    X2_TABLE), computed once per process: "synthetic" (:func:`generate`) or "fermi"
+    (:func:`phlegethon_b200.helm_fermi.generate`, spread over ``workers`` processes, default
+    all host cores)."""
+    import os
+    r = dict(X2_TABLE if ranges is None else ranges)
+    key = (model,) + tuple(sorted(r.items()))
+    if key not in _CACHE:
+        if model == "synthetic":
+            _CACHE[key] = generate(**r)
+        elif model == "fermi":
+            from . import helm_fermi
+            _CACHE[key] = helm_fermi.generate(workers=os.cpu_count() if workers is None else workers, **r)
+        else:
+            raise KeyError(model)
+    return _CACHE[key]

@@ -78,6 +78,44 @@ def analytic_temperature(rho, p, abar, zbar, T0=1e8):
     return T
 
 
+# The electron-positron Fermi gas of helm_fermi (the model of helm_fermi.generate's table)
+# plus the same ions and radiation.
+def fermi_pressure(rho, T, abar, zbar):
+    from . import helm_fermi
+    rho, T = np.broadcast_arrays(np.asarray(rho, dtype=np.float64), np.asarray(T, dtype=np.float64))
+    th = helm_fermi.thermo((rho * (zbar / abar)).ravel(), T.ravel())
+    pe = th["P"].reshape(rho.shape)
+    return pe + CONST_RGAS * rho * T / abar + CONST_RAD * T ** 4 / 3.0
+
+
+def fermi_energy(rho, T, abar, zbar):
+    from . import helm_fermi
+    rho, T = np.broadcast_arrays(np.asarray(rho, dtype=np.float64), np.asarray(T, dtype=np.float64))
+    th = helm_fermi.thermo((rho * (zbar / abar)).ravel(), T.ravel())
+    ee = th["E"].reshape(rho.shape) / rho
+    return ee + 1.5 * CONST_RGAS * T / abar + CONST_RAD * T ** 4 / rho
+
+
+def fermi_temperature(rho, p, abar, zbar, T0=1e8):
+    from . import helm_fermi
+    rho = np.asarray(rho, dtype=np.float64)
+    T = np.full(rho.shape, T0, dtype=np.float64)
+    d = (rho * (zbar / abar)).ravel()
+    for _ in range(60):
+        th = helm_fermi.thermo(d, T.ravel())
+        f = th["P"].reshape(rho.shape) + CONST_RGAS * rho * T / abar + CONST_RAD * T ** 4 / 3.0 - p
+        dfdT = th["P_T"].reshape(rho.shape) + CONST_RGAS * rho / abar + 4.0 / 3.0 * CONST_RAD * T ** 3
+        dT = f / dfdT
+        T = np.clip(T - dT, 1e3, 1e13)
+        if np.all(np.abs(dT) <= 1e-14 * T):
+            break
+    return T
+
+
+EOS_MODELS = {"synthetic": (analytic_pressure, analytic_energy, analytic_temperature),
+              "fermi": (fermi_pressure, fermi_energy, fermi_temperature)}
+
+
 # ------------------------------------------------------------------------------ config 1
 def hot_bubble_2d(n=256, riemann="lhllc", seed=None, shock_flattening=False, eps_sf=0.25):
     """2D hot bubble: [0,1]^2, periodic x / reflecting y, g = -1 in y, isothermal atmosphere
@@ -171,7 +209,8 @@ STRAT_ZBAR = 6.9
 
 
 def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, seed=12345,
-                  riemann=None, table=X2_TABLE, fasteos=True, rec="lim2nd", shock_flattening=False, eps_sf=0.25):
+                  riemann=None, table=X2_TABLE, fasteos=True, rec="lim2nd", shock_flattening=False, eps_sf=0.25,
+                  eos_model="synthetic"):
     """3D stratified convection box with the Helmholtz EoS.
 
     x2 is vertical (reflecting walls), x1 and x3 periodic.  rho_eq(y) falls exponentially from
@@ -182,8 +221,11 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     mid-height is added and the LHLLD solver with constrained transport is used.  fasteos=False
     selects the Helmholtz path without USE_FASTEOS (helm_rhoP_given per Riemann side); rec picks
     the reconstruction (lim2nd, pph, lim5th; lim5th uses 3 ghost layers); shock_flattening
-    enables USE_SHOCK_FLATTENING with threshold eps_sf (3 ghost layers).
+    enables USE_SHOCK_FLATTENING with threshold eps_sf (3 ghost layers).  eos_model names the
+    electron free energy the table is built from ("synthetic": helm_table.generate, "fermi":
+    helm_fermi.generate); the hydrostatic background is computed with the same model.
     """
+    pressure, energy, temperature = EOS_MODELS[eos_model]
     ny = n if ny is None else ny
     nz = n if nz is None else nz
     abar, zbar = STRAT_ABAR, STRAT_ZBAR
@@ -192,8 +234,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     Hrho = 1.0e8
     L = Hrho * math.log(rho_bot / rho_top)
     Lx = L
-    p_top = float(analytic_pressure(rho_top, 1.0e8, abar, zbar))
-    p_bot = float(analytic_pressure(rho_bot, 3.0e8, abar, zbar))
+    p_top = float(pressure(rho_top, 1.0e8, abar, zbar))
+    p_bot = float(pressure(rho_bot, 3.0e8, abar, zbar))
     g = (p_bot - p_top) / (rho_bot * Hrho * (1.0 - rho_top / rho_bot))
     cfg = Config(sdims=3, nx1=n, nx2=ny, nx3=nz, ngc=3 if (rec == "lim5th" or shock_flattening) else 2, nas=2,
                  mhd=mhd, wb=True, gravity=True, etot=True, rec=rec, helmholtz=True, fasteos=fasteos,
@@ -219,8 +261,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     dy = cfg.dx()[1]
     yc = cfg.x2l + (np.arange(1 - cfg.ngc, ny + cfg.ngc + 1) - 0.5) * dy
     re1, pe1 = rho_of(yc), p_of(yc)
-    Te1 = analytic_temperature(re1, pe1, abar, zbar, T0=2e8)
-    ee1 = re1 * analytic_energy(re1, Te1, abar, zbar)
+    Te1 = temperature(re1, pe1, abar, zbar, T0=2e8)
+    ee1 = re1 * energy(re1, Te1, abar, zbar)
     shp = (1, -1, 1)
     re, pe, Te, ee = (a.reshape(shp) for a in (re1, pe1, Te1, ee1))
     h.prim[0] = re
@@ -250,8 +292,8 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
         nyf = ny + (d == 1)
         yf = cfg.x2l + (np.arange(1, nyf + 1) - (1.0 if d == 1 else 0.5)) * dy
         rf, pf = rho_of(yf), p_of(yf)
-        Tf = analytic_temperature(rf, pf, abar, zbar, T0=2e8)
-        gf = pf / (rf * analytic_energy(rf, Tf, abar, zbar)) + 1.0
+        Tf = temperature(rf, pf, abar, zbar, T0=2e8)
+        gf = pf / (rf * energy(rf, Tf, abar, zbar)) + 1.0
         h.eq_prim_x[d][0] = rf.reshape(shp)
         h.eq_prim_x[d][1] = pf.reshape(shp)
         h.eq_prim_x[d][2] = Tf.reshape(shp)

@@ -237,3 +237,18 @@ def test_stratified_shock_flattening(gpu_lib, oracle, table, mhd, rec, fasteos):
     assert st["nonfinite"] == 0
     if mhd:
         assert div_b_max(hg) <= 1e-13
+
+
+# ------------------------------------------------------------------------------ Fermi-gas table
+@pytest.mark.parametrize("mhd", [False, True])
+def test_stratified_on_fermi_table(gpu_lib, oracle, mhd):
+    """The stratified box on the electron-positron Fermi-gas table (helm_fermi), bit for bit."""
+    from phlegethon_b200 import helm_fermi
+    from test_helm_fermi import SMALL
+    table = helm_fermi.generate(**SMALL)
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd, table=dict(SMALL), eos_model="fermi")
+    hg, ho, st = run_pair(cfg, h, 3, table=table, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["newton_nonconverged"] == 0 and st["nonfinite"] == 0
+    if mhd:
+        assert div_b_max(hg) <= 1e-13

@@ -178,3 +178,17 @@ def test_split_stratified_higher_order(gpu_lib, table, mhd, riemann, rec, dims):
         assert err[f] <= 1e-8, (f, err)
     for f in ("v1", "v2", "v3"):
         assert err[f] <= 1e-5, (f, err)
+
+
+@pytest.mark.parametrize("mhd,riemann", [(False, "lhllc"), (True, "lhlld")])
+def test_split_on_fermi_table(gpu_lib, mhd, riemann):
+    """The split form on the electron-positron Fermi-gas table against FP64."""
+    from phlegethon_b200 import helm_fermi
+    from test_helm_fermi import SMALL
+    table = helm_fermi.generate(**SMALL)
+    cfg, h = problems.stratified_3d(16, ny=24, nz=12, mhd=mhd, riemann=riemann, table=dict(SMALL), eos_model="fermi")
+    h64, _ = run_form(cfg, h, 20, table, "fp64")
+    h32, st = run_form(cfg, h, 20, table, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    assert err["rho"] <= 1e-6 and err["p"] <= 1e-6 and err["T"] <= 1e-6, err
