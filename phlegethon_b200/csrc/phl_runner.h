@@ -21,6 +21,6 @@ struct Runner {
 };
 
 // factory of the FP32 split-precision runners (phl_split.cu); nullptr when not built
-Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec);
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec, bool sf);
 
 }  // namespace phl

@@ -387,10 +387,6 @@ int check_cfg(const phl_config *c) {
   if (c->flags & PHL_SHOCK_FLATTENING) {
     // the detector tests cells lx-2..ux+2 with central differences: 3 ghost layers
     if (c->ngc < 3 || !(c->eps_sf == c->eps_sf)) return PHL_E_INVALID;
-    if (c->precision != PHL_FP64) {
-      g_last_error = "USE_SHOCK_FLATTENING is built for PHL_FP64";
-      return PHL_E_UNSUPPORTED;
-    }
   }
   // the step's Newton starts from the previous stage's temperature (the reference's warm start);
   // the learned guess is offered by the batch inversion entry points only
@@ -463,7 +459,8 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   c->split = cfg->precision == PHL_FP32_SPLIT;
   const bool fast = cfg->flags & PHL_FASTEOS;
   if (c->split)
-    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction));
+    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction,
+                                      (cfg->flags & PHL_SHOCK_FLATTENING) != 0));
   else
     c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction,
                                 (cfg->flags & PHL_SHOCK_FLATTENING) != 0));

@@ -38,7 +38,7 @@ __device__ __forceinline__ void plm_f32(float qm, float qc, float qp, float &lo,
 template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float *qR, const float *gL,
                                                     const float *gR, float pe, float gm, float mach_cutoff,
-                                                    float *flux) {
+                                                    float *flux, bool flat = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const float igmm1 = 1.0f / (gm - 1.0f);
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
@@ -64,6 +64,32 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
   float rhoestarL = rhostarL * (rhoeL * inv_rhoL + (ustar - vx1L) * (ustar + pL * inv_rhoL / dsuL));
   float rhostarR = rhoR * (dsuR / (sR - ustar));
   float rhoestarR = rhostarR * (rhoeR * inv_rhoR + (ustar - vx1R) * (ustar + pR * inv_rhoR / dsuR));
+  if (flat) {
+    // HLL on a flattened face (USE_SHOCK_FLATTENING, source.F90:15929-16010); the momentum
+    // flux takes the pressure deviations, sR pe - sL pe over sR - sL being exactly pe
+    sL = fminf(0.0f, sL);
+    sR = fmaxf(0.0f, sR);
+    float UL[NV], UR[NV], fL[NV], fR[NV];
+    UL[0] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (DIM == 3) UL[3] = rhoL * vx3L; UL[IP] = rhoeL;
+    UR[0] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (DIM == 3) UR[3] = rhoR * vx3R; UR[IP] = rhoeR;
+    fL[0] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + pLd; fL[2] = rhoL * vx1L * vx2L;
+    if (DIM == 3) fL[3] = rhoL * vx1L * vx3L;
+    fL[IP] = (rhoeL + pL) * vx1L;
+    fR[0] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + pRd; fR[2] = rhoR * vx1R * vx2R;
+    if (DIM == 3) fR[3] = rhoR * vx1R * vx3R;
+    fR[IP] = (rhoeR + pR) * vx1R;
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) {
+      UL[iv] = rhoL * qL[iv];
+      UR[iv] = rhoR * qR[iv];
+      fL[iv] = UL[iv] * vx1L;
+      fR[iv] = UR[iv] * vx1R;
+    }
+    const float dh = 1.0f / (sR - sL), ph = sL * sR;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = dh * (sR * fL[iv] - sL * fR[iv] + ph * (UR[iv] - UL[iv]));
+    return;
+  }
   if (RIEM == R_LHLLC) {
     float machL = sqrtf(v2L) / cL, machR = sqrtf(v2R) / cR;
     float chi = fminf(1.0f, fmaxf(machL, machR));
@@ -121,7 +147,8 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
 template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *qR, const float *bL,
                                                   const float *bR, const float *gL, const float *gR, float pe,
-                                                  float gm, float mach_cutoff, float *flux, float *fluxb) {
+                                                  float gm, float mach_cutoff, float *flux, float *fluxb,
+                                                  bool flat = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const float igmm1 = 1.0f / (gm - 1.0f);
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
@@ -174,6 +201,37 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
       chi = fmaxf(mach_cutoff, chi);
       phi = chi * (2.0f - chi);
     }
+  }
+  if (flat) {
+    // HLL on a flattened face (source.F90:14386-14495), total-pressure deviations in the
+    // momentum flux as in the HLL of riemann_hydro_split
+    sL = fminf(0.0f, sL);
+    sR = fmaxf(0.0f, sR);
+    float UL[NV], UR[NV], fL[NV], fR[NV];
+    UL[0] = rhoL; UL[1] = rhoL * vx1L; UL[2] = rhoL * vx2L; if (DIM == 3) UL[3] = rhoL * vx3L; UL[IP] = rhoeL;
+    UR[0] = rhoR; UR[1] = rhoR * vx1R; UR[2] = rhoR * vx2R; if (DIM == 3) UR[3] = rhoR * vx3R; UR[IP] = rhoeR;
+    fL[0] = rhoL * vx1L; fL[1] = rhoL * vx1L * vx1L + ptLd - bx1_2; fL[2] = rhoL * vx1L * vx2L - bx1 * bx2L;
+    if (DIM == 3) fL[3] = rhoL * vx1L * vx3L - bx1 * bx3L;
+    fL[IP] = (rhoeL + ptL) * vx1L - bx1 * (bx1 * vx1L + bx2L * vx2L + bx3L * vx3L);
+    fR[0] = rhoR * vx1R; fR[1] = rhoR * vx1R * vx1R + ptRd - bx1_2; fR[2] = rhoR * vx1R * vx2R - bx1 * bx2R;
+    if (DIM == 3) fR[3] = rhoR * vx1R * vx3R - bx1 * bx3R;
+    fR[IP] = (rhoeR + ptR) * vx1R - bx1 * (bx1 * vx1R + bx2R * vx2R + bx3R * vx3R);
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) {
+      UL[iv] = rhoL * qL[iv];
+      UR[iv] = rhoR * qR[iv];
+      fL[iv] = UL[iv] * vx1L;
+      fR[iv] = UR[iv] * vx1R;
+    }
+    const float UbL[3] = {bx1, bx2L, bx3L}, UbR[3] = {bx1, bx2R, bx3R};
+    const float fbL[3] = {0.0f, vx1L * bx2L - vx2L * bx1, vx1L * bx3L - vx3L * bx1};
+    const float fbR[3] = {0.0f, vx1R * bx2R - vx2R * bx1, vx1R * bx3R - vx3R * bx1};
+    const float dh = 1.0f / (sR - sL), ph = sL * sR;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) flux[iv] = dh * (sR * fL[iv] - sL * fR[iv] + ph * (UR[iv] - UL[iv]));
+#pragma unroll
+    for (int iv = 0; iv < DIM; ++iv) fluxb[iv] = dh * (sR * fbL[iv] - sL * fbR[iv] + ph * (UbR[iv] - UbL[iv]));
+    return;
   }
   // star total pressure: the weights sum to one, so pe factors out
   float pstar_d = (dsuR * rhoR * ptLd - dsuL * rhoL * ptRd - phi * rhoL * rhoR * dsuR * dsuL * (vx1L - vx1R)) *
@@ -390,6 +448,43 @@ __device__ __forceinline__ void rec_face_f32(const float v[6], bool limited, flo
   }
 }
 
+// USE_SHOCK_FLATTENING on the FP32 edge values: v holds cells m-3..m+2 of the face; a flagged
+// cell m-1 (fa) or m (fb) gives its edge by LIM2ND PLM (source.F90:8743-8827, 9635-9700)
+__device__ __forceinline__ void flatten_face_f32(const float v[6], bool fa, bool fb, float &qL, float &qR) {
+  float lo, hi;
+  if (fa) {
+    plm_f32(v[1], v[2], v[3], lo, hi);
+    qL = hi;
+  }
+  if (fb) {
+    plm_f32(v[2], v[3], v[4], lo, hi);
+    qR = lo;
+  }
+}
+// the x1 sweep's gamma handling on flagged faces with WB (source.F90:8829-8872), reproduced as
+// written: PLM gammas without the equilibrium gamma_e replace the flagged side, and the face's
+// eq_gammae_x1 is added once more to the other side; cell m-1 before cell m
+__device__ __forceinline__ void flatten_gamma_x1(const float gv[2][6], bool fa, bool fb, float ge, float gL[2],
+                                                 float gR[2]) {
+  float lo, hi;
+  if (fa) {
+#pragma unroll
+    for (int iv = 0; iv < 2; ++iv) {
+      plm_f32(gv[iv][1], gv[iv][2], gv[iv][3], lo, hi);
+      gL[iv] = hi;
+    }
+    gR[0] = gR[0] + ge;
+  }
+  if (fb) {
+#pragma unroll
+    for (int iv = 0; iv < 2; ++iv) {
+      plm_f32(gv[iv][2], gv[iv][3], gv[iv][4], lo, hi);
+      gR[iv] = lo;
+    }
+    gL[0] = gL[0] + ge;
+  }
+}
+
 // flux through the low face of cell m along d from the FP32 deviation states of cells m-2..m+1
 template <class C, class Cells>
 __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int fj, int fk, const Cells &cl,
@@ -397,11 +492,19 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
   static_assert(C::SW == 2, "cell-accessor faces read two cells per side");
+  // USE_SHOCK_FLATTENING: is_flattened of cells m-1 (fa) and m (fb); a flagged cell's edges
+  // fall back to LIM2ND PLM, and the face takes the HLL flux
+  bool fa = false, fb = false;
+  if (C::SF) {
+    fa = P.sf_flag[sf_flag_index<C>(g, fi - (d == 0), fj - (d == 1), fk - (d == 2))] != 0;
+    fb = P.sf_flag[sf_flag_index<C>(g, fi, fj, fk)] != 0;
+  }
   float qL[NV], qR[NV];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
     const float v[6] = {0.0f, cl.w(0, iv), cl.w(1, iv), cl.w(2, iv), cl.w(3, iv), 0.0f};
     rec_face_f32<C>(v, iv >= C::IAS, qL[iv], qR[iv]);
+    if (C::SF && C::REC != REC_LIM2ND) flatten_face_f32(v, fa, fb, qL[iv], qR[iv]);
   }
   if (d == 1) {
     float a = qL[1], b = qL[2]; qL[1] = b; qL[2] = -a;
@@ -411,25 +514,31 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     a = qR[1]; b = qR[2]; c = qR[3]; qR[1] = c; qR[2] = a; qR[3] = b;
   }
   float pe = 0.0f, phi_f = 0.0f;
-  long long fb = 0;
-  if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
+  long long fbg = 0;
+  if (C::WB || C::ETOT) fbg = bg_face(g, d, fi, fj, fk);
   if (C::WB) {
-    float rho_eq = __ldg(P.sf_rho_f[d] + fb);
+    float rho_eq = __ldg(P.sf_rho_f[d] + fbg);
     qL[0] = rho_eq + qL[0];
     qR[0] = rho_eq + qR[0];
-    pe = __ldg(P.sf_p_f[d] + fb);
+    pe = __ldg(P.sf_p_f[d] + fbg);
   }
   float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
   if (C::FAST) {
+    const bool late = C::SF && C::WB && d == 0;
+    float gv[2][6];
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      const float v[6] = {0.0f, cl.g(0, iv), cl.g(1, iv), cl.g(2, iv), cl.g(3, iv), 0.0f};
-      rec_face_f32<C>(v, false, gL[iv], gR[iv]);
+      gv[iv][0] = gv[iv][5] = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) gv[iv][1 + q] = cl.g(q, iv);
+      rec_face_f32<C>(gv[iv], false, gL[iv], gR[iv]);
+      if (C::SF && C::REC != REC_LIM2ND && !late) flatten_face_f32(gv[iv], fa, fb, gL[iv], gR[iv]);
     }
     if (C::WB) {
-      float ge = __ldg(P.sf_ge_f[d] + fb);
+      float ge = __ldg(P.sf_ge_f[d] + fbg);
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
+      if (late) flatten_gamma_x1(gv, fa, fb, ge, gL, gR);
     }
   } else if (C::HELM) {
     // without USE_FASTEOS the first gamma slot holds the stage input's temperature
@@ -437,14 +546,15 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
-  riemann_hydro_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F);
+  riemann_hydro_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
+                                                    C::SF && (fa || fb));
   if (d == 1) {
     float a = F[1], b = F[2]; F[1] = -b; F[2] = a;
   } else if (C::DIM == 3 && d == 2) {
     float a = F[1], b = F[2], c = F[3]; F[1] = b; F[2] = c; F[3] = a;
   }
   if (C::ETOT) {
-    phi_f = __ldg(P.sf_phi_f[d] + fb);
+    phi_f = __ldg(P.sf_phi_f[d] + fbg);
     F[IP] = F[IP] + F[0] * phi_f;
   }
 }
@@ -831,6 +941,54 @@ __global__ void __launch_bounds__(TX * TY, C::FAST || !C::HELM ? 2 : 1) k_stage_
   split_stat_flush<C>(P, st);
 }
 
+// --------------------------------------------------------------------- shock detector (split)
+// USE_SHOCK_FLATTENING on the split state (source.F90:8073-8136): the full pressure of a
+// (possibly ghost) cell is its FP32 deviation in physical units plus the equilibrium stored
+// for that ghost cell; marks go to P.sf_mark, and k_sf_flag forms is_flattened as in FP64
+template <class C>
+__device__ __forceinline__ double sf_pressure_split(const Prm &P, int i, int j, int k) {
+  const Geo &g = P.g;
+  bool f = false;
+  int si = map_index(i, g.nx[0], g.bc[0][0], g.bc[0][1], f);
+  int sj = map_index(j, g.nx[1], g.bc[1][0], g.bc[1][1], f);
+  int sk = C::DIM == 3 ? map_index(k, g.nx[2], g.bc[2][0], g.bc[2][1], f) : 0;
+  double p = (double)__ldg(P.Wf_in + (long long)C::IP * g.N + lin(g, si, sj, sk)) * P.p_ref;
+  if (C::WB) {
+    const int G = P.sf_G, G3 = C::DIM == 3 ? P.sf_G : 0;
+    long long e = P.sf_eq_profile ? (long long)(j + G)
+                                  : (long long)(i + G) + (long long)(g.nx[0] + 2 * G) *
+                                        ((long long)(j + G) + (long long)(g.nx[1] + 2 * G) * (k + G3));
+    p = p + __ldg(P.sf_eq_p + e);
+  }
+  return p;
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) k_sf_mark_split(Prm P) {
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  const long long n = sf_mark_cells<C>(g);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int m0 = g.nx[0] + 4, m1 = g.nx[1] + 4;
+  int i, j, k;
+  unflatten3(t, m0, m1, i, j, k);
+  i -= 2;
+  j -= 2;
+  k = C::DIM == 3 ? k - 2 : 0;
+  double tmp;
+  if (C::DIM == 3)
+    tmp = (fabs(sf_pressure_split<C>(P, i, j, k + 1) - sf_pressure_split<C>(P, i, j, k - 1)) +
+           fabs(sf_pressure_split<C>(P, i, j + 1, k) - sf_pressure_split<C>(P, i, j - 1, k)) +
+           fabs(sf_pressure_split<C>(P, i + 1, j, k) - sf_pressure_split<C>(P, i - 1, j, k))) /
+          sf_pressure_split<C>(P, i, j, k);
+  else
+    tmp = (fabs(sf_pressure_split<C>(P, i, j + 1, k) - sf_pressure_split<C>(P, i, j - 1, k)) +
+           fabs(sf_pressure_split<C>(P, i + 1, j, k) - sf_pressure_split<C>(P, i - 1, j, k))) /
+          sf_pressure_split<C>(P, i, j, k);
+  P.sf_mark[t] = tmp > P.eps_sf ? 1 : 0;
+}
+
 // --------------------------------------------------------------------- split MHD
 // Cell-centred B of a (possibly ghost) cell in units of b_ref, component d negated for each
 // mirrored dimension d.
@@ -866,11 +1024,17 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
                                                     float Fb[3], float &rho_sum) {
   constexpr int NV = C::NV, IP = C::IP;
   const Geo &g = P.g;
+  bool fa = false, fb = false;  // USE_SHOCK_FLATTENING: is_flattened of cells m-1 and m
+  if (C::SF) {
+    fa = P.sf_flag[sf_flag_index<C>(g, fi - (d == 0), fj - (d == 1), fk - (d == 2))] != 0;
+    fb = P.sf_flag[sf_flag_index<C>(g, fi, fj, fk)] != 0;
+  }
   float qL[NV], qR[NV];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
     const float v[6] = {w[0][iv], w[1][iv], w[2][iv], w[3][iv], w[4][iv], w[5][iv]};
     rec_face_f32<C>(v, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
+    if (C::SF && C::REC != REC_LIM2ND) flatten_face_f32(v, fa, fb, qL[iv], qR[iv]);
   }
   float bL[3] = {0, 0, 0}, bR[3] = {0, 0, 0};
 #pragma unroll
@@ -878,6 +1042,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     if (iv == d) continue;
     const float v[6] = {b[0][iv], b[1][iv], b[2][iv], b[3][iv], b[4][iv], b[5][iv]};
     rec_face_f32<C>(v, C::REC == REC_LIM5TH, bL[iv], bR[iv]);
+    if (C::SF && C::REC != REC_LIM2ND) flatten_face_f32(v, fa, fb, bL[iv], bR[iv]);
   }
   const float bn = (float)(P.bf[d][face_lin(g, d, fi, fj, fk)] * P.inv_b_ref);
   bL[d] = bn;
@@ -894,25 +1059,30 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     a = bR[0]; c = bR[1]; e = bR[2]; bR[0] = e; bR[1] = a; bR[2] = c;
   }
   float pe = 0.0f;
-  long long fb = 0;
-  if (C::WB || C::ETOT) fb = bg_face(g, d, fi, fj, fk);
+  long long fbg = 0;
+  if (C::WB || C::ETOT) fbg = bg_face(g, d, fi, fj, fk);
   if (C::WB) {
-    float rho_eq = __ldg(P.sf_rho_f[d] + fb);
+    float rho_eq = __ldg(P.sf_rho_f[d] + fbg);
     qL[0] = rho_eq + qL[0];
     qR[0] = rho_eq + qR[0];
-    pe = __ldg(P.sf_p_f[d] + fb);
+    pe = __ldg(P.sf_p_f[d] + fbg);
   }
   float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
   if (C::FAST) {
+    const bool late = C::SF && C::WB && d == 0;
+    float gv[2][6];
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      const float v[6] = {gm[0][iv], gm[1][iv], gm[2][iv], gm[3][iv], gm[4][iv], gm[5][iv]};
-      rec_face_f32<C>(v, C::REC == REC_LIM5TH, gL[iv], gR[iv]);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) gv[iv][q] = gm[q][iv];
+      rec_face_f32<C>(gv[iv], C::REC == REC_LIM5TH, gL[iv], gR[iv]);
+      if (C::SF && C::REC != REC_LIM2ND && !late) flatten_face_f32(gv[iv], fa, fb, gL[iv], gR[iv]);
     }
     if (C::WB) {
-      float ge = __ldg(P.sf_ge_f[d] + fb);
+      float ge = __ldg(P.sf_ge_f[d] + fbg);
       gL[0] = gL[0] + ge;
       gR[0] = gR[0] + ge;
+      if (late) flatten_gamma_x1(gv, fa, fb, ge, gL, gR);
     }
   } else if (C::HELM) {
     const float tface = 0.5f * (gm[2][0] + gm[3][0]);
@@ -920,7 +1090,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
   riemann_mhd_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
-                                                   Fb);
+                                                   Fb, C::SF && (fa || fb));
   if (d == 1) {
     float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
     a = Fb[0]; c = Fb[1]; Fb[0] = -c; Fb[1] = a;
@@ -929,7 +1099,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     a = Fb[0]; c = Fb[1]; e = Fb[2]; Fb[0] = c; Fb[1] = e; Fb[2] = a;
   }
   rho_sum = qL[0] + qR[0];
-  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.sf_phi_f[d] + fb);
+  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.sf_phi_f[d] + fbg);
 }
 
 // FP32 face EMF components (units v_ref b_ref) and the CT mass-flux sign (source.F90:8926-8951)
@@ -1456,6 +1626,10 @@ struct SplitRunnerT : Runner {
     return allow_tiled && C::DIM == 3 && g.nx[0] % TX == 0 && g.nx[1] % TY == 0 && g.nx[2] % KZ == 0;
   }
   void stage(const Prm &P, cudaStream_t s) override {
+    if constexpr (C::SF) {
+      k_sf_mark_split<C><<<nblk(sf_mark_cells<C>(P.g), 256), 256, 0, s>>>(P);
+      k_sf_flag<C><<<nblk(sf_flag_cells<C>(P.g), 256), 256, 0, s>>>(P);
+    }
     if constexpr (C::MHD) {
       const Geo &g = P.g;
       for (int d = 0; d < C::DIM; ++d) {
@@ -1508,32 +1682,38 @@ struct SplitRunnerT : Runner {
 };
 
 #define PHL_SPLIT_LIST(X)                                   \
-  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND)    \
-  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
-  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND)    \
-  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND)   \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND)      \
-  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND)       \
-  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND)     \
-  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
-  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND)   \
-  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND)   \
-  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
-  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND)  \
-  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND)   \
-  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND)     \
-  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND)      \
-  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND)    \
-  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND)     \
-  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH)    \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH)         \
-  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH)      \
-  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH)        
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND, false) \
+  X(2, 4, true, false, false, R_LHLLD, false, REC_LIM2ND, false) \
+  X(3, 5, true, false, false, R_HLLD, false, REC_LIM2ND, false) \
+  X(3, 5, true, false, false, R_LHLLD, false, REC_LIM2ND, false) \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND, false) \
+  X(3, 7, true, true, true, R_HLLD, true, REC_LIM2ND, false) \
+  X(3, 7, true, true, true, R_LHLLD, false, REC_LIM2ND, false) \
+  X(2, 4, false, false, false, R_LHLLC, false, REC_LIM2ND, false) \
+  X(2, 4, false, false, false, R_HLLC, false, REC_LIM2ND, false) \
+  X(2, 4, false, false, true, R_LHLLC, false, REC_LIM2ND, false) \
+  X(2, 6, false, true, true, R_LHLLC, true, REC_LIM2ND, false) \
+  X(3, 5, false, false, false, R_LHLLC, false, REC_LIM2ND, false) \
+  X(3, 5, false, false, false, R_HLLC, false, REC_LIM2ND, false) \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND, false) \
+  X(3, 7, false, true, true, R_HLLC, true, REC_LIM2ND, false) \
+  X(3, 7, false, true, true, R_LHLLC, false, REC_LIM2ND, false) \
+  X(3, 7, false, true, true, R_HLLC, false, REC_LIM2ND, false) \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM5TH, false) \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_PPH, false) \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH, false) \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH, false) \
+  X(2, 5, false, false, false, R_HLLC, false, REC_LIM2ND, true) \
+  X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND, true) \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND, true) \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_PPH, true) \
+  X(3, 7, true, true, true, R_LHLLD, true, REC_LIM2ND, true)
 
-Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec) {
-#define X(D, N, M, H, S, R, F, REC)                                                                           \
-  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) && rec == REC) \
-    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC>>();
+Runner *make_split_runner(int dim, int nv, bool mhd, bool helm, bool strat, int riem, bool fast, int rec, bool sf) {
+#define X(D, N, M, H, S, R, F, REC, SF)                                                                      \
+  if (dim == D && nv == N && mhd == M && helm == H && strat == S && riem == R && (!H || fast == F) &&         \
+      rec == REC && sf == SF)                                                                                 \
+    return new SplitRunnerT<Cfg<D, N, M, H, S, S, S, R, F, REC, SF>>();
   PHL_SPLIT_LIST(X)
 #undef X
   return nullptr;

@@ -192,3 +192,40 @@ def test_split_on_fermi_table(gpu_lib, mhd, riemann):
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
     assert err["rho"] <= 1e-6 and err["p"] <= 1e-6 and err["T"] <= 1e-6, err
+
+
+# ------------------------------------------------------------------------------ USE_SHOCK_FLATTENING
+def test_split_blast_shock_flattening(gpu_lib):
+    """Detector on the FP32 state, PLM fallback and HLL faces, against the FP64 form."""
+    cfg, h = problems.blast_2d(64, riemann="hllc")
+    h64, _ = run_form(cfg, h, 20, None, "fp64")
+    h32, st = run_form(cfg, h, 20, None, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0
+    for f in ("rho", "p", "e"):
+        assert err[f] <= 1e-5, (f, err)
+
+
+def test_split_orszag_tang_shock_flattening(gpu_lib):
+    from util import div_b_max
+    cfg, h = problems.orszag_tang_2d(64, riemann="hlld", shock_flattening=True)
+    h64, _ = run_form(cfg, h, 30, None, "fp64")
+    h32, st = run_form(cfg, h, 30, None, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0
+    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
+        assert err[f] <= lim, (f, err)
+    assert div_b_max(h32) <= 1e-13
+
+
+@pytest.mark.parametrize("mhd,rec", [(False, "lim2nd"), (False, "pph"), (True, "lim2nd")])
+def test_split_stratified_shock_flattening(gpu_lib, table, mhd, rec):
+    """eps_sf = 0.4 flags the upper part of the box; with WB and FASTEOS this includes the x1
+    sweep's gamma_e handling on flagged faces."""
+    cfg, h = problems.stratified_3d(16, ny=16, nz=12, mhd=mhd, rec=rec, shock_flattening=True, eps_sf=0.4)
+    h64, _ = run_form(cfg, h, 20, table, "fp64")
+    h32, st = run_form(cfg, h, 20, table, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    for f in ("rho", "p", "e", "T"):
+        assert err[f] <= 1e-6, (f, err)
