@@ -86,7 +86,11 @@ def stage_kernels(cfg, form):
 # (dram__bytes_read.sum + dram__bytes_write.sum over 2,097,152 cells); the kernel streams the
 # domain once per launch, so the per-launch traffic scales with the cell count
 TRAFFIC_PER_CELL = {("stratified", "fp32_split"): 499.604224e6 / 2097152,
-                    ("stratified", "fp64"): 557.258496e6 / 2097152}
+                    ("stratified", "fp64"): 557.258496e6 / 2097152,
+                    # one split MHD stage at 128^3: 3 x the x1 face launch (169.7 MB), corners
+                    # 3 x 42.4 MB, face-B 3 x 34.0 MB, cons->prim 799.8 MB
+                    ("stratified_mhd", "fp32_split"): (3 * 169.697024e6 + 3 * 42.4e6 + 3 * 33.96e6 + 799.823872e6)
+                    / 2097152}
 
 
 def step_bytes_per_cell(cfg):
@@ -412,7 +416,8 @@ def run_ours(args):
     tpc = TRAFFIC_PER_CELL.get((name, head_form))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": tpc * cells if tpc else None,
-            "traffic_source": "ncu DRAM bytes of one launch at 128^3, scaled by cells" if tpc else None,
+            "traffic_source": ("ncu DRAM bytes at 128^3 (profiles/), scaled by cells; per stage" if name == "stratified_mhd"
+                               else "ncu DRAM bytes of one launch at 128^3, scaled by cells") if tpc else None,
             "kernel": kname, "peak_kind": peak_kind,
             "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
 
