@@ -56,6 +56,7 @@ extern "C" {
 #define PHL_FASTEOS (1 << 5)          /* USE_FASTEOS */
 #define PHL_ADVECT_YE_IABAR (1 << 6)  /* ADVECT_YE_IABAR */
 #define PHL_SHOCK_FLATTENING (1 << 7) /* USE_SHOCK_FLATTENING (ngc >= 3) */
+#define PHL_FLUX_IS_ALL_MACH (1 << 8) /* FLUX_IS_ALL_MACH (LHLLC/LHLLD: upwind states outside the fan) */
 
 /* arithmetic of the flux path */
 #define PHL_FP64 0        /* FP64 throughout, bit-compatible with the reference order */

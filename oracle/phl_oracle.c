@@ -225,6 +225,20 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
     double phi = chi * (2.0 - chi);
     double rhobar = 0.5 * (rhoL + rhoR), cbar = 0.5 * (cL + cR);
     double pstar = 0.5 * (pL + pR) - 0.5 * phi * rhobar * cbar * (vx1R - vx1L);
+    if (g->all_mach && (sL > 0.0 || sR < 0.0)) {
+      /* FLUX_IS_ALL_MACH: the upwind state's flux outside the wave fan (source.F90:16032-16077) */
+      const int left = sL > 0.0;
+      const double *q = left ? qL : qR;
+      double rho = left ? rhoL : rhoR, vx1 = left ? vx1L : vx1R, vx2 = left ? vx2L : vx2R, vx3 = left ? vx3L : vx3R;
+      double p = left ? pL : pR, rhoe = left ? rhoeL : rhoeR;
+      flux[IRHO] = rho * vx1;
+      flux[1] = rho * vx1 * vx1 + p;
+      flux[2] = rho * vx1 * vx2;
+      if (three) flux[3] = rho * vx1 * vx3;
+      flux[ip] = (rhoe + p) * vx1;
+      for (int iv = ias; iv < nv; ++iv) flux[iv] = rho * q[iv] * vx1;
+      return;
+    }
     double sgn = sgnf(ustar);
     double hp = 0.5 * (1.0 + sgn), hm = 0.5 * (1.0 - sgn);
     double rhostar = hp * rhostarL + hm * rhostarR;
@@ -399,17 +413,21 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
   fluxb[0] = 0.0;
   if (g->riemann == PHLO_LHLLD) {
     /* source.F90:14663-14732 */
-    double rho, vx1, vx2, vx3, rhoe, bx2, bx3, pres;
-    if (sstarL > 0.0) {
+    double rho, vx1, vx2, vx3, rhoe, bx2, bx3, pres = pstar;
+    if (g->all_mach && sL > 0.0) {
+      /* FLUX_IS_ALL_MACH: the outer states as well (source.F90:14576-14632) */
+      rho = rhoL; vx1 = vx1L; vx2 = vx2L; vx3 = vx3L; rhoe = rhoeL; bx2 = bx2L; bx3 = bx3L; pres = ptL;
+    } else if (sstarL > 0.0) {
       rho = rhostarL; vx1 = ustar; vx2 = vx2starL; vx3 = vx3starL; rhoe = rhoestarL; bx2 = bx2starL; bx3 = bx3starL;
     } else if (ustar > 0.0) {
       rho = rhostarL; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starL; bx2 = bx22star; bx3 = bx32star;
     } else if (sstarR > 0.0) {
       rho = rhostarR; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starR; bx2 = bx22star; bx3 = bx32star;
-    } else {
+    } else if (!g->all_mach || sR > 0.0) {
       rho = rhostarR; vx1 = ustar; vx2 = vx2starR; vx3 = vx3starR; rhoe = rhoestarR; bx2 = bx2starR; bx3 = bx3starR;
+    } else {
+      rho = rhoR; vx1 = vx1R; vx2 = vx2R; vx3 = vx3R; rhoe = rhoeR; bx2 = bx2R; bx3 = bx3R; pres = ptR;
     }
-    pres = pstar;
     flux[IRHO] = rho * vx1;
     flux[1] = rho * vx1 * vx1 + pres - bx1_2;
     flux[2] = rho * vx1 * vx2 - bx1 * bx2;

@@ -30,6 +30,7 @@ struct Geo {
   double inv_dx[3];
   double gm, mu, cfl, mach_cutoff, mach_ct;
   int bg_profile;     // 1: background fields stored as profiles along x2
+  int all_mach;       // FLUX_IS_ALL_MACH: LHLLC / LHLLD take the upwind state outside the wave fan
 };
 
 // Map a (possibly ghost) 0-based index along dimension d to its interior image.
@@ -131,7 +132,8 @@ __device__ __forceinline__ R sgn1(R x) { return copysign(R(1), x); }
 enum { EOS_IDEAL = 0, EOS_FAST = 1, EOS_GIVEN = 2 };
 template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R *gL, const R *gR,
-                                              R gm, R mach_cutoff, R *flux, bool flat = false) {
+                                              R gm, R mach_cutoff, R *flux, bool flat = false,
+                                              bool all_mach = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const R gmm1 = gm - R(1), igmm1 = R(1) / gmm1;
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
@@ -190,6 +192,21 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
     R phi = chi * (R(2) - chi);
     R rhobar = R(0.5) * (rhoL + rhoR), cbar = R(0.5) * (cL + cR);
     R pstar = R(0.5) * (pL + pR) - R(0.5) * phi * rhobar * cbar * (vx1R - vx1L);
+    if (all_mach && (sL > R(0) || sR < R(0))) {
+      // FLUX_IS_ALL_MACH: the upwind state's flux outside the wave fan (source.F90:16032-16077)
+      const bool left = sL > R(0);
+      const R *q = left ? qL : qR;
+      R rho = left ? rhoL : rhoR, vx1 = left ? vx1L : vx1R, vx2 = left ? vx2L : vx2R, vx3 = left ? vx3L : vx3R;
+      R p = left ? pL : pR, rhoe = left ? rhoeL : rhoeR;
+      flux[0] = rho * vx1;
+      flux[1] = rho * vx1 * vx1 + p;
+      flux[2] = rho * vx1 * vx2;
+      if (DIM == 3) flux[3] = rho * vx1 * vx3;
+      flux[IP] = (rhoe + p) * vx1;
+#pragma unroll
+      for (int iv = IAS; iv < NV; ++iv) flux[iv] = rho * q[iv] * vx1;
+      return;
+    }
     R sgn = sgn1(ustar);
     R hp = R(0.5) * (R(1) + sgn), hm = R(0.5) * (R(1) - sgn);
     R rhostar = hp * rhostarL + hm * rhostarR;
@@ -235,7 +252,7 @@ __device__ __forceinline__ void riemann_hydro(const R *qL, const R *qR, const R 
 template <typename R, int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *bL, const R *bR,
                                             const R *gL, const R *gR, R gm, R mach_cutoff,
-                                            R *flux, R *fluxb, bool flat = false) {
+                                            R *flux, R *fluxb, bool flat = false, bool all_mach = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const R gmm1 = gm - R(1), igmm1 = R(1) / gmm1;
   R rhoL = qL[0], inv_rhoL = R(1) / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : R(0);
@@ -356,17 +373,21 @@ __device__ __forceinline__ void riemann_mhd(const R *qL, const R *qR, const R *b
 
   fluxb[0] = R(0);
   if (RIEM == R_LHLLD) {
-    R rho, vx1, vx2, vx3, rhoe, bx2, bx3;
-    if (sstarL > R(0)) {
+    R rho, vx1, vx2, vx3, rhoe, bx2, bx3, pres = pstar;
+    if (all_mach && sL > R(0)) {
+      // FLUX_IS_ALL_MACH: the outer states as well (source.F90:14576-14632)
+      rho = rhoL; vx1 = vx1L; vx2 = vx2L; vx3 = vx3L; rhoe = rhoeL; bx2 = bx2L; bx3 = bx3L; pres = ptL;
+    } else if (sstarL > R(0)) {
       rho = rhostarL; vx1 = ustar; vx2 = vx2starL; vx3 = vx3starL; rhoe = rhoestarL; bx2 = bx2starL; bx3 = bx3starL;
     } else if (ustar > R(0)) {
       rho = rhostarL; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starL; bx2 = bx22star; bx3 = bx32star;
     } else if (sstarR > R(0)) {
       rho = rhostarR; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starR; bx2 = bx22star; bx3 = bx32star;
-    } else {
+    } else if (!all_mach || sR > R(0)) {
       rho = rhostarR; vx1 = ustar; vx2 = vx2starR; vx3 = vx3starR; rhoe = rhoestarR; bx2 = bx2starR; bx3 = bx3starR;
+    } else {
+      rho = rhoR; vx1 = vx1R; vx2 = vx2R; vx3 = vx3R; rhoe = rhoeR; bx2 = bx2R; bx3 = bx3R; pres = ptR;
     }
-    R pres = pstar;
     flux[0] = rho * vx1;
     flux[1] = rho * vx1 * vx1 + pres - bx1_2;
     flux[2] = rho * vx1 * vx2 - bx1 * bx2;

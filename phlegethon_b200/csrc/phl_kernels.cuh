@@ -360,9 +360,11 @@ __device__ __forceinline__ void face_flux(const Prm &P, int d, int fi, int fj, i
   }
   const double gm = P.g.gm, mc = P.g.mach_cutoff;
   if (C::MHD) {
-    riemann_mhd<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb, C::SF && (fa || fb));
+    riemann_mhd<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, gm, mc, F, Fb, C::SF && (fa || fb),
+                                                      g.all_mach != 0);
   } else {
-    riemann_hydro<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, gm, mc, F, C::SF && (fa || fb));
+    riemann_hydro<double, C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, gm, mc, F, C::SF && (fa || fb),
+                                                        g.all_mach != 0);
   }
   // back to the lab frame
   if (d == 1) {

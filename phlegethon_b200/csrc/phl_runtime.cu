@@ -480,6 +480,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   g.inv_dx[0] = 1.0 / dx1; g.inv_dx[1] = 1.0 / dx2; g.inv_dx[2] = cfg->sdims == 3 ? 1.0 / dx3 : 0.0;
   g.gm = cfg->gamma_ad; g.mu = cfg->mu; g.cfl = cfg->cfl;
   g.mach_cutoff = cfg->mach_cutoff; g.mach_ct = cfg->mach_ct;
+  g.all_mach = (cfg->flags & PHL_FLUX_IS_ALL_MACH) ? 1 : 0;
   c->N = g.N;
   long long N = g.N;
   int nv = cfg->nvars;

@@ -38,7 +38,7 @@ __device__ __forceinline__ void plm_f32(float qm, float qc, float qp, float &lo,
 template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float *qR, const float *gL,
                                                     const float *gR, float pe, float gm, float mach_cutoff,
-                                                    float *flux, bool flat = false) {
+                                                    float *flux, bool flat = false, bool all_mach = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const float igmm1 = 1.0f / (gm - 1.0f);
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
@@ -97,6 +97,21 @@ __device__ __forceinline__ void riemann_hydro_split(const float *qL, const float
     float phi = chi * (2.0f - chi);
     float rhobar = 0.5f * (rhoL + rhoR), cbar = 0.5f * (cL + cR);
     float pstar_d = 0.5f * (pLd + pRd) - 0.5f * phi * rhobar * cbar * (vx1R - vx1L);
+    if (all_mach && (sL > 0.0f || sR < 0.0f)) {
+      // FLUX_IS_ALL_MACH: the upwind state outside the wave fan, pe removed from the momentum flux
+      const bool left = sL > 0.0f;
+      const float *q = left ? qL : qR;
+      float rho = left ? rhoL : rhoR, vx1 = left ? vx1L : vx1R, vx2 = left ? vx2L : vx2R, vx3 = left ? vx3L : vx3R;
+      float p = left ? pL : pR, pd = left ? pLd : pRd, rhoe = left ? rhoeL : rhoeR;
+      flux[0] = rho * vx1;
+      flux[1] = rho * vx1 * vx1 + pd;
+      flux[2] = rho * vx1 * vx2;
+      if (DIM == 3) flux[3] = rho * vx1 * vx3;
+      flux[IP] = (rhoe + p) * vx1;
+#pragma unroll
+      for (int iv = IAS; iv < NV; ++iv) flux[iv] = rho * q[iv] * vx1;
+      return;
+    }
     float sgn = copysignf(1.0f, ustar);
     float hp = 0.5f * (1.0f + sgn), hm = 0.5f * (1.0f - sgn);
     float rhostar = hp * rhostarL + hm * rhostarR;
@@ -148,7 +163,7 @@ template <int DIM, int NV, int EOSM, int RIEM>
 __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *qR, const float *bL,
                                                   const float *bR, const float *gL, const float *gR, float pe,
                                                   float gm, float mach_cutoff, float *flux, float *fluxb,
-                                                  bool flat = false) {
+                                                  bool flat = false, bool all_mach = false) {
   constexpr int IP = 1 + DIM, IAS = 2 + DIM;
   const float igmm1 = 1.0f / (gm - 1.0f);
   float rhoL = qL[0], inv_rhoL = 1.0f / rhoL, vx1L = qL[1], vx2L = qL[2], vx3L = DIM == 3 ? qL[3] : 0.0f;
@@ -274,21 +289,26 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
 
   fluxb[0] = 0.0f;
   if (RIEM == R_LHLLD) {
-    float rho, vx1, vx2, vx3, rhoe, bx2, bx3;
-    if (sstarL > 0.0f) {
+    float rho, vx1, vx2, vx3, rhoe, bx2, bx3, pres_d = pstar_d;
+    if (all_mach && sL > 0.0f) {
+      // FLUX_IS_ALL_MACH: the outer states as well (source.F90:14576-14632)
+      rho = rhoL; vx1 = vx1L; vx2 = vx2L; vx3 = vx3L; rhoe = rhoeL; bx2 = bx2L; bx3 = bx3L; pres_d = ptLd;
+    } else if (sstarL > 0.0f) {
       rho = rhostarL; vx1 = ustar; vx2 = vx2starL; vx3 = vx3starL; rhoe = rhoestarL; bx2 = bx2starL; bx3 = bx3starL;
     } else if (ustar > 0.0f) {
       rho = rhostarL; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starL; bx2 = bx22star; bx3 = bx32star;
     } else if (sstarR > 0.0f) {
       rho = rhostarR; vx1 = ustar; vx2 = vx22star; vx3 = vx32star; rhoe = rhoe2starR; bx2 = bx22star; bx3 = bx32star;
-    } else {
+    } else if (!all_mach || sR > 0.0f) {
       rho = rhostarR; vx1 = ustar; vx2 = vx2starR; vx3 = vx3starR; rhoe = rhoestarR; bx2 = bx2starR; bx3 = bx3starR;
+    } else {
+      rho = rhoR; vx1 = vx1R; vx2 = vx2R; vx3 = vx3R; rhoe = rhoeR; bx2 = bx2R; bx3 = bx3R; pres_d = ptRd;
     }
     flux[0] = rho * vx1;
-    flux[1] = rho * vx1 * vx1 + pstar_d - bx1_2;
+    flux[1] = rho * vx1 * vx1 + pres_d - bx1_2;
     flux[2] = rho * vx1 * vx2 - bx1 * bx2;
     if (DIM == 3) flux[3] = rho * vx1 * vx3 - bx1 * bx3;
-    flux[IP] = (rhoe + (pe + pstar_d)) * vx1 - bx1 * (bx1 * vx1 + vx2 * bx2 + vx3 * bx3);
+    flux[IP] = (rhoe + (pe + pres_d)) * vx1 - bx1 * (bx1 * vx1 + vx2 * bx2 + vx3 * bx3);
     float sg = copysignf(1.0f, vx1), hp = 0.5f * (1.0f + sg), hm = 0.5f * (1.0f - sg);
 #pragma unroll
     for (int iv = IAS; iv < NV; ++iv) flux[iv] = rho * vx1 * (hp * qL[iv] + hm * qR[iv]);
@@ -547,7 +567,7 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
   riemann_hydro_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
-                                                    C::SF && (fa || fb));
+                                                    C::SF && (fa || fb), g.all_mach != 0);
   if (d == 1) {
     float a = F[1], b = F[2]; F[1] = -b; F[2] = a;
   } else if (C::DIM == 3 && d == 2) {
@@ -1090,7 +1110,7 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
   riemann_mhd_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
-                                                   Fb, C::SF && (fa || fb));
+                                                   Fb, C::SF && (fa || fb), g.all_mach != 0);
   if (d == 1) {
     float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
     a = Fb[0]; c = Fb[1]; Fb[0] = -c; Fb[1] = a;

@@ -25,6 +25,7 @@ FLAG_HELMHOLTZ = 1 << 4
 FLAG_FASTEOS = 1 << 5
 FLAG_ADVECT_YE_IABAR = 1 << 6
 FLAG_SHOCK_FLATTENING = 1 << 7
+FLAG_FLUX_IS_ALL_MACH = 1 << 8
 
 PRECISION = {"fp64": 0, "fp32_split": 1}
 GUESS = {"warm": 0, "mlp": 1, "bracket": 2}
@@ -49,6 +50,7 @@ class Config:
     rec: str = "lim2nd"              # LIM2ND_REC, PPH_REC or LIM5TH_REC (needs ngc >= 3)
     shock_flattening: bool = False   # USE_SHOCK_FLATTENING (needs ngc >= 3)
     eps_sf: float = 0.25             # eps_sf_make
+    all_mach: bool = False           # FLUX_IS_ALL_MACH (LHLLC / LHLLD: upwind states outside the fan)
     rk_stages: int = 3
     bc: list = field(default_factory=lambda: [["periodic", "periodic"]] * 3)
     precision: str = "fp64"
@@ -93,6 +95,8 @@ class Config:
                 f |= FLAG_FASTEOS
         if self.shock_flattening:
             f |= FLAG_SHOCK_FLATTENING
+        if self.all_mach:
+            f |= FLAG_FLUX_IS_ALL_MACH
         return f
 
     @property

@@ -252,3 +252,16 @@ def test_stratified_on_fermi_table(gpu_lib, oracle, mhd):
     assert st["newton_nonconverged"] == 0 and st["nonfinite"] == 0
     if mhd:
         assert div_b_max(hg) <= 1e-13
+
+
+# ------------------------------------------------------------------------------ FLUX_IS_ALL_MACH
+@pytest.mark.parametrize("maker", ["orszag_tang", "blast"])
+def test_all_mach_parity(gpu_lib, oracle, maker):
+    """Upwind outer states of LHLLD / LHLLC (FLUX_IS_ALL_MACH) on flows with supersonic faces."""
+    if maker == "orszag_tang":
+        cfg, h = problems.orszag_tang_2d(48, riemann="lhlld")
+    else:
+        cfg, h = problems.blast_2d(48, riemann="lhllc")
+    h.cfg = cfg = cfg.replace(all_mach=True)
+    hg, ho, _ = run_pair(cfg, h, 12, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0

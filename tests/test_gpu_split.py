@@ -229,3 +229,15 @@ def test_split_stratified_shock_flattening(gpu_lib, table, mhd, rec):
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
     for f in ("rho", "p", "e", "T"):
         assert err[f] <= 1e-6, (f, err)
+
+
+def test_split_all_mach_orszag_tang(gpu_lib):
+    """FLUX_IS_ALL_MACH in the FP32 LHLLD against the FP64 form."""
+    cfg, h = problems.orszag_tang_2d(64, riemann="lhlld")
+    h.cfg = cfg = cfg.replace(all_mach=True)
+    h64, _ = run_form(cfg, h, 30, None, "fp64")
+    h32, st = run_form(cfg, h, 30, None, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0
+    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
+        assert err[f] <= lim, (f, err)

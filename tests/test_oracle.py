@@ -301,3 +301,37 @@ def test_flattening_conserves_mass_and_energy(oracle):
     m1, e1 = totals()
     assert abs(m1 - m0) <= 1e-13 * m0
     assert abs(e1 - e0) <= 1e-12 * e0
+
+
+# ------------------------------------------------------------------------------ FLUX_IS_ALL_MACH
+def test_all_mach_supersonic_face_takes_the_upwind_flux(oracle):
+    """With FLUX_IS_ALL_MACH a face whose whole wave fan moves right (sL > 0) carries the left
+    state's physical flux exactly; without it LHLLC keeps its star flux."""
+    import ctypes as C
+    P = C.POINTER(C.c_double)
+    qL = np.array([1.0, 5.0, 0.3, -0.2, 1.0, 0.4])
+    qR = np.array([0.8, 4.5, 0.1, 0.1, 0.7, 0.6])
+    out = {}
+    for am in (False, True):
+        cfg = Config(sdims=3, nx1=8, nx2=8, nx3=8, nas=1, riemann="lhllc", all_mach=am, mach_cutoff=1e-4,
+                     bc=[["periodic", "periodic"]] * 3)
+        og = oracle.OracleGrid(HostGrid(cfg))
+        f = np.zeros(6)
+        oracle.load().phlo_riemann_hydro(C.byref(og.g), qL.ctypes.data_as(P), qR.ctypes.data_as(P), None, None,
+                                         f.ctypes.data_as(P), 0)
+        out[am] = f
+    rho, v1, v2, v3, p, s = qL
+    e = p / (5.0 / 3.0 - 1.0) + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3)
+    exact = np.array([rho * v1, rho * v1 * v1 + p, rho * v1 * v2, rho * v1 * v3, (e + p) * v1, rho * s * v1])
+    np.testing.assert_allclose(out[True], exact, rtol=1e-15)
+    assert not np.allclose(out[False], exact, rtol=1e-6)
+
+
+def test_all_mach_leaves_subsonic_flow_unchanged(oracle):
+    res = []
+    for am in (False, True):
+        cfg, h = problems.hot_bubble_2d(32)
+        h.cfg = cfg.replace(all_mach=am)
+        _run(oracle, h, steps=10)
+        res.append(h.interior(h.prim).copy())
+    assert np.array_equal(res[0], res[1])
