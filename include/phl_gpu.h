@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PHL_ABI_VERSION 3
+#define PHL_ABI_VERSION 4
 
 /* return codes */
 #define PHL_OK 0
@@ -57,6 +57,7 @@ extern "C" {
 #define PHL_ADVECT_YE_IABAR (1 << 6)  /* ADVECT_YE_IABAR */
 #define PHL_SHOCK_FLATTENING (1 << 7) /* USE_SHOCK_FLATTENING (ngc >= 3) */
 #define PHL_FLUX_IS_ALL_MACH (1 << 8) /* FLUX_IS_ALL_MACH (LHLLC/LHLLD: upwind states outside the fan) */
+#define PHL_CONSTANT_ACCELERATION (1 << 9) /* USE_CONSTANT_ACCELERATION with phl_config.acc */
 
 /* arithmetic of the flux path */
 #define PHL_FP64 0        /* FP64 throughout, bit-compatible with the reference order */
@@ -95,6 +96,8 @@ typedef struct phl_config {
   double eps_sf;                   /* eps_sf_make (reference default 0.25): a cell whose summed
                                       central pressure jumps exceed eps_sf * p flags itself and
                                       its neighbours; read with PHL_SHOCK_FLATTENING */
+  double acc[3];                   /* lgrid%acc (source.F90:965): body acceleration of
+                                      USE_CONSTANT_ACCELERATION (cm/s^2; acc[2] unused in 2D) */
 } phl_config;
 
 /* Host arrays, laid out exactly as the locgrid members of the same name

@@ -18,6 +18,7 @@
  *   EMF ghosts + reflective EMF BCs          11374-11964
  *   CT corner EMFs, face-B update, b_cc      11966-12487
  *   gravity source                           12606-12644
+ *   constant acceleration                    12806-12836
  *   RK combine                               13518-13531
  *   cons->prim + EoS                         13533-13686
  *   hyperbolic dt                            13707-13960
@@ -1199,6 +1200,23 @@ void phlo_hydro_step(phlo_grid *g) {
             double rho = g->prim[OFF(&sc, IRHO, i, j, k)];
             double *r = S.res + OFF(&sin_, 0, i, j, k);
             for (int d = 0; d < sd; ++d) r[IVX(d)] = r[IVX(d)] - rho * g->grav[OFF(&sg, d, i, j, k)];
+          }
+    }
+    /* USE_CONSTANT_ACCELERATION: rho a from the current state (source.F90:12806-12836) */
+    if (g->use_acc) {
+#pragma omp parallel for collapse(2) num_threads(nthr)
+      for (int k = 1; k <= g->nx3; ++k)
+        for (int j = 1; j <= g->nx2; ++j)
+          for (int i = 1; i <= g->nx1; ++i) {
+            const double *u = S.state + OFF(&sin_, 0, i, j, k);
+            double *r = S.res + OFF(&sin_, 0, i, j, k);
+            double rho = u[IRHO];
+            for (int d = 0; d < sd; ++d) r[IVX(d)] = r[IVX(d)] - rho * g->acc[d];
+            double e = r[ip];
+            if (three) e = e - u[3] * g->acc[2];
+            e = e - u[1] * g->acc[0];
+            e = e - u[2] * g->acc[1];
+            r[ip] = e;
           }
     }
     /* RK combine + cons -> prim (+EoS) (source.F90:13518-13686) */

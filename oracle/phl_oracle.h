@@ -50,6 +50,8 @@ typedef struct phlo_grid {
   int rec;                /* reconstruction: 0 LIM2ND_REC, 1 PPH_REC, 2 LIM5TH_REC (ngc >= 3) */
   int sf;                 /* USE_SHOCK_FLATTENING (ngc >= 3) */
   int all_mach;           /* FLUX_IS_ALL_MACH: upwind L/R states outside the wave fan (LHLLC, LHLLD) */
+  int use_acc;            /* USE_CONSTANT_ACCELERATION with acc */
+  double acc[3];
   int riemann, rk_stages;
   int bc[3][2];           /* [dim][lower/upper] */
   double gm, mu, cfl, mach_cutoff, mach_ct;

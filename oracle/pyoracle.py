@@ -30,7 +30,8 @@ class _Grid(C.Structure):
     _fields_ = [
         ("sdims", C.c_int), ("nx1", C.c_int), ("nx2", C.c_int), ("nx3", C.c_int), ("ngc", C.c_int),
         ("nas", C.c_int), ("nvars", C.c_int), ("mhd", C.c_int), ("wb", C.c_int), ("gravity", C.c_int),
-        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("rec", C.c_int), ("sf", C.c_int), ("all_mach", C.c_int),
+        ("etot", C.c_int), ("helm", C.c_int), ("fasteos", C.c_int), ("rec", C.c_int), ("sf", C.c_int),
+        ("all_mach", C.c_int), ("use_acc", C.c_int), ("acc", C.c_double * 3),
         ("riemann", C.c_int), ("rk_stages", C.c_int), ("bc", (C.c_int * 2) * 3), ("gm", C.c_double), ("mu", C.c_double),
         ("cfl", C.c_double), ("mach_cutoff", C.c_double), ("mach_ct", C.c_double), ("eps_sf", C.c_double),
         ("dx1", C.c_double),
@@ -169,6 +170,9 @@ class OracleGrid:
         g.rec = {"lim2nd": 0, "pph": 1, "lim5th": 2}[c.rec]
         g.sf = int(c.shock_flattening)
         g.all_mach = int(c.all_mach)
+        g.use_acc = int(c.constant_acceleration)
+        for d in range(3):
+            g.acc[d] = float(c.acc[d]) if c.constant_acceleration else 0.0
         g.eps_sf = c.eps_sf
         if c.shock_flattening and c.ngc < 3:
             raise ValueError("USE_SHOCK_FLATTENING reads 3 ghost layers: ngc >= 3")

@@ -21,7 +21,7 @@ from .grid import BC, GUESS, PRECISION, RIEMANN, Config, HostGrid
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libphl_b200.so")
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 PHL_OK = 0
 ERRORS = {-1: "PHL_E_INVALID", -2: "PHL_E_CUDA", -3: "PHL_E_NO_TABLE", -4: "PHL_E_STATE",
@@ -50,7 +50,7 @@ class PhlConfig(C.Structure):
         ("cfl", C.c_double), ("mach_cutoff", C.c_double), ("mach_ct", C.c_double),
         ("helm_nT", C.c_int), ("helm_nrho", C.c_int), ("helm_ltlo", C.c_double),
         ("helm_lthi", C.c_double), ("helm_ldlo", C.c_double), ("helm_ldhi", C.c_double),
-        ("reconstruction", C.c_int), ("eps_sf", C.c_double),
+        ("reconstruction", C.c_int), ("eps_sf", C.c_double), ("acc", C.c_double * 3),
     ]
 
 
@@ -173,6 +173,8 @@ def make_config_struct(cfg: Config) -> PhlConfig:
     s.eos_guess = GUESS[cfg.eos_guess]
     s.reconstruction = {"lim2nd": 0, "pph": 1, "lim5th": 2}[cfg.rec]
     s.eps_sf = float(cfg.eps_sf)
+    for d in range(3):
+        s.acc[d] = float(cfg.acc[d])
     s.device = cfg.device
     for k in ("x1l", "x1u", "x2l", "x2u", "x3l", "x3u", "gamma_ad", "mu", "cfl", "mach_cutoff",
               "mach_ct", "helm_ltlo", "helm_lthi", "helm_ldlo", "helm_ldhi"):

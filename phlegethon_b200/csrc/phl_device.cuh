@@ -31,7 +31,24 @@ struct Geo {
   double gm, mu, cfl, mach_cutoff, mach_ct;
   int bg_profile;     // 1: background fields stored as profiles along x2
   int all_mach;       // FLUX_IS_ALL_MACH: LHLLC / LHLLD take the upwind state outside the wave fan
+  int use_acc;        // USE_CONSTANT_ACCELERATION with the vector acc
+  double acc[3];
 };
+
+// USE_CONSTANT_ACCELERATION (source.F90:12806-12836): body force rho a on the momenta and its
+// work on the energy, from the current RK state u (before the stage's combine), subtracted from
+// the residual in the reference's order
+template <int DIM, int IP>
+__device__ __forceinline__ void constant_acceleration(const Geo &g, const double *u, double *res) {
+  const double rho = u[0];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) res[1 + d] = res[1 + d] - rho * g.acc[d];
+  double r = res[IP];
+  if (DIM == 3) r = r - u[3] * g.acc[2];
+  r = r - u[1] * g.acc[0];
+  r = r - u[2] * g.acc[1];
+  res[IP] = r;
+}
 
 // Map a (possibly ghost) 0-based index along dimension d to its interior image.
 // Periodic: wrap; reflective: mirror (ghost -1 <- 0, -2 <- 1), flip set.  The composition over

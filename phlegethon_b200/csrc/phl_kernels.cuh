@@ -739,6 +739,7 @@ __global__ void __launch_bounds__(128, C::MINB_C2P64) k_c2p(Prm P) {
         u[iv] = P.U[(long long)iv * g.N + c];
       }
     }
+    if (g.use_acc) constant_acceleration<DIM, IP>(g, u, res);
     {
       const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * P.scal[1];
 #pragma unroll

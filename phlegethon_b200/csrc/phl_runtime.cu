@@ -481,6 +481,8 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   g.gm = cfg->gamma_ad; g.mu = cfg->mu; g.cfl = cfg->cfl;
   g.mach_cutoff = cfg->mach_cutoff; g.mach_ct = cfg->mach_ct;
   g.all_mach = (cfg->flags & PHL_FLUX_IS_ALL_MACH) ? 1 : 0;
+  g.use_acc = (cfg->flags & PHL_CONSTANT_ACCELERATION) ? 1 : 0;
+  for (int d = 0; d < 3; ++d) g.acc[d] = g.use_acc ? cfg->acc[d] : 0.0;
   c->N = g.N;
   long long N = g.N;
   int nv = cfg->nvars;

@@ -636,6 +636,7 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
       u[iv] = P.U[(long long)iv * g.N + c];
     }
   }
+  if (g.use_acc) constant_acceleration<DIM, IP>(g, u, rd);
   const double a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
@@ -1390,17 +1391,20 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
     double u[NV];
     {
       const double dt = P.scal[1], a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
+      double un[NV];
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) un[iv] = P.U[(long long)iv * g.N + c];
+      if (g.use_acc) constant_acceleration<DIM, IP>(g, un, rd);
 #pragma unroll
       for (int iv = 0; iv < NV; ++iv) {
-        const double un = P.U[(long long)iv * g.N + c];
         double u0;
         if (P.first_stage) {
-          u0 = un;
-          P.U0[(long long)iv * g.N + c] = un;
+          u0 = un[iv];
+          P.U0[(long long)iv * g.N + c] = un[iv];
         } else {
           u0 = P.U0[(long long)iv * g.N + c];
         }
-        u[iv] = a1 * u0 + a2 * un + a3 * rd[iv];
+        u[iv] = a1 * u0 + a2 * un[iv] + a3 * rd[iv];
         P.U[(long long)iv * g.N + c] = u[iv];
       }
     }

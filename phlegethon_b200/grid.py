@@ -26,6 +26,7 @@ FLAG_FASTEOS = 1 << 5
 FLAG_ADVECT_YE_IABAR = 1 << 6
 FLAG_SHOCK_FLATTENING = 1 << 7
 FLAG_FLUX_IS_ALL_MACH = 1 << 8
+FLAG_CONSTANT_ACCELERATION = 1 << 9
 
 PRECISION = {"fp64": 0, "fp32_split": 1}
 GUESS = {"warm": 0, "mlp": 1, "bracket": 2}
@@ -51,6 +52,8 @@ class Config:
     shock_flattening: bool = False   # USE_SHOCK_FLATTENING (needs ngc >= 3)
     eps_sf: float = 0.25             # eps_sf_make
     all_mach: bool = False           # FLUX_IS_ALL_MACH (LHLLC / LHLLD: upwind states outside the fan)
+    constant_acceleration: bool = False  # USE_CONSTANT_ACCELERATION with the vector acc
+    acc: tuple = (0.0, 0.0, 0.0)
     rk_stages: int = 3
     bc: list = field(default_factory=lambda: [["periodic", "periodic"]] * 3)
     precision: str = "fp64"
@@ -97,6 +100,8 @@ class Config:
             f |= FLAG_SHOCK_FLATTENING
         if self.all_mach:
             f |= FLAG_FLUX_IS_ALL_MACH
+        if self.constant_acceleration:
+            f |= FLAG_CONSTANT_ACCELERATION
         return f
 
     @property

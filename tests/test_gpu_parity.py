@@ -265,3 +265,18 @@ def test_all_mach_parity(gpu_lib, oracle, maker):
     h.cfg = cfg = cfg.replace(all_mach=True)
     hg, ho, _ = run_pair(cfg, h, 12, oracle=oracle)
     assert max_abs_diff(hg, ho) == 0.0
+
+
+# ------------------------------------------------------------------------------ USE_CONSTANT_ACCELERATION
+@pytest.mark.parametrize("maker", ["hot_bubble", "stratified_mhd"])
+def test_constant_acceleration_parity(gpu_lib, oracle, table, maker):
+    if maker == "hot_bubble":
+        cfg, h = problems.hot_bubble_2d(48)
+        acc = (0.05, -0.02, 0.0)
+    else:
+        cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=True)
+        acc = (3.0e5, 0.0, -2.0e5)
+    h.cfg = cfg = cfg.replace(constant_acceleration=True, acc=acc)
+    hg, ho, st = run_pair(cfg, h, 4, table=table if cfg.helmholtz else None, oracle=oracle)
+    assert max_abs_diff(hg, ho) == 0.0
+    assert st["nonfinite"] == 0

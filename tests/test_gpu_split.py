@@ -241,3 +241,18 @@ def test_split_all_mach_orszag_tang(gpu_lib):
     assert st["nonfinite"] == 0
     for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
         assert err[f] <= lim, (f, err)
+
+
+@pytest.mark.parametrize("mhd", [False, True])
+def test_split_constant_acceleration(gpu_lib, table, mhd):
+    """USE_CONSTANT_ACCELERATION in the split form's FP64 update against the FP64 form."""
+    cfg, h = problems.stratified_3d(16, ny=16, nz=16, mhd=mhd)
+    h.cfg = cfg = cfg.replace(constant_acceleration=True, acc=(3.0e5, 0.0, -2.0e5))
+    h64, _ = run_form(cfg, h, 20, table, "fp64")
+    h32, st = run_form(cfg, h, 20, table, "fp32_split")
+    err = field_errors(h32, h64)
+    assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    for f in ("rho", "p", "e", "T"):
+        assert err[f] <= 1e-6, (f, err)
+    for f in ("v1", "v3"):
+        assert err[f] <= 1e-5, (f, err)

@@ -335,3 +335,24 @@ def test_all_mach_leaves_subsonic_flow_unchanged(oracle):
         _run(oracle, h, steps=10)
         res.append(h.interior(h.prim).copy())
     assert np.array_equal(res[0], res[1])
+
+
+# ------------------------------------------------------------------------------ USE_CONSTANT_ACCELERATION
+def test_constant_acceleration_uniform_state(oracle):
+    """A uniform periodic state under a constant acceleration a: every cell gains momentum
+    rho a t and kinetic energy (rho v + rho a t)^2 / (2 rho) - (rho v)^2 / (2 rho), exactly up
+    to rounding (RK3 integrates the linear-in-time momentum exactly)."""
+    cfg = Config(sdims=2, nx1=16, nx2=12, riemann="hllc", bc=[["periodic", "periodic"]] * 3,
+                 constant_acceleration=True, acc=(0.3, -0.2, 0.0))
+    h = HostGrid(cfg)
+    h.prim[0] = 1.3
+    h.prim[1] = 0.2
+    h.prim[2] = -0.1
+    h.prim[3] = 0.7
+    o = _run(oracle, h, steps=5)
+    t = o.g.time
+    s = h.interior(h.prim)
+    np.testing.assert_allclose(s[1], 0.2 + 0.3 * t, rtol=1e-13)
+    np.testing.assert_allclose(s[2], -0.1 - 0.2 * t, rtol=1e-13)
+    np.testing.assert_allclose(s[3], 0.7, rtol=1e-13)  # the work goes into kinetic energy only
+    assert np.all(s == s[:, :1, :1, :1])
