@@ -1148,8 +1148,10 @@ __device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long l
 
 // MHD stage, part 1: one thread per face of direction d solves it once: the FP32 flux goes to
 // P.fflux[d] ([NV][faces]), the face EMF and the CT sign to their arrays
-template <class C>
-__global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P, int d) {
+// (one instantiation per direction D: index strides and rotations fold into constants)
+template <class C, int D>
+__global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
+  constexpr int d = D;
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -1247,13 +1249,13 @@ __device__ __forceinline__ float emf_cell_split(const Prm &P, int a, int i, int 
   return flip ? -e : e;
 }
 
-// corner EMF along axis a (source.F90:11966-12206), FP32; one thread per corner
-template <class C>
-__global__ void __launch_bounds__(256) k_corner_split(Prm P, int a) {
+// corner EMF along axis A (source.F90:11966-12206), FP32; one thread per corner (one
+// instantiation per axis: the face and cell strides fold into constants)
+template <class C, int A>
+__global__ void __launch_bounds__(256) k_corner_split(Prm P) {
+  constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
   if (!*P.active) return;
   const Geo &g = P.g;
-  int pa, qa;
-  if (a == 2) { pa = 0; qa = 1; } else if (a == 0) { pa = 1; qa = 2; } else { pa = 2; qa = 0; }
   int n0 = g.nx[0] + (a != 0), n1 = g.nx[1] + (a != 1), n2 = C::DIM == 3 ? g.nx[2] + (a != 2) : 1;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)n0 * n1 * n2) return;
@@ -1305,8 +1307,9 @@ __global__ void __launch_bounds__(256) k_corner_split(Prm P, int a) {
 }
 
 // face-B update (source.F90:12208-12437) in FP64 from the FP32 corner EMFs; one thread per face
-template <class C>
-__global__ void __launch_bounds__(256) k_bface_split(Prm P, int d) {
+template <class C, int D>
+__global__ void __launch_bounds__(256) k_bface_split(Prm P) {
+  constexpr int d = D;
   if (!*P.active) return;
   const Geo &g = P.g;
   long long nf = nfaces(g, d);
@@ -1656,19 +1659,23 @@ struct SplitRunnerT : Runner {
     }
     if constexpr (C::MHD) {
       const Geo &g = P.g;
-      for (int d = 0; d < C::DIM; ++d) {
-        long long nf = (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
-        k_face_split_mhd<C><<<nblk(nf, 128), 128, 0, s>>>(P, d);
+      auto nfc = [&](int d) {
+        return (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
+      };
+      auto ncor = [&](int a) {
+        return (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
+      };
+      k_face_split_mhd<C, 0><<<nblk(nfc(0), 128), 128, 0, s>>>(P);
+      k_face_split_mhd<C, 1><<<nblk(nfc(1), 128), 128, 0, s>>>(P);
+      if constexpr (C::DIM == 3) {
+        k_face_split_mhd<C, 2><<<nblk(nfc(2), 128), 128, 0, s>>>(P);
+        k_corner_split<C, 0><<<nblk(ncor(0), 256), 256, 0, s>>>(P);
+        k_corner_split<C, 1><<<nblk(ncor(1), 256), 256, 0, s>>>(P);
       }
-      for (int a = 0; a < 3; ++a) {
-        if (C::DIM == 2 && a != 2) continue;
-        long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
-        k_corner_split<C><<<nblk(n, 256), 256, 0, s>>>(P, a);
-      }
-      for (int d = 0; d < C::DIM; ++d) {
-        long long nf = (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
-        k_bface_split<C><<<nblk(nf, 256), 256, 0, s>>>(P, d);
-      }
+      k_corner_split<C, 2><<<nblk(ncor(2), 256), 256, 0, s>>>(P);
+      k_bface_split<C, 0><<<nblk(nfc(0), 256), 256, 0, s>>>(P);
+      k_bface_split<C, 1><<<nblk(nfc(1), 256), 256, 0, s>>>(P);
+      if constexpr (C::DIM == 3) k_bface_split<C, 2><<<nblk(nfc(2), 256), 256, 0, s>>>(P);
       k_c2p_mhd_split<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
     } else {
       hydro_stage(P, s);
