@@ -492,8 +492,9 @@ __global__ void __launch_bounds__(256) k_sf_flag(Prm P) {
 // 9107-10301, 10303-11364), stored in P.dflux[d] for the divergence of k_c2p; for MHD also the
 // face EMF and CT sign.  Each face is solved once; with --fmad=false the result equals what a
 // per-cell loop over both faces of every cell computes.
-template <class C>
-__global__ void __launch_bounds__(128, C::MINB_FACE64) k_face(Prm P, int d) {
+template <class C, int D>
+__global__ void __launch_bounds__(128, C::MINB_FACE64) k_face(Prm P) {
+  constexpr int d = D;  // one instantiation per direction: strides and rotations fold
   if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
@@ -594,8 +595,9 @@ __device__ __forceinline__ double emf_cell(const Prm &P, int a, int i, int j, in
 }
 
 // corner EMF along axis a (source.F90:11966-12206); one thread per corner
-template <class C>
-__global__ void __launch_bounds__(256) k_corner(Prm P, int a) {
+template <class C, int A>
+__global__ void __launch_bounds__(256) k_corner(Prm P) {
+  constexpr int a = A;  // one instantiation per corner axis
   if (!*P.active) return;
   const Geo &g = P.g;
   int pa, qa;
@@ -636,8 +638,9 @@ __device__ __forceinline__ long long cor_lin(const Geo &g, int a, int i, int j, 
 }
 
 // face-B update (source.F90:12208-12437); one thread per face of direction d
-template <class C>
-__global__ void __launch_bounds__(256) k_bface(Prm P, int d) {
+template <class C, int D>
+__global__ void __launch_bounds__(256) k_bface(Prm P) {
+  constexpr int d = D;
   if (!*P.active) return;
   const Geo &g = P.g;
   long long nf = nfaces(g, d);

@@ -45,15 +45,21 @@ struct RunnerT : Runner {
       k_sf_mark<C><<<nblk(sf_mark_cells<C>(g), 256), 256, 0, s>>>(P);
       k_sf_flag<C><<<nblk(sf_flag_cells<C>(g), 256), 256, 0, s>>>(P);
     }
-    for (int d = 0; d < C::DIM; ++d) k_face<C><<<nblk(nfaces_host(g, d), 128), 128, 0, s>>>(P, d);
+    k_face<C, 0><<<nblk(nfaces_host(g, 0), 128), 128, 0, s>>>(P);
+    k_face<C, 1><<<nblk(nfaces_host(g, 1), 128), 128, 0, s>>>(P);
+    if constexpr (C::DIM == 3) k_face<C, 2><<<nblk(nfaces_host(g, 2), 128), 128, 0, s>>>(P);
     if constexpr (C::MHD) {
-      for (int a = 0; a < 3; ++a) {
-        if (C::DIM == 2 && a != 2) continue;
-        long long n = (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) *
-                      (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
-        k_corner<C><<<nblk(n, 256), 256, 0, s>>>(P, a);
+      auto ncor = [&](int a) {
+        return (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
+      };
+      if constexpr (C::DIM == 3) {
+        k_corner<C, 0><<<nblk(ncor(0), 256), 256, 0, s>>>(P);
+        k_corner<C, 1><<<nblk(ncor(1), 256), 256, 0, s>>>(P);
       }
-      for (int d = 0; d < C::DIM; ++d) k_bface<C><<<nblk(nfaces_host(g, d), 256), 256, 0, s>>>(P, d);
+      k_corner<C, 2><<<nblk(ncor(2), 256), 256, 0, s>>>(P);
+      k_bface<C, 0><<<nblk(nfaces_host(g, 0), 256), 256, 0, s>>>(P);
+      k_bface<C, 1><<<nblk(nfaces_host(g, 1), 256), 256, 0, s>>>(P);
+      if constexpr (C::DIM == 3) k_bface<C, 2><<<nblk(nfaces_host(g, 2), 256), 256, 0, s>>>(P);
     }
     k_c2p<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
   }
