@@ -282,15 +282,19 @@ def generate(nrho=541, nT=201, ldlo=-12.0, ldhi=15.0, ltlo=3.0, lthi=13.0, dlog=
     The table's density variable is d = rho Ye over [10^ldlo, 10^ldhi] (the free energy per
     unit d does not depend on Ye).  Third and fourth derivatives are central differences in
     ln d with step ``dlog``.  ``workers`` > 1 spreads the node blocks over that many processes
-    (started with "spawn", so it is safe after CUDA has been initialised)."""
+    (started with "spawn", so it is safe after CUDA has been initialised; the calling script
+    needs the usual ``if __name__ == "__main__":`` guard)."""
     rho, T, _, _ = nodes(nrho, nT, ldlo, ldhi, ltlo, lthi)
     dd = np.repeat(rho, nT)          # node (i, j) at i * nT + j
     tt = np.tile(T, nrho)
     blocks = [(dd[a:a + chunk], tt[a:a + chunk], dlog) for a in range(0, dd.size, chunk)]
     if workers and workers > 1:
+        # spawned workers (safe after CUDA has been initialised); the executor raises instead of
+        # waiting forever if a worker dies, e.g. when the main script lacks a __main__ guard
         import multiprocessing as mp
-        with mp.get_context("spawn").Pool(workers) as pool:
-            parts = pool.map(_chunk, blocks)
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            parts = list(ex.map(_chunk, blocks))
     else:
         parts = [_chunk(b) for b in blocks]
     keys = ("f", "f_d", "f_t", "f_dd", "f_dt", "f_tt", "c", "p_t")

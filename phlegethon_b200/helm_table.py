@@ -141,9 +141,8 @@ _CACHE = {}
 def make(model="synthetic", ranges=None, workers=None):
     """``(tab, dpdr)`` of the named electron free-energy model over ``ranges`` (a dict like
     X2_TABLE), computed once per process: "synthetic" (:func:`generate`) or "fermi"
-    (:func:`phlegethon_b200.helm_fermi.generate`, spread over ``workers`` processes, default
-    all host cores)."""
-    import os
+    (:func:`phlegethon_b200.helm_fermi.generate`; ``workers`` > 1 spreads it over that many
+    spawned processes, which needs a ``__main__`` guard in the calling script)."""
     r = dict(X2_TABLE if ranges is None else ranges)
     key = (model,) + tuple(sorted(r.items()))
     if key not in _CACHE:
@@ -151,7 +150,7 @@ def make(model="synthetic", ranges=None, workers=None):
             _CACHE[key] = generate(**r)
         elif model == "fermi":
             from . import helm_fermi
-            _CACHE[key] = helm_fermi.generate(workers=os.cpu_count() if workers is None else workers, **r)
+            _CACHE[key] = helm_fermi.generate(workers=workers or 1, **r)
         else:
             raise KeyError(model)
     return _CACHE[key]
