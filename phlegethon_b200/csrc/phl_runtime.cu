@@ -404,6 +404,22 @@ int check_cfg(const phl_config *c) {
   return PHL_OK;
 }
 
+// Copy the interior box of a reference-layout host array (rows of `row` doubles, `pitch`
+// doubles apart, `rows` of `rows_alloc` rows per slice, `slices` slices) from a compact device
+// buffer, as one strided DMA: the host's ghost layers are left as they are.  Used device to
+// host, where it runs at the link rate (host-to-device strided copies measured slower than
+// sending the ghost layers along, so uploads copy whole arrays).
+cudaError_t copy_box_d2h(const double *dev, double *host_start, size_t row, size_t pitch, size_t rows,
+                         size_t rows_alloc, size_t slices, cudaStream_t s) {
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  p.srcPtr = make_cudaPitchedPtr(const_cast<double *>(dev), row * sizeof(double), row, rows);
+  p.dstPtr = make_cudaPitchedPtr(host_start, pitch * sizeof(double), pitch, rows_alloc);
+  p.extent = make_cudaExtent(row * sizeof(double), rows, slices);
+  p.kind = cudaMemcpyDeviceToHost;
+  return cudaMemcpy3DAsync(&p, s);
+}
+
 // A background array (nv comps with a component index `comp`) is a profile along x2 when all
 // its interior values agree along x1 and x3 for every x2 index.  On success fills prof[0..n2).
 bool extract_profile(const double *a, int nv, int comp, int n1, int n2, int n3, int o1, int o2, int o3,
@@ -791,13 +807,13 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
     ctx->split_to_prim();
     CK(cudaGetLastError());
   }
-  // pack into a staging copy of the host array so its ghost cells are preserved
+  // transpose into a compact staging block, then one strided copy into the interior of the host
+  // array (its ghost cells are left as they are); the stream orders the reuse of the block
   auto pack_cell = [&](double *h, int ncomp, const double *src) -> int {
-    CK(cudaMemcpyAsync(ctx->stage_buf, h, sizeof(double) * (size_t)ncomp * Ng, cudaMemcpyHostToDevice, s));
-    k_pack<<<nblk(N, 256), 256, 0, s>>>(src, ctx->stage_buf, ncomp, nx, ny, nz, n1, n2, G, G, G3, ncomp, N);
+    k_pack<<<nblk(N, 256), 256, 0, s>>>(src, ctx->stage_buf, ncomp, nx, ny, nz, nx, ny, 0, 0, 0, ncomp, N);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h, ctx->stage_buf, sizeof(double) * (size_t)ncomp * Ng, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    double *start = h + (size_t)ncomp * ((size_t)G + (size_t)n1 * ((size_t)G + (size_t)n2 * G3));
+    CK(copy_box_d2h(ctx->stage_buf, start, (size_t)ncomp * nx, (size_t)ncomp * n1, ny, n2, nz, s));
     return PHL_OK;
   };
   if (f->prim && (rc = pack_cell(f->prim, nv, ctx->W[ctx->cur]))) return rc;
@@ -810,15 +826,16 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
       if (!f->b_x[d]) continue;
       int b1 = nx + 2 + (d == 0), b2 = ny + 2 + (d == 1), b3 = sd == 3 ? nz + 2 + (d == 2) : 1;
       int o3 = sd == 3 ? 1 : 0;
-      long long nb = (long long)b1 * b2 * b3;
-      CK(cudaMemcpyAsync(ctx->stage_buf, f->b_x[d], sizeof(double) * nb, cudaMemcpyHostToDevice, s));
-      k_pack<<<nblk(ctx->nfaces(d), 256), 256, 0, s>>>(ctx->bf[d], ctx->stage_buf, 1, nx + (d == 0), ny + (d == 1),
-                                                       nz + (d == 2), b1, b2, 1, 1, o3, 1, ctx->nfaces(d));
+      (void)b3;
+      const int fx = nx + (d == 0), fy = ny + (d == 1), fz = nz + (d == 2);
+      k_pack<<<nblk(ctx->nfaces(d), 256), 256, 0, s>>>(ctx->bf[d], ctx->stage_buf, 1, fx, fy, fz, fx, fy, 0, 0, 0, 1,
+                                                       ctx->nfaces(d));
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(f->b_x[d], ctx->stage_buf, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
+      double *start = f->b_x[d] + (1 + (size_t)b1 * (1 + (size_t)b2 * o3));
+      CK(copy_box_d2h(ctx->stage_buf, start, fx, b1, fy, b2, fz, s));
     }
   }
+  CK(cudaStreamSynchronize(s));
   return PHL_OK;
 }
 
