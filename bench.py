@@ -260,14 +260,27 @@ def pinned_like(a):
     return t, v
 
 
-def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind, want_e2e):
-    """Time one arithmetic form on the workload; returns timings and the final host state."""
+def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind, want_e2e, learned=False):
+    """Time one arithmetic form on the workload; returns timings and the final host state.
+    learned: the split form with the learned temperature guess in the step's Newton (the
+    network is trained on the device first, untimed)."""
+    import ctypes as C
+
     import torch
     from phlegethon_b200 import abi
     from phlegethon_b200.grid import HostGrid
 
-    c = cfg.replace(precision=form, device=local)
+    c = cfg.replace(precision=form, device=local, eos_guess="mlp" if learned else cfg.eos_guess)
     sim = abi.Simulation(c, table)
+    train = None
+    if learned:
+        loss = C.c_double()
+        t0 = time.perf_counter()
+        rc = sim.lib.phl_mlp_train(sim.ctx, 1 << 22, 12345, args.train_epochs, 8192, C.c_double(3e-3), C.byref(loss))
+        if rc != 0:
+            raise RuntimeError("phl_mlp_train failed: %d" % rc)
+        train = {"samples": 1 << 22, "epochs": args.train_epochs, "seconds": time.perf_counter() - t0,
+                 "loss": loss.value}
     sim.upload(h)
     sim.init_thermo()
     sim.compute_hyperbolic_dt()
@@ -290,7 +303,10 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
     status = sim.status()
     out = h.copy()
     sim.download(out)
-    res = {"form": form, "ms": ms, "done": done, "clocks": clocks, "status": status, "state": out}
+    res = {"form": form, "ms": ms, "done": done, "clocks": clocks, "status": status, "state": out, "train": train}
+    if learned:
+        sim.close()
+        return res
 
     # dominant kernel: hydro_step launches the RK stage kernels back to back (no graph); their
     # average duration is measured with events on the library's stream
@@ -398,6 +414,21 @@ def run_ours(args):
         results[form] = measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
                                      want_e2e=(form == head_form))
     head = results[head_form]
+    learned_step = None
+    if head_form == "fp32_split" and name == "stratified_mhd" and not args.no_learned:
+        # the same split form with the learned temperature guess in the step (metric's
+        # "FP32+learned-EoS"), timed the same way; the warm-start form stays the headline
+        lr = measure_form(args, name, cfg, h, table, head_form, local, dist, peaks, peak_kind, want_e2e=False,
+                          learned=True)
+        from util import field_errors
+        st = lr["status"]
+        learned_step = {"value": aggregate_rate(world, lr["done"], cells, lr["ms"]),
+                        "ms_per_step": lr["ms"] / max(lr["done"], 1),
+                        "newton_iters_per_call": st["newton_iterations"] / max(st["newton_calls"], 1),
+                        "warm_newton_iters_per_call": head["status"]["newton_iterations"]
+                        / max(head["status"]["newton_calls"], 1),
+                        "accepted": st["mlp_accepted"] / max(st["newton_calls"], 1),
+                        "l1_vs_warm": field_errors(lr["state"], head["state"]), "train": lr["train"]}
     l1_long = None
     if args.l1_steps and head_form != "fp64":
         l1_long = {"steps": args.l1_steps, "errors": long_run_errors(cfg, h, table, head_form, args.l1_steps, local)}
@@ -441,7 +472,7 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
                 "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
                                "speedup_of_form": value / fp64_value},
-                "l1_vs_fp64": errors, "l1_vs_fp64_long": l1_long,
+                "l1_vs_fp64": errors, "l1_vs_fp64_long": l1_long, "learned_guess_step": learned_step,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": head["h2d"],
                         "d2h_bytes_per_step": head["h2d"]},
@@ -606,6 +637,8 @@ def main():
     ap.add_argument("--no-fasteos", action="store_true",
                     help="Helmholtz boxes without USE_FASTEOS (helm_rhoP_given per Riemann side)")
     ap.add_argument("--form", default="fp32_split", choices=["fp32_split", "fp64"])
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the split MHD form with the learned temperature guess in the step")
     ap.add_argument("--eos-table", default="fermi", choices=["fermi", "synthetic"],
                     help="electron free-energy table of the Helmholtz workloads: the electron-positron "
                          "Fermi gas (helm_fermi) or the closed-form synthetic model (helm_table.generate)")

@@ -83,8 +83,9 @@ typedef struct phl_config {
   int rk_stages;                   /* 2 (RK2_STEPPER) or 3 (RK3_STEPPER) */
   int bc[3][2];                    /* [dim][0 lower, 1 upper] PHL_BC_* */
   int precision;                   /* PHL_FP64 or PHL_FP32_SPLIT */
-  int eos_guess;                   /* PHL_GUESS_WARM (PHL_GUESS_MLP: PHL_E_UNSUPPORTED for the
-                                      step; the batch inversion takes the guess per call) */
+  int eos_guess;                   /* PHL_GUESS_WARM, or PHL_GUESS_MLP for the learned guess in
+                                      the step's Newton (FP32 split MHD form with the Helmholtz
+                                      EoS; train or set the network before the first step) */
   int device;                      /* CUDA device ordinal */
   double x1l, x1u, x2l, x2u, x3l, x3u;
   double gamma_ad, mu;             /* initialize_simulation arguments */

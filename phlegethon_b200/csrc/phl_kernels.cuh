@@ -11,6 +11,7 @@
 // The kernels take `Prm` by value.  Arithmetic follows source/source.F90 operation by operation
 // so that the FP64 instantiation (compiled with --fmad=false) reproduces the reference.
 #pragma once
+#include <cuda_bf16.h>
 #include "phl_device.cuh"
 
 namespace phl {
@@ -85,6 +86,10 @@ struct Prm {
   // the detector's marks of cells -2..n+1 (index + 2), the pressure equilibrium with its ghost
   // layers (profile along x2 or full ghosted array, ghost offset sf_G), and eps_sf
   unsigned char *sf_flag, *sf_mark;
+  // learned temperature guess inside the step (eos_guess = PHL_GUESS_MLP): the trained
+  // network's FP32 parameters and BF16 copy of W2, nullptr for the warm start
+  const float *mlp_w;
+  const __nv_bfloat16 *mlp_w2bf;
   const double *sf_eq_p;
   int sf_G, sf_eq_profile;
   double eps_sf;

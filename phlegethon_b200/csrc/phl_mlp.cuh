@@ -75,7 +75,7 @@ __device__ __forceinline__ double u01(unsigned long long seed, long long i, int 
   return (double)(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
-__global__ void k_mlp_make_samples(HelmTable h, long long n, unsigned long long seed, float *feat, float *target) {
+static __global__ void k_mlp_make_samples(HelmTable h, long long n, unsigned long long seed, float *feat, float *target) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double lrho = -2.0 + 11.0 * u01(seed, i, 0);
@@ -106,7 +106,7 @@ struct MlpTrainSmem {
   alignas(32) float dW2[MLP_H][MLP_H];
 };
 
-__global__ void __launch_bounds__(128) k_mlp_train_step(const float *params, const __nv_bfloat16 *w2bf,
+static __global__ void __launch_bounds__(128) k_mlp_train_step(const float *params, const __nv_bfloat16 *w2bf,
                                                         const float *feat, const float *target, long long n,
                                                         long long offset, int batch, float *partial,
                                                         float *loss_partial) {
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128) k_mlp_train_step(const float *params, con
 }
 
 // fixed-order sum of the per-CTA partial gradients
-__global__ void k_mlp_reduce(const float *partial, int nblocks, float *grad) {
+static __global__ void k_mlp_reduce(const float *partial, int nblocks, float *grad) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= MLP_NPARAM) return;
   float s = 0.0f;
@@ -253,7 +253,7 @@ __global__ void k_mlp_reduce(const float *partial, int nblocks, float *grad) {
   grad[p] = s;
 }
 
-__global__ void k_mlp_adam(float *params, const float *grad, float *m, float *v, float lr, float b1, float b2,
+static __global__ void k_mlp_adam(float *params, const float *grad, float *m, float *v, float lr, float b1, float b2,
                            float eps, int step, __nv_bfloat16 *w2bf) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= MLP_NPARAM) return;
@@ -268,12 +268,12 @@ __global__ void k_mlp_adam(float *params, const float *grad, float *m, float *v,
   if (p >= MLP_OFF_W2 && p < MLP_OFF_B2) w2bf[p - MLP_OFF_W2] = __float2bfloat16(w);
 }
 
-__global__ void k_mlp_to_bf16(const float *params, __nv_bfloat16 *w2bf) {
+static __global__ void k_mlp_to_bf16(const float *params, __nv_bfloat16 *w2bf) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < MLP_H * MLP_H) w2bf[q] = __float2bfloat16(params[MLP_OFF_W2 + q]);
 }
 
-__global__ void k_mlp_init(float *params, unsigned long long seed) {
+static __global__ void k_mlp_init(float *params, unsigned long long seed) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= MLP_NPARAM) return;
   double u = u01(seed, p, 7) * 2.0 - 1.0;
@@ -371,7 +371,7 @@ __device__ __forceinline__ float mlp_forward_cta(const MlpWeights &m, const floa
 }
 
 // per-sample inference kernel (features n x 4 -> log10 T), 128 threads per block
-__global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out,
+static __global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out,
                                                    unsigned long long *stalled) {
   __shared__ MlpUmmaSmem S;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

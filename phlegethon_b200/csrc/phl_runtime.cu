@@ -305,6 +305,11 @@ struct phl_ctx {
     }
     P.bcc_in = bcc;
     P.bcc_out = bcc;
+    if (cfg.eos_guess == PHL_GUESS_MLP && eos.mlp.ready) {
+      MlpWeights mw = eos.mlp.weights();
+      P.mlp_w = mw.w;
+      P.mlp_w2bf = mw.w2bf;
+    }
     P.sf_flag = sf_flag;
     P.sf_mark = sf_mark;
     P.sf_eq_p = sf_eq_p;
@@ -359,6 +364,10 @@ struct phl_ctx {
     P.gout = gam[cur];
     runner->split_to_prim(P, stream);
   }
+  void drop_graphs() {
+    for (int p = 0; p < 2; ++p)
+      if (graph[p]) { cudaGraphExecDestroy(graph[p]); graph[p] = nullptr; }
+  }
   // hydro_step: all RK stages starting from W[cur]
   void launch_stages() {
     for (int s = 0; s < cfg.rk_stages; ++s) runner->stage(prm(s), stream);
@@ -394,13 +403,15 @@ int check_cfg(const phl_config *c) {
     // the detector tests cells lx-2..ux+2 with central differences: 3 ghost layers
     if (c->ngc < 3 || !(c->eps_sf == c->eps_sf)) return PHL_E_INVALID;
   }
-  // the step's Newton starts from the previous stage's temperature (the reference's warm start);
-  // the learned guess is offered by the batch inversion entry points only
-  if (c->eos_guess == PHL_GUESS_MLP) {
-    g_last_error = "eos_guess = PHL_GUESS_MLP: the step uses the warm start; use the batch inversion";
+  // the FP64 form keeps the reference's warm start (bit-exact); the learned guess inside the step
+  // is built for the split MHD stage (Helmholtz), judged by the Newton with the warm start as
+  // the fallback
+  if (c->eos_guess == PHL_GUESS_MLP &&
+      !(c->precision == PHL_FP32_SPLIT && (c->flags & PHL_MHD) && (c->flags & PHL_HELMHOLTZ))) {
+    g_last_error = "eos_guess = PHL_GUESS_MLP in the step is built for the FP32 split MHD form with the Helmholtz EoS";
     return PHL_E_UNSUPPORTED;
   }
-  if (c->eos_guess != PHL_GUESS_WARM) return PHL_E_INVALID;
+  if (c->eos_guess != PHL_GUESS_WARM && c->eos_guess != PHL_GUESS_MLP) return PHL_E_INVALID;
   return PHL_OK;
 }
 
@@ -843,6 +854,10 @@ static int ready(phl_ctx *ctx) {
   if (!ctx) return PHL_E_INVALID;
   if (!ctx->uploaded) return PHL_E_STATE;
   if ((ctx->cfg.flags & PHL_HELMHOLTZ) && !ctx->table_loaded) return PHL_E_NO_TABLE;
+  if (ctx->cfg.eos_guess == PHL_GUESS_MLP && !ctx->eos.mlp.ready) {
+    g_last_error = "eos_guess = PHL_GUESS_MLP: train the network (phl_mlp_train) or set its parameters first";
+    return PHL_E_STATE;
+  }
   return PHL_OK;
 }
 
@@ -1145,7 +1160,9 @@ int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs
   if (!ctx || n <= 0 || epochs < 0 || batch <= 0) return PHL_E_INVALID;
   if (!ctx->table_loaded) return PHL_E_NO_TABLE;
   CK(cudaSetDevice(ctx->cfg.device));
-  return ctx->eos.mlp_train(ctx->helm, ctx->stream, n, seed, epochs, batch, lr, final_loss);
+  int rc = ctx->eos.mlp_train(ctx->helm, ctx->stream, n, seed, epochs, batch, lr, final_loss);
+  ctx->drop_graphs();  // step graphs bake the network's parameter pointers into their kernels
+  return rc;
 }
 
 int phl_mlp_gradient(phl_ctx *ctx, long long n, const float *features, const float *targets, float *grad,
@@ -1164,7 +1181,9 @@ int phl_mlp_get_params(phl_ctx *ctx, float *params) {
 int phl_mlp_set_params(phl_ctx *ctx, const float *params) {
   if (!ctx || !params) return PHL_E_INVALID;
   CK(cudaSetDevice(ctx->cfg.device));
-  return ctx->eos.mlp_set(ctx->stream, params);
+  int rc = ctx->eos.mlp_set(ctx->stream, params);
+  ctx->drop_graphs();
+  return rc;
 }
 
 int phl_mlp_infer_device(phl_ctx *ctx, long long n, const float *features, float *out) {

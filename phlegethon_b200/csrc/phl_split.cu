@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include "phl_eos_fast.cuh"
+#include "phl_mlp.cuh"
 #include "phl_umma.cuh"
 #include "phl_runner.h"
 
@@ -593,6 +594,7 @@ __device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int
 struct SplitStat {
   double smax = 0.0;
   unsigned long long calls = 0, iters = 0, nonconv = 0, clamp = 0, bad = 0;
+  unsigned long long mlp_acc = 0, mlp_rej = 0, gevals = 0;  // learned guess in the step
 };
 
 // Everything of a stage after the flux divergence, for one cell: flux divergence to physical
@@ -704,6 +706,11 @@ __device__ __forceinline__ void split_stat_flush(const Prm &P, const SplitStat &
     block_sum_atomic(st.iters, P.stat + STAT_NEWTON_ITERS);
     block_sum_atomic(st.nonconv, P.stat + STAT_NEWTON_NONCONV);
     block_sum_atomic(st.clamp, P.stat + STAT_NEWTON_CLAMP);
+    if (P.mlp_w) {
+      block_sum_atomic(st.mlp_acc, P.stat + STAT_MLP_ACC);
+      block_sum_atomic(st.mlp_rej, P.stat + STAT_MLP_REJ);
+      block_sum_atomic(st.gevals, P.stat + STAT_GUESS_EVALS);
+    }
   }
   block_sum_atomic(st.bad, P.stat + STAT_NONFINITE);
 }
@@ -1345,19 +1352,25 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P) {
 
 // MHD stage, part 3: flux divergence from the face fluxes, gravity and the RK combine of U (FP64),
 // b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
-// deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed
-template <class C>
+// deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed.
+// LEARNED (eos_guess = PHL_GUESS_MLP): the block's 128 cells get the learned temperature guess
+// from one tensor-core product (mlp_forward_cta); a guess is accepted when the reference Newton
+// converges from it within 3 iterations without leaving the table, otherwise the cell's Newton
+// starts again from the warm guess (the previous stage's temperature)
+template <class C, bool LEARNED = false>
 __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = c < g.N;
   SplitStat st;
-  if (c < g.N) {
+  long long bc = 0;
+  double bcc[3] = {0, 0, 0}, u[NV], rho = 1.0, inv_rho = 1.0, eint = 0.0;
+  if (valid) {
     int i, j, k;
     unflatten3(c, g.nx[0], g.nx[1], i, j, k);
-    const long long bc = bg_cc(g, i, j, k);
-    double bcc[3] = {0, 0, 0};
+    bc = bg_cc(g, i, j, k);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
@@ -1391,7 +1404,6 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
       for (int d = 0; d < DIM; ++d)
         rd[1 + d] -= rho_dev_phys * __ldg(P.grav + (long long)d * (g.bg_profile ? g.nx[1] : g.N) + bc);
     }
-    double u[NV];
     {
       const double dt = P.scal[1], a1 = P.a1, a2 = P.a2, a3 = P.c3 * dt;
       double un[NV];
@@ -1411,21 +1423,54 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
         P.U[(long long)iv * g.N + c] = u[iv];
       }
     }
-    double rho = u[0], inv_rho = 1.0 / rho;
+    rho = u[0];
+    inv_rho = 1.0 / rho;
     double ke = u[1] * u[1] + u[2] * u[2] + (DIM == 3 ? u[3] * u[3] : 0.0);
-    double eint = u[IP] - 0.5 * ke * inv_rho;
+    eint = u[IP] - 0.5 * ke * inv_rho;
     eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
     if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
+  }
+  float lT_mlp = 0.0f;
+  if constexpr (LEARNED && C::HELM) {
+    // features from the new state (one EoS evaluation for the cold energy), then one CTA-wide
+    // tensor-core product for the 128 cells of the block (all threads take part)
+    extern __shared__ __align__(128) unsigned char mlp_sm[];
+    MlpUmmaSmem &S = *reinterpret_cast<MlpUmmaSmem *>(mlp_sm);
+    float feat[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (valid) {
+      const double ye = u[IAS] * inv_rho, abar = 1.0 / (u[IAS + 1] * inv_rho), zbar = ye * abar;
+      mlp_features(rho, eint * inv_rho - mlp_cold_energy(P.helm, rho, abar, zbar), abar, zbar, feat);
+      st.gevals += 1;
+    }
+    lT_mlp = mlp_forward_cta(MlpWeights{P.mlp_w, P.mlp_w2bf}, feat, S, P.stat + STAT_TC_STALLED);
+  }
+  if (valid) {
     double p, T, sound;
     if (C::HELM) {
       double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
       double abar = 1.0 / inv_abar, zbar = ye * abar;
-      T = P.temp[c];
-      int clamped = 0;
+      int clamped = 0, it = 0;
       bool conv = false;
       HelmCell hc;
-      helm_cell_init(P.helm, hc, rho, abar, zbar, T);
-      int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+      if constexpr (LEARNED) {
+        // judged guess: at most 3 reference Newton iterations from the learned guess
+        T = fmin(fmax(exp10((double)lT_mlp), P.helm.Tl * 1.000001), P.helm.Th * 0.999999);
+        helm_cell_init(P.helm, hc, rho, abar, zbar, T);
+        it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 3, clamped, conv);
+        if (conv && clamped == 0) {
+          st.mlp_acc += 1;
+        } else {
+          st.mlp_rej += 1;
+          st.iters += it;
+          clamped = 0;
+          conv = false;
+        }
+      }
+      if (!LEARNED || !conv) {
+        T = P.temp[c];
+        helm_cell_init(P.helm, hc, rho, abar, zbar, T);
+        it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+      }
       st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
       helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
       if (C::FAST) {
@@ -1676,6 +1721,12 @@ struct SplitRunnerT : Runner {
       k_bface_split<C, 0><<<nblk(nfc(0), 256), 256, 0, s>>>(P);
       k_bface_split<C, 1><<<nblk(nfc(1), 256), 256, 0, s>>>(P);
       if constexpr (C::DIM == 3) k_bface_split<C, 2><<<nblk(nfc(2), 256), 256, 0, s>>>(P);
+      if constexpr (C::HELM) {
+        if (P.mlp_w) {
+          k_c2p_mhd_split<C, true><<<nblk(g.N, 128), 128, sizeof(MlpUmmaSmem), s>>>(P);
+          return;
+        }
+      }
       k_c2p_mhd_split<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
     } else {
       hydro_stage(P, s);

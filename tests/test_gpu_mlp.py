@@ -130,3 +130,41 @@ def test_bracket_guess_matches_oracle_bitwise(gpu_lib, oracle, table):
     To, ito = helm.invert_batch(rho, e, abar, zbar, guess=2, nthreads=4)
     assert np.array_equal(Tg, To)
     assert np.array_equal(itg, ito)
+
+
+# ------------------------------------------------------------------------------ learned guess in the step
+def test_learned_guess_inside_the_split_mhd_step(gpu_lib, table):
+    """eos_guess = PHL_GUESS_MLP: every cell's Newton starts from the trained network's guess,
+    judged by at most 3 reference iterations with the warm start as the fallback.  The state
+    equals the warm-start run to the Newton tolerance, and most guesses are accepted (about 70%
+    in this moderately degenerate box, where the network's 0.2% error leaves the third Newton
+    step just above the tolerance for the rest)."""
+    import ctypes as C
+    from phlegethon_b200.abi import Simulation
+    from util import field_errors
+    cfg, h = problems.stratified_3d(16, ny=16, nz=16, mhd=True)
+    out, stats = {}, {}
+    for guess in ("warm", "mlp"):
+        c = cfg.replace(precision="fp32_split", eos_guess=guess)
+        hg = h.copy()
+        with Simulation(c, table) as sim:
+            if guess == "mlp":
+                loss = C.c_double()
+                # the full training of the EoS benchmark (2^22 samples, 256 epochs, ~5 s)
+                assert sim.lib.phl_mlp_train(sim.ctx, 1 << 22, 11, 256, 8192, C.c_double(3e-3), C.byref(loss)) == 0
+            sim.upload(hg)
+            sim.init_thermo()
+            sim.compute_hyperbolic_dt()
+            sim.reset_status()
+            done, _ = sim.time_loop(10)
+            assert done == 10
+            sim.download(hg)
+            stats[guess] = sim.status()
+        out[guess] = hg
+    err = field_errors(out["mlp"], out["warm"])
+    assert max(err[f] for f in ("rho", "p", "e", "T")) <= 1e-9, err
+    s = stats["mlp"]
+    assert s["nonfinite"] == 0 and s["newton_nonconverged"] == 0
+    assert s["mlp_accepted"] + s["mlp_rejected"] == s["newton_calls"]
+    assert s["mlp_accepted"] > 0.5 * s["newton_calls"], s
+    assert s["guess_evaluations"] == s["newton_calls"]
