@@ -1043,14 +1043,66 @@ __device__ __forceinline__ void load_bccf_at(const Prm &P, long long c, float b[
   b[2] = C::DIM == 3 ? __ldg(P.bccf + 2 * P.g.N + c) : 0.0f;
 }
 
-// MHD flux through the low face of cell m along d (cells m-2..m+1); also the induction flux
-// Fb (lab frame) and rho_L + rho_R at the face for the CT upwinding sign (source.F90:8138-9105
-// with the MHD parts 8327-8469, 8926-8959)
+// Riemann part of an MHD face along d (face index fidx, background index fbg): the edge states
+// in the cell frame (qL/qR in the order of the FP32 state, transverse B in bL/bR; FASTEOS gammas
+// gL/gR with the equilibrium gamma_e already added, or the face temperature guess tface of the
+// Helmholtz configurations without FASTEOS) are rotated to the normal frame, the WB background
+// and the face-normal B are added, and the flux and the induction flux Fb come back in the cell
+// frame with rho_L + rho_R for the CT upwinding sign (source.F90:8138-9105 with the MHD parts
+// 8327-8469, 8926-8959)
+template <class C>
+__device__ __forceinline__ void face_solve_split_mhd(const Prm &P, int d, long long fidx, long long fbg, float qL[C::NV],
+                                                     float qR[C::NV], float bL[3], float bR[3], const float gLin[2],
+                                                     const float gRin[2], float tface, bool flat, float F[C::NV],
+                                                     float Fb[3], float &rho_sum) {
+  constexpr int NV = C::NV, IP = C::IP;
+  const Geo &g = P.g;
+  const float bn = (float)(P.bf[d][fidx] * P.inv_b_ref);
+  bL[d] = bn;
+  bR[d] = bn;
+  if (d == 1) {
+    float a = qL[1], c = qL[2]; qL[1] = c; qL[2] = -a;
+    a = qR[1]; c = qR[2]; qR[1] = c; qR[2] = -a;
+    a = bL[0]; c = bL[1]; bL[0] = c; bL[1] = -a;
+    a = bR[0]; c = bR[1]; bR[0] = c; bR[1] = -a;
+  } else if (C::DIM == 3 && d == 2) {
+    float a = qL[1], c = qL[2], e = qL[3]; qL[1] = e; qL[2] = a; qL[3] = c;
+    a = qR[1]; c = qR[2]; e = qR[3]; qR[1] = e; qR[2] = a; qR[3] = c;
+    a = bL[0]; c = bL[1]; e = bL[2]; bL[0] = e; bL[1] = a; bL[2] = c;
+    a = bR[0]; c = bR[1]; e = bR[2]; bR[0] = e; bR[1] = a; bR[2] = c;
+  }
+  float pe = 0.0f;
+  if (C::WB) {
+    float rho_eq = __ldg(P.sf_rho_f[d] + fbg);
+    qL[0] = rho_eq + qL[0];
+    qR[0] = rho_eq + qR[0];
+    pe = __ldg(P.sf_p_f[d] + fbg);
+  }
+  float gL[2] = {gLin[0], gLin[1]}, gR[2] = {gRin[0], gRin[1]};
+  if (!C::FAST && C::HELM) {
+    split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
+    split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
+  }
+  riemann_mhd_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
+                                                   Fb, flat, g.all_mach != 0);
+  if (d == 1) {
+    float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
+    a = Fb[0]; c = Fb[1]; Fb[0] = -c; Fb[1] = a;
+  } else if (C::DIM == 3 && d == 2) {
+    float a = F[1], c = F[2], e = F[3]; F[1] = c; F[2] = e; F[3] = a;
+    a = Fb[0]; c = Fb[1]; e = Fb[2]; Fb[0] = c; Fb[1] = e; Fb[2] = a;
+  }
+  rho_sum = qL[0] + qR[0];
+  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.sf_phi_f[d] + fbg);
+}
+
+// MHD flux through the low face of cell m along d from cells m-SW..m+SW-1 (w, gm, b: cells
+// m-3..m+2); reconstruction, then face_solve_split_mhd
 template <class C>
 __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi, int fj, int fk, const float *const w[6],
                                                     const float *const gm[6], const float *const b[6], float F[C::NV],
                                                     float Fb[3], float &rho_sum) {
-  constexpr int NV = C::NV, IP = C::IP;
+  constexpr int NV = C::NV;
   const Geo &g = P.g;
   bool fa = false, fb = false;  // USE_SHOCK_FLATTENING: is_flattened of cells m-1 and m
   if (C::SF) {
@@ -1072,30 +1124,9 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
     rec_face_f32<C>(v, C::REC == REC_LIM5TH, bL[iv], bR[iv]);
     if (C::SF && C::REC != REC_LIM2ND) flatten_face_f32(v, fa, fb, bL[iv], bR[iv]);
   }
-  const float bn = (float)(P.bf[d][face_lin(g, d, fi, fj, fk)] * P.inv_b_ref);
-  bL[d] = bn;
-  bR[d] = bn;
-  if (d == 1) {
-    float a = qL[1], c = qL[2]; qL[1] = c; qL[2] = -a;
-    a = qR[1]; c = qR[2]; qR[1] = c; qR[2] = -a;
-    a = bL[0]; c = bL[1]; bL[0] = c; bL[1] = -a;
-    a = bR[0]; c = bR[1]; bR[0] = c; bR[1] = -a;
-  } else if (C::DIM == 3 && d == 2) {
-    float a = qL[1], c = qL[2], e = qL[3]; qL[1] = e; qL[2] = a; qL[3] = c;
-    a = qR[1]; c = qR[2]; e = qR[3]; qR[1] = e; qR[2] = a; qR[3] = c;
-    a = bL[0]; c = bL[1]; e = bL[2]; bL[0] = e; bL[1] = a; bL[2] = c;
-    a = bR[0]; c = bR[1]; e = bR[2]; bR[0] = e; bR[1] = a; bR[2] = c;
-  }
-  float pe = 0.0f;
   long long fbg = 0;
   if (C::WB || C::ETOT) fbg = bg_face(g, d, fi, fj, fk);
-  if (C::WB) {
-    float rho_eq = __ldg(P.sf_rho_f[d] + fbg);
-    qL[0] = rho_eq + qL[0];
-    qR[0] = rho_eq + qR[0];
-    pe = __ldg(P.sf_p_f[d] + fbg);
-  }
-  float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
+  float gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f}, tface = 0.0f;
   if (C::FAST) {
     const bool late = C::SF && C::WB && d == 0;
     float gv[2][6];
@@ -1113,21 +1144,10 @@ __device__ __forceinline__ void face_flux_split_mhd(const Prm &P, int d, int fi,
       if (late) flatten_gamma_x1(gv, fa, fb, ge, gL, gR);
     }
   } else if (C::HELM) {
-    const float tface = 0.5f * (gm[2][0] + gm[3][0]);
-    split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
-    split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
+    tface = 0.5f * (gm[2][0] + gm[3][0]);
   }
-  riemann_mhd_split<C::DIM, NV, C::EOSM, C::RIEM>(qL, qR, bL, bR, gL, gR, pe, (float)g.gm, (float)g.mach_cutoff, F,
-                                                   Fb, C::SF && (fa || fb), g.all_mach != 0);
-  if (d == 1) {
-    float a = F[1], c = F[2]; F[1] = -c; F[2] = a;
-    a = Fb[0]; c = Fb[1]; Fb[0] = -c; Fb[1] = a;
-  } else if (C::DIM == 3 && d == 2) {
-    float a = F[1], c = F[2], e = F[3]; F[1] = c; F[2] = e; F[3] = a;
-    a = Fb[0]; c = Fb[1]; e = Fb[2]; Fb[0] = c; Fb[1] = e; Fb[2] = a;
-  }
-  rho_sum = qL[0] + qR[0];
-  if (C::ETOT) F[IP] = F[IP] + F[0] * __ldg(P.sf_phi_f[d] + fbg);
+  face_solve_split_mhd<C>(P, d, face_lin(g, d, fi, fj, fk), fbg, qL, qR, bL, bR, gL, gR, tface, C::SF && (fa || fb), F,
+                          Fb, rho_sum);
 }
 
 // FP32 face EMF components (units v_ref b_ref) and the CT mass-flux sign (source.F90:8926-8951)
@@ -1201,6 +1221,123 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.fflux[d][(long long)iv * nf + f] = F[iv];
   store_face_emf_split<C>(P, d, f, d == 0 ? fi : (d == 1 ? fj : fk), Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
+}
+
+// faces per thread of the walking face kernels: along x (threads of a warp step K0 cells apart,
+// so their loads stay within a few cache lines) and along y, z (threads of a warp are
+// neighbours in x and walk side by side)
+constexpr int WALK_K0 = 4, WALK_K = 8;
+// resident blocks of 128 threads per SM the walking kernels are compiled for
+constexpr int WALK_MINB = 6;
+
+// Raw values of one cell for the walking face kernel: the FP32 state (0..NV-1), cell B (NV..NV+2)
+// and the two FASTEOS gammas or the temperature (NV+3, NV+4).  q is the cell's index along D and
+// c[] its other two coordinates; a cell inside the domain along D is read by linear index lc,
+// a ghost maps its index.
+template <class C, int D>
+__device__ __forceinline__ void load_walk_cell(const Prm &P, const int c[3], int q, long long lc, float r[C::NV + 5]) {
+  float *w = r, *b = r + C::NV, *gm = r + C::NV + 3;
+  gm[0] = gm[1] = 0.0f;
+  if (q >= 0 && q < P.g.nx[D]) {
+    load_wf_at<C>(P, lc, w, gm);
+    load_bccf_at<C>(P, lc, b);
+  } else {
+    const int i = D == 0 ? q : c[0], j = D == 1 ? q : c[1], k = D == 2 ? q : c[2];
+    load_wf<C>(P, i, j, k, w, gm);
+    load_bccf<C>(P, i, j, k, b);
+  }
+}
+
+// MHD stage, part 1 for LIM2ND reconstruction: one thread walks K consecutive faces along D.  A
+// cell borders two faces of the walk, so its values are loaded and its PLM slope formed once
+// (the per-face kernel does both twice) and its edge values are carried to the next face.  The
+// faces, their arithmetic and the stored results are those of k_face_split_mhd.
+template <class C, int D, int K>
+__global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_face_split_mhd_walk(Prm P) {
+  static_assert(C::REC == REC_LIM2ND, "the walk carries LIM2ND edge values");
+  if (!*P.active) return;
+  constexpr int NV = C::NV, NR = NV + 5;
+  const Geo &g = P.g;
+  const int nd = g.nx[D] + 1, nch = (nd + K - 1) / K;
+  const int e0 = D == 0 ? nch : g.nx[0], e1 = D == 1 ? nch : g.nx[1];
+  const int e2 = D == 2 ? nch : (C::DIM == 3 ? g.nx[2] : 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)e0 * e1 * e2) return;
+  int c[3];
+  unflatten3(t, e0, e1, c[0], c[1], c[2]);
+  const int q0 = c[D] * K, qend = min(q0 + K, nd);
+  c[D] = 0;
+  const long long nf = nfaces(g, D), cstride = dir_stride(g, D);
+  const long long fstride = D == 0 ? 1 : (D == 1 ? (long long)g.nx[0] : (long long)g.nx[0] * g.nx[1]);
+  const long long crow = lin(g, c[0], c[1], c[2]), frow = face_lin(g, D, c[0], c[1], c[2]);
+  const long long sfrow = C::SF ? sf_flag_index<C>(g, c[0], c[1], c[2]) : 0;
+  const long long sfstride = D == 0 ? 1 : (D == 1 ? (long long)(g.nx[0] + 2) : (long long)(g.nx[0] + 2) * (g.nx[1] + 2));
+  const float smax_s = (float)(P.scal[2] * P.inv_v_ref);
+  // window: rm, rc = cells q-1, q; hip = edge values at the high side of cell q-1
+  float rm[NR], rc[NR], rp[NR], lo[NR], hi[NR], hip[NR];
+  load_walk_cell<C, D>(P, c, q0 - 2, crow + (long long)(q0 - 2) * cstride, rm);
+  load_walk_cell<C, D>(P, c, q0 - 1, crow + (long long)(q0 - 1) * cstride, rc);
+  load_walk_cell<C, D>(P, c, q0, crow + (long long)q0 * cstride, rp);
+#pragma unroll
+  for (int v = 0; v < NR; ++v) {
+    plm_f32(rm[v], rc[v], rp[v], lo[v], hip[v]);
+    rm[v] = rc[v];
+    rc[v] = rp[v];
+  }
+  bool fprev = C::SF && P.sf_flag[sfrow + (long long)(q0 - 1) * sfstride] != 0;
+#pragma unroll 1
+  for (int q = q0; q < qend; ++q) {
+    load_walk_cell<C, D>(P, c, q + 1, crow + (long long)(q + 1) * cstride, rp);
+#pragma unroll
+    for (int v = 0; v < NR; ++v) plm_f32(rm[v], rc[v], rp[v], lo[v], hi[v]);
+    const bool fa = fprev, fb = C::SF && P.sf_flag[sfrow + (long long)q * sfstride] != 0;
+    float qL[NV], qR[NV], bL[3] = {0.f, 0.f, 0.f}, bR[3] = {0.f, 0.f, 0.f}, gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+      qL[iv] = hip[iv];
+      qR[iv] = lo[iv];
+    }
+#pragma unroll
+    for (int a = 0; a < C::DIM; ++a) {
+      if (a == D) continue;
+      bL[a] = hip[NV + a];
+      bR[a] = lo[NV + a];
+    }
+    const long long fidx = frow + (long long)q * fstride;
+    long long fbg = 0;
+    if (C::WB || C::ETOT) fbg = g.bg_profile ? (long long)(D == 1 ? q : c[1]) : fidx;
+    float tface = 0.0f;
+    if (C::FAST) {
+      gL[0] = hip[NV + 3]; gL[1] = hip[NV + 4];
+      gR[0] = lo[NV + 3]; gR[1] = lo[NV + 4];
+      if (C::WB) {
+        const float ge = __ldg(P.sf_ge_f[D] + fbg);
+        const float rL[2] = {gL[0], gL[1]}, rR[2] = {gR[0], gR[1]};
+        gL[0] = gL[0] + ge;
+        gR[0] = gR[0] + ge;
+        // the x1 sweep's gamma handling on flagged faces (flatten_gamma_x1 with the LIM2ND
+        // edges already at hand)
+        if (C::SF && D == 0) {
+          if (fa) { gL[0] = rL[0]; gL[1] = rL[1]; gR[0] = gR[0] + ge; }
+          if (fb) { gR[0] = rR[0]; gR[1] = rR[1]; gL[0] = gL[0] + ge; }
+        }
+      }
+    } else if (C::HELM) {
+      tface = 0.5f * (rm[NV + 3] + rc[NV + 3]);
+    }
+    float F[NV], Fb[3], rs;
+    face_solve_split_mhd<C>(P, D, fidx, fbg, qL, qR, bL, bR, gL, gR, tface, C::SF && (fa || fb), F, Fb, rs);
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) P.fflux[D][(long long)iv * nf + fidx] = F[iv];
+    store_face_emf_split<C>(P, D, fidx, q, Fb, F[0], rs, smax_s);
+#pragma unroll
+    for (int v = 0; v < NR; ++v) {
+      hip[v] = hi[v];
+      rm[v] = rc[v];
+      rc[v] = rp[v];
+    }
+    fprev = fb;
+  }
 }
 
 // FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
@@ -1710,10 +1847,23 @@ struct SplitRunnerT : Runner {
       auto ncor = [&](int a) {
         return (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
       };
-      k_face_split_mhd<C, 0><<<nblk(nfc(0), 128), 128, 0, s>>>(P);
-      k_face_split_mhd<C, 1><<<nblk(nfc(1), 128), 128, 0, s>>>(P);
+      if constexpr (C::REC == REC_LIM2ND) {
+        // threads of the walking kernels: faces along D in chunks of K, times the other extents
+        auto nwalk = [&](int d, int k) {
+          long long n = (g.nx[d] + 1 + k - 1) / k;
+          for (int a = 0; a < C::DIM; ++a)
+            if (a != d) n *= g.nx[a];
+          return n;
+        };
+        k_face_split_mhd_walk<C, 0, WALK_K0><<<nblk(nwalk(0, WALK_K0), 128), 128, 0, s>>>(P);
+        k_face_split_mhd_walk<C, 1, WALK_K><<<nblk(nwalk(1, WALK_K), 128), 128, 0, s>>>(P);
+        if constexpr (C::DIM == 3) k_face_split_mhd_walk<C, 2, WALK_K><<<nblk(nwalk(2, WALK_K), 128), 128, 0, s>>>(P);
+      } else {
+        k_face_split_mhd<C, 0><<<nblk(nfc(0), 128), 128, 0, s>>>(P);
+        k_face_split_mhd<C, 1><<<nblk(nfc(1), 128), 128, 0, s>>>(P);
+        if constexpr (C::DIM == 3) k_face_split_mhd<C, 2><<<nblk(nfc(2), 128), 128, 0, s>>>(P);
+      }
       if constexpr (C::DIM == 3) {
-        k_face_split_mhd<C, 2><<<nblk(nfc(2), 128), 128, 0, s>>>(P);
         k_corner_split<C, 0><<<nblk(ncor(0), 256), 256, 0, s>>>(P);
         k_corner_split<C, 1><<<nblk(ncor(1), 256), 256, 0, s>>>(P);
       }
