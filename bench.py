@@ -268,21 +268,27 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
 
     import torch
     from phlegethon_b200 import abi
-    from phlegethon_b200.grid import HostGrid
+    from phlegethon_b200.grid import HostGrid, helm_state_range
 
     c = cfg.replace(precision=form, device=local, eos_guess="mlp" if learned else cfg.eos_guess)
     sim = abi.Simulation(c, table)
     train = None
+    sim.upload(h)
+    sim.init_thermo()
     if learned:
+        # the network is fitted over the states of the run: log10 rho and log10 T of the initial
+        # state widened by 0.1 dex, its Abar and Zbar
+        h0 = h.copy()
+        sim.download(h0)
+        lo, hi = helm_state_range(h0, cfg)
+        sim.set_mlp_sample_range(lo, hi)
         loss = C.c_double()
         t0 = time.perf_counter()
         rc = sim.lib.phl_mlp_train(sim.ctx, 1 << 22, 12345, args.train_epochs, 8192, C.c_double(3e-3), C.byref(loss))
         if rc != 0:
             raise RuntimeError("phl_mlp_train failed: %d" % rc)
         train = {"samples": 1 << 22, "epochs": args.train_epochs, "seconds": time.perf_counter() - t0,
-                 "loss": loss.value}
-    sim.upload(h)
-    sim.init_thermo()
+                 "loss": loss.value, "range_lo": lo, "range_hi": hi}
     sim.compute_hyperbolic_dt()
     stream = torch.cuda.ExternalStream(sim.stream(), device=torch.device("cuda", local))
     sim.time_loop(args.warmup)

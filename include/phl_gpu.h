@@ -211,14 +211,20 @@ int phl_eos_energy_device(phl_ctx *ctx, long long n, const double *rho, const do
 /* ---- learned temperature guess: MLP 4-64-64-1 (log10 rho, log10 e, Abar, Zbar -> log10 T),
  * BF16 weights with FP32 accumulation on the tensor cores.  No reference counterpart. */
 #define PHL_MLP_NPARAMS (4 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
-/* Sample n (rho, T, Abar, Zbar) points from the given log ranges with a counter-based RNG
- * (seed), evaluate e with the EoS, and train for `epochs` passes with Adam.  final_loss may be
- * NULL.  Everything runs on the device with the project's own kernels. */
+/* Sample n (rho, T, Abar, Zbar) points from the sample range (phl_mlp_set_sample_range) with a
+ * counter-based RNG (seed), evaluate e with the EoS, and train for `epochs` passes with Adam.
+ * final_loss may be NULL.  Everything runs on the device with the project's own kernels. */
 int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs, int batch,
                   double lr, double *final_loss);
+/* Range the training samples are drawn from, uniform in each coordinate: lo/hi[0] log10 rho,
+ * [1] log10 T (inside the table), [2] Abar, [3] Zbar (1 <= lo <= hi); lo[k] == hi[k] fixes a
+ * coordinate.  lo == NULL restores the default: log10 rho in [-2, 9], log10 T in [4, 10], Abar
+ * in [1, 56], Zbar in [1, max(Abar/2, 1)].  A network trained on the range of the states a run
+ * holds guesses them closer.  Takes effect at the next phl_mlp_train. */
+int phl_mlp_set_sample_range(phl_ctx *ctx, const double *lo, const double *hi);
 /* One gradient evaluation of the mean-squared loss on n training pairs (host pointers:
- * features n x 4 FP32, targets n FP32 as (log10 T - 7)/3), with the current parameters; n must
- * be a multiple of 64.  grad receives PHL_MLP_NPARAMS floats; loss may be NULL. */
+ * features n x 4 FP32, targets n FP32 in the network's output units), with the current
+ * parameters; n must be a multiple of 64.  grad receives PHL_MLP_NPARAMS floats; loss may be NULL. */
 int phl_mlp_gradient(phl_ctx *ctx, long long n, const float *features, const float *targets, float *grad,
                      double *loss);
 /* FP32 master weights in the order W1(64x4), b1(64), W2(64x64), b2(64), W3(1x64), b3(1). */

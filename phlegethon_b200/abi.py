@@ -35,6 +35,7 @@ EXPORTS = [
     "phl_reset_status", "phl_eos_invert_batch_device", "phl_eos_invert_batch",
     "phl_eos_energy_device", "phl_mlp_train", "phl_mlp_get_params", "phl_mlp_set_params",
     "phl_mlp_infer_device", "phl_mlp_gradient", "phl_device_field", "phl_stream", "phl_eos_invert_batch_noalloc",
+    "phl_mlp_set_sample_range",
 ]
 
 
@@ -125,6 +126,7 @@ def load_library(path: str = LIB_PATH):
         "phl_mlp_set_params": ([vp, C.POINTER(C.c_float)], C.c_int),
         "phl_mlp_infer_device": ([vp, C.c_longlong, vp, vp], C.c_int),
         "phl_mlp_gradient": ([vp, C.c_longlong, vp, vp, vp, _P], C.c_int),
+        "phl_mlp_set_sample_range": ([vp, _P, _P], C.c_int),
         "phl_device_field": ([vp, C.c_char_p], vp),
         "phl_stream": ([vp], vp),
     }
@@ -258,6 +260,15 @@ class Simulation:
         t, dt, smax = C.c_double(), C.c_double(), C.c_double()
         _check(self.lib.phl_get_time(self.ctx, C.byref(t), C.byref(dt), C.byref(smax)), "phl_get_time")
         return t.value, dt.value, smax.value
+
+    def set_mlp_sample_range(self, lo=None, hi=None):
+        """Range the learned guess is trained on: lo/hi = (log10 rho, log10 T, Abar, Zbar);
+        None restores the default (the EoS benchmark range)."""
+        if lo is None:
+            rc = self.lib.phl_mlp_set_sample_range(self.ctx, None, None)
+        else:
+            rc = self.lib.phl_mlp_set_sample_range(self.ctx, (C.c_double * 4)(*lo), (C.c_double * 4)(*hi))
+        _check(rc, "phl_mlp_set_sample_range")
 
     def time_loop(self, nsteps, tmax=float("inf")):
         done, t = C.c_int(), C.c_double()

@@ -68,15 +68,40 @@ __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell 
   helm_cell_contract_with(h, c, jh, r0, r1, c.A);
 }
 
-__device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, double rho, double abar,
-                                               double zbar, double T) {
-  c.Ye = zbar / abar;
+// density part of the cell: table row of rho * Ye and the position in it
+__device__ __forceinline__ void helm_cell_init_rho(const HelmTable &h, HelmCell &c, double rho, double ye) {
+  c.Ye = ye;
   c.rhos = rho * c.Ye;
   c.ih = helm_node_index(h.rho, h.nrho, h.log10_rho1, h.drho, c.rhos);
   double r_lo = __ldg(h.rho + c.ih - 1);
   c.drho = __ldg(h.rho + c.ih) - r_lo;
   c.x = (c.rhos - r_lo) * (1.0 / c.drho);
+}
+
+__device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, double rho, double abar,
+                                               double zbar, double T) {
+  helm_cell_init_rho(h, c, rho, zbar / abar);
   helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
+}
+
+// specific energy at the table's lowest temperature T_lo (the cold energy the learned guess's
+// features subtract) from the density part of the cell: at a temperature node the quintic T
+// basis reduces to the node's value and first derivative, so only f and f_T of the row's first
+// T node are contracted (given2's E at T_lo to rounding)
+__device__ __forceinline__ double helm_cell_cold_energy(const HelmTable &h, const HelmCell &c, double irho,
+                                                        double inv_abar) {
+  double r0[3], r1[3];
+  helm_cell_rbasis(c, r0, r1);
+  const double *lo = h.tab + 9 * (long long)(c.ih - 1), *hi = lo + 9;
+  const int var[2][3] = {{0, 3, 4}, {1, 5, 6}};
+  double f = 0.0, fT = 0.0;
+#pragma unroll
+  for (int orr = 0; orr < 3; ++orr) {
+    f = fma(__ldg(lo + var[0][orr]), r0[orr], fma(__ldg(hi + var[0][orr]), r1[orr], f));
+    fT = fma(__ldg(lo + var[1][orr]), r0[orr], fma(__ldg(hi + var[1][orr]), r1[orr], fT));
+  }
+  const double T = __ldg(h.T), T3 = T * T * T;
+  return c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T3 * T * irho;
 }
 
 // f, f_T, f_TT at T (T inside the current cell)

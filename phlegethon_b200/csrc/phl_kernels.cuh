@@ -41,6 +41,8 @@ struct Cfg {
   static constexpr int MINB_C2P32 = HELM_ ? 6 : 1;
 };
 
+struct MlpSmall;
+
 struct Prm {
   Geo g;
   const double *__restrict__ Win;
@@ -90,6 +92,10 @@ struct Prm {
   // network's FP32 parameters and BF16 copy of W2, nullptr for the warm start
   const float *mlp_w;
   const __nv_bfloat16 *mlp_w2bf;
+  // host copy of the network's FP32 layer-1 and layer-3 parameters, read by the host when it
+  // launches the learned cons->prim kernel (never dereferenced on the device)
+  const MlpSmall *mlp_small;
+  float *mlp_feat, *mlp_out;  // per-cell network inputs [cells][4] and log10 T guesses (NaN: none)
   const double *sf_eq_p;
   int sf_G, sf_eq_profile;
   double eps_sf;

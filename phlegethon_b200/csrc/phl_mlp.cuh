@@ -62,8 +62,15 @@ struct MlpWeights {
   const __nv_bfloat16 *w2bf;    // BF16 copy of W2 (row-major [out][in])
 };
 
-// counter-based sample of the EoS benchmark distribution: log10 rho ~ U[-2,9],
-// log10 T ~ U[4,10], Abar ~ U[1,56], Zbar ~ U[1, max(Abar/2,1)]
+// Training-sample distribution: log10 rho ~ U[lrho], log10 T ~ U[lT], Abar ~ U[abar], and
+// Zbar ~ U[zbar] when zbar[1] > 0, else Zbar ~ U[1, max(Abar/2, 1)].  The default is the EoS
+// benchmark range; a run can narrow it to the states it holds (a network fitted over a smaller
+// range guesses closer).
+struct MlpRange {
+  double lrho[2] = {-2.0, 9.0}, lT[2] = {4.0, 10.0}, abar[2] = {1.0, 56.0}, zbar[2] = {1.0, -1.0};
+};
+
+// counter-based hash for the samples
 __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -75,13 +82,15 @@ __device__ __forceinline__ double u01(unsigned long long seed, long long i, int 
   return (double)(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
-static __global__ void k_mlp_make_samples(HelmTable h, long long n, unsigned long long seed, float *feat, float *target) {
+static __global__ void k_mlp_make_samples(HelmTable h, long long n, unsigned long long seed, MlpRange r, float *feat,
+                                          float *target) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double lrho = -2.0 + 11.0 * u01(seed, i, 0);
-  double lT = 4.0 + 6.0 * u01(seed, i, 1);
-  double abar = 1.0 + 55.0 * u01(seed, i, 2);
-  double zbar = 1.0 + fmax(abar * 0.5 - 1.0, 0.0) * u01(seed, i, 3);
+  double lrho = r.lrho[0] + (r.lrho[1] - r.lrho[0]) * u01(seed, i, 0);
+  double lT = r.lT[0] + (r.lT[1] - r.lT[0]) * u01(seed, i, 1);
+  double abar = r.abar[0] + (r.abar[1] - r.abar[0]) * u01(seed, i, 2);
+  double zbar = r.zbar[1] > 0.0 ? r.zbar[0] + (r.zbar[1] - r.zbar[0]) * u01(seed, i, 3)
+                                : 1.0 + fmax(abar * 0.5 - 1.0, 0.0) * u01(seed, i, 3);
   double rho = exp10(lrho), T = exp10(lT), E, dE;
   helm_given2(h, rho, T, abar, zbar, E, dE, false);
   float f[4];
@@ -370,6 +379,116 @@ __device__ __forceinline__ float mlp_forward_cta(const MlpWeights &m, const floa
   return mlp_prior(x) + out * MLP_OUT_SCALE + MLP_OUT_SHIFT;
 }
 
+// The FP32 parameters of layers 1 and 3 by value: passed as a __grid_constant__ kernel argument
+// they sit in the constant bank, and the fully unrolled layer arithmetic takes them as operands
+// instead of loading them.
+struct MlpSmall {
+  float w1[MLP_H * MLP_IN], b1[MLP_H], b2[MLP_H], w3[MLP_H], b3;
+};
+inline void mlp_small_from_params(const float *p, MlpSmall &w) {
+  for (int i = 0; i < MLP_H * MLP_IN; ++i) w.w1[i] = p[MLP_OFF_W1 + i];
+  for (int i = 0; i < MLP_H; ++i) {
+    w.b1[i] = p[MLP_OFF_B1 + i];
+    w.b2[i] = p[MLP_OFF_B2 + i];
+    w.w3[i] = p[MLP_OFF_W3 + i];
+  }
+  w.b3 = p[MLP_OFF_B3];
+}
+
+// Persistent form of mlp_forward_cta for a block that runs the network on many tiles of 128
+// samples: the tensor-memory columns, the mbarrier and W2 in shared memory are set up once per
+// block (mlp_cta_setup) and released once (mlp_cta_teardown); each tile (mlp_forward_tile, all
+// 128 threads, uniform control flow) waits on the mbarrier phase of its parity.
+__device__ __forceinline__ void mlp_cta_setup(const __nv_bfloat16 *w2bf, MlpUmmaSmem &S) {
+  const int tid = threadIdx.x;
+  if ((tid >> 5) == 0) {
+    tmem_alloc(&S.tmem, MLP_UMMA_COLS);
+    tmem_relinquish();
+  }
+  if (tid == 0) mbar_init(&S.mbar, 1);
+  for (int q = tid; q < MLP_H * 8; q += blockDim.x) {
+    const int n = q >> 3, c = q & 7;
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(w2bf + n * MLP_H) + c);
+    *reinterpret_cast<uint4 *>(S.B + umma_kmajor_offset(n, 8 * c)) = v;
+  }
+}
+
+// One tile: returns log10 T of this thread's sample.  ok (uniform over the block) says that the
+// tensor-core path is usable: a product that does not complete within the poll limit counts in
+// *stalled, gives no guess for its tile (*have = false) and turns ok off for the block's later
+// tiles, whose samples then get no guess either.
+__device__ __forceinline__ float mlp_forward_tile(const MlpSmall &w, const float x[4], MlpUmmaSmem &S,
+                                                  uint32_t parity, bool &ok, bool &have,
+                                                  unsigned long long *stalled) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+#pragma unroll
+  for (int c = 0; c < MLP_H / 8; ++c) {
+    uint32_t pk[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float h2[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int o = 8 * c + 2 * j + e;
+        float a = w.b1[o];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a = fmaf(w.w1[o * 4 + k], x[k], a);
+        h2[e] = fmaxf(a, 0.0f);
+      }
+      __nv_bfloat162 b2v = __floats2bfloat162_rn(h2[0], h2[1]);
+      pk[j] = *reinterpret_cast<uint32_t *>(&b2v);
+    }
+    *reinterpret_cast<uint4 *>(S.A + umma_kmajor_offset(tid, 8 * c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+  }
+  fence_proxy_async_smem();
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+  const uint32_t tbase = S.tmem;
+  bool done = false;
+  if (ok) {
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(S.A), b0 = smem_u32(S.B);
+      constexpr uint32_t idesc = umma_idesc_bf16(128, MLP_H);
+#pragma unroll
+      for (int kk = 0; kk < MLP_H / 16; ++kk)
+        umma_bf16_f32(tbase, umma_desc(a0 + kk * UMMA_KSTEP_BYTES, UMMA_KCORE_BYTES, UMMA_ROW_GROUP_BYTES),
+                      umma_desc(b0 + kk * UMMA_KSTEP_BYTES, UMMA_KCORE_BYTES, UMMA_ROW_GROUP_BYTES), idesc, kk > 0);
+      umma_commit(&S.mbar);
+    }
+    done = __any_sync(0xffffffffu, mbar_wait_bounded(&S.mbar, parity, MLP_UMMA_POLLS));
+    tc_fence_after_sync();
+  }
+  float out = w.b3;
+  if (done) {
+    const uint32_t row_addr = tbase + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c = 0; c < MLP_H / 16; ++c) {
+      float z[16];
+      tmem_ld16(row_addr + 16 * c, z);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) out = fmaf(w.w3[16 * c + q], fmaxf(z[q] + w.b2[16 * c + q], 0.0f), out);
+    }
+  } else if (ok) {
+    if (lane == 0 && stalled) atomicAdd(stalled, 1ull);
+    // a second bounded chance for the product to land before A and the columns are reused
+    mbar_wait_bounded(&S.mbar, parity, MLP_UMMA_POLLS);
+  }
+  tc_fence_before_sync();
+  const bool all_done = __syncthreads_and(done);
+  tc_fence_after_sync();
+  have = done;
+  ok = ok && all_done;
+  return mlp_prior(x) + out * MLP_OUT_SCALE + MLP_OUT_SHIFT;
+}
+
+__device__ __forceinline__ void mlp_cta_teardown(MlpUmmaSmem &S) {
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(S.tmem, MLP_UMMA_COLS);
+}
+
 // per-sample inference kernel (features n x 4 -> log10 T), 128 threads per block
 static __global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long long n, const float *feat, float *out,
                                                    unsigned long long *stalled) {
@@ -384,6 +503,7 @@ static __global__ void __launch_bounds__(128) k_mlp_infer(MlpWeights m, long lon
 
 struct Mlp {
   bool ready = false;
+  MlpRange range;
   float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *partial = nullptr, *lossp = nullptr;
   float *feat = nullptr, *target = nullptr;
   __nv_bfloat16 *w2bf = nullptr;
@@ -463,7 +583,7 @@ struct Mlp {
     if (cudaFuncSetAttribute(k_mlp_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(MlpTrainSmem)) != cudaSuccess)
       return -2;
-    k_mlp_make_samples<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h, n, seed, feat, target);
+    k_mlp_make_samples<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h, n, seed, range, feat, target);
     if (!ready) {
       k_mlp_init<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(params, seed ^ 0xABCDEFull);
       k_mlp_to_bf16<<<(MLP_H * MLP_H + 255) / 256, 256, 0, s>>>(params, w2bf);

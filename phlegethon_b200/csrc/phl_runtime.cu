@@ -207,6 +207,7 @@ struct phl_ctx {
   float *bccf = nullptr, *femf[3] = {}, *fsgn[3] = {}, *fcor[3] = {};                // split MHD
   float *fflux[3] = {};
   float *fecell = nullptr;                                                             // split MHD
+  float *mlp_feat = nullptr, *mlp_out = nullptr;  // learned guess in the split MHD step
   double *dflux[3] = {};                                                               // FP64 MHD
   // USE_SHOCK_FLATTENING: flags, detector marks, ghosted pressure equilibrium (see Prm)
   unsigned char *sf_flag = nullptr, *sf_mark = nullptr;
@@ -222,6 +223,9 @@ struct phl_ctx {
   double *htab = nullptr, *hdpd = nullptr, *hrho = nullptr, *hT = nullptr;
   HelmTable helm{};
   bool table_loaded = false, uploaded = false, bg_uploaded = false;
+  // host copy of the network's FP32 layers 1 and 3 (argument of the learned cons->prim kernel)
+  MlpSmall mlp_small{};
+  bool mlp_small_ok = false;
   // staging
   double *stage_buf = nullptr;
   size_t stage_bytes = 0;
@@ -289,6 +293,8 @@ struct phl_ctx {
     P.inv_b_ref = 1.0 / P.b_ref;
     P.bccf = bccf;
     P.fecell = fecell;
+    P.mlp_feat = mlp_feat;
+    P.mlp_out = mlp_out;
     for (int d = 0; d < 3; ++d) {
       P.femf[d] = femf[d]; P.fsgn[d] = fsgn[d]; P.fcor[d] = fcor[d]; P.fflux[d] = fflux[d];
       P.dflux[d] = dflux[d];
@@ -309,6 +315,7 @@ struct phl_ctx {
       MlpWeights mw = eos.mlp.weights();
       P.mlp_w = mw.w;
       P.mlp_w2bf = mw.w2bf;
+      P.mlp_small = mlp_small_ok ? &mlp_small : nullptr;
     }
     P.sf_flag = sf_flag;
     P.sf_mark = sf_mark;
@@ -559,6 +566,10 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
     if (c->split) {
       if ((rc = c->alloc(&c->bccf, (size_t)3 * N))) return rc;
       if ((rc = c->alloc(&c->fecell, (size_t)3 * N))) return rc;
+      if (cfg->eos_guess == PHL_GUESS_MLP) {
+        if ((rc = c->alloc(&c->mlp_feat, (size_t)4 * N))) return rc;
+        if ((rc = c->alloc(&c->mlp_out, (size_t)N))) return rc;
+      }
       for (int d = 0; d < cfg->sdims; ++d) {
         long long nf = c->nfaces(d);
         if ((rc = c->alloc(&c->femf[d], (size_t)3 * nf))) return rc;
@@ -850,11 +861,12 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
   return PHL_OK;
 }
 
-static int ready(phl_ctx *ctx) {
+// step: the call advances the state (and so runs the cons->prim Newton with the selected guess)
+static int ready(phl_ctx *ctx, bool step = false) {
   if (!ctx) return PHL_E_INVALID;
   if (!ctx->uploaded) return PHL_E_STATE;
   if ((ctx->cfg.flags & PHL_HELMHOLTZ) && !ctx->table_loaded) return PHL_E_NO_TABLE;
-  if (ctx->cfg.eos_guess == PHL_GUESS_MLP && !ctx->eos.mlp.ready) {
+  if (step && ctx->cfg.eos_guess == PHL_GUESS_MLP && !ctx->eos.mlp.ready) {
     g_last_error = "eos_guess = PHL_GUESS_MLP: train the network (phl_mlp_train) or set its parameters first";
     return PHL_E_STATE;
   }
@@ -899,7 +911,7 @@ int phl_compute_hyperbolic_dt(phl_ctx *ctx, double *dt, double *smax) {
 }
 
 int phl_hydro_step(phl_ctx *ctx) {
-  int rc = ready(ctx);
+  int rc = ready(ctx, true);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
   k_set_active<<<1, 1, 0, ctx->stream>>>(ctx->active, ctx->smax_bits);
@@ -932,7 +944,7 @@ int phl_get_time(phl_ctx *ctx, double *time, double *dt, double *smax) {
 }
 
 int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double *time) {
-  int rc = ready(ctx);
+  int rc = ready(ctx, true);
   if (rc) return rc;
   if (nsteps < 0) return PHL_E_INVALID;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1161,8 +1173,38 @@ int phl_mlp_train(phl_ctx *ctx, long long n, unsigned long long seed, int epochs
   if (!ctx->table_loaded) return PHL_E_NO_TABLE;
   CK(cudaSetDevice(ctx->cfg.device));
   int rc = ctx->eos.mlp_train(ctx->helm, ctx->stream, n, seed, epochs, batch, lr, final_loss);
-  ctx->drop_graphs();  // step graphs bake the network's parameter pointers into their kernels
+  ctx->drop_graphs();  // step graphs bake the network's parameters into their kernels
+  ctx->mlp_small_ok = false;
+  if (rc == 0) {
+    std::vector<float> p(MLP_NPARAM);
+    rc = ctx->eos.mlp_get(ctx->stream, p.data());
+    if (rc == 0) {
+      mlp_small_from_params(p.data(), ctx->mlp_small);
+      ctx->mlp_small_ok = true;
+    }
+  }
   return rc;
+}
+
+int phl_mlp_set_sample_range(phl_ctx *ctx, const double *lo, const double *hi) {
+  if (!ctx) return PHL_E_INVALID;
+  MlpRange r;
+  if (lo) {
+    if (!hi) return PHL_E_INVALID;
+    for (int k = 0; k < 4; ++k)
+      if (!std::isfinite(lo[k]) || !std::isfinite(hi[k]) || lo[k] > hi[k]) return PHL_E_INVALID;
+    if (lo[2] < 1.0 || lo[3] < 1.0) return PHL_E_INVALID;
+    if (ctx->table_loaded && (lo[1] < std::log10(ctx->helm.Tl) || hi[1] > std::log10(ctx->helm.Th))) {
+      g_last_error = "phl_mlp_set_sample_range: the log10 T range leaves the table";
+      return PHL_E_INVALID;
+    }
+    r.lrho[0] = lo[0]; r.lrho[1] = hi[0];
+    r.lT[0] = lo[1]; r.lT[1] = hi[1];
+    r.abar[0] = lo[2]; r.abar[1] = hi[2];
+    r.zbar[0] = lo[3]; r.zbar[1] = hi[3];
+  }
+  ctx->eos.mlp.range = r;
+  return PHL_OK;
 }
 
 int phl_mlp_gradient(phl_ctx *ctx, long long n, const float *features, const float *targets, float *grad,
@@ -1183,6 +1225,8 @@ int phl_mlp_set_params(phl_ctx *ctx, const float *params) {
   CK(cudaSetDevice(ctx->cfg.device));
   int rc = ctx->eos.mlp_set(ctx->stream, params);
   ctx->drop_graphs();
+  ctx->mlp_small_ok = rc == 0;
+  if (rc == 0) mlp_small_from_params(params, ctx->mlp_small);
   return rc;
 }
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include "phl_eos_fast.cuh"
 #include "phl_mlp.cuh"
@@ -1487,27 +1488,28 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P) {
   P.bf[d][t] = a1 * b0 + a2 * b + a3 * tmp;
 }
 
-// MHD stage, part 3: flux divergence from the face fluxes, gravity and the RK combine of U (FP64),
-// b_cc from the updated faces (FP64), cons -> prim with the Helmholtz Newton (FP64), FP32
-// deviations and scaled b_cc out; last stage also the CFL max with the Alfven speed.
-// LEARNED (eos_guess = PHL_GUESS_MLP): the block's 128 cells get the learned temperature guess
-// from one tensor-core product (mlp_forward_cta); a guess is accepted when the reference Newton
-// converges from it within 3 iterations without leaving the table, otherwise the cell's Newton
-// starts again from the warm guess (the previous stage's temperature)
-template <class C, bool LEARNED = false>
-__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
-  if (!*P.active) return;
+// New state of one cell that the EoS part of cons->prim needs (the rest is stored before it)
+struct C2pState {
+  double rho = 1.0, inv_rho = 1.0, eint = 0.0, ye = 0.0, inv_abar = 1.0, ca2 = 0.0, vabs[3] = {0.0, 0.0, 0.0};
+  long long bc = 0;
+};
+
+// MHD stage, part 3a: flux divergence from the face fluxes, gravity and the RK combine of U
+// (FP64), b_cc from the updated faces (FP64); stores U (U0 in the first stage), scaled b_cc and
+// what depends on the conserved state alone (FP32 velocities and scalars, cell EMFs), and
+// returns what the EoS part needs (the CFL speeds' inputs in the last stage)
+template <class C>
+__device__ __forceinline__ void c2p_mhd_split_combine(const Prm &P, long long c, C2pState &cs) {
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = c < g.N;
-  SplitStat st;
-  long long bc = 0;
-  double bcc[3] = {0, 0, 0}, u[NV], rho = 1.0, inv_rho = 1.0, eint = 0.0;
-  if (valid) {
+  double &rho = cs.rho, &inv_rho = cs.inv_rho, &eint = cs.eint, &ye = cs.ye, &inv_abar = cs.inv_abar, &ca2 = cs.ca2;
+  double *vabs = cs.vabs;
+  long long &bc = cs.bc;
+  {
     int i, j, k;
     unflatten3(c, g.nx[0], g.nx[1], i, j, k);
     bc = bg_cc(g, i, j, k);
+    double bcc[3] = {0, 0, 0}, u[NV];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       int ui = i + (d == 0), uj = j + (d == 1), uk = k + (d == 2);
@@ -1566,44 +1568,74 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
     eint = u[IP] - 0.5 * ke * inv_rho;
     eint = eint - 0.5 * (bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2]);
     if (C::ETOT) eint = eint - rho * __ldg(P.phi_cc + bc);
-  }
-  float lT_mlp = 0.0f;
-  if constexpr (LEARNED && C::HELM) {
-    // features from the new state (one EoS evaluation for the cold energy), then one CTA-wide
-    // tensor-core product for the 128 cells of the block (all threads take part)
-    extern __shared__ __align__(128) unsigned char mlp_sm[];
-    MlpUmmaSmem &S = *reinterpret_cast<MlpUmmaSmem *>(mlp_sm);
-    float feat[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    if (valid) {
-      const double ye = u[IAS] * inv_rho, abar = 1.0 / (u[IAS + 1] * inv_rho), zbar = ye * abar;
-      mlp_features(rho, eint * inv_rho - mlp_cold_energy(P.helm, rho, abar, zbar), abar, zbar, feat);
-      st.gevals += 1;
+    float vf[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vf[d] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
+      P.Wf_out[(long long)(1 + d) * g.N + c] = vf[d];
     }
-    lT_mlp = mlp_forward_cta(MlpWeights{P.mlp_w, P.mlp_w2bf}, feat, S, P.stat + STAT_TC_STALLED);
+    {
+      const float bf3[3] = {(float)(bcc[0] * P.inv_b_ref), (float)(bcc[1] * P.inv_b_ref),
+                            DIM == 3 ? (float)(bcc[2] * P.inv_b_ref) : 0.0f};
+      store_cell_emf(P, c, vf, bf3);
+    }
+#pragma unroll
+    for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
+    if (C::HELM) {
+      ye = u[IAS] * inv_rho;
+      inv_abar = u[IAS + 1] * inv_rho;
+    }
+    if (P.last_stage) {
+      ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vabs[d] = fabs(u[1 + d] * inv_rho);
+    }
   }
-  if (valid) {
+}
+
+// MHD stage, part 3b: cons -> prim of the new state with the Helmholtz Newton (FP64) from the
+// warm guess (the previous stage's temperature), or with LEARNED from the network's guess lT
+// (log10 T; NaN for none): the guess is accepted when the reference Newton converges from it
+// within 3 iterations without leaving the table, otherwise the Newton starts again from the
+// warm guess.  FP32 density and pressure deviations, gammas, T and eint out; last stage the
+// cell's CFL speed with the Alfven speed.
+template <class C, bool LEARNED>
+__device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, const C2pState &cs, float lT_mlp,
+                                                  SplitStat &st) {
+  constexpr int IP = C::IP, DIM = C::DIM;
+  const Geo &g = P.g;
+  const double rho = cs.rho, inv_rho = cs.inv_rho, eint = cs.eint, ye = cs.ye, inv_abar = cs.inv_abar, ca2 = cs.ca2;
+  const double *vabs = cs.vabs;
+  const long long bc = cs.bc;
+  HelmCell hc;
+  {
     double p, T, sound;
     if (C::HELM) {
-      double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
-      double abar = 1.0 / inv_abar, zbar = ye * abar;
+      const double abar = 1.0 / inv_abar, zbar = ye * abar;
       int clamped = 0, it = 0;
       bool conv = false;
-      HelmCell hc;
       if constexpr (LEARNED) {
-        // judged guess: at most 3 reference Newton iterations from the learned guess
-        T = fmin(fmax(exp10((double)lT_mlp), P.helm.Tl * 1.000001), P.helm.Th * 0.999999);
-        helm_cell_init(P.helm, hc, rho, abar, zbar, T);
-        it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 3, clamped, conv);
-        if (conv && clamped == 0) {
+        // judged guess: at most 3 reference Newton iterations from the learned guess (the
+        // density part of the cell is already set)
+        const bool have_guess = !isnan(lT_mlp);
+        helm_cell_init_rho(P.helm, hc, rho, zbar / abar);
+        if (have_guess) {
+          T = fmin(fmax((double)exp10f(lT_mlp), P.helm.Tl * 1.000001), P.helm.Th * 0.999999);
+          helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+          it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 3, clamped, conv);
+        }
+        if (have_guess && conv && clamped == 0) {
           st.mlp_acc += 1;
         } else {
           st.mlp_rej += 1;
           st.iters += it;
           clamped = 0;
           conv = false;
+          T = P.temp[c];
+          helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+          it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
         }
-      }
-      if (!LEARNED || !conv) {
+      } else {
         T = P.temp[c];
         helm_cell_init(P.helm, hc, rho, abar, zbar, T);
         it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
@@ -1629,34 +1661,113 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
       pdev = p - __ldg(P.eq_p_cc + bc);
     }
     P.Wf_out[c] = (float)(rdev * P.inv_rho_ref);
-    float vf[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      vf[d] = (float)(u[1 + d] * inv_rho * P.inv_v_ref);
-      P.Wf_out[(long long)(1 + d) * g.N + c] = vf[d];
-    }
-    {
-      const float bf3[3] = {(float)(bcc[0] * P.inv_b_ref), (float)(bcc[1] * P.inv_b_ref),
-                            DIM == 3 ? (float)(bcc[2] * P.inv_b_ref) : 0.0f};
-      store_cell_emf(P, c, vf, bf3);
-    }
     P.Wf_out[(long long)IP * g.N + c] = (float)(pdev * P.inv_p_ref);
-#pragma unroll
-    for (int iv = IAS; iv < NV; ++iv) P.Wf_out[(long long)iv * g.N + c] = (float)(u[iv] * inv_rho);
     P.temp[c] = T;
     P.eint[c] = eint;
     if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) st.bad += 1;
     if (P.last_stage) {
-      double ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
-      double cs = sqrt(sound * sound + ca2 * inv_rho);
-      double sx1 = (fabs(u[1] * inv_rho) + cs) * g.inv_dx[0];
-      double sx2 = (fabs(u[2] * inv_rho) + cs) * g.inv_dx[1];
+      double csnd = sqrt(sound * sound + ca2 * inv_rho);
+      double sx1 = (vabs[0] + csnd) * g.inv_dx[0];
+      double sx2 = (vabs[1] + csnd) * g.inv_dx[1];
       double sm = sx1 + sx2;
-      if (DIM == 3) sm = (fabs(u[3] * inv_rho) + cs) * g.inv_dx[2] + sm;
+      if (DIM == 3) sm = (vabs[2] + csnd) * g.inv_dx[2] + sm;
       st.smax = sm;
     }
   }
+}
+
+template <class C>
+__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
+  if (!*P.active) return;
+  SplitStat st;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < P.g.N) {
+    C2pState cs;
+    c2p_mhd_split_combine<C>(P, c, cs);
+    c2p_mhd_split_eos<C, false>(P, c, cs, 0.0f, st);
+  }
   split_stat_flush<C>(P, st);
+}
+
+// Learned guess in the step, in three launches so that the cons->prim kernels keep their
+// occupancy (a block-wide tensor-core product inside them would hold all their warps at its
+// barriers): (1) the combine, storing eint and the network's features, (2) k_mlp_guess over
+// all cells, (3) the EoS part from the stored state and guess.
+template <class C>
+__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_features(Prm P) {
+  if (!*P.active) return;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= P.g.N) return;
+  C2pState cs;
+  c2p_mhd_split_combine<C>(P, c, cs);
+  P.eint[c] = cs.eint;
+  // features (the cold energy from the density row of the table)
+  HelmCell hc;
+  const double abar = 1.0 / cs.inv_abar, zbar = cs.ye * abar;
+  helm_cell_init_rho(P.helm, hc, cs.rho, zbar / abar);
+  const double e_th = cs.eint * cs.inv_rho - helm_cell_cold_energy(P.helm, hc, cs.inv_rho, cs.inv_abar);
+  float4 f;
+  f.x = (log10f((float)cs.rho) - 3.5f) / 5.5f;
+  f.y = (log10f((float)fmax(e_th, 1e-30)) - 19.5f) / 8.5f;
+  f.z = (float)((abar - 28.5) / 27.5);
+  f.w = (float)((zbar - 14.0) / 14.0);
+  reinterpret_cast<float4 *>(P.mlp_feat)[c] = f;
+}
+
+template <class C>
+__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_guessed(Prm P) {
+  if (!*P.active) return;
+  constexpr int IAS = C::IAS, DIM = C::DIM;
+  SplitStat st;
+  const Geo &g = P.g;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < g.N) {
+    // the state of the combine, read back: U, eint, and in the last stage b_cc from the faces
+    C2pState cs;
+    int i, j, k;
+    unflatten3(c, g.nx[0], g.nx[1], i, j, k);
+    cs.bc = bg_cc(g, i, j, k);
+    cs.rho = P.U[c];
+    cs.inv_rho = 1.0 / cs.rho;
+    cs.eint = P.eint[c];
+    cs.ye = P.U[(long long)IAS * g.N + c] * cs.inv_rho;
+    cs.inv_abar = P.U[(long long)(IAS + 1) * g.N + c] * cs.inv_rho;
+    if (P.last_stage) {
+      double b2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const double b = 0.5 * (P.bf[d][face_lin(g, d, i + (d == 0), j + (d == 1), k + (d == 2))] +
+                                P.bf[d][face_lin(g, d, i, j, k)]);
+        b2 = d == 0 ? b * b : b2 + b * b;
+        cs.vabs[d] = fabs(P.U[(long long)(1 + d) * g.N + c] * cs.inv_rho);
+      }
+      cs.ca2 = b2;
+    }
+    st.gevals += 1;
+    c2p_mhd_split_eos<C, true>(P, c, cs, P.mlp_out[c], st);
+  }
+  split_stat_flush<C>(P, st);
+}
+
+// network guesses for n samples (features [n][4] -> log10 T, NaN where the product stalled);
+// the FP32 layers come in as a kernel argument (constant-bank operands)
+static __global__ void __launch_bounds__(128) k_mlp_guess(const __grid_constant__ MlpSmall w,
+                                                          const __nv_bfloat16 *w2bf, long long n, const float *feat,
+                                                          float *out, const int *active, unsigned long long *stalled) {
+  if (!*active) return;
+  extern __shared__ __align__(128) unsigned char mlp_sm[];
+  MlpUmmaSmem &S = *reinterpret_cast<MlpUmmaSmem *>(mlp_sm);
+  mlp_cta_setup(w2bf, S);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (t < n) {
+    const float4 f = reinterpret_cast<const float4 *>(feat)[t];
+    x[0] = f.x; x[1] = f.y; x[2] = f.z; x[3] = f.w;
+  }
+  bool ok = true, have = false;
+  const float y = mlp_forward_tile(w, x, S, 0u, ok, have, stalled);
+  mlp_cta_teardown(S);
+  if (t < n) out[t] = have ? y : __int_as_float(0x7fc00000);
 }
 
 // FP64 primitives (+eint, gammaf) -> U (FP64) and FP32 deviations (prim->cons of
@@ -1872,8 +1983,11 @@ struct SplitRunnerT : Runner {
       k_bface_split<C, 1><<<nblk(nfc(1), 256), 256, 0, s>>>(P);
       if constexpr (C::DIM == 3) k_bface_split<C, 2><<<nblk(nfc(2), 256), 256, 0, s>>>(P);
       if constexpr (C::HELM) {
-        if (P.mlp_w) {
-          k_c2p_mhd_split<C, true><<<nblk(g.N, 128), 128, sizeof(MlpUmmaSmem), s>>>(P);
+        if (P.mlp_w && P.mlp_small && P.mlp_feat && P.mlp_out) {
+          k_c2p_mhd_split_features<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+          k_mlp_guess<<<nblk(g.N, 128), 128, sizeof(MlpUmmaSmem), s>>>(*P.mlp_small, P.mlp_w2bf, g.N, P.mlp_feat,
+                                                                       P.mlp_out, P.active, P.stat + STAT_TC_STALLED);
+          k_c2p_mhd_split_guessed<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
           return;
         }
       }

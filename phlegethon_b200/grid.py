@@ -246,3 +246,19 @@ class HostGrid:
 
     def state_bytes(self) -> int:
         return int(sum(a.nbytes for a in self.dynamic_arrays().values()))
+
+
+def helm_state_range(h, cfg, margin=0.1):
+    """(log10 rho, log10 T, Abar, Zbar) lower and upper bounds of a Helmholtz state with the
+    ADVECT_YE_IABAR scalars, the two logarithms widened by ``margin`` dex and the temperatures
+    clipped to the table's (the sample range of ``Simulation.set_mlp_sample_range``)."""
+    w = h.interior(h.prim)
+    ias = 2 + cfg.sdims
+    abar = 1.0 / w[ias + 1]
+    zbar = w[ias] * abar
+    lr, lt = np.log10(w[0]), np.log10(h.interior(h.temp))
+    lo = [float(lr.min()) - margin, max(float(lt.min()) - margin, float(cfg.helm_ltlo)), float(abar.min()),
+          float(zbar.min())]
+    hi = [float(lr.max()) + margin, min(float(lt.max()) + margin, float(cfg.helm_lthi)), float(abar.max()),
+          float(zbar.max())]
+    return lo, hi

@@ -168,3 +168,47 @@ def test_learned_guess_inside_the_split_mhd_step(gpu_lib, table):
     assert s["mlp_accepted"] + s["mlp_rejected"] == s["newton_calls"]
     assert s["mlp_accepted"] > 0.5 * s["newton_calls"], s
     assert s["guess_evaluations"] == s["newton_calls"]
+
+
+@pytest.mark.gpu
+def test_learned_guess_trained_on_the_run_range(gpu_lib, table):
+    """A network fitted over the run's own states (phl_mlp_set_sample_range with log10 rho and
+    log10 T of the box widened by 0.1 dex and its Abar, Zbar) passes the 3-iteration judgment for
+    every cell, and the state equals the warm-start run to the Newton tolerance.  Ranges that
+    are empty or leave the table are refused."""
+    import ctypes as C
+    from phlegethon_b200.abi import PhlError, Simulation
+    from phlegethon_b200.grid import helm_state_range
+    from util import field_errors
+    cfg, h = problems.stratified_3d(16, ny=16, nz=16, mhd=True)
+    out, stats = {}, {}
+    for guess in ("warm", "mlp"):
+        c = cfg.replace(precision="fp32_split", eos_guess=guess)
+        hg = h.copy()
+        with Simulation(c, table) as sim:
+            sim.upload(hg)
+            sim.init_thermo()
+            if guess == "mlp":
+                with pytest.raises(PhlError):
+                    sim.set_mlp_sample_range([5.0, 8.0, 2.0, 1.0], [4.0, 9.0, 2.0, 1.0])
+                with pytest.raises(PhlError):
+                    sim.set_mlp_sample_range([5.0, 8.0, 2.0, 1.0], [6.0, 14.0, 2.0, 1.0])
+                h0 = h.copy()
+                sim.download(h0)
+                lo, hi = helm_state_range(h0, cfg)
+                sim.set_mlp_sample_range(lo, hi)
+                loss = C.c_double()
+                assert sim.lib.phl_mlp_train(sim.ctx, 1 << 22, 11, 256, 8192, C.c_double(3e-3), C.byref(loss)) == 0
+            sim.compute_hyperbolic_dt()
+            sim.reset_status()
+            done, _ = sim.time_loop(10)
+            assert done == 10
+            sim.download(hg)
+            stats[guess] = sim.status()
+        out[guess] = hg
+    err = field_errors(out["mlp"], out["warm"])
+    assert max(err[f] for f in ("rho", "p", "e", "T")) <= 1e-9, err
+    s = stats["mlp"]
+    assert s["nonfinite"] == 0 and s["newton_nonconverged"] == 0
+    assert s["mlp_accepted"] + s["mlp_rejected"] == s["newton_calls"]
+    assert s["mlp_accepted"] >= 0.99 * s["newton_calls"], s
