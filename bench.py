@@ -87,10 +87,11 @@ def stage_kernels(cfg, form):
 # domain once per launch, so the per-launch traffic scales with the cell count
 TRAFFIC_PER_CELL = {("stratified", "fp32_split"): 499.604224e6 / 2097152,
                     ("stratified", "fp64"): 557.258496e6 / 2097152,
-                    # one split MHD stage at 128^3: 3 x the x1 face launch (169.7 MB), corners
-                    # 3 x 42.4 MB, face-B 3 x 34.0 MB, cons->prim 799.8 MB
-                    ("stratified_mhd", "fp32_split"): (3 * 169.697024e6 + 3 * 42.4e6 + 3 * 33.96e6 + 799.823872e6)
-                    / 2097152}
+                    # one split MHD stage at 128^3 (a middle stage: U0 read): walking face
+                    # kernels 213.8 + 171.7 + 175.6 MB, corners 3 x 42.2 MB, face-B 3 x 50.9 MB,
+                    # cons->prim 755.5 MB
+                    ("stratified_mhd", "fp32_split"): (213.8e6 + 171.7e6 + 175.6e6 + 3 * 42.2e6 + 3 * 50.9e6
+                                                       + 755.5e6) / 2097152}
 
 
 def step_bytes_per_cell(cfg):
