@@ -126,11 +126,11 @@ __device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, doub
 
 // Newton on E(rho, T) = E0 from the warm start T (helm_rhoe_given's loop and exit rules);
 // returns iterations, sets converged / clamped.  On return `c` holds the cell of the final T.
-__device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, double rho, double E0,
+__device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, double irho, double E0,
                                               double inv_abar, double &T, int max_iter, int &clamped,
                                               bool &converged) {
   const double Told = T;
-  const double irho = 1.0 / rho, inv_E0 = 1.0 / E0;
+  const double inv_E0 = 1.0 / E0;
   converged = false;
   int used = 0;
   for (int iter = 1; iter <= max_iter; ++iter) {
@@ -155,9 +155,10 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
   return used;
 }
 
-// pressure and relativistic sound speed at (rho, T) from the prepared cell (given_full's output)
-__device__ __forceinline__ void helm_cell_p_sound(const HelmTable &h, const HelmCell &c, double rho, double T,
-                                                  double inv_abar, double &P, double &sound) {
+// pressure and the square of the relativistic sound speed at (rho, T) from the prepared cell
+// (given_full's output; irho = 1 / rho)
+__device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const HelmCell &c, double rho, double irho,
+                                                   double T, double inv_abar, double &P, double &sound2) {
   const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
@@ -206,19 +207,17 @@ __device__ __forceinline__ void helm_cell_p_sound(const HelmTable &h, const Helm
   double dP_drho = c.Ye * dpd;
   double r2 = c.rhos * c.rhos;
   double T3 = T * T * T, T4 = T3 * T;
-  double irho = 1.0 / rho;
   P = r2 * fd + CONST_RGAS * rho * T * inv_abar + CONST_RAD * T4 * (1.0 / 3.0);
   double dP_dT = r2 * fdT + CONST_RGAS * rho * inv_abar + (4.0 / 3.0) * CONST_RAD * T3;
   dP_drho = dP_drho + CONST_RGAS * T * inv_abar;
   double E = c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T4 * irho;
   double cv = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
-  double zz = P * irho;
-  double chiT = T / P * dP_dT;
-  double chirho = dP_drho / zz;
-  double xx = zz * chiT / (T * cv);
-  double gam1 = chiT * xx + chirho;
-  double z = 1.0 + (E + CONST_C2) / zz;
-  sound = CONST_C * sqrt(gam1 / z);
+  // the reference's gam1 / z (chiT = T dP/dT / P, chirho = rho dP/drho / P, x = (P / rho) chiT /
+  // (T cv), gam1 = chiT x + chirho, z = 1 + (E + c^2) rho / P) with the common factor 1 / P
+  // cancelled: two divisions instead of five
+  const double num = T * dP_dT * dP_dT / (rho * cv) + rho * dP_drho;
+  const double den = P + (E + CONST_C2) * rho;
+  sound2 = CONST_C2 * (num / den);
 }
 
 }  // namespace phl

@@ -654,17 +654,19 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
   double p, T, sound = 0.0;
   if (C::HELM) {
     double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
-    double abar = 1.0 / inv_abar, zbar = ye * abar;
     T = P.temp[c];
     int clamped = 0;
     bool conv = false;
     HelmCell hc;
-    helm_cell_init(P.helm, hc, rho, abar, zbar, T);
-    int it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+    helm_cell_init_rho(P.helm, hc, rho, ye);
+    helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+    int it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
     st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
-    helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
+    double sound2;
+    helm_cell_p_sound2(P.helm, hc, rho, inv_rho, T, inv_abar, p, sound2);
+    if (P.last_stage) sound = sqrt(sound2);
     if (C::FAST) {
-      double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+      double ge = p / eint + 1.0, gc = sound2 * rho / p;
       if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
       P.gf_out[c] = (float)ge;
       P.gf_out[g.N + c] = (float)gc;
@@ -1490,20 +1492,19 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P) {
 
 // New state of one cell that the EoS part of cons->prim needs (the rest is stored before it)
 struct C2pState {
-  double rho = 1.0, inv_rho = 1.0, eint = 0.0, ye = 0.0, inv_abar = 1.0, ca2 = 0.0, vabs[3] = {0.0, 0.0, 0.0};
+  double rho = 1.0, inv_rho = 1.0, eint = 0.0, ye = 0.0, inv_abar = 1.0;
   long long bc = 0;
 };
 
 // MHD stage, part 3a: flux divergence from the face fluxes, gravity and the RK combine of U
 // (FP64), b_cc from the updated faces (FP64); stores U (U0 in the first stage), scaled b_cc and
 // what depends on the conserved state alone (FP32 velocities and scalars, cell EMFs), and
-// returns what the EoS part needs (the CFL speeds' inputs in the last stage)
+// returns what the EoS part needs
 template <class C>
 __device__ __forceinline__ void c2p_mhd_split_combine(const Prm &P, long long c, C2pState &cs) {
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
-  double &rho = cs.rho, &inv_rho = cs.inv_rho, &eint = cs.eint, &ye = cs.ye, &inv_abar = cs.inv_abar, &ca2 = cs.ca2;
-  double *vabs = cs.vabs;
+  double &rho = cs.rho, &inv_rho = cs.inv_rho, &eint = cs.eint, &ye = cs.ye, &inv_abar = cs.inv_abar;
   long long &bc = cs.bc;
   {
     int i, j, k;
@@ -1585,11 +1586,6 @@ __device__ __forceinline__ void c2p_mhd_split_combine(const Prm &P, long long c,
       ye = u[IAS] * inv_rho;
       inv_abar = u[IAS + 1] * inv_rho;
     }
-    if (P.last_stage) {
-      ca2 = bcc[0] * bcc[0] + bcc[1] * bcc[1] + bcc[2] * bcc[2];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) vabs[d] = fabs(u[1 + d] * inv_rho);
-    }
   }
 }
 
@@ -1604,25 +1600,23 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
                                                   SplitStat &st) {
   constexpr int IP = C::IP, DIM = C::DIM;
   const Geo &g = P.g;
-  const double rho = cs.rho, inv_rho = cs.inv_rho, eint = cs.eint, ye = cs.ye, inv_abar = cs.inv_abar, ca2 = cs.ca2;
-  const double *vabs = cs.vabs;
+  const double rho = cs.rho, inv_rho = cs.inv_rho, eint = cs.eint, ye = cs.ye, inv_abar = cs.inv_abar;
   const long long bc = cs.bc;
   HelmCell hc;
   {
-    double p, T, sound;
+    double p, T, sound2;
     if (C::HELM) {
-      const double abar = 1.0 / inv_abar, zbar = ye * abar;
       int clamped = 0, it = 0;
       bool conv = false;
       if constexpr (LEARNED) {
         // judged guess: at most 3 reference Newton iterations from the learned guess (the
         // density part of the cell is already set)
         const bool have_guess = !isnan(lT_mlp);
-        helm_cell_init_rho(P.helm, hc, rho, zbar / abar);
+        helm_cell_init_rho(P.helm, hc, rho, ye);
         if (have_guess) {
           T = fmin(fmax((double)exp10f(lT_mlp), P.helm.Tl * 1.000001), P.helm.Th * 0.999999);
           helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
-          it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 3, clamped, conv);
+          it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 3, clamped, conv);
         }
         if (have_guess && conv && clamped == 0) {
           st.mlp_acc += 1;
@@ -1633,17 +1627,18 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
           conv = false;
           T = P.temp[c];
           helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
-          it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+          it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
         }
       } else {
         T = P.temp[c];
-        helm_cell_init(P.helm, hc, rho, abar, zbar, T);
-        it = helm_rhoe_fast(P.helm, hc, rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
+        helm_cell_init_rho(P.helm, hc, rho, ye);
+        helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+        it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
       }
       st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
-      helm_cell_p_sound(P.helm, hc, rho, T, inv_abar, p, sound);
+      helm_cell_p_sound2(P.helm, hc, rho, inv_rho, T, inv_abar, p, sound2);
       if (C::FAST) {
-        double ge = p / eint + 1.0, gc = sound * sound * rho / p;
+        double ge = p / eint + 1.0, gc = sound2 * rho / p;
         if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
         P.gf_out[c] = (float)ge;
         P.gf_out[g.N + c] = (float)gc;
@@ -1653,7 +1648,7 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
     } else {
       p = (g.gm - 1.0) * eint;
       T = p / (rho * CONST_RGAS * (1.0 / g.mu));
-      sound = sqrt(g.gm * p / rho);
+      sound2 = g.gm * p / rho;
     }
     double rdev = rho, pdev = p;
     if (C::WB) {
@@ -1666,7 +1661,18 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
     P.eint[c] = eint;
     if (!(rho > 0.0) || !(p > 0.0) || !(T > 0.0) || !isfinite(eint)) st.bad += 1;
     if (P.last_stage) {
-      double csnd = sqrt(sound * sound + ca2 * inv_rho);
+      // |v| and b_cc^2 of the new state, read back (U and the face B are this cell's own)
+      int i, j, k;
+      unflatten3(c, g.nx[0], g.nx[1], i, j, k);
+      double vabs[3] = {0.0, 0.0, 0.0}, ca2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const double b = 0.5 * (P.bf[d][face_lin(g, d, i + (d == 0), j + (d == 1), k + (d == 2))] +
+                                P.bf[d][face_lin(g, d, i, j, k)]);
+        ca2 = d == 0 ? b * b : ca2 + b * b;
+        vabs[d] = fabs(P.U[(long long)(1 + d) * g.N + c] * inv_rho);
+      }
+      double csnd = sqrt(sound2 + ca2 * inv_rho);
       double sx1 = (vabs[0] + csnd) * g.inv_dx[0];
       double sx2 = (vabs[1] + csnd) * g.inv_dx[1];
       double sm = sx1 + sx2;
@@ -1704,7 +1710,7 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_features(P
   // features (the cold energy from the density row of the table)
   HelmCell hc;
   const double abar = 1.0 / cs.inv_abar, zbar = cs.ye * abar;
-  helm_cell_init_rho(P.helm, hc, cs.rho, zbar / abar);
+  helm_cell_init_rho(P.helm, hc, cs.rho, cs.ye);
   const double e_th = cs.eint * cs.inv_rho - helm_cell_cold_energy(P.helm, hc, cs.inv_rho, cs.inv_abar);
   float4 f;
   f.x = (log10f((float)cs.rho) - 3.5f) / 5.5f;
@@ -1717,12 +1723,12 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_features(P
 template <class C>
 __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_guessed(Prm P) {
   if (!*P.active) return;
-  constexpr int IAS = C::IAS, DIM = C::DIM;
+  constexpr int IAS = C::IAS;
   SplitStat st;
   const Geo &g = P.g;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < g.N) {
-    // the state of the combine, read back: U, eint, and in the last stage b_cc from the faces
+    // the state of the combine, read back: U and eint
     C2pState cs;
     int i, j, k;
     unflatten3(c, g.nx[0], g.nx[1], i, j, k);
@@ -1732,17 +1738,6 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_guessed(Pr
     cs.eint = P.eint[c];
     cs.ye = P.U[(long long)IAS * g.N + c] * cs.inv_rho;
     cs.inv_abar = P.U[(long long)(IAS + 1) * g.N + c] * cs.inv_rho;
-    if (P.last_stage) {
-      double b2 = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const double b = 0.5 * (P.bf[d][face_lin(g, d, i + (d == 0), j + (d == 1), k + (d == 2))] +
-                                P.bf[d][face_lin(g, d, i, j, k)]);
-        b2 = d == 0 ? b * b : b2 + b * b;
-        cs.vabs[d] = fabs(P.U[(long long)(1 + d) * g.N + c] * cs.inv_rho);
-      }
-      cs.ca2 = b2;
-    }
     st.gevals += 1;
     c2p_mhd_split_eos<C, true>(P, c, cs, P.mlp_out[c], st);
   }
