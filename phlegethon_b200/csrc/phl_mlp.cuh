@@ -395,10 +395,11 @@ inline void mlp_small_from_params(const float *p, MlpSmall &w) {
   w.b3 = p[MLP_OFF_B3];
 }
 
-// Persistent form of mlp_forward_cta for a block that runs the network on many tiles of 128
-// samples: the tensor-memory columns, the mbarrier and W2 in shared memory are set up once per
-// block (mlp_cta_setup) and released once (mlp_cta_teardown); each tile (mlp_forward_tile, all
-// 128 threads, uniform control flow) waits on the mbarrier phase of its parity.
+// mlp_forward_cta in three pieces, with the FP32 layers taken from an MlpSmall: the block sets up
+// its tensor-memory columns, mbarrier and W2 in shared memory once (mlp_cta_setup), runs tiles of
+// 128 samples (mlp_forward_tile: all 128 threads, uniform control flow; tile n of the block waits
+// on the mbarrier phase of parity n & 1) and releases the columns (mlp_cta_teardown).  The step's
+// guess kernel (k_mlp_guess) runs one tile per block.
 __device__ __forceinline__ void mlp_cta_setup(const __nv_bfloat16 *w2bf, MlpUmmaSmem &S) {
   const int tid = threadIdx.x;
   if ((tid >> 5) == 0) {
@@ -415,7 +416,7 @@ __device__ __forceinline__ void mlp_cta_setup(const __nv_bfloat16 *w2bf, MlpUmma
 
 // One tile: returns log10 T of this thread's sample.  ok (uniform over the block) says that the
 // tensor-core path is usable: a product that does not complete within the poll limit counts in
-// *stalled, gives no guess for its tile (*have = false) and turns ok off for the block's later
+// *stalled, gives no guess for its tile (have = false) and turns ok off for the block's later
 // tiles, whose samples then get no guess either.
 __device__ __forceinline__ float mlp_forward_tile(const MlpSmall &w, const float x[4], MlpUmmaSmem &S,
                                                   uint32_t parity, bool &ok, bool &have,

@@ -1,15 +1,23 @@
-// phl_split.cu -- FP32 split-precision form of the explicit FV step (hydro configurations).
+// phl_split.cu -- FP32 split-precision form of the explicit FV step (hydro and MHD
+// configurations).
 //
 // Storage per cell: conserved state U (FP64, carried across stages and steps), primitive
 // deviations W' = (rho - rho_eq, v, p - p_eq, scalars) and (gammae - gammae_eq, gammac) in FP32,
-// temperature and internal energy in FP64.  Reconstruction (LIM2ND), the Riemann solver and
-// the flux divergence run in FP32 on the well-balanced deviations: the pressure enters every
-// flux as a deviation, so pR - pL, p* - p_eq,face and the momentum flux after the WB fix
+// temperature and internal energy in FP64; MHD adds the face B (FP64), the scaled cell B and
+// cell EMFs (FP32).  Reconstruction (LIM2ND, PPH, LIM5TH), the Riemann solvers, face and corner
+// EMFs and the flux divergence run in FP32 on the well-balanced deviations: the pressure enters
+// every flux as a deviation, so pR - pL, p* - p_eq,face and the momentum flux after the WB fix
 // (source/source.F90:8953-8959) are formed without cancelling large numbers, and Mach 1e-3
-// perturbations keep their FP32 precision.  The RK combine, cons->prim, the Helmholtz Newton
-// inversion and the CFL maximum stay in FP64.  All FP32 quantities are in scaled units
-// (rho / rho_ref, p / p_ref, v / v_ref with v_ref^2 = p_ref / rho_ref, phi / v_ref^2), fixed per run,
-// so products of deviations never leave FP32 range whatever the problem's cgs magnitudes.
+// perturbations keep their FP32 precision.  The RK combine, the face-B update, cons->prim, the
+// Helmholtz Newton inversion and the CFL maximum stay in FP64.  All FP32 quantities are in scaled
+// units (rho / rho_ref, p / p_ref, v / v_ref with v_ref^2 = p_ref / rho_ref, phi / v_ref^2,
+// B / sqrt(p_ref)), fixed per run, so products of deviations never leave FP32 range whatever the
+// problem's cgs magnitudes.
+//
+// Hydro stage: one fused kernel (k_stage_split_tiled, TMA-staged planes; k_stage_split per
+// cell).  MHD stage: k_face_split_mhd_walk (PLM) or k_face_split_mhd (PPH, LIM5TH) per
+// direction, k_corner_split per axis, k_bface_split per direction, k_c2p_mhd_split; with the
+// learned temperature guess k_c2p_mhd_split_features, k_mlp_guess, k_c2p_mhd_split_guessed.
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <cstdlib>
