@@ -136,9 +136,10 @@ def test_bracket_guess_matches_oracle_bitwise(gpu_lib, oracle, table):
 def test_learned_guess_inside_the_split_mhd_step(gpu_lib, table):
     """eos_guess = PHL_GUESS_MLP: every cell's Newton starts from the trained network's guess,
     judged by at most 3 reference iterations with the warm start as the fallback.  The state
-    equals the warm-start run to the Newton tolerance, and most guesses are accepted (about 70%
-    in this moderately degenerate box, where the network's 0.2% error leaves the third Newton
-    step just above the tolerance for the rest)."""
+    equals the warm-start run to the Newton tolerance, and most guesses are accepted with a
+    network fitted over the whole EoS benchmark range (about 70% in this moderately degenerate
+    box, where the network's 0.2% error leaves the third Newton step just above the tolerance
+    for the rest; fitted over the run's own range, all of them: the next test)."""
     import ctypes as C
     from phlegethon_b200.abi import Simulation
     from util import field_errors
