@@ -475,6 +475,9 @@ def run_ours(args):
                 "config": {"workload": name + ("_no_fasteos" if args.no_fasteos else ""), "n": n, "cells": cells,
                            "eos_table": args.eos_table,
                            "form": head_form,
+                           # the headline Newton starts from the previous stage's temperature;
+                           # learned_guess_step times the network's judged guess on the same box
+                           "eos_guess": "warm",
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
                 "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
