@@ -84,6 +84,31 @@ def test_hydro_riemann_mirror_symmetry(oracle, riemann, flat):
         np.testing.assert_allclose(fm, sgn * f, rtol=1e-12, atol=1e-12)
 
 
+def test_lhllc_low_mach_dissipation_scales_with_phi(oracle):
+    """LHLLC on a symmetric converging flow (u* = 0): the normal momentum flux is the star
+    pressure p* = p + phi rho c v with phi = chi (2 - chi), chi = max(Mach_cutoff, min(1, M)) —
+    the pressure dissipation falls with the Mach number instead of staying rho c v as in HLLC
+    (source.F90:16012-16122)."""
+    import ctypes as C
+    cfg = Config(sdims=3, nx1=8, nx2=8, nx3=8, nas=0, riemann="lhllc", mach_cutoff=1e-4,
+                 bc=[["periodic", "periodic"]] * 3)
+    og = oracle.OracleGrid(HostGrid(cfg))
+    P = C.POINTER(C.c_double)
+    rho, p = 1.3, 0.7
+    c = math.sqrt(cfg.gamma_ad * p / rho)
+    for mach, chi in ((1e-6, 1e-4), (1e-3, 1e-3), (1e-2, 1e-2), (0.3, 0.3), (2.0, 1.0)):
+        v = mach * c
+        qL = np.array([rho, v, 0.0, 0.0, p])
+        qR = np.array([rho, -v, 0.0, 0.0, p])
+        f = np.zeros(5)
+        oracle.load().phlo_riemann_hydro(C.byref(og.g), qL.ctypes.data_as(P), qR.ctypes.data_as(P), None, None,
+                                         f.ctypes.data_as(P), 0)
+        assert abs(f[0]) < 1e-15 * rho * c
+        phi = chi * (2.0 - chi)
+        # p* - p is formed from p* (rounded at ~1e-16 p): allow that cancellation
+        assert abs((f[1] - p) - phi * rho * c * v) <= 1e-9 * phi * rho * c * v + 8 * np.finfo(float).eps * p
+
+
 @pytest.mark.parametrize("flat", [0, 1])
 @pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
 def test_mhd_riemann_mirror_symmetry(oracle, riemann, flat):
