@@ -109,6 +109,32 @@ def test_lhllc_low_mach_dissipation_scales_with_phi(oracle):
         assert abs((f[1] - p) - phi * rho * c * v) <= 1e-9 * phi * rho * c * v + 8 * np.finfo(float).eps * p
 
 
+@pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
+def test_lhlld_low_mach_dissipation_scales_with_phi(oracle, riemann):
+    """HLLD / LHLLD on a symmetric converging flow without B (u* = 0): the normal momentum flux
+    is the star total pressure p + phi rho (c + 2v) v, with phi = 1 for HLLD and, for LHLLD,
+    phi = chi (2 - chi) below a fast Mach number of 0.6 and 1 above it
+    (source.F90:14364-14384, 14497-14498)."""
+    import ctypes as C
+    cfg = Config(sdims=3, nx1=8, nx2=8, nx3=8, mhd=True, riemann=riemann, mach_cutoff=1e-4,
+                 bc=[["periodic", "periodic"]] * 3)
+    og = oracle.OracleGrid(HostGrid(cfg))
+    P = C.POINTER(C.c_double)
+    rho, p = 1.3, 0.7
+    c = math.sqrt(cfg.gamma_ad * p / rho)
+    for mach in (1e-3, 1e-2, 0.3, 0.8):
+        v = mach * c
+        qL, qR = np.array([rho, v, 0.0, 0.0, p]), np.array([rho, -v, 0.0, 0.0, p])
+        bL, bR = np.zeros(3), np.zeros(3)
+        f, fb = np.zeros(5), np.zeros(3)
+        oracle.load().phlo_riemann_mhd(C.byref(og.g), qL.ctypes.data_as(P), qR.ctypes.data_as(P),
+                                       bL.ctypes.data_as(P), bR.ctypes.data_as(P), None, None,
+                                       f.ctypes.data_as(P), fb.ctypes.data_as(P), 0)
+        phi = mach * (2.0 - mach) if riemann == "lhlld" and mach < 0.6 else 1.0
+        d = rho * (c + 2.0 * v) * v
+        assert abs((f[1] - p) - phi * d) <= 1e-9 * phi * d + 8 * np.finfo(float).eps * p
+
+
 @pytest.mark.parametrize("flat", [0, 1])
 @pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
 def test_mhd_riemann_mirror_symmetry(oracle, riemann, flat):
