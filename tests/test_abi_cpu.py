@@ -79,3 +79,18 @@ def test_bench_algorithmic_bytes():
     assert bench.step_bytes_per_cell(cfgm.replace(precision="fp32_split")) == 2072
     name, launches = bench.stage_kernels(cfgm.replace(precision="fp32_split"), "fp32_split")
     assert "k_face_split_mhd" in name and launches == 3 * (3 + 3 + 3 + 1) + 2
+
+
+def test_python_binding_matches_header_arity(lib_path):
+    """Every entry point bound in phlegethon_b200.abi takes as many arguments as its prototype
+    in include/phl_gpu.h declares (a drifted binding would pass garbage across the ABI)."""
+    from phlegethon_b200 import abi
+    lib = abi.load_library(lib_path)
+    src = open(os.path.join(ROOT, "include", "phl_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    protos = dict(re.findall(r"\b(phl_\w+)\s*\(([^()]*)\)\s*;", src, flags=re.S))
+    assert set(abi.EXPORTS) <= set(protos)
+    for name in abi.EXPORTS:
+        params = protos[name].strip()
+        n = 0 if params in ("", "void") else len(params.split(","))
+        assert len(getattr(lib, name).argtypes) == n, name
