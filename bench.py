@@ -454,7 +454,7 @@ def run_ours(args):
     tpc = TRAFFIC_PER_CELL.get((name, head_form))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": tpc * cells if tpc else None,
-            "traffic_source": ("ncu DRAM bytes at 128^3 (profiles/), scaled by cells; per stage" if name == "stratified_mhd"
+            "traffic_source": ("ncu DRAM bytes of one stage at 128^3, scaled by cells" if name == "stratified_mhd"
                                else "ncu DRAM bytes of one launch at 128^3, scaled by cells") if tpc else None,
             "kernel": kname, "peak_kind": peak_kind,
             "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}

@@ -8,7 +8,7 @@
  * plus the step-0 thermodynamics loop of time_loop (source/source.F90:6271-6383) and the table
  * reader load_helm_table (source/source.F90:23077-23156).  This header exports those entry points
  * with plain pointers and sizes so the Fortran driver can bind them with ISO_C_BINDING
- * (`bind(C)` interfaces in INTEGRATION.md).  Host arrays use the reference's own layout
+ * (`bind(C)` interfaces).  Host arrays use the reference's own layout
  * (column-major, variable index fastest, ghost cells included, bounds of
  * initialize_simulation, source/source.F90:1219-1714); the library transposes them into its
  * device layout.
@@ -63,13 +63,17 @@ extern "C" {
 #define PHL_FP64 0        /* FP64 throughout, bit-compatible with the reference order */
 #define PHL_FP32_SPLIT 1  /* FP32 reconstruction/Riemann/EMF on WB deviations, FP64 state + EoS */
 
-/* initial temperature guess for the (rho, e) -> T Newton inversion */
+/* reconstruction (phl_config.reconstruction) */
 #define PHL_REC_LIM2ND 0  /* LIM2ND_REC: van Leer PLM (source.F90:8141-8181) */
 #define PHL_REC_PPH 1     /* PPH_REC: third order, scalars limited (source.F90:8183-8259) */
 #define PHL_REC_LIM5TH 2  /* LIM5TH_REC: limited fifth order (source.F90:8261-8323) */
+
+/* initial temperature guess for the (rho, e) -> T Newton inversion */
 #define PHL_GUESS_WARM 0  /* previous-stage temperature, as the reference (source.F90:13649) */
 #define PHL_GUESS_MLP 1   /* learned 4-64-64-1 guess, judged by <=3 Newton steps, else the
                                      warm guess (hydro step) or the bracket guess (EoS batch) */
+#define PHL_GUESS_BRACKET 2 /* EoS batch only: cold guess from the table nodes bracketing e(rho, T)
+                               at fixed rho*Ye (monotone search in T); T_inout is not read */
 
 typedef struct phl_config {
   int abi_version;                 /* must be PHL_ABI_VERSION */
@@ -192,14 +196,17 @@ int phl_eos_invert_batch(phl_ctx *ctx, long long n, const double *rho, const dou
                          double *cs, int *iters, int guess);
 /* Same as phl_eos_invert_batch, but allocates no device memory: the device copies of the
  * inputs and outputs live in one fixed array compiled into the library.  No counterpart in the
- * reference.  For callers that must not allocate GPU memory during the call: a driver whose
- * device memory is already claimed by its own pool allocator, or code that runs while a CUDA
- * stream capture is open (cudaMalloc is not allowed there and would break the capture).
- * At most PHL_NOALLOC_MAX_SAMPLES samples per call; larger n returns PHL_E_TOO_LARGE.
- * The first call on each device looks up the array's device address: make that first call
- * before any stream capture.  The array is shared by every call and every context on a device
- * (it stays allocated until the process exits), so calls that overlap on the GPU race; issue
- * them one after another.  Host pointers; copies in and out are included. */
+ * reference.  For callers that cannot call cudaMalloc during a run: a Fortran or C driver that
+ * hands all free device memory to its own pool allocator at start-up (a cudaMalloc would then
+ * fail), or one whose time loop must not allocate because cudaMalloc/cudaFree can synchronise
+ * the whole device and stall the step pipeline.
+ * At most PHL_NOALLOC_MAX_SAMPLES samples per call; larger n returns PHL_E_TOO_LARGE and does
+ * nothing.  The first call on each device looks up the array's device address (a one-time,
+ * thread-safe set-up): make that first call before any stream capture.  The array is shared by
+ * every call and every context on a device and stays allocated until the process exits; it
+ * keeps the last call's contents, and calls that overlap on the GPU race, so issue them one
+ * after another.  Host pointers; copies in and out are included, and the call returns after
+ * its results have reached the host. */
 #define PHL_NOALLOC_MAX_SAMPLES 65536
 int phl_eos_invert_batch_noalloc(phl_ctx *ctx, long long n, const double *rho, const double *e,
                                  const double *abar, const double *zbar, double *T_inout, double *p,

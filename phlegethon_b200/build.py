@@ -53,15 +53,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(BUILDDIR, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    objs, procs = [], []
+    # the units are independent: compile them concurrently
     for src, extra in UNITS:
         obj = os.path.join(BUILDDIR, src.replace(".cu", ".o"))
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-rdc=false",
                "-Xptxas", "-warn-spills", *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        procs.append((src, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
     tmp = LIB + ".tmp"
     subprocess.run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

@@ -408,6 +408,18 @@ __device__ __forceinline__ void store_face_emf(const Prm &P, int d, long long fi
   P.sgnf[d][fidx] = sgn;
 }
 
+// Every kernel below is a template that two translation units instantiate (the FP64 unit,
+// compiled without FMA contraction, and the FP32 split unit, compiled with contraction and
+// approximate division).  The host stub of a template kernel is a weak symbol: if both units
+// instantiated the same kernel under the same name, the linker would keep one stub for two
+// device images and the image that runs would depend on module load order.  Each unit therefore
+// defines PHL_KERNEL_UNIT to its own name before including this header, which puts its
+// instantiations into a namespace of its own (inline, so the code below names them as phl::).
+#ifndef PHL_KERNEL_UNIT
+#error "define PHL_KERNEL_UNIT (the including translation unit's kernel namespace) before including phl_kernels.cuh"
+#endif
+inline namespace PHL_KERNEL_UNIT {
+
 // --------------------------------------------------------------------- shock detector
 // USE_SHOCK_FLATTENING (source.F90:8073-8136).  is_flattened is kept for cells -1..n of every
 // dimension (the cells whose edges the faces read), the detector's marks for cells -2..n+1.
@@ -914,4 +926,5 @@ __global__ void __launch_bounds__(128) k_init_thermo(Prm P) {
   P.temp[c] = T;
 }
 
+}  // inline namespace PHL_KERNEL_UNIT
 }  // namespace phl

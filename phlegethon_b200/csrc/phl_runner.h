@@ -11,10 +11,12 @@ struct Runner {
   virtual ~Runner() {}
   // one RK stage (all kernels of the stage)
   virtual void stage(const Prm &P, cudaStream_t s) = 0;
-  // standalone CFL maximum over the FP64 primitive state
-  virtual void dt(const Prm &P, cudaStream_t s) = 0;
-  // step-0 thermodynamics
-  virtual void init_thermo(const Prm &P, cudaStream_t s) = 0;
+  // FP64 runners (phl_runtime.cu) only: the standalone CFL maximum over the FP64 primitive
+  // state and the step-0 thermodynamics.  A split-precision context runs these two through the
+  // FP64 runner of its option set, so each of these kernels is compiled once, with the FP64
+  // unit's reference rounding.
+  virtual void dt(const Prm &, cudaStream_t) {}
+  virtual void init_thermo(const Prm &, cudaStream_t) {}
   // split path only: FP64 primitives -> (U, FP32 deviations) and back
   virtual void split_from_prim(const Prm &, cudaStream_t) {}
   virtual void split_to_prim(const Prm &, cudaStream_t) {}

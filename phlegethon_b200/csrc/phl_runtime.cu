@@ -10,10 +10,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/phl_gpu.h"
+// kernel namespace of this unit (FP64, no FMA contraction); see phl_kernels.cuh
+#define PHL_KERNEL_UNIT fp64_unit
 #include "phl_kernels.cuh"
 #include "phl_runner.h"
 #include "phl_eos_batch.cuh"
@@ -186,6 +189,10 @@ struct phl_ctx {
   phl_config cfg;
   Geo geo;
   std::unique_ptr<Runner> runner;
+  // FP64 runner of the same option set: dt and step-0 thermodynamics in both precision forms
+  // (the split runner's own when that is the form; a second instance otherwise)
+  std::unique_ptr<Runner> fp64_runner;
+  Runner *thermo() { return fp64_runner ? fp64_runner.get() : runner.get(); }
   cudaStream_t stream = nullptr;
   int dim = 2, nv = 0;
   long long N = 0;
@@ -498,12 +505,14 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
   if (!(wb == etot && etot == grav)) return PHL_E_UNSUPPORTED;
   c->split = cfg->precision == PHL_FP32_SPLIT;
   const bool fast = cfg->flags & PHL_FASTEOS;
-  if (c->split)
-    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction,
-                                      (cfg->flags & PHL_SHOCK_FLATTENING) != 0));
-  else
-    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction,
-                                (cfg->flags & PHL_SHOCK_FLATTENING) != 0));
+  const bool sf = (cfg->flags & PHL_SHOCK_FLATTENING) != 0;
+  if (c->split) {
+    c->runner.reset(make_split_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction, sf));
+    c->fp64_runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction, sf));
+    if (!c->fp64_runner) return PHL_E_UNSUPPORTED;
+  } else {
+    c->runner.reset(make_runner(cfg->sdims, cfg->nvars, mhd, helm, wb, cfg->riemann, fast, cfg->reconstruction, sf));
+  }
   if (!c->runner) return PHL_E_UNSUPPORTED;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   Geo &g = c->geo;
@@ -881,7 +890,7 @@ int phl_init_thermo(phl_ctx *ctx) {
   // write gammaf into the current buffer: gout must alias gin here
   P.Win = ctx->W[ctx->cur];
   P.gout = ctx->gam[ctx->cur];
-  ctx->runner->init_thermo(P, ctx->stream);
+  ctx->thermo()->init_thermo(P, ctx->stream);
   CK(cudaGetLastError());
   if (ctx->split) {
     ctx->split_from_prim();
@@ -899,7 +908,7 @@ int phl_compute_hyperbolic_dt(phl_ctx *ctx, double *dt, double *smax) {
   Prm P = ctx->prm(0);
   P.Win = ctx->W[ctx->cur];
   CK(cudaMemsetAsync(ctx->smax_bits, 0, sizeof(unsigned long long), ctx->stream));
-  ctx->runner->dt(P, ctx->stream);
+  ctx->thermo()->dt(P, ctx->stream);
   k_finish_dt<<<1, 1, 0, ctx->stream>>>(ctx->scal, ctx->smax_bits, ctx->cfg.cfl);
   CK(cudaGetLastError());
   double sc[3];
@@ -1105,9 +1114,13 @@ int noalloc_symbol(void **dst, const void *symbol, const char *name) {
   return PHL_E_CUDA;
 }
 
-// once per device, with that device current
+std::mutex g_noalloc_mutex;
+
+// once per device, with that device current; the mutex makes the first calls of several host
+// threads on one device look the addresses up once
 int noalloc_setup(int device, double **buf, int **ibuf, unsigned long long **queue) {
   if (device < 0 || device >= NOALLOC_MAX_DEVICES) return PHL_E_INVALID;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_dev[device]) {
     void *p = nullptr, *q = nullptr, *r = nullptr;
     int rc;

@@ -26,6 +26,8 @@
 #include "phl_eos_fast.cuh"
 #include "phl_mlp.cuh"
 #include "phl_umma.cuh"
+// kernel namespace of this unit (FP32 flux arithmetic with contraction); see phl_kernels.cuh
+#define PHL_KERNEL_UNIT split_unit
 #include "phl_runner.h"
 
 namespace phl {
@@ -2017,10 +2019,6 @@ struct SplitRunnerT : Runner {
       }
     }
     k_stage_split<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P);
-  }
-  void dt(const Prm &P, cudaStream_t s) override { k_dt<C><<<nblk(P.g.N, 256), 256, 0, s>>>(P); }
-  void init_thermo(const Prm &P, cudaStream_t s) override {
-    k_init_thermo<C><<<nblk(P.g.N, 128), 128, 0, s>>>(P);
   }
   void split_from_prim(const Prm &P, cudaStream_t s) override {
     k_split_from_prim<C><<<nblk(P.g.N, 256), 256, 0, s>>>(P);

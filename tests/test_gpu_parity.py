@@ -280,3 +280,22 @@ def test_constant_acceleration_parity(gpu_lib, oracle, table, maker):
     hg, ho, st = run_pair(cfg, h, 4, table=table if cfg.helmholtz else None, oracle=oracle)
     assert max_abs_diff(hg, ho) == 0.0
     assert st["nonfinite"] == 0
+
+
+def test_fp64_unchanged_after_split_contexts(gpu_lib, oracle, table):
+    """Regression for a build defect: the FP64 and split units once instantiated the same
+    dt / step-0 thermodynamics kernels under one weak host symbol, so after split contexts had
+    run, an FP64 context could launch the split unit's FMA-contracted copy.  Run split contexts
+    of the same option sets first, in this process, then require the FP64 boxes bit for bit."""
+    from phlegethon_b200.abi import Simulation
+    for mhd in (False, True):
+        cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd)
+        with Simulation(cfg.replace(precision="fp32_split"), table) as sim:
+            sim.upload(h.copy())
+            sim.init_thermo()
+            sim.compute_hyperbolic_dt()
+            sim.time_loop(2)
+    for mhd in (False, True):
+        cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd)
+        hg, ho, _ = run_pair(cfg, h, 3, table=table, oracle=oracle)
+        assert max_abs_diff(hg, ho) == 0.0, field_errors(hg, ho)
