@@ -30,7 +30,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "zone-updates/s on 1 B200: FP32+learned-EoS vs FP64 plain vs CPU, at stated L1 err"
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line is the only stdout output)."""
+    print("[bench %7.1fs] %s" % (time.perf_counter() - _T0, msg), file=sys.stderr, flush=True)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+MLP_NPARAMS = 4 * 64 + 64 + 64 * 64 + 64 + 64 + 1  # PHL_MLP_NPARAMS
 
 
 def load_peaks():
@@ -94,8 +101,29 @@ TRAFFIC_PER_CELL = {("stratified", "fp32_split"): 499.604224e6 / 2097152,
                                                        + 755.5e6) / 2097152}
 
 
+# Algorithmic HBM bytes per zone-update of the workloads (minimum traffic of one step of a fused
+# stage: every field the step needs read once and every field it produces written once, per
+# stage; no intermediate such as face fluxes or EMFs counted).  FP64 plain / FP32 split:
+#   2D hot bubble, ideal gas, nv = 4                          448 B  (FP64)
+#   2D Orszag-Tang, nv = 4 + 2 face-B components               576 B  (FP64)
+#   3D Helmholtz box, nv = 7 + T + (gamma_e, gamma_c)          928 B / 712 B
+#   3D Helmholtz MHD box, adds 3 face-B (r+w) and B^n reads   1120 B / 904 B
+# The split form stores W' and the gammas in FP32; U, U0, T and the face B stay FP64.
+ALGORITHMIC_BYTES = {("hot_bubble", "fp64"): 448, ("orszag_tang", "fp64"): 576,
+                     ("stratified", "fp64"): 928, ("stratified", "fp32_split"): 712,
+                     ("stratified_mhd", "fp64"): 1120, ("stratified_mhd", "fp32_split"): 904}
+
+
+def algorithmic_bytes_per_cell(name, form):
+    """Roofline numerator: algorithmic HBM bytes per zone-update (ALGORITHMIC_BYTES)."""
+    return ALGORITHMIC_BYTES[(name, form)]
+
+
 def step_bytes_per_cell(cfg):
-    """Algorithmic HBM bytes per zone-update of the fused stage kernel (minimum traffic).
+    """Traffic model of the implementation: HBM bytes per zone-update with every intermediate
+    the kernels materialise (FP32 face fluxes, face EMFs, CT signs, corner EMFs) counted.  Kept
+    beside the algorithmic bytes as `roofline.traffic_model`; the excess over the algorithmic
+    figure is the traffic a fused stage would not need.
 
     Stage 1 reads W (nv) and eint and writes U0, U, W; middle stages read W, U0, U and write U,
     W; the last stage reads W, U0, U and writes W and eint.  Helmholtz adds temp (read+write per
@@ -261,22 +289,28 @@ def pinned_like(a):
     return t, v
 
 
-def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind, want_e2e, learned=False):
+def measure_form(args, name, cfg, h, table, form, local, dist, want_e2e, guess="warm", mlp_params=None,
+                 kernel_timing=True):
     """Time one arithmetic form on the workload; returns timings and the final host state.
-    learned: the split form with the learned temperature guess in the step's Newton (the
-    network is trained on the device first, untimed)."""
+    guess: the temperature guess of the step's Newton -- "warm" (previous stage), "mlp_rescue"
+    (warm, and the learned guess where the warm start is poor) or "mlp" (learned guess for every
+    cell).  A learned guess needs the network: trained on the device first (untimed) unless
+    mlp_params (a previous run's parameters) is given."""
     import ctypes as C
 
     import torch
     from phlegethon_b200 import abi
     from phlegethon_b200.grid import HostGrid, helm_state_range
 
-    c = cfg.replace(precision=form, device=local, eos_guess="mlp" if learned else cfg.eos_guess)
+    c = cfg.replace(precision=form, device=local, eos_guess=guess)
+    log("measure %s %s (%d cells)" % (form, guess, cfg.n_cells))
     sim = abi.Simulation(c, table)
     train = None
     sim.upload(h)
     sim.init_thermo()
-    if learned:
+    if guess != "warm" and mlp_params is not None:
+        assert sim.lib.phl_mlp_set_params(sim.ctx, mlp_params.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    elif guess != "warm":
         # the network is fitted over the states of the run: log10 rho and log10 T of the initial
         # state widened by 0.1 dex, its Abar and Zbar
         h0 = h.copy()
@@ -290,6 +324,8 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
             raise RuntimeError("phl_mlp_train failed: %d" % rc)
         train = {"samples": 1 << 22, "epochs": args.train_epochs, "seconds": time.perf_counter() - t0,
                  "loss": loss.value, "range_lo": lo, "range_hi": hi}
+        mlp_params = np.zeros(MLP_NPARAMS, dtype=np.float32)
+        assert sim.lib.phl_mlp_get_params(sim.ctx, mlp_params.ctypes.data_as(C.POINTER(C.c_float))) == 0
     sim.compute_hyperbolic_dt()
     stream = torch.cuda.ExternalStream(sim.stream(), device=torch.device("cuda", local))
     sim.time_loop(args.warmup)
@@ -310,8 +346,9 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
     status = sim.status()
     out = h.copy()
     sim.download(out)
-    res = {"form": form, "ms": ms, "done": done, "clocks": clocks, "status": status, "state": out, "train": train}
-    if learned:
+    res = {"form": form, "guess": guess, "ms": ms, "done": done, "clocks": clocks, "status": status, "state": out,
+           "train": train, "mlp_params": mlp_params}
+    if not kernel_timing:
         sim.close()
         return res
 
@@ -355,43 +392,172 @@ def measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
         dyn.eq_prim_x = [None] * 3
         dyn.eq_gammae_x = [None] * 3
         sim.download(dyn)
-        e2e_steps = max(1, min(args.steps, 5))
+        e2e_steps = max(1, min(args.steps, 10))
+        # bytes per step: each call uploads the whole host arrays (ghost layers included) and
+        # downloads their interiors
         h2d = sum(a.nbytes for a in [dyn.prim, dyn.temp, dyn.eint, dyn.gammaf, dyn.b_cc] + bx if a is not None)
+        cells = cfg.n_cells
+        d2h = 8 * sum(x for x in [cfg.nvars * cells, cells, cells,
+                                  2 * cells if (cfg.helmholtz and cfg.fasteos) else 0,
+                                  cfg.sdims * cells if cfg.mhd else 0] if x)
+        if cfg.mhd:
+            n3 = [cfg.nx1, cfg.nx2, cfg.nx3]
+            for d in range(cfg.sdims):
+                d2h += 8 * int(np.prod([n3[a] + (a == d) for a in range(3)]))
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         x0 = torch.cuda.Event(enable_timing=True)
         x1 = torch.cuda.Event(enable_timing=True)
         x0.record(stream)
+        # the public host-state call: upload, one step, download, queued per step; a step's
+        # uploads wait for the previous step's downloads of the same host planes
         for _ in range(e2e_steps):
-            sim.upload(dyn)
-            sim.time_loop(1)
-            sim.download(dyn)
+            sim.time_loop_host_async(dyn, 1)
+        sim.wait_host()
         x1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(x0.elapsed_time(x1), dist)
         res["e2e_ms_per_step"] = e2e_ms / e2e_steps
         res["h2d"] = int(h2d)
+        res["d2h"] = int(d2h)
     sim.close()
     return res
 
 
-def long_run_errors(cfg, h, table, form, steps, local):
-    """Per-field relative L1 of `form` against the FP64 form after `steps` steps from h."""
+def long_run_errors(cfg, h, table, form, steps, local, guess="warm", mlp_params=None):
+    """Per-field relative L1 of `form` (with its EoS guess) against the FP64 form after `steps`
+    steps from h."""
+    import ctypes as C
+
     from phlegethon_b200 import abi
     from util import field_errors
     out = {}
-    for f in (form, "fp64"):
+    log("long run: %d steps of %s and fp64" % (steps, form))
+    for f, gs in ((form, guess), ("fp64", "warm")):
         hh = h.copy()
-        with abi.Simulation(cfg.replace(precision=f, device=local), table) as sim:
+        with abi.Simulation(cfg.replace(precision=f, device=local, eos_guess=gs), table) as sim:
             sim.upload(hh)
             sim.init_thermo()
+            if gs != "warm":
+                assert sim.lib.phl_mlp_set_params(sim.ctx, mlp_params.ctypes.data_as(C.POINTER(C.c_float))) == 0
             sim.compute_hyperbolic_dt()
             done, _ = sim.time_loop(steps)
             assert done == steps
             sim.download(hh)
         out[f] = hh
     return field_errors(out[form], out["fp64"])
+
+
+def run_case(cfg, h, table, local, nsteps, tmax=float("inf"), warmup=3, guess="warm", mlp_params=None):
+    """Advance h by `nsteps` steps (or until tmax) on a fresh context, timed on the device after
+    `warmup` untimed steps from the same start (the state is re-uploaded and the clock reset, so
+    the graphs are captured before the timed region).  Returns (ms, steps, time, final state,
+    status)."""
+    import ctypes as C
+
+    import torch
+    from phlegethon_b200 import abi
+    c = cfg.replace(device=local, eos_guess=guess)
+    log("case %dx%dx%d %s %s" % (cfg.nx1, cfg.nx2, cfg.nx3, cfg.precision, guess))
+    sim = abi.Simulation(c, table if cfg.helmholtz else None)
+    sim.upload(h)
+    sim.init_thermo()
+    if guess != "warm":
+        assert sim.lib.phl_mlp_set_params(sim.ctx, mlp_params.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    dt0, smax0 = sim.compute_hyperbolic_dt()
+    start = h.dynamic_copy()
+    sim.download(start)
+    sim.time_loop(warmup, tmax)
+    sim.upload(start)
+    sim.set_time(0.0, dt0, smax0)
+    sim.reset_status()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=torch.device("cuda", local))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    if tmax == float("inf"):
+        done, t = sim.time_loop(nsteps, tmax)
+    else:
+        # to a final time: batches of steps until the device stops at tmax (the host learns the
+        # time once per batch)
+        done, t = 0, 0.0
+        while done < nsteps and t < tmax:
+            d, t = sim.time_loop(min(256, nsteps - done), tmax)
+            done += d
+            if d == 0:
+                break
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out = h.copy()
+    sim.download(out)
+    st = sim.status()
+    sim.close()
+    return e0.elapsed_time(e1), done, t, out, st
+
+
+def run_suite(args, local, mlp_params):
+    """The other workloads, each at its stated size: zone-updates/s of the FP64 and split forms,
+    the split form's per-field L1 against FP64, div B where there is a magnetic field, and a
+    bounded CPU oracle sample (same zone-update metric)."""
+    from util import div_b_max, field_errors
+    suite = {}
+
+    def rate(cfg, ms, done):
+        return done * cfg.n_cells / (ms * 1e-3)
+
+    # north_star config 1: 2D hot bubble 256^2, 100 steps
+    cfg, h, _ = build_problem("hot_bubble", 256)
+    r = {}
+    for form in ("fp64", "fp32_split"):
+        ms, done, t, out, st = run_case(cfg.replace(precision=form), h, None, local, 100)
+        r[form] = (ms, done, out)
+    cpu = cpu_rate("hot_bubble", 5) if not args.no_cpu else None
+    suite["hot_bubble_256"] = {
+        "steps": r["fp64"][1], "fp64": {"value": rate(cfg, r["fp64"][0], r["fp64"][1]),
+                                        "ms_per_step": r["fp64"][0] / r["fp64"][1]},
+        "fp32_split": {"value": rate(cfg, r["fp32_split"][0], r["fp32_split"][1]),
+                       "ms_per_step": r["fp32_split"][0] / r["fp32_split"][1],
+                       "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
+        "cpu_oracle": {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]} if cpu else None}
+    # config 2: Orszag-Tang 1024^2 (HLLD, CT) to t = 0.5
+    cfg, h, _ = build_problem("orszag_tang", 1024)
+    r = {}
+    for form in ("fp64", "fp32_split"):
+        ms, done, t, out, st = run_case(cfg.replace(precision=form), h, None, local, 1 << 20, tmax=0.5)
+        r[form] = (ms, done, out, t)
+    cpu = cpu_rate("orszag_tang", 2) if not args.no_cpu else None
+    suite["orszag_tang_1024"] = {
+        "t_end": r["fp64"][3], "steps": r["fp64"][1],
+        "fp64": {"value": rate(cfg, r["fp64"][0], r["fp64"][1]), "ms_per_step": r["fp64"][0] / r["fp64"][1],
+                 "div_b_max": div_b_max(r["fp64"][2])},
+        "fp32_split": {"value": rate(cfg, r["fp32_split"][0], r["fp32_split"][1]), "steps": r["fp32_split"][1],
+                       "ms_per_step": r["fp32_split"][0] / r["fp32_split"][1],
+                       "div_b_max": div_b_max(r["fp32_split"][2]),
+                       "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
+        "cpu_oracle": {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]} if cpu else None}
+    # config 4: EoS inversion batch of 2^24 samples, learned vs bracket guess
+    ea = argparse.Namespace(**vars(args))
+    ea.n, ea.steps, ea.warmup = 0, 5, 3
+    el = eos_line(ea, with_cpu=False)
+    suite["eos_batch_2^24"] = {k: el[k] for k in ("value", "unit", "ms_per_step", "bracket", "mlp", "agreement", "e2e")}
+    # config 5: magnetised box 384^3, the headline form and FP64, a few steps each
+    cfg, h, table = build_problem("stratified_mhd", 384, eos_table=args.eos_table)
+    r = {}
+    for form, guess in (("fp32_split", "mlp_rescue" if mlp_params is not None else "warm"), ("fp64", "warm")):
+        ms, done, t, out, st = run_case(cfg.replace(precision=form), h, table, local, 5, guess=guess,
+                                        mlp_params=mlp_params)
+        r[form] = (ms, done, out, st)
+    suite["stratified_mhd_384"] = {
+        "steps": r["fp32_split"][1],
+        "fp32_split": {"value": rate(cfg, r["fp32_split"][0], r["fp32_split"][1]),
+                       "ms_per_step": r["fp32_split"][0] / r["fp32_split"][1],
+                       "eos_guess": "mlp_rescue" if mlp_params is not None else "warm",
+                       "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
+        "fp64": {"value": rate(cfg, r["fp64"][0], r["fp64"][1]), "ms_per_step": r["fp64"][0] / r["fp64"][1]},
+        "div_b_max_split": div_b_max(r["fp32_split"][2])}
+    return suite
 
 
 def run_ours(args):
@@ -411,34 +577,53 @@ def run_ours(args):
 
     name = args.config
     n = args.n or default_size(name)
+    log("building %s at %d" % (name, n))
     cfg, h, table = build_problem(name, n, fasteos=not args.no_fasteos, eos_table=args.eos_table)
+    log("built")
     peaks, peak_kind = load_peaks()
     cells = cfg.n_cells
     head_form = args.form
-    forms = [head_form] + [f for f in ("fp64",) if f != head_form]
-    results = {}
-    for form in forms:
-        results[form] = measure_form(args, name, cfg, h, table, form, local, dist, peaks, peak_kind,
-                                     want_e2e=(form == head_form))
-    head = results[head_form]
-    learned_step = None
-    if head_form == "fp32_split" and name == "stratified_mhd" and not args.no_learned:
-        # the same split form with the learned temperature guess in the step (metric's
-        # "FP32+learned-EoS"), timed the same way; the warm-start form stays the headline
-        lr = measure_form(args, name, cfg, h, table, head_form, local, dist, peaks, peak_kind, want_e2e=False,
-                          learned=True)
-        from util import field_errors
-        st = lr["status"]
-        learned_step = {"value": aggregate_rate(world, lr["done"], cells, lr["ms"]),
-                        "ms_per_step": lr["ms"] / max(lr["done"], 1),
-                        "newton_iters_per_call": st["newton_iterations"] / max(st["newton_calls"], 1),
-                        "warm_newton_iters_per_call": head["status"]["newton_iterations"]
-                        / max(head["status"]["newton_calls"], 1),
-                        "accepted": st["mlp_accepted"] / max(st["newton_calls"], 1),
-                        "l1_vs_warm": field_errors(lr["state"], head["state"]), "train": lr["train"]}
+    # the metric's form: FP32 split fluxes with the learned EoS guess in the step (the warm start,
+    # and the network's judged guess for every cell whose warm start is poor); the learned guess
+    # in the step is built for the Helmholtz MHD box
+    learned_ok = head_form == "fp32_split" and name == "stratified_mhd" and not args.no_learned
+    head_guess = "mlp_rescue" if learned_ok else "warm"
+    from util import field_errors
+    head = measure_form(args, name, cfg, h, table, head_form, local, dist, want_e2e=True, guess=head_guess)
+    results = {head_form: head}
+    if head_form != "fp64":
+        results["fp64"] = measure_form(args, name, cfg, h, table, "fp64", local, dist, want_e2e=False)
+    side = {}
+    if learned_ok:
+        def summary(r, ref):
+            st = r["status"]
+            return {"value": aggregate_rate(world, r["done"], cells, r["ms"]),
+                    "ms_per_step": r["ms"] / max(r["done"], 1),
+                    "newton_iters_per_call": st["newton_iterations"] / max(st["newton_calls"], 1),
+                    "learned_guesses": st["mlp_accepted"] + st["mlp_rejected"],
+                    "learned_accepted": st["mlp_accepted"],
+                    "l1_vs_headline": field_errors(r["state"], ref["state"])}
+        # the same split form with the reference's warm start alone, and with the learned guess
+        # for every cell, timed the same way (network parameters shared with the headline run)
+        for key, guess in (("warm_guess_step", "warm"), ("learned_every_cell_step", "mlp")):
+            r = measure_form(args, name, cfg, h, table, head_form, local, dist, want_e2e=False, guess=guess,
+                             mlp_params=head["mlp_params"], kernel_timing=False)
+            side[key] = summary(r, head)
+    hst = head["status"]
+    learned_info = None
+    if learned_ok:
+        learned_info = {"mode": "mlp_rescue: warm start; cells whose first warm Newton correction exceeds 2% "
+                                "of T take the network's judged guess",
+                        "learned_guesses": hst["mlp_accepted"] + hst["mlp_rejected"],
+                        "learned_accepted": hst["mlp_accepted"],
+                        "newton_iters_per_call": hst["newton_iterations"] / max(hst["newton_calls"], 1),
+                        "train": head["train"]}
     l1_long = None
-    if args.l1_steps and head_form != "fp64":
-        l1_long = {"steps": args.l1_steps, "errors": long_run_errors(cfg, h, table, head_form, args.l1_steps, local)}
+    l1_steps = args.l1_steps if args.l1_steps >= 0 else (1000 if cfg.helmholtz else 0)
+    if l1_steps and head_form != "fp64":
+        l1_long = {"steps": l1_steps, "form": head_form, "eos_guess": head_guess,
+                   "errors": long_run_errors(cfg, h, table, head_form, l1_steps, local, guess=head_guess,
+                                             mlp_params=head["mlp_params"])}
     value = aggregate_rate(world, head["done"], cells, head["ms"])
     fp64 = results["fp64"]
     fp64_value = aggregate_rate(world, fp64["done"], cells, fp64["ms"])
@@ -447,7 +632,10 @@ def run_ours(args):
         from util import field_errors
         errors = field_errors(head["state"], fp64["state"])
 
-    bytes_per_cell = step_bytes_per_cell(cfg.replace(precision=head_form))
+    # roofline of one RK stage (all kernels of the stage, CUDA events on the library's stream):
+    # algorithmic bytes of a stage = the per-zone-update figure / stages x cells
+    bytes_per_cell = algorithmic_bytes_per_cell(name, head_form)
+    model_bytes = step_bytes_per_cell(cfg.replace(precision=head_form))
     launch_ms = head["launch_ms"]
     achieved = bytes_per_cell * cells / cfg.rk_stages / (launch_ms * 1e-3) / 1e9
     kname, launches_per_step = stage_kernels(cfg, head_form)
@@ -457,11 +645,17 @@ def run_ours(args):
             "traffic_source": ("ncu DRAM bytes of one stage at 128^3, scaled by cells" if name == "stratified_mhd"
                                else "ncu DRAM bytes of one launch at 128^3, scaled by cells") if tpc else None,
             "kernel": kname, "peak_kind": peak_kind,
-            "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell}
+            "launch_ms": launch_ms, "bytes_per_zone_update": bytes_per_cell,
+            "traffic_model": {"bytes_per_zone_update": model_bytes,
+                              "note": "every materialised intermediate counted (face fluxes, EMFs, signs)"}}
 
+    suite = None
+    if rank == 0 and world == 1 and not args.no_suite and name == "stratified_mhd" and not args.n:
+        suite = run_suite(args, local, head["mlp_params"])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, cores, sample = cpu_rate(name, steps=1, fasteos=not args.no_fasteos, eos_table=args.eos_table)
+        log("cpu baseline")
+        rate, cores, sample = cpu_rate(name, steps=5, fasteos=not args.no_fasteos, eos_table=args.eos_table)
         cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -475,17 +669,17 @@ def run_ours(args):
                 "config": {"workload": name + ("_no_fasteos" if args.no_fasteos else ""), "n": n, "cells": cells,
                            "eos_table": args.eos_table,
                            "form": head_form,
-                           # the headline Newton starts from the previous stage's temperature;
-                           # learned_guess_step times the network's judged guess on the same box
-                           "eos_guess": "warm",
+                           "eos_guess": head_guess,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.0f MB dynamic state)" % (h.state_bytes() / 1e6)},
                 "fp64_plain": {"value": fp64_value, "ms_per_step": fp64["ms"] / max(fp64["done"], 1),
                                "speedup_of_form": value / fp64_value},
-                "l1_vs_fp64": errors, "l1_vs_fp64_long": l1_long, "learned_guess_step": learned_step,
+                "l1_vs_fp64": errors, "l1_vs_fp64_long": l1_long, "learned_eos": learned_info, **side,
+                "suite": suite,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": head["h2d"],
-                        "d2h_bytes_per_step": head["h2d"]},
+                        "d2h_bytes_per_step": head["d2h"], "ms_per_step": head["e2e_ms_per_step"],
+                        "api": "phl_run_steps_host_async (pinned host arrays; upload, step, download per step)"},
                 "gpu_launches": int(head["done"] * launches_per_step), "clocks": head["clocks"],
                 "newton": {k: status[k] for k in ("newton_calls", "newton_iterations", "newton_nonconverged")},
                 "nonfinite": status["nonfinite"]}
@@ -500,6 +694,10 @@ EOS_BYTES_PER_SAMPLE = 44  # rho, e, Abar, Zbar in (FP64), T out (FP64), iterati
 
 
 def run_eos(args):
+    print(json.dumps(eos_line(args)), flush=True)
+
+
+def eos_line(args, with_cpu=True):
     """EoS inversion batch: 2^24 samples over the full table range, bracket vs learned guess.
 
     A step is one inversion of the whole batch (inputs resident in HBM, 2^24 x 44 B > L2).
@@ -586,7 +784,7 @@ def run_eos(args):
                  "frac_within_1e-10_plus_4e-11_kappa": (rel <= 1e-10 + 4e-11 * kappa).double().mean().item()}
     m, b = out["mlp"], out["bracket"]
     cpu = None
-    if not args.no_cpu:
+    if with_cpu and not args.no_cpu:
         k = min(n, 1 << 20)
         cpu = eos_cpu_rate(rho[:k], e_host[:k], abar[:k], zbar[:k], eos_table=args.eos_table)
     achieved = EOS_BYTES_PER_SAMPLE * m["rate"] / 1e9
@@ -609,7 +807,7 @@ def run_eos(args):
             "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "inversions/s", "h2d_bytes_per_step": 40 * n,
                     "d2h_bytes_per_step": 12 * n},
             "gpu_launches": 2 * args.steps, "clocks": m["clocks"]}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def eos_cpu_rate(rho, e, abar, zbar, seconds=10.0, eos_table="fermi"):
@@ -638,9 +836,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="stratified_mhd",
                     choices=["stratified", "stratified_mhd", "hot_bubble", "orszag_tang", "eos"])
-    ap.add_argument("--l1-steps", type=int, default=0,
+    ap.add_argument("--l1-steps", type=int, default=-1,
                     help="also run both forms this many steps from the initial state and report the "
-                         "per-field relative L1 difference (untimed)")
+                         "per-field relative L1 difference (untimed); default 1000 for the Helmholtz boxes")
+    ap.add_argument("--no-suite", action="store_true",
+                    help="skip the other workloads (hot bubble 256^2, Orszag-Tang 1024^2 to t = 0.5, EoS "
+                         "batch 2^24, MHD box 384^3) reported under `suite`")
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--train-epochs", type=int, default=256, help="MLP training epochs (eos workload)")

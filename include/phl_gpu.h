@@ -74,6 +74,9 @@ extern "C" {
                                      warm guess (hydro step) or the bracket guess (EoS batch) */
 #define PHL_GUESS_BRACKET 2 /* EoS batch only: cold guess from the table nodes bracketing e(rho, T)
                                at fixed rho*Ye (monotone search in T); T_inout is not read */
+#define PHL_GUESS_MLP_RESCUE 3 /* hydro step only: the warm guess, and for every cell whose first
+                                  warm Newton correction exceeds 2% of T the learned guess
+                                  (judged as PHL_GUESS_MLP, the warm guess as its fallback) */
 
 typedef struct phl_config {
   int abi_version;                 /* must be PHL_ABI_VERSION */
@@ -87,9 +90,10 @@ typedef struct phl_config {
   int rk_stages;                   /* 2 (RK2_STEPPER) or 3 (RK3_STEPPER) */
   int bc[3][2];                    /* [dim][0 lower, 1 upper] PHL_BC_* */
   int precision;                   /* PHL_FP64 or PHL_FP32_SPLIT */
-  int eos_guess;                   /* PHL_GUESS_WARM, or PHL_GUESS_MLP for the learned guess in
-                                      the step's Newton (FP32 split MHD form with the Helmholtz
-                                      EoS; train or set the network before the first step) */
+  int eos_guess;                   /* PHL_GUESS_WARM, or PHL_GUESS_MLP / PHL_GUESS_MLP_RESCUE for
+                                      the learned guess in the step's Newton (FP32 split MHD form
+                                      with the Helmholtz EoS; train or set the network before the
+                                      first step) */
   int device;                      /* CUDA device ordinal */
   double x1l, x1u, x2l, x2u, x3l, x3u;
   double gamma_ad, mu;             /* initialize_simulation arguments */
@@ -180,6 +184,23 @@ int phl_get_time(phl_ctx *ctx, double *time, double *dt, double *smax);
  * compute_hyperbolic_dt.  Runs asynchronously on the device as CUDA graphs; returns after the
  * last step has finished.  steps_done/time may be NULL. */
 int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double *time);
+
+/* Host-resident state, asynchronous: upload the dynamic state from `host` (prim, temp, eint,
+ * gammaf, b_cc, b_x, laid out as for phl_upload_state; background members are not read),
+ * advance exactly nsteps steps of time_loop (no tmax clamp), and download the dynamic state back
+ * into the same arrays -- all queued on the context's streams; the call returns without waiting.
+ * This is the per-step exchange of a driver that keeps its state in host memory (the reference's
+ * own arrays) and wants the copies off the critical path: the upload of each chunk of host
+ * planes waits only for the previous call's download of the same planes, so the two PCIe
+ * directions overlap across consecutive calls.  Host arrays must be page-locked for the copies
+ * to run asynchronously (pageable memory works but serialises them) and must not be touched
+ * until phl_wait_host returns.  The context must have been set up by phl_upload_state (with the
+ * background) and phl_compute_hyperbolic_dt first.  Every other entry point waits for pending
+ * downloads before it starts.  No counterpart in the reference (its state never leaves the
+ * host); the step it runs is hydro_step + compute_hyperbolic_dt as in phl_run_steps. */
+int phl_run_steps_host_async(phl_ctx *ctx, phl_fields *host, int nsteps);
+/* Block until every queued phl_run_steps_host_async call has written its results to host memory. */
+int phl_wait_host(phl_ctx *ctx);
 
 int phl_get_status(phl_ctx *ctx, phl_status *st);
 int phl_reset_status(phl_ctx *ctx);

@@ -35,7 +35,7 @@ EXPORTS = [
     "phl_reset_status", "phl_eos_invert_batch_device", "phl_eos_invert_batch",
     "phl_eos_energy_device", "phl_mlp_train", "phl_mlp_get_params", "phl_mlp_set_params",
     "phl_mlp_infer_device", "phl_mlp_gradient", "phl_device_field", "phl_stream", "phl_eos_invert_batch_noalloc",
-    "phl_mlp_set_sample_range",
+    "phl_mlp_set_sample_range", "phl_run_steps_host_async", "phl_wait_host",
 ]
 
 
@@ -115,6 +115,8 @@ def load_library(path: str = LIB_PATH):
         "phl_set_time": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
         "phl_get_time": ([vp, _P, _P, _P], C.c_int),
         "phl_run_steps": ([vp, C.c_int, C.c_double, C.POINTER(C.c_int), _P], C.c_int),
+        "phl_run_steps_host_async": ([vp, C.POINTER(PhlFields), C.c_int], C.c_int),
+        "phl_wait_host": ([vp], C.c_int),
         "phl_get_status": ([vp, C.POINTER(PhlStatus)], C.c_int),
         "phl_reset_status": ([vp], C.c_int),
         "phl_eos_invert_batch_device": ([vp, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int], C.c_int),
@@ -274,6 +276,15 @@ class Simulation:
         done, t = C.c_int(), C.c_double()
         _check(self.lib.phl_run_steps(self.ctx, int(nsteps), float(tmax), C.byref(done), C.byref(t)), "phl_run_steps")
         return done.value, t.value
+
+    def time_loop_host_async(self, h: HostGrid, nsteps=1):
+        """Queue upload of h's dynamic state, `nsteps` steps and the download back into h
+        (phl_run_steps_host_async); h must stay alive and untouched until wait_host()."""
+        f = fields_struct(h)
+        _check(self.lib.phl_run_steps_host_async(self.ctx, C.byref(f), int(nsteps)), "phl_run_steps_host_async")
+
+    def wait_host(self):
+        _check(self.lib.phl_wait_host(self.ctx), "phl_wait_host")
 
     def status(self):
         st = PhlStatus()

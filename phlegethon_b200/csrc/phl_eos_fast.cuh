@@ -124,12 +124,13 @@ __device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, doub
   }
 }
 
-// Newton on E(rho, T) = E0 from the warm start T (helm_rhoe_given's loop and exit rules);
-// returns iterations, sets converged / clamped.  On return `c` holds the cell of the final T.
-__device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, double irho, double E0,
-                                              double inv_abar, double &T, int max_iter, int &clamped,
-                                              bool &converged) {
-  const double Told = T;
+// Newton on E(rho, T) = E0 from T (helm_rhoe_given's loop and exit rules); an iterate outside
+// the table is reset to Told and ends the loop, as in the reference.  Returns iterations, sets
+// converged / clamped.  On return `c` holds the cell of the final T.  A solve split into two
+// calls (the second with the first call's starting T as Told) runs the same iterates as one.
+__device__ __forceinline__ int helm_rhoe_fast_from(const HelmTable &h, HelmCell &c, double irho, double E0,
+                                                   double inv_abar, double &T, double Told, int max_iter,
+                                                   int &clamped, bool &converged) {
   const double inv_E0 = 1.0 / E0;
   converged = false;
   int used = 0;
@@ -153,6 +154,13 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
   }
   if (T < c.T0 || T >= c.T0 + c.dT) helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
   return used;
+}
+
+// the same from the warm start T (Told = T)
+__device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, double irho, double E0,
+                                              double inv_abar, double &T, int max_iter, int &clamped,
+                                              bool &converged) {
+  return helm_rhoe_fast_from(h, c, irho, E0, inv_abar, T, T, max_iter, clamped, converged);
 }
 
 // pressure and the square of the relativistic sound speed at (rho, T) from the prepared cell

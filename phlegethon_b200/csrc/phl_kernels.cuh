@@ -96,6 +96,9 @@ struct Prm {
   // launches the learned cons->prim kernel (never dereferenced on the device)
   const MlpSmall *mlp_small;
   float *mlp_feat, *mlp_out;  // per-cell network inputs [cells][4] and log10 T guesses (NaN: none)
+  // eos_guess = PHL_GUESS_MLP_RESCUE: cells whose warm start is poor, queued by cons->prim for
+  // the learned guess ([0] count, then cell indices)
+  unsigned int *rescue_q;
   const double *sf_eq_p;
   int sf_G, sf_eq_profile;
   double eps_sf;

@@ -215,6 +215,7 @@ struct phl_ctx {
   float *fflux[3] = {};
   float *fecell = nullptr;                                                             // split MHD
   float *mlp_feat = nullptr, *mlp_out = nullptr;  // learned guess in the split MHD step
+  unsigned *rescue_q = nullptr;                    // PHL_GUESS_MLP_RESCUE queue (count + cells)
   double *dflux[3] = {};                                                               // FP64 MHD
   // USE_SHOCK_FLATTENING: flags, detector marks, ghosted pressure equilibrium (see Prm)
   unsigned char *sf_flag = nullptr, *sf_mark = nullptr;
@@ -238,6 +239,25 @@ struct phl_ctx {
   size_t stage_bytes = 0;
   // graphs: one per parity of the W ping-pong
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // asynchronous host-state pipeline (phl_run_steps_host_async): copy streams, staging images
+  // of the dynamic host arrays, and the events that order one call's uploads after the previous
+  // call's downloads chunk by chunk
+  struct HostSlot {
+    int ncomp = 0, h1 = 0, h2 = 0, h3 = 0;  // host extents (ghosts included; h3 = 1 in 2D)
+    int fx = 0, fy = 0, fz = 0;             // interior extents (cells or faces)
+    int o1 = 0, o2 = 0, o3 = 0;             // offset of the interior in the host array
+    double *dev = nullptr;                  // SoA device field (cells: [ncomp][N])
+    long long dev_stride = 0;
+    double *in = nullptr, *out = nullptr;   // staging: ghosted host image, compact interior
+    int chunk0 = 0, nchunk = 0, ppc = 1;    // chunks of ppc host planes along x3
+    size_t plane() const { return (size_t)ncomp * h1 * h2; }
+  };
+  static constexpr int HOST_SLOTS = 8;  // prim, temp, eint, gammaf, b_cc, b_x1..3
+  HostSlot hslot[HOST_SLOTS];
+  bool hpipe_ready = false, hpipe_pending = false;
+  cudaStream_t cin = nullptr, cout = nullptr;
+  std::vector<cudaEvent_t> ev_chunk_out;  // per chunk: its download has landed
+  cudaEvent_t ev_in[HOST_SLOTS] = {}, ev_pack[HOST_SLOTS] = {};
   // EoS batch scratch and MLP
   EosBatch eos;
   std::vector<void *> allocs;
@@ -246,8 +266,24 @@ struct phl_ctx {
     for (int p = 0; p < 2; ++p)
       if (graph[p]) cudaGraphExecDestroy(graph[p]);
     eos.release();
+    for (cudaEvent_t e : ev_chunk_out) cudaEventDestroy(e);
+    for (int q = 0; q < HOST_SLOTS; ++q) {
+      if (ev_in[q]) cudaEventDestroy(ev_in[q]);
+      if (ev_pack[q]) cudaEventDestroy(ev_pack[q]);
+    }
+    if (cin) cudaStreamDestroy(cin);
+    if (cout) cudaStreamDestroy(cout);
     for (void *a : allocs) cudaFree(a);
     if (stream) cudaStreamDestroy(stream);
+  }
+  // wait for the downloads of earlier asynchronous host-state calls (every entry point that
+  // reads or writes caller memory runs this first)
+  int drain_host() {
+    if (!hpipe_pending) return PHL_OK;
+    CK(cudaStreamSynchronize(cout));
+    CK(cudaStreamSynchronize(stream));
+    hpipe_pending = false;
+    return PHL_OK;
   }
   template <class T>
   int alloc(T **p, size_t count) {
@@ -318,11 +354,12 @@ struct phl_ctx {
     }
     P.bcc_in = bcc;
     P.bcc_out = bcc;
-    if (cfg.eos_guess == PHL_GUESS_MLP && eos.mlp.ready) {
+    if ((cfg.eos_guess == PHL_GUESS_MLP || cfg.eos_guess == PHL_GUESS_MLP_RESCUE) && eos.mlp.ready) {
       MlpWeights mw = eos.mlp.weights();
       P.mlp_w = mw.w;
       P.mlp_w2bf = mw.w2bf;
       P.mlp_small = mlp_small_ok ? &mlp_small : nullptr;
+      P.rescue_q = cfg.eos_guess == PHL_GUESS_MLP_RESCUE ? rescue_q : nullptr;
     }
     P.sf_flag = sf_flag;
     P.sf_mark = sf_mark;
@@ -386,6 +423,28 @@ struct phl_ctx {
   void launch_stages() {
     for (int s = 0; s < cfg.rk_stages; ++s) runner->stage(prm(s), stream);
   }
+  // one time_loop iteration as a CUDA graph (captured on first use per W parity): tmax clamp,
+  // the RK stages, time += dt, the next dt
+  int launch_step_graph() {
+    int p = cur;
+    if (!graph[p]) {
+      cudaGraph_t gph;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      k_pre_step<<<1, 1, 0, stream>>>(scal, active, smax_bits, step, (long long)1 << 62);
+      launch_stages();
+      k_post_step<<<1, 1, 0, stream>>>(scal, active, smax_bits, step, cfg.cfl);
+      CK(cudaStreamEndCapture(stream, &gph));
+      cudaError_t e = cudaGraphInstantiate(&graph[p], gph, 0);
+      cudaGraphDestroy(gph);
+      if (e != cudaSuccess) {
+        g_last_error = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        return PHL_E_CUDA;
+      }
+    }
+    CK(cudaGraphLaunch(graph[p], stream));
+    cur = (cur + cfg.rk_stages) & 1;
+    return PHL_OK;
+  }
 };
 
 namespace {
@@ -420,12 +479,12 @@ int check_cfg(const phl_config *c) {
   // the FP64 form keeps the reference's warm start (bit-exact); the learned guess inside the step
   // is built for the split MHD stage (Helmholtz), judged by the Newton with the warm start as
   // the fallback
-  if (c->eos_guess == PHL_GUESS_MLP &&
-      !(c->precision == PHL_FP32_SPLIT && (c->flags & PHL_MHD) && (c->flags & PHL_HELMHOLTZ))) {
-    g_last_error = "eos_guess = PHL_GUESS_MLP in the step is built for the FP32 split MHD form with the Helmholtz EoS";
+  const bool learned = c->eos_guess == PHL_GUESS_MLP || c->eos_guess == PHL_GUESS_MLP_RESCUE;
+  if (learned && !(c->precision == PHL_FP32_SPLIT && (c->flags & PHL_MHD) && (c->flags & PHL_HELMHOLTZ))) {
+    g_last_error = "a learned eos_guess in the step is built for the FP32 split MHD form with the Helmholtz EoS";
     return PHL_E_UNSUPPORTED;
   }
-  if (c->eos_guess != PHL_GUESS_WARM && c->eos_guess != PHL_GUESS_MLP) return PHL_E_INVALID;
+  if (c->eos_guess != PHL_GUESS_WARM && !learned) return PHL_E_INVALID;
   return PHL_OK;
 }
 
@@ -579,6 +638,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
         if ((rc = c->alloc(&c->mlp_feat, (size_t)4 * N))) return rc;
         if ((rc = c->alloc(&c->mlp_out, (size_t)N))) return rc;
       }
+      if (cfg->eos_guess == PHL_GUESS_MLP_RESCUE && (rc = c->alloc(&c->rescue_q, (size_t)N + 1))) return rc;
       for (int d = 0; d < cfg->sdims; ++d) {
         long long nf = c->nfaces(d);
         if ((rc = c->alloc(&c->femf[d], (size_t)3 * nf))) return rc;
@@ -609,6 +669,7 @@ int phl_init(const phl_config *cfg, phl_ctx **out) {
 void phl_finalize(phl_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->cfg.device);
+  ctx->drain_host();
   cudaStreamSynchronize(ctx->stream);
   delete ctx;
 }
@@ -652,6 +713,7 @@ int phl_upload_state(phl_ctx *ctx, const phl_fields *f) {
   if (!ctx || !f || !f->prim) return PHL_E_INVALID;
   const phl_config &c = ctx->cfg;
   CK(cudaSetDevice(c.device));
+  if (int rc = ctx->drain_host()) return rc;
   cudaStream_t s = ctx->stream;
   const int G = c.ngc, G3 = c.sdims == 3 ? c.ngc : 0, sd = c.sdims, nv = c.nvars;
   const int nx = c.nx1, ny = c.nx2, nz = c.nx3;
@@ -826,6 +888,7 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
   if (!ctx || !f) return PHL_E_INVALID;
   const phl_config &c = ctx->cfg;
   CK(cudaSetDevice(c.device));
+  if (int rc = ctx->drain_host()) return rc;
   cudaStream_t s = ctx->stream;
   const int G = c.ngc, G3 = c.sdims == 3 ? c.ngc : 0, sd = c.sdims, nv = c.nvars;
   const int nx = c.nx1, ny = c.nx2, nz = c.nx3;
@@ -873,9 +936,11 @@ int phl_download_state(phl_ctx *ctx, phl_fields *f) {
 // step: the call advances the state (and so runs the cons->prim Newton with the selected guess)
 static int ready(phl_ctx *ctx, bool step = false) {
   if (!ctx) return PHL_E_INVALID;
+  if (int rc = ctx->drain_host()) return rc;
   if (!ctx->uploaded) return PHL_E_STATE;
   if ((ctx->cfg.flags & PHL_HELMHOLTZ) && !ctx->table_loaded) return PHL_E_NO_TABLE;
-  if (step && ctx->cfg.eos_guess == PHL_GUESS_MLP && !ctx->eos.mlp.ready) {
+  if (step && (ctx->cfg.eos_guess == PHL_GUESS_MLP || ctx->cfg.eos_guess == PHL_GUESS_MLP_RESCUE) &&
+      !ctx->eos.mlp.ready) {
     g_last_error = "eos_guess = PHL_GUESS_MLP: train the network (phl_mlp_train) or set its parameters first";
     return PHL_E_STATE;
   }
@@ -964,25 +1029,8 @@ int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double
   CK(cudaStreamSynchronize(s));
   // graphs run with no device-side step limit: the host launches exactly nsteps of them and
   // the device stops by itself once time >= tmax.
-  for (int n = 0; n < nsteps; ++n) {
-    int p = ctx->cur;
-    if (!ctx->graph[p]) {
-      cudaGraph_t gph;
-      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      k_pre_step<<<1, 1, 0, s>>>(ctx->scal, ctx->active, ctx->smax_bits, ctx->step, (long long)1 << 62);
-      ctx->launch_stages();
-      k_post_step<<<1, 1, 0, s>>>(ctx->scal, ctx->active, ctx->smax_bits, ctx->step, ctx->cfg.cfl);
-      CK(cudaStreamEndCapture(s, &gph));
-      cudaError_t e = cudaGraphInstantiate(&ctx->graph[p], gph, 0);
-      cudaGraphDestroy(gph);
-      if (e != cudaSuccess) {
-        g_last_error = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
-        return PHL_E_CUDA;
-      }
-    }
-    CK(cudaGraphLaunch(ctx->graph[p], s));
-    ctx->cur = (ctx->cur + ctx->cfg.rk_stages) & 1;
-  }
+  for (int n = 0; n < nsteps; ++n)
+    if ((rc = ctx->launch_step_graph())) return rc;
   long long step1 = 0;
   double t = 0;
   CK(cudaMemcpyAsync(&step1, ctx->step, sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -994,6 +1042,155 @@ int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double
   if (skipped > 0 && (ctx->cfg.rk_stages & 1)) ctx->cur = (int)((ctx->cur + skipped) & 1);
   if (steps_done) *steps_done = (int)(step1 - step0);
   if (time) *time = t;
+  return PHL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Lay out the pipeline's slots for this context (once): extents of each dynamic host array,
+// its device field, staging images and chunking along x3.
+int host_pipe_setup(phl_ctx *ctx) {
+  if (ctx->hpipe_ready) return PHL_OK;
+  const phl_config &c = ctx->cfg;
+  const int G = c.ngc, G3 = c.sdims == 3 ? c.ngc : 0, sd = c.sdims, nv = c.nvars;
+  const int nx = c.nx1, ny = c.nx2, nz = c.nx3;
+  const bool mhd = c.flags & PHL_MHD, helm = c.flags & PHL_HELMHOLTZ, fast = c.flags & PHL_FASTEOS;
+  auto cell = [&](int q, int ncomp, double *dev) {
+    phl_ctx::HostSlot &h = ctx->hslot[q];
+    h.ncomp = ncomp; h.h1 = nx + 2 * G; h.h2 = ny + 2 * G; h.h3 = nz + 2 * G3;
+    h.fx = nx; h.fy = ny; h.fz = nz; h.o1 = G; h.o2 = G; h.o3 = G3;
+    h.dev = dev; h.dev_stride = ctx->N;
+  };
+  cell(0, nv, nullptr);  // prim: W[cur], chosen per call
+  cell(1, 1, ctx->temp);
+  cell(2, 1, ctx->eint);
+  if (helm && fast) cell(3, 2, nullptr);  // gammaf: gam[cur]
+  if (mhd) cell(4, sd, ctx->bcc);
+  for (int d = 0; d < sd && mhd; ++d) {
+    phl_ctx::HostSlot &h = ctx->hslot[5 + d];
+    h.ncomp = 1;
+    h.h1 = nx + 2 + (d == 0); h.h2 = ny + 2 + (d == 1); h.h3 = sd == 3 ? nz + 2 + (d == 2) : 1;
+    h.fx = nx + (d == 0); h.fy = ny + (d == 1); h.fz = sd == 3 ? nz + (d == 2) : 1;
+    h.o1 = 1; h.o2 = 1; h.o3 = sd == 3 ? 1 : 0;
+    h.dev = ctx->bf[d]; h.dev_stride = ctx->nfaces(d);
+  }
+  // chunks of about 64 MB: the upload of a chunk waits only for the previous call's download
+  // of the same host planes, so the two directions overlap with a lag of one chunk
+  const size_t chunk_bytes = (size_t)64 << 20;
+  int nchunks = 0;
+  for (int q = 0; q < phl_ctx::HOST_SLOTS; ++q) {
+    phl_ctx::HostSlot &h = ctx->hslot[q];
+    if (!h.ncomp) continue;
+    size_t pb = h.plane() * sizeof(double);
+    h.ppc = (int)std::max<size_t>(1, chunk_bytes / std::max<size_t>(pb, 1));
+    h.nchunk = (h.h3 + h.ppc - 1) / h.ppc;
+    h.chunk0 = nchunks;
+    nchunks += h.nchunk;
+    int rc;
+    if ((rc = ctx->alloc(&h.in, h.plane() * h.h3)) ||
+        (rc = ctx->alloc(&h.out, (size_t)h.ncomp * h.fx * h.fy * h.fz)))
+      return rc;
+    CK(cudaEventCreateWithFlags(&ctx->ev_in[q], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_pack[q], cudaEventDisableTiming));
+  }
+  ctx->ev_chunk_out.assign(nchunks, nullptr);
+  for (int k = 0; k < nchunks; ++k) CK(cudaEventCreateWithFlags(&ctx->ev_chunk_out[k], cudaEventDisableTiming));
+  CK(cudaStreamCreateWithFlags(&ctx->cin, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->cout, cudaStreamNonBlocking));
+  CK(cudaStreamSynchronize(ctx->stream));  // the staging allocations are zeroed on it
+  ctx->hpipe_ready = true;
+  return PHL_OK;
+}
+
+__global__ void k_set_tmax_inf(double *scal) { scal[3] = __longlong_as_double(0x7ff0000000000000LL); }
+}  // namespace
+
+extern "C" {
+
+int phl_run_steps_host_async(phl_ctx *ctx, phl_fields *f, int nsteps) {
+  if (!ctx || !f || !f->prim || nsteps < 0) return PHL_E_INVALID;
+  if ((ctx->cfg.flags & PHL_HELMHOLTZ) && !ctx->table_loaded) return PHL_E_NO_TABLE;
+  if (!ctx->uploaded) return PHL_E_STATE;
+  if ((ctx->cfg.eos_guess == PHL_GUESS_MLP || ctx->cfg.eos_guess == PHL_GUESS_MLP_RESCUE) && !ctx->eos.mlp.ready)
+    return PHL_E_STATE;
+  const phl_config &c = ctx->cfg;
+  const bool mhd = c.flags & PHL_MHD, helm = c.flags & PHL_HELMHOLTZ, fast = c.flags & PHL_FASTEOS;
+  for (int d = 0; d < c.sdims && mhd; ++d)
+    if (!f->b_x[d]) return PHL_E_INVALID;
+  CK(cudaSetDevice(c.device));
+  int rc;
+  if ((rc = host_pipe_setup(ctx))) return rc;
+  cudaStream_t S = ctx->stream;
+  double *host[phl_ctx::HOST_SLOTS] = {f->prim, f->temp, f->eint, (helm && fast) ? f->gammaf : nullptr,
+                                       mhd ? f->b_cc : nullptr, mhd ? f->b_x[0] : nullptr,
+                                       mhd ? f->b_x[1] : nullptr, mhd ? f->b_x[2] : nullptr};
+  // ---- upload: whole host arrays (ghost layers included) chunk by chunk on the input stream
+  ctx->cur = 0;
+  ctx->hslot[0].dev = ctx->W[0];
+  ctx->hslot[3].dev = ctx->gam[0];
+  for (int q = 0; q < phl_ctx::HOST_SLOTS; ++q) {
+    phl_ctx::HostSlot &h = ctx->hslot[q];
+    if (!h.ncomp || !host[q]) continue;
+    for (int k = 0; k < h.nchunk; ++k) {
+      const int p0 = k * h.ppc, p1 = std::min(h.h3, p0 + h.ppc);
+      const size_t off = h.plane() * p0;
+      CK(cudaStreamWaitEvent(ctx->cin, ctx->ev_chunk_out[h.chunk0 + k], 0));
+      CK(cudaMemcpyAsync(h.in + off, host[q] + off, sizeof(double) * h.plane() * (p1 - p0), cudaMemcpyHostToDevice,
+                         ctx->cin));
+    }
+    CK(cudaEventRecord(ctx->ev_in[q], ctx->cin));
+    CK(cudaStreamWaitEvent(S, ctx->ev_in[q], 0));
+    const long long n = (long long)h.fx * h.fy * h.fz;
+    k_unpack<<<nblk(n, 256), 256, 0, S>>>(h.in, h.dev, h.ncomp, h.fx, h.fy, h.fz, h.h1, h.h2, h.o1, h.o2, h.o3,
+                                          h.ncomp, h.dev_stride);
+    CK(cudaGetLastError());
+  }
+  // without USE_FASTEOS the first gamma slot carries the stage input's temperature
+  if (helm && !fast && f->temp)
+    CK(cudaMemcpyAsync(ctx->gam[0], ctx->temp, sizeof(double) * (size_t)ctx->N, cudaMemcpyDeviceToDevice, S));
+  if (ctx->split) ctx->split_from_prim();
+  // ---- exactly nsteps steps (no tmax clamp: a skipped step would leave W's parity unknown to
+  // the host without a round trip)
+  k_set_tmax_inf<<<1, 1, 0, S>>>(ctx->scal);
+  for (int n = 0; n < nsteps; ++n)
+    if ((rc = ctx->launch_step_graph())) return rc;
+  CK(cudaGetLastError());
+  // ---- download: interior of each array, chunk by chunk on the output stream
+  if (ctx->split) ctx->split_to_prim();
+  ctx->hslot[0].dev = ctx->W[ctx->cur];
+  ctx->hslot[3].dev = ctx->gam[ctx->cur];
+  for (int q = 0; q < phl_ctx::HOST_SLOTS; ++q) {
+    phl_ctx::HostSlot &h = ctx->hslot[q];
+    if (!h.ncomp || !host[q]) continue;
+    const long long n = (long long)h.fx * h.fy * h.fz;
+    k_pack<<<nblk(n, 256), 256, 0, S>>>(h.dev, h.out, h.ncomp, h.fx, h.fy, h.fz, h.fx, h.fy, 0, 0, 0, h.ncomp,
+                                        h.dev_stride);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev_pack[q], S));
+    CK(cudaStreamWaitEvent(ctx->cout, ctx->ev_pack[q], 0));
+    for (int k = 0; k < h.nchunk; ++k) {
+      // interior planes inside host planes [p0, p1)
+      const int p0 = k * h.ppc, p1 = std::min(h.h3, p0 + h.ppc);
+      const int q0 = std::max(p0 - h.o3, 0), q1 = std::min(p1 - h.o3, h.fz);
+      if (q1 > q0) {
+        const double *src = h.out + (size_t)h.ncomp * h.fx * h.fy * q0;
+        double *dst = host[q] + (size_t)h.ncomp * ((size_t)h.o1 + (size_t)h.h1 * ((size_t)h.o2 + (size_t)h.h2 * (q0 + h.o3)));
+        CK(copy_box_d2h(src, dst, (size_t)h.ncomp * h.fx, (size_t)h.ncomp * h.h1, h.fy, h.h2, q1 - q0, ctx->cout));
+      }
+      CK(cudaEventRecord(ctx->ev_chunk_out[h.chunk0 + k], ctx->cout));
+    }
+  }
+  ctx->hpipe_pending = true;
+  return PHL_OK;
+}
+
+int phl_wait_host(phl_ctx *ctx) {
+  if (!ctx) return PHL_E_INVALID;
+  CK(cudaSetDevice(ctx->cfg.device));
+  int rc = ctx->drain_host();
+  if (rc) return rc;
+  CK(cudaGetLastError());
   return PHL_OK;
 }
 

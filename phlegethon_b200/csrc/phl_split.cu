@@ -1240,6 +1240,8 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
 // so their loads stay within a few cache lines) and along y, z (threads of a warp are
 // neighbours in x and walk side by side)
 constexpr int WALK_K0 = 4, WALK_K = 8;
+// grid of the rescue-queue kernels: 4 blocks of 128 threads per SM of a B200 (148 SMs)
+constexpr int RESCUE_BLOCKS = 4 * 148;
 // resident blocks of 128 threads per SM the walking kernels are compiled for
 constexpr int WALK_MINB = 6;
 
@@ -1599,15 +1601,29 @@ __device__ __forceinline__ void c2p_mhd_split_combine(const Prm &P, long long c,
   }
 }
 
+// Temperature guess of the split MHD cons->prim Newton
+enum { C2P_WARM = 0,    // the previous stage's temperature (the reference's warm start)
+       C2P_LEARNED = 1, // the network's guess, judged by <= 3 Newton iterations
+       C2P_RESCUE = 2   // the warm start; a cell whose first Newton correction exceeds
+                        // RESCUE_STEP * T is queued for the learned guess instead
+};
+// first warm-start correction (relative) above which a cell is handed to the learned guess: the
+// network's guesses are within ~0.2% (0.001 dex); from a start 2% off the warm Newton needs
+// ~4 more iterations, from the learned guess ~3 in all
+constexpr double RESCUE_STEP = 0.02;
+
 // MHD stage, part 3b: cons -> prim of the new state with the Helmholtz Newton (FP64) from the
-// warm guess (the previous stage's temperature), or with LEARNED from the network's guess lT
+// warm guess (the previous stage's temperature), or (C2P_LEARNED) from the network's guess lT
 // (log10 T; NaN for none): the guess is accepted when the reference Newton converges from it
 // within 3 iterations without leaving the table, otherwise the Newton starts again from the
 // warm guess.  FP32 density and pressure deviations, gammas, T and eint out; last stage the
-// cell's CFL speed with the Alfven speed.
-template <class C, bool LEARNED>
-__device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, const C2pState &cs, float lT_mlp,
+// cell's CFL speed with the Alfven speed.  C2P_RESCUE: a cell whose warm start is poor stores
+// eint, joins P.rescue_q and returns false with nothing else written (the rescue kernels finish
+// it from the learned guess); the other cells run the warm-start Newton unchanged.
+template <class C, int MODE>
+__device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, const C2pState &cs, float lT_mlp,
                                                   SplitStat &st) {
+  constexpr bool LEARNED = MODE == C2P_LEARNED;
   constexpr int IP = C::IP, DIM = C::DIM;
   const Geo &g = P.g;
   const double rho = cs.rho, inv_rho = cs.inv_rho, eint = cs.eint, ye = cs.ye, inv_abar = cs.inv_abar;
@@ -1639,6 +1655,21 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
           helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
           it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
         }
+      } else if constexpr (MODE == C2P_RESCUE) {
+        const double Tw = P.temp[c];
+        T = Tw;
+        helm_cell_init_rho(P.helm, hc, rho, ye);
+        helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+        it = helm_rhoe_fast_from(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, Tw, 1, clamped, conv);
+        if (!conv && fabs(T - Tw) > RESCUE_STEP * Tw) {
+          // poor warm start: the learned guess finishes this cell (its iteration is counted)
+          st.iters += it;
+          P.eint[c] = eint;
+          const unsigned slot = atomicAdd(P.rescue_q, 1u);
+          P.rescue_q[1 + slot] = (unsigned)c;
+          return false;
+        }
+        if (!conv) it += helm_rhoe_fast_from(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, Tw, 99, clamped, conv);
       } else {
         T = P.temp[c];
         helm_cell_init_rho(P.helm, hc, rho, ye);
@@ -1687,12 +1718,13 @@ __device__ __forceinline__ void c2p_mhd_split_eos(const Prm &P, long long c, con
       double sx2 = (vabs[1] + csnd) * g.inv_dx[1];
       double sm = sx1 + sx2;
       if (DIM == 3) sm = (vabs[2] + csnd) * g.inv_dx[2] + sm;
-      st.smax = sm;
+      st.smax = fmax(st.smax, sm);
     }
   }
+  return true;
 }
 
-template <class C>
+template <class C, int MODE>
 __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   SplitStat st;
@@ -1700,9 +1732,40 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
   if (c < P.g.N) {
     C2pState cs;
     c2p_mhd_split_combine<C>(P, c, cs);
-    c2p_mhd_split_eos<C, false>(P, c, cs, 0.0f, st);
+    c2p_mhd_split_eos<C, MODE>(P, c, cs, 0.0f, st);
   }
   split_stat_flush<C>(P, st);
+}
+
+// the state of the combine for cell c, read back from U and eint
+template <class C>
+__device__ __forceinline__ void c2p_state_from_u(const Prm &P, long long c, C2pState &cs) {
+  constexpr int IAS = C::IAS;
+  const Geo &g = P.g;
+  int i, j, k;
+  unflatten3(c, g.nx[0], g.nx[1], i, j, k);
+  cs.bc = bg_cc(g, i, j, k);
+  cs.rho = P.U[c];
+  cs.inv_rho = 1.0 / cs.rho;
+  cs.eint = P.eint[c];
+  cs.ye = P.U[(long long)IAS * g.N + c] * cs.inv_rho;
+  cs.inv_abar = P.U[(long long)(IAS + 1) * g.N + c] * cs.inv_rho;
+}
+
+// the network's input features of a cell: log10 rho, log10 of the thermal energy (the cold
+// energy E(rho, T_lo) from the density row of the table subtracted), Abar, Zbar, each scaled
+template <class C>
+__device__ __forceinline__ float4 c2p_features(const Prm &P, const C2pState &cs) {
+  HelmCell hc;
+  const double abar = 1.0 / cs.inv_abar, zbar = cs.ye * abar;
+  helm_cell_init_rho(P.helm, hc, cs.rho, cs.ye);
+  const double e_th = cs.eint * cs.inv_rho - helm_cell_cold_energy(P.helm, hc, cs.inv_rho, cs.inv_abar);
+  float4 f;
+  f.x = (log10f((float)cs.rho) - 3.5f) / 5.5f;
+  f.y = (log10f((float)fmax(e_th, 1e-30)) - 19.5f) / 8.5f;
+  f.z = (float)((abar - 28.5) / 27.5);
+  f.w = (float)((zbar - 14.0) / 14.0);
+  return f;
 }
 
 // Learned guess in the step, in three launches so that the cons->prim kernels keep their
@@ -1717,39 +1780,20 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_features(P
   C2pState cs;
   c2p_mhd_split_combine<C>(P, c, cs);
   P.eint[c] = cs.eint;
-  // features (the cold energy from the density row of the table)
-  HelmCell hc;
-  const double abar = 1.0 / cs.inv_abar, zbar = cs.ye * abar;
-  helm_cell_init_rho(P.helm, hc, cs.rho, cs.ye);
-  const double e_th = cs.eint * cs.inv_rho - helm_cell_cold_energy(P.helm, hc, cs.inv_rho, cs.inv_abar);
-  float4 f;
-  f.x = (log10f((float)cs.rho) - 3.5f) / 5.5f;
-  f.y = (log10f((float)fmax(e_th, 1e-30)) - 19.5f) / 8.5f;
-  f.z = (float)((abar - 28.5) / 27.5);
-  f.w = (float)((zbar - 14.0) / 14.0);
-  reinterpret_cast<float4 *>(P.mlp_feat)[c] = f;
+  reinterpret_cast<float4 *>(P.mlp_feat)[c] = c2p_features<C>(P, cs);
 }
 
 template <class C>
 __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_guessed(Prm P) {
   if (!*P.active) return;
-  constexpr int IAS = C::IAS;
   SplitStat st;
-  const Geo &g = P.g;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < g.N) {
+  if (c < P.g.N) {
     // the state of the combine, read back: U and eint
     C2pState cs;
-    int i, j, k;
-    unflatten3(c, g.nx[0], g.nx[1], i, j, k);
-    cs.bc = bg_cc(g, i, j, k);
-    cs.rho = P.U[c];
-    cs.inv_rho = 1.0 / cs.rho;
-    cs.eint = P.eint[c];
-    cs.ye = P.U[(long long)IAS * g.N + c] * cs.inv_rho;
-    cs.inv_abar = P.U[(long long)(IAS + 1) * g.N + c] * cs.inv_rho;
+    c2p_state_from_u<C>(P, c, cs);
     st.gevals += 1;
-    c2p_mhd_split_eos<C, true>(P, c, cs, P.mlp_out[c], st);
+    c2p_mhd_split_eos<C, C2P_LEARNED>(P, c, cs, P.mlp_out[c], st);
   }
   split_stat_flush<C>(P, st);
 }
@@ -1773,6 +1817,46 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const __grid_constant_
   const float y = mlp_forward_tile(w, x, S, 0u, ok, have, stalled);
   mlp_cta_teardown(S);
   if (t < n) out[t] = have ? y : __int_as_float(0x7fc00000);
+}
+
+// ---- learned rescue of poor warm starts (eos_guess = PHL_GUESS_MLP_RESCUE): one kernel on a
+// fixed grid over the queue that k_c2p_mhd_split<C, C2P_RESCUE> fills.  Tiles of 128 queue
+// slots, strided over the blocks: each thread reads its cell's state back (U, eint) and forms
+// the network's features, the block runs one tensor-core product for the tile, and each thread
+// finishes its cell from the judged guess.  With an empty queue every block reads the count and
+// returns; a block without a tile returns before it claims tensor memory.
+template <class C>
+__global__ void __launch_bounds__(128) k_c2p_rescue(Prm P, const __grid_constant__ MlpSmall w) {
+  if (!*P.active) return;
+  const long long n = P.rescue_q[0];
+  if ((long long)blockIdx.x * blockDim.x >= n) return;
+  extern __shared__ __align__(128) unsigned char mlp_sm[];
+  MlpUmmaSmem &S = *reinterpret_cast<MlpUmmaSmem *>(mlp_sm);
+  mlp_cta_setup(P.mlp_w2bf, S);
+  SplitStat st;
+  bool ok = true;
+  uint32_t parity = 0;
+  for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < n; t0 += (long long)gridDim.x * blockDim.x) {
+    const long long q = t0 + threadIdx.x;
+    C2pState cs;
+    long long c = -1;
+    float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (q < n) {
+      c = P.rescue_q[1 + q];
+      c2p_state_from_u<C>(P, c, cs);
+      const float4 f = c2p_features<C>(P, cs);
+      x[0] = f.x; x[1] = f.y; x[2] = f.z; x[3] = f.w;
+    }
+    bool have = false;
+    const float y = mlp_forward_tile(w, x, S, parity, ok, have, P.stat + STAT_TC_STALLED);
+    parity ^= 1u;
+    if (c >= 0) {
+      st.gevals += 1;
+      c2p_mhd_split_eos<C, C2P_LEARNED>(P, c, cs, have ? y : __int_as_float(0x7fc00000), st);
+    }
+  }
+  mlp_cta_teardown(S);
+  split_stat_flush<C>(P, st);
 }
 
 // FP64 primitives (+eint, gammaf) -> U (FP64) and FP32 deviations (prim->cons of
@@ -1988,6 +2072,13 @@ struct SplitRunnerT : Runner {
       k_bface_split<C, 1><<<nblk(nfc(1), 256), 256, 0, s>>>(P);
       if constexpr (C::DIM == 3) k_bface_split<C, 2><<<nblk(nfc(2), 256), 256, 0, s>>>(P);
       if constexpr (C::HELM) {
+        if (P.mlp_w && P.mlp_small && P.rescue_q) {
+          // warm start everywhere; cells with a poor warm start through the learned guess
+          cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
+          k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, 128), 128, 0, s>>>(P);
+          k_c2p_rescue<C><<<RESCUE_BLOCKS, 128, sizeof(MlpUmmaSmem), s>>>(P, *P.mlp_small);
+          return;
+        }
         if (P.mlp_w && P.mlp_small && P.mlp_feat && P.mlp_out) {
           k_c2p_mhd_split_features<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
           k_mlp_guess<<<nblk(g.N, 128), 128, sizeof(MlpUmmaSmem), s>>>(*P.mlp_small, P.mlp_w2bf, g.N, P.mlp_feat,
@@ -1996,7 +2087,7 @@ struct SplitRunnerT : Runner {
           return;
         }
       }
-      k_c2p_mhd_split<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, 128), 128, 0, s>>>(P);
     } else {
       hydro_stage(P, s);
     }

@@ -29,7 +29,7 @@ FLAG_FLUX_IS_ALL_MACH = 1 << 8
 FLAG_CONSTANT_ACCELERATION = 1 << 9
 
 PRECISION = {"fp64": 0, "fp32_split": 1}
-GUESS = {"warm": 0, "mlp": 1, "bracket": 2}
+GUESS = {"warm": 0, "mlp": 1, "bracket": 2, "mlp_rescue": 3}
 
 
 @dataclass
@@ -232,6 +232,18 @@ class HostGrid:
                 setattr(h, name, v.copy(order="F"))
             elif isinstance(v, list):
                 setattr(h, name, [a.copy(order="F") if isinstance(a, np.ndarray) else a for a in v])
+        return h
+
+    def dynamic_copy(self) -> "HostGrid":
+        """A copy that carries only the dynamic state (background members None): what a driver
+        passes to phl_upload_state to refresh the state without re-sending the background, and
+        what phl_run_steps_host_async exchanges every call."""
+        h = self.copy()
+        for name in ("grav", "phi_cc", "eq_prim_cc", "eq_gammae_cc"):
+            setattr(h, name, None)
+        h.phi_x = [None] * 3
+        h.eq_prim_x = [None] * 3
+        h.eq_gammae_x = [None] * 3
         return h
 
     def dynamic_arrays(self):

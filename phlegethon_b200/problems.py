@@ -107,7 +107,8 @@ def fermi_temperature(rho, p, abar, zbar, T0=1e8):
         dfdT = th["P_T"].reshape(rho.shape) + CONST_RGAS * rho / abar + 4.0 / 3.0 * CONST_RAD * T ** 3
         dT = f / dfdT
         T = np.clip(T - dT, 1e3, 1e13)
-        if np.all(np.abs(dT) <= 1e-14 * T):
+        # the quadrature of the Fermi integrals leaves a rounding floor near 4e-14 in dT / T
+        if np.all(np.abs(dT) <= 1e-12 * T):
             break
     return T
 

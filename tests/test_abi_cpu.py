@@ -77,6 +77,11 @@ def test_bench_algorithmic_bytes():
     assert bench.step_bytes_per_cell(cfg.replace(precision="fp32_split")) == 776
     cfgm, _ = problems.stratified_3d(8, mhd=True)
     assert bench.step_bytes_per_cell(cfgm.replace(precision="fp32_split")) == 2072
+    # roofline numerators: algorithmic bytes, below the materialised traffic model
+    assert bench.algorithmic_bytes_per_cell("stratified_mhd", "fp32_split") == 904
+    assert bench.algorithmic_bytes_per_cell("stratified_mhd", "fp64") == 1120
+    assert bench.algorithmic_bytes_per_cell("stratified", "fp32_split") == 712
+    assert bench.algorithmic_bytes_per_cell("hot_bubble", "fp64") == 448
     name, launches = bench.stage_kernels(cfgm.replace(precision="fp32_split"), "fp32_split")
     assert "k_face_split_mhd" in name and launches == 3 * (3 + 3 + 3 + 1) + 2
 

@@ -213,3 +213,74 @@ def test_learned_guess_trained_on_the_run_range(gpu_lib, table):
     assert s["nonfinite"] == 0 and s["newton_nonconverged"] == 0
     assert s["mlp_accepted"] + s["mlp_rejected"] == s["newton_calls"]
     assert s["mlp_accepted"] >= 0.99 * s["newton_calls"], s
+
+
+def test_learned_rescue_of_poor_warm_starts(gpu_lib, table):
+    """eos_guess = PHL_GUESS_MLP_RESCUE: every cell starts from the warm guess; a cell whose first
+    warm Newton correction exceeds 2% of T is queued and finished from the network's judged
+    guess (the warm guess as its fallback).  In the steady step no cell is queued and the state
+    equals the warm-start run bit for bit.  After a restart from a temperature field 30% off
+    (the stage input's T is the Newton's warm start) every cell of the first stage is rescued,
+    the state equals the warm run to the Newton tolerance, and the rescued Newton needs fewer
+    iterations than the one from the poor warm start.  The box (92,160 cells) fills more rescue
+    tiles than the queue kernel has blocks, so blocks run several tensor-core tiles."""
+    import ctypes as C
+    from phlegethon_b200.abi import Simulation
+    from phlegethon_b200.grid import helm_state_range
+    from util import field_errors, max_abs_diff
+    cfg, h = problems.stratified_3d(48, ny=40, nz=48, mhd=True)
+    n = cfg.n_cells
+    params = None
+    out, stats = {}, {}
+    for perturb in (False, True):
+        for guess in ("warm", "mlp_rescue"):
+            c = cfg.replace(precision="fp32_split", eos_guess=guess)
+            hg = h.copy()
+            with Simulation(c, table) as sim:
+                sim.upload(hg)
+                sim.init_thermo()
+                if guess != "warm":
+                    if params is None:
+                        h0 = h.copy()
+                        sim.download(h0)
+                        lo, hi = helm_state_range(h0, cfg)
+                        # wide enough in T for the perturbed restart's states
+                        lo[1] -= 0.3
+                        hi[1] += 0.3
+                        sim.set_mlp_sample_range(lo, hi)
+                        assert sim.lib.phl_mlp_train(sim.ctx, 1 << 22, 11, 256, 8192, C.c_double(3e-3), None) == 0
+                        params = np.zeros(PHL_MLP_NPARAMS, dtype=np.float32)
+                        assert sim.lib.phl_mlp_get_params(sim.ctx, params.ctypes.data_as(C.POINTER(C.c_float))) == 0
+                    else:
+                        assert sim.lib.phl_mlp_set_params(sim.ctx, params.ctypes.data_as(C.POINTER(C.c_float))) == 0
+                if perturb:
+                    dyn = h.dynamic_copy()
+                    sim.download(dyn)
+                    dyn.temp *= 1.3
+                    sim.upload(dyn)
+                sim.compute_hyperbolic_dt()
+                sim.reset_status()
+                done, _ = sim.time_loop(3)
+                assert done == 3
+                sim.download(hg)
+                stats[perturb, guess] = sim.status()
+            out[perturb, guess] = hg
+    for perturb in (False, True):
+        s = stats[perturb, "mlp_rescue"]
+        assert s["nonfinite"] == 0 and s["newton_nonconverged"] == 0 and s["tensor_core_stalls"] == 0
+        assert s["newton_calls"] == 9 * n  # 3 steps x 3 stages, one inversion per cell
+    # steady step: nothing queued, identical to the warm start
+    s = stats[False, "mlp_rescue"]
+    assert s["mlp_accepted"] + s["mlp_rejected"] == 0, s
+    assert max_abs_diff(out[False, "mlp_rescue"], out[False, "warm"]) == 0.0
+    # poor warm start: the first stage goes through the network, the answer is unchanged
+    s, w = stats[True, "mlp_rescue"], stats[True, "warm"]
+    rescued = s["mlp_accepted"] + s["mlp_rejected"]
+    assert rescued >= n, s
+    assert s["mlp_accepted"] >= 0.95 * rescued, s
+    err = field_errors(out[True, "mlp_rescue"], out[True, "warm"])
+    assert max(err[f] for f in ("rho", "p", "e", "T")) <= 1e-9, err
+    assert s["newton_iterations"] < w["newton_iterations"], (s, w)
+
+
+PHL_MLP_NPARAMS = 4 * 64 + 64 + 64 * 64 + 64 + 64 + 1

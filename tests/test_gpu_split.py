@@ -256,3 +256,42 @@ def test_split_constant_acceleration(gpu_lib, table, mhd):
         assert err[f] <= 1e-6, (f, err)
     for f in ("v1", "v3"):
         assert err[f] <= 1e-5, (f, err)
+
+
+# ------------------------------------------------------------------------------ split against the oracle
+def _oracle_run(oracle, cfg, h, nsteps, table):
+    ho = h.copy()
+    helm = oracle.Helm.for_config(cfg, *table) if cfg.helmholtz else None
+    o = oracle.OracleGrid(ho, helm)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(nsteps)
+    return ho
+
+
+# per family: (maker, steps, {field group: limit}); the limits sit a few times above the errors
+# measured on the B200 for these cases
+ORACLE_CASES = {
+    "hot_bubble": (lambda: problems.hot_bubble_2d(48), 20, {"thermo": 1e-9, "v": 1e-6}),
+    "orszag_tang_lhlld": (lambda: problems.orszag_tang_2d(48, riemann="lhlld"), 20, {"thermo": 1e-5, "v": 1e-5, "b": 1e-5}),
+    "stratified": (lambda: problems.stratified_3d(12, ny=16, nz=10), 10, {"thermo": 1e-8, "v": 1e-5}),
+    "stratified_mhd": (lambda: problems.stratified_3d(12, ny=16, nz=10, mhd=True), 10,
+                       {"thermo": 1e-8, "v": 1e-5, "b": 1e-6}),
+}
+
+
+@pytest.mark.parametrize("family", sorted(ORACLE_CASES))
+def test_split_against_oracle(gpu_lib, oracle, table, family):
+    """The split form directly against the CPU oracle (not through the FP64 GPU form)."""
+    maker, nsteps, lim = ORACLE_CASES[family]
+    cfg, h = maker()
+    tab = table if cfg.helmholtz else None
+    ho = _oracle_run(oracle, cfg, h, nsteps, tab)
+    h32, st = run_form(cfg, h, nsteps, tab, "fp32_split")
+    err = field_errors(h32, ho)
+    assert st["nonfinite"] == 0
+    groups = {"thermo": ("rho", "p", "e", "T"), "v": ("v1", "v2", "v3"), "b": ("b1", "b2", "b3")}
+    for grp, limit in lim.items():
+        for f in groups[grp]:
+            if f in err:
+                assert err[f] <= limit, (f, err)
