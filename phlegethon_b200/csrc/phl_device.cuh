@@ -482,6 +482,9 @@ struct HelmTable {
   const double *dpdr;   // dpdrho_table_var(1:4, 1:nrho, 1:nT)
   const double *rho;    // helm_rho(1:nrho)
   const double *T;      // helm_T(1:nT)
+  // reciprocal node spacings 1 / (helm_rho(i+1) - helm_rho(i)), 1 / (helm_T(j+1) - helm_T(j)),
+  // index i-1 / j-1 (the same IEEE quotients a division at the point of use gives)
+  const double *inv_drho, *inv_dT;
   int nrho, nT;
   double drho, dT, log10_rho1, log10_T1;  // log10(helm_rho(1)), log10(helm_T(1)) from the host
   double Tl, Th;

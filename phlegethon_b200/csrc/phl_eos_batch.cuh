@@ -9,6 +9,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 #include "phl_device.cuh"
 #include "phl_mlp.cuh"
@@ -19,6 +20,8 @@
 #endif
 
 namespace phl {
+
+constexpr int EOS_MINB_DEFAULT = 1;
 
 // cold guess; returns the number of EoS evaluations the search used
 __device__ __forceinline__ int bracket_guess(const HelmTable &h, double rho, double e, double abar, double zbar,
@@ -88,8 +91,8 @@ __device__ __forceinline__ void eos_finish(const HelmTable &h, long long t, doub
 // appended to `queue` (queue[0] = count, then index | judged iterations << 56) for phase 2, so
 // that the fallback runs in converged warps instead of stalling the accepted lanes.
 // LEARNED selects the learned-guess instantiation (guess 1); the other carries no tensor-core code.
-template <bool LEARNED>
-__global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, const double *rho, const double *e,
+template <bool LEARNED, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_eos_invert(HelmTable h, long long n, const double *rho, const double *e,
                                                     const double *abar, const double *zbar, double *T,
                                                     double *p, double *cs, int *iters, int guess, MlpWeights mw,
                                                     unsigned long long *stat, unsigned long long *queue) {
@@ -158,7 +161,8 @@ __global__ void __launch_bounds__(128) k_eos_invert(HelmTable h, long long n, co
 
 // Phase 2 of the learned guess: the reference Newton from the bracket guess for the rejected
 // samples (grid-stride over the queue written by phase 1)
-__global__ void __launch_bounds__(128) k_eos_fallback(HelmTable h, const unsigned long long *queue,
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_eos_fallback(HelmTable h, const unsigned long long *queue,
                                                       const double *rho, const double *e, const double *abar,
                                                       const double *zbar, double *T, double *p, double *cs,
                                                       int *iters, unsigned long long *stat) {
@@ -192,23 +196,49 @@ __global__ void __launch_bounds__(128) k_eos_fallback(HelmTable h, const unsigne
 
 // Launch the inversion on stream s (no synchronisation).  `queue` (n + 1 entries) is needed for
 // the learned guess only.  Returns 0 or a cudaError_t.
-inline int eos_launch(const HelmTable &h, cudaStream_t s, long long n, const double *rho, const double *e,
-                      const double *abar, const double *zbar, double *T, double *p, double *cs, int *iters,
-                      int guess, MlpWeights mw, unsigned long long *stat, unsigned long long *queue, int nsm) {
+// Resident blocks per SM the inversion kernels are compiled for: 1 lets the compiler keep the
+// whole inlined evaluation in registers (~180), 3 and 4 cap them (168, 128) at the cost of
+// spills; PHL_EOS_MINB selects one of the three instantiations.
+inline int eos_minb() {
+  static const int v = [] {
+    const char *e = getenv("PHL_EOS_MINB");
+    const int m = e ? atoi(e) : EOS_MINB_DEFAULT;
+    return (m == 1 || m == 3 || m == 4) ? m : EOS_MINB_DEFAULT;
+  }();
+  return v;
+}
+
+template <int MINB>
+inline int eos_launch_t(const HelmTable &h, cudaStream_t s, long long n, const double *rho, const double *e,
+                        const double *abar, const double *zbar, double *T, double *p, double *cs, int *iters,
+                        int guess, MlpWeights mw, unsigned long long *stat, unsigned long long *queue, int nsm) {
   const unsigned blocks = (unsigned)((n + 127) / 128);
   if (guess != PHL_GUESS_MLP) {
-    k_eos_invert<false><<<blocks, 128, 0, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, nullptr);
+    k_eos_invert<false, MINB><<<blocks, 128, 0, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat,
+                                                      nullptr);
     return (int)cudaGetLastError();
   }
   const size_t sm = sizeof(MlpUmmaSmem);
-  cudaError_t err = cudaFuncSetAttribute(k_eos_invert<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t err = cudaFuncSetAttribute(k_eos_invert<true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
   if (err != cudaSuccess) return (int)err;
-  k_eos_invert<true><<<blocks, 128, sm, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue);
+  k_eos_invert<true, MINB><<<blocks, 128, sm, s>>>(h, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue);
   // enough resident blocks to cover every SM several times; the loop covers any queue length
   const unsigned fb = (unsigned)std::min<long long>((long long)nsm * 8, (long long)blocks);
-  k_eos_fallback<<<fb, 128, 0, s>>>(h, queue, rho, e, abar, zbar, T, p, cs, iters, stat);
+  k_eos_fallback<MINB><<<fb, 128, 0, s>>>(h, queue, rho, e, abar, zbar, T, p, cs, iters, stat);
   return (int)cudaGetLastError();
+}
+
+// Launch the inversion on stream s (no synchronisation).  `queue` (n + 1 entries) is needed for
+// the learned guess only.  Returns 0 or a cudaError_t.
+inline int eos_launch(const HelmTable &h, cudaStream_t s, long long n, const double *rho, const double *e,
+                      const double *abar, const double *zbar, double *T, double *p, double *cs, int *iters,
+                      int guess, MlpWeights mw, unsigned long long *stat, unsigned long long *queue, int nsm) {
+  switch (eos_minb()) {
+    case 3: return eos_launch_t<3>(h, s, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue, nsm);
+    case 4: return eos_launch_t<4>(h, s, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue, nsm);
+    default: return eos_launch_t<1>(h, s, n, rho, e, abar, zbar, T, p, cs, iters, guess, mw, stat, queue, nsm);
+  }
 }
 
 struct EosBatch {

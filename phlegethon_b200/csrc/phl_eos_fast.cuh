@@ -62,7 +62,7 @@ __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell 
   c.jh = jh;
   c.T0 = __ldg(h.T + jh - 1);
   c.dT = __ldg(h.T + jh) - c.T0;
-  c.idT = 1.0 / c.dT;
+  c.idT = __ldg(h.inv_dT + jh - 1);
   double r0[3], r1[3];
   helm_cell_rbasis(c, r0, r1);
   helm_cell_contract_with(h, c, jh, r0, r1, c.A);
@@ -75,7 +75,7 @@ __device__ __forceinline__ void helm_cell_init_rho(const HelmTable &h, HelmCell 
   c.ih = helm_node_index(h.rho, h.nrho, h.log10_rho1, h.drho, c.rhos);
   double r_lo = __ldg(h.rho + c.ih - 1);
   c.drho = __ldg(h.rho + c.ih) - r_lo;
-  c.x = (c.rhos - r_lo) * (1.0 / c.drho);
+  c.x = (c.rhos - r_lo) * __ldg(h.inv_drho + c.ih - 1);
 }
 
 __device__ __forceinline__ void helm_cell_init(const HelmTable &h, HelmCell &c, double rho, double abar,
@@ -179,7 +179,7 @@ __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const Hel
   // d/drho contraction of the final cell
   double B[3][2];
   {
-    const double idrho = 1.0 / c.drho;
+    const double idrho = __ldg(h.inv_drho + c.ih - 1);
     double dr0[3], dr1[3];
     hb1(c.x, idrho, c.drho, dr0);
     hb1m(1.0 - c.x, idrho, c.drho, dr1);

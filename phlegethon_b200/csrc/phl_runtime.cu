@@ -228,7 +228,7 @@ struct phl_ctx {
   long long *step = nullptr;
   unsigned long long *stat = nullptr;
   // table
-  double *htab = nullptr, *hdpd = nullptr, *hrho = nullptr, *hT = nullptr;
+  double *htab = nullptr, *hdpd = nullptr, *hrho = nullptr, *hT = nullptr, *hirho = nullptr, *hiT = nullptr;
   HelmTable helm{};
   bool table_loaded = false, uploaded = false, bg_uploaded = false;
   // host copy of the network's FP32 layers 1 and 3 (argument of the learned cons->prim kernel)
@@ -686,6 +686,8 @@ int phl_load_helm_table(phl_ctx *ctx, const double *tab, const double *dpdr) {
     if ((rc = ctx->alloc(&ctx->hdpd, (size_t)4 * nr * nT))) return rc;
     if ((rc = ctx->alloc(&ctx->hrho, (size_t)nr))) return rc;
     if ((rc = ctx->alloc(&ctx->hT, (size_t)nT))) return rc;
+    if ((rc = ctx->alloc(&ctx->hirho, (size_t)nr))) return rc;
+    if ((rc = ctx->alloc(&ctx->hiT, (size_t)nT))) return rc;
   }
   // nodes as load_helm_table builds them (source.F90:23091-23104)
   double dT = (c.helm_lthi - c.helm_ltlo) / (double)(nT - 1);
@@ -693,13 +695,19 @@ int phl_load_helm_table(phl_ctx *ctx, const double *tab, const double *dpdr) {
   std::vector<double> T(nT), rho(nr);
   for (int j = 0; j < nT; ++j) T[j] = std::pow(10.0, c.helm_ltlo + (double)j * dT);
   for (int i = 0; i < nr; ++i) rho[i] = std::pow(10.0, c.helm_ldlo + (double)i * drho);
+  std::vector<double> irho(nr, 0.0), iT(nT, 0.0);
+  for (int i = 0; i + 1 < nr; ++i) irho[i] = 1.0 / (rho[i + 1] - rho[i]);
+  for (int j = 0; j + 1 < nT; ++j) iT[j] = 1.0 / (T[j + 1] - T[j]);
   CK(cudaMemcpyAsync(ctx->htab, tab, sizeof(double) * 9 * nr * nT, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->hdpd, dpdr, sizeof(double) * 4 * nr * nT, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->hrho, rho.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->hT, T.data(), sizeof(double) * nT, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hirho, irho.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hiT, iT.data(), sizeof(double) * nT, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   HelmTable &h = ctx->helm;
   h.tab = ctx->htab; h.dpdr = ctx->hdpd; h.rho = ctx->hrho; h.T = ctx->hT;
+  h.inv_drho = ctx->hirho; h.inv_dT = ctx->hiT;
   h.nrho = nr; h.nT = nT; h.drho = drho; h.dT = dT;
   h.log10_rho1 = std::log10(rho[0]);
   h.log10_T1 = std::log10(T[0]);

@@ -1190,14 +1190,11 @@ __device__ __forceinline__ void store_face_emf_split(const Prm &P, int d, long l
 // P.fflux[d] ([NV][faces]), the face EMF and the CT sign to their arrays
 // (one instantiation per direction D: index strides and rotations fold into constants)
 template <class C, int D>
-__global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
+__device__ __forceinline__ void face_split_mhd_at(const Prm &P, long long f) {
   constexpr int d = D;
-  if (!*P.active) return;
   constexpr int NV = C::NV;
   const Geo &g = P.g;
   const long long nf = nfaces(g, d);
-  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nf) return;
   const int n0 = g.nx[0] + (d == 0), n1 = g.nx[1] + (d == 1);
   int fi, fj, fk;
   unflatten3(f, n0, n1, fi, fj, fk);
@@ -1234,6 +1231,14 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) P.fflux[d][(long long)iv * nf + f] = F[iv];
   store_face_emf_split<C>(P, d, f, d == 0 ? fi : (d == 1 ? fj : fk), Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
+}
+
+template <class C, int D>
+__global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
+  if (!*P.active) return;
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nfaces(P.g, D)) return;
+  face_split_mhd_at<C, D>(P, f);
 }
 
 // faces per thread of the walking face kernels: along x (threads of a warp step K0 cells apart,
@@ -1353,6 +1358,174 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_fa
     }
     fprev = fb;
   }
+}
+
+// MHD stage, part 1 for LIM2ND on grids that the direction's face tile divides: faces along D
+// from tiles of cells staged in shared memory.  Tile (TX, TY, TZ) cells, one face per thread (the
+// face below each cell along D).  Bulk tensor copies (TMA) stage the tile with two extra layers
+// on either side along D (x1: four, so that the copy starts on a 16-byte boundary) of W', the
+// cell B and the two gamma slots; layers outside the domain arrive zero-filled and the ghost
+// layers the stencils need are then written by their threads with the ghost mapping and
+// mirroring of load_wf.  Each thread forms the LIM2ND edges of its cell once into shared memory
+// (the first TT threads also those of the layer below the tile), then solves its face and stores
+// flux, face EMF and CT sign with coalesced stores.  The faces at the upper domain boundary along
+// D are solved by tail blocks of the same launch.  Faces, arithmetic and the solver are those of
+// the walking kernels, which carry the same edges in registers (80 per thread, with spills) and,
+// along x1, stride 4 cells per thread.
+template <int D> struct FaceTile;
+template <> struct FaceTile<0> { static constexpr int TX = 128, TY = 1, TZ = 1, MINB = 8; };
+template <> struct FaceTile<1> { static constexpr int TX = 32, TY = 8, TZ = 1, MINB = 4; };
+template <> struct FaceTile<2> { static constexpr int TX = 32, TY = 1, TZ = 8, MINB = 4; };
+
+template <class C, int D>
+struct FaceTileSmem {
+  using T = FaceTile<D>;
+  static constexpr int NT = T::TX * T::TY * T::TZ;                  // threads = faces per tile
+  static constexpr int TD = D == 0 ? T::TX : (D == 1 ? T::TY : T::TZ);
+  static constexpr int TT = NT / TD;                                // columns along D
+  static constexpr int OX = D == 0 ? 4 : 0, OY = D == 1 ? 2 : 0, OZ = D == 2 ? 2 : 0;
+  static constexpr int SX = T::TX + 2 * OX, SY = T::TY + 2 * OY, SZ = T::TZ + 2 * OZ;
+  static constexpr int SC = SX * SY * SZ;                           // staged cells per variable
+  static constexpr int SD = D == 0 ? 1 : (D == 1 ? SX : SX * SY);   // staged stride along D
+  static constexpr int NE = C::NV + 5;                              // W', B (3), gamma slots (2)
+  static constexpr int RW = ((C::NV * SC + 31) / 32) * 32;          // region sizes in floats,
+  static constexpr int RB = ((3 * SC + 31) / 32) * 32;              // multiples of 128 bytes
+  static constexpr int RG = ((2 * SC + 31) / 32) * 32;
+  static constexpr int NEDGE = (TD + 1) * TT;                       // edge slots: layers -1 .. TD-1
+  static constexpr bool STAGE_G = C::HELM;                          // gammas (FASTEOS) or T (without)
+  static constexpr uint32_t BYTES = 4u * SC * (C::NV + 3 + (STAGE_G ? 2 : 0));
+  float w[RW], b[RB], gm[RG];
+  float lo[NE * NEDGE], hi[NE * NEDGE];
+  uint64_t mbar;
+};
+struct FaceTileMaps {
+  CUtensorMap w, b, g;
+};
+
+template <class C, int D>
+__global__ void __launch_bounds__(FaceTileSmem<C, D>::NT, FaceTile<D>::MINB)
+    k_face_split_mhd_tile(Prm P, const __grid_constant__ FaceTileMaps maps, int ntiles) {
+  static_assert(C::REC == REC_LIM2ND && !C::SF, "tiled faces carry LIM2ND edges without flattening");
+  if (!*P.active) return;
+  using S_ = FaceTileSmem<C, D>;
+  using T = FaceTile<D>;
+  constexpr int NV = C::NV, NE = S_::NE, NED = S_::NEDGE, TT = S_::TT, SX = S_::SX, SY = S_::SY, SC = S_::SC;
+  const Geo &g = P.g;
+  const int t = threadIdx.x;
+  if ((int)blockIdx.x >= ntiles) {
+    // tail: the faces at the upper domain boundary along D, one per thread
+    const long long q = (long long)(blockIdx.x - ntiles) * S_::NT + t;
+    const int e0 = D == 0 ? g.nx[1] : g.nx[0], e1 = D == 2 ? g.nx[1] : (C::DIM == 3 ? g.nx[2] : 1);
+    if (q >= (long long)e0 * e1) return;
+    const int a = (int)(q % e0), c = (int)(q / e0);
+    const int fi = D == 0 ? g.nx[0] : a, fj = D == 0 ? a : (D == 1 ? g.nx[1] : c), fk = D == 2 ? g.nx[2] : c;
+    face_split_mhd_at<C, D>(P, face_lin(g, D, fi, fj, fk));
+    return;
+  }
+  __shared__ __align__(128) S_ S;
+  const int nbx = g.nx[0] / T::TX, nby = g.nx[1] / T::TY;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
+  const int i0 = bx * T::TX, j0 = by * T::TY, k0 = bz * T::TZ;
+  const int tx = t % T::TX, ty = (t / T::TX) % T::TY, tz = t / (T::TX * T::TY);
+  const int td = D == 0 ? tx : (D == 1 ? ty : tz);
+  const int col = D == 0 ? ty + T::TY * tz : (D == 1 ? tx + T::TX * tz : tx + T::TX * ty);  // < TT
+  const int c0 = D == 0 ? i0 : (D == 1 ? j0 : k0), nD = g.nx[D];
+  if (t == 0) mbar_init(&S.mbar, 1);
+  __syncthreads();
+  if (t == 0) {
+    mbar_arrive_expect_tx(&S.mbar, S_::BYTES);
+    tma_load_4d(S.w, &maps.w, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
+    tma_load_4d(S.b, &maps.b, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
+    if (S_::STAGE_G) tma_load_4d(S.gm, &maps.g, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
+  }
+  if (!mbar_wait_bounded(&S.mbar, 0, SPLIT_TMA_POLLS)) {
+    // the copy did not land in time: report it and give it a second bounded chance to finish
+    // before shared memory is read or released; this tile's faces are then not trustworthy
+    if (t == 0) atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
+    mbar_wait_bounded(&S.mbar, 0, SPLIT_TMA_POLLS);
+  }
+  // staged position of tile cell (x, y, z) relative to the tile origin
+  auto spos = [&](int x, int y, int z) { return (x + S_::OX) + SX * ((y + S_::OY) + SY * (z + S_::OZ)); };
+  // tile coordinates of column `cl` at layer `l` along D
+  auto cell_of = [&](int cl, int l, int &x, int &y, int &z) {
+    if (D == 0) { x = l; y = cl % T::TY; z = cl / T::TY; }
+    else if (D == 1) { x = cl % T::TX; y = l; z = cl / T::TX; }
+    else { x = cl % T::TX; y = cl / T::TX; z = l; }
+  };
+  // ghost layers -2, -1 (tile at the lower domain boundary) and nD, nD + 1 (upper) along D
+  if (t < 4 * TT) {
+    const int side = t / (2 * TT), layer = (t / TT) % 2, cl = t % TT;
+    const int l = side == 0 ? layer - 2 : S_::TD + layer;
+    if ((side == 0 && c0 == 0) || (side == 1 && c0 + S_::TD == nD)) {
+      int x, y, z;
+      cell_of(cl, l, x, y, z);
+      float wv[NV], gv[2] = {0.0f, 0.0f}, bv[3];
+      load_wf<C>(P, i0 + x, j0 + y, k0 + z, wv, gv);
+      load_bccf<C>(P, i0 + x, j0 + y, k0 + z, bv);
+      const int pos = spos(x, y, z);
+#pragma unroll
+      for (int iv = 0; iv < NV; ++iv) S.w[iv * SC + pos] = wv[iv];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) S.b[a * SC + pos] = bv[a];
+      S.gm[pos] = gv[0];
+      S.gm[SC + pos] = gv[1];
+    }
+  }
+  __syncthreads();
+  // LIM2ND edges of the cell at layer l of column cl into edge slot (l + 1) * TT + cl
+  auto edges = [&](int cl, int l) {
+    int x, y, z;
+    cell_of(cl, l, x, y, z);
+    const int pos = spos(x, y, z), slot = (l + 1) * TT + cl;
+#pragma unroll
+    for (int v = 0; v < NE; ++v) {
+      const float *src = v < NV ? S.w + v * SC : (v < NV + 3 ? S.b + (v - NV) * SC : S.gm + (v - NV - 3) * SC);
+      float lo, hi;
+      plm_f32(src[pos - S_::SD], src[pos], src[pos + S_::SD], lo, hi);
+      S.lo[v * NED + slot] = lo;
+      S.hi[v * NED + slot] = hi;
+    }
+  };
+  edges(col, td);
+  if (t < TT) edges(t, -1);
+  __syncthreads();
+  // the face below the own cell along D: edges of layers td - 1 (slot td * TT + col) and td
+  const int sL = td * TT + col, sR = sL + TT;
+  float qL[NV], qR[NV], bL[3] = {0.f, 0.f, 0.f}, bR[3] = {0.f, 0.f, 0.f}, gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    qL[iv] = S.hi[iv * NED + sL];
+    qR[iv] = S.lo[iv * NED + sR];
+  }
+#pragma unroll
+  for (int a = 0; a < C::DIM; ++a) {
+    if (a == D) continue;
+    bL[a] = S.hi[(NV + a) * NED + sL];
+    bR[a] = S.lo[(NV + a) * NED + sR];
+  }
+  const int fi = i0 + tx, fj = j0 + ty, fk = k0 + tz;
+  const long long fidx = face_lin(g, D, fi, fj, fk);
+  long long fbg = 0;
+  if (C::WB || C::ETOT) fbg = g.bg_profile ? (long long)fj : fidx;
+  float tface = 0.0f;
+  if (C::FAST) {
+    gL[0] = S.hi[(NV + 3) * NED + sL]; gL[1] = S.hi[(NV + 4) * NED + sL];
+    gR[0] = S.lo[(NV + 3) * NED + sR]; gR[1] = S.lo[(NV + 4) * NED + sR];
+    if (C::WB) {
+      const float ge = __ldg(P.sf_ge_f[D] + fbg);
+      gL[0] = gL[0] + ge;
+      gR[0] = gR[0] + ge;
+    }
+  } else if (C::HELM) {
+    const int pos = spos(tx, ty, tz);
+    tface = 0.5f * (S.gm[pos - S_::SD] + S.gm[pos]);
+  }
+  float F[NV], Fb[3], rs;
+  face_solve_split_mhd<C>(P, D, fidx, fbg, qL, qR, bL, bR, gL, gR, tface, false, F, Fb, rs);
+  const long long nf = nfaces(g, D);
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) P.fflux[D][(long long)iv * nf + fidx] = F[iv];
+  store_face_emf_split<C>(P, D, fidx, c0 + td, Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
 }
 
 // FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
@@ -1978,18 +2151,21 @@ PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
   return fn;
 }
 
-// 4D map (x1, x2, x3, variable) over an FP32 SoA field block, box = (bx, by, 1, nvar)
-bool encode_plane_map(CUtensorMap *m, const float *base, int nvar, const Geo &g, int bx, int by) {
+// 4D map (x1, x2, x3, variable) over an FP32 SoA field block, box = (bx, by, bz, nvar)
+bool encode_box_map(CUtensorMap *m, const float *base, int nvar, const Geo &g, int bx, int by, int bz) {
   PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
   if (!enc || !base) return false;
   const cuuint64_t nx = (cuuint64_t)g.nx[0], ny = (cuuint64_t)g.nx[1], nz = (cuuint64_t)g.nx[2];
   const cuuint64_t dims[4] = {nx, ny, nz, (cuuint64_t)nvar};
   const cuuint64_t strides[3] = {nx * 4, nx * ny * 4, (cuuint64_t)g.N * 4};
-  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)nvar};
+  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, (cuuint32_t)nvar};
   const cuuint32_t es[4] = {1, 1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides, box, es,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+bool encode_plane_map(CUtensorMap *m, const float *base, int nvar, const Geo &g, int bx, int by) {
+  return encode_box_map(m, base, nvar, g, bx, by, 1);
 }
 }
 
@@ -2020,6 +2196,55 @@ struct SplitRunnerT : Runner {
     if (e.ok && C::HELM) e.ok = encode_plane_map(&e.maps.g, P.gf_in, 2, g, T::SX, T::SY);
     out = e.maps;
     return e.ok;
+  }
+  // tensor maps of the tiled face kernels, per direction and stage input (W' and the gammas
+  // alternate with the stage)
+  struct TileMapEntry {
+    const float *w = nullptr;
+    FaceTileMaps maps;
+    bool ok = false;
+  } tile_cache[3][2];
+  template <int D>
+  bool tile_maps(const Prm &P, FaceTileMaps &out) {
+    using S_ = FaceTileSmem<C, D>;
+    for (auto &e : tile_cache[D])
+      if (e.w == P.Wf_in) {
+        out = e.maps;
+        return e.ok;
+      }
+    TileMapEntry &e = tile_cache[D][tile_cache[D][0].w ? 1 : 0];
+    e.w = P.Wf_in;
+    e.ok = encode_box_map(&e.maps.w, P.Wf_in, C::NV, P.g, S_::SX, S_::SY, S_::SZ) &&
+           encode_box_map(&e.maps.b, P.bccf, 3, P.g, S_::SX, S_::SY, S_::SZ);
+    if (e.ok && C::HELM) e.ok = encode_box_map(&e.maps.g, P.gf_in, 2, P.g, S_::SX, S_::SY, S_::SZ);
+    out = e.maps;
+    return e.ok;
+  }
+  // PHL_FACE_KERNEL=walk keeps the walking face kernels on every grid (comparison of the two)
+  const bool allow_face_tiles = [] {
+    const char *e = getenv("PHL_FACE_KERNEL");
+    return !(e && strcmp(e, "walk") == 0);
+  }();
+  // faces along D from shared-memory tiles, when the grid is a multiple of the tile; false to
+  // fall back to the walking kernel
+  template <int D>
+  bool launch_face_tiles(const Prm &P, cudaStream_t s) {
+    if constexpr (C::SF || C::REC != REC_LIM2ND) {
+      return false;
+    } else {
+      using T = FaceTile<D>;
+      using S_ = FaceTileSmem<C, D>;
+      const Geo &g = P.g;
+      const int nz = C::DIM == 3 ? g.nx[2] : 1;
+      if (!allow_face_tiles || g.nx[0] % T::TX || g.nx[1] % T::TY || nz % T::TZ) return false;
+      FaceTileMaps m;
+      if (!tile_maps<D>(P, m)) return false;
+      const long long ntiles = (long long)(g.nx[0] / T::TX) * (g.nx[1] / T::TY) * (nz / T::TZ);
+      const long long ntail = (long long)(D == 0 ? g.nx[1] : g.nx[0]) * (D == 2 ? g.nx[1] : nz);
+      const long long nb = ntiles + (ntail + S_::NT - 1) / S_::NT;
+      k_face_split_mhd_tile<C, D><<<(unsigned)nb, S_::NT, 0, s>>>(P, m, (int)ntiles);
+      return true;
+    }
   }
   // PHL_STAGE_KERNEL=cell selects the per-cell kernel on any grid, =tiled_cpasync the tiled
   // kernel with cell-by-cell copies only (comparisons of the three)
@@ -2055,9 +2280,13 @@ struct SplitRunnerT : Runner {
             if (a != d) n *= g.nx[a];
           return n;
         };
-        k_face_split_mhd_walk<C, 0, WALK_K0><<<nblk(nwalk(0, WALK_K0), 128), 128, 0, s>>>(P);
-        k_face_split_mhd_walk<C, 1, WALK_K><<<nblk(nwalk(1, WALK_K), 128), 128, 0, s>>>(P);
-        if constexpr (C::DIM == 3) k_face_split_mhd_walk<C, 2, WALK_K><<<nblk(nwalk(2, WALK_K), 128), 128, 0, s>>>(P);
+        if (!launch_face_tiles<0>(P, s))
+          k_face_split_mhd_walk<C, 0, WALK_K0><<<nblk(nwalk(0, WALK_K0), 128), 128, 0, s>>>(P);
+        if (!launch_face_tiles<1>(P, s))
+          k_face_split_mhd_walk<C, 1, WALK_K><<<nblk(nwalk(1, WALK_K), 128), 128, 0, s>>>(P);
+        if constexpr (C::DIM == 3)
+          if (!launch_face_tiles<2>(P, s))
+            k_face_split_mhd_walk<C, 2, WALK_K><<<nblk(nwalk(2, WALK_K), 128), 128, 0, s>>>(P);
       } else {
         k_face_split_mhd<C, 0><<<nblk(nfc(0), 128), 128, 0, s>>>(P);
         k_face_split_mhd<C, 1><<<nblk(nfc(1), 128), 128, 0, s>>>(P);

@@ -2,8 +2,9 @@
 
 The split form keeps the conserved state in FP64 and computes fluxes in FP32 on well-balanced
 deviations, so its results are not bitwise equal to FP64; the bar is the per-field relative L1
-error the split form is built for (density <= 1e-5 after 1000 steps of the 256^3 box), checked
-here on short runs of small boxes with proportionally tighter limits.
+error the split form is built for (density <= 1e-5 after 1000 steps of the 256^3 box).  The
+limits here sit 5-20x above the errors measured on the B200 for each case (FP32 rounding moves
+with code generation; a real regression moves them by orders of magnitude).
 """
 import numpy as np
 import pytest
@@ -36,11 +37,14 @@ def test_split_stratified_helmholtz(gpu_lib, oracle, table, riemann):
     h32, st = run_form(cfg, h, 40, table, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
-    assert err["rho"] <= 1e-6, err
-    assert err["p"] <= 1e-6, err
-    assert err["T"] <= 1e-6, err
+    # measured after 40 steps: LHLLC rho 2e-10, T 5e-10, v <= 1.8e-7; HLLC (dissipative at
+    # Mach 1e-3, see MHD_LIMITS) rho 1.3e-7, T 3.2e-7, v <= 1.2e-4
+    thermo, vlim = (1e-8, 1e-6) if riemann == "lhllc" else (1e-6, 5e-4)
+    assert err["rho"] <= thermo, err
+    assert err["p"] <= thermo, err
+    assert err["T"] <= thermo, err
     for d in (1, 2, 3):
-        assert err["v%d" % d] <= 2e-3, err
+        assert err["v%d" % d] <= vlim, err
 
 
 def test_split_hot_bubble(gpu_lib, oracle):
@@ -48,9 +52,10 @@ def test_split_hot_bubble(gpu_lib, oracle):
     h64, _ = run_form(cfg, h, 60, None, "fp64")
     h32, _ = run_form(cfg, h, 60, None, "fp32_split")
     err = field_errors(h32, h64)
-    assert err["rho"] <= 1e-6, err
-    assert err["p"] <= 1e-6, err
-    assert err["v2"] <= 1e-3, err
+    # measured after 60 steps: rho 1.9e-10, p 1e-10, v <= 8.6e-8
+    assert err["rho"] <= 1e-8, err
+    assert err["p"] <= 1e-8, err
+    assert err["v1"] <= 1e-6 and err["v2"] <= 1e-6, err
 
 
 def test_split_keeps_hydrostatic_balance(gpu_lib, table):
@@ -107,16 +112,17 @@ def test_split_orszag_tang(gpu_lib, riemann):
     h32, st = run_form(cfg, h, 30, None, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0
-    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
-        assert err[f] <= lim, (f, err)
+    # measured <= 1e-7 in every field (Orszag-Tang variants, 30 steps)
+    for f in ("rho", "p", "e", "v1", "v2", "b1", "b2"):
+        assert err[f] <= 5e-7, (f, err)
     assert div_b_max(h32) <= 1e-13
 
 
 # LHLLD (the low-dissipation solver the low-Mach box is run with) keeps FP32 rounding-level
 # errors; HLLD's dissipative flux f + s (U* - U) cancels O(Mach) differences of O(1) states, so
 # its FP32 velocity and induction fluxes carry relative errors ~ eps / Mach
-MHD_LIMITS = {"lhlld": {"thermo": 1e-8, "v": 1e-5, "b": 1e-6},
-              "hlld": {"thermo": 1e-6, "v": 2e-3, "b": 1e-3}}
+MHD_LIMITS = {"lhlld": {"thermo": 1e-8, "v": 1e-6, "b": 1e-6},   # measured 3.6e-10, 1.2e-7, 5.7e-8
+              "hlld": {"thermo": 1e-6, "v": 5e-4, "b": 1e-3}}    # measured 2.9e-7, 1.1e-4, 2e-4
 
 
 @pytest.mark.parametrize("riemann", ["lhlld", "hlld"])
@@ -147,10 +153,11 @@ def test_split_helmholtz_without_fasteos(gpu_lib, table, mhd, riemann):
         h32, st = run_form(cfg, h, 20, table, "fp32_split")
         err = field_errors(h32, h64)
         assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+        # measured: rho, p, e, T <= 2.3e-10, v <= 8.5e-8
         for f in ("rho", "p", "e", "T"):
             assert err[f] <= 1e-8, (f, err)
         for f in ("v1", "v2", "v3"):
-            assert err[f] <= 1e-5, (f, err)
+            assert err[f] <= 1e-6, (f, err)
 
 
 def test_split_orszag_tang_lim5th(gpu_lib):
@@ -160,8 +167,9 @@ def test_split_orszag_tang_lim5th(gpu_lib):
     h32, st = run_form(cfg, h, 30, None, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0
-    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
-        assert err[f] <= lim, (f, err)
+    # measured <= 1e-7 in every field (Orszag-Tang variants, 30 steps)
+    for f in ("rho", "p", "e", "v1", "v2", "b1", "b2"):
+        assert err[f] <= 5e-7, (f, err)
     assert div_b_max(h32) <= 1e-13
 
 
@@ -174,10 +182,11 @@ def test_split_stratified_higher_order(gpu_lib, table, mhd, riemann, rec, dims):
     h32, st = run_form(cfg, h, 20, table, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    # measured: thermodynamic fields <= 3.4e-10, v <= 1.1e-7
     for f in ("rho", "p", "e", "T"):
         assert err[f] <= 1e-8, (f, err)
     for f in ("v1", "v2", "v3"):
-        assert err[f] <= 1e-5, (f, err)
+        assert err[f] <= 1e-6, (f, err)
 
 
 @pytest.mark.parametrize("mhd,riemann", [(False, "lhllc"), (True, "lhlld")])
@@ -191,7 +200,7 @@ def test_split_on_fermi_table(gpu_lib, mhd, riemann):
     h32, st = run_form(cfg, h, 20, table, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
-    assert err["rho"] <= 1e-6 and err["p"] <= 1e-6 and err["T"] <= 1e-6, err
+    assert err["rho"] <= 1e-8 and err["p"] <= 1e-8 and err["T"] <= 1e-8, err  # measured <= 2.8e-10
 
 
 # ------------------------------------------------------------------------------ USE_SHOCK_FLATTENING
@@ -203,7 +212,7 @@ def test_split_blast_shock_flattening(gpu_lib):
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0
     for f in ("rho", "p", "e"):
-        assert err[f] <= 1e-5, (f, err)
+        assert err[f] <= 5e-7, (f, err)  # measured rho 3.4e-9, p and e 4.1e-8
 
 
 def test_split_orszag_tang_shock_flattening(gpu_lib):
@@ -213,8 +222,9 @@ def test_split_orszag_tang_shock_flattening(gpu_lib):
     h32, st = run_form(cfg, h, 30, None, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0
-    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
-        assert err[f] <= lim, (f, err)
+    # measured <= 1e-7 in every field (Orszag-Tang variants, 30 steps)
+    for f in ("rho", "p", "e", "v1", "v2", "b1", "b2"):
+        assert err[f] <= 5e-7, (f, err)
     assert div_b_max(h32) <= 1e-13
 
 
@@ -228,7 +238,7 @@ def test_split_stratified_shock_flattening(gpu_lib, table, mhd, rec):
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
     for f in ("rho", "p", "e", "T"):
-        assert err[f] <= 1e-6, (f, err)
+        assert err[f] <= 2e-7, (f, err)  # measured <= 2.6e-8
 
 
 def test_split_all_mach_orszag_tang(gpu_lib):
@@ -239,8 +249,9 @@ def test_split_all_mach_orszag_tang(gpu_lib):
     h32, st = run_form(cfg, h, 30, None, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0
-    for f, lim in (("rho", 1e-5), ("p", 1e-5), ("e", 1e-5), ("v1", 1e-4), ("v2", 1e-4), ("b1", 1e-4), ("b2", 1e-4)):
-        assert err[f] <= lim, (f, err)
+    # measured <= 1e-7 in every field (Orszag-Tang variants, 30 steps)
+    for f in ("rho", "p", "e", "v1", "v2", "b1", "b2"):
+        assert err[f] <= 5e-7, (f, err)
 
 
 @pytest.mark.parametrize("mhd", [False, True])
@@ -252,10 +263,11 @@ def test_split_constant_acceleration(gpu_lib, table, mhd):
     h32, st = run_form(cfg, h, 20, table, "fp32_split")
     err = field_errors(h32, h64)
     assert st["nonfinite"] == 0 and st["newton_nonconverged"] == 0
+    # measured: thermodynamic fields <= 3e-10, v <= 1e-7
     for f in ("rho", "p", "e", "T"):
-        assert err[f] <= 1e-6, (f, err)
+        assert err[f] <= 1e-8, (f, err)
     for f in ("v1", "v3"):
-        assert err[f] <= 1e-5, (f, err)
+        assert err[f] <= 1e-6, (f, err)
 
 
 # ------------------------------------------------------------------------------ split against the oracle
@@ -273,10 +285,10 @@ def _oracle_run(oracle, cfg, h, nsteps, table):
 # measured on the B200 for these cases
 ORACLE_CASES = {
     "hot_bubble": (lambda: problems.hot_bubble_2d(48), 20, {"thermo": 1e-9, "v": 1e-6}),
-    "orszag_tang_lhlld": (lambda: problems.orszag_tang_2d(48, riemann="lhlld"), 20, {"thermo": 1e-5, "v": 1e-5, "b": 1e-5}),
-    "stratified": (lambda: problems.stratified_3d(12, ny=16, nz=10), 10, {"thermo": 1e-8, "v": 1e-5}),
+    "orszag_tang_lhlld": (lambda: problems.orszag_tang_2d(48, riemann="lhlld"), 20, {"thermo": 5e-7, "v": 5e-7, "b": 5e-7}),
+    "stratified": (lambda: problems.stratified_3d(12, ny=16, nz=10), 10, {"thermo": 1e-8, "v": 5e-7}),
     "stratified_mhd": (lambda: problems.stratified_3d(12, ny=16, nz=10, mhd=True), 10,
-                       {"thermo": 1e-8, "v": 1e-5, "b": 1e-6}),
+                       {"thermo": 1e-8, "v": 5e-7, "b": 1e-6}),
 }
 
 
@@ -295,3 +307,30 @@ def test_split_against_oracle(gpu_lib, oracle, table, family):
         for f in groups[grp]:
             if f in err:
                 assert err[f] <= limit, (f, err)
+
+
+@pytest.mark.parametrize("mhd_case", ["stratified_mhd", "orszag_tang"])
+def test_tiled_faces_equal_walking_faces(gpu_lib, table, mhd_case, monkeypatch):
+    """The face kernels that stage tiles in shared memory with bulk tensor copies (grids whose
+    extents are multiples of the tiles) against the walking face kernels: the same edges and the
+    same solver on the same inputs, so both sit at the same FP32 rounding distance from the FP64
+    form and apart by rounding noise only (the compiler contracts the edge arithmetic differently
+    in the two kernels)."""
+    if mhd_case == "stratified_mhd":
+        cfg, h = problems.stratified_3d(128, ny=16, nz=8, mhd=True)
+        tab = table
+    else:
+        cfg, h = problems.orszag_tang_2d(256)
+        tab = None
+    monkeypatch.setenv("PHL_FACE_KERNEL", "walk")
+    ha, sta = run_form(cfg, h, 3, tab, "fp32_split")
+    monkeypatch.setenv("PHL_FACE_KERNEL", "auto")
+    hb, stb = run_form(cfg, h, 3, tab, "fp32_split")
+    h64, _ = run_form(cfg, h, 3, tab, "fp64")
+    assert stb["nonfinite"] == 0 and stb["tensor_core_stalls"] == 0
+    e_w = field_errors(ha, h64)
+    e_t = field_errors(hb, h64)
+    diff = field_errors(hb, ha)
+    for f in e_w:
+        assert e_t[f] <= 1.5 * e_w[f] + 1e-13, (f, e_t, e_w)
+        assert diff[f] <= 2.0 * e_w[f] + 1e-13, (f, diff, e_w)
