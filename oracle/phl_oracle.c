@@ -28,6 +28,22 @@
  * reference's operand order.
  */
 #include <math.h>
+
+/* Iteration counts of the per-face helm_rhoP_given solves of the Riemann sides (Helmholtz without
+ * USE_FASTEOS): how far the reference's face temperature guess 0.5 (T_L + T_R) is from the
+ * answer, measured on the reference's own algorithm.  Test statistics only. */
+static long long g_face_newton_calls = 0, g_face_newton_iters = 0;
+static void face_newton_count(int iters) {
+#pragma omp atomic
+  g_face_newton_calls += 1;
+#pragma omp atomic
+  g_face_newton_iters += iters;
+}
+void phlo_face_newton_stats(long long *calls, long long *iters, int reset) {
+  *calls = g_face_newton_calls;
+  *iters = g_face_newton_iters;
+  if (reset) g_face_newton_calls = g_face_newton_iters = 0;
+}
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -164,7 +180,7 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
   } else if (g->helm) {
     /* helm_rhoP_given from the face temperature guess (source.F90:15705-15720, 15777-15781) */
     double ye = qL[ias], abar = 1.0 / qL[ias + 1], zbar = ye * abar, T = gL[0];
-    phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &cL, 1);
+    face_newton_count(phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &cL, 1));
     eint = eint * rhoL;
   } else {
     eint = igmm1 * pL;
@@ -179,7 +195,7 @@ void phlo_riemann_hydro(const phlo_grid *g, const double *qL, const double *qR,
     cR = sqrt(gR[1] * pR * inv_rhoR);
   } else if (g->helm) {
     double ye = qR[ias], abar = 1.0 / qR[ias + 1], zbar = ye * abar, T = gR[0];
-    phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &cR, 1);
+    face_newton_count(phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &cR, 1));
     eint = eint * rhoR;
   } else {
     eint = igmm1 * pR;
@@ -293,7 +309,7 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
   else if (g->helm) {
     /* helm_rhoP_given from the face temperature guess (source.F90:14266-14275) */
     double ye = qL[ias], abar = 1.0 / qL[ias + 1], zbar = ye * abar, T = gL[0], sound;
-    phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &sound, 1);
+    face_newton_count(phlo_helm_rhoP_given(g->eos, rhoL, pL, abar, zbar, &T, &eint, &sound, 1));
     eint = eint * rhoL;
     c2L = sound * sound;
   }
@@ -306,7 +322,7 @@ void phlo_riemann_mhd(const phlo_grid *g, const double *qL, const double *qR,
   if (g->fasteos) { eint = pR / (gR[0] - 1.0); c2R = gR[1] * pR * inv_rhoR; }
   else if (g->helm) {
     double ye = qR[ias], abar = 1.0 / qR[ias + 1], zbar = ye * abar, T = gR[0], sound;
-    phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &sound, 1);
+    face_newton_count(phlo_helm_rhoP_given(g->eos, rhoR, pR, abar, zbar, &T, &eint, &sound, 1));
     eint = eint * rhoR;
     c2R = sound * sound;
   }

@@ -89,6 +89,8 @@ void phlo_helm_rhoT_given1(const phlo_helm *h, double rho, double T, double abar
 void phlo_helm_rhoT_given2(const phlo_helm *h, double rho, double T, double abar, double zbar,
                            double *E, double *dEdT, int return_dEdT);
 /* Newton inversions; return the iteration count used (<=100). */
+/* per-face helm_rhoP_given calls and iterations since the last reset (test statistics) */
+void phlo_face_newton_stats(long long *calls, long long *iters, int reset);
 int phlo_helm_rhoP_given(const phlo_helm *h, double rho, double P0, double abar, double zbar,
                          double *T, double *E, double *sound, int return_sound);
 int phlo_helm_rhoe_given(const phlo_helm *h, double rho, double E0, double abar, double zbar,

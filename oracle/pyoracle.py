@@ -71,6 +71,8 @@ def load():
         lib.phlo_helm_rhoe_given.argtypes = [C.POINTER(_Helm), C.c_double, C.c_double, C.c_double,
                                              C.c_double, _P, _P, _P, C.c_int]
         lib.phlo_helm_rhoe_given.restype = C.c_int
+        lib.phlo_face_newton_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
+        lib.phlo_face_newton_stats.restype = None
         lib.phlo_helm_rhoP_given.argtypes = [C.POINTER(_Helm), C.c_double, C.c_double, C.c_double,
                                              C.c_double, _P, _P, _P, C.c_int]
         lib.phlo_helm_rhoP_given.restype = C.c_int
@@ -149,6 +151,13 @@ class Helm:
         T, E, s = C.c_double(T0), C.c_double(), C.c_double()
         it = load().phlo_helm_rhoP_given(C.byref(self.s), rho, P0, abar, zbar, C.byref(T), C.byref(E), C.byref(s), 1)
         return T.value, E.value, s.value, it
+
+
+def face_newton_stats(reset=False):
+    """(calls, iterations) of the per-face helm_rhoP_given solves since the last reset."""
+    calls, iters = C.c_longlong(), C.c_longlong()
+    load().phlo_face_newton_stats(C.byref(calls), C.byref(iters), int(reset))
+    return calls.value, iters.value
 
 
 class OracleGrid:

@@ -166,7 +166,8 @@ __device__ __forceinline__ int helm_rhoe_fast(const HelmTable &h, HelmCell &c, d
 // pressure and the square of the relativistic sound speed at (rho, T) from the prepared cell
 // (given_full's output; irho = 1 / rho)
 __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const HelmCell &c, double rho, double irho,
-                                                   double T, double inv_abar, double &P, double &sound2) {
+                                                   double T, double inv_abar, double &P, double &sound2,
+                                                   double *E_out = nullptr) {
   const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
@@ -226,6 +227,78 @@ __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const Hel
   const double num = T * dP_dT * dP_dT / (rho * cv) + rho * dP_drho;
   const double den = P + (E + CONST_C2) * rho;
   sound2 = CONST_C2 * (num / den);
+  if (E_out) *E_out = E;
+}
+
+// Newton on P(rho, T) = P0 from T (helm_rhoP_given's loop and exit rules, source.F90:24943-24980:
+// helm_tol on |P - P0| / P0, at most 100 iterations, an iterate outside the table resets to the
+// start and ends the loop).  The density is fixed, so the d/drho coefficients of the current T
+// cell are contracted once (B, 36 table values); an iteration needs the T basis and 12
+// products for f_rho and f_rhoT: P = (rho Ye)^2 f_rho + ions + radiation and dP/dT alike.  On
+// return `c` holds the value contraction (A) of the final T's cell, for helm_cell_p_sound2.
+__device__ __forceinline__ int helm_rhoP_fast(const HelmTable &h, HelmCell &c, double rho, double P0,
+                                              double inv_abar, double &T, int &clamped) {
+  const double Told = T, inv_P0 = 1.0 / P0, r2 = c.rhos * c.rhos;
+  double B[3][2], dr0[3], dr1[3];
+  {
+    const double idrho = __ldg(h.inv_drho + c.ih - 1);
+    hb1(c.x, idrho, c.drho, dr0);
+    hb1m(1.0 - c.x, idrho, c.drho, dr1);
+  }
+  int jh = -1;
+  double T0 = 0.0, dT = 0.0, idT = 0.0;
+  int used = 0;
+  for (int iter = 1; iter <= 100; ++iter) {
+    used = iter;
+    if (jh < 0 || T < T0 || T >= T0 + dT) {
+      jh = helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T);
+      T0 = __ldg(h.T + jh - 1);
+      dT = __ldg(h.T + jh) - T0;
+      idT = __ldg(h.inv_dT + jh - 1);
+      helm_cell_contract_with(h, c, jh, dr0, dr1, B);
+    }
+    const double y = (T - T0) * idT, omy = 1.0 - y;
+    double t0[3], t1[3], d0[3], d1[3];
+    hb0(y, dT, dT * dT, t0);
+    hb0m(omy, dT, dT * dT, t1);
+    hb1(y, idT, dT, d0);
+    hb1m(omy, idT, dT, d1);
+    double fd = 0.0, fdT = 0.0;
+#pragma unroll
+    for (int ot = 0; ot < 3; ++ot) {
+      fd = fma(B[ot][0], t0[ot], fma(B[ot][1], t1[ot], fd));
+      fdT = fma(B[ot][0], d0[ot], fma(B[ot][1], d1[ot], fdT));
+    }
+    const double T3 = T * T * T;
+    const double P = r2 * fd + CONST_RGAS * rho * T * inv_abar + CONST_RAD * T3 * T * (1.0 / 3.0);
+    const double dP = r2 * fdT + CONST_RGAS * rho * inv_abar + (4.0 / 3.0) * CONST_RAD * T3;
+    const double res = P - P0;
+    T = T - res / dP;
+    double error = fabs(res * inv_P0);
+    if ((T < h.Tl) || (T > h.Th)) {
+      T = Told;
+      error = EM15;
+      ++clamped;
+    }
+    if (error < HELM_TOL) break;
+  }
+  helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
+  return used;
+}
+
+// helm_rhoP_given with return_sound for one Riemann side of the split form: rho * e and the
+// sound speed at (rho, p), from the temperature guess T
+__device__ __forceinline__ void helm_side_eos_fast_inl(const HelmTable &h, double rho, double p, double abar,
+                                                       double zbar, double T, double &rhoe, double &sound) {
+  HelmCell c;
+  const double inv_abar = 1.0 / abar, irho = 1.0 / rho;
+  helm_cell_init_rho(h, c, rho, zbar * inv_abar);
+  int clamped = 0;
+  helm_rhoP_fast(h, c, rho, p, inv_abar, T, clamped);
+  double P, sound2, E;
+  helm_cell_p_sound2(h, c, rho, irho, T, inv_abar, P, sound2, &E);
+  rhoe = E * rho;
+  sound = sqrt(sound2);
 }
 
 }  // namespace phl

@@ -429,7 +429,7 @@ __device__ __forceinline__ long long dir_stride(const Geo &g, int d) {
 // w(s, iv), FASTEOS gamma q is g(s, q).
 template <int NV>
 struct RegCells {
-  const float *w_[4], *g_[4];
+  const float *w_[6], *g_[6];
   __device__ __forceinline__ float w(int s, int iv) const { return w_[s][iv]; }
   __device__ __forceinline__ float g(int s, int q) const { return g_[s][q]; }
 };
@@ -442,11 +442,13 @@ struct SmemCells {
   __device__ __forceinline__ float g(int s, int q) const { return base[off[s] + (NV + q) * vs]; }
 };
 
-// helm_side_eos_inl out of line: the split stage kernels call it twice per face, and an inlined
-// full Helmholtz evaluation at each site costs them their registers
+// the per-side helm_rhoP_given of the split form, out of line: the split stage kernels call it
+// twice per face, and an inlined Helmholtz evaluation at each site costs them their registers.
+// It runs the contracted-coefficient evaluation of phl_eos_fast.cuh (the FP64 form keeps the
+// reference's evaluation order, helm_side_eos_inl); results agree to rounding.
 static __device__ __noinline__ void helm_side_eos(const HelmTable &h, double rho, double p, double abar,
                                                   double zbar, double T, double &rhoe, double &sound) {
-  helm_side_eos_inl(h, rho, p, abar, zbar, T, rhoe, sound);
+  helm_side_eos_fast_inl(h, rho, p, abar, zbar, T, rhoe, sound);
 }
 
 // Helmholtz without USE_FASTEOS, split form: helm_rhoP_given (FP64) for one side of a face from
@@ -521,9 +523,9 @@ __device__ __forceinline__ void flatten_gamma_x1(const float gv[2][6], bool fa, 
 template <class C, class Cells>
 __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int fj, int fk, const Cells &cl,
                                                 float F[C::NV]) {
-  constexpr int NV = C::NV, IP = C::IP;
+  constexpr int NV = C::NV, IP = C::IP, SW = C::SW;
   const Geo &g = P.g;
-  static_assert(C::SW == 2, "cell-accessor faces read two cells per side");
+  // cl holds cells m-SW .. m+SW-1; v[] of rec_face_f32 holds cells m-3 .. m+2
   // USE_SHOCK_FLATTENING: is_flattened of cells m-1 (fa) and m (fb); a flagged cell's edges
   // fall back to LIM2ND PLM, and the face takes the HLL flux
   bool fa = false, fb = false;
@@ -534,8 +536,10 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
   float qL[NV], qR[NV];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv) {
-    const float v[6] = {0.0f, cl.w(0, iv), cl.w(1, iv), cl.w(2, iv), cl.w(3, iv), 0.0f};
-    rec_face_f32<C>(v, iv >= C::IAS, qL[iv], qR[iv]);
+    float v[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] = (q >= 3 - SW && q < 3 + SW) ? cl.w(q - (3 - SW), iv) : 0.0f;
+    rec_face_f32<C>(v, C::REC == REC_LIM5TH || iv >= C::IAS, qL[iv], qR[iv]);
     if (C::SF && C::REC != REC_LIM2ND) flatten_face_f32(v, fa, fb, qL[iv], qR[iv]);
   }
   if (d == 1) {
@@ -560,10 +564,9 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     float gv[2][6];
 #pragma unroll
     for (int iv = 0; iv < 2; ++iv) {
-      gv[iv][0] = gv[iv][5] = 0.0f;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) gv[iv][1 + q] = cl.g(q, iv);
-      rec_face_f32<C>(gv[iv], false, gL[iv], gR[iv]);
+      for (int q = 0; q < 6; ++q) gv[iv][q] = (q >= 3 - SW && q < 3 + SW) ? cl.g(q - (3 - SW), iv) : 0.0f;
+      rec_face_f32<C>(gv[iv], C::REC == REC_LIM5TH, gL[iv], gR[iv]);
       if (C::SF && C::REC != REC_LIM2ND && !late) flatten_face_f32(gv[iv], fa, fb, gL[iv], gR[iv]);
     }
     if (C::WB) {
@@ -574,7 +577,7 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
     }
   } else if (C::HELM) {
     // without USE_FASTEOS the first gamma slot holds the stage input's temperature
-    const float tface = 0.5f * (cl.g(1, 0) + cl.g(2, 0));
+    const float tface = 0.5f * (cl.g(SW - 1, 0) + cl.g(SW, 0));
     split_side_eos<C>(P, qL, pe, tface, gL[0], gL[1]);
     split_side_eos<C>(P, qR, pe, tface, gR[0], gR[1]);
   }
@@ -592,11 +595,14 @@ __device__ __forceinline__ void face_flux_cells(const Prm &P, int d, int fi, int
 }
 
 template <class C>
-__device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int fj, int fk, const float *wl2,
-                                                const float *wl1, const float *wr1, const float *wr2,
-                                                const float *gl2, const float *gl1, const float *gr1,
-                                                const float *gr2, float F[C::NV]) {
-  RegCells<C::NV> cl{{wl2, wl1, wr1, wr2}, {gl2, gl1, gr1, gr2}};
+__device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int fj, int fk, const float *const *w,
+                                                const float *const *gm, float F[C::NV]) {
+  RegCells<C::NV> cl;
+#pragma unroll
+  for (int q = 0; q < 2 * C::SW; ++q) {
+    cl.w_[q] = w[q];
+    cl.g_[q] = gm[q];
+  }
   face_flux_cells<C>(P, d, fi, fj, fk, cl, F);
 }
 
@@ -743,17 +749,24 @@ __global__ void __launch_bounds__(128) k_stage_split(Prm P) {
     float rho_dev = 0.0f;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-      float w[5][NV], gm5[5][2];
+      // cells c-SW .. c+SW along d: the low face reads the first 2 SW, the high face the last
+      constexpr int NS = 2 * C::SW + 1;
+      float w[NS][NV], gmv[NS][2];
 #pragma unroll
-      for (int s = 0; s < 5; ++s) {
-        int ii = i + (d == 0 ? s - 2 : 0), jj = j + (d == 1 ? s - 2 : 0), kk = k + (d == 2 ? s - 2 : 0);
-        load_wf<C>(P, ii, jj, kk, w[s], gm5[s]);
+      for (int s = 0; s < NS; ++s) {
+        int ii = i + (d == 0 ? s - C::SW : 0), jj = j + (d == 1 ? s - C::SW : 0), kk = k + (d == 2 ? s - C::SW : 0);
+        load_wf<C>(P, ii, jj, kk, w[s], gmv[s]);
       }
-      if (d == 0) rho_dev = w[2][0];
+      if (d == 0) rho_dev = w[C::SW][0];
+      const float *wp[NS], *gp[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        wp[s] = w[s];
+        gp[s] = gmv[s];
+      }
       float Flo[NV], Fhi[NV];
-      face_flux_split<C>(P, d, i, j, k, w[0], w[1], w[2], w[3], gm5[0], gm5[1], gm5[2], gm5[3], Flo);
-      face_flux_split<C>(P, d, i + (d == 0), j + (d == 1), k + (d == 2), w[1], w[2], w[3], w[4], gm5[1], gm5[2],
-                         gm5[3], gm5[4], Fhi);
+      face_flux_split<C>(P, d, i, j, k, wp, gp, Flo);
+      face_flux_split<C>(P, d, i + (d == 0), j + (d == 1), k + (d == 2), wp + 1, gp + 1, Fhi);
       const float inv_dl = (float)g.inv_dx[d];
 #pragma unroll
       for (int iv = 0; iv < NV; ++iv) {
@@ -1245,6 +1258,8 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32) k_face_split_mhd(Prm P) {
 // so their loads stay within a few cache lines) and along y, z (threads of a warp are
 // neighbours in x and walk side by side)
 constexpr int WALK_K0 = 4, WALK_K = 8;
+// resident blocks of 128 threads per SM of the EoS half of the two-launch cons->prim
+constexpr int C2P_EOS_MINB = 7;
 // grid of the rescue-queue kernels: 4 blocks of 128 threads per SM of a B200 (148 SMs)
 constexpr int RESCUE_BLOCKS = 4 * 148;
 // resident blocks of 128 threads per SM the walking kernels are compiled for
@@ -1910,6 +1925,21 @@ __global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
   split_stat_flush<C>(P, st);
 }
 
+// cons->prim in two launches (PHL_C2P=two): the combine with the stores that depend on the
+// conserved state alone (and eint), then the EoS part from U and eint read back; the second
+// kernel holds only the Newton's registers and runs at a higher occupancy
+template <class C>
+__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split_combine(Prm P) {
+  if (!*P.active) return;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= P.g.N) return;
+  C2pState cs;
+  c2p_mhd_split_combine<C>(P, c, cs);
+  P.eint[c] = cs.eint;
+}
+template <class C>
+__global__ void __launch_bounds__(128, C2P_EOS_MINB) k_c2p_mhd_split_eos(Prm P);
+
 // the state of the combine for cell c, read back from U and eint
 template <class C>
 __device__ __forceinline__ void c2p_state_from_u(const Prm &P, long long c, C2pState &cs) {
@@ -1990,6 +2020,19 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const __grid_constant_
   const float y = mlp_forward_tile(w, x, S, 0u, ok, have, stalled);
   mlp_cta_teardown(S);
   if (t < n) out[t] = have ? y : __int_as_float(0x7fc00000);
+}
+
+template <class C>
+__global__ void __launch_bounds__(128, C2P_EOS_MINB) k_c2p_mhd_split_eos(Prm P) {
+  if (!*P.active) return;
+  SplitStat st;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < P.g.N) {
+    C2pState cs;
+    c2p_state_from_u<C>(P, c, cs);
+    c2p_mhd_split_eos<C, C2P_WARM>(P, c, cs, 0.0f, st);
+  }
+  split_stat_flush<C>(P, st);
 }
 
 // ---- learned rescue of poor warm starts (eos_guess = PHL_GUESS_MLP_RESCUE): one kernel on a
@@ -2220,6 +2263,11 @@ struct SplitRunnerT : Runner {
     out = e.maps;
     return e.ok;
   }
+  // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
+  const bool c2p_two = [] {
+    const char *e = getenv("PHL_C2P");
+    return e && strcmp(e, "two") == 0;
+  }();
   // PHL_FACE_KERNEL=walk keeps the walking face kernels on every grid (comparison of the two)
   const bool allow_face_tiles = [] {
     const char *e = getenv("PHL_FACE_KERNEL");
@@ -2316,13 +2364,18 @@ struct SplitRunnerT : Runner {
           return;
         }
       }
-      k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      if (c2p_two) {
+        k_c2p_mhd_split_combine<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+        k_c2p_mhd_split_eos<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      } else {
+        k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      }
     } else {
       hydro_stage(P, s);
     }
   }
   void hydro_stage(const Prm &P, cudaStream_t s) {
-    if constexpr (C::DIM == 3) {
+    if constexpr (C::DIM == 3 && C::SW == 2) {
       if (tiled(P.g)) {
         constexpr size_t sm = SplitTile<C, TX, TY>::bytes();
         if (!attr_set) {
@@ -2370,6 +2423,7 @@ struct SplitRunnerT : Runner {
   X(3, 7, true, true, true, R_LHLLD, true, REC_PPH, false) \
   X(3, 7, true, true, true, R_LHLLD, true, REC_LIM5TH, false) \
   X(3, 7, false, true, true, R_LHLLC, true, REC_PPH, false) \
+  X(3, 7, false, true, true, R_LHLLC, true, REC_LIM5TH, false) \
   X(2, 5, false, false, false, R_HLLC, false, REC_LIM2ND, true) \
   X(2, 4, true, false, false, R_HLLD, false, REC_LIM2ND, true) \
   X(3, 7, false, true, true, R_LHLLC, true, REC_LIM2ND, true) \

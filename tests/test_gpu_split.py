@@ -174,7 +174,8 @@ def test_split_orszag_tang_lim5th(gpu_lib):
 
 
 @pytest.mark.parametrize("mhd,riemann,rec,dims", [(True, "lhlld", "pph", (16, 24, 12)), (True, "lhlld", "lim5th", (16, 24, 12)),
-                                                  (False, "lhllc", "pph", (32, 16, 16))])
+                                                  (False, "lhllc", "pph", (32, 16, 16)),
+                                                  (False, "lhllc", "lim5th", (32, 16, 16))])
 def test_split_stratified_higher_order(gpu_lib, table, mhd, riemann, rec, dims):
     n, ny, nz = dims
     cfg, h = problems.stratified_3d(n, ny=ny, nz=nz, mhd=mhd, riemann=riemann, rec=rec)

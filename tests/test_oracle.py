@@ -407,3 +407,29 @@ def test_constant_acceleration_uniform_state(oracle):
     np.testing.assert_allclose(s[2], -0.1 - 0.2 * t, rtol=1e-13)
     np.testing.assert_allclose(s[3], 0.7, rtol=1e-13)  # the work goes into kinetic energy only
     assert np.all(s == s[:, :1, :1, :1])
+
+
+def test_face_temperature_guess_beats_a_learned_accuracy_guess(oracle, table):
+    """Helmholtz without USE_FASTEOS solves helm_rhoP_given on both sides of every face from the
+    guess 0.5 (T_L + T_R) (source.F90:8488-8495, 15777-15781).  On the stratified box that guess
+    converges in fewer iterations (about 2.6) than a guess as accurate as the trained network's
+    (0.2% in T, 3 iterations), so a learned guess cannot pay on these solves."""
+    from phlegethon_b200 import problems
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, fasteos=False)
+    helm = oracle.Helm.for_config(cfg, *table)
+    o = oracle.OracleGrid(h, helm)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    oracle.face_newton_stats(reset=True)
+    o.time_loop(2)
+    calls, iters = oracle.face_newton_stats(reset=True)
+    assert calls > 0
+    face = iters / calls
+    w, T = h.interior(h.prim), h.interior(h.temp)
+    rho, p, ye, ia = (w[q].ravel() for q in (0, 4, 5, 6))
+    abar = 1.0 / ia
+    sel = range(0, rho.size, 7)
+    learned_like = np.mean([helm.rhoP_given(rho[i], p[i], abar[i], ye[i] * abar[i], T.ravel()[i] * 1.002)[3]
+                            for i in sel])
+    assert face < learned_like, (face, learned_like)
+    assert face < 2.8 and learned_like >= 3.0, (face, learned_like)
