@@ -25,6 +25,45 @@ __device__ __forceinline__ int helm_node_index(const double *nodes, int n, doubl
   return i;
 }
 
+// The quintic Hermite bases of the table interpolation (source.F90:24708-24738) and their first
+// and second derivatives, in nested (Horner) form with fused multiply-adds: the same polynomials
+// as hb0 .. hb2m of phl_device.cuh, which keep the reference's term order for the FP64 form;
+// here they cost about half the operations and agree to rounding.
+__device__ __forceinline__ void fhb0(double x, double d, double d2, double b[3]) {
+  const double x2 = x * x;
+  b[0] = fma(x2 * x, fma(x, fma(-6.0, x, 15.0), -10.0), 1.0);
+  b[1] = x * fma(x2, fma(x, fma(-3.0, x, 8.0), -6.0), 1.0) * d;
+  b[2] = 0.5 * x2 * fma(x, fma(x, 3.0 - x, -3.0), 1.0) * d2;
+}
+__device__ __forceinline__ void fhb0m(double om, double d, double d2, double b[3]) {
+  const double o2 = om * om;
+  b[0] = fma(o2 * om, fma(om, fma(-6.0, om, 15.0), -10.0), 1.0);
+  b[1] = -(om * fma(o2, fma(om, fma(-3.0, om, 8.0), -6.0), 1.0)) * d;
+  b[2] = 0.5 * o2 * fma(om, fma(om, 3.0 - om, -3.0), 1.0) * d2;
+}
+__device__ __forceinline__ void fhb1(double x, double id, double d, double b[3]) {
+  const double x2 = x * x;
+  b[0] = x2 * fma(x, fma(-30.0, x, 60.0), -30.0) * id;
+  b[1] = fma(x2, fma(x, fma(-15.0, x, 32.0), -18.0), 1.0);
+  b[2] = 0.5 * x * fma(x, fma(x, fma(-5.0, x, 12.0), -9.0), 2.0) * d;
+}
+__device__ __forceinline__ void fhb1m(double om, double id, double d, double b[3]) {
+  const double o2 = om * om;
+  b[0] = -(o2 * fma(om, fma(-30.0, om, 60.0), -30.0)) * id;
+  b[1] = fma(o2, fma(om, fma(-15.0, om, 32.0), -18.0), 1.0);
+  b[2] = -(0.5 * om * fma(om, fma(om, fma(-5.0, om, 12.0), -9.0), 2.0)) * d;
+}
+__device__ __forceinline__ void fhb2(double y, double id2, double id, double b[3]) {
+  b[0] = y * fma(y, fma(-120.0, y, 180.0), -60.0) * id2;
+  b[1] = y * fma(y, fma(-60.0, y, 96.0), -36.0) * id;
+  b[2] = fma(y, fma(y, fma(-10.0, y, 18.0), -9.0), 1.0);
+}
+__device__ __forceinline__ void fhb2m(double om, double id2, double id, double b[3]) {
+  b[0] = om * fma(om, fma(-120.0, om, 180.0), -60.0) * id2;
+  b[1] = -(om * fma(om, fma(-60.0, om, 96.0), -36.0)) * id;
+  b[2] = fma(om, fma(om, fma(-10.0, om, 18.0), -9.0), 1.0);
+}
+
 struct HelmCell {
   int ih, jh;
   double Ye, rhos, x, drho;
@@ -54,8 +93,8 @@ __device__ __forceinline__ void helm_cell_contract_with(const HelmTable &h, cons
 
 // density basis (value) of the cell, recomputed where needed instead of kept in registers
 __device__ __forceinline__ void helm_cell_rbasis(const HelmCell &c, double r0[3], double r1[3]) {
-  hb0(c.x, c.drho, c.drho * c.drho, r0);
-  hb0m(1.0 - c.x, c.drho, c.drho * c.drho, r1);
+  fhb0(c.x, c.drho, c.drho * c.drho, r0);
+  fhb0m(1.0 - c.x, c.drho, c.drho * c.drho, r1);
 }
 
 __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell &c, int jh) {
@@ -109,12 +148,12 @@ __device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, doub
   const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
-  hb0(y, c.dT, c.dT * c.dT, t0);
-  hb0m(omy, c.dT, c.dT * c.dT, t1);
-  hb1(y, idT, c.dT, d0);
-  hb1m(omy, idT, c.dT, d1);
-  hb2(y, idT * idT, idT, e0);
-  hb2m(omy, idT * idT, idT, e1);
+  fhb0(y, c.dT, c.dT * c.dT, t0);
+  fhb0m(omy, c.dT, c.dT * c.dT, t1);
+  fhb1(y, idT, c.dT, d0);
+  fhb1m(omy, idT, c.dT, d1);
+  fhb2(y, idT * idT, idT, e0);
+  fhb2m(omy, idT * idT, idT, e1);
   f = fT = fTT = 0.0;
 #pragma unroll
   for (int ot = 0; ot < 3; ++ot) {
@@ -171,19 +210,19 @@ __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const Hel
   const double idT = c.idT;
   double y = (T - c.T0) * idT, omy = 1.0 - y;
   double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
-  hb0(y, c.dT, c.dT * c.dT, t0);
-  hb0m(omy, c.dT, c.dT * c.dT, t1);
-  hb1(y, idT, c.dT, d0);
-  hb1m(omy, idT, c.dT, d1);
-  hb2(y, idT * idT, idT, e0);
-  hb2m(omy, idT * idT, idT, e1);
+  fhb0(y, c.dT, c.dT * c.dT, t0);
+  fhb0m(omy, c.dT, c.dT * c.dT, t1);
+  fhb1(y, idT, c.dT, d0);
+  fhb1m(omy, idT, c.dT, d1);
+  fhb2(y, idT * idT, idT, e0);
+  fhb2m(omy, idT * idT, idT, e1);
   // d/drho contraction of the final cell
   double B[3][2];
   {
     const double idrho = __ldg(h.inv_drho + c.ih - 1);
     double dr0[3], dr1[3];
-    hb1(c.x, idrho, c.drho, dr0);
-    hb1m(1.0 - c.x, idrho, c.drho, dr1);
+    fhb1(c.x, idrho, c.drho, dr0);
+    fhb1m(1.0 - c.x, idrho, c.drho, dr1);
     helm_cell_contract_with(h, c, c.jh, dr0, dr1, B);
   }
   double f = 0, fT = 0, fTT = 0, fd = 0, fdT = 0;
@@ -242,8 +281,8 @@ __device__ __forceinline__ int helm_rhoP_fast(const HelmTable &h, HelmCell &c, d
   double B[3][2], dr0[3], dr1[3];
   {
     const double idrho = __ldg(h.inv_drho + c.ih - 1);
-    hb1(c.x, idrho, c.drho, dr0);
-    hb1m(1.0 - c.x, idrho, c.drho, dr1);
+    fhb1(c.x, idrho, c.drho, dr0);
+    fhb1m(1.0 - c.x, idrho, c.drho, dr1);
   }
   int jh = -1;
   double T0 = 0.0, dT = 0.0, idT = 0.0;
@@ -259,10 +298,10 @@ __device__ __forceinline__ int helm_rhoP_fast(const HelmTable &h, HelmCell &c, d
     }
     const double y = (T - T0) * idT, omy = 1.0 - y;
     double t0[3], t1[3], d0[3], d1[3];
-    hb0(y, dT, dT * dT, t0);
-    hb0m(omy, dT, dT * dT, t1);
-    hb1(y, idT, dT, d0);
-    hb1m(omy, idT, dT, d1);
+    fhb0(y, dT, dT * dT, t0);
+    fhb0m(omy, dT, dT * dT, t1);
+    fhb1(y, idT, dT, d0);
+    fhb1m(omy, idT, dT, d1);
     double fd = 0.0, fdT = 0.0;
 #pragma unroll
     for (int ot = 0; ot < 3; ++ot) {

@@ -623,6 +623,8 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
   constexpr int NV = C::NV, IP = C::IP, IAS = C::IAS, DIM = C::DIM;
   const Geo &g = P.g;
   const double dt = P.scal[1];
+  // the Newton's warm start, loaded before the state stores so that its latency overlaps them
+  const double Tw = C::HELM ? P.temp[c] : 0.0;
   // back to physical units: mass and scalar fluxes scale with rho_ref v_ref, momentum with
   // p_ref, energy with p_ref v_ref
   const double fm = P.rho_ref * P.v_ref, fe = P.p_ref * P.v_ref;
@@ -670,7 +672,7 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
   double p, T, sound = 0.0;
   if (C::HELM) {
     double ye = u[IAS] * inv_rho, inv_abar = u[IAS + 1] * inv_rho;
-    T = P.temp[c];
+    T = Tw;
     int clamped = 0;
     bool conv = false;
     HelmCell hc;
@@ -1693,6 +1695,7 @@ __global__ void __launch_bounds__(256) k_bface_split(Prm P) {
 // New state of one cell that the EoS part of cons->prim needs (the rest is stored before it)
 struct C2pState {
   double rho = 1.0, inv_rho = 1.0, eint = 0.0, ye = 0.0, inv_abar = 1.0;
+  double Tw = 0.0;  // the stage input's temperature (the Newton's warm start), loaded up front
   long long bc = 0;
 };
 
@@ -1839,12 +1842,12 @@ __device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, con
           st.iters += it;
           clamped = 0;
           conv = false;
-          T = P.temp[c];
+          T = cs.Tw;
           helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
           it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
         }
       } else if constexpr (MODE == C2P_RESCUE) {
-        const double Tw = P.temp[c];
+        const double Tw = cs.Tw;
         T = Tw;
         helm_cell_init_rho(P.helm, hc, rho, ye);
         helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
@@ -1859,7 +1862,7 @@ __device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, con
         }
         if (!conv) it += helm_rhoe_fast_from(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, Tw, 99, clamped, conv);
       } else {
-        T = P.temp[c];
+        T = cs.Tw;
         helm_cell_init_rho(P.helm, hc, rho, ye);
         helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
         it = helm_rhoe_fast(P.helm, hc, inv_rho, eint * inv_rho, inv_abar, T, 100, clamped, conv);
@@ -1912,13 +1915,15 @@ __device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, con
   return true;
 }
 
-template <class C, int MODE>
-__global__ void __launch_bounds__(128, C::MINB_C2P32) k_c2p_mhd_split(Prm P) {
+template <class C, int MODE, int MINB = C::MINB_C2P32>
+__global__ void __launch_bounds__(128, MINB) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   SplitStat st;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < P.g.N) {
     C2pState cs;
+    // the warm start first: its load then overlaps the combine instead of following its stores
+    if (C::HELM) cs.Tw = P.temp[c];
     c2p_mhd_split_combine<C>(P, c, cs);
     c2p_mhd_split_eos<C, MODE>(P, c, cs, 0.0f, st);
   }
@@ -1951,6 +1956,7 @@ __device__ __forceinline__ void c2p_state_from_u(const Prm &P, long long c, C2pS
   cs.rho = P.U[c];
   cs.inv_rho = 1.0 / cs.rho;
   cs.eint = P.eint[c];
+  if (C::HELM) cs.Tw = P.temp[c];
   cs.ye = P.U[(long long)IAS * g.N + c] * cs.inv_rho;
   cs.inv_abar = P.U[(long long)(IAS + 1) * g.N + c] * cs.inv_rho;
 }
@@ -2263,6 +2269,12 @@ struct SplitRunnerT : Runner {
     out = e.maps;
     return e.ok;
   }
+  // PHL_C2P_MINB=7 compiles the Helmholtz MHD cons->prim for 7 resident blocks per SM (72
+  // registers) instead of 6 (80)
+  const int c2p_minb = [] {
+    const char *e = getenv("PHL_C2P_MINB");
+    return e ? atoi(e) : 0;
+  }();
   // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
   const bool c2p_two = [] {
     const char *e = getenv("PHL_C2P");
@@ -2352,7 +2364,8 @@ struct SplitRunnerT : Runner {
         if (P.mlp_w && P.mlp_small && P.rescue_q) {
           // warm start everywhere; cells with a poor warm start through the learned guess
           cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
-          k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, 128), 128, 0, s>>>(P);
+          if (c2p_minb == 7) k_c2p_mhd_split<C, C2P_RESCUE, 7><<<nblk(g.N, 128), 128, 0, s>>>(P);
+          else k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, 128), 128, 0, s>>>(P);
           k_c2p_rescue<C><<<RESCUE_BLOCKS, 128, sizeof(MlpUmmaSmem), s>>>(P, *P.mlp_small);
           return;
         }
@@ -2367,6 +2380,8 @@ struct SplitRunnerT : Runner {
       if (c2p_two) {
         k_c2p_mhd_split_combine<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
         k_c2p_mhd_split_eos<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
+      } else if (C::HELM && c2p_minb == 7) {
+        k_c2p_mhd_split<C, C2P_WARM, 7><<<nblk(g.N, 128), 128, 0, s>>>(P);
       } else {
         k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, 128), 128, 0, s>>>(P);
       }

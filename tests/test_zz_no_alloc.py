@@ -1,11 +1,12 @@
 """The allocation-free EoS inversion entry point against the allocating one.
 
-phl_eos_invert_batch_noalloc serves callers that must not allocate device memory during the
-call (a driver whose GPU memory is already held by its own pool allocator, or code running
-while a CUDA stream capture is open).  Its device copies live in one array compiled into the
-library and shared by all calls, so two calls in a row must each give the same answer as
-phl_eos_invert_batch, with nothing carried over from the call before.  The file is named so
-that pytest collects it last.
+phl_eos_invert_batch_noalloc serves callers that cannot call cudaMalloc during a run: a driver
+that hands all free device memory to its own pool allocator at start-up, or one whose time loop
+must not allocate because cudaMalloc/cudaFree can synchronise the whole device.  Its device
+copies live in one array compiled into the library and shared by all calls, so calls in a row
+must each give the same answer as phl_eos_invert_batch, with nothing carried over from the call
+before -- including a call at the full capacity of PHL_NOALLOC_MAX_SAMPLES samples.  The file is
+named so that pytest collects it last.
 """
 import ctypes as C
 
@@ -34,7 +35,8 @@ def test_noalloc_matches_allocating_entry_point(gpu_lib, table):
     with Simulation(cfg, table) as sim:
         lib = sim.lib
         assert lib.phl_mlp_train(sim.ctx, 1 << 16, 7, 4, 4096, C.c_double(3e-3), None) == 0
-        for call, (n, seed) in enumerate([(5000, 11), (3000, 12)]):
+        # two calls in a row, then one at the array's capacity (65536 samples)
+        for call, (n, seed) in enumerate([(5000, 11), (3000, 12), (65536, 13)]):
             rho, T, abar, zbar = problems.eos_samples(n, seed=seed)
             e = np.zeros(n)
             d = {}
