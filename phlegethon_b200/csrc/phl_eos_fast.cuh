@@ -13,12 +13,13 @@
 
 namespace phl {
 
-// table node index (1-based like the reference) of x in the log-spaced nodes, from a single
-// precision log and exact comparisons against the node values
+// table node index (1-based like the reference) of x in the log-spaced nodes: an estimate in
+// single precision (within one node of the cell for any x in the table's range), then exact
+// comparisons against the node values
 __device__ __forceinline__ int helm_node_index(const double *nodes, int n, double log10_first, double dlog,
                                                double x) {
-  float lx = __log2f((float)x) * 0.30102999566398120f;
-  int i = (int)(((double)lx - log10_first) / dlog) + 1;
+  const float lx = __log2f((float)x) * 0.30102999566398120f;
+  int i = (int)(__fdividef(lx - (float)log10_first, (float)dlog)) + 1;
   i = max(1, min(i, n - 1));
   if (i < n - 1 && __ldg(nodes + i) <= x) ++i;
   if (i > 1 && __ldg(nodes + i - 1) > x) --i;

@@ -1267,21 +1267,35 @@ constexpr int RESCUE_BLOCKS = 4 * 148;
 // resident blocks of 128 threads per SM the walking kernels are compiled for
 constexpr int WALK_MINB = 6;
 
-// Raw values of one cell for the walking face kernel: the FP32 state (0..NV-1), cell B (NV..NV+2)
-// and the two FASTEOS gammas or the temperature (NV+3, NV+4).  q is the cell's index along D and
-// c[] its other two coordinates; a cell inside the domain along D is read by linear index lc,
-// a ghost maps its index.
+// Raw values of one cell for the walking face kernel along D: the FP32 state (0 .. NV-1), the
+// cell B components transverse to D (NBT of them from NV on; the component along D is not
+// reconstructed, the face carries it) and the two FASTEOS gammas or the temperature (IG, IG+1).
 template <class C, int D>
-__device__ __forceinline__ void load_walk_cell(const Prm &P, const int c[3], int q, long long lc, float r[C::NV + 5]) {
-  float *w = r, *b = r + C::NV, *gm = r + C::NV + 3;
+struct WalkCell {
+  static constexpr int NBT = C::DIM - 1, IG = C::NV + NBT, NR = IG + 2;
+  // cell B component held in transverse slot t
+  static __device__ __forceinline__ constexpr int comp(int t) { return t < D ? t : t + 1; }
+};
+
+// q is the cell's index along D and c[] its other two coordinates; a cell inside the domain
+// along D is read by linear index lc, a ghost maps its index.
+template <class C, int D>
+__device__ __forceinline__ void load_walk_cell(const Prm &P, const int c[3], int q, long long lc,
+                                               float r[WalkCell<C, D>::NR]) {
+  using L = WalkCell<C, D>;
+  float *gm = r + L::IG;
   gm[0] = gm[1] = 0.0f;
   if (q >= 0 && q < P.g.nx[D]) {
-    load_wf_at<C>(P, lc, w, gm);
-    load_bccf_at<C>(P, lc, b);
+    load_wf_at<C>(P, lc, r, gm);
+#pragma unroll
+    for (int t = 0; t < L::NBT; ++t) r[C::NV + t] = __ldg(P.bccf + L::comp(t) * P.g.N + lc);
   } else {
     const int i = D == 0 ? q : c[0], j = D == 1 ? q : c[1], k = D == 2 ? q : c[2];
-    load_wf<C>(P, i, j, k, w, gm);
+    float b[3];
+    load_wf<C>(P, i, j, k, r, gm);
     load_bccf<C>(P, i, j, k, b);
+#pragma unroll
+    for (int t = 0; t < L::NBT; ++t) r[C::NV + t] = b[L::comp(t)];
   }
 }
 
@@ -1293,7 +1307,8 @@ template <class C, int D, int K>
 __global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_face_split_mhd_walk(Prm P) {
   static_assert(C::REC == REC_LIM2ND, "the walk carries LIM2ND edge values");
   if (!*P.active) return;
-  constexpr int NV = C::NV, NR = NV + 5;
+  using L = WalkCell<C, D>;
+  constexpr int NV = C::NV, NR = L::NR, IG = L::IG;
   const Geo &g = P.g;
   const int nd = g.nx[D] + 1, nch = (nd + K - 1) / K;
   const int e0 = D == 0 ? nch : g.nx[0], e1 = D == 1 ? nch : g.nx[1];
@@ -1335,18 +1350,17 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_fa
       qR[iv] = lo[iv];
     }
 #pragma unroll
-    for (int a = 0; a < C::DIM; ++a) {
-      if (a == D) continue;
-      bL[a] = hip[NV + a];
-      bR[a] = lo[NV + a];
+    for (int t = 0; t < L::NBT; ++t) {
+      bL[L::comp(t)] = hip[NV + t];
+      bR[L::comp(t)] = lo[NV + t];
     }
     const long long fidx = frow + (long long)q * fstride;
     long long fbg = 0;
     if (C::WB || C::ETOT) fbg = g.bg_profile ? (long long)(D == 1 ? q : c[1]) : fidx;
     float tface = 0.0f;
     if (C::FAST) {
-      gL[0] = hip[NV + 3]; gL[1] = hip[NV + 4];
-      gR[0] = lo[NV + 3]; gR[1] = lo[NV + 4];
+      gL[0] = hip[IG]; gL[1] = hip[IG + 1];
+      gR[0] = lo[IG]; gR[1] = lo[IG + 1];
       if (C::WB) {
         const float ge = __ldg(P.sf_ge_f[D] + fbg);
         const float rL[2] = {gL[0], gL[1]}, rR[2] = {gR[0], gR[1]};
@@ -1360,7 +1374,7 @@ __global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_fa
         }
       }
     } else if (C::HELM) {
-      tface = 0.5f * (rm[NV + 3] + rc[NV + 3]);
+      tface = 0.5f * (rm[IG] + rc[IG]);
     }
     float F[NV], Fb[3], rs;
     face_solve_split_mhd<C>(P, D, fidx, fbg, qL, qR, bL, bR, gL, gR, tface, C::SF && (fa || fb), F, Fb, rs);
@@ -1915,12 +1929,18 @@ __device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, con
   return true;
 }
 
+// cells per block of the cons->prim kernels
+constexpr int C2P_BLOCK = 128;
+
 template <class C, int MODE, int MINB = C::MINB_C2P32>
-__global__ void __launch_bounds__(128, MINB) k_c2p_mhd_split(Prm P) {
+__global__ void __launch_bounds__(C2P_BLOCK, MINB) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   SplitStat st;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < P.g.N) {
+  // a grid of one resident wave strides over the cells: the warps drift apart in phase (their
+  // Newton iteration counts differ), so that the memory waits of some overlap the FP64
+  // arithmetic of others instead of every block of a wave waiting at the same time
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.g.N;
+       c += (long long)gridDim.x * blockDim.x) {
     C2pState cs;
     // the warm start first: its load then overlaps the combine instead of following its stores
     if (C::HELM) cs.Tw = P.temp[c];
@@ -2275,15 +2295,50 @@ struct SplitRunnerT : Runner {
     const char *e = getenv("PHL_C2P_MINB");
     return e ? atoi(e) : 0;
   }();
+  // grid of each cons->prim kernel: one wave of resident blocks (found at construction, outside
+  // any stream capture) striding over the cells, or one block per 128 cells with
+  // PHL_C2P_GRID=cells (comparison)
+  unsigned grid_warm = 0, grid_warm7 = 0, grid_rescue = 0, grid_rescue7 = 0;
+  template <class K>
+  static unsigned wave_blocks(K kernel) {
+    int dev = 0, sms = 0, nb = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, C2P_BLOCK, 0) != cudaSuccess)
+      return 0;
+    return (unsigned)(sms * nb);
+  }
+  SplitRunnerT() {
+    const char *e = getenv("PHL_C2P_GRID");
+    if (e && strcmp(e, "cells") == 0) return;
+    if constexpr (C::MHD) {
+      grid_warm = wave_blocks(k_c2p_mhd_split<C, C2P_WARM>);
+      grid_warm7 = wave_blocks(k_c2p_mhd_split<C, C2P_WARM, 7>);
+      if constexpr (C::HELM) {
+        grid_rescue = wave_blocks(k_c2p_mhd_split<C, C2P_RESCUE>);
+        grid_rescue7 = wave_blocks(k_c2p_mhd_split<C, C2P_RESCUE, 7>);
+      }
+    }
+  }
+  // blocks of a cons->prim launch over n cells: the wave, or fewer where the cells need fewer
+  static unsigned c2p_grid(unsigned wave, long long n) {
+    const unsigned cells = nblk(n, C2P_BLOCK);
+    return wave && wave < cells ? wave : cells;
+  }
   // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
   const bool c2p_two = [] {
     const char *e = getenv("PHL_C2P");
     return e && strcmp(e, "two") == 0;
   }();
-  // PHL_FACE_KERNEL=walk keeps the walking face kernels on every grid (comparison of the two)
-  const bool allow_face_tiles = [] {
+  // face kernel per direction: by default the shared-memory tiles along x1 (where the walking
+  // kernel's threads stride K0 cells apart) and the walking kernels along x2 and x3 (threads of
+  // a warp are neighbours in x1 there, and the walk, with no block barrier and the edges in
+  // registers, ran 0.80 -> 0.67 ms per direction at 256^3); PHL_FACE_KERNEL=walk / =tile select
+  // one kind for every direction (comparisons)
+  const int face_kind = [] {
     const char *e = getenv("PHL_FACE_KERNEL");
-    return !(e && strcmp(e, "walk") == 0);
+    if (e && strcmp(e, "walk") == 0) return 0;
+    if (e && strcmp(e, "tile") == 0) return 2;
+    return 1;
   }();
   // faces along D from shared-memory tiles, when the grid is a multiple of the tile; false to
   // fall back to the walking kernel
@@ -2296,7 +2351,8 @@ struct SplitRunnerT : Runner {
       using S_ = FaceTileSmem<C, D>;
       const Geo &g = P.g;
       const int nz = C::DIM == 3 ? g.nx[2] : 1;
-      if (!allow_face_tiles || g.nx[0] % T::TX || g.nx[1] % T::TY || nz % T::TZ) return false;
+      if (face_kind == 0 || (face_kind == 1 && D != 0)) return false;
+      if (g.nx[0] % T::TX || g.nx[1] % T::TY || nz % T::TZ) return false;
       FaceTileMaps m;
       if (!tile_maps<D>(P, m)) return false;
       const long long ntiles = (long long)(g.nx[0] / T::TX) * (g.nx[1] / T::TY) * (nz / T::TZ);
@@ -2364,8 +2420,10 @@ struct SplitRunnerT : Runner {
         if (P.mlp_w && P.mlp_small && P.rescue_q) {
           // warm start everywhere; cells with a poor warm start through the learned guess
           cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
-          if (c2p_minb == 7) k_c2p_mhd_split<C, C2P_RESCUE, 7><<<nblk(g.N, 128), 128, 0, s>>>(P);
-          else k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, 128), 128, 0, s>>>(P);
+          if (c2p_minb == 7)
+            k_c2p_mhd_split<C, C2P_RESCUE, 7><<<c2p_grid(grid_rescue7, g.N), C2P_BLOCK, 0, s>>>(P);
+          else
+            k_c2p_mhd_split<C, C2P_RESCUE><<<c2p_grid(grid_rescue, g.N), C2P_BLOCK, 0, s>>>(P);
           k_c2p_rescue<C><<<RESCUE_BLOCKS, 128, sizeof(MlpUmmaSmem), s>>>(P, *P.mlp_small);
           return;
         }
@@ -2381,9 +2439,9 @@ struct SplitRunnerT : Runner {
         k_c2p_mhd_split_combine<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
         k_c2p_mhd_split_eos<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
       } else if (C::HELM && c2p_minb == 7) {
-        k_c2p_mhd_split<C, C2P_WARM, 7><<<nblk(g.N, 128), 128, 0, s>>>(P);
+        k_c2p_mhd_split<C, C2P_WARM, 7><<<c2p_grid(grid_warm7, g.N), C2P_BLOCK, 0, s>>>(P);
       } else {
-        k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, 128), 128, 0, s>>>(P);
+        k_c2p_mhd_split<C, C2P_WARM><<<c2p_grid(grid_warm, g.N), C2P_BLOCK, 0, s>>>(P);
       }
     } else {
       hydro_stage(P, s);

@@ -325,7 +325,7 @@ def test_tiled_faces_equal_walking_faces(gpu_lib, table, mhd_case, monkeypatch):
         tab = None
     monkeypatch.setenv("PHL_FACE_KERNEL", "walk")
     ha, sta = run_form(cfg, h, 3, tab, "fp32_split")
-    monkeypatch.setenv("PHL_FACE_KERNEL", "auto")
+    monkeypatch.setenv("PHL_FACE_KERNEL", "tile")
     hb, stb = run_form(cfg, h, 3, tab, "fp32_split")
     h64, _ = run_form(cfg, h, 3, tab, "fp64")
     assert stb["nonfinite"] == 0 and stb["tensor_core_stalls"] == 0
