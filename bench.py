@@ -393,8 +393,8 @@ def measure_form(args, name, cfg, h, table, form, local, dist, want_e2e, guess="
         dyn.eq_gammae_x = [None] * 3
         sim.download(dyn)
         e2e_steps = max(1, min(args.steps, 10))
-        # bytes per step: each call uploads the whole host arrays (ghost layers included) and
-        # downloads their interiors
+        # bytes per step: each call uploads the whole host arrays (ghost layers included:
+        # contiguous copies) and downloads their interiors
         h2d = sum(a.nbytes for a in [dyn.prim, dyn.temp, dyn.eint, dyn.gammaf, dyn.b_cc] + bx if a is not None)
         cells = cfg.n_cells
         d2h = 8 * sum(x for x in [cfg.nvars * cells, cells, cells,

@@ -189,6 +189,8 @@ int phl_run_steps(phl_ctx *ctx, int nsteps, double tmax, int *steps_done, double
  * gammaf, b_cc, b_x, laid out as for phl_upload_state; background members are not read),
  * advance exactly nsteps steps of time_loop (no tmax clamp), and download the dynamic state back
  * into the same arrays -- all queued on the context's streams; the call returns without waiting.
+ * The whole arrays travel up (contiguous copies) and their interiors come down; the ghost
+ * layers are neither read by the step nor written.
  * This is the per-step exchange of a driver that keeps its state in host memory (the reference's
  * own arrays) and wants the copies off the critical path: the upload of each chunk of host
  * planes waits only for the previous call's download of the same planes, so the two PCIe

@@ -2175,11 +2175,17 @@ __global__ void k_split_to_prim(Prm P) {
   double eint = P.eint[c];
   double p;
   if (C::HELM) {
-    double ye = u[IAS] * inv_rho, abar = rho / u[IAS + 1], zbar = ye * abar, E, s, cv;
-    helm_given_full(P.helm, rho, P.temp[c], abar, zbar, p, E, s, cv);
+    // pressure and sound speed at the state's temperature from the contracted table cell (the
+    // evaluation of the split form's cons->prim, equal to given_full to rounding)
+    const double inv_abar = u[IAS + 1] * inv_rho, ye = u[IAS] * inv_rho, T = P.temp[c];
+    HelmCell hc;
+    helm_cell_init_rho(P.helm, hc, rho, ye);
+    helm_cell_contract(P.helm, hc, helm_node_index(P.helm.T, P.helm.nT, P.helm.log10_T1, P.helm.dT, T));
+    double s2;
+    helm_cell_p_sound2(P.helm, hc, rho, inv_rho, T, inv_abar, p, s2);
     if (C::FAST) {
       P.gout[c] = p / eint + 1.0;
-      P.gout[g.N + c] = s * s * rho / p;
+      P.gout[g.N + c] = s2 * rho / p;
     } else {
       P.gout[c] = P.temp[c];
     }

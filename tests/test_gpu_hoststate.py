@@ -82,3 +82,40 @@ def test_host_pipeline_then_synchronous_calls(gpu_lib, table):
     for x, y in zip(arrays(dyn), arrays(out)):
         assert np.array_equal(x, y)
     sim.close()
+
+
+def test_host_pipeline_reads_and_writes_interiors_only(gpu_lib, table):
+    """The pipeline moves only the interior of each host array: NaN in every ghost layer
+    (cells and faces) changes nothing inside and stays NaN outside."""
+    cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=True)
+    cfg = cfg.replace(precision="fp32_split")
+    h.cfg = cfg
+    sim_a, dyn_a = start(cfg, h.copy(), table)
+    sim_b, dyn_b = start(cfg, h.copy(), table)
+    ghost_masks = []
+    for nm in DYNAMIC:
+        a = getattr(dyn_b, nm)
+        if a is None:
+            continue
+        keep = dyn_b.interior(a).copy()
+        a[...] = np.nan
+        dyn_b.interior(a)[...] = keep
+        ghost_masks.append((nm, np.isnan(a)))
+    for d in range(cfg.sdims):
+        keep = dyn_b.bface_interior(d).copy()
+        dyn_b.b_x[d][...] = np.nan
+        dyn_b.bface_interior(d)[...] = keep
+    for _ in range(3):
+        sim_a.time_loop_host_async(dyn_a, 1)
+        sim_b.time_loop_host_async(dyn_b, 1)
+    sim_a.wait_host()
+    sim_b.wait_host()
+    sim_a.close()
+    sim_b.close()
+    for nm, mask in ghost_masks:
+        a, b = getattr(dyn_a, nm), getattr(dyn_b, nm)
+        assert np.array_equal(dyn_a.interior(a), dyn_b.interior(b)), nm
+        assert np.isnan(b[mask]).all(), nm
+    for d in range(cfg.sdims):
+        assert np.array_equal(dyn_a.bface_interior(d), dyn_b.bface_interior(d))
+        assert np.isnan(dyn_b.b_x[d]).sum() == dyn_b.b_x[d].size - dyn_b.bface_interior(d).size
