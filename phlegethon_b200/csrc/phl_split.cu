@@ -608,10 +608,12 @@ __device__ __forceinline__ void face_flux_split(const Prm &P, int d, int fi, int
 
 // --------------------------------------------------------------------- split stage kernels
 // Per-cell statistics of a stage, reduced once per block.
+// per-thread counters (32-bit: a thread's cells times 100 iterations stay far below 2^32; the
+// block sums go to the 64-bit counters of the context)
 struct SplitStat {
   double smax = 0.0;
-  unsigned long long calls = 0, iters = 0, nonconv = 0, clamp = 0, bad = 0;
-  unsigned long long mlp_acc = 0, mlp_rej = 0, gevals = 0;  // learned guess in the step
+  unsigned calls = 0, iters = 0, nonconv = 0, clamp = 0, bad = 0;
+  unsigned mlp_acc = 0, mlp_rej = 0, gevals = 0;  // learned guess in the step
 };
 
 // Everything of a stage after the flux divergence, for one cell: flux divergence to physical
@@ -1936,11 +1938,8 @@ template <class C, int MODE, int MINB = C::MINB_C2P32>
 __global__ void __launch_bounds__(C2P_BLOCK, MINB) k_c2p_mhd_split(Prm P) {
   if (!*P.active) return;
   SplitStat st;
-  // a grid of one resident wave strides over the cells: the warps drift apart in phase (their
-  // Newton iteration counts differ), so that the memory waits of some overlap the FP64
-  // arithmetic of others instead of every block of a wave waiting at the same time
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.g.N;
-       c += (long long)gridDim.x * blockDim.x) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < P.g.N) {
     C2pState cs;
     // the warm start first: its load then overlaps the combine instead of following its stores
     if (C::HELM) cs.Tw = P.temp[c];
@@ -2301,35 +2300,6 @@ struct SplitRunnerT : Runner {
     const char *e = getenv("PHL_C2P_MINB");
     return e ? atoi(e) : 0;
   }();
-  // grid of each cons->prim kernel: one wave of resident blocks (found at construction, outside
-  // any stream capture) striding over the cells, or one block per 128 cells with
-  // PHL_C2P_GRID=cells (comparison)
-  unsigned grid_warm = 0, grid_warm7 = 0, grid_rescue = 0, grid_rescue7 = 0;
-  template <class K>
-  static unsigned wave_blocks(K kernel) {
-    int dev = 0, sms = 0, nb = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, C2P_BLOCK, 0) != cudaSuccess)
-      return 0;
-    return (unsigned)(sms * nb);
-  }
-  SplitRunnerT() {
-    const char *e = getenv("PHL_C2P_GRID");
-    if (e && strcmp(e, "cells") == 0) return;
-    if constexpr (C::MHD) {
-      grid_warm = wave_blocks(k_c2p_mhd_split<C, C2P_WARM>);
-      grid_warm7 = wave_blocks(k_c2p_mhd_split<C, C2P_WARM, 7>);
-      if constexpr (C::HELM) {
-        grid_rescue = wave_blocks(k_c2p_mhd_split<C, C2P_RESCUE>);
-        grid_rescue7 = wave_blocks(k_c2p_mhd_split<C, C2P_RESCUE, 7>);
-      }
-    }
-  }
-  // blocks of a cons->prim launch over n cells: the wave, or fewer where the cells need fewer
-  static unsigned c2p_grid(unsigned wave, long long n) {
-    const unsigned cells = nblk(n, C2P_BLOCK);
-    return wave && wave < cells ? wave : cells;
-  }
   // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
   const bool c2p_two = [] {
     const char *e = getenv("PHL_C2P");
@@ -2427,9 +2397,9 @@ struct SplitRunnerT : Runner {
           // warm start everywhere; cells with a poor warm start through the learned guess
           cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
           if (c2p_minb == 7)
-            k_c2p_mhd_split<C, C2P_RESCUE, 7><<<c2p_grid(grid_rescue7, g.N), C2P_BLOCK, 0, s>>>(P);
+            k_c2p_mhd_split<C, C2P_RESCUE, 7><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
           else
-            k_c2p_mhd_split<C, C2P_RESCUE><<<c2p_grid(grid_rescue, g.N), C2P_BLOCK, 0, s>>>(P);
+            k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
           k_c2p_rescue<C><<<RESCUE_BLOCKS, 128, sizeof(MlpUmmaSmem), s>>>(P, *P.mlp_small);
           return;
         }
@@ -2445,9 +2415,9 @@ struct SplitRunnerT : Runner {
         k_c2p_mhd_split_combine<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
         k_c2p_mhd_split_eos<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
       } else if (C::HELM && c2p_minb == 7) {
-        k_c2p_mhd_split<C, C2P_WARM, 7><<<c2p_grid(grid_warm7, g.N), C2P_BLOCK, 0, s>>>(P);
+        k_c2p_mhd_split<C, C2P_WARM, 7><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
       } else {
-        k_c2p_mhd_split<C, C2P_WARM><<<c2p_grid(grid_warm, g.N), C2P_BLOCK, 0, s>>>(P);
+        k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
       }
     } else {
       hydro_stage(P, s);
