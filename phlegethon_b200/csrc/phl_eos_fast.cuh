@@ -5,9 +5,11 @@
 // E(T) = e with the reference's tolerance, iteration cap and out-of-table reset.  The evaluation
 // order differs: the density is fixed during a solve, so for the current table cell the 36
 // coefficients are contracted once with the density basis into A[ot][jt] (value) and B[ot][jt]
-// (d/drho), ot = T-derivative order of the table variable, jt = lower/upper T node.  An
-// iteration then needs the T basis and 3 x 6 products; the contraction is redone only when T
-// leaves the cell.  Results agree with the reference evaluation to rounding.
+// (d/drho), ot = T-derivative order of the table variable, jt = lower/upper T node, and the
+// quintic Hermite combination in T is rewritten once as the monomial coefficients of a quintic
+// in y = (T - T0) / dT.  An iteration then evaluates f, df/dy and d2f/dy2 by one Horner pass
+// (15 fused multiply-adds); the contraction is redone only when T leaves the cell.  Results
+// agree with the reference evaluation to rounding.
 #pragma once
 #include "phl_device.cuh"
 
@@ -27,9 +29,10 @@ __device__ __forceinline__ int helm_node_index(const double *nodes, int n, doubl
 }
 
 // The quintic Hermite bases of the table interpolation (source.F90:24708-24738) and their first
-// and second derivatives, in nested (Horner) form with fused multiply-adds: the same polynomials
-// as hb0 .. hb2m of phl_device.cuh, which keep the reference's term order for the FP64 form;
-// here they cost about half the operations and agree to rounding.
+// derivatives, in nested (Horner) form with fused multiply-adds: the same polynomials as hb0 ..
+// hb1m of phl_device.cuh, which keep the reference's term order for the FP64 form; here they
+// cost about half the operations and agree to rounding.  They weight the density direction of
+// the contraction; the temperature direction is a quintic in monomial form (helm_hermite_poly).
 __device__ __forceinline__ void fhb0(double x, double d, double d2, double b[3]) {
   const double x2 = x * x;
   b[0] = fma(x2 * x, fma(x, fma(-6.0, x, 15.0), -10.0), 1.0);
@@ -54,23 +57,42 @@ __device__ __forceinline__ void fhb1m(double om, double id, double d, double b[3
   b[1] = fma(o2, fma(om, fma(-15.0, om, 32.0), -18.0), 1.0);
   b[2] = -(0.5 * om * fma(om, fma(om, fma(-5.0, om, 12.0), -9.0), 2.0)) * d;
 }
-__device__ __forceinline__ void fhb2(double y, double id2, double id, double b[3]) {
-  b[0] = y * fma(y, fma(-120.0, y, 180.0), -60.0) * id2;
-  b[1] = y * fma(y, fma(-60.0, y, 96.0), -36.0) * id;
-  b[2] = fma(y, fma(y, fma(-10.0, y, 18.0), -9.0), 1.0);
-}
-__device__ __forceinline__ void fhb2m(double om, double id2, double id, double b[3]) {
-  b[0] = om * fma(om, fma(-120.0, om, 180.0), -60.0) * id2;
-  b[1] = -(om * fma(om, fma(-60.0, om, 96.0), -36.0)) * id;
-  b[2] = fma(om, fma(om, fma(-10.0, om, 18.0), -9.0), 1.0);
-}
-
 struct HelmCell {
   int ih, jh;
   double Ye, rhos, x, drho;
-  double A[3][2];                       // contracted coefficients of the current T cell
+  double c[6];                          // f of the current T cell: sum of c[m] y^m
   double T0, dT, idT;                   // lower T node, spacing and its inverse, current T cell
 };
+
+// Monomial coefficients in y of the quintic Hermite interpolant in T with nodal values, first
+// and second T-derivatives A[0..2][0] (lower node) and A[0..2][1] (upper node) over a cell of
+// width dT.  The bases psi0(y) = 1 - 10y^3 + 15y^4 - 6y^5, psi1(y) = y - 6y^3 + 8y^4 - 3y^5,
+// psi2(y) = (y^2 - 3y^3 + 3y^4 - y^5) / 2 (the functions of source.F90:24708-24738) and their
+// mirror images psi(1 - y) expanded in powers of y; the nodal difference b0 - a0 is formed first,
+// so the large cubic-to-quintic terms carry it instead of the values themselves.
+__device__ __forceinline__ void helm_hermite_poly(const double A[3][2], double dT, double c[6]) {
+  const double a0 = A[0][0], a1 = A[1][0] * dT, a2 = A[2][0] * (dT * dT);
+  const double b1 = A[1][1] * dT, b2 = A[2][1] * (dT * dT), d0 = A[0][1] - a0;
+  c[0] = a0;
+  c[1] = a1;
+  c[2] = 0.5 * a2;
+  c[3] = fma(10.0, d0, fma(-6.0, a1, fma(-4.0, b1, fma(-1.5, a2, 0.5 * b2))));
+  c[4] = fma(-15.0, d0, fma(8.0, a1, fma(7.0, b1, fma(1.5, a2, -b2))));
+  c[5] = fma(6.0, d0, fma(-3.0, a1, fma(-3.0, b1, fma(-0.5, a2, 0.5 * b2))));
+}
+
+// p(y), p'(y) and p''(y) / 2 of the quintic sum c[m] y^m in one Horner pass
+__device__ __forceinline__ void poly5_eval(const double c[6], double y, double &p, double &d1, double &d2h) {
+  p = c[5];
+  d1 = 0.0;
+  d2h = 0.0;
+#pragma unroll
+  for (int m = 4; m >= 0; --m) {
+    d2h = fma(d2h, y, d1);
+    d1 = fma(d1, y, p);
+    p = fma(p, y, c[m]);
+  }
+}
 
 // coefficients of T order ot (variables {0,3,4}, {1,5,6}, {2,7,8}: value, d/drho, d2/drho2 of
 // f, f_T, f_TT) at the lower/upper T node jt, contracted with a density basis (r0, r1)
@@ -103,9 +125,10 @@ __device__ __forceinline__ void helm_cell_contract(const HelmTable &h, HelmCell 
   c.T0 = __ldg(h.T + jh - 1);
   c.dT = __ldg(h.T + jh) - c.T0;
   c.idT = __ldg(h.inv_dT + jh - 1);
-  double r0[3], r1[3];
+  double r0[3], r1[3], A[3][2];
   helm_cell_rbasis(c, r0, r1);
-  helm_cell_contract_with(h, c, jh, r0, r1, c.A);
+  helm_cell_contract_with(h, c, jh, r0, r1, A);
+  helm_hermite_poly(A, c.dT, c.c);
 }
 
 // density part of the cell: table row of rho * Ye and the position in it
@@ -147,21 +170,10 @@ __device__ __forceinline__ double helm_cell_cold_energy(const HelmTable &h, cons
 // f, f_T, f_TT at T (T inside the current cell)
 __device__ __forceinline__ void helm_cell_eval(const HelmCell &c, double T, double &f, double &fT, double &fTT) {
   const double idT = c.idT;
-  double y = (T - c.T0) * idT, omy = 1.0 - y;
-  double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
-  fhb0(y, c.dT, c.dT * c.dT, t0);
-  fhb0m(omy, c.dT, c.dT * c.dT, t1);
-  fhb1(y, idT, c.dT, d0);
-  fhb1m(omy, idT, c.dT, d1);
-  fhb2(y, idT * idT, idT, e0);
-  fhb2m(omy, idT * idT, idT, e1);
-  f = fT = fTT = 0.0;
-#pragma unroll
-  for (int ot = 0; ot < 3; ++ot) {
-    f = fma(c.A[ot][0], t0[ot], fma(c.A[ot][1], t1[ot], f));
-    fT = fma(c.A[ot][0], d0[ot], fma(c.A[ot][1], d1[ot], fT));
-    fTT = fma(c.A[ot][0], e0[ot], fma(c.A[ot][1], e1[ot], fTT));
-  }
+  double d1, d2h;
+  poly5_eval(c.c, (T - c.T0) * idT, f, d1, d2h);
+  fT = d1 * idT;
+  fTT = 2.0 * d2h * (idT * idT);
 }
 
 // Newton on E(rho, T) = E0 from T (helm_rhoe_given's loop and exit rules); an iterate outside
@@ -179,12 +191,17 @@ __device__ __forceinline__ int helm_rhoe_fast_from(const HelmTable &h, HelmCell 
     if (T < c.T0 || T >= c.T0 + c.dT) helm_cell_contract(h, c, helm_node_index(h.T, h.nT, h.log10_T1, h.dT, T));
     double f, fT, fTT;
     helm_cell_eval(c, T, f, fT, fTT);
-    double T3 = T * T * T;
-    double E = c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T3 * T * irho;
-    double dE = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
-    double res = E - E0;
-    T = T - res / dE;
-    double error = fabs(res * inv_E0);
+    // every operation spelled out (no contraction left to the compiler), so that the solve is
+    // the same bit for bit wherever it is inlined and however its iterations are split
+    const double T3 = __dmul_rn(__dmul_rn(T, T), T);
+    const double ion = __dmul_rn(__dmul_rn(1.5 * CONST_RGAS, T), inv_abar);
+    const double rad = __dmul_rn(__dmul_rn(CONST_RAD, __dmul_rn(T3, T)), irho);
+    const double E = __fma_rn(c.Ye, __fma_rn(-T, fT, f), __dadd_rn(ion, rad));
+    const double dE = __fma_rn(-__dmul_rn(c.Ye, T), fTT,
+                               __dadd_rn(__dmul_rn(1.5 * CONST_RGAS, inv_abar), __dmul_rn(__dmul_rn(4.0 * CONST_RAD, T3), irho)));
+    const double res = __dsub_rn(E, E0);
+    T = __dsub_rn(T, __ddiv_rn(res, dE));
+    double error = fabs(__dmul_rn(res, inv_E0));
     if ((T < h.Tl) || (T > h.Th)) {
       T = Told;
       error = EM15;
@@ -209,31 +226,19 @@ __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const Hel
                                                    double T, double inv_abar, double &P, double &sound2,
                                                    double *E_out = nullptr) {
   const double idT = c.idT;
-  double y = (T - c.T0) * idT, omy = 1.0 - y;
-  double t0[3], t1[3], d0[3], d1[3], e0[3], e1[3];
-  fhb0(y, c.dT, c.dT * c.dT, t0);
-  fhb0m(omy, c.dT, c.dT * c.dT, t1);
-  fhb1(y, idT, c.dT, d0);
-  fhb1m(omy, idT, c.dT, d1);
-  fhb2(y, idT * idT, idT, e0);
-  fhb2m(omy, idT * idT, idT, e1);
-  // d/drho contraction of the final cell
-  double B[3][2];
+  const double y = (T - c.T0) * idT, omy = 1.0 - y;
+  double f, fT, fTT, fd, fdT;
+  helm_cell_eval(c, T, f, fT, fTT);
+  // d/drho contraction of the final cell, as a quintic in y
   {
     const double idrho = __ldg(h.inv_drho + c.ih - 1);
-    double dr0[3], dr1[3];
+    double dr0[3], dr1[3], B[3][2], q[6], d2h;
     fhb1(c.x, idrho, c.drho, dr0);
     fhb1m(1.0 - c.x, idrho, c.drho, dr1);
     helm_cell_contract_with(h, c, c.jh, dr0, dr1, B);
-  }
-  double f = 0, fT = 0, fTT = 0, fd = 0, fdT = 0;
-#pragma unroll
-  for (int ot = 0; ot < 3; ++ot) {
-    f = fma(c.A[ot][0], t0[ot], fma(c.A[ot][1], t1[ot], f));
-    fT = fma(c.A[ot][0], d0[ot], fma(c.A[ot][1], d1[ot], fT));
-    fTT = fma(c.A[ot][0], e0[ot], fma(c.A[ot][1], e1[ot], fTT));
-    fd = fma(B[ot][0], t0[ot], fma(B[ot][1], t1[ot], fd));
-    fdT = fma(B[ot][0], d0[ot], fma(B[ot][1], d1[ot], fdT));
+    helm_hermite_poly(B, c.dT, q);
+    poly5_eval(q, y, fd, fdT, d2h);
+    fdT *= idT;
   }
   // bicubic dP/d(rho Ye) (source.F90:24082-24118)
   double x = c.x, omx = 1.0 - x;
@@ -286,7 +291,7 @@ __device__ __forceinline__ int helm_rhoP_fast(const HelmTable &h, HelmCell &c, d
     fhb1m(1.0 - c.x, idrho, c.drho, dr1);
   }
   int jh = -1;
-  double T0 = 0.0, dT = 0.0, idT = 0.0;
+  double T0 = 0.0, dT = 0.0, idT = 0.0, q[6];
   int used = 0;
   for (int iter = 1; iter <= 100; ++iter) {
     used = iter;
@@ -296,19 +301,11 @@ __device__ __forceinline__ int helm_rhoP_fast(const HelmTable &h, HelmCell &c, d
       dT = __ldg(h.T + jh) - T0;
       idT = __ldg(h.inv_dT + jh - 1);
       helm_cell_contract_with(h, c, jh, dr0, dr1, B);
+      helm_hermite_poly(B, dT, q);
     }
-    const double y = (T - T0) * idT, omy = 1.0 - y;
-    double t0[3], t1[3], d0[3], d1[3];
-    fhb0(y, dT, dT * dT, t0);
-    fhb0m(omy, dT, dT * dT, t1);
-    fhb1(y, idT, dT, d0);
-    fhb1m(omy, idT, dT, d1);
-    double fd = 0.0, fdT = 0.0;
-#pragma unroll
-    for (int ot = 0; ot < 3; ++ot) {
-      fd = fma(B[ot][0], t0[ot], fma(B[ot][1], t1[ot], fd));
-      fdT = fma(B[ot][0], d0[ot], fma(B[ot][1], d1[ot], fdT));
-    }
+    double fd, fdT, d2h;
+    poly5_eval(q, (T - T0) * idT, fd, fdT, d2h);
+    fdT *= idT;
     const double T3 = T * T * T;
     const double P = r2 * fd + CONST_RGAS * rho * T * inv_abar + CONST_RAD * T3 * T * (1.0 / 3.0);
     const double dP = r2 * fdT + CONST_RGAS * rho * inv_abar + (4.0 / 3.0) * CONST_RAD * T3;

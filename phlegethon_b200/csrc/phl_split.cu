@@ -2294,11 +2294,12 @@ struct SplitRunnerT : Runner {
     out = e.maps;
     return e.ok;
   }
-  // PHL_C2P_MINB=7 compiles the Helmholtz MHD cons->prim for 7 resident blocks per SM (72
-  // registers) instead of 6 (80)
+  // resident blocks per SM the Helmholtz MHD cons->prim is compiled for: 7 (72 registers, a few
+  // spills), which ran 2% faster per step at 256^3 than 6 (80 registers) since the Newton's
+  // arithmetic is spelled out; PHL_C2P_MINB=6 selects the 80-register build (comparison)
   const int c2p_minb = [] {
     const char *e = getenv("PHL_C2P_MINB");
-    return e ? atoi(e) : 0;
+    return e && atoi(e) == 6 ? 6 : 7;
   }();
   // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
   const bool c2p_two = [] {
@@ -2396,7 +2397,7 @@ struct SplitRunnerT : Runner {
         if (P.mlp_w && P.mlp_small && P.rescue_q) {
           // warm start everywhere; cells with a poor warm start through the learned guess
           cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
-          if (c2p_minb == 7)
+          if (C::HELM && c2p_minb == 7)
             k_c2p_mhd_split<C, C2P_RESCUE, 7><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
           else
             k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
