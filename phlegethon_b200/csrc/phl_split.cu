@@ -1614,24 +1614,14 @@ __device__ __forceinline__ float emf_cell_split(const Prm &P, int a, int i, int 
   return flip ? -e : e;
 }
 
-// corner EMF along axis A (source.F90:11966-12206), FP32; one thread per corner (one
-// instantiation per axis: the face and cell strides fold into constants)
-template <class C, int A>
-__global__ void __launch_bounds__(256) k_corner_split(Prm P) {
+// corner EMF along axis A (source.F90:11966-12206), FP32, at corner (c[0], c[1], c[2]); INTERIOR:
+// all four faces and cells lie inside the domain (linear indices, no wrap or mirror)
+template <class C, int A, bool INTERIOR>
+__device__ __forceinline__ float corner_emf_split(const Prm &P, const int c[3]) {
   constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
-  if (!*P.active) return;
   const Geo &g = P.g;
-  int n0 = g.nx[0] + (a != 0), n1 = g.nx[1] + (a != 1), n2 = C::DIM == 3 ? g.nx[2] + (a != 2) : 1;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)n0 * n1 * n2) return;
-  int c[3];
-  unflatten3(t, n0, n1, c[0], c[1], c[2]);
-  int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
-  int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
-  int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
   float emf_N, emf_E, emf_S, emf_W, sgS, sgN, sgW, sgE, emf_SW, emf_NW, emf_NE, emf_SE;
-  if (c[pa] >= 1 && c[pa] < g.nx[pa] && c[qa] >= 1 && c[qa] < g.nx[qa]) {
-    // all four faces and cells inside the domain: linear indices, no wrap or mirror
+  if (INTERIOR) {
     const long long fp = face_lin(g, pa, c[0], c[1], c[2]), fq = face_lin(g, qa, c[0], c[1], c[2]);
     const int p0 = g.nx[0] + (pa == 0), p1 = g.nx[1] + (pa == 1);  // face array of pa
     const int q0 = g.nx[0] + (qa == 0), q1 = g.nx[1] + (qa == 1);  // face array of qa
@@ -1651,6 +1641,9 @@ __global__ void __launch_bounds__(256) k_corner_split(Prm P) {
     emf_SE = __ldg(ec + cc - cq);
     emf_SW = __ldg(ec + cc - cp - cq);
   } else {
+    int cqm[3] = {c[0], c[1], c[2]}; cqm[qa] -= 1;
+    int cpm[3] = {c[0], c[1], c[2]}; cpm[pa] -= 1;
+    int cpq[3] = {c[0], c[1], c[2]}; cpq[pa] -= 1; cpq[qa] -= 1;
     face_emf_split_at<C>(P, pa, a, c[0], c[1], c[2], emf_N, sgN);
     face_emf_split_at<C>(P, qa, a, c[0], c[1], c[2], emf_E, sgE);
     face_emf_split_at<C>(P, pa, a, cqm[0], cqm[1], cqm[2], emf_S, sgS);
@@ -1668,7 +1661,52 @@ __global__ void __launch_bounds__(256) k_corner_split(Prm P) {
   float demf_W = 0.5f * (1.0f + sgn) * (emf_S - emf_SW) + 0.5f * (1.0f - sgn) * (emf_N - emf_NW);
   sgn = sgE;
   float demf_E = 0.5f * (1.0f + sgn) * (emf_SE - emf_S) + 0.5f * (1.0f - sgn) * (emf_NE - emf_N);
-  P.fcor[a][t] = 0.25f * (emf_S + emf_W + emf_N + emf_E + demf_S - demf_N + demf_W - demf_E);
+  return 0.25f * (emf_S + emf_W + emf_N + emf_E + demf_S - demf_N + demf_W - demf_E);
+}
+
+// Corner EMFs along axis A, one thread per corner, in two launches (one instantiation per
+// axis: the face and cell strides fold into constants): the interior corners (1 <= c[pa] <
+// nx[pa], 1 <= c[qa] < nx[qa]) read their faces and cells by linear index with no branch, the
+// corners on the domain faces of pa and qa map their ghost indices; a single launch over all
+// corners had a quarter of its warps diverge into the mapping path where the rows of corners
+// (nx + 1 long) straddle the warps.
+template <class C, int A>
+__global__ void __launch_bounds__(256) k_corner_split(Prm P) {
+  constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  // interior extents per dimension (x1 fastest, as the arrays): nx - 1 from index 1 along pa
+  // and qa, nx from index 0 along a
+  const int e0 = a == 0 ? g.nx[0] : g.nx[0] - 1, e1 = a == 1 ? g.nx[1] : g.nx[1] - 1;
+  const int e2 = C::DIM == 3 ? (a == 2 ? g.nx[2] : g.nx[2] - 1) : 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)e0 * e1 * e2) return;
+  int c[3];
+  unflatten3(t, e0, e1, c[0], c[1], c[2]);
+  c[0] += a != 0;
+  c[1] += a != 1;
+  if (C::DIM == 3) c[2] += a != 2;
+  P.fcor[a][cor_lin(g, a, c[0], c[1], c[2])] = corner_emf_split<C, A, true>(P, c);
+}
+
+// the corners on the domain faces of pa and qa: per index along a, the rim of the
+// (nx[pa] + 1) x (nx[qa] + 1) rectangle of corners, 2 (nx[pa] + nx[qa]) of them
+template <class C, int A>
+__global__ void __launch_bounds__(256) k_corner_split_rim(Prm P) {
+  constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
+  if (!*P.active) return;
+  const Geo &g = P.g;
+  const int np_ = g.nx[pa], nq = g.nx[qa], na = C::DIM == 3 ? g.nx[a] : 1, rim = 2 * (np_ + nq);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)rim * na) return;
+  const int m = (int)(t % rim);
+  int c[3];
+  c[a] = (int)(t / rim);
+  if (m < np_ + 1) { c[pa] = m; c[qa] = 0; }                             // qa = 0 row
+  else if (m < 2 * (np_ + 1)) { c[pa] = m - (np_ + 1); c[qa] = nq; }       // qa = nx[qa] row
+  else if (m < 2 * (np_ + 1) + (nq - 1)) { c[pa] = 0; c[qa] = m - 2 * (np_ + 1) + 1; }  // pa = 0 column
+  else { c[pa] = np_; c[qa] = m - 2 * (np_ + 1) - (nq - 1) + 1; }         // pa = nx[pa] column
+  P.fcor[a][cor_lin(g, a, c[0], c[1], c[2])] = corner_emf_split<C, A, false>(P, c);
 }
 
 // face-B update (source.F90:12208-12437) in FP64 from the FP32 corner EMFs; one thread per face
@@ -2362,9 +2400,6 @@ struct SplitRunnerT : Runner {
       auto nfc = [&](int d) {
         return (long long)(g.nx[0] + (d == 0)) * (g.nx[1] + (d == 1)) * (g.nx[2] + (d == 2));
       };
-      auto ncor = [&](int a) {
-        return (long long)(g.nx[0] + (a != 0)) * (g.nx[1] + (a != 1)) * (C::DIM == 3 ? g.nx[2] + (a != 2) : 1);
-      };
       if constexpr (C::REC == REC_LIM2ND) {
         // threads of the walking kernels: faces along D in chunks of K, times the other extents
         auto nwalk = [&](int d, int k) {
@@ -2386,10 +2421,10 @@ struct SplitRunnerT : Runner {
         if constexpr (C::DIM == 3) k_face_split_mhd<C, 2><<<nblk(nfc(2), 128), 128, 0, s>>>(P);
       }
       if constexpr (C::DIM == 3) {
-        k_corner_split<C, 0><<<nblk(ncor(0), 256), 256, 0, s>>>(P);
-        k_corner_split<C, 1><<<nblk(ncor(1), 256), 256, 0, s>>>(P);
+        corners<0>(P, s);
+        corners<1>(P, s);
       }
-      k_corner_split<C, 2><<<nblk(ncor(2), 256), 256, 0, s>>>(P);
+      corners<2>(P, s);
       k_bface_split<C, 0><<<nblk(nfc(0), 256), 256, 0, s>>>(P);
       k_bface_split<C, 1><<<nblk(nfc(1), 256), 256, 0, s>>>(P);
       if constexpr (C::DIM == 3) k_bface_split<C, 2><<<nblk(nfc(2), 256), 256, 0, s>>>(P);
@@ -2423,6 +2458,17 @@ struct SplitRunnerT : Runner {
     } else {
       hydro_stage(P, s);
     }
+  }
+  // corner EMFs along axis A: interior corners, then the rim on the domain faces
+  template <int A>
+  void corners(const Prm &P, cudaStream_t s) {
+    constexpr int pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
+    const Geo &g = P.g;
+    const long long na = C::DIM == 3 ? g.nx[A] : 1;
+    const long long nin = (long long)(g.nx[pa] - 1) * (g.nx[qa] - 1) * na;
+    const long long nrim = 2ll * (g.nx[pa] + g.nx[qa]) * na;
+    if (nin > 0) k_corner_split<C, A><<<nblk(nin, 256), 256, 0, s>>>(P);
+    k_corner_split_rim<C, A><<<nblk(nrim, 256), 256, 0, s>>>(P);
   }
   void hydro_stage(const Prm &P, cudaStream_t s) {
     if constexpr (C::DIM == 3 && C::SW == 2) {

@@ -10,6 +10,15 @@ equations, independent of any restatement of the reference.
   along x1 in a 3D box with HLLD and constrained transport: the transverse B and v come back in
   phase with second-order convergence, without exciting compressive motion, and div B stays at
   rounding.
+* A stationary contact discontinuity (density jump at uniform pressure and zero velocity; with B
+  uniform for MHD) is an exact steady solution that the contact-resolving solvers (HLLC and
+  LHLLC, HLLD and LHLLD) keep without diffusing it: the mass flux through every face is zero.
+* A linear sound wave travels one period at the sound speed: the convergence rate of the
+  density's L1 error shows the order of each reconstruction.  LIM2ND_REC sets the edge values
+  to q -+ slope / 2 with slope = df db / (df + db) (source.F90:8141-8181): half the van Leer
+  slope, so on smooth data the scheme is first order (the error halves per doubling); PPH_REC
+  and LIM5TH_REC converge faster than second order until their extremum limiters and the
+  third-order Runge-Kutta stepper set the rate.
 """
 import math
 
@@ -209,6 +218,87 @@ def test_alfven_wave_returns_after_one_period(oracle, riemann):
     assert abs(va3 - a3) < 0.02, res
 
 
+# ------------------------------------------------------------------------------ stationary contact
+def stationary_contact(n, riemann, mhd=False):
+    """rho = 1 in 0.25 < x < 0.75 and 0.125 elsewhere (periodic), p = 1, v = 0; MHD: B = (0.75, 0.5)
+    uniform, so the total pressure is uniform too."""
+    cfg = Config(sdims=2, nx1=n, nx2=4, nx3=1, ngc=2, nas=0, riemann=riemann, rk_stages=3, mhd=mhd,
+                 bc=[["periodic", "periodic"]] * 3, x1l=0.0, x1u=1.0, x2l=0.0, x2u=4.0 / n, x3l=0.0, x3u=1.0,
+                 gamma_ad=1.4, mu=1.0, cfl=0.8, mach_cutoff=1e-4, mach_ct=1e-6)
+    h = HostGrid(cfg)
+    x, _, _ = h.coords()
+    h.prim[0] = np.where((x > 0.25) & (x < 0.75), 1.0, 0.125)
+    h.prim[1] = 0.0
+    h.prim[2] = 0.0
+    h.prim[3] = 1.0
+    h.temp[...] = h.prim[3] / h.prim[0]
+    if mhd:
+        h.b_x[0][...] = 0.75
+        h.b_x[1][...] = 0.5
+    return cfg, h
+
+
+@pytest.mark.parametrize("riemann,mhd", [("hllc", False), ("lhllc", False), ("hlld", True), ("lhlld", True)])
+def test_stationary_contact_is_kept(oracle, riemann, mhd):
+    """50 steps: density and pressure unchanged bit for bit, the velocity at rounding (LHLLD forms
+    its star total pressure as a weighted mean of the two equal sides, which rounds)."""
+    cfg, h = stationary_contact(64, riemann, mhd)
+    w0 = h.interior(h.prim).copy()
+    o = oracle.OracleGrid(h, None)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(50)
+    w = h.interior(h.prim)
+    assert np.array_equal(w[0], w0[0]) and np.array_equal(w[3], w0[3])
+    assert float(np.abs(w[1:3]).max()) <= 1e-14
+
+
+# ------------------------------------------------------------------------------ sound wave
+SOUND_EPS = 1e-6
+
+
+def sound_wave(n, rec="lim2nd", riemann="hllc"):
+    """Linear sound wave rho = 1 + eps sin 2 pi x, v = c eps sin 2 pi x, p = 1 + gamma eps sin 2 pi x
+    (gamma = 1.4, c = sqrt(1.4)); it returns in place after t = 1 / c."""
+    g = 1.4
+    cfg = Config(sdims=2, nx1=n, nx2=4, nx3=1, ngc=3 if rec == "lim5th" else 2, nas=0, riemann=riemann, rk_stages=3,
+                 rec=rec, bc=[["periodic", "periodic"]] * 3, x1l=0.0, x1u=1.0, x2l=0.0, x2u=4.0 / n, x3l=0.0,
+                 x3u=1.0, gamma_ad=g, mu=1.0, cfl=0.8, mach_cutoff=1e-4)
+    h = HostGrid(cfg)
+    x, _, _ = h.coords()
+    s = np.sin(2 * np.pi * x)
+    h.prim[0] = 1.0 + SOUND_EPS * s
+    h.prim[1] = math.sqrt(g) * SOUND_EPS * s
+    h.prim[2] = 0.0
+    h.prim[3] = 1.0 + g * SOUND_EPS * s
+    h.temp[...] = h.prim[3] / h.prim[0]
+    return cfg, h
+
+
+def sound_wave_error(oracle, n, rec):
+    """L1 error of the density after one period against the exact cell averages, over eps."""
+    cfg, h = sound_wave(n, rec)
+    run_oracle(oracle, cfg, h, 1.0 / math.sqrt(1.4))
+    x, _, _ = h.coords()
+    xs = h.interior(x)[:, 0, 0]
+    k = 2.0 * np.pi
+    exact = 1.0 + SOUND_EPS * (np.cos(k * (xs - 0.5 / n)) - np.cos(k * (xs + 0.5 / n))) / (k / n)
+    return float(np.mean(np.abs(h.interior(h.prim)[0][:, 0, 0] - exact))) / SOUND_EPS
+
+
+def test_sound_wave_convergence_by_reconstruction(oracle):
+    e2 = [sound_wave_error(oracle, n, "lim2nd") for n in (32, 64, 128)]
+    # LIM2ND: first order (measured 0.170, 0.091, 0.047: rates 0.90, 0.95)
+    r2 = [math.log2(e2[i] / e2[i + 1]) for i in range(2)]
+    assert all(0.8 < r < 1.2 for r in r2) and 0.1 < e2[0] < 0.25, (e2, r2)
+    # PPH and LIM5TH: at 64 cells over 10x below LIM2ND, above second order from 16 to 64 cells
+    # (measured PPH 0.0160, 0.00157, 7.0e-5; LIM5TH 0.040, 0.0075, 0.0015)
+    for rec in ("pph", "lim5th"):
+        e = [sound_wave_error(oracle, n, rec) for n in (16, 32, 64)]
+        rate = math.log2(e[0] / e[2]) / 2
+        assert e[2] < 0.1 * e2[1] and rate > 2.2, (rec, e, rate)
+
+
 # ------------------------------------------------------------------------------ the CUDA forms
 def run_gpu(cfg, h, tmax, precision):
     from phlegethon_b200.abi import Simulation
@@ -244,3 +334,25 @@ def test_alfven_wave_on_the_gpu(gpu_lib, precision):
     amp, ph = fit_wave(h.bface_interior(1)[:, 0, 0], n)
     assert abs(ph) < 2e-3 and amp / ALFVEN_AMP > 0.9, (amp, ph)
     assert div_b_max(h) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("riemann,mhd", [("lhllc", False), ("lhlld", True)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_stationary_contact_on_the_gpu(gpu_lib, riemann, mhd, precision):
+    cfg, h = stationary_contact(64, riemann, mhd)
+    w0 = h.interior(h.prim).copy()
+    from phlegethon_b200.abi import Simulation
+    with Simulation(cfg.replace(precision=precision)) as sim:
+        sim.upload(h)
+        sim.init_thermo()
+        sim.compute_hyperbolic_dt()
+        done, _ = sim.time_loop(50)
+        sim.download(h)
+    assert done == 50
+    w = h.interior(h.prim)
+    # FP64: the oracle's answer (density and pressure bit for bit); FP32 split: the FP32 state
+    # carries the jump exactly and the fluxes vanish, so the same holds to FP32 rounding
+    tol = 0.0 if precision == "fp64" else 1e-7
+    assert float(np.abs(w[0] - w0[0]).max()) <= tol and float(np.abs(w[3] - w0[3]).max()) <= tol
+    assert float(np.abs(w[1:3]).max()) <= (1e-14 if precision == "fp64" else 1e-7)
