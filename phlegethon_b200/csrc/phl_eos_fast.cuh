@@ -267,11 +267,12 @@ __device__ __forceinline__ void helm_cell_p_sound2(const HelmTable &h, const Hel
   double E = c.Ye * (f - T * fT) + 1.5 * CONST_RGAS * T * inv_abar + CONST_RAD * T4 * irho;
   double cv = -c.Ye * T * fTT + 1.5 * CONST_RGAS * inv_abar + 4.0 * CONST_RAD * T3 * irho;
   // the reference's gam1 / z (chiT = T dP/dT / P, chirho = rho dP/drho / P, x = (P / rho) chiT /
-  // (T cv), gam1 = chiT x + chirho, z = 1 + (E + c^2) rho / P) with the common factor 1 / P
-  // cancelled: two divisions instead of five
-  const double num = T * dP_dT * dP_dT / (rho * cv) + rho * dP_drho;
+  // (T cv), gam1 = chiT x + chirho, z = 1 + (E + c^2) rho / P) with the common factors 1 / P
+  // and 1 / (rho cv) cancelled: one division instead of five
+  const double rcv = rho * cv;
+  const double num = T * dP_dT * dP_dT + rcv * (rho * dP_drho);
   const double den = P + (E + CONST_C2) * rho;
-  sound2 = CONST_C2 * (num / den);
+  sound2 = CONST_C2 * num / (rcv * den);
   if (E_out) *E_out = E;
 }
 

@@ -205,9 +205,10 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
   float a2L = 2.0f * pbL * inv_rhoL, a2R = 2.0f * pbR * inv_rhoR;
   float an2L = bx1_2 * inv_rhoL, an2R = bx1_2 * inv_rhoR;
   float dummy = c2L + a2L;
-  float cL = sqrtf(0.5f * (c2L + a2L + sqrtf(fmaxf(dummy * dummy - 4.0f * c2L * an2L, 0.0f))));
+  const float cf2L = 0.5f * (c2L + a2L + sqrtf(fmaxf(dummy * dummy - 4.0f * c2L * an2L, 0.0f)));
   dummy = c2R + a2R;
-  float cR = sqrtf(0.5f * (c2R + a2R + sqrtf(fmaxf(dummy * dummy - 4.0f * c2R * an2R, 0.0f))));
+  const float cf2R = 0.5f * (c2R + a2R + sqrtf(fmaxf(dummy * dummy - 4.0f * c2R * an2R, 0.0f)));
+  float cL = sqrtf(cf2L), cR = sqrtf(cf2R);
   float max_c = fmaxf(cL, cR);
   float sL = fminf(vx1L, vx1R) - max_c;
   float sR = fmaxf(vx1L, vx1R) + max_c;
@@ -221,10 +222,10 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
     float cu2L = 0.5f * (v2L + a2L + sqrtf(fmaxf(dummy * dummy - 4.0f * v2L * an2L, 0.0f)));
     dummy = v2R + a2R;
     float cu2R = 0.5f * (v2R + a2R + sqrtf(fmaxf(dummy * dummy - 4.0f * v2R * an2R, 0.0f)));
-    float machL = sqrtf(cu2L) / cL, machR = sqrtf(cu2R) / cR;
-    float mm = fmaxf(machL, machR);
-    if (mm < 0.6f) {
-      float chi = fminf(1.0f, fmaxf(machL, machR));
+    // the fast Mach numbers compared as squares (cu^2 / cf^2): one square root, for the larger
+    const float mm2 = fmaxf(cu2L / cf2L, cu2R / cf2R);
+    if (mm2 < 0.36f) {
+      float chi = fminf(1.0f, sqrtf(mm2));
       chi = fmaxf(mach_cutoff, chi);
       phi = chi * (2.0f - chi);
     }
@@ -263,7 +264,8 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
   // star total pressure: the weights sum to one, so pe factors out
   float pstar_d = (dsuR * rhoR * ptLd - dsuL * rhoL * ptRd - phi * rhoL * rhoR * dsuR * dsuL * (vx1L - vx1R)) *
                   inv_temp1;
-  float rhostarL = rhoL * dsuL / dsumL, rhostarR = rhoR * dsuR / dsumR;
+  const float idsumL = 1.0f / dsumL, idsumR = 1.0f / dsumR;
+  float rhostarL = rhoL * dsuL * idsumL, rhostarR = rhoR * dsuR * idsumR;
   float a1_inv = 1.0f / (rhoL * dsuL * dsumL - bx1_2);
   float vx2starL = vx2L - bx1 * bx2L * (ustar - vx1L) * a1_inv;
   float bx2starL = bx2L * (rhoL * dsuL * dsuL - bx1_2) * a1_inv;
@@ -280,13 +282,15 @@ __device__ __forceinline__ void riemann_mhd_split(const float *qL, const float *
   float vdotbstarR = ustar * bx1 + vx2starR * bx2starR + vx3starR * bx3starR;
   // -pT u + pT* u* with pe factored: pe (u* - u) + (pT*' u* - pT' u)
   float rhoestarL = (dsuL * rhoeL + pe * (ustar - vx1L) + (pstar_d * ustar - ptLd * vx1L) +
-                     bx1 * (vdotbL - vdotbstarL)) / dsumL;
+                     bx1 * (vdotbL - vdotbstarL)) * idsumL;
   float rhoestarR = (dsuR * rhoeR + pe * (ustar - vx1R) + (pstar_d * ustar - ptRd * vx1R) +
-                     bx1 * (vdotbR - vdotbstarR)) / dsumR;
-  float sqrt_rhostarL = sqrtf(rhostarL), sqrt_rhostarR = sqrtf(rhostarR);
+                     bx1 * (vdotbR - vdotbstarR)) * idsumR;
+  // sqrt(rho*) and 1 / sqrt(rho*) from one reciprocal square root per side
+  const float rsqL = rsqrtf(rhostarL), rsqR = rsqrtf(rhostarR);
+  float sqrt_rhostarL = rhostarL * rsqL, sqrt_rhostarR = rhostarR * rsqR;
   float abs_bx1 = fabsf(bx1);
-  float sstarL = ustar - abs_bx1 / sqrt_rhostarL;
-  float sstarR = ustar + abs_bx1 / sqrt_rhostarR;
+  float sstarL = ustar - abs_bx1 * rsqL;
+  float sstarR = ustar + abs_bx1 * rsqR;
   float inv_sqr_bar = 1.0f / (sqrt_rhostarL + sqrt_rhostarR);
   float sgn = copysignf(1.0f, bx1);
   float vx22star = (sqrt_rhostarL * vx2starL + sqrt_rhostarR * vx2starR + (bx2starR - bx2starL) * sgn) * inv_sqr_bar;
@@ -686,10 +690,12 @@ __device__ __forceinline__ void split_cell_update(const Prm &P, long long c, int
     helm_cell_p_sound2(P.helm, hc, rho, inv_rho, T, inv_abar, p, sound2);
     if (P.last_stage) sound = sqrt(sound2);
     if (C::FAST) {
-      double ge = p / eint + 1.0, gc = sound2 * rho / p;
+      // gamma_e to FP32 as a deviation from equilibrium (formed in FP64), gamma_c to FP32 as it is
+      double ge = p / eint + 1.0;
+      const float gc = (float)(sound2 * rho) / (float)p;
       if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
       P.gf_out[c] = (float)ge;
-      P.gf_out[g.N + c] = (float)gc;
+      P.gf_out[g.N + c] = gc;
     } else {
       P.gf_out[c] = (float)T;
     }
@@ -1924,10 +1930,13 @@ __device__ __forceinline__ bool c2p_mhd_split_eos(const Prm &P, long long c, con
       st.calls += 1; st.iters += it; st.nonconv += !conv; st.clamp += clamped;
       helm_cell_p_sound2(P.helm, hc, rho, inv_rho, T, inv_abar, p, sound2);
       if (C::FAST) {
-        double ge = p / eint + 1.0, gc = sound2 * rho / p;
+        // gamma_e goes to FP32 as a deviation from its equilibrium value, so it is formed in FP64;
+        // gamma_c is stored as it is, to FP32 precision
+        double ge = p / eint + 1.0;
+        const float gc = (float)(sound2 * rho) / (float)p;
         if (C::WB) ge = ge - __ldg(P.eq_ge_cc + bc);
         P.gf_out[c] = (float)ge;
-        P.gf_out[g.N + c] = (float)gc;
+        P.gf_out[g.N + c] = gc;
       } else {
         P.gf_out[c] = (float)T;
       }
