@@ -1272,8 +1272,9 @@ constexpr int WALK_K0 = 4, WALK_K = 8;
 constexpr int C2P_EOS_MINB = 7;
 // grid of the rescue-queue kernels: 4 blocks of 128 threads per SM of a B200 (148 SMs)
 constexpr int RESCUE_BLOCKS = 4 * 148;
-// resident blocks of 128 threads per SM the walking kernels are compiled for
-constexpr int WALK_MINB = 6;
+// resident blocks of 128 threads per SM the walking kernels are compiled for (72 registers; the
+// 256^3 MHD stage took 4.46 ms at 7 against 4.53 at 6 and 4.50 at 8)
+constexpr int WALK_MINB = 7;
 
 // Raw values of one cell for the walking face kernel along D: the FP32 state (0 .. NV-1), the
 // cell B components transverse to D (NBT of them from NV on; the component along D is not
@@ -2341,12 +2342,13 @@ struct SplitRunnerT : Runner {
     out = e.maps;
     return e.ok;
   }
-  // resident blocks per SM the Helmholtz MHD cons->prim is compiled for: 7 (72 registers, a few
-  // spills), which ran 2% faster per step at 256^3 than 6 (80 registers) since the Newton's
-  // arithmetic is spelled out; PHL_C2P_MINB=6 selects the 80-register build (comparison)
+  // resident blocks per SM the Helmholtz MHD cons->prim is compiled for: 8 (64 registers, ~100
+  // B of spills), which ran a step at 256^3 in 13.56 ms against 13.89 at 7 (72 registers), 14.37
+  // at 6 (80), 13.73 at 9 and 14.14 at 10: its time is latency, and more resident warps hide it
+  // until the spills dominate; PHL_C2P_MINB=6 selects the 80-register build (comparison)
   const int c2p_minb = [] {
     const char *e = getenv("PHL_C2P_MINB");
-    return e && atoi(e) == 6 ? 6 : 7;
+    return e && atoi(e) == 6 ? 6 : 8;
   }();
   // PHL_C2P=two runs the warm-start cons->prim of the MHD stage as two launches
   const bool c2p_two = [] {
@@ -2441,8 +2443,8 @@ struct SplitRunnerT : Runner {
         if (P.mlp_w && P.mlp_small && P.rescue_q) {
           // warm start everywhere; cells with a poor warm start through the learned guess
           cudaMemsetAsync(P.rescue_q, 0, sizeof(unsigned), s);
-          if (C::HELM && c2p_minb == 7)
-            k_c2p_mhd_split<C, C2P_RESCUE, 7><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
+          if (C::HELM && c2p_minb == 8)
+            k_c2p_mhd_split<C, C2P_RESCUE, 8><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
           else
             k_c2p_mhd_split<C, C2P_RESCUE><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
           k_c2p_rescue<C><<<RESCUE_BLOCKS, 128, sizeof(MlpUmmaSmem), s>>>(P, *P.mlp_small);
@@ -2459,8 +2461,8 @@ struct SplitRunnerT : Runner {
       if (c2p_two) {
         k_c2p_mhd_split_combine<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
         k_c2p_mhd_split_eos<C><<<nblk(g.N, 128), 128, 0, s>>>(P);
-      } else if (C::HELM && c2p_minb == 7) {
-        k_c2p_mhd_split<C, C2P_WARM, 7><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
+      } else if (C::HELM && c2p_minb == 8) {
+        k_c2p_mhd_split<C, C2P_WARM, 8><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
       } else {
         k_c2p_mhd_split<C, C2P_WARM><<<nblk(g.N, C2P_BLOCK), C2P_BLOCK, 0, s>>>(P);
       }
