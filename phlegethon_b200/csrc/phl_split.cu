@@ -1452,38 +1452,29 @@ __global__ void __launch_bounds__(FaceTileSmem<C, D>::NT, FaceTile<D>::MINB)
   constexpr int NV = C::NV, NE = S_::NE, NED = S_::NEDGE, TT = S_::TT, SX = S_::SX, SY = S_::SY, SC = S_::SC;
   const Geo &g = P.g;
   const int t = threadIdx.x;
-  if ((int)blockIdx.x >= ntiles) {
-    // tail: the faces at the upper domain boundary along D, one per thread
-    const long long q = (long long)(blockIdx.x - ntiles) * S_::NT + t;
-    const int e0 = D == 0 ? g.nx[1] : g.nx[0], e1 = D == 2 ? g.nx[1] : (C::DIM == 3 ? g.nx[2] : 1);
-    if (q >= (long long)e0 * e1) return;
-    const int a = (int)(q % e0), c = (int)(q / e0);
-    const int fi = D == 0 ? g.nx[0] : a, fj = D == 0 ? a : (D == 1 ? g.nx[1] : c), fk = D == 2 ? g.nx[2] : c;
-    face_split_mhd_at<C, D>(P, face_lin(g, D, fi, fj, fk));
-    return;
-  }
   __shared__ __align__(128) S_ S;
   const int nbx = g.nx[0] / T::TX, nby = g.nx[1] / T::TY;
-  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
-  const int i0 = bx * T::TX, j0 = by * T::TY, k0 = bz * T::TZ;
   const int tx = t % T::TX, ty = (t / T::TX) % T::TY, tz = t / (T::TX * T::TY);
   const int td = D == 0 ? tx : (D == 1 ? ty : tz);
   const int col = D == 0 ? ty + T::TY * tz : (D == 1 ? tx + T::TX * tz : tx + T::TX * ty);  // < TT
-  const int c0 = D == 0 ? i0 : (D == 1 ? j0 : k0), nD = g.nx[D];
-  if (t == 0) mbar_init(&S.mbar, 1);
-  __syncthreads();
-  if (t == 0) {
+  const int nD = g.nx[D];
+  // origin of tile `tile`
+  auto origin = [&](int tile, int &i0, int &j0, int &k0) {
+    i0 = (tile % nbx) * T::TX;
+    j0 = ((tile / nbx) % nby) * T::TY;
+    k0 = (tile / (nbx * nby)) * T::TZ;
+  };
+  // one thread: the bulk tensor copies of a tile into the staging area, counted on the mbarrier
+  // (the fence orders the generic-proxy reads and writes of the previous tile before the copy)
+  auto issue = [&](int tile) {
+    int i0, j0, k0;
+    origin(tile, i0, j0, k0);
+    fence_proxy_async_smem();
     mbar_arrive_expect_tx(&S.mbar, S_::BYTES);
     tma_load_4d(S.w, &maps.w, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
     tma_load_4d(S.b, &maps.b, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
     if (S_::STAGE_G) tma_load_4d(S.gm, &maps.g, &S.mbar, i0 - S_::OX, j0 - S_::OY, k0 - S_::OZ, 0);
-  }
-  if (!mbar_wait_bounded(&S.mbar, 0, SPLIT_TMA_POLLS)) {
-    // the copy did not land in time: report it and give it a second bounded chance to finish
-    // before shared memory is read or released; this tile's faces are then not trustworthy
-    if (t == 0) atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
-    mbar_wait_bounded(&S.mbar, 0, SPLIT_TMA_POLLS);
-  }
+  };
   // staged position of tile cell (x, y, z) relative to the tile origin
   auto spos = [&](int x, int y, int z) { return (x + S_::OX) + SX * ((y + S_::OY) + SY * (z + S_::OZ)); };
   // tile coordinates of column `cl` at layer `l` along D
@@ -1492,80 +1483,111 @@ __global__ void __launch_bounds__(FaceTileSmem<C, D>::NT, FaceTile<D>::MINB)
     else if (D == 1) { x = cl % T::TX; y = l; z = cl / T::TX; }
     else { x = cl % T::TX; y = cl / T::TX; z = l; }
   };
-  // ghost layers -2, -1 (tile at the lower domain boundary) and nD, nD + 1 (upper) along D
-  if (t < 4 * TT) {
-    const int side = t / (2 * TT), layer = (t / TT) % 2, cl = t % TT;
-    const int l = side == 0 ? layer - 2 : S_::TD + layer;
-    if ((side == 0 && c0 == 0) || (side == 1 && c0 + S_::TD == nD)) {
+  if (t == 0) mbar_init(&S.mbar, 1);
+  __syncthreads();
+  int tile = blockIdx.x;
+  if (t == 0 && tile < ntiles) issue(tile);
+  // the block strides over the tiles; each copy is issued as soon as the previous tile's staged
+  // values are consumed, so that it lands while that tile's faces are solved
+  for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    int i0, j0, k0;
+    origin(tile, i0, j0, k0);
+    const int c0 = D == 0 ? i0 : (D == 1 ? j0 : k0);
+    if (!mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS)) {
+      // the copy did not land in time: report it, give it a second bounded chance to finish
+      // before shared memory is read again, and leave the remaining tiles of this block (their
+      // faces are then not trustworthy; the count says so)
+      if (t == 0) atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
+      mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS);
+      break;
+    }
+    // ghost layers -2, -1 (tile at the lower domain boundary) and nD, nD + 1 (upper) along D
+    if (t < 4 * TT) {
+      const int side = t / (2 * TT), layer = (t / TT) % 2, cl = t % TT;
+      const int l = side == 0 ? layer - 2 : S_::TD + layer;
+      if ((side == 0 && c0 == 0) || (side == 1 && c0 + S_::TD == nD)) {
+        int x, y, z;
+        cell_of(cl, l, x, y, z);
+        float wv[NV], gv[2] = {0.0f, 0.0f}, bv[3];
+        load_wf<C>(P, i0 + x, j0 + y, k0 + z, wv, gv);
+        load_bccf<C>(P, i0 + x, j0 + y, k0 + z, bv);
+        const int pos = spos(x, y, z);
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) S.w[iv * SC + pos] = wv[iv];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) S.b[a * SC + pos] = bv[a];
+        S.gm[pos] = gv[0];
+        S.gm[SC + pos] = gv[1];
+      }
+    }
+    __syncthreads();
+    // LIM2ND edges of the cell at layer l of column cl into edge slot (l + 1) * TT + cl
+    auto edges = [&](int cl, int l) {
       int x, y, z;
       cell_of(cl, l, x, y, z);
-      float wv[NV], gv[2] = {0.0f, 0.0f}, bv[3];
-      load_wf<C>(P, i0 + x, j0 + y, k0 + z, wv, gv);
-      load_bccf<C>(P, i0 + x, j0 + y, k0 + z, bv);
-      const int pos = spos(x, y, z);
+      const int pos = spos(x, y, z), slot = (l + 1) * TT + cl;
 #pragma unroll
-      for (int iv = 0; iv < NV; ++iv) S.w[iv * SC + pos] = wv[iv];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) S.b[a * SC + pos] = bv[a];
-      S.gm[pos] = gv[0];
-      S.gm[SC + pos] = gv[1];
+      for (int v = 0; v < NE; ++v) {
+        const float *src = v < NV ? S.w + v * SC : (v < NV + 3 ? S.b + (v - NV) * SC : S.gm + (v - NV - 3) * SC);
+        float lo, hi;
+        plm_f32(src[pos - S_::SD], src[pos], src[pos + S_::SD], lo, hi);
+        S.lo[v * NED + slot] = lo;
+        S.hi[v * NED + slot] = hi;
+      }
+    };
+    edges(col, td);
+    if (t < TT) edges(t, -1);
+    // without FASTEOS the face's temperature guess comes from the staged T, read before the
+    // staging area is handed to the next copy
+    float tface = 0.0f;
+    if (!C::FAST && C::HELM) {
+      const int pos = spos(tx, ty, tz);
+      tface = 0.5f * (S.gm[pos - S_::SD] + S.gm[pos]);
     }
-  }
-  __syncthreads();
-  // LIM2ND edges of the cell at layer l of column cl into edge slot (l + 1) * TT + cl
-  auto edges = [&](int cl, int l) {
-    int x, y, z;
-    cell_of(cl, l, x, y, z);
-    const int pos = spos(x, y, z), slot = (l + 1) * TT + cl;
+    __syncthreads();
+    // the staged values are consumed: the next tile's copy overlaps this tile's solves
+    if (t == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    // the face below the own cell along D: edges of layers td - 1 (slot td * TT + col) and td
+    const int sL = td * TT + col, sR = sL + TT;
+    float qL[NV], qR[NV], bL[3] = {0.f, 0.f, 0.f}, bR[3] = {0.f, 0.f, 0.f}, gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
 #pragma unroll
-    for (int v = 0; v < NE; ++v) {
-      const float *src = v < NV ? S.w + v * SC : (v < NV + 3 ? S.b + (v - NV) * SC : S.gm + (v - NV - 3) * SC);
-      float lo, hi;
-      plm_f32(src[pos - S_::SD], src[pos], src[pos + S_::SD], lo, hi);
-      S.lo[v * NED + slot] = lo;
-      S.hi[v * NED + slot] = hi;
+    for (int iv = 0; iv < NV; ++iv) {
+      qL[iv] = S.hi[iv * NED + sL];
+      qR[iv] = S.lo[iv * NED + sR];
     }
-  };
-  edges(col, td);
-  if (t < TT) edges(t, -1);
-  __syncthreads();
-  // the face below the own cell along D: edges of layers td - 1 (slot td * TT + col) and td
-  const int sL = td * TT + col, sR = sL + TT;
-  float qL[NV], qR[NV], bL[3] = {0.f, 0.f, 0.f}, bR[3] = {0.f, 0.f, 0.f}, gL[2] = {0.f, 0.f}, gR[2] = {0.f, 0.f};
 #pragma unroll
-  for (int iv = 0; iv < NV; ++iv) {
-    qL[iv] = S.hi[iv * NED + sL];
-    qR[iv] = S.lo[iv * NED + sR];
-  }
-#pragma unroll
-  for (int a = 0; a < C::DIM; ++a) {
-    if (a == D) continue;
-    bL[a] = S.hi[(NV + a) * NED + sL];
-    bR[a] = S.lo[(NV + a) * NED + sR];
-  }
-  const int fi = i0 + tx, fj = j0 + ty, fk = k0 + tz;
-  const long long fidx = face_lin(g, D, fi, fj, fk);
-  long long fbg = 0;
-  if (C::WB || C::ETOT) fbg = g.bg_profile ? (long long)fj : fidx;
-  float tface = 0.0f;
-  if (C::FAST) {
-    gL[0] = S.hi[(NV + 3) * NED + sL]; gL[1] = S.hi[(NV + 4) * NED + sL];
-    gR[0] = S.lo[(NV + 3) * NED + sR]; gR[1] = S.lo[(NV + 4) * NED + sR];
-    if (C::WB) {
-      const float ge = __ldg(P.sf_ge_f[D] + fbg);
-      gL[0] = gL[0] + ge;
-      gR[0] = gR[0] + ge;
+    for (int a = 0; a < C::DIM; ++a) {
+      if (a == D) continue;
+      bL[a] = S.hi[(NV + a) * NED + sL];
+      bR[a] = S.lo[(NV + a) * NED + sR];
     }
-  } else if (C::HELM) {
-    const int pos = spos(tx, ty, tz);
-    tface = 0.5f * (S.gm[pos - S_::SD] + S.gm[pos]);
-  }
-  float F[NV], Fb[3], rs;
-  face_solve_split_mhd<C>(P, D, fidx, fbg, qL, qR, bL, bR, gL, gR, tface, false, F, Fb, rs);
-  const long long nf = nfaces(g, D);
+    const int fi = i0 + tx, fj = j0 + ty, fk = k0 + tz;
+    const long long fidx = face_lin(g, D, fi, fj, fk);
+    long long fbg = 0;
+    if (C::WB || C::ETOT) fbg = g.bg_profile ? (long long)fj : fidx;
+    if (C::FAST) {
+      gL[0] = S.hi[(NV + 3) * NED + sL]; gL[1] = S.hi[(NV + 4) * NED + sL];
+      gR[0] = S.lo[(NV + 3) * NED + sR]; gR[1] = S.lo[(NV + 4) * NED + sR];
+      if (C::WB) {
+        const float ge = __ldg(P.sf_ge_f[D] + fbg);
+        gL[0] = gL[0] + ge;
+        gR[0] = gR[0] + ge;
+      }
+    }
+    float F[NV], Fb[3], rs;
+    face_solve_split_mhd<C>(P, D, fidx, fbg, qL, qR, bL, bR, gL, gR, tface, false, F, Fb, rs);
+    const long long nf = nfaces(g, D);
 #pragma unroll
-  for (int iv = 0; iv < NV; ++iv) P.fflux[D][(long long)iv * nf + fidx] = F[iv];
-  store_face_emf_split<C>(P, D, fidx, c0 + td, Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
+    for (int iv = 0; iv < NV; ++iv) P.fflux[D][(long long)iv * nf + fidx] = F[iv];
+    store_face_emf_split<C>(P, D, fidx, c0 + td, Fb, F[0], rs, (float)(P.scal[2] * P.inv_v_ref));
+  }
+  // the faces at the upper domain boundary along D, one per thread, strided over the grid
+  const int e0 = D == 0 ? g.nx[1] : g.nx[0], e1 = D == 2 ? g.nx[1] : (C::DIM == 3 ? g.nx[2] : 1);
+  for (long long q = (long long)blockIdx.x * S_::NT + t; q < (long long)e0 * e1; q += (long long)gridDim.x * S_::NT) {
+    const int a = (int)(q % e0), c = (int)(q / e0);
+    const int fi = D == 0 ? g.nx[0] : a, fj = D == 0 ? a : (D == 1 ? g.nx[1] : c), fk = D == 2 ? g.nx[2] : c;
+    face_split_mhd_at<C, D>(P, face_lin(g, D, fi, fj, fk));
+  }
 }
 
 // FP32 face EMF / sign at a possibly-ghost transverse index (periodic wrap, or the reflective
@@ -2342,6 +2364,24 @@ struct SplitRunnerT : Runner {
     out = e.maps;
     return e.ok;
   }
+  // blocks of the tiled face kernels resident on the GPU at once, per direction: the grid of
+  // their tile loop (found at construction, outside any stream capture; 0 if unknown)
+  long long tile_wave[3] = {0, 0, 0};
+  template <class K>
+  static long long wave_of(K kernel, int threads) {
+    int dev = 0, sms = 0, nb = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0) != cudaSuccess)
+      return 0;
+    return (long long)sms * nb;
+  }
+  SplitRunnerT() {
+    if constexpr (C::MHD && C::REC == REC_LIM2ND && !C::SF) {
+      tile_wave[0] = wave_of(k_face_split_mhd_tile<C, 0>, FaceTileSmem<C, 0>::NT);
+      tile_wave[1] = wave_of(k_face_split_mhd_tile<C, 1>, FaceTileSmem<C, 1>::NT);
+      if constexpr (C::DIM == 3) tile_wave[2] = wave_of(k_face_split_mhd_tile<C, 2>, FaceTileSmem<C, 2>::NT);
+    }
+  }
   // resident blocks per SM the Helmholtz MHD cons->prim is compiled for: 8 (64 registers, ~100
   // B of spills), which ran a step at 256^3 in 13.56 ms against 13.89 at 7 (72 registers), 14.37
   // at 6 (80), 13.73 at 9 and 14.14 at 10: its time is latency, and more resident warps hide it
@@ -2382,9 +2422,9 @@ struct SplitRunnerT : Runner {
       FaceTileMaps m;
       if (!tile_maps<D>(P, m)) return false;
       const long long ntiles = (long long)(g.nx[0] / T::TX) * (g.nx[1] / T::TY) * (nz / T::TZ);
-      const long long ntail = (long long)(D == 0 ? g.nx[1] : g.nx[0]) * (D == 2 ? g.nx[1] : nz);
-      const long long nb = ntiles + (ntail + S_::NT - 1) / S_::NT;
-      k_face_split_mhd_tile<C, D><<<(unsigned)nb, S_::NT, 0, s>>>(P, m, (int)ntiles);
+      // one resident wave of blocks striding over the tiles (found at construction)
+      const long long wave = tile_wave[D] > 0 ? tile_wave[D] : ntiles;
+      k_face_split_mhd_tile<C, D><<<(unsigned)std::max(1ll, std::min(ntiles, wave)), S_::NT, 0, s>>>(P, m, (int)ntiles);
       return true;
     }
   }
