@@ -1693,43 +1693,38 @@ __device__ __forceinline__ float corner_emf_split(const Prm &P, const int c[3]) 
   return 0.25f * (emf_S + emf_W + emf_N + emf_E + demf_S - demf_N + demf_W - demf_E);
 }
 
-// Corner EMFs along axis A, one thread per corner, in two launches (one instantiation per
-// axis: the face and cell strides fold into constants): the interior corners (1 <= c[pa] <
-// nx[pa], 1 <= c[qa] < nx[qa]) read their faces and cells by linear index with no branch, the
-// corners on the domain faces of pa and qa map their ghost indices; a single launch over all
-// corners had a quarter of its warps diverge into the mapping path where the rows of corners
-// (nx + 1 long) straddle the warps.
+// Corner EMFs along axis A, one thread per corner (one instantiation per axis: the face and cell
+// strides fold into constants).  The first nin_blocks blocks take the interior corners (1 <=
+// c[pa] < nx[pa], 1 <= c[qa] < nx[qa]), which read their faces and cells by linear index with no
+// branch; the blocks after them take the corners on the domain faces of pa and qa, which map
+// their ghost indices.  Threads over all corners in array order had a quarter of their warps
+// diverge into the mapping path, where the rows of corners (nx + 1 long) straddle the warps.
 template <class C, int A>
-__global__ void __launch_bounds__(256) k_corner_split(Prm P) {
+__global__ void __launch_bounds__(256) k_corner_split(Prm P, unsigned nin_blocks) {
   constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
   if (!*P.active) return;
   const Geo &g = P.g;
-  // interior extents per dimension (x1 fastest, as the arrays): nx - 1 from index 1 along pa
-  // and qa, nx from index 0 along a
-  const int e0 = a == 0 ? g.nx[0] : g.nx[0] - 1, e1 = a == 1 ? g.nx[1] : g.nx[1] - 1;
-  const int e2 = C::DIM == 3 ? (a == 2 ? g.nx[2] : g.nx[2] - 1) : 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)e0 * e1 * e2) return;
   int c[3];
-  unflatten3(t, e0, e1, c[0], c[1], c[2]);
-  c[0] += a != 0;
-  c[1] += a != 1;
-  if (C::DIM == 3) c[2] += a != 2;
-  P.fcor[a][cor_lin(g, a, c[0], c[1], c[2])] = corner_emf_split<C, A, true>(P, c);
-}
-
-// the corners on the domain faces of pa and qa: per index along a, the rim of the
-// (nx[pa] + 1) x (nx[qa] + 1) rectangle of corners, 2 (nx[pa] + nx[qa]) of them
-template <class C, int A>
-__global__ void __launch_bounds__(256) k_corner_split_rim(Prm P) {
-  constexpr int a = A, pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
-  if (!*P.active) return;
-  const Geo &g = P.g;
+  if (blockIdx.x < nin_blocks) {
+    // interior extents per dimension (x1 fastest, as the arrays): nx - 1 from index 1 along pa
+    // and qa, nx from index 0 along a
+    const int e0 = a == 0 ? g.nx[0] : g.nx[0] - 1, e1 = a == 1 ? g.nx[1] : g.nx[1] - 1;
+    const int e2 = C::DIM == 3 ? (a == 2 ? g.nx[2] : g.nx[2] - 1) : 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)e0 * e1 * e2) return;
+    unflatten3(t, e0, e1, c[0], c[1], c[2]);
+    c[0] += a != 0;
+    c[1] += a != 1;
+    if (C::DIM == 3) c[2] += a != 2;
+    P.fcor[a][cor_lin(g, a, c[0], c[1], c[2])] = corner_emf_split<C, A, true>(P, c);
+    return;
+  }
+  // the rim: per index along a, the border of the (nx[pa] + 1) x (nx[qa] + 1) rectangle of
+  // corners, 2 (nx[pa] + nx[qa]) of them
   const int np_ = g.nx[pa], nq = g.nx[qa], na = C::DIM == 3 ? g.nx[a] : 1, rim = 2 * (np_ + nq);
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)(blockIdx.x - nin_blocks) * blockDim.x + threadIdx.x;
   if (t >= (long long)rim * na) return;
   const int m = (int)(t % rim);
-  int c[3];
   c[a] = (int)(t / rim);
   if (m < np_ + 1) { c[pa] = m; c[qa] = 0; }                             // qa = 0 row
   else if (m < 2 * (np_ + 1)) { c[pa] = m - (np_ + 1); c[qa] = nq; }       // qa = nx[qa] row
@@ -2510,7 +2505,7 @@ struct SplitRunnerT : Runner {
       hydro_stage(P, s);
     }
   }
-  // corner EMFs along axis A: interior corners, then the rim on the domain faces
+  // corner EMFs along axis A: the interior corners' blocks, then the rim's, in one launch
   template <int A>
   void corners(const Prm &P, cudaStream_t s) {
     constexpr int pa = A == 2 ? 0 : (A == 0 ? 1 : 2), qa = A == 2 ? 1 : (A == 0 ? 2 : 0);
@@ -2518,8 +2513,8 @@ struct SplitRunnerT : Runner {
     const long long na = C::DIM == 3 ? g.nx[A] : 1;
     const long long nin = (long long)(g.nx[pa] - 1) * (g.nx[qa] - 1) * na;
     const long long nrim = 2ll * (g.nx[pa] + g.nx[qa]) * na;
-    if (nin > 0) k_corner_split<C, A><<<nblk(nin, 256), 256, 0, s>>>(P);
-    k_corner_split_rim<C, A><<<nblk(nrim, 256), 256, 0, s>>>(P);
+    const unsigned bin = nblk(nin, 256);
+    k_corner_split<C, A><<<bin + nblk(nrim, 256), 256, 0, s>>>(P, bin);
   }
   void hydro_stage(const Prm &P, cudaStream_t s) {
     if constexpr (C::DIM == 3 && C::SW == 2) {
