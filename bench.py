@@ -95,10 +95,10 @@ def stage_kernels(cfg, form):
 TRAFFIC_PER_CELL = {("stratified", "fp32_split"): 499.604224e6 / 2097152,
                     ("stratified", "fp64"): 557.258496e6 / 2097152,
                     # one split MHD stage at 128^3 (a middle stage: U0 read): x1 tile faces
-                    # 220.8 MB, walking x2/x3 faces 171.9 + 175.2 MB, corners 3 x 42.2 MB,
-                    # face-B 3 x 50.9 MB, cons->prim 725.8 MB
-                    ("stratified_mhd", "fp32_split"): (220.8e6 + 171.9e6 + 175.2e6 + 3 * 42.2e6 + 3 * 50.9e6
-                                                       + 725.8e6) / 2097152}
+                    # 216.9 MB, walking x2/x3 faces 186.1 + 190.0 MB, corners 3 x 42.2 MB,
+                    # face-B 3 x 50.9 MB, cons->prim 755.2 MB
+                    ("stratified_mhd", "fp32_split"): (216.9e6 + 186.1e6 + 190.0e6 + 3 * 42.2e6 + 3 * 50.9e6
+                                                       + 755.2e6) / 2097152}
 
 
 # Algorithmic HBM bytes per zone-update of the workloads (minimum traffic of one step of a fused
