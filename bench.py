@@ -588,6 +588,23 @@ def run_suite(args, local, mlp_params):
     ea.n, ea.steps, ea.warmup = 0, 5, 3
     el = eos_line(ea, with_cpu=False)
     suite["eos_batch_2^24"] = {k: el[k] for k in ("value", "unit", "ms_per_step", "bracket", "mlp", "agreement", "e2e")}
+    # config 3: the Helmholtz hydro box 256^3 (no B), split and FP64 rates, and the split form's
+    # per-field L1 against FP64 after 1000 steps
+    cfg, h, table = build_problem("stratified", 256, eos_table=args.eos_table)
+    r = {}
+    for form in ("fp32_split", "fp64"):
+        ms, done, t, out, st = run_case(cfg.replace(precision=form), h, table, local, 10)
+        r[form] = (ms, done, out)
+    suite["stratified_hydro_256"] = {
+        "steps": r["fp32_split"][1],
+        "fp32_split": {"value": rate(cfg, r["fp32_split"][0], r["fp32_split"][1]),
+                       "ms_per_step": r["fp32_split"][0] / r["fp32_split"][1], "eos_guess": "warm",
+                       "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
+        "fp64": {"value": rate(cfg, r["fp64"][0], r["fp64"][1]), "ms_per_step": r["fp64"][0] / r["fp64"][1]},
+        "l1_vs_fp64_1000_steps": long_run_errors(cfg, h, table, "fp32_split", 1000, local)}
+    if not args.no_cpu:
+        cpu = cpu_rate("stratified", 2, eos_table=args.eos_table)
+        suite["stratified_hydro_256"]["cpu_oracle"] = {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]}
     # config 5: magnetised box 384^3, the headline form and FP64, a few steps each
     cfg, h, table = build_problem("stratified_mhd", 384, eos_table=args.eos_table)
     r = {}
@@ -887,7 +904,7 @@ def main():
                          "per-field relative L1 difference (untimed); default 1000 for the Helmholtz boxes")
     ap.add_argument("--no-suite", action="store_true",
                     help="skip the other workloads (hot bubble 256^2, Orszag-Tang 1024^2 to t = 0.5, EoS "
-                         "batch 2^24, MHD box 384^3) reported under `suite`")
+                         "batch 2^24, Helmholtz hydro box 256^3, MHD box 384^3) reported under `suite`")
     ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--train-epochs", type=int, default=256, help="MLP training epochs (eos workload)")
