@@ -299,6 +299,45 @@ def test_sound_wave_convergence_by_reconstruction(oracle):
         assert e[2] < 0.1 * e2[1] and rate > 2.2, (rec, e, rate)
 
 
+# ------------------------------------------------------------------------------ conservation
+def conserved_totals(h, gamma):
+    """Sums over the interior of rho, rho v (per component) and the total energy e + rho v^2 / 2
+    (+ B_cc^2 / 2), with e = p / (gamma - 1) (ideal gas)."""
+    w = h.interior(h.prim)
+    rho, v, p = w[0], w[1:1 + h.cfg.sdims], w[1 + h.cfg.sdims]
+    E = p / (gamma - 1.0) + 0.5 * rho * np.sum(v * v, axis=0)
+    if h.cfg.mhd:
+        b = h.interior(h.b_cc)
+        E = E + 0.5 * np.sum(b * b, axis=0)
+    return float(rho.sum()), [float((rho * vd).sum()) for vd in v], float(E.sum()), \
+        float(np.abs(rho * v).sum())
+
+
+@pytest.mark.parametrize("case", ["blast_hllc", "blast_lhllc", "orszag_tang_hlld", "orszag_tang_lhlld"])
+def test_periodic_box_conserves_mass_momentum_energy(oracle, case):
+    """Finite-volume conservation: in a periodic box without sources every face flux leaves one
+    cell and enters its neighbour, so the totals of mass, momentum and energy change only by
+    rounding (a flux used with different values on its two sides, a wrong face index or a sign
+    error shows up as a drift of order the flux)."""
+    from phlegethon_b200 import problems
+    if case.startswith("blast"):
+        cfg, h = problems.blast_2d(64, riemann=case.split("_")[1], shock_flattening=False, nas=0)
+    else:
+        cfg, h = problems.orszag_tang_2d(64, riemann=case.split("_")[2])
+    g = cfg.gamma_ad
+    o = oracle.OracleGrid(h, None)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    m0, p0, e0, pabs0 = conserved_totals(h, g)
+    o.time_loop(50)
+    m1, p1, e1, pabs1 = conserved_totals(h, g)
+    assert abs(m1 - m0) <= 1e-13 * m0, (m0, m1)
+    scale = max(pabs0, pabs1)
+    for a, b in zip(p0, p1):
+        assert abs(b - a) <= 1e-13 * scale, (p0, p1)
+    assert abs(e1 - e0) <= 1e-13 * e0, (e0, e1)
+
+
 # ------------------------------------------------------------------------------ the CUDA forms
 def run_gpu(cfg, h, tmax, precision):
     from phlegethon_b200.abi import Simulation
@@ -358,3 +397,35 @@ def test_stationary_contact_on_the_gpu(gpu_lib, riemann, mhd, precision):
     tol = 0.0 if precision == "fp64" else 1e-7
     assert float(np.abs(w[0] - w0[0]).max()) <= tol and float(np.abs(w[3] - w0[3]).max()) <= tol
     assert float(np.abs(w[1:3]).max()) <= (1e-14 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["blast_lhllc", "orszag_tang_lhlld"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_conservation_on_the_gpu(gpu_lib, case, precision):
+    """The periodic box's totals on the GPU: at rounding in the FP64 form; in the split form the
+    flux divergence is formed from FP32 face fluxes in FP32 before it enters the FP64 state, so
+    the sums over cells telescope to FP32 rounding of the fluxes (measured drifts are recorded
+    in the assertion messages)."""
+    from phlegethon_b200 import problems
+    from phlegethon_b200.abi import Simulation
+    if case.startswith("blast"):
+        cfg, h = problems.blast_2d(64, riemann="lhllc", shock_flattening=False, nas=0)
+    else:
+        cfg, h = problems.orszag_tang_2d(64, riemann="lhlld")
+    g = cfg.gamma_ad
+    with Simulation(cfg.replace(precision=precision)) as sim:
+        sim.upload(h)
+        sim.init_thermo()
+        sim.compute_hyperbolic_dt()
+        sim.download(h)
+        m0, p0, e0, pabs0 = conserved_totals(h, g)
+        done, _ = sim.time_loop(50)
+        sim.download(h)
+    assert done == 50
+    m1, p1, e1, pabs1 = conserved_totals(h, g)
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    scale = max(pabs0, pabs1)
+    assert abs(m1 - m0) <= tol * m0, (m0, m1)
+    assert all(abs(b - a) <= tol * scale for a, b in zip(p0, p1)), (p0, p1)
+    assert abs(e1 - e0) <= tol * e0, (e0, e1)
