@@ -1493,16 +1493,9 @@ __global__ void __launch_bounds__(FaceTileSmem<C, D>::NT, FaceTile<D>::MINB)
     int i0, j0, k0;
     origin(tile, i0, j0, k0);
     const int c0 = D == 0 ? i0 : (D == 1 ? j0 : k0);
-    if (!mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS)) {
-      // the copy did not land in time: report it, give it a second bounded chance to finish
-      // before shared memory is read again, and leave the remaining tiles of this block (their
-      // faces are then not trustworthy; the count says so)
-      if (t == 0) atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
-      mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS);
-      break;
-    }
+    const bool landed = mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS);
     // ghost layers -2, -1 (tile at the lower domain boundary) and nD, nD + 1 (upper) along D
-    if (t < 4 * TT) {
+    if (landed && t < 4 * TT) {
       const int side = t / (2 * TT), layer = (t / TT) % 2, cl = t % TT;
       const int l = side == 0 ? layer - 2 : S_::TD + layer;
       if ((side == 0 && c0 == 0) || (side == 1 && c0 + S_::TD == nD)) {
@@ -1520,7 +1513,15 @@ __global__ void __launch_bounds__(FaceTileSmem<C, D>::NT, FaceTile<D>::MINB)
         S.gm[SC + pos] = gv[1];
       }
     }
-    __syncthreads();
+    if (__syncthreads_or(!landed)) {
+      // a copy did not land in time (the whole block learns it at the barrier, so that every
+      // thread leaves the loop together): report it, give it a second bounded chance to finish
+      // before the block leaves, and leave the remaining tiles of this block (their faces are
+      // then not trustworthy; the count says so)
+      if (t == 0) atomicAdd(P.stat + STAT_TC_STALLED, 1ull);
+      mbar_wait_bounded(&S.mbar, it & 1u, SPLIT_TMA_POLLS);
+      break;
+    }
     // LIM2ND edges of the cell at layer l of column cl into edge slot (l + 1) * TT + cl
     auto edges = [&](int cl, int l) {
       int x, y, z;
