@@ -21,7 +21,7 @@
 
 namespace phl {
 
-constexpr int EOS_MINB_DEFAULT = 1;
+constexpr int EOS_MINB_DEFAULT = 4;
 
 // cold guess; returns the number of EoS evaluations the search used
 __device__ __forceinline__ int bracket_guess(const HelmTable &h, double rho, double e, double abar, double zbar,
@@ -196,9 +196,10 @@ __global__ void __launch_bounds__(128, MINB) k_eos_fallback(HelmTable h, const u
 
 // Launch the inversion on stream s (no synchronisation).  `queue` (n + 1 entries) is needed for
 // the learned guess only.  Returns 0 or a cudaError_t.
-// Resident blocks per SM the inversion kernels are compiled for: 1 lets the compiler keep the
-// whole inlined evaluation in registers (~180), 3 and 4 cap them (168, 128) at the cost of
-// spills; PHL_EOS_MINB selects one of the three instantiations.
+// Resident blocks per SM the inversion kernels are compiled for: 4 caps them at 128 registers
+// (2^24 samples on B200: learned guess 1.66e9 inversions/s, bracket 1.39e9, against 1.34e9 and
+// 1.07e9 with 1, which lets the compiler keep the whole inlined evaluation in ~190 registers at
+// two blocks per SM, and 1.17e9 / 1.04e9 with 6); PHL_EOS_MINB=1 or 3 selects the others.
 inline int eos_minb() {
   static const int v = [] {
     const char *e = getenv("PHL_EOS_MINB");
