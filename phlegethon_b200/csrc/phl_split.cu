@@ -860,7 +860,7 @@ struct SplitMaps {
 constexpr int SPLIT_TMA_POLLS = 1 << 22;  // mbarrier polls before a stalled copy is reported
 
 template <class C, int TX, int TY, int KZ>
-__global__ void __launch_bounds__(TX * TY, C::FAST || !C::HELM ? 2 : 1) k_stage_split_tiled(Prm P, const __grid_constant__ SplitMaps maps,
+__global__ void __launch_bounds__(TX * TY, 2) k_stage_split_tiled(Prm P, const __grid_constant__ SplitMaps maps,
                                                                   int use_tma) {
   if (!*P.active) return;
   using T = SplitTile<C, TX, TY>;
@@ -1273,8 +1273,10 @@ constexpr int C2P_EOS_MINB = 7;
 // grid of the rescue-queue kernels: 4 blocks of 128 threads per SM of a B200 (148 SMs)
 constexpr int RESCUE_BLOCKS = 4 * 148;
 // resident blocks of 128 threads per SM the walking kernels are compiled for (72 registers; the
-// 256^3 MHD stage took 4.46 ms at 7 against 4.53 at 6 and 4.50 at 8)
-constexpr int WALK_MINB = 7;
+// 256^3 MHD stage took 4.46 ms at 7 against 4.53 at 6 and 4.50 at 8); without USE_FASTEOS, where
+// each face runs two FP64 (rho, P) -> T solves, 4 (128 registers): a 256^3 MHD step took 36.9
+// ms against 43.4 with the registers unbounded (253 registers, 2 blocks per SM), 37.5 at 3
+constexpr int WALK_MINB = 7, WALK_MINB_GIVEN = 4;
 
 // Raw values of one cell for the walking face kernel along D: the FP32 state (0 .. NV-1), the
 // cell B components transverse to D (NBT of them from NV on; the component along D is not
@@ -1313,7 +1315,7 @@ __device__ __forceinline__ void load_walk_cell(const Prm &P, const int c[3], int
 // (the per-face kernel does both twice) and its edge values are carried to the next face.  The
 // faces, their arithmetic and the stored results are those of k_face_split_mhd.
 template <class C, int D, int K>
-__global__ void __launch_bounds__(128, C::MINB_FACE32 == 1 ? 1 : WALK_MINB) k_face_split_mhd_walk(Prm P) {
+__global__ void __launch_bounds__(128, C::EOSM == EOS_GIVEN ? WALK_MINB_GIVEN : WALK_MINB) k_face_split_mhd_walk(Prm P) {
   static_assert(C::REC == REC_LIM2ND, "the walk carries LIM2ND edge values");
   if (!*P.active) return;
   using L = WalkCell<C, D>;
@@ -2413,7 +2415,9 @@ struct SplitRunnerT : Runner {
       using S_ = FaceTileSmem<C, D>;
       const Geo &g = P.g;
       const int nz = C::DIM == 3 ? g.nx[2] : 1;
-      if (face_kind == 0 || (face_kind == 1 && D != 0)) return false;
+      // without USE_FASTEOS the walks serve every direction (36.9 ms per 256^3 MHD step against
+      // 37.5 with the x1 tiles, whose 64 registers spill the two per-face EoS solves)
+      if (face_kind == 0 || (face_kind == 1 && (D != 0 || C::EOSM == EOS_GIVEN))) return false;
       if (g.nx[0] % T::TX || g.nx[1] % T::TY || nz % T::TZ) return false;
       FaceTileMaps m;
       if (!tile_maps<D>(P, m)) return false;
