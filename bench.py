@@ -49,15 +49,20 @@ def load_peaks():
     return dict(PEAKS_FALLBACK), "fallback"
 
 
+def table_workers():
+    """Host processes for the Fermi-gas table: the cores shared among the ranks of this node."""
+    return max(1, (os.cpu_count() or 1) // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", "1"))))
+
+
 def build_problem(name, n, fasteos=True, eos_table="fermi"):
     from phlegethon_b200 import helm_table, problems
     table = None
     if name == "stratified":
         cfg, h = problems.stratified_3d(n, fasteos=fasteos, eos_model=eos_table)
-        table = helm_table.make(eos_table, workers=os.cpu_count())
+        table = helm_table.make(eos_table, workers=table_workers())
     elif name == "stratified_mhd":
         cfg, h = problems.stratified_3d(n, mhd=True, fasteos=fasteos, eos_model=eos_table)
-        table = helm_table.make(eos_table, workers=os.cpu_count())
+        table = helm_table.make(eos_table, workers=table_workers())
     elif name == "hot_bubble":
         cfg, h = problems.hot_bubble_2d(n)
     elif name == "orszag_tang":
@@ -274,7 +279,7 @@ def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True, eos_table="fermi"
         nz = slab or 32
         cfg, h = problems.stratified_3d(n, nz=nz, mhd=(name == "stratified_mhd"), fasteos=fasteos,
                                         eos_model=eos_table)
-        tab, dpdr = helm_table.make(eos_table, workers=os.cpu_count())
+        tab, dpdr = helm_table.make(eos_table, workers=table_workers())
         helm = pyoracle.Helm.for_config(cfg, tab, dpdr)
         sample = "%dx%dx%d slab of the %d^3 workload" % (cfg.nx1, cfg.nx2, cfg.nx3, n)
     else:
@@ -770,7 +775,7 @@ def eos_line(args, with_cpu=True):
     from phlegethon_b200.abi import Simulation
     n = args.n or (1 << 24)
     cfg, _ = problems.stratified_3d(8)
-    table = helm_table.make(args.eos_table, workers=os.cpu_count())
+    table = helm_table.make(args.eos_table, workers=table_workers())
     peaks, peak_kind = load_peaks()
     import ctypes as C
     with Simulation(cfg, table) as sim:
@@ -879,7 +884,7 @@ def eos_cpu_rate(rho, e, abar, zbar, seconds=10.0, eos_table="fermi"):
     import pyoracle
     from phlegethon_b200 import helm_table, problems
     cfg, _ = problems.stratified_3d(8)
-    helm = pyoracle.Helm.for_config(cfg, *helm_table.make(eos_table, workers=os.cpu_count()))
+    helm = pyoracle.Helm.for_config(cfg, *helm_table.make(eos_table, workers=table_workers()))
     done = 0
     t0 = time.perf_counter()
     while time.perf_counter() - t0 < seconds:
