@@ -433,3 +433,51 @@ def test_face_temperature_guess_beats_a_learned_accuracy_guess(oracle, table):
                             for i in sel])
     assert face < learned_like, (face, learned_like)
     assert face < 2.8 and learned_like >= 3.0, (face, learned_like)
+
+
+def test_helmholtz_evaluation_is_thermodynamically_consistent(oracle, table):
+    """P and E of the oracle's helm_rhoT_given_full come from one interpolated free energy (the
+    electron part) plus the analytic ions and radiation, so they obey the Maxwell relation
+    (dE/drho)_T = (P - T (dP/dT)_rho) / rho^2, and c_v equals (dE/dT)_rho; both checked by central
+    differences over the stratified boxes' and the EoS batch's (rho, T) ranges.  The c_v check
+    allows for the rounding of E in the difference quotient where the electrons are degenerate
+    (T c_v down to 1e-5 of E)."""
+    cfg, _ = problems.stratified_3d(8)
+    helm = oracle.Helm.for_config(cfg, *table)
+    abar, zbar, h = 13.7, 6.9, 1e-5
+    for lr in np.linspace(-1.0, 8.0, 10):
+        for lt in np.linspace(5.0, 9.5, 10):
+            rho, T = 10.0 ** lr, 10.0 ** lt
+            P, E, _, cv = helm.given_full(rho, T, abar, zbar)
+            dEdr = (helm.given_full(rho * (1 + h), T, abar, zbar)[1] -
+                    helm.given_full(rho * (1 - h), T, abar, zbar)[1]) / (2 * rho * h)
+            dPdT = (helm.given_full(rho, T * (1 + h), abar, zbar)[0] -
+                    helm.given_full(rho, T * (1 - h), abar, zbar)[0]) / (2 * T * h)
+            dEdT = (helm.given_full(rho, T * (1 + h), abar, zbar)[1] -
+                    helm.given_full(rho, T * (1 - h), abar, zbar)[1]) / (2 * T * h)
+            scale = (abs(P) + abs(T * dPdT)) / rho ** 2
+            assert abs(dEdr - (P - T * dPdT) / rho ** 2) <= 1e-7 * scale, (lr, lt)
+            assert abs(dEdT - cv) <= 1e-6 * cv + 1e-12 * abs(E) / (2 * T * h), (lr, lt, dEdT, cv)
+
+
+def test_helmholtz_sound_speed_from_finite_differences(oracle, table):
+    """The sound speed of helm_rhoT_given_full, formed from the bicubic dP/d(rho Ye) table, c_v
+    and the biquintic dP/dT, equals the same relativistic expression (c^2 gamma_1 / z with
+    gamma_1 = chi_T^2 P / (rho T c_v) + chi_rho and z = 1 + (E + c^2) rho / P, the quantities of
+    source.F90:24223-24230) evaluated with central differences of P: a wrong derivative term
+    shows up at the 1e-2 level, the two dP/drho interpolants agree to ~1e-6."""
+    cfg, _ = problems.stratified_3d(8)
+    helm = oracle.Helm.for_config(cfg, *table)
+    abar, zbar, h, clight = 13.7, 6.9, 1e-5, 2.99792458e10
+    for lr in np.linspace(-1.0, 8.0, 10):
+        for lt in np.linspace(5.0, 9.5, 10):
+            rho, T = 10.0 ** lr, 10.0 ** lt
+            P, E, sound, cv = helm.given_full(rho, T, abar, zbar)
+            dPdT = (helm.given_full(rho, T * (1 + h), abar, zbar)[0] -
+                    helm.given_full(rho, T * (1 - h), abar, zbar)[0]) / (2 * T * h)
+            dPdr = (helm.given_full(rho * (1 + h), T, abar, zbar)[0] -
+                    helm.given_full(rho * (1 - h), T, abar, zbar)[0]) / (2 * rho * h)
+            chi_t, chi_r = T * dPdT / P, rho * dPdr / P
+            gam1 = chi_t * (P / rho) * chi_t / (T * cv) + chi_r
+            z = 1.0 + (E + clight * clight) * rho / P
+            assert abs(clight * math.sqrt(gam1 / z) - sound) <= 1e-5 * sound, (lr, lt)
