@@ -1410,10 +1410,11 @@ __global__ void __launch_bounds__(128, C::EOSM == EOS_GIVEN ? WALK_MINB_GIVEN : 
 // layers the stencils need are then written by their threads with the ghost mapping and
 // mirroring of load_wf.  Each thread forms the LIM2ND edges of its cell once into shared memory
 // (the first TT threads also those of the layer below the tile), then solves its face and stores
-// flux, face EMF and CT sign with coalesced stores.  The faces at the upper domain boundary along
-// D are solved by tail blocks of the same launch.  Faces, arithmetic and the solver are those of
-// the walking kernels, which carry the same edges in registers (80 per thread, with spills) and,
-// along x1, stride 4 cells per thread.
+// flux, face EMF and CT sign with coalesced stores.  A grid of one resident wave of blocks
+// strides over the tiles, each block issuing its next tile's copies once the staged values are
+// consumed; the faces at the upper domain boundary along D are solved after the tile loop.
+// Faces, arithmetic and the solver are those of the walking kernels, which carry the same edges
+// in registers and, along x1, would stride 4 cells per thread.
 template <int D> struct FaceTile;
 template <> struct FaceTile<0> { static constexpr int TX = 128, TY = 1, TZ = 1, MINB = 8; };
 template <> struct FaceTile<1> { static constexpr int TX = 32, TY = 8, TZ = 1, MINB = 4; };
