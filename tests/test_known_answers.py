@@ -218,6 +218,59 @@ def test_alfven_wave_returns_after_one_period(oracle, riemann):
     assert abs(va3 - a3) < 0.02, res
 
 
+# ------------------------------------------------------------------------------ fast magnetosonic wave
+FAST_EPS = 1e-6
+
+
+def fast_wave(n, riemann):
+    """Linear fast magnetosonic wave along x1 across a uniform B = (0, 1): rho = 1 + eps sin 2 pi x,
+    v_x = c_f eps sin, p = 1 + c_s^2 eps sin, B_y = 1 + eps sin, with c_s^2 = gamma p / rho = 5/3,
+    v_A = 1 and c_f = sqrt(c_s^2 + v_A^2); it returns in place after t = 1 / c_f.  (c_s differs
+    from v_A on purpose: where they are equal along a face normal the reference's fast-speed
+    discriminant is zero in exact arithmetic and can round negative.)"""
+    g, p0, b0 = 5.0 / 3.0, 1.0, 1.0
+    cfg = Config(sdims=2, nx1=n, nx2=4, nx3=1, ngc=2, nas=0, mhd=True, riemann=riemann, rk_stages=3,
+                 bc=[["periodic", "periodic"]] * 3, x1l=0.0, x1u=1.0, x2l=0.0, x2u=4.0 / n, x3l=0.0, x3u=1.0,
+                 gamma_ad=g, mu=1.0, cfl=0.8, mach_cutoff=1e-4, mach_ct=1e-6)
+    h = HostGrid(cfg)
+    x, _, _ = h.coords()
+    cs2 = g * p0
+    cf = math.sqrt(cs2 + b0 * b0)
+    s = np.sin(2.0 * np.pi * x)
+    h.prim[0] = 1.0 + FAST_EPS * s
+    h.prim[1] = cf * FAST_EPS * s
+    h.prim[2] = 0.0
+    h.prim[3] = p0 + cs2 * FAST_EPS * s
+    h.temp[...] = h.prim[3] / h.prim[0]
+    h.b_x[0][...] = 0.0
+    # B_y on x2 faces depends on x1 only; the arrays' first index i holds cell i - 1
+    xc = (np.arange(h.b_x[1].shape[0]) - 1 + 0.5) / n
+    h.b_x[1][...] = (b0 * (1.0 + FAST_EPS * np.sin(2.0 * np.pi * xc)))[:, None, None]
+    return cfg, h, cf
+
+
+@pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
+def test_fast_magnetosonic_wave_returns_after_one_period(oracle, riemann):
+    """After t = 1 / c_f the compressive wave is back in phase to second order (it travels at the
+    fast speed, which the magnetic pressure in the flux sets: at the sound speed alone it would
+    lag by 2 pi (1 - c_s / c_f) = 0.66 rad), density and B_y stay in the eigenvector ratio
+    dB_y / B_y = drho / rho, the amplitude decays at first order (the LIM2ND limiter) and no
+    transverse velocity appears."""
+    res = []
+    for n in (32, 64, 128):
+        cfg, h, cf = fast_wave(n, riemann)
+        run_oracle(oracle, cfg, h, 1.0 / cf)
+        amp, ph = fit_wave(h.interior(h.prim)[0][:, 0, 0] - 1.0, n)
+        bamp, bph = fit_wave(h.bface_interior(1)[:n, 0, 0] - 1.0, n)
+        res.append((amp / FAST_EPS, abs(ph), bamp / FAST_EPS, abs(bph)))
+        assert float(np.abs(h.interior(h.prim)[2]).max()) == 0.0
+    (a1, p1, b1, q1), (a2, p2, b2, q2), (a3, p3, b3, q3) = res
+    # measured phase 0.0110, 0.0026, 0.00064; amplitude 0.731, 0.857, 0.926
+    assert p2 < 0.3 * p1 and p3 < 0.3 * p2 and p3 < 1e-3, res
+    assert (1 - a2) < 0.6 * (1 - a1) and (1 - a3) < 0.6 * (1 - a2) and a3 > 0.9, res
+    assert abs(b3 - a3) < 1e-3 * a3 and abs(q3 - p3) < 1e-6, res
+
+
 # ------------------------------------------------------------------------------ stationary contact
 def stationary_contact(n, riemann, mhd=False):
     """rho = 1 in 0.25 < x < 0.75 and 0.125 elsewhere (periodic), p = 1, v = 0; MHD: B = (0.75, 0.5)
