@@ -1207,7 +1207,9 @@ void phlo_hydro_step(phlo_grid *g) {
       emf_ghosts(g, &S);
       ct_update(g, &S, a1, a2, a3);
     }
-    /* gravity source: rho is the deviation under WB (source.F90:12606-12644) */
+    /* gravity source: rho is the deviation under WB (source.F90:12606-12644); without
+     * EVOLVE_ETOT the energy gains the work of gravity on the current RK state's momentum
+     * (source.F90:12631-12638, the x3 term first in 3D) */
     if (g->gravity) {
 #pragma omp parallel for collapse(2) num_threads(nthr)
       for (int k = 1; k <= g->nx3; ++k)
@@ -1216,6 +1218,14 @@ void phlo_hydro_step(phlo_grid *g) {
             double rho = g->prim[OFF(&sc, IRHO, i, j, k)];
             double *r = S.res + OFF(&sin_, 0, i, j, k);
             for (int d = 0; d < sd; ++d) r[IVX(d)] = r[IVX(d)] - rho * g->grav[OFF(&sg, d, i, j, k)];
+            if (!g->etot) {
+              const double *u = S.state + OFF(&sin_, 0, i, j, k);
+              double e = r[ip];
+              if (three) e = e - u[3] * g->grav[OFF(&sg, 2, i, j, k)];
+              e = e - u[1] * g->grav[OFF(&sg, 0, i, j, k)];
+              e = e - u[2] * g->grav[OFF(&sg, 1, i, j, k)];
+              r[ip] = e;
+            }
           }
     }
     /* USE_CONSTANT_ACCELERATION: rho a from the current state (source.F90:12806-12836) */

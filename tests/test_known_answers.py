@@ -271,6 +271,44 @@ def test_fast_magnetosonic_wave_returns_after_one_period(oracle, riemann):
     assert abs(b3 - a3) < 1e-3 * a3 and abs(q3 - p3) < 1e-6, res
 
 
+# ------------------------------------------------------------------------------ free fall
+@pytest.mark.parametrize("etot", [False, True])
+@pytest.mark.parametrize("riemann", ["hllc", "lhllc"])
+def test_uniform_gas_falls_freely(oracle, riemann, etot):
+    """A uniform gas at rest (rho = 1, p = 1) between reflecting walls under g = -1 (no
+    well-balancing) falls freely away from the walls: after 5 steps the cells beyond the walls'
+    numerical reach (3 stages x 2 cells per step) move at v = g t exactly (third-order
+    Runge-Kutta integrates the constant acceleration exactly), at unchanged density and
+    pressure: gravity's work (source.F90:12631-12638, or the potential carried by the mass flux
+    under EVOLVE_ETOT) goes into kinetic energy alone."""
+    from phlegethon_b200.problems import CONST_RGAS
+    cfg = Config(sdims=2, nx1=16, nx2=128, nx3=1, ngc=2, nas=0, gravity=True, etot=etot, riemann=riemann,
+                 rk_stages=3, bc=[["periodic", "periodic"], ["reflective", "reflective"], ["periodic", "periodic"]],
+                 gamma_ad=5.0 / 3.0, mu=1.0, cfl=0.8, mach_cutoff=1e-4)
+    h = HostGrid(cfg)
+    _, y, _ = h.coords()
+    h.prim[0] = 1.0
+    h.prim[1] = 0.0
+    h.prim[2] = 0.0
+    h.prim[3] = 1.0
+    h.grav[0] = 0.0
+    h.grav[1] = -1.0
+    if etot:
+        h.phi_cc[...] = y
+        for d in range(2):
+            _, fy, _ = h.face_coords(d)
+            h.phi_x[d][...] = fy
+    h.temp[...] = 1.0 / CONST_RGAS
+    o = oracle.OracleGrid(h, None)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(5)
+    t = o.g.time
+    w = h.interior(h.prim)[:, :, 40:88, 0]
+    assert float(np.abs(w[2] + t).max()) <= 1e-14 and float(np.abs(w[1]).max()) == 0.0
+    assert float(np.abs(w[0] - 1.0).max()) <= 1e-14 and float(np.abs(w[3] - 1.0).max()) <= 1e-14
+
+
 # ------------------------------------------------------------------------------ stationary contact
 def stationary_contact(n, riemann, mhd=False):
     """rho = 1 in 0.25 < x < 0.75 and 0.125 elsewhere (periodic), p = 1, v = 0; MHD: B = (0.75, 0.5)
