@@ -182,6 +182,36 @@ def test_stratified_mhd_div_b_reflective(oracle):
     assert div_b_max(h) <= 1e-13
 
 
+@pytest.mark.parametrize("sdims", [2, 3])
+@pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
+def test_magnetised_uniform_state_between_walls(oracle, riemann, sdims):
+    """A uniform magnetised gas streaming along x1 between reflective x2 walls, with B parallel
+    to the walls, is an exact steady state: the mirrored ghost cells equal the interior (v_x1
+    and B are tangential), every face sees L = R, and the CT corner EMFs cancel.  Twenty RK3
+    steps leave the density, the velocity and every face B unchanged to the bit; the pressure,
+    recovered from E - rho v^2 / 2 - B^2 / 2, moves by rounding only."""
+    cfg = Config(sdims=sdims, nx1=12, nx2=16, nx3=8 if sdims == 3 else 1, mhd=True,
+                 riemann=riemann, gamma_ad=5.0 / 3.0, mu=1.0,
+                 bc=[["periodic", "periodic"], ["reflective", "reflective"],
+                     ["periodic", "periodic"]])
+    h = HostGrid(cfg)
+    h.prim[0] = 1.3
+    h.prim[1] = 0.3
+    h.prim[sdims + 1] = 0.7  # pressure
+    h.temp[...] = 1.0
+    h.b_x[0][...] = 0.6
+    if sdims == 3:
+        h.b_x[2][...] = -0.4
+    w0 = h.interior(h.prim).copy()
+    b0 = [h.bface_interior(d).copy() for d in range(sdims)]
+    _run(oracle, h, steps=20)
+    w = h.interior(h.prim)
+    assert np.array_equal(w[:sdims + 1], w0[:sdims + 1])
+    assert float(np.abs(w[sdims + 1] - 0.7).max()) <= 4 * np.finfo(float).eps * 0.7
+    for d in range(sdims):
+        assert np.array_equal(h.bface_interior(d), b0[d])
+
+
 def test_helmholtz_round_trips(oracle, table):
     cfg, _ = problems.stratified_3d(8)
     helm = oracle.Helm.for_config(cfg, *table)
