@@ -51,3 +51,42 @@ def div_b_max(h):
         div = div + (b[tuple(sl_hi)] - b[tuple(sl_lo)]) / dx[d]
     bmax = max(float(np.abs(h.bface_interior(d)).max()) for d in range(c.sdims))
     return float(np.abs(div).max() * min(dx[: c.sdims]) / bmax)
+
+
+def permute_axes(h, perm):
+    """A copy of host grid `h` with its coordinate axes permuted: new axis a is old axis
+    perm[a] (perm a permutation of 0..2; in 2D perm[2] == 2).  Cell arrays are transposed,
+    vector components (velocity, gravity, cell B) and per-direction face arrays (face B, face
+    potentials and equilibria) are re-indexed, and the configuration's extents, boundary
+    conditions and acceleration follow the axes."""
+    from phlegethon_b200.grid import HostGrid
+    cfg, sd = h.cfg, h.cfg.sdims
+    ax = lambda *v: [v[perm[d]] for d in range(3)]
+    nx, xl, xu = ax(cfg.nx1, cfg.nx2, cfg.nx3), ax(cfg.x1l, cfg.x2l, cfg.x3l), ax(cfg.x1u, cfg.x2u, cfg.x3u)
+    c2 = cfg.replace(nx1=nx[0], nx2=nx[1], nx3=nx[2], x1l=xl[0], x2l=xl[1], x3l=xl[2],
+                     x1u=xu[0], x2u=xu[1], x3u=xu[2], bc=[list(b) for b in ax(*cfg.bc)],
+                     acc=tuple(ax(*cfg.acc)))
+    h2 = HostGrid(c2)
+    cell = lambda a: np.transpose(a, perm)
+    comp = lambda a: np.transpose(a, (0,) + tuple(1 + p for p in perm))
+
+    def vector(a, b, lo):
+        for d in range(sd):
+            b[lo + d] = cell(a[lo + perm[d]])
+
+    vector(h.prim, h2.prim, 1)
+    for iv in [0] + list(range(sd + 1, cfg.nvars)):
+        h2.prim[iv] = cell(h.prim[iv])
+    for name, tr in (("temp", cell), ("eint", cell), ("phi_cc", cell), ("eq_gammae_cc", cell),
+                     ("gammaf", comp), ("eq_prim_cc", comp)):
+        if getattr(h, name) is not None:
+            getattr(h2, name)[...] = tr(getattr(h, name))
+    for name in ("grav", "b_cc"):
+        if getattr(h, name) is not None:
+            vector(getattr(h, name), getattr(h2, name), 0)
+    for name, tr in (("phi_x", cell), ("eq_gammae_x", cell), ("b_x", cell), ("eq_prim_x", comp)):
+        a, b = getattr(h, name), getattr(h2, name)
+        for d in range(sd):
+            if a[perm[d]] is not None:
+                b[d][...] = tr(a[perm[d]])
+    return h2
