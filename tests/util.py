@@ -90,3 +90,36 @@ def permute_axes(h, perm):
             if a[perm[d]] is not None:
                 b[d][...] = tr(a[perm[d]])
     return h2
+
+
+def mirror_axis(h, a):
+    """A copy of host grid `h` mirrored along axis a (x_a -> x_al + x_au - x_a): every array
+    is reversed along a (ghost layers and staggered faces map onto themselves), and the a
+    components of the vectors (velocity, gravity, face and cell B) change sign.  The boundary
+    conditions of the two sides of axis a swap."""
+    cfg, sd = h.cfg, h.cfg.sdims
+    bc = [list(b) for b in cfg.bc]
+    bc[a] = bc[a][::-1]
+    h2 = h.copy()
+    h2.cfg = cfg.replace(bc=bc)
+    flip = lambda x, lead: np.flip(x, axis=a + lead)
+    for name in ("prim", "gammaf", "eq_prim_cc", "grav", "b_cc"):
+        x = getattr(h, name)
+        if x is not None:
+            getattr(h2, name)[...] = flip(x, 1)
+    for name in ("temp", "eint", "phi_cc", "eq_gammae_cc"):
+        x = getattr(h, name)
+        if x is not None:
+            getattr(h2, name)[...] = flip(x, 0)
+    for name, lead in (("phi_x", 0), ("eq_gammae_x", 0), ("b_x", 0), ("eq_prim_x", 1)):
+        for d in range(sd):
+            x = getattr(h, name)[d]
+            if x is not None:
+                getattr(h2, name)[d][...] = flip(x, lead)
+    h2.prim[1 + a] *= -1.0
+    for name in ("grav", "b_cc"):
+        if getattr(h2, name) is not None:
+            getattr(h2, name)[a] *= -1.0
+    if h2.b_x[a] is not None:
+        h2.b_x[a] *= -1.0
+    return h2
