@@ -322,6 +322,69 @@ def test_mirror_commutes_with_the_step(oracle, sdims, axis, riemann, rec):
             assert float(np.abs(hm.bface_interior(d) - ref.bface_interior(d)).max()) <= 2e-15
 
 
+
+def _offcentre_blast(riemann, rec):
+    """A drifting blast off the centre of a 24 x 20 periodic box (p 10 inside r^2 < 0.02, 0.1
+    outside; B = (0.5, 0.3) for the MHD solvers), run with USE_SHOCK_FLATTENING at eps_sf 0.25:
+    the flattener flags the front, and its detector, PLM fallback and HLL faces enter the step."""
+    mhd = riemann in ("hlld", "lhlld")
+    cfg, _ = problems.blast_2d(24, riemann=riemann, rec=rec, shock_flattening=True, eps_sf=0.25)
+    h = HostGrid(cfg.replace(nx2=20, x2u=20.0 / 24.0, mhd=mhd))
+    x, y, _ = h.coords()
+    inside = (x - 0.42) ** 2 + (y - 0.47) ** 2 < 0.02
+    h.prim[0] = 1.0
+    h.prim[1] = 0.1
+    h.prim[2] = -0.05
+    h.prim[3] = np.where(inside, 10.0, 0.1)
+    h.prim[4] = np.where(inside, 1.0, 0.0)
+    if mhd:
+        h.b_x[0][...] = 0.5
+        h.b_x[1][...] = 0.3
+    return h
+
+
+def _supersonic_box(sdims, riemann, rec):
+    """The smooth periodic box streaming at Mach ~2 along x1 with FLUX_IS_ALL_MACH: the x1
+    faces take the upwind flux where the whole fan moves one way."""
+    h = _smooth_box(sdims, riemann, rec, mhd=riemann == "lhlld")
+    h.cfg = h.cfg.replace(all_mach=True)
+    h.prim[1] += 2.5
+    return h
+
+
+@pytest.mark.parametrize("rec", ["lim2nd", "pph", "lim5th"])
+@pytest.mark.parametrize("case", ["blast-hllc", "blast-lhllc", "blast-hlld", "blast-lhlld",
+                                  "allmach2d-lhllc", "allmach2d-lhlld", "allmach3d-lhllc",
+                                  "allmach3d-lhlld"])
+def test_symmetries_with_flattening_and_all_mach(oracle, case, rec):
+    """The permutation and reflection symmetries with the two options that change the face
+    solve: shock flattening on a blast front, and FLUX_IS_ALL_MACH on a supersonic stream
+    (both options change these states at O(1): with eps_sf out of reach, or without the
+    all-Mach switch, the results differ).  Equal to 8e-15 (pressures up to 10, velocities up
+    to 3)."""
+    kind, riemann = case.split("-")
+    if kind == "blast":
+        h, sdims = _offcentre_blast(riemann, rec), 2
+    else:
+        sdims = int(kind[-2])
+        h = _supersonic_box(sdims, riemann, rec)
+    stepped = h.copy()
+    _run(oracle, stepped, steps=6)
+    without = h.copy()
+    without.cfg = h.cfg.replace(eps_sf=1e300) if kind == "blast" else h.cfg.replace(all_mach=False)
+    _run(oracle, without, steps=6)
+    assert not np.allclose(without.interior(without.prim), stepped.interior(stepped.prim), atol=1e-6)
+    transforms = [lambda g, a=a: mirror_axis(g, a) for a in range(sdims)]
+    transforms.append(lambda g: permute_axes(g, (1, 0, 2) if sdims == 2 else (1, 2, 0)))
+    for tr in transforms:
+        moved = tr(h)
+        _run(oracle, moved, steps=6)
+        ref = tr(stepped)
+        assert float(np.abs(moved.interior(moved.prim) - ref.interior(ref.prim)).max()) <= 8e-15
+        if h.cfg.mhd:
+            for d in range(sdims):
+                assert float(np.abs(moved.bface_interior(d) - ref.bface_interior(d)).max()) <= 8e-15
+
 @pytest.mark.parametrize("mhd", [False, True])
 @pytest.mark.parametrize("axis", [0, 1, 2])
 def test_mirror_of_the_stratified_helmholtz_box(oracle, axis, mhd):
