@@ -560,7 +560,7 @@ def run_suite(args, local, mlp_params):
     def rate(cfg, ms, done):
         return done * cfg.n_cells / (ms * 1e-3)
 
-    # north_star config 1: 2D hot bubble 256^2, 100 steps
+    # 2D hot bubble 256^2, 100 steps
     cfg, h, _ = build_problem("hot_bubble", 256)
     r = {}
     for form in ("fp64", "fp32_split"):
@@ -574,7 +574,7 @@ def run_suite(args, local, mlp_params):
                        "ms_per_step": r["fp32_split"][0] / r["fp32_split"][1],
                        "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
         "cpu_oracle": {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]} if cpu else None}
-    # config 2: Orszag-Tang 1024^2 (HLLD, CT) to t = 0.5
+    # Orszag-Tang 1024^2 (HLLD, CT) to t = 0.5
     cfg, h, _ = build_problem("orszag_tang", 1024)
     r = {}
     for form in ("fp64", "fp32_split"):
@@ -590,12 +590,12 @@ def run_suite(args, local, mlp_params):
                        "div_b_max": div_b_max(r["fp32_split"][2]),
                        "l1_vs_fp64": field_errors(r["fp32_split"][2], r["fp64"][2])},
         "cpu_oracle": {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]} if cpu else None}
-    # config 4: EoS inversion batch of 2^24 samples, learned vs bracket guess
+    # EoS inversion batch of 2^24 samples, learned vs bracket guess
     ea = argparse.Namespace(**vars(args))
     ea.n, ea.steps, ea.warmup = 0, 5, 3
     el = eos_line(ea, with_cpu=False)
     suite["eos_batch_2^24"] = {k: el[k] for k in ("value", "unit", "ms_per_step", "bracket", "mlp", "agreement", "e2e")}
-    # config 3: the Helmholtz hydro box 256^3 (no B), split and FP64 rates, and the split form's
+    # the Helmholtz hydro box 256^3 (no B), split and FP64 rates, and the split form's
     # per-field L1 against FP64 after 1000 steps
     cfg, h, table = build_problem("stratified", 256, eos_table=args.eos_table)
     r = {}
@@ -612,7 +612,7 @@ def run_suite(args, local, mlp_params):
     if not args.no_cpu:
         cpu = cpu_rate("stratified", 2, eos_table=args.eos_table)
         suite["stratified_hydro_256"]["cpu_oracle"] = {"value": cpu[0], "cores": cpu[1], "sample": cpu[2]}
-    # config 5: magnetised box 384^3, the headline form and FP64, a few steps each
+    # magnetised box 384^3, the headline form and FP64, a few steps each
     cfg, h, table = build_problem("stratified_mhd", 384, eos_table=args.eos_table)
     r = {}
     for form, guess in (("fp32_split", "mlp_rescue" if mlp_params is not None else "warm"), ("fp64", "warm")):

@@ -1271,7 +1271,7 @@ void *phl_device_field(phl_ctx *ctx, const char *name) {
 
 void *phl_stream(phl_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
-// ---- EoS batch (config 4) and MLP live in phl_eos_batch.cuh / phl_mlp.cu
+// ---- the EoS batch and the MLP live in phl_eos_batch.cuh / phl_mlp.cu
 int phl_eos_invert_batch_device(phl_ctx *ctx, long long n, const double *rho, const double *e,
                                 const double *abar, const double *zbar, double *T_inout, double *p,
                                 double *cs, int *iters, int guess) {

@@ -117,7 +117,7 @@ EOS_MODELS = {"synthetic": (analytic_pressure, analytic_energy, analytic_tempera
               "fermi": (fermi_pressure, fermi_energy, fermi_temperature)}
 
 
-# ------------------------------------------------------------------------------ config 1
+# ------------------------------------------------------------------------------ hot bubble
 def hot_bubble_2d(n=256, riemann="lhllc", seed=None, shock_flattening=False, eps_sf=0.25):
     """2D hot bubble: [0,1]^2, periodic x / reflecting y, g = -1 in y, isothermal atmosphere
     rho = exp(-y/H), H = 0.5, p = rho*H*|g|, Gaussian temperature bump
@@ -154,7 +154,7 @@ def hot_bubble_2d(n=256, riemann="lhllc", seed=None, shock_flattening=False, eps
     return cfg, h
 
 
-# ------------------------------------------------------------------------------ config 2
+# ------------------------------------------------------------------------------ Orszag-Tang
 def orszag_tang_2d(n=1024, riemann="hlld", rec="lim2nd", shock_flattening=False, eps_sf=0.25):
     """Orszag-Tang vortex on the periodic unit square (tests/orszag-tang/app.F90:13-79; the
     reference's test runs it with LIM5TH_REC, tests/orszag-tang/Makefile:29)."""
@@ -204,7 +204,7 @@ def blast_2d(n=128, riemann="hllc", rec="lim2nd", shock_flattening=True, eps_sf=
     return cfg, h
 
 
-# ------------------------------------------------------------------------------ configs 3 / 5
+# ------------------------------------------------------------------------------ stratified Helmholtz boxes
 STRAT_ABAR = 13.7
 STRAT_ZBAR = 6.9
 
@@ -308,7 +308,7 @@ def stratified_3d(n=256, ny=None, nz=None, mhd=False, beta=1.0e4, mach=1.0e-3, s
     return cfg, h
 
 
-# ------------------------------------------------------------------------------ config 4
+# ------------------------------------------------------------------------------ EoS samples
 def eos_samples(n, seed=20240601):
     """(rho, T, Abar, Zbar) with log10 rho ~ U[-2, 9], log10 T ~ U[4, 10], Abar ~ U[1, 56],
     Zbar ~ U[1, Abar/2]  (n samples, counter-based hash stream)."""

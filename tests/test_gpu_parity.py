@@ -66,7 +66,7 @@ def periodic_3d(n=12, mhd=False, riemann=None):
     return cfg, h
 
 
-# ------------------------------------------------------------------------------ config 1
+# ------------------------------------------------------------------------------ hot bubble
 @pytest.mark.parametrize("riemann", ["lhllc", "hllc"])
 def test_hot_bubble_one_step(gpu_lib, oracle, riemann):
     cfg, h = problems.hot_bubble_2d(64, riemann=riemann)
@@ -103,7 +103,7 @@ def test_hydrostatic_balance_kept(gpu_lib):
     assert float(np.abs(out.interior(out.prim)[3] - p0).max() / p0.max()) < 1e-14
 
 
-# ------------------------------------------------------------------------------ config 2
+# ------------------------------------------------------------------------------ Orszag-Tang
 @pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
 def test_orszag_tang(gpu_lib, oracle, riemann):
     cfg, h = problems.orszag_tang_2d(64, riemann=riemann)
@@ -126,7 +126,7 @@ def test_periodic_3d(gpu_lib, oracle, mhd, riemann):
         assert div_b_max(hg) <= 1e-13
 
 
-# ------------------------------------------------------------------------------ configs 3 / 5
+# ------------------------------------------------------------------------------ stratified Helmholtz boxes
 @pytest.mark.parametrize("mhd", [False, True])
 def test_stratified_helmholtz(gpu_lib, oracle, table, mhd):
     cfg, h = problems.stratified_3d(12, ny=16, nz=10, mhd=mhd)
