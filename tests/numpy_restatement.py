@@ -1,4 +1,4 @@
-"""An independent, vectorised numpy restatement of the 2D ideal-gas hydro step.
+"""An independent, vectorised numpy restatement of the 2D ideal-gas hydro and MHD steps.
 
 Written from the reference (source/source.F90) separately from the C oracle, in a different
 style (whole-array operations on a ghost-padded grid instead of per-line loops), so that a
@@ -9,6 +9,8 @@ WB momentum fix and EVOLVE_ETOT potential flux (S:8953-8966), gravity (S:12606-1
 (S:7018-7048, S:13518-13531), cons->prim (S:13533-13686) and the CFL dt (S:13707-13960).
 With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073-8136) and
 the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
+`mhd_2d_steps` restates the periodic ideal-MHD step with HLLD or LHLLD and constrained
+transport, read from the same Fortran (its docstring lists the lines).
 Test infrastructure only.
 """
 import numpy as np
@@ -206,3 +208,260 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
             eint = e
         dt = cfl_dt(W)
     return W, eint, temp, dt
+
+
+# ------------------------------------------------------------------------------ 2D ideal MHD
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach):
+    """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
+    array in the face frame, 2D (v3 = B3 = 0), ideal gas (S:13969-15024).  q = (rho, v1, v2,
+    p), b = (B normal, B transverse).  Returns the four fluxes and fluxb(2)."""
+    igmm1 = 1.0 / (gm - 1.0)
+    z = np.zeros_like(qL[0])
+    rhoL, v1L, v2L, pL = qL
+    rhoR, v1R, v2R, pR = qR
+    v3L = v3R = z
+    iL = 1.0 / rhoL
+    iR = 1.0 / rhoR
+    v2sL = v1L * v1L + v2L * v2L + v3L * v3L
+    v2sR = v1R * v1R + v2R * v2R + v3R * v3R
+    c2L = gm * pL * iL
+    c2R = gm * pR * iR
+    reL = pL * igmm1 + 0.5 * rhoL * v2sL
+    reR = pR * igmm1 + 0.5 * rhoR * v2sR
+    b2L, b2R, b3L, b3R = bL[1], bR[1], z, z
+    bx1 = 0.5 * (bL[0] + bR[0])
+    bx1_2 = bx1 * bx1
+    pbL = 0.5 * (bx1_2 + b2L * b2L + b3L * b3L)
+    pbR = 0.5 * (bx1_2 + b2R * b2R + b3R * b3R)
+    reL = reL + pbL
+    reR = reR + pbR
+    ptL = pL + pbL
+    ptR = pR + pbR
+    a2L = 2.0 * pbL * iL
+    a2R = 2.0 * pbR * iR
+    an2L = bx1_2 * iL
+    an2R = bx1_2 * iR
+    d = c2L + a2L
+    cL = np.sqrt(0.5 * (c2L + a2L + np.sqrt(d * d - 4.0 * c2L * an2L)))
+    d = c2R + a2R
+    cR = np.sqrt(0.5 * (c2R + a2R + np.sqrt(d * d - 4.0 * c2R * an2R)))
+    mc = np.maximum(cL, cR)
+    sL = np.minimum(v1L, v1R) - mc
+    sR = np.maximum(v1L, v1R) + mc
+    dsuL = sL - v1L
+    dsuR = sR - v1R
+    it1 = 1.0 / (dsuR * rhoR - dsuL * rhoL)
+    us = (dsuR * rhoR * v1R - dsuL * rhoL * v1L - ptR + ptL) * it1
+    dsumL = sL - us
+    dsumR = sR - us
+    if low_mach:
+        d = v2sL + a2L
+        cu2L = 0.5 * (v2sL + a2L + np.sqrt(d * d - 4.0 * v2sL * an2L))
+        d = v2sR + a2R
+        cu2R = 0.5 * (v2sR + a2R + np.sqrt(d * d - 4.0 * v2sR * an2R))
+        mL = np.sqrt(cu2L) / cL
+        mR = np.sqrt(cu2R) / cR
+        mmax = np.maximum(mL, mR)
+        chi = np.maximum(mach_cutoff, np.minimum(1.0, mmax))
+        phi = np.where(mmax < 0.6, chi * (2.0 - chi), 1.0)
+    else:
+        phi = 1.0
+    pst = (dsuR * rhoR * ptL - dsuL * rhoL * ptR - phi * rhoL * rhoR * dsuR * dsuL * (v1L - v1R)) * it1
+    rsL = rhoL * dsuL / dsumL
+    rsR = rhoR * dsuR / dsumR
+    a1i = 1.0 / (rhoL * dsuL * dsumL - bx1_2)
+    v2sL_ = v2L - bx1 * b2L * (us - v1L) * a1i
+    b2sL = b2L * (rhoL * dsuL * dsuL - bx1_2) * a1i
+    v3sL = v3L - bx1 * b3L * (us - v1L) * a1i
+    b3sL = b3L * (rhoL * dsuL * dsuL - bx1_2) * a1i
+    a2i = 1.0 / (rhoR * dsuR * dsumR - bx1_2)
+    v2sR_ = v2R - bx1 * b2R * (us - v1R) * a2i
+    b2sR = b2R * (rhoR * dsuR * dsuR - bx1_2) * a2i
+    v3sR = v3R - bx1 * b3R * (us - v1R) * a2i
+    b3sR = b3R * (rhoR * dsuR * dsuR - bx1_2) * a2i
+    vbL = v1L * bx1 + v2L * b2L + v3L * b3L
+    vbR = v1R * bx1 + v2R * b2R + v3R * b3R
+    vbsL = us * bx1 + v2sL_ * b2sL + v3sL * b3sL
+    vbsR = us * bx1 + v2sR_ * b2sR + v3sR * b3sR
+    resL = (dsuL * reL - ptL * v1L + pst * us + bx1 * (vbL - vbsL)) / dsumL
+    resR = (dsuR * reR - ptR * v1R + pst * us + bx1 * (vbR - vbsR)) / dsumR
+    srL = np.sqrt(rsL)
+    srR = np.sqrt(rsR)
+    ab = np.abs(bx1)
+    ssL = us - ab / srL
+    ssR = us + ab / srR
+    isb = 1.0 / (srL + srR)
+    sgn = np.copysign(1.0, bx1)
+    v22 = (srL * v2sL_ + srR * v2sR_ + (b2sR - b2sL) * sgn) * isb
+    b22 = (srL * b2sR + srR * b2sL + srL * srR * (v2sR_ - v2sL_) * sgn) * isb
+    v32 = (srL * v3sL + srR * v3sR + (b3sR - b3sL) * sgn) * isb
+    b32 = (srL * b3sR + srR * b3sL + srL * srR * (v3sR - v3sL) * sgn) * isb
+    vb2 = us * bx1 + v22 * b22 + v32 * b32
+    re2L = resL - srL * (vbsL - vb2) * sgn
+    re2R = resR + srR * (vbsR - vb2) * sgn
+    if low_mach:
+        # the state at x/t = 0 among L*, L**, R**, R* and its physical flux
+        sel = [ssL > 0.0, us > 0.0, ssR > 0.0]
+
+        def pick(a, b, c, d):
+            return np.where(sel[0], a, np.where(sel[1], b, np.where(sel[2], c, d)))
+        rho = pick(rsL, rsL, rsR, rsR)
+        u = us
+        v2 = pick(v2sL_, v22, v22, v2sR_)
+        v3 = pick(v3sL, v32, v32, v3sR)
+        re = pick(resL, re2L, re2R, resR)
+        b2 = pick(b2sL, b22, b22, b2sR)
+        b3 = pick(b3sL, b32, b32, b3sR)
+        F = [rho * u, rho * u * u + pst - bx1_2, rho * u * v2 - bx1 * b2,
+             (re + pst) * u - bx1 * (bx1 * u + v2 * b2 + v3 * b3)]
+        return F, u * b2 - bx1 * v2
+    # HLLD: f + s (U* - U) + s* (U** - U*) on the side of u*
+    out = []
+    for side in ("L", "R"):
+        if side == "L":
+            rho_, v1_, v2_, re_, pt_, b2_, vb_ = rhoL, v1L, v2L, reL, ptL, b2L, vbL
+            s, ss, rs, v2s, b2s, v2ss, b2ss, res_, ress = sL, ssL, rsL, v2sL_, b2sL, v22, b22, resL, re2L
+        else:
+            rho_, v1_, v2_, re_, pt_, b2_, vb_ = rhoR, v1R, v2R, reR, ptR, b2R, vbR
+            s, ss, rs, v2s, b2s, v2ss, b2ss, res_, ress = sR, ssR, rsR, v2sR_, b2sR, v22, b22, resR, re2R
+        U = [rho_, rho_ * v1_, rho_ * v2_, re_, b2_]
+        f = [rho_ * v1_, rho_ * v1_ * v1_ + pt_ - bx1_2, rho_ * v1_ * v2_ - bx1 * b2_,
+             (re_ + pt_) * v1_ - bx1 * vb_, v1_ * b2_ - bx1 * v2_]
+        Us = [rs, rs * us, rs * v2s, res_, b2s]
+        Uss = [rs, rs * us, rs * v2ss, ress, b2ss]
+        outer = (s > 0.0) if side == "L" else (s < 0.0)
+        inner = (ss > 0.0) if side == "L" else (ss < 0.0)
+        out.append([np.where(outer, fi, np.where(inner, fi + s * (a - u0), fi + s * (a - u0) + ss * (b - a)))
+                    for fi, u0, a, b in zip(f, U, Us, Uss)])
+    left = us > 0.0
+    F = [np.where(left, a, b) for a, b in zip(out[0], out[1])]
+    return F[:4], F[4]
+
+
+def _fill_periodic(a, G):
+    nx = a.shape[0] - 2 * G
+    ny = a.shape[1] - 2 * G
+    a[:G, :] = a[nx:nx + G, :]
+    a[nx + G:, :] = a[G:2 * G, :]
+    a[:, :G] = a[:, ny:ny + G]
+    a[:, ny + G:] = a[:, G:2 * G]
+
+
+def mhd_2d_steps(h, nsteps, low_mach):
+    """Advance a 2D periodic ideal-gas MHD HostGrid `h` (LIM2ND, RK, no WB / gravity / scalars)
+    in place of copies with HLLD (low_mach False) or LHLLD (True) and constrained transport:
+    face EMFs and mass-flux signs (S:8926-8951, S:10101-10144), the upwinded corner EMF
+    (S:11970-12029), the face-B update (S:12258-12380) and b_cc (S:12440-12470), the magnetic
+    energy in prim->cons and cons->prim (S:7057-7117, S:13533-13560) and the magnetosonic CFL
+    bound (S:13827-13836).  Returns (W, eint, temp, b1, b2, dt): padded primitives, interior
+    eint and T, interior face fields (nx+1, ny) and (nx, ny+1), and the next dt."""
+    c = h.cfg
+    G = c.ngc
+    gm = c.gamma_ad
+    igmm1 = 1.0 / (gm - 1.0)
+    inv_mu = 1.0 / c.mu
+    dx1, dx2, _ = c.dx()
+    idx1, idx2 = 1.0 / dx1, 1.0 / dx2
+    nx, ny = c.nx1, c.nx2
+    I = (slice(G, G + nx), slice(G, G + ny))
+    W = [h.prim[v, :, :, 0].copy() for v in range(4)]
+    b1 = h.b_x[0][1:nx + 2, 1:ny + 1, 0].copy()
+    b2 = h.b_x[1][1:nx + 1, 1:ny + 2, 0].copy()
+    B = [np.zeros_like(W[0]), np.zeros_like(W[0])]
+
+    def cell_b():
+        B[0][I] = 0.5 * (b1[1:] + b1[:-1])
+        B[1][I] = 0.5 * (b2[:, 1:] + b2[:, :-1])
+        for a in B:
+            _fill_periodic(a, G)
+
+    cell_b()
+    eint = W[3][I] * igmm1
+    temp = W[3][I] / (RGAS * W[0][I] * inv_mu)
+
+    def cfl():
+        r, v1, v2, pp = (w[I] for w in W)
+        cs = np.sqrt(gm * pp / r)
+        ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0
+        cs = np.sqrt(cs * cs + ca2 / r)
+        smax = ((np.abs(v1) + cs) * idx1 + (np.abs(v2) + cs) * idx2).max()
+        return smax, c.cfl / smax
+
+    def mass_sign(f, rl, rr, smax):
+        m = f / (0.5 * (rl + rr) * smax)
+        return np.where(m > c.mach_ct, 1.0, np.where(m < -c.mach_ct, -1.0, 0.0))
+
+    smax, dt = cfl()
+    # RK2_STEPPER / RK3_STEPPER coefficients (S:7018-7038)
+    rk = {2: [(1.0, 0.0, -1.0), (0.5, 0.5, -0.5)],
+          3: [(1.0, 0.0, -1.0), (0.75, 0.25, -0.25), (1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0))]}[c.rk_stages]
+    for _ in range(nsteps):
+        r, v1, v2 = W[0][I].copy(), W[1][I].copy(), W[2][I].copy()
+        U0 = [r, r * v1, r * v2,
+              eint + 0.5 * r * (v1 * v1 + v2 * v2 + 0.0 * 0.0)
+              + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0)]
+        U = [u.copy() for u in U0]
+        b10, b20 = b1.copy(), b2.copy()
+        for a1, a2, c3 in rk:
+            for w in W:
+                _fill_periodic(w, G)
+            # x1 faces i = 1..nx+1: cells G-1+f | G+f
+            lo, hi = zip(*[_plm(w[G - 2:G + nx, G:G + ny], w[G - 1:G + nx + 1, G:G + ny], w[G:G + nx + 2, G:G + ny])
+                           for w in W + [B[1]]])
+            qL = [x[0:nx + 1] for x in hi[:4]]
+            qR = [x[1:nx + 2] for x in lo[:4]]
+            F, fb = _hlld(qL, qR, [b1, hi[4][0:nx + 1]], [b1, lo[4][1:nx + 2]], gm, c.mach_cutoff, low_mach)
+            e1 = -fb
+            s1 = mass_sign(F[0], qL[0], qR[0], smax)
+            res = [(f[1:] - f[:-1]) * idx1 for f in F]
+            # x2 faces with (v1, v2) -> (v2, -v1) and (B1, B2) -> (B2, -B1)
+            lo, hi = zip(*[_plm(w[G:G + nx, G - 2:G + ny], w[G:G + nx, G - 1:G + ny + 1], w[G:G + nx, G:G + ny + 2])
+                           for w in W + [B[0]]])
+            qL = [x[:, 0:ny + 1] for x in hi[:4]]
+            qR = [x[:, 1:ny + 2] for x in lo[:4]]
+            qL = [qL[0], qL[2], -qL[1], qL[3]]
+            qR = [qR[0], qR[2], -qR[1], qR[3]]
+            F, fb = _hlld(qL, qR, [b2, -hi[4][:, 0:ny + 1]], [b2, -lo[4][:, 1:ny + 2]], gm, c.mach_cutoff, low_mach)
+            F = [F[0], -F[2], F[1], F[3]]
+            e2 = -fb
+            s2 = mass_sign(F[0], qL[0], qR[0], smax)
+            res = [rr + (f[:, 1:] - f[:, :-1]) * idx2 for rr, f in zip(res, F)]
+            # corner EMFs (i = 1..nx+1, j = 1..ny+1), face arrays wrapped by one layer
+            e1x = np.concatenate([e1[:, -1:], e1, e1[:, :1]], axis=1)
+            s1x = np.concatenate([s1[:, -1:], s1, s1[:, :1]], axis=1)
+            e2x = np.concatenate([e2[-1:], e2, e2[:1]], axis=0)
+            s2x = np.concatenate([s2[-1:], s2, s2[:1]], axis=0)
+            ec = -W[1] * B[1] + W[2] * B[0]
+            eN, eS = e1x[:, 1:], e1x[:, :-1]
+            eE, eW = e2x[1:], e2x[:-1]
+            eSW = ec[G - 1:G + nx, G - 1:G + ny]
+            eNW = ec[G - 1:G + nx, G:G + ny + 1]
+            eNE = ec[G:G + nx + 1, G:G + ny + 1]
+            eSE = ec[G:G + nx + 1, G - 1:G + ny]
+            sg = s1x[:, :-1]
+            dS = 0.5 * (1.0 + sg) * (eW - eSW) + 0.5 * (1.0 - sg) * (eE - eSE)
+            sg = s1x[:, 1:]
+            dN = 0.5 * (1.0 + sg) * (eNW - eW) + 0.5 * (1.0 - sg) * (eNE - eE)
+            sg = s2x[:-1]
+            dW = 0.5 * (1.0 + sg) * (eS - eSW) + 0.5 * (1.0 - sg) * (eN - eNW)
+            sg = s2x[1:]
+            dE = 0.5 * (1.0 + sg) * (eSE - eS) + 0.5 * (1.0 - sg) * (eNE - eN)
+            cor = 0.25 * (eS + eW + eN + eE + dS - dN + dW - dE)
+            a3 = c3 * dt
+            b1 = a1 * b10 + a2 * b1 + a3 * ((cor[:, 1:] - cor[:, :-1]) * idx2)
+            b2 = a1 * b20 + a2 * b2 + a3 * ((cor[:-1] - cor[1:]) * idx1)
+            cell_b()
+            U = [a1 * u0 + a2 * u + a3 * rr for u0, u, rr in zip(U0, U, res)]
+            rho = U[0]
+            inv_rho = 1.0 / rho
+            e = U[3] - 0.5 * (U[1] * U[1] + U[2] * U[2] + 0.0 * 0.0) * inv_rho
+            e = e - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0)
+            p = (gm - 1.0) * e
+            W[0][I] = rho
+            W[1][I] = U[1] * inv_rho
+            W[2][I] = U[2] * inv_rho
+            W[3][I] = p
+            temp = p / (rho * RGAS * inv_mu)
+            eint = e
+        smax, dt = cfl()
+    return W, eint, temp, b1, b2, dt
