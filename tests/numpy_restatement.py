@@ -9,8 +9,8 @@ WB momentum fix and EVOLVE_ETOT potential flux (S:8953-8966), gravity (S:12606-1
 (S:7018-7048, S:13518-13531), cons->prim (S:13533-13686) and the CFL dt (S:13707-13960).
 With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073-8136) and
 the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
-`mhd_2d_steps` restates the periodic ideal-MHD step with HLLD or LHLLD and constrained
-transport, read from the same Fortran (its docstring lists the lines).
+`mhd_2d_steps` and `mhd_3d_steps` restate the periodic ideal-MHD step with HLLD or LHLLD
+and constrained transport, read from the same Fortran (their docstrings list the lines).
 Test infrastructure only.
 """
 import numpy as np
@@ -210,16 +210,16 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
     return W, eint, temp, dt
 
 
-# ------------------------------------------------------------------------------ 2D ideal MHD
-def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach):
+# ------------------------------------------------------------------------------ ideal MHD
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=()):
     """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
-    array in the face frame, 2D (v3 = B3 = 0), ideal gas (S:13969-15024).  q = (rho, v1, v2,
-    p), b = (B normal, B transverse).  Returns the four fluxes and fluxb(2)."""
+    array in the face frame, ideal gas (S:13969-15024).  q = (rho, v1, v2, v3, p), b = (B
+    normal, B transverse 2, B transverse 3); in 2D v3 and B3 are zero arrays, as the reference
+    sets them; x the passive scalars' edge values.  Returns the fluxes (rho, m1, m2, m3, E, then
+    one per scalar) and fluxb(2), fluxb(3)."""
     igmm1 = 1.0 / (gm - 1.0)
-    z = np.zeros_like(qL[0])
-    rhoL, v1L, v2L, pL = qL
-    rhoR, v1R, v2R, pR = qR
-    v3L = v3R = z
+    rhoL, v1L, v2L, v3L, pL = qL
+    rhoR, v1R, v2R, v3R, pR = qR
     iL = 1.0 / rhoL
     iR = 1.0 / rhoR
     v2sL = v1L * v1L + v2L * v2L + v3L * v3L
@@ -228,7 +228,7 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach):
     c2R = gm * pR * iR
     reL = pL * igmm1 + 0.5 * rhoL * v2sL
     reR = pR * igmm1 + 0.5 * rhoR * v2sR
-    b2L, b2R, b3L, b3R = bL[1], bR[1], z, z
+    b2L, b2R, b3L, b3R = bL[1], bR[1], bL[2], bR[2]
     bx1 = 0.5 * (bL[0] + bR[0])
     bx1_2 = bx1 * bx1
     pbL = 0.5 * (bx1_2 + b2L * b2L + b3L * b3L)
@@ -312,30 +312,37 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach):
         re = pick(resL, re2L, re2R, resR)
         b2 = pick(b2sL, b22, b22, b2sR)
         b3 = pick(b3sL, b32, b32, b3sR)
-        F = [rho * u, rho * u * u + pst - bx1_2, rho * u * v2 - bx1 * b2,
+        F = [rho * u, rho * u * u + pst - bx1_2, rho * u * v2 - bx1 * b2, rho * u * v3 - bx1 * b3,
              (re + pst) * u - bx1 * (bx1 * u + v2 * b2 + v3 * b3)]
-        return F, u * b2 - bx1 * v2
+        up = np.copysign(1.0, u)
+        hp = 0.5 * (1.0 + up)
+        hm = 0.5 * (1.0 - up)
+        F += [rho * u * (hp * a + hm * b) for a, b in zip(xL, xR)]
+        return F, [u * b2 - bx1 * v2, u * b3 - bx1 * v3]
     # HLLD: f + s (U* - U) + s* (U** - U*) on the side of u*
     out = []
     for side in ("L", "R"):
         if side == "L":
-            rho_, v1_, v2_, re_, pt_, b2_, vb_ = rhoL, v1L, v2L, reL, ptL, b2L, vbL
-            s, ss, rs, v2s, b2s, v2ss, b2ss, res_, ress = sL, ssL, rsL, v2sL_, b2sL, v22, b22, resL, re2L
+            rho_, v1_, v2_, v3_, re_, pt_, b2_, b3_, vb_ = rhoL, v1L, v2L, v3L, reL, ptL, b2L, b3L, vbL
+            s, ss, rs, v2s, v3s, b2s, b3s, res_ = sL, ssL, rsL, v2sL_, v3sL, b2sL, b3sL, resL
+            ress, xs = re2L, xL
         else:
-            rho_, v1_, v2_, re_, pt_, b2_, vb_ = rhoR, v1R, v2R, reR, ptR, b2R, vbR
-            s, ss, rs, v2s, b2s, v2ss, b2ss, res_, ress = sR, ssR, rsR, v2sR_, b2sR, v22, b22, resR, re2R
-        U = [rho_, rho_ * v1_, rho_ * v2_, re_, b2_]
+            rho_, v1_, v2_, v3_, re_, pt_, b2_, b3_, vb_ = rhoR, v1R, v2R, v3R, reR, ptR, b2R, b3R, vbR
+            s, ss, rs, v2s, v3s, b2s, b3s, res_ = sR, ssR, rsR, v2sR_, v3sR, b2sR, b3sR, resR
+            ress, xs = re2R, xR
+        U = [rho_, rho_ * v1_, rho_ * v2_, rho_ * v3_, re_, b2_, b3_] + [rho_ * x for x in xs]
         f = [rho_ * v1_, rho_ * v1_ * v1_ + pt_ - bx1_2, rho_ * v1_ * v2_ - bx1 * b2_,
-             (re_ + pt_) * v1_ - bx1 * vb_, v1_ * b2_ - bx1 * v2_]
-        Us = [rs, rs * us, rs * v2s, res_, b2s]
-        Uss = [rs, rs * us, rs * v2ss, ress, b2ss]
+             rho_ * v1_ * v3_ - bx1 * b3_, (re_ + pt_) * v1_ - bx1 * vb_,
+             v1_ * b2_ - bx1 * v2_, v1_ * b3_ - bx1 * v3_] + [rho_ * v1_ * x for x in xs]
+        Us = [rs, rs * us, rs * v2s, rs * v3s, res_, b2s, b3s] + [rs * x for x in xs]
+        Uss = [rs, rs * us, rs * v22, rs * v32, ress, b22, b32] + [rs * x for x in xs]
         outer = (s > 0.0) if side == "L" else (s < 0.0)
         inner = (ss > 0.0) if side == "L" else (ss < 0.0)
         out.append([np.where(outer, fi, np.where(inner, fi + s * (a - u0), fi + s * (a - u0) + ss * (b - a)))
                     for fi, u0, a, b in zip(f, U, Us, Uss)])
     left = us > 0.0
     F = [np.where(left, a, b) for a, b in zip(out[0], out[1])]
-    return F[:4], F[4]
+    return F[:5] + F[7:], F[5:7]
 
 
 def _fill_periodic(a, G):
@@ -410,8 +417,11 @@ def mhd_2d_steps(h, nsteps, low_mach):
                            for w in W + [B[1]]])
             qL = [x[0:nx + 1] for x in hi[:4]]
             qR = [x[1:nx + 2] for x in lo[:4]]
-            F, fb = _hlld(qL, qR, [b1, hi[4][0:nx + 1]], [b1, lo[4][1:nx + 2]], gm, c.mach_cutoff, low_mach)
-            e1 = -fb
+            z = np.zeros_like(b1)
+            F, fb = _hlld(qL[:3] + [z, qL[3]], qR[:3] + [z, qR[3]], [b1, hi[4][0:nx + 1], z],
+                          [b1, lo[4][1:nx + 2], z], gm, c.mach_cutoff, low_mach)
+            F = F[:3] + F[4:]
+            e1 = -fb[0]
             s1 = mass_sign(F[0], qL[0], qR[0], smax)
             res = [(f[1:] - f[:-1]) * idx1 for f in F]
             # x2 faces with (v1, v2) -> (v2, -v1) and (B1, B2) -> (B2, -B1)
@@ -421,9 +431,11 @@ def mhd_2d_steps(h, nsteps, low_mach):
             qR = [x[:, 1:ny + 2] for x in lo[:4]]
             qL = [qL[0], qL[2], -qL[1], qL[3]]
             qR = [qR[0], qR[2], -qR[1], qR[3]]
-            F, fb = _hlld(qL, qR, [b2, -hi[4][:, 0:ny + 1]], [b2, -lo[4][:, 1:ny + 2]], gm, c.mach_cutoff, low_mach)
-            F = [F[0], -F[2], F[1], F[3]]
-            e2 = -fb
+            z = np.zeros_like(b2)
+            F, fb = _hlld(qL[:3] + [z, qL[3]], qR[:3] + [z, qR[3]], [b2, -hi[4][:, 0:ny + 1], z],
+                          [b2, -lo[4][:, 1:ny + 2], z], gm, c.mach_cutoff, low_mach)
+            F = [F[0], -F[2], F[1], F[4]]
+            e2 = -fb[0]
             s2 = mass_sign(F[0], qL[0], qR[0], smax)
             res = [rr + (f[:, 1:] - f[:, :-1]) * idx2 for rr, f in zip(res, F)]
             # corner EMFs (i = 1..nx+1, j = 1..ny+1), face arrays wrapped by one layer
@@ -465,3 +477,188 @@ def mhd_2d_steps(h, nsteps, low_mach):
             eint = e
         smax, dt = cfl()
     return W, eint, temp, b1, b2, dt
+
+
+def _wrap(a, axis):
+    """One periodic layer on either side of `a` along `axis` (the self-copy of a face array's
+    ghost layer, S:2293-2306)."""
+    n = a.shape[axis]
+    return np.concatenate([np.take(a, [n - 1], axis=axis), a, np.take(a, [0], axis=axis)], axis=axis)
+
+
+def _corner(eA, eB, ec, sA, sB):
+    """Upwinded corner EMF (S:11970-12029 and its x1 / x2 counterparts) from corner-aligned
+    arrays: eA / sA the face EMF and mass-flux sign of the face array that varies along the
+    corner's second axis (N = eA[q], S = eA[q-1]), eB / sB of the one that varies along its
+    first axis (E = eB[p], W = eB[p-1]), ec = (SW, NW, NE, SE) the cell EMFs."""
+    eN, eS, eE, eW, sgN, sgS, sgE, sgW = eA[1], eA[0], eB[1], eB[0], sA[1], sA[0], sB[1], sB[0]
+    eSW, eNW, eNE, eSE = ec
+    dS = 0.5 * (1.0 + sgS) * (eW - eSW) + 0.5 * (1.0 - sgS) * (eE - eSE)
+    dN = 0.5 * (1.0 + sgN) * (eNW - eW) + 0.5 * (1.0 - sgN) * (eNE - eE)
+    dW = 0.5 * (1.0 + sgW) * (eS - eSW) + 0.5 * (1.0 - sgW) * (eN - eNW)
+    dE = 0.5 * (1.0 + sgE) * (eSE - eS) + 0.5 * (1.0 - sgE) * (eNE - eN)
+    return 0.25 * (eS + eW + eN + eE + dS - dN + dW - dE)
+
+
+def mhd_3d_steps(h, nsteps, low_mach):
+    """The 3D counterpart of `mhd_2d_steps` on a triply periodic box: the x2 and x3 frame
+    rotations of states, fluxes and B (S:9715-9747, S:10101-10144, S:10845-10889,
+    S:11241-11286), all three face-EMF components (S:8926-8951 and counterparts), the three
+    corner EMFs (S:11970-12200), the three face-B updates (S:12258-12432) and the 3D dt sum
+    sx3 + sx1 + sx2, with the passive scalars the configuration carries (upwinded by the sign
+    of the contact speed).  Returns (W, eint, temp, [b1, b2, b3], dt)."""
+    c = h.cfg
+    G = c.ngc
+    gm = c.gamma_ad
+    igmm1 = 1.0 / (gm - 1.0)
+    inv_mu = 1.0 / c.mu
+    idx = [1.0 / d for d in c.dx()]
+    n = [c.nx1, c.nx2, c.nx3]
+    I = tuple(slice(G, G + m) for m in n)
+    nv = c.nvars
+    W = [h.prim[v].copy() for v in range(nv)]
+    b = [h.b_x[d][tuple(slice(1, 1 + n[a] + (a == d)) for a in range(3))].copy() for d in range(3)]
+    B = [np.zeros_like(W[0]) for _ in range(3)]
+
+    def cell_b():
+        B[0][I] = 0.5 * (b[0][1:] + b[0][:-1])
+        B[1][I] = 0.5 * (b[1][:, 1:] + b[1][:, :-1])
+        B[2][I] = 0.5 * (b[2][:, :, 1:] + b[2][:, :, :-1])
+        for a in B:
+            _fill_periodic3(a, G)
+
+    cell_b()
+    eint = W[4][I] * igmm1
+    temp = W[4][I] / (RGAS * W[0][I] * inv_mu)
+
+    def cfl():
+        r, v1, v2, v3, pp = (w[I] for w in W[:5])
+        cs = np.sqrt(gm * pp / r)
+        ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]
+        cs = np.sqrt(cs * cs + ca2 / r)
+        sx1 = (np.abs(v1) + cs) * idx[0]
+        sx2 = (np.abs(v2) + cs) * idx[1]
+        sx3 = (np.abs(v3) + cs) * idx[2]
+        smax = (sx3 + sx1 + sx2).max()
+        return smax, c.cfl / smax
+
+    def mass_sign(f, rl, rr, smax):
+        m = f / (0.5 * (rl + rr) * smax)
+        return np.where(m > c.mach_ct, 1.0, np.where(m < -c.mach_ct, -1.0, 0.0))
+
+    def along(a, lo, hi):
+        return tuple(slice(lo, hi) if x == a else I[x] for x in range(3))
+
+    def sweep(a, trans):
+        """Edge states of the faces normal to axis a (face f between padded cells G-1+f and
+        G+f) for the five primitives and the two transverse cell-B components `trans`."""
+        m = n[a]
+        lo, hi = zip(*[_plm(w[along(a, G - 2, G + m)], w[along(a, G - 1, G + m + 1)], w[along(a, G, G + m + 2)])
+                       for w in W + [B[t] for t in trans]])
+        L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
+        R = [np.take(x, range(1, m + 2), axis=a) for x in lo]
+        # primitives, transverse cell B, scalars
+        return L[:5] + L[nv:] + L[5:nv], R[:5] + R[nv:] + R[5:nv]
+
+    smax, dt = cfl()
+    rk = {2: [(1.0, 0.0, -1.0), (0.5, 0.5, -0.5)],
+          3: [(1.0, 0.0, -1.0), (0.75, 0.25, -0.25), (1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0))]}[c.rk_stages]
+    for _ in range(nsteps):
+        r, v1, v2, v3 = (W[v][I].copy() for v in range(4))
+        U0 = [r, r * v1, r * v2, r * v3,
+              eint + 0.5 * r * (v1 * v1 + v2 * v2 + v3 * v3)
+              + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])]
+        U0 += [r * W[v][I] for v in range(5, nv)]
+        U = [u.copy() for u in U0]
+        b0 = [x.copy() for x in b]
+        for a1, a2, c3 in rk:
+            for w in W:
+                _fill_periodic3(w, G)
+            emf = [None, None, None]
+            sgn = [None, None, None]
+            res = None
+            for a in range(3):
+                trans = [t for t in range(3) if t != a]
+                L, R = sweep(a, trans)
+                # face frame: x1 as is, x2 (v1, v2, v3) -> (v2, -v1, v3), x3 -> (v3, v1, v2)
+                if a == 0:
+                    qL, qR = L[:5], R[:5]
+                    bL, bR = [b[0], L[5], L[6]], [b[0], R[5], R[6]]
+                elif a == 1:
+                    qL = [L[0], L[2], -L[1], L[3], L[4]]
+                    qR = [R[0], R[2], -R[1], R[3], R[4]]
+                    bL, bR = [b[1], -L[5], L[6]], [b[1], -R[5], R[6]]
+                else:
+                    qL = [L[0], L[3], L[1], L[2], L[4]]
+                    qR = [R[0], R[3], R[1], R[2], R[4]]
+                    bL, bR = [b[2], L[5], L[6]], [b[2], R[5], R[6]]
+                F, fb = _hlld(qL, qR, bL, bR, gm, c.mach_cutoff, low_mach, L[7:], R[7:])
+                if a == 0:
+                    emf[0] = (None, fb[1], -fb[0])
+                elif a == 1:
+                    F = [F[0], -F[2], F[1]] + F[3:]
+                    emf[1] = (-fb[1], None, -fb[0])
+                else:
+                    F = [F[0], F[2], F[3], F[1]] + F[4:]
+                    emf[2] = (fb[1], -fb[0], None)
+                sgn[a] = mass_sign(F[0], qL[0], qR[0], smax)
+                div = [np.diff(f, axis=a) * idx[a] for f in F]
+                res = div if res is None else [rr + d for rr, d in zip(res, div)]
+            # cell EMFs at the padded cells, then the corners of each axis
+            ec3 = -W[1] * B[1] + W[2] * B[0]
+            ec1 = W[3] * B[1] - W[2] * B[2]
+            ec2 = W[1] * B[2] - W[3] * B[0]
+            nx, ny, nz = n
+            Ix, Iy, Iz = I
+            e, s = _wrap(emf[0][2], 1), _wrap(sgn[0], 1)
+            f, t = _wrap(emf[1][2], 0), _wrap(sgn[1], 0)
+            cor3 = _corner((e[:, :-1], e[:, 1:]), (f[:-1], f[1:]),
+                           (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
+                            ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
+                           (s[:, :-1], s[:, 1:]), (t[:-1], t[1:]))
+            e, s = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
+            f, t = _wrap(emf[2][0], 1), _wrap(sgn[2], 1)
+            cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
+                           (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
+                            ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
+                           (s[:, :, :-1], s[:, :, 1:]), (t[:, :-1], t[:, 1:]))
+            e, s = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
+            f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
+            cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
+                           (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
+                            ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),
+                           (s[:-1], s[1:]), (t[:, :, :-1], t[:, :, 1:]))
+            a3 = c3 * dt
+            t1 = -(cor2[:, :, 1:] - cor2[:, :, :-1]) * idx[2] + (cor3[:, 1:] - cor3[:, :-1]) * idx[1]
+            t2 = (cor1[:, :, 1:] - cor1[:, :, :-1]) * idx[2] + (cor3[:-1] - cor3[1:]) * idx[0]
+            t3 = (cor2[1:] - cor2[:-1]) * idx[0] - (cor1[:, 1:] - cor1[:, :-1]) * idx[1]
+            b = [a1 * x0 + a2 * x + a3 * tt for x0, x, tt in zip(b0, b, (t1, t2, t3))]
+            cell_b()
+            U = [a1 * u0 + a2 * u + a3 * rr for u0, u, rr in zip(U0, U, res)]
+            rho = U[0]
+            inv_rho = 1.0 / rho
+            e = U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * inv_rho
+            e = e - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])
+            p = (gm - 1.0) * e
+            W[0][I] = rho
+            W[1][I] = U[1] * inv_rho
+            W[2][I] = U[2] * inv_rho
+            W[3][I] = U[3] * inv_rho
+            W[4][I] = p
+            for v in range(5, nv):
+                W[v][I] = U[v] * inv_rho
+            temp = p / (rho * RGAS * inv_mu)
+            eint = e
+        smax, dt = cfl()
+    return W, eint, temp, b, dt
+
+
+def _fill_periodic3(a, G):
+    for ax in range(3):
+        m = a.shape[ax] - 2 * G
+        lo = [slice(None)] * 3
+        src = [slice(None)] * 3
+        lo[ax], src[ax] = slice(0, G), slice(m, m + G)
+        a[tuple(lo)] = a[tuple(src)]
+        lo[ax], src[ax] = slice(m + G, m + 2 * G), slice(G, 2 * G)
+        a[tuple(lo)] = a[tuple(src)]

@@ -19,7 +19,7 @@ import pytest
 
 from phlegethon_b200 import helm_table, problems
 from phlegethon_b200.grid import Config, HostGrid
-from util import div_b_max, mirror_axis, permute_axes
+from util import div_b_max, mirror_axis, permute_axes, smooth_box
 
 
 def _run(oracle, h, helm=None, steps=3):
@@ -216,42 +216,6 @@ def test_magnetised_uniform_state_between_walls(oracle, riemann, sdims):
 
 
 # ------------------------------------------------------------------------------ axis permutations
-def _smooth_periodic(shape, periods, rng, stagger=None):
-    """Three random Fourier modes over the index grid of a padded array, periodic with the
-    interior extent along every axis whose period is given (constant along the others);
-    `stagger` marks the face axis, whose index 1 is the left face of cell 1."""
-    idx = np.meshgrid(*[np.arange(s, dtype=float) for s in shape], indexing="ij")
-    f = np.zeros(shape)
-    for _ in range(3):
-        ph, kk, a = rng.uniform(0, 2 * np.pi, 3), rng.integers(1, 3, 3), rng.normal()
-        arg = sum(2 * np.pi * kk[d] * (idx[d] - (0.0 if stagger == d else 0.5)) / periods[d] + ph[d]
-                  for d in range(3) if periods[d] is not None)
-        f += a * np.cos(arg)
-    return f / 3.0
-
-
-def _smooth_box(sdims, riemann, rec, mhd):
-    n = (12, 16, 8 if sdims == 3 else 1)
-    cfg = Config(sdims=sdims, nx1=n[0], nx2=n[1], nx3=n[2], ngc=3 if rec == "lim5th" else 2, nas=1,
-                 mhd=mhd, riemann=riemann, rec=rec, x1u=1.2, x2u=1.0, x3u=0.9, mach_cutoff=1e-4,
-                 bc=[["periodic", "periodic"]] * 3)
-    h = HostGrid(cfg)
-    rng = np.random.default_rng(5)
-    per = [n[d] if d < sdims else None for d in range(3)]
-    h.prim[0] = 1.0 + 0.2 * _smooth_periodic(h.cell_shape, per, rng)
-    for d in range(sdims):
-        h.prim[1 + d] = 0.3 * _smooth_periodic(h.cell_shape, per, rng)
-    h.prim[sdims + 1] = 1.0 + 0.2 * _smooth_periodic(h.cell_shape, per, rng)
-    h.prim[sdims + 2] = 0.5 + 0.2 * _smooth_periodic(h.cell_shape, per, rng)
-    if mhd:
-        for d in range(sdims):
-            # B_d independent of x_d: divergence-free on the faces
-            pd = list(per)
-            pd[d] = None
-            h.b_x[d][...] = 0.4 + 0.3 * _smooth_periodic(h.b_x[d].shape, pd, rng, stagger=d)
-    return h
-
-
 @pytest.mark.parametrize("rec", ["lim2nd", "pph", "lim5th"])
 @pytest.mark.parametrize("riemann", ["hllc", "lhllc", "hlld", "lhlld"])
 @pytest.mark.parametrize("sdims, perm", [(2, (1, 0, 2)), (3, (1, 2, 0))])
@@ -263,7 +227,7 @@ def test_axis_permutation_commutes_with_the_step(oracle, sdims, perm, riemann, r
     direction: a transposed index or a swapped normal component shows up at O(1).  The two runs
     differ only in the order in which the directions' flux differences are summed (2D hydro
     happens to round identically)."""
-    h = _smooth_box(sdims, riemann, rec, mhd=riemann in ("hlld", "lhlld"))
+    h = smooth_box(sdims, riemann, rec, mhd=riemann in ("hlld", "lhlld"))
     hp = permute_axes(h, perm)
     o1 = _run(oracle, h, steps=6)
     o2 = _run(oracle, hp, steps=6)
@@ -310,7 +274,7 @@ def test_mirror_commutes_with_the_step(oracle, sdims, axis, riemann, rec):
     alike and the solvers the left and right states (their single-interface mirror symmetry is
     tested above), the CT corner averages are symmetric, and the update does not favour one
     end of a sweep.  Equal to 4e-15 in the state, 2e-15 in the face B."""
-    h = _smooth_box(sdims, riemann, rec, mhd=riemann in ("hlld", "lhlld"))
+    h = smooth_box(sdims, riemann, rec, mhd=riemann in ("hlld", "lhlld"))
     hm = mirror_axis(h, axis)
     o1 = _run(oracle, h, steps=6)
     o2 = _run(oracle, hm, steps=6)
@@ -346,7 +310,7 @@ def _offcentre_blast(riemann, rec):
 def _supersonic_box(sdims, riemann, rec):
     """The smooth periodic box streaming at Mach ~2 along x1 with FLUX_IS_ALL_MACH: the x1
     faces take the upwind flux where the whole fan moves one way."""
-    h = _smooth_box(sdims, riemann, rec, mhd=riemann == "lhlld")
+    h = smooth_box(sdims, riemann, rec, mhd=riemann == "lhlld")
     h.cfg = h.cfg.replace(all_mach=True)
     h.prim[1] += 2.5
     return h

@@ -123,3 +123,43 @@ def mirror_axis(h, a):
     if h2.b_x[a] is not None:
         h2.b_x[a] *= -1.0
     return h2
+
+
+def smooth_periodic(shape, periods, rng, stagger=None):
+    """Three random Fourier modes over the index grid of a padded array, periodic with the
+    interior extent along every axis whose period is given (constant along the others);
+    `stagger` marks the face axis, whose index 1 is the left face of cell 1."""
+    idx = np.meshgrid(*[np.arange(s, dtype=float) for s in shape], indexing="ij")
+    f = np.zeros(shape)
+    for _ in range(3):
+        ph, kk, a = rng.uniform(0, 2 * np.pi, 3), rng.integers(1, 3, 3), rng.normal()
+        arg = sum(2 * np.pi * kk[d] * (idx[d] - (0.0 if stagger == d else 0.5)) / periods[d] + ph[d]
+                  for d in range(3) if periods[d] is not None)
+        f += a * np.cos(arg)
+    return f / 3.0
+
+
+def smooth_box(sdims, riemann, rec, mhd):
+    """A smooth periodic box of unequal extents and cell counts (12 x 16 [x 8]) with one passive
+    scalar: density, velocity, pressure, scalar and (mhd) face B from `smooth_periodic`, B_d
+    independent of x_d so that div B = 0 on the faces."""
+    from phlegethon_b200.grid import Config, HostGrid
+    n = (12, 16, 8 if sdims == 3 else 1)
+    cfg = Config(sdims=sdims, nx1=n[0], nx2=n[1], nx3=n[2], ngc=3 if rec == "lim5th" else 2, nas=1,
+                 mhd=mhd, riemann=riemann, rec=rec, x1u=1.2, x2u=1.0, x3u=0.9, mach_cutoff=1e-4,
+                 bc=[["periodic", "periodic"]] * 3)
+    h = HostGrid(cfg)
+    rng = np.random.default_rng(5)
+    per = [n[d] if d < sdims else None for d in range(3)]
+    h.prim[0] = 1.0 + 0.2 * smooth_periodic(h.cell_shape, per, rng)
+    for d in range(sdims):
+        h.prim[1 + d] = 0.3 * smooth_periodic(h.cell_shape, per, rng)
+    h.prim[sdims + 1] = 1.0 + 0.2 * smooth_periodic(h.cell_shape, per, rng)
+    h.prim[sdims + 2] = 0.5 + 0.2 * smooth_periodic(h.cell_shape, per, rng)
+    if mhd:
+        for d in range(sdims):
+            # B_d independent of x_d: divergence-free on the faces
+            pd = list(per)
+            pd[d] = None
+            h.b_x[d][...] = 0.4 + 0.3 * smooth_periodic(h.b_x[d].shape, pd, rng, stagger=d)
+    return h
