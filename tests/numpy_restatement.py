@@ -10,7 +10,8 @@ WB momentum fix and EVOLVE_ETOT potential flux (S:8953-8966), gravity (S:12606-1
 With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073-8136) and
 the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
 `mhd_2d_steps` and `mhd_3d_steps` restate the periodic ideal-MHD step with HLLD or LHLLD
-and constrained transport, read from the same Fortran (their docstrings list the lines).
+and constrained transport, and `wb_mhd_2d_steps` the MHD step of the well-balanced gravitating
+box with reflective walls, read from the same Fortran (their docstrings list the lines).
 Test infrastructure only.
 """
 import numpy as np
@@ -662,3 +663,139 @@ def _fill_periodic3(a, G):
         a[tuple(lo)] = a[tuple(src)]
         lo[ax], src[ax] = slice(m + G, m + 2 * G), slice(G, 2 * G)
         a[tuple(lo)] = a[tuple(src)]
+
+
+def wb_mhd_2d_steps(h, nsteps, low_mach):
+    """The 2D MHD step with the hot bubble's well-balanced, gravitating set-up: periodic x,
+    reflective y walls, USE_WB (deviations of rho and p reconstructed, S:7151-7168, and the
+    equilibrium added back at the faces, S:8473-8486), EVOLVE_ETOT, gravity on rho', ideal gas;
+    HLLD or LHLLD with constrained transport.  At the walls the cell values are mirrored with
+    v2 and B2 negated (S:7640-7720) and the ghost face EMFs of the x1 faces take the
+    reflective factor -1 on their E3 with the mass-flux sign copied (S:11494-11590).  Returns
+    (W, eint, temp, b1, b2, dt)."""
+    c = h.cfg
+    G = c.ngc
+    gm = c.gamma_ad
+    igmm1 = 1.0 / (gm - 1.0)
+    inv_mu = 1.0 / c.mu
+    dx1, dx2, _ = c.dx()
+    idx1, idx2 = 1.0 / dx1, 1.0 / dx2
+    nx, ny = c.nx1, c.nx2
+    I = (slice(G, G + nx), slice(G, G + ny))
+    W = [h.prim[v, :, :, 0].copy() for v in range(4)]
+    b1 = h.b_x[0][1:nx + 2, 1:ny + 1, 0].copy()
+    b2 = h.b_x[1][1:nx + 1, 1:ny + 2, 0].copy()
+    B = [np.zeros_like(W[0]), np.zeros_like(W[0])]
+    eq_r = h.eq_prim_cc[0, :, :, 0][I]
+    eq_p = h.eq_prim_cc[1, :, :, 0][I]
+    phi_cc = h.phi_cc[:, :, 0][I]
+    gx, gy = h.grav[0, :, :, 0][I], h.grav[1, :, :, 0][I]
+    erx, epx, phx = h.eq_prim_x[0][0, :, :, 0], h.eq_prim_x[0][1, :, :, 0], h.phi_x[0][:, :, 0]
+    ery, epy, phy = h.eq_prim_x[1][0, :, :, 0], h.eq_prim_x[1][1, :, :, 0], h.phi_x[1][:, :, 0]
+
+    def cell_b():
+        B[0][I] = 0.5 * (b1[1:] + b1[:-1])
+        B[1][I] = 0.5 * (b2[:, 1:] + b2[:, :-1])
+        _fill(B[0], False, G)
+        _fill(B[1], True, G)
+
+    cell_b()
+    eint = W[3][I] * igmm1
+    temp = W[3][I] / (RGAS * W[0][I] * inv_mu)
+
+    def cfl():
+        r, v1, v2, pp = (w[I] for w in W)
+        cs = np.sqrt(gm * pp / r)
+        ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0
+        cs = np.sqrt(cs * cs + ca2 / r)
+        smax = ((np.abs(v1) + cs) * idx1 + (np.abs(v2) + cs) * idx2).max()
+        return smax, c.cfl / smax
+
+    def mass_sign(f, rl, rr, smax):
+        m = f / (0.5 * (rl + rr) * smax)
+        return np.where(m > c.mach_ct, 1.0, np.where(m < -c.mach_ct, -1.0, 0.0))
+
+    smax, dt = cfl()
+    rk = {2: [(1.0, 0.0, -1.0), (0.5, 0.5, -0.5)],
+          3: [(1.0, 0.0, -1.0), (0.75, 0.25, -0.25), (1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0))]}[c.rk_stages]
+    for _ in range(nsteps):
+        r, v1, v2 = W[0][I].copy(), W[1][I].copy(), W[2][I].copy()
+        U0 = [r, r * v1, r * v2,
+              eint + 0.5 * r * (v1 * v1 + v2 * v2 + 0.0 * 0.0)
+              + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0) + r * phi_cc]
+        U = [u.copy() for u in U0]
+        b10, b20 = b1.copy(), b2.copy()
+        for a1, a2, c3 in rk:
+            Wd = [w.copy() for w in W]
+            Wd[0][I] = W[0][I] - eq_r
+            Wd[3][I] = W[3][I] - eq_p
+            for v in range(4):
+                _fill(Wd[v], v == 2, G)
+            z = np.zeros((nx + 1, ny))
+            lo, hi = zip(*[_plm(w[G - 2:G + nx, G:G + ny], w[G - 1:G + nx + 1, G:G + ny], w[G:G + nx + 2, G:G + ny])
+                           for w in Wd + [B[1]]])
+            qL = [x[0:nx + 1] for x in hi[:4]]
+            qR = [x[1:nx + 2] for x in lo[:4]]
+            qL[0] = qL[0] + erx
+            qR[0] = qR[0] + erx
+            qL[3] = qL[3] + epx
+            qR[3] = qR[3] + epx
+            F, fb = _hlld(qL[:3] + [z, qL[3]], qR[:3] + [z, qR[3]], [b1, hi[4][0:nx + 1], z],
+                          [b1, lo[4][1:nx + 2], z], gm, c.mach_cutoff, low_mach)
+            F = F[:3] + F[4:]
+            e1 = -fb[0]
+            s1 = mass_sign(F[0], qL[0], qR[0], smax)
+            F[1] = F[1] - epx
+            F[3] = F[3] + F[0] * phx
+            res = [(f[1:] - f[:-1]) * idx1 for f in F]
+            z = np.zeros((nx, ny + 1))
+            lo, hi = zip(*[_plm(w[G:G + nx, G - 2:G + ny], w[G:G + nx, G - 1:G + ny + 1], w[G:G + nx, G:G + ny + 2])
+                           for w in Wd + [B[0]]])
+            qL = [x[:, 0:ny + 1] for x in hi[:4]]
+            qR = [x[:, 1:ny + 2] for x in lo[:4]]
+            qL = [qL[0], qL[2], -qL[1], qL[3]]
+            qR = [qR[0], qR[2], -qR[1], qR[3]]
+            qL[0] = qL[0] + ery
+            qR[0] = qR[0] + ery
+            qL[3] = qL[3] + epy
+            qR[3] = qR[3] + epy
+            F, fb = _hlld(qL[:3] + [z, qL[3]], qR[:3] + [z, qR[3]], [b2, -hi[4][:, 0:ny + 1], z],
+                          [b2, -lo[4][:, 1:ny + 2], z], gm, c.mach_cutoff, low_mach)
+            F = [F[0], -F[2], F[1], F[4]]
+            e2 = -fb[0]
+            s2 = mass_sign(F[0], qL[0], qR[0], smax)
+            F[2] = F[2] - epy
+            F[3] = F[3] + F[0] * phy
+            res = [rr + (f[:, 1:] - f[:, :-1]) * idx2 for rr, f in zip(res, F)]
+            rdev = Wd[0][I]
+            res[1] = res[1] - rdev * gx
+            res[2] = res[2] - rdev * gy
+            # x1-face EMFs past the walls: E3 negated, the sign copied; x2 faces periodic in x
+            e1x = np.concatenate([-e1[:, :1], e1, -e1[:, -1:]], axis=1)
+            s1x = np.concatenate([s1[:, :1], s1, s1[:, -1:]], axis=1)
+            e2x = _wrap(e2, 0)
+            s2x = _wrap(s2, 0)
+            ec = -Wd[1] * B[1] + Wd[2] * B[0]
+            cor = _corner((e1x[:, :-1], e1x[:, 1:]), (e2x[:-1], e2x[1:]),
+                          (ec[G - 1:G + nx, G - 1:G + ny], ec[G - 1:G + nx, G:G + ny + 1],
+                           ec[G:G + nx + 1, G:G + ny + 1], ec[G:G + nx + 1, G - 1:G + ny]),
+                          (s1x[:, :-1], s1x[:, 1:]), (s2x[:-1], s2x[1:]))
+            a3 = c3 * dt
+            b1 = a1 * b10 + a2 * b1 + a3 * ((cor[:, 1:] - cor[:, :-1]) * idx2)
+            b2 = a1 * b20 + a2 * b2 + a3 * ((cor[:-1] - cor[1:]) * idx1)
+            cell_b()
+            U = [a1 * u0 + a2 * u + a3 * rr for u0, u, rr in zip(U0, U, res)]
+            rho = U[0]
+            inv_rho = 1.0 / rho
+            e = U[3] - 0.5 * (U[1] * U[1] + U[2] * U[2] + 0.0 * 0.0) * inv_rho
+            e = e - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + 0.0 * 0.0)
+            e = e - rho * phi_cc
+            p = (gm - 1.0) * e
+            W[0][I] = rho
+            W[1][I] = U[1] * inv_rho
+            W[2][I] = U[2] * inv_rho
+            W[3][I] = p
+            temp = p / (rho * RGAS * inv_mu)
+            eint = e
+        smax, dt = cfl()
+    return W, eint, temp, b1, b2, dt
