@@ -138,3 +138,56 @@ def test_oracle_wb_mhd_with_walls_matches_numpy_restatement(oracle, riemann):
     np.testing.assert_array_equal(h.bface_interior(0)[:, :, 0], b1)
     np.testing.assert_array_equal(h.bface_interior(1)[:, :, 0], b2)
     assert o.g.dt == dt
+
+
+@pytest.fixture(scope="module")
+def eos_case(oracle):
+    from phlegethon_b200 import helm_table
+    import numpy_restatement_eos as R
+    tab, dpdr = helm_table.generate(nrho=271, nT=101)
+    k = dict(nT=101, nrho=271, ltlo=3.0, lthi=13.0, ldlo=-12.0, ldhi=15.0)
+    helm = oracle.Helm(tab, dpdr, **k)
+    rng = np.random.default_rng(1)
+    n = 2000
+    rho = 10 ** rng.uniform(-2, 9, n)
+    T = 10 ** rng.uniform(4, 10, n)
+    abar = rng.uniform(1, 56, n)
+    zbar = abar * rng.uniform(0.3, 0.6, n)
+    return R, tab, dpdr, R.nodes(**k), helm, rng, (rho, T, abar, zbar)
+
+
+def test_oracle_helmholtz_evaluation_matches_numpy_restatement(eos_case):
+    """helm_rhoT_given_full, given1 and given2 of the C oracle equal the numpy restatement bit
+    for bit over 2000 random (rho, T, Abar, Zbar) across the table, and so do the table nodes."""
+    R, tab, dpdr, nd, helm, _, (rho, T, abar, zbar) = eos_case
+    assert np.array_equal(nd[0], helm.T) and np.array_equal(nd[1], helm.rho)
+    full = R.given_full(tab, dpdr, nd, rho, T, abar, zbar)
+    o = np.array([helm.given_full(*a) for a in zip(rho, T, abar, zbar)])
+    for i in range(4):
+        np.testing.assert_array_equal(full[i], o[:, i])
+    for deriv in (True, False):
+        e2 = R.given2(tab, nd, rho, T, abar, zbar, deriv)
+        o2 = np.array([helm.given2(*a, deriv=deriv) for a in zip(rho, T, abar, zbar)])
+        p1 = R.given1(tab, nd, rho, T, abar, zbar, deriv)
+        o1 = np.array([helm.given1(*a, deriv=deriv) for a in zip(rho, T, abar, zbar)])
+        for i in range(2):
+            np.testing.assert_array_equal(e2[i], o2[:, i])
+            np.testing.assert_array_equal(p1[i], o1[:, i])
+
+
+def test_oracle_newton_inversions_match_numpy_restatement(eos_case):
+    """helm_rhoe_given and helm_rhoP_given from guesses 30% off: the same temperature, pressure
+    or energy, sound speed and number of iterations for every sample."""
+    R, tab, dpdr, nd, helm, rng, (rho, T, abar, zbar) = eos_case
+    tl, th = 10.0 ** 3.0, 10.0 ** 13.0   # Tl_eos, Th_eos = 10**helm_ltlo, 10**helm_lthi
+    T0 = T * rng.uniform(0.7, 1.3, T.size)
+    E0 = R.given2(tab, nd, rho, T, abar, zbar)[0]
+    got = R.rhoe_given(tab, dpdr, nd, rho, E0, abar, zbar, T0, tl, th)
+    o = np.array([helm.rhoe_given(*a) for a in zip(rho, E0, abar, zbar, T0)])
+    for i in range(4):
+        np.testing.assert_array_equal(got[i], o[:, i])
+    P0 = R.given1(tab, nd, rho, T, abar, zbar)[0]
+    got = R.rhoP_given(tab, dpdr, nd, rho, P0, abar, zbar, T0, tl, th)
+    o = np.array([helm.rhoP_given(*a) for a in zip(rho, P0, abar, zbar, T0)])
+    for i in range(4):
+        np.testing.assert_array_equal(got[i], o[:, i])
