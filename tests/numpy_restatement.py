@@ -29,6 +29,36 @@ def _plm(qm, qc, qp):
     return qc - t, qc + t
 
 
+def _rec(q, kind, limited):
+    """Edge values (left, right) of a row of cells from the views q = (q_{i-2}, q_{i-1}, q_i,
+    q_{i+1}, q_{i+2}) (the outer two may be None for LIM2ND and PPH): LIM2ND PLM, PPH (third
+    order, with the limiter only where `limited`) or LIM5TH (fifth order, always limited)
+    (S:8141-8323)."""
+    qmm, qm, qc, qp, qpp = q
+    if kind == "lim2nd":
+        return _plm(qm, qc, qp)
+    if kind == "pph":
+        tmp = (5.0 / 6.0) * qc
+        am = (1.0 / 3.0) * qm + tmp - (1.0 / 6.0) * qp
+        ap = -(1.0 / 6.0) * qm + tmp + (1.0 / 3.0) * qp
+        if not limited:
+            return am, ap
+    else:
+        tmp = 329.0 * qc
+        am = (-21.0 * qmm + 189.0 * qm + tmp - 91.0 * qp + 14.0 * qpp) * (1.0 / 420.0)
+        ap = (14.0 * qmm - 91.0 * qm + tmp + 189.0 * qp - 21.0 * qpp) * (1.0 / 420.0)
+    am = np.minimum(np.maximum(am, np.minimum(qm, qc)), np.maximum(qm, qc))
+    ap = np.minimum(np.maximum(ap, np.minimum(qc, qp)), np.maximum(qc, qp))
+    am = am - qc
+    ap = ap - qc
+    flat = ap * am >= 0.0
+    ap = np.where(~flat & (np.abs(ap) >= 2.0 * np.abs(am)), -2.0 * am, ap)
+    am = np.where(~flat & (np.abs(am) >= 2.0 * np.abs(ap)), -2.0 * ap, am)
+    ap = np.where(flat, 0.0, ap)
+    am = np.where(flat, 0.0, am)
+    return am + qc, ap + qc
+
+
 def _lhllc(qL, qR, gm, mach_cutoff):
     igmm1 = 1.0 / (gm - 1.0)
     rhoL, v1L, v2L, pL = qL
@@ -108,9 +138,10 @@ def _fill(a, flip_y, G):
         a[:, ny + G - 1 + g] = (-1.0 if flip_y else 1.0) * a[:, ny + G - g]
 
 
-def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
+def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None, rec="lim2nd"):
     """Advance the hot-bubble HostGrid `h` (2D, ideal, WB+ETOT+gravity, LHLLC, RK3) in place;
-    eps_sf: USE_SHOCK_FLATTENING with that threshold (ngc >= 3)."""
+    eps_sf: USE_SHOCK_FLATTENING with that threshold (ngc >= 3); rec: LIM2ND, PPH or LIM5TH
+    (ngc >= 3) edge values of the primitives (no scalars: PPH leaves them unlimited)."""
     c = h.cfg
     G = c.ngc
     gm = c.gamma_ad
@@ -157,8 +188,8 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
             if eps_sf is not None:
                 fl = _flags(Wd[3] + h.eq_prim_cc[1, :, :, 0], G, nx, ny, eps_sf)
             # x1 sweep: faces i = 0..nx (index of the low face of interior cell i)
-            lo, hi = zip(*[_plm(w[G - 2:G + nx, G:G + ny], w[G - 1:G + nx + 1, G:G + ny], w[G:G + nx + 2, G:G + ny])
-                           for w in Wd])
+            lo, hi = zip(*[_rec([w[G - 3 + o:G + nx - 1 + o, G:G + ny] if G - 3 + o >= 0 else None
+                                 for o in range(5)], rec, False) for w in Wd])
             qL = [x[0:nx + 1] for x in hi]
             qR = [x[1:nx + 2] for x in lo]
             qL[0] = qL[0] + erx
@@ -173,8 +204,8 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None):
             F[3] = F[3] + F[0] * phx
             res = [(f[1:] - f[:-1]) * idx1 for f in F]
             # x2 sweep with rotation (v1, v2) <- (v2, -v1)
-            lo, hi = zip(*[_plm(w[G:G + nx, G - 2:G + ny], w[G:G + nx, G - 1:G + ny + 1], w[G:G + nx, G:G + ny + 2])
-                           for w in Wd])
+            lo, hi = zip(*[_rec([w[G:G + nx, G - 3 + o:G + ny - 1 + o] if G - 3 + o >= 0 else None
+                                 for o in range(5)], rec, False) for w in Wd])
             qL = [x[:, 0:ny + 1] for x in hi]
             qR = [x[:, 1:ny + 2] for x in lo]
             qL = [qL[0], qL[2], -qL[1], qL[3]]
@@ -507,7 +538,8 @@ def mhd_3d_steps(h, nsteps, low_mach):
     S:11241-11286), all three face-EMF components (S:8926-8951 and counterparts), the three
     corner EMFs (S:11970-12200), the three face-B updates (S:12258-12432) and the 3D dt sum
     sx3 + sx1 + sx2, with the passive scalars the configuration carries (upwinded by the sign
-    of the contact speed).  Returns (W, eint, temp, [b1, b2, b3], dt)."""
+    of the contact speed) and its reconstruction (LIM2ND, PPH or LIM5TH; the cell B edges by
+    the same formulas, S:8327-8469).  Returns (W, eint, temp, [b1, b2, b3], dt)."""
     c = h.cfg
     G = c.ngc
     gm = c.gamma_ad
@@ -552,10 +584,13 @@ def mhd_3d_steps(h, nsteps, low_mach):
 
     def sweep(a, trans):
         """Edge states of the faces normal to axis a (face f between padded cells G-1+f and
-        G+f) for the five primitives and the two transverse cell-B components `trans`."""
+        G+f) for the five primitives and the two transverse cell-B components `trans`; with
+        PPH only the scalars are limited."""
         m = n[a]
-        lo, hi = zip(*[_plm(w[along(a, G - 2, G + m)], w[along(a, G - 1, G + m + 1)], w[along(a, G, G + m + 2)])
-                       for w in W + [B[t] for t in trans]])
+        arrs = W + [B[t] for t in trans]
+        lim = [c.rec == "lim5th" or (c.rec == "pph" and 5 <= v < nv) for v in range(len(arrs))]
+        lo, hi = zip(*[_rec([w[along(a, G - 3 + o, G + m - 1 + o)] if G - 3 + o >= 0 else None for o in range(5)],
+                            c.rec, lv) for w, lv in zip(arrs, lim)])
         L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
         R = [np.take(x, range(1, m + 2), axis=a) for x in lo]
         # primitives, transverse cell B, scalars

@@ -24,6 +24,26 @@ def test_oracle_matches_numpy_restatement(oracle):
     assert o.g.dt == dt
 
 
+@pytest.mark.parametrize("rec", ["pph", "lim5th"])
+def test_oracle_higher_order_reconstruction_matches_numpy_restatement(oracle, rec):
+    """The hot bubble with PPH_REC (third order, unlimited primitives) or LIM5TH_REC (fifth
+    order, limited), three ghost layers: bit for bit after five steps."""
+    cfg, h = problems.hot_bubble_2d(32, shock_flattening=True, eps_sf=1e300)
+    h.cfg = cfg = cfg.replace(shock_flattening=False, rec=rec)
+    hn = h.copy()
+    o = oracle.OracleGrid(h, nthreads=2)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(5)
+    W, eint, temp, dt = hot_bubble_steps(hn, 5, rec=rec)
+    G = cfg.ngc
+    I = (slice(G, G + cfg.nx1), slice(G, G + cfg.nx2))
+    for v in range(4):
+        np.testing.assert_array_equal(h.prim[v, :, :, 0][I], W[v][I])
+    np.testing.assert_array_equal(h.interior(h.eint)[:, :, 0], eint)
+    assert o.g.dt == dt
+
+
 @pytest.mark.parametrize("eps_sf", [0.1, 0.1251])
 def test_oracle_shock_flattening_matches_numpy_restatement(oracle, eps_sf):
     """Detector over 3 ghost layers (deviation + ghost equilibrium) and HLL on flagged faces.
@@ -71,13 +91,15 @@ def test_oracle_mhd_matches_numpy_restatement(oracle, riemann, rk_stages):
     assert o.g.dt == dt
 
 
+@pytest.mark.parametrize("rec", ["lim2nd", "pph", "lim5th"])
 @pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
-def test_oracle_3d_mhd_matches_numpy_restatement(oracle, riemann):
+def test_oracle_3d_mhd_matches_numpy_restatement(oracle, riemann, rec):
     """A smooth triply periodic MHD box (12 x 16 x 8, unequal extents, one passive scalar):
     the x2 / x3 frame rotations, the three face-EMF components, the three upwinded corner EMFs
-    and face-B updates, the scalar's upwinded flux and the 3D dt sum of the C oracle equal the
-    numpy restatement bit for bit after four steps."""
-    h = smooth_box(3, riemann, "lim2nd", mhd=True)
+    and face-B updates, the scalar's upwinded flux, the reconstruction of primitives, scalar
+    (limited under PPH) and cell B, and the 3D dt sum of the C oracle equal the numpy
+    restatement bit for bit after four steps."""
+    h = smooth_box(3, riemann, rec, mhd=True)
     hn = h.copy()
     o = oracle.OracleGrid(h, nthreads=2)
     o.init_thermo()
