@@ -10,8 +10,10 @@ WB momentum fix and EVOLVE_ETOT potential flux (S:8953-8966), gravity (S:12606-1
 With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073-8136) and
 the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
 `mhd_2d_steps` and `mhd_3d_steps` restate the periodic ideal-MHD step with HLLD or LHLLD
-and constrained transport, and `wb_mhd_2d_steps` the MHD step of the well-balanced gravitating
-box with reflective walls, read from the same Fortran (their docstrings list the lines).
+and constrained transport, `wb_mhd_2d_steps` the MHD step of the well-balanced gravitating
+box with reflective walls, and `stratified_mhd_steps` the magnetised stratified Helmholtz box
+of the benchmark (with the EoS of numpy_restatement_eos), read from the same Fortran (their
+docstrings list the lines).
 Test infrastructure only.
 """
 import numpy as np
@@ -243,12 +245,14 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None, rec="lim2nd"):
 
 
 # ------------------------------------------------------------------------------ ideal MHD
-def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=()):
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None):
     """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
     array in the face frame, ideal gas (S:13969-15024).  q = (rho, v1, v2, v3, p), b = (B
     normal, B transverse 2, B transverse 3); in 2D v3 and B3 are zero arrays, as the reference
-    sets them; x the passive scalars' edge values.  Returns the fluxes (rho, m1, m2, m3, E, then
-    one per scalar) and fluxb(2), fluxb(3)."""
+    sets them; x the passive scalars' edge values; fasteos = (gamma_e L, gamma_c L, gamma_e R,
+    gamma_c R) replaces the ideal gas by USE_FASTEOS's face gammas (e = p / (gamma_e - 1),
+    c^2 = gamma_c p / rho).  Returns the fluxes (rho, m1, m2, m3, E, then one per scalar) and
+    fluxb(2), fluxb(3)."""
     igmm1 = 1.0 / (gm - 1.0)
     rhoL, v1L, v2L, v3L, pL = qL
     rhoR, v1R, v2R, v3R, pR = qR
@@ -256,10 +260,17 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=()):
     iR = 1.0 / rhoR
     v2sL = v1L * v1L + v2L * v2L + v3L * v3L
     v2sR = v1R * v1R + v2R * v2R + v3R * v3R
-    c2L = gm * pL * iL
-    c2R = gm * pR * iR
-    reL = pL * igmm1 + 0.5 * rhoL * v2sL
-    reR = pR * igmm1 + 0.5 * rhoR * v2sR
+    if fasteos is None:
+        c2L = gm * pL * iL
+        c2R = gm * pR * iR
+        reL = pL * igmm1 + 0.5 * rhoL * v2sL
+        reR = pR * igmm1 + 0.5 * rhoR * v2sR
+    else:
+        geL, gcL, geR, gcR = fasteos
+        reL = pL / (geL - 1.0) + 0.5 * rhoL * v2sL
+        c2L = gcL * pL * iL
+        reR = pR / (geR - 1.0) + 0.5 * rhoR * v2sR
+        c2R = gcR * pR * iR
     b2L, b2R, b3L, b3R = bL[1], bR[1], bL[2], bR[2]
     bx1 = 0.5 * (bL[0] + bR[0])
     bx1_2 = bx1 * bx1
@@ -834,3 +845,210 @@ def wb_mhd_2d_steps(h, nsteps, low_mach):
             eint = e
         smax, dt = cfl()
     return W, eint, temp, b1, b2, dt
+
+
+def _fill_strat(a, G, flip):
+    """Ghosts of a padded 3D cell array of the stratified box: periodic along x1 and x3,
+    mirrored at the x2 walls (negated when `flip`: v2, B2) over every x1 / x3 index
+    (S:7640-7720)."""
+    for ax in (0, 2):
+        m = a.shape[ax] - 2 * G
+        lo = [slice(None)] * 3
+        src = [slice(None)] * 3
+        lo[ax], src[ax] = slice(0, G), slice(m, m + G)
+        a[tuple(lo)] = a[tuple(src)]
+        lo[ax], src[ax] = slice(m + G, m + 2 * G), slice(G, 2 * G)
+        a[tuple(lo)] = a[tuple(src)]
+    ny = a.shape[1] - 2 * G
+    f = -1.0 if flip else 1.0
+    for g in range(1, G + 1):
+        a[:, G - g] = f * a[:, G + g - 1]
+        a[:, ny + G - 1 + g] = f * a[:, ny + G - g]
+
+
+def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
+    """The magnetised stratified Helmholtz box (3D, x2 vertical between reflective walls, x1 /
+    x3 periodic): USE_WB on rho, p and gamma_e (S:7151-7168, the equilibria added back at the
+    faces, S:8473-8486, S:8714-8727), USE_FASTEOS face gammas in the Riemann solver
+    (S:14223-14226), EVOLVE_ETOT, gravity on rho' (S:12606-12644), ADVECT_YE_IABAR scalars,
+    LHLLD (or HLLD) with constrained transport and the reflective EMF ghosts of the x1 and x3
+    faces (S:11494-11590), the step-0 thermodynamics through helm_rhoP_given (S:6350-6357),
+    cons->prim through helm_rhoe_given from the previous temperature with the gammas renewed
+    (S:13640-13647), and the dt from helm_rhoT_given_full.  LIM2ND.  Returns (W, eint, temp,
+    gammaf, [b1, b2, b3], dt)."""
+    from numpy_restatement_eos import given_full, rhoe_given, rhoP_given
+    c = h.cfg
+    G = c.ngc
+    tl, th = 10.0 ** c.helm_ltlo, 10.0 ** c.helm_lthi
+    idx = [1.0 / d for d in c.dx()]
+    n = [c.nx1, c.nx2, c.nx3]
+    I = tuple(slice(G, G + m) for m in n)
+    nv = c.nvars
+    W = [h.prim[v].copy() for v in range(nv)]
+    temp = h.temp[I].copy()
+    b = [h.b_x[d][tuple(slice(1, 1 + n[a] + (a == d)) for a in range(3))].copy() for d in range(3)]
+    B = [np.zeros_like(W[0]) for _ in range(3)]
+    ge, gc = np.zeros_like(W[0]), np.zeros_like(W[0])
+    eq_r, eq_p, eq_ge = h.eq_prim_cc[0][I], h.eq_prim_cc[1][I], h.eq_gammae_cc[I]
+    phi = h.phi_cc[I]
+    grav = [h.grav[d][I] for d in range(3)]
+    eqf = [(h.eq_prim_x[d][0], h.eq_prim_x[d][1], h.eq_gammae_x[d], h.phi_x[d]) for d in range(3)]
+
+    def cell_b():
+        B[0][I] = 0.5 * (b[0][1:] + b[0][:-1])
+        B[1][I] = 0.5 * (b[1][:, 1:] + b[1][:, :-1])
+        B[2][I] = 0.5 * (b[2][:, :, 1:] + b[2][:, :, :-1])
+        for d, a in enumerate(B):
+            _fill_strat(a, G, d == 1)
+
+    cell_b()
+    # step-0 thermodynamics
+    rho, p = W[0][I], W[4][I]
+    abar = 1.0 / W[6][I]
+    zbar = abar * W[5][I]
+    temp, E, snd, _ = rhoP_given(tab, dpdr, nd, rho, p, abar, zbar, temp, tl, th)
+    eint = rho * E
+    ge[I] = p / eint + 1.0
+    gc[I] = snd * snd * rho / p
+
+    def cfl():
+        r, v1, v2, v3 = (W[v][I] for v in range(4))
+        ab = 1.0 / W[6][I]
+        _, _, cs, _ = given_full(tab, dpdr, nd, r, temp, ab, W[5][I] * ab)
+        ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]
+        cs = np.sqrt(cs * cs + ca2 / r)
+        sx1 = (np.abs(v1) + cs) * idx[0]
+        sx2 = (np.abs(v2) + cs) * idx[1]
+        sx3 = (np.abs(v3) + cs) * idx[2]
+        smax = (sx3 + sx1 + sx2).max()
+        return smax, c.cfl / smax
+
+    def mass_sign(f, rl, rr, smax):
+        m = f / (0.5 * (rl + rr) * smax)
+        return np.where(m > c.mach_ct, 1.0, np.where(m < -c.mach_ct, -1.0, 0.0))
+
+    def along(a, lo, hi):
+        return tuple(slice(lo, hi) if x == a else I[x] for x in range(3))
+
+    def wall_wrap(e, flip):
+        """One ghost layer of a face array along x2: the mirrored row times the wall factor."""
+        f = -1.0 if flip else 1.0
+        return np.concatenate([f * e[:, :1], e, f * e[:, -1:]], axis=1)
+
+    smax, dt = cfl()
+    rk = {2: [(1.0, 0.0, -1.0), (0.5, 0.5, -0.5)],
+          3: [(1.0, 0.0, -1.0), (0.75, 0.25, -0.25), (1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0))]}[c.rk_stages]
+    for _ in range(nsteps):
+        r, v1, v2, v3 = (W[v][I].copy() for v in range(4))
+        U0 = [r, r * v1, r * v2, r * v3,
+              eint + 0.5 * r * (v1 * v1 + v2 * v2 + v3 * v3)
+              + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]) + r * phi]
+        U0 += [r * W[v][I] for v in range(5, nv)]
+        U = [u.copy() for u in U0]
+        b0 = [x.copy() for x in b]
+        for a1, a2, c3 in rk:
+            Wd = [w.copy() for w in W]
+            Wd[0][I] = W[0][I] - eq_r
+            Wd[4][I] = W[4][I] - eq_p
+            ged = ge.copy()
+            ged[I] = ge[I] - eq_ge
+            gcd = gc.copy()
+            for v, w in enumerate(Wd):
+                _fill_strat(w, G, v == 2)
+            _fill_strat(ged, G, False)
+            _fill_strat(gcd, G, False)
+            emf = [None, None, None]
+            sgn = [None, None, None]
+            res = None
+            for a in range(3):
+                m = n[a]
+                trans = [t for t in range(3) if t != a]
+                arrs = Wd + [B[t] for t in trans] + [ged, gcd]
+                lo, hi = zip(*[_plm(w[along(a, G - 2, G + m)], w[along(a, G - 1, G + m + 1)],
+                                    w[along(a, G, G + m + 2)]) for w in arrs])
+                L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
+                R = [np.take(x, range(1, m + 2), axis=a) for x in lo]
+                er, ep, eg, ph = eqf[a]
+                for side in (L, R):
+                    side[0] = side[0] + er
+                    side[4] = side[4] + ep
+                    side[nv + 2] = side[nv + 2] + eg
+                bt = (L[nv], L[nv + 1]), (R[nv], R[nv + 1])
+                if a == 0:
+                    qL, qR = L[:5], R[:5]
+                    bL, bR = [b[0], bt[0][0], bt[0][1]], [b[0], bt[1][0], bt[1][1]]
+                elif a == 1:
+                    qL = [L[0], L[2], -L[1], L[3], L[4]]
+                    qR = [R[0], R[2], -R[1], R[3], R[4]]
+                    bL, bR = [b[1], -bt[0][0], bt[0][1]], [b[1], -bt[1][0], bt[1][1]]
+                else:
+                    qL = [L[0], L[3], L[1], L[2], L[4]]
+                    qR = [R[0], R[3], R[1], R[2], R[4]]
+                    bL, bR = [b[2], bt[0][0], bt[0][1]], [b[2], bt[1][0], bt[1][1]]
+                F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv],
+                              fasteos=(L[nv + 2], L[nv + 3], R[nv + 2], R[nv + 3]))
+                if a == 0:
+                    emf[0] = (None, fb[1], -fb[0])
+                elif a == 1:
+                    F = [F[0], -F[2], F[1]] + F[3:]
+                    emf[1] = (-fb[1], None, -fb[0])
+                else:
+                    F = [F[0], F[2], F[3], F[1]] + F[4:]
+                    emf[2] = (fb[1], -fb[0], None)
+                sgn[a] = mass_sign(F[0], qL[0], qR[0], smax)
+                F[1 + a] = F[1 + a] - ep
+                F[4] = F[4] + F[0] * ph
+                div = [np.diff(f, axis=a) * idx[a] for f in F]
+                res = div if res is None else [rr + d for rr, d in zip(res, div)]
+            rdev = Wd[0][I]
+            for d in range(3):
+                res[1 + d] = res[1 + d] - rdev * grav[d]
+            ec3 = -Wd[1] * B[1] + Wd[2] * B[0]
+            ec1 = Wd[3] * B[1] - Wd[2] * B[2]
+            ec2 = Wd[1] * B[2] - Wd[3] * B[0]
+            nx, ny, nz = n
+            Ix, Iy, Iz = I
+            e, s_ = wall_wrap(emf[0][2], True), wall_wrap(sgn[0], False)
+            f, t = _wrap(emf[1][2], 0), _wrap(sgn[1], 0)
+            cor3 = _corner((e[:, :-1], e[:, 1:]), (f[:-1], f[1:]),
+                           (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
+                            ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
+                           (s_[:, :-1], s_[:, 1:]), (t[:-1], t[1:]))
+            e, s_ = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
+            f, t = wall_wrap(emf[2][0], True), wall_wrap(sgn[2], False)
+            cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
+                           (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
+                            ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
+                           (s_[:, :, :-1], s_[:, :, 1:]), (t[:, :-1], t[:, 1:]))
+            e, s_ = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
+            f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
+            cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
+                           (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
+                            ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),
+                           (s_[:-1], s_[1:]), (t[:, :, :-1], t[:, :, 1:]))
+            a3 = c3 * dt
+            t1 = -(cor2[:, :, 1:] - cor2[:, :, :-1]) * idx[2] + (cor3[:, 1:] - cor3[:, :-1]) * idx[1]
+            t2 = (cor1[:, :, 1:] - cor1[:, :, :-1]) * idx[2] + (cor3[:-1] - cor3[1:]) * idx[0]
+            t3 = (cor2[1:] - cor2[:-1]) * idx[0] - (cor1[:, 1:] - cor1[:, :-1]) * idx[1]
+            b = [a1 * x0 + a2 * x + a3 * tt for x0, x, tt in zip(b0, b, (t1, t2, t3))]
+            cell_b()
+            U = [a1 * u0 + a2 * u + a3 * rr for u0, u, rr in zip(U0, U, res)]
+            rho = U[0]
+            inv_rho = 1.0 / rho
+            e_ = U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * inv_rho
+            e_ = e_ - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])
+            e_ = e_ - rho * phi
+            ye = U[5] * inv_rho
+            ab = rho / U[6]
+            temp, p, snd, _ = rhoe_given(tab, dpdr, nd, rho, e_ * inv_rho, ab, ye * ab, temp, tl, th)
+            ge[I] = p / e_ + 1.0
+            gc[I] = snd * snd * rho / p
+            W[0][I] = rho
+            for d in range(3):
+                W[1 + d][I] = U[1 + d] * inv_rho
+            W[4][I] = p
+            for v in range(5, nv):
+                W[v][I] = U[v] * inv_rho
+            eint = e_
+        smax, dt = cfl()
+    return W, eint, temp, (ge, gc), b, dt
