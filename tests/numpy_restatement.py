@@ -245,14 +245,15 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None, rec="lim2nd"):
 
 
 # ------------------------------------------------------------------------------ ideal MHD
-def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None):
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None, side_eos=None):
     """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
     array in the face frame, ideal gas (S:13969-15024).  q = (rho, v1, v2, v3, p), b = (B
     normal, B transverse 2, B transverse 3); in 2D v3 and B3 are zero arrays, as the reference
     sets them; x the passive scalars' edge values; fasteos = (gamma_e L, gamma_c L, gamma_e R,
     gamma_c R) replaces the ideal gas by USE_FASTEOS's face gammas (e = p / (gamma_e - 1),
-    c^2 = gamma_c p / rho).  Returns the fluxes (rho, m1, m2, m3, E, then one per scalar) and
-    fluxb(2), fluxb(3)."""
+    c^2 = gamma_c p / rho); side_eos = (e L, c^2 L, e R, c^2 R) takes each side's internal
+    energy and sound speed squared as given (the Helmholtz solves without USE_FASTEOS).
+    Returns the fluxes (rho, m1, m2, m3, E, then one per scalar) and fluxb(2), fluxb(3)."""
     igmm1 = 1.0 / (gm - 1.0)
     rhoL, v1L, v2L, v3L, pL = qL
     rhoR, v1R, v2R, v3R, pR = qR
@@ -260,7 +261,11 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None)
     iR = 1.0 / rhoR
     v2sL = v1L * v1L + v2L * v2L + v3L * v3L
     v2sR = v1R * v1R + v2R * v2R + v3R * v3R
-    if fasteos is None:
+    if side_eos is not None:
+        eL, c2L, eR, c2R = side_eos
+        reL = eL + 0.5 * rhoL * v2sL
+        reR = eR + 0.5 * rhoR * v2sR
+    elif fasteos is None:
         c2L = gm * pL * iL
         c2R = gm * pR * iR
         reL = pL * igmm1 + 0.5 * rhoL * v2sL
@@ -874,8 +879,11 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
     LHLLD (or HLLD) with constrained transport and the reflective EMF ghosts of the x1 and x3
     faces (S:11494-11590), the step-0 thermodynamics through helm_rhoP_given (S:6350-6357),
     cons->prim through helm_rhoe_given from the previous temperature with the gammas renewed
-    (S:13640-13647), and the dt from helm_rhoT_given_full.  LIM2ND.  Returns (W, eint, temp,
-    gammaf, [b1, b2, b3], dt)."""
+    (S:13640-13647), and the dt from helm_rhoT_given_full.  Without USE_FASTEOS each Riemann
+    side solves helm_rhoP_given from the face guess (T(i-1) + T(i)) / 2 of the stage input's
+    temperatures (S:8488-8495, S:14250-14256) with its own reconstructed Ye and 1/Abar, and the
+    gammas are neither reconstructed nor kept.  LIM2ND.  Returns (W, eint, temp, gammaf,
+    [b1, b2, b3], dt)."""
     from numpy_restatement_eos import given_full, rhoe_given, rhoP_given
     c = h.cfg
     G = c.ngc
@@ -906,10 +914,12 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
     rho, p = W[0][I], W[4][I]
     abar = 1.0 / W[6][I]
     zbar = abar * W[5][I]
-    temp, E, snd, _ = rhoP_given(tab, dpdr, nd, rho, p, abar, zbar, temp, tl, th)
+    fast = c.fasteos
+    temp, E, snd, _ = rhoP_given(tab, dpdr, nd, rho, p, abar, zbar, temp, tl, th, return_sound=fast)
     eint = rho * E
-    ge[I] = p / eint + 1.0
-    gc[I] = snd * snd * rho / p
+    if fast:
+        ge[I] = p / eint + 1.0
+        gc[I] = snd * snd * rho / p
 
     def cfl():
         r, v1, v2, v3 = (W[v][I] for v in range(4))
@@ -957,6 +967,9 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
                 _fill_strat(w, G, v == 2)
             _fill_strat(ged, G, False)
             _fill_strat(gcd, G, False)
+            tpad = np.zeros_like(W[0])
+            tpad[I] = temp
+            _fill_strat(tpad, G, False)
             emf = [None, None, None]
             sgn = [None, None, None]
             res = None
@@ -985,8 +998,17 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
                     qL = [L[0], L[3], L[1], L[2], L[4]]
                     qR = [R[0], R[3], R[1], R[2], R[4]]
                     bL, bR = [b[2], bt[0][0], bt[0][1]], [b[2], bt[1][0], bt[1][1]]
-                F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv],
-                              fasteos=(L[nv + 2], L[nv + 3], R[nv + 2], R[nv + 3]))
+                if fast:
+                    eos = dict(fasteos=(L[nv + 2], L[nv + 3], R[nv + 2], R[nv + 3]))
+                else:
+                    tg = 0.5 * (tpad[along(a, G - 1, G + m)] + tpad[along(a, G, G + m + 1)])
+                    sides = []
+                    for q in (L, R):
+                        ab = 1.0 / q[6]
+                        _, e1, s1, _ = rhoP_given(tab, dpdr, nd, q[0], q[4], ab, q[5] * ab, tg, tl, th)
+                        sides += [e1 * q[0], s1 * s1]
+                    eos = dict(side_eos=tuple(sides))
+                F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], **eos)
                 if a == 0:
                     emf[0] = (None, fb[1], -fb[0])
                 elif a == 1:
@@ -1040,9 +1062,11 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
             e_ = e_ - rho * phi
             ye = U[5] * inv_rho
             ab = rho / U[6]
-            temp, p, snd, _ = rhoe_given(tab, dpdr, nd, rho, e_ * inv_rho, ab, ye * ab, temp, tl, th)
-            ge[I] = p / e_ + 1.0
-            gc[I] = snd * snd * rho / p
+            temp, p, snd, _ = rhoe_given(tab, dpdr, nd, rho, e_ * inv_rho, ab, ye * ab, temp, tl, th,
+                                         return_sound=fast)
+            if fast:
+                ge[I] = p / e_ + 1.0
+                gc[I] = snd * snd * rho / p
             W[0][I] = rho
             for d in range(3):
                 W[1 + d][I] = U[1 + d] * inv_rho

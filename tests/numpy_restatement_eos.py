@@ -153,16 +153,22 @@ def _newton(fn, target, T0, tl, th, tol=1.0e-11):
     return T, used
 
 
-def rhoe_given(tab, dpdr, nd, rho, E0, abar, zbar, T0, tl, th):
-    """helm_rhoe_given with return_sound: T, P, sound speed and the evaluation count."""
+def rhoe_given(tab, dpdr, nd, rho, E0, abar, zbar, T0, tl, th, return_sound=True):
+    """helm_rhoe_given: T, P, sound speed (0 without return_sound, P then from given1) and the
+    evaluation count."""
     T, used = _newton(lambda t: given2(tab, nd, rho, t, abar, zbar), E0, T0, tl, th)
+    if not return_sound:
+        return T, given1(tab, nd, rho, T, abar, zbar, deriv=False)[0], 0.0, used
     P, _, sound, _ = given_full(tab, dpdr, nd, rho, T, abar, zbar)
     return T, P, sound, used
 
 
-def rhoP_given(tab, dpdr, nd, rho, P0, abar, zbar, T0, tl, th):
-    """helm_rhoP_given with return_sound: T, E, sound speed and the evaluation count."""
+def rhoP_given(tab, dpdr, nd, rho, P0, abar, zbar, T0, tl, th, return_sound=True):
+    """helm_rhoP_given: T, E, sound speed (0 without return_sound, E then from given2) and the
+    evaluation count."""
     T, used = _newton(lambda t: given1(tab, nd, rho, t, abar, zbar), P0, T0, tl, th)
+    if not return_sound:
+        return T, given2(tab, nd, rho, T, abar, zbar, deriv=False)[0], 0.0, used
     _, E, sound, _ = given_full(tab, dpdr, nd, rho, T, abar, zbar)
     return T, E, sound, used
 
