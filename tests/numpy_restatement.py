@@ -11,9 +11,9 @@ With eps_sf set it adds USE_SHOCK_FLATTENING: the pressure-jump detector (S:8073
 the HLL flux on faces next to a flagged cell (S:15929-16010); LIM2ND cells need no fallback.
 `mhd_2d_steps` and `mhd_3d_steps` restate the periodic ideal-MHD step with HLLD or LHLLD
 and constrained transport, `wb_mhd_2d_steps` the MHD step of the well-balanced gravitating
-box with reflective walls, and `stratified_mhd_steps` the magnetised stratified Helmholtz box
-of the benchmark (with the EoS of numpy_restatement_eos), read from the same Fortran (their
-docstrings list the lines).
+box with reflective walls, and `stratified_steps` the stratified Helmholtz boxes of the
+benchmark, hydro (LHLLC / HLLC, FLUX_IS_ALL_MACH) or magnetised (with the EoS of
+numpy_restatement_eos), read from the same Fortran (their docstrings list the lines).
 Test infrastructure only.
 """
 import numpy as np
@@ -527,6 +527,74 @@ def mhd_2d_steps(h, nsteps, low_mach):
     return W, eint, temp, b1, b2, dt
 
 
+def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fasteos=None, side_eos=None):
+    """LHLLC (low_mach True) or HLLC flux of one face array in the face frame, 3D with
+    scalars (S:15611-16260): q = (rho, v1, v2, v3, p); the side EoS as in `_hlld` (here
+    side_eos carries the sound speed itself, as helm_rhoP_given returns it); all_mach:
+    FLUX_IS_ALL_MACH, the upwind state's flux outside the fan (LHLLC only)."""
+    rhoL, v1L, v2L, v3L, pL = qL
+    rhoR, v1R, v2R, v3R, pR = qR
+    iL = 1.0 / rhoL
+    iR = 1.0 / rhoR
+    w2L = v1L * v1L + v2L * v2L + v3L * v3L
+    w2R = v1R * v1R + v2R * v2R + v3R * v3R
+    if side_eos is not None:
+        eL, cL, eR, cR = side_eos
+    elif fasteos is not None:
+        geL, gcL, geR, gcR = fasteos
+        eL = pL / (geL - 1.0)
+        cL = np.sqrt(gcL * pL * iL)
+        eR = pR / (geR - 1.0)
+        cR = np.sqrt(gcR * pR * iR)
+    else:
+        igmm1 = 1.0 / (gm - 1.0)
+        eL = igmm1 * pL
+        cL = np.sqrt(gm * pL * iL)
+        eR = igmm1 * pR
+        cR = np.sqrt(gm * pR * iR)
+    reL = eL + 0.5 * rhoL * w2L
+    reR = eR + 0.5 * rhoR * w2R
+    mc = np.maximum(cL, cR)
+    sL = np.minimum(v1L, v1R) - mc
+    sR = np.maximum(v1L, v1R) + mc
+    dL = sL - v1L
+    dR = sR - v1R
+    us = (pR - pL + rhoL * v1L * dL - rhoR * v1R * dR) / (rhoL * dL - rhoR * dR)
+    rsL = rhoL * (dL / (sL - us))
+    resL = rsL * (reL * iL + (us - v1L) * (us + pL * iL / dL))
+    rsR = rhoR * (dR / (sR - us))
+    resR = rsR * (reR * iR + (us - v1R) * (us + pR * iR / dR))
+    if low_mach:
+        chi = np.maximum(mach_cutoff, np.minimum(1.0, np.maximum(np.sqrt(w2L) / cL, np.sqrt(w2R) / cR)))
+        phi = chi * (2.0 - chi)
+        pst = 0.5 * (pL + pR) - 0.5 * phi * (0.5 * (rhoL + rhoR)) * (0.5 * (cL + cR)) * (v1R - v1L)
+        sg = np.copysign(1.0, us)
+        hp = 0.5 * (1.0 + sg)
+        hm = 0.5 * (1.0 - sg)
+        rs = hp * rsL + hm * rsR
+        F = [rs * us, rs * us * us + pst, rs * us * (hp * v2L + hm * v2R), rs * us * (hp * v3L + hm * v3R),
+             (hp * resL + hm * resR + pst) * us] + [rs * us * (hp * a + hm * b) for a, b in zip(xL, xR)]
+        if all_mach:
+            fL = [rhoL * v1L, rhoL * v1L * v1L + pL, rhoL * v1L * v2L, rhoL * v1L * v3L, (reL + pL) * v1L]
+            fL += [rhoL * a * v1L for a in xL]
+            fR = [rhoR * v1R, rhoR * v1R * v1R + pR, rhoR * v1R * v2R, rhoR * v1R * v3R, (reR + pR) * v1R]
+            fR += [rhoR * a * v1R for a in xR]
+            F = [np.where(sL > 0.0, a, np.where(sR < 0.0, b, c)) for a, b, c in zip(fL, fR, F)]
+        return F
+    out = []
+    for side in ("L", "R"):
+        rho_, v1_, v2_, v3_, re_, p_, x_, s, rs, res_ = (
+            (rhoL, v1L, v2L, v3L, reL, pL, xL, sL, rsL, resL) if side == "L" else
+            (rhoR, v1R, v2R, v3R, reR, pR, xR, sR, rsR, resR))
+        U = [rho_, rho_ * v1_, rho_ * v2_, rho_ * v3_, re_] + [rho_ * a for a in x_]
+        f = [rho_ * v1_, rho_ * v1_ * v1_ + p_, rho_ * v1_ * v2_, rho_ * v1_ * v3_, (re_ + p_) * v1_]
+        f += [rho_ * v1_ * a for a in x_]
+        Us = [rs, rs * us, rs * v2_, rs * v3_, res_] + [rs * a for a in x_]
+        outer = (s >= 0.0) if side == "L" else (s < 0.0)
+        out.append([np.where(outer, fi, fi + s * (a - u0)) for fi, u0, a in zip(f, U, Us)])
+    return [np.where(us > 0.0, a, b) for a, b in zip(out[0], out[1])]
+
+
 def _wrap(a, axis):
     """One periodic layer on either side of `a` along `axis` (the self-copy of a face array's
     ghost layer, S:2293-2306)."""
@@ -871,9 +939,10 @@ def _fill_strat(a, G, flip):
         a[:, ny + G - 1 + g] = f * a[:, ny + G - g]
 
 
-def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
-    """The magnetised stratified Helmholtz box (3D, x2 vertical between reflective walls, x1 /
-    x3 periodic): USE_WB on rho, p and gamma_e (S:7151-7168, the equilibria added back at the
+def stratified_steps(h, tab, dpdr, nd, nsteps):
+    """The stratified Helmholtz box (3D, x2 vertical between reflective walls, x1 / x3
+    periodic), magnetised (HLLD / LHLLD with constrained transport) or not (HLLC / LHLLC, with
+    FLUX_IS_ALL_MACH when the configuration sets it): USE_WB on rho, p and gamma_e (S:7151-7168, the equilibria added back at the
     faces, S:8473-8486, S:8714-8727), USE_FASTEOS face gammas in the Riemann solver
     (S:14223-14226), EVOLVE_ETOT, gravity on rho' (S:12606-12644), ADVECT_YE_IABAR scalars,
     LHLLD (or HLLD) with constrained transport and the reflective EMF ghosts of the x1 and x3
@@ -892,9 +961,11 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
     n = [c.nx1, c.nx2, c.nx3]
     I = tuple(slice(G, G + m) for m in n)
     nv = c.nvars
+    mhd = c.mhd
+    low_mach = c.riemann in ("lhlld", "lhllc")
     W = [h.prim[v].copy() for v in range(nv)]
     temp = h.temp[I].copy()
-    b = [h.b_x[d][tuple(slice(1, 1 + n[a] + (a == d)) for a in range(3))].copy() for d in range(3)]
+    b = [h.b_x[d][tuple(slice(1, 1 + n[a] + (a == d)) for a in range(3))].copy() for d in range(3)] if mhd else None
     B = [np.zeros_like(W[0]) for _ in range(3)]
     ge, gc = np.zeros_like(W[0]), np.zeros_like(W[0])
     eq_r, eq_p, eq_ge = h.eq_prim_cc[0][I], h.eq_prim_cc[1][I], h.eq_gammae_cc[I]
@@ -909,7 +980,8 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
         for d, a in enumerate(B):
             _fill_strat(a, G, d == 1)
 
-    cell_b()
+    if mhd:
+        cell_b()
     # step-0 thermodynamics
     rho, p = W[0][I], W[4][I]
     abar = 1.0 / W[6][I]
@@ -925,8 +997,9 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
         r, v1, v2, v3 = (W[v][I] for v in range(4))
         ab = 1.0 / W[6][I]
         _, _, cs, _ = given_full(tab, dpdr, nd, r, temp, ab, W[5][I] * ab)
-        ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]
-        cs = np.sqrt(cs * cs + ca2 / r)
+        if mhd:
+            ca2 = B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]
+            cs = np.sqrt(cs * cs + ca2 / r)
         sx1 = (np.abs(v1) + cs) * idx[0]
         sx2 = (np.abs(v2) + cs) * idx[1]
         sx3 = (np.abs(v3) + cs) * idx[2]
@@ -950,12 +1023,12 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
           3: [(1.0, 0.0, -1.0), (0.75, 0.25, -0.25), (1.0 / 3.0, 2.0 / 3.0, -(2.0 / 3.0))]}[c.rk_stages]
     for _ in range(nsteps):
         r, v1, v2, v3 = (W[v][I].copy() for v in range(4))
-        U0 = [r, r * v1, r * v2, r * v3,
-              eint + 0.5 * r * (v1 * v1 + v2 * v2 + v3 * v3)
-              + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I]) + r * phi]
-        U0 += [r * W[v][I] for v in range(5, nv)]
+        e0 = eint + 0.5 * r * (v1 * v1 + v2 * v2 + v3 * v3)
+        if mhd:
+            e0 = e0 + 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])
+        U0 = [r, r * v1, r * v2, r * v3, e0 + r * phi] + [r * W[v][I] for v in range(5, nv)]
         U = [u.copy() for u in U0]
-        b0 = [x.copy() for x in b]
+        b0 = [x.copy() for x in b] if mhd else None
         for a1, a2, c3 in rk:
             Wd = [w.copy() for w in W]
             Wd[0][I] = W[0][I] - eq_r
@@ -976,7 +1049,8 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
             for a in range(3):
                 m = n[a]
                 trans = [t for t in range(3) if t != a]
-                arrs = Wd + [B[t] for t in trans] + [ged, gcd]
+                nb = 2 if mhd else 0
+                arrs = Wd + ([B[t] for t in trans] if mhd else []) + [ged, gcd]
                 lo, hi = zip(*[_plm(w[along(a, G - 2, G + m)], w[along(a, G - 1, G + m + 1)],
                                     w[along(a, G, G + m + 2)]) for w in arrs])
                 L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
@@ -985,39 +1059,41 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
                 for side in (L, R):
                     side[0] = side[0] + er
                     side[4] = side[4] + ep
-                    side[nv + 2] = side[nv + 2] + eg
-                bt = (L[nv], L[nv + 1]), (R[nv], R[nv + 1])
+                    side[nv + nb] = side[nv + nb] + eg
                 if a == 0:
                     qL, qR = L[:5], R[:5]
-                    bL, bR = [b[0], bt[0][0], bt[0][1]], [b[0], bt[1][0], bt[1][1]]
                 elif a == 1:
                     qL = [L[0], L[2], -L[1], L[3], L[4]]
                     qR = [R[0], R[2], -R[1], R[3], R[4]]
-                    bL, bR = [b[1], -bt[0][0], bt[0][1]], [b[1], -bt[1][0], bt[1][1]]
                 else:
                     qL = [L[0], L[3], L[1], L[2], L[4]]
                     qR = [R[0], R[3], R[1], R[2], R[4]]
-                    bL, bR = [b[2], bt[0][0], bt[0][1]], [b[2], bt[1][0], bt[1][1]]
+                if mhd:
+                    bt = (L[nv], L[nv + 1]), (R[nv], R[nv + 1])
+                    sg = -1.0 if a == 1 else 1.0
+                    bL = [b[a], sg * bt[0][0], bt[0][1]]
+                    bR = [b[a], sg * bt[1][0], bt[1][1]]
                 if fast:
-                    eos = dict(fasteos=(L[nv + 2], L[nv + 3], R[nv + 2], R[nv + 3]))
+                    eos = dict(fasteos=(L[nv + nb], L[nv + nb + 1], R[nv + nb], R[nv + nb + 1]))
                 else:
                     tg = 0.5 * (tpad[along(a, G - 1, G + m)] + tpad[along(a, G, G + m + 1)])
                     sides = []
                     for q in (L, R):
                         ab = 1.0 / q[6]
                         _, e1, s1, _ = rhoP_given(tab, dpdr, nd, q[0], q[4], ab, q[5] * ab, tg, tl, th)
-                        sides += [e1 * q[0], s1 * s1]
+                        sides += [e1 * q[0], s1 * s1 if mhd else s1]
                     eos = dict(side_eos=tuple(sides))
-                F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], **eos)
-                if a == 0:
-                    emf[0] = (None, fb[1], -fb[0])
-                elif a == 1:
-                    F = [F[0], -F[2], F[1]] + F[3:]
-                    emf[1] = (-fb[1], None, -fb[0])
+                if mhd:
+                    F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], **eos)
+                    emf[a] = [(None, fb[1], -fb[0]), (-fb[1], None, -fb[0]), (fb[1], -fb[0], None)][a]
                 else:
+                    F = _hllc3(qL, qR, c.gamma_ad, c.mach_cutoff, low_mach, c.all_mach, L[5:nv], R[5:nv], **eos)
+                if a == 1:
+                    F = [F[0], -F[2], F[1]] + F[3:]
+                elif a == 2:
                     F = [F[0], F[2], F[3], F[1]] + F[4:]
-                    emf[2] = (fb[1], -fb[0], None)
-                sgn[a] = mass_sign(F[0], qL[0], qR[0], smax)
+                if mhd:
+                    sgn[a] = mass_sign(F[0], qL[0], qR[0], smax)
                 F[1 + a] = F[1 + a] - ep
                 F[4] = F[4] + F[0] * ph
                 div = [np.diff(f, axis=a) * idx[a] for f in F]
@@ -1025,40 +1101,15 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
             rdev = Wd[0][I]
             for d in range(3):
                 res[1 + d] = res[1 + d] - rdev * grav[d]
-            ec3 = -Wd[1] * B[1] + Wd[2] * B[0]
-            ec1 = Wd[3] * B[1] - Wd[2] * B[2]
-            ec2 = Wd[1] * B[2] - Wd[3] * B[0]
-            nx, ny, nz = n
-            Ix, Iy, Iz = I
-            e, s_ = wall_wrap(emf[0][2], True), wall_wrap(sgn[0], False)
-            f, t = _wrap(emf[1][2], 0), _wrap(sgn[1], 0)
-            cor3 = _corner((e[:, :-1], e[:, 1:]), (f[:-1], f[1:]),
-                           (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
-                            ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
-                           (s_[:, :-1], s_[:, 1:]), (t[:-1], t[1:]))
-            e, s_ = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
-            f, t = wall_wrap(emf[2][0], True), wall_wrap(sgn[2], False)
-            cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
-                           (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
-                            ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
-                           (s_[:, :, :-1], s_[:, :, 1:]), (t[:, :-1], t[:, 1:]))
-            e, s_ = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
-            f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
-            cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
-                           (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
-                            ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),
-                           (s_[:-1], s_[1:]), (t[:, :, :-1], t[:, :, 1:]))
-            a3 = c3 * dt
-            t1 = -(cor2[:, :, 1:] - cor2[:, :, :-1]) * idx[2] + (cor3[:, 1:] - cor3[:, :-1]) * idx[1]
-            t2 = (cor1[:, :, 1:] - cor1[:, :, :-1]) * idx[2] + (cor3[:-1] - cor3[1:]) * idx[0]
-            t3 = (cor2[1:] - cor2[:-1]) * idx[0] - (cor1[:, 1:] - cor1[:, :-1]) * idx[1]
-            b = [a1 * x0 + a2 * x + a3 * tt for x0, x, tt in zip(b0, b, (t1, t2, t3))]
-            cell_b()
-            U = [a1 * u0 + a2 * u + a3 * rr for u0, u, rr in zip(U0, U, res)]
+            if mhd:
+                b = _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, c3 * dt, wall_wrap)
+                cell_b()
+            U = [a1 * u0 + a2 * u + c3 * dt * rr for u0, u, rr in zip(U0, U, res)]
             rho = U[0]
             inv_rho = 1.0 / rho
             e_ = U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) * inv_rho
-            e_ = e_ - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])
+            if mhd:
+                e_ = e_ - 0.5 * (B[0][I] * B[0][I] + B[1][I] * B[1][I] + B[2][I] * B[2][I])
             e_ = e_ - rho * phi
             ye = U[5] * inv_rho
             ab = rho / U[6]
@@ -1076,3 +1127,37 @@ def stratified_mhd_steps(h, tab, dpdr, nd, nsteps, low_mach=True):
             eint = e_
         smax, dt = cfl()
     return W, eint, temp, (ge, gc), b, dt
+
+
+def _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, a3, wall_wrap):
+    """Corner EMFs of the stratified box (reflective x2 walls, x1 / x3 periodic) and the RK
+    update of the three face-B arrays."""
+    I = tuple(slice(G, G + m) for m in n)
+    ec3 = -Wd[1] * B[1] + Wd[2] * B[0]
+    ec1 = Wd[3] * B[1] - Wd[2] * B[2]
+    ec2 = Wd[1] * B[2] - Wd[3] * B[0]
+    nx, ny, nz = n
+    Ix, Iy, Iz = I
+    e, s_ = wall_wrap(emf[0][2], True), wall_wrap(sgn[0], False)
+    f, t = _wrap(emf[1][2], 0), _wrap(sgn[1], 0)
+    cor3 = _corner((e[:, :-1], e[:, 1:]), (f[:-1], f[1:]),
+                   (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
+                    ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
+                   (s_[:, :-1], s_[:, 1:]), (t[:-1], t[1:]))
+    e, s_ = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
+    f, t = wall_wrap(emf[2][0], True), wall_wrap(sgn[2], False)
+    cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
+                   (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
+                    ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
+                   (s_[:, :, :-1], s_[:, :, 1:]), (t[:, :-1], t[:, 1:]))
+    e, s_ = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
+    f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
+    cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
+                   (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
+                    ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),
+                   (s_[:-1], s_[1:]), (t[:, :, :-1], t[:, :, 1:]))
+    t1 = -(cor2[:, :, 1:] - cor2[:, :, :-1]) * idx[2] + (cor3[:, 1:] - cor3[:, :-1]) * idx[1]
+    t2 = (cor1[:, :, 1:] - cor1[:, :, :-1]) * idx[2] + (cor3[:-1] - cor3[1:]) * idx[0]
+    t3 = (cor2[1:] - cor2[:-1]) * idx[0] - (cor1[:, 1:] - cor1[:, :-1]) * idx[1]
+    b = [a1 * x0 + a2 * x + a3 * tt for x0, x, tt in zip(b0, b, (t1, t2, t3))]
+    return b

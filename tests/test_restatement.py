@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from phlegethon_b200 import problems
-from numpy_restatement import hot_bubble_steps, mhd_2d_steps, mhd_3d_steps, stratified_mhd_steps, wb_mhd_2d_steps
+from numpy_restatement import hot_bubble_steps, mhd_2d_steps, mhd_3d_steps, stratified_steps, wb_mhd_2d_steps
 from util import smooth_box
 
 
@@ -216,32 +216,35 @@ def test_oracle_newton_inversions_match_numpy_restatement(eos_case):
 
 
 @pytest.mark.parametrize("fasteos", [True, False])
-@pytest.mark.parametrize("riemann", ["lhlld", "hlld"])
-def test_oracle_stratified_helmholtz_mhd_matches_numpy_restatement(oracle, riemann, fasteos):
-    """The benchmark's workload in small: the magnetised stratified Helmholtz box (WB on rho, p
-    and gamma_e, FASTEOS face gammas, EVOLVE_ETOT, gravity, Ye and 1/Abar, reflective x2 walls,
-    constrained transport), with a divergence-free perturbation of B_2 and B_3 added to the
-    uniform B_1 so that every EMF component and wall ghost matters.  The step-0 thermodynamics,
-    three steps of LHLLD / HLLD with the in-step Newton, the gammas, temperatures, face fields
-    and dt equal the numpy restatement bit for bit; without USE_FASTEOS every Riemann side's
-    helm_rhoP_given from the face temperature guess is part of it."""
+@pytest.mark.parametrize("riemann", ["lhlld", "hlld", "lhllc", "hllc"])
+def test_oracle_stratified_helmholtz_matches_numpy_restatement(oracle, riemann, fasteos):
+    """The benchmark's workloads in small: the stratified Helmholtz box (WB on rho, p and
+    gamma_e, FASTEOS face gammas, EVOLVE_ETOT, gravity, Ye and 1/Abar, reflective x2 walls),
+    magnetised (LHLLD / HLLD with constrained transport, a divergence-free perturbation of B_2
+    and B_3 added to the uniform B_1 so that every EMF component and wall ghost matters) or not
+    (LHLLC / HLLC).  The step-0 thermodynamics, three steps with the in-step Newton, the gammas,
+    temperatures, face fields and dt equal the numpy restatement bit for bit; without
+    USE_FASTEOS every Riemann side's helm_rhoP_given from the face temperature guess is part of
+    it."""
     from phlegethon_b200 import helm_table
     import numpy_restatement_eos as RE
     from util import smooth_periodic
     tab, dpdr = helm_table.generate(nrho=271, nT=101)
-    cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=True, mach=0.05, table=helm_table.X1_TABLE,
+    mhd = riemann in ("lhlld", "hlld")
+    cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=mhd, mach=0.05, table=helm_table.X1_TABLE,
                                     riemann=riemann, fasteos=fasteos)
-    rng = np.random.default_rng(7)
-    b0 = float(h.b_x[0][1, 1, 1])
-    h.b_x[1][...] += 0.3 * b0 * smooth_periodic(h.b_x[1].shape, (8, None, 6), rng, stagger=1)
-    h.b_x[2][...] += 0.3 * b0 * smooth_periodic(h.b_x[2].shape, (8, 12, None), rng, stagger=2)
+    if mhd:
+        rng = np.random.default_rng(7)
+        b0 = float(h.b_x[0][1, 1, 1])
+        h.b_x[1][...] += 0.3 * b0 * smooth_periodic(h.b_x[1].shape, (8, None, 6), rng, stagger=1)
+        h.b_x[2][...] += 0.3 * b0 * smooth_periodic(h.b_x[2].shape, (8, 12, None), rng, stagger=2)
     nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
     hn = h.copy()
     o = oracle.OracleGrid(h, oracle.Helm.for_config(cfg, tab, dpdr), nthreads=2)
     o.init_thermo()
     o.compute_hyperbolic_dt()
     o.time_loop(3)
-    W, eint, temp, (ge, gc), b, dt = stratified_mhd_steps(hn, tab, dpdr, nd, 3, low_mach=riemann == "lhlld")
+    W, eint, temp, (ge, gc), b, dt = stratified_steps(hn, tab, dpdr, nd, 3)
     for v in range(cfg.nvars):
         np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
     np.testing.assert_array_equal(h.interior(h.eint), eint)
@@ -249,6 +252,34 @@ def test_oracle_stratified_helmholtz_mhd_matches_numpy_restatement(oracle, riema
     if fasteos:
         np.testing.assert_array_equal(h.interior(h.gammaf[0]), hn.interior(ge))
         np.testing.assert_array_equal(h.interior(h.gammaf[1]), hn.interior(gc))
-    for d in range(3):
+    for d in range(3 if mhd else 0):
         np.testing.assert_array_equal(h.bface_interior(d), b[d])
     assert o.g.dt == dt
+
+
+def test_oracle_supersonic_all_mach_matches_numpy_restatement(oracle):
+    """The stratified hydro box streaming along x1 at twice its sound speed with
+    FLUX_IS_ALL_MACH (LHLLC takes the upwind state's flux where the whole fan moves one way):
+    bit for bit with the restatement, and different from the run without the switch."""
+    from phlegethon_b200 import helm_table
+    import numpy_restatement_eos as RE
+    tab, dpdr = helm_table.generate(nrho=271, nT=101)
+    out = []
+    for all_mach in (True, False):
+        cfg, h = problems.stratified_3d(8, ny=12, nz=6, mach=0.05, table=helm_table.X1_TABLE, riemann="lhllc")
+        h.cfg = cfg = cfg.replace(all_mach=all_mach)
+        v1 = h.interior(h.prim[1])
+        v1 += 2.0 * np.sqrt(5.0 / 3.0 * h.interior(h.prim[4]) / h.interior(h.prim[0]))
+        nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
+        hn = h.copy()
+        o = oracle.OracleGrid(h, oracle.Helm.for_config(cfg, tab, dpdr), nthreads=2)
+        o.init_thermo()
+        o.compute_hyperbolic_dt()
+        o.time_loop(3)
+        W, eint, temp, _, _, dt = stratified_steps(hn, tab, dpdr, nd, 3)
+        for v in range(cfg.nvars):
+            np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
+        np.testing.assert_array_equal(h.interior(h.temp), temp)
+        assert o.g.dt == dt
+        out.append(h.interior(h.prim).copy())
+    assert not np.array_equal(out[0], out[1])
