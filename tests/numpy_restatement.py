@@ -245,15 +245,25 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None, rec="lim2nd"):
 
 
 # ------------------------------------------------------------------------------ ideal MHD
-def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None, side_eos=None):
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None, side_eos=None, flat=None):
     """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
     array in the face frame, ideal gas (S:13969-15024).  q = (rho, v1, v2, v3, p), b = (B
     normal, B transverse 2, B transverse 3); in 2D v3 and B3 are zero arrays, as the reference
     sets them; x the passive scalars' edge values; fasteos = (gamma_e L, gamma_c L, gamma_e R,
     gamma_c R) replaces the ideal gas by USE_FASTEOS's face gammas (e = p / (gamma_e - 1),
     c^2 = gamma_c p / rho); side_eos = (e L, c^2 L, e R, c^2 R) takes each side's internal
-    energy and sound speed squared as given (the Helmholtz solves without USE_FASTEOS).
-    Returns the fluxes (rho, m1, m2, m3, E, then one per scalar) and fluxb(2), fluxb(3)."""
+    energy and sound speed squared as given (the Helmholtz solves without USE_FASTEOS); flat
+    marks the faces of USE_SHOCK_FLATTENING, which take the two-wave HLL flux with
+    sL = min(0, sL), sR = max(0, sR) (S:14386-14493).  Returns the fluxes (rho, m1, m2, m3, E,
+    then one per scalar) and fluxb(2), fluxb(3)."""
+    (F, hF), (fb, hfb) = _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos)
+    if flat is None:
+        return F, fb
+    return [np.where(flat, a, b) for a, b in zip(hF, F)], [np.where(flat, a, b) for a, b in zip(hfb, fb)]
+
+
+def _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos):
+    """`_hlld`'s arithmetic; returns ((F, HLL F), (fb, HLL fb))."""
     igmm1 = 1.0 / (gm - 1.0)
     rhoL, v1L, v2L, v3L, pL = qL
     rhoR, v1R, v2R, v3R, pR = qR
@@ -296,6 +306,20 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None,
     mc = np.maximum(cL, cR)
     sL = np.minimum(v1L, v1R) - mc
     sR = np.maximum(v1L, v1R) + mc
+    # the flattened faces' HLL flux
+    hsL = np.minimum(0.0, sL)
+    hsR = np.maximum(0.0, sR)
+    hUL = [rhoL, rhoL * v1L, rhoL * v2L, rhoL * v3L, reL] + [rhoL * a for a in xL]
+    hUR = [rhoR, rhoR * v1R, rhoR * v2R, rhoR * v3R, reR] + [rhoR * a for a in xR]
+    hfL = [rhoL * v1L, rhoL * v1L * v1L + ptL - bx1_2, rhoL * v1L * v2L - bx1 * b2L, rhoL * v1L * v3L - bx1 * b3L,
+           (reL + ptL) * v1L - bx1 * (bx1 * v1L + b2L * v2L + b3L * v3L)] + [u * v1L for u in hUL[5:]]
+    hfR = [rhoR * v1R, rhoR * v1R * v1R + ptR - bx1_2, rhoR * v1R * v2R - bx1 * b2R, rhoR * v1R * v3R - bx1 * b3R,
+           (reR + ptR) * v1R - bx1 * (bx1 * v1R + b2R * v2R + b3R * v3R)] + [u * v1R for u in hUR[5:]]
+    hd = 1.0 / (hsR - hsL)
+    hph = hsL * hsR
+    hF = [hd * (hsR * a - hsL * b + hph * (ur - ul)) for a, b, ul, ur in zip(hfL, hfR, hUL, hUR)]
+    hfb = [hd * (hsR * (v1L * b2L - v2L * bx1) - hsL * (v1R * b2R - v2R * bx1) + hph * (b2R - b2L)),
+           hd * (hsR * (v1L * b3L - v3L * bx1) - hsL * (v1R * b3R - v3R * bx1) + hph * (b3R - b3L))]
     dsuL = sL - v1L
     dsuR = sR - v1R
     it1 = 1.0 / (dsuR * rhoR - dsuL * rhoL)
@@ -366,7 +390,7 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None,
         hp = 0.5 * (1.0 + up)
         hm = 0.5 * (1.0 - up)
         F += [rho * u * (hp * a + hm * b) for a, b in zip(xL, xR)]
-        return F, [u * b2 - bx1 * v2, u * b3 - bx1 * v3]
+        return (F, hF), ([u * b2 - bx1 * v2, u * b3 - bx1 * v3], hfb)
     # HLLD: f + s (U* - U) + s* (U** - U*) on the side of u*
     out = []
     for side in ("L", "R"):
@@ -390,7 +414,7 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None,
                     for fi, u0, a, b in zip(f, U, Us, Uss)])
     left = us > 0.0
     F = [np.where(left, a, b) for a, b in zip(out[0], out[1])]
-    return F[:5] + F[7:], F[5:7]
+    return (F[:5] + F[7:], hF), (F[5:7], hfb)
 
 
 def _fill_periodic(a, G):
@@ -527,11 +551,19 @@ def mhd_2d_steps(h, nsteps, low_mach):
     return W, eint, temp, b1, b2, dt
 
 
-def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fasteos=None, side_eos=None):
+def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fasteos=None, side_eos=None,
+           flat=None):
     """LHLLC (low_mach True) or HLLC flux of one face array in the face frame, 3D with
     scalars (S:15611-16260): q = (rho, v1, v2, v3, p); the side EoS as in `_hlld` (here
     side_eos carries the sound speed itself, as helm_rhoP_given returns it); all_mach:
-    FLUX_IS_ALL_MACH, the upwind state's flux outside the fan (LHLLC only)."""
+    FLUX_IS_ALL_MACH, the upwind state's flux outside the fan (LHLLC only); flat: the faces of
+    USE_SHOCK_FLATTENING, with the HLL flux (S:15929-16008)."""
+    F, hF = _hllc3_fan(qL, qR, gm, mach_cutoff, low_mach, all_mach, xL, xR, fasteos, side_eos)
+    return F if flat is None else [np.where(flat, a, b) for a, b in zip(hF, F)]
+
+
+def _hllc3_fan(qL, qR, gm, mach_cutoff, low_mach, all_mach, xL, xR, fasteos, side_eos):
+    """`_hllc3`'s arithmetic; returns (F, HLL F)."""
     rhoL, v1L, v2L, v3L, pL = qL
     rhoR, v1R, v2R, v3R, pR = qR
     iL = 1.0 / rhoL
@@ -564,6 +596,17 @@ def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fast
     resL = rsL * (reL * iL + (us - v1L) * (us + pL * iL / dL))
     rsR = rhoR * (dR / (sR - us))
     resR = rsR * (reR * iR + (us - v1R) * (us + pR * iR / dR))
+    hsL = np.minimum(0.0, sL)
+    hsR = np.maximum(0.0, sR)
+    hUL = [rhoL, rhoL * v1L, rhoL * v2L, rhoL * v3L, reL] + [rhoL * a for a in xL]
+    hUR = [rhoR, rhoR * v1R, rhoR * v2R, rhoR * v3R, reR] + [rhoR * a for a in xR]
+    hfL = [rhoL * v1L, rhoL * v1L * v1L + pL, rhoL * v1L * v2L, rhoL * v1L * v3L, (reL + pL) * v1L]
+    hfL += [u * v1L for u in hUL[5:]]
+    hfR = [rhoR * v1R, rhoR * v1R * v1R + pR, rhoR * v1R * v2R, rhoR * v1R * v3R, (reR + pR) * v1R]
+    hfR += [u * v1R for u in hUR[5:]]
+    hd = 1.0 / (hsR - hsL)
+    hph = hsL * hsR
+    hF = [hd * (hsR * a - hsL * b + hph * (ur - ul)) for a, b, ul, ur in zip(hfL, hfR, hUL, hUR)]
     if low_mach:
         chi = np.maximum(mach_cutoff, np.minimum(1.0, np.maximum(np.sqrt(w2L) / cL, np.sqrt(w2R) / cR)))
         phi = chi * (2.0 - chi)
@@ -580,7 +623,7 @@ def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fast
             fR = [rhoR * v1R, rhoR * v1R * v1R + pR, rhoR * v1R * v2R, rhoR * v1R * v3R, (reR + pR) * v1R]
             fR += [rhoR * a * v1R for a in xR]
             F = [np.where(sL > 0.0, a, np.where(sR < 0.0, b, c)) for a, b, c in zip(fL, fR, F)]
-        return F
+        return F, hF
     out = []
     for side in ("L", "R"):
         rho_, v1_, v2_, v3_, re_, p_, x_, s, rs, res_ = (
@@ -592,7 +635,7 @@ def _hllc3(qL, qR, gm, mach_cutoff, low_mach, all_mach=False, xL=(), xR=(), fast
         Us = [rs, rs * us, rs * v2_, rs * v3_, res_] + [rs * a for a in x_]
         outer = (s >= 0.0) if side == "L" else (s < 0.0)
         out.append([np.where(outer, fi, fi + s * (a - u0)) for fi, u0, a in zip(f, U, Us)])
-    return [np.where(us > 0.0, a, b) for a, b in zip(out[0], out[1])]
+    return [np.where(us > 0.0, a, b) for a, b in zip(out[0], out[1])], hF
 
 
 def _wrap(a, axis):
@@ -952,7 +995,8 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
     side solves helm_rhoP_given from the face guess (T(i-1) + T(i)) / 2 of the stage input's
     temperatures (S:8488-8495, S:14250-14256) with its own reconstructed Ye and 1/Abar, and the
     gammas are neither reconstructed nor kept.  LIM2ND.  Returns (W, eint, temp, gammaf,
-    [b1, b2, b3], dt)."""
+    [b1, b2, b3], dt).  With USE_SHOCK_FLATTENING (3 ghost layers) the flagged faces take the
+    HLL flux and the x1 sweep's gamma_e follows the reference's flattened branch."""
     from numpy_restatement_eos import given_full, rhoe_given, rhoP_given
     c = h.cfg
     G = c.ngc
@@ -1043,6 +1087,7 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
             tpad = np.zeros_like(W[0])
             tpad[I] = temp
             _fill_strat(tpad, G, False)
+            fl = _flatten_flags(Wd[4] + h.eq_prim_cc[1], G, n, c.eps_sf) if c.shock_flattening else None
             emf = [None, None, None]
             sgn = [None, None, None]
             res = None
@@ -1056,10 +1101,24 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
                 L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
                 R = [np.take(x, range(1, m + 2), axis=a) for x in lo]
                 er, ep, eg, ph = eqf[a]
+                devL, devR = L[nv + nb], R[nv + nb]
                 for side in (L, R):
                     side[0] = side[0] + er
                     side[4] = side[4] + ep
                     side[nv + nb] = side[nv + nb] + eg
+                flat = None
+                if fl is not None:
+                    ins = [slice(1, 1 + n[x]) for x in range(3)]
+                    fleft = fl[tuple(slice(0, m + 1) if x == a else ins[x] for x in range(3))]
+                    fright = fl[tuple(slice(1, m + 2) if x == a else ins[x] for x in range(3))]
+                    flat = fleft | fright
+                    if a == 0 and fast:
+                        # the x1 sweep's flattened gamma_e (S:8834-8869): a flagged cell's PLM edge
+                        # replaces the face value without the equilibrium, which is added to the
+                        # other side of that face instead; LIM2ND edges are the PLM edges
+                        gl = np.where(fleft, devL, devL + eg)
+                        L[nv + nb] = np.where(fright, gl + eg, gl)
+                        R[nv + nb] = np.where(fright, devR, np.where(fleft, (devR + eg) + eg, devR + eg))
                 if a == 0:
                     qL, qR = L[:5], R[:5]
                 elif a == 1:
@@ -1084,10 +1143,12 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
                         sides += [e1 * q[0], s1 * s1 if mhd else s1]
                     eos = dict(side_eos=tuple(sides))
                 if mhd:
-                    F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], **eos)
+                    F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], flat=flat,
+                                  **eos)
                     emf[a] = [(None, fb[1], -fb[0]), (-fb[1], None, -fb[0]), (fb[1], -fb[0], None)][a]
                 else:
-                    F = _hllc3(qL, qR, c.gamma_ad, c.mach_cutoff, low_mach, c.all_mach, L[5:nv], R[5:nv], **eos)
+                    F = _hllc3(qL, qR, c.gamma_ad, c.mach_cutoff, low_mach, c.all_mach, L[5:nv], R[5:nv],
+                               flat=flat, **eos)
                 if a == 1:
                     F = [F[0], -F[2], F[1]] + F[3:]
                 elif a == 2:
@@ -1127,6 +1188,24 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
             eint = e_
         smax, dt = cfl()
     return W, eint, temp, (ge, gc), b, dt
+
+
+def _flatten_flags(pf, G, n, eps_sf):
+    """is_flattened of the padded cells G-1 .. G+n along every axis (S:8073-8136): a cell
+    G-2 .. G+n+1 whose summed central jumps of the full pressure pf (deviation plus the stored
+    equilibrium, ghosts included), x3 + x2 + x1, exceed eps_sf times its pressure marks its
+    3 x 3 x 3 neighbourhood.  fl[i, j, k] is padded cell (G-1+i, G-1+j, G-1+k)."""
+    def win(a, o):
+        return tuple(slice(G - 2 + (o if x == a else 0), G + n[x] + 2 + (o if x == a else 0)) for x in range(3))
+    d = [np.abs(pf[win(a, 1)] - pf[win(a, -1)]) for a in range(3)]
+    tmp = (d[2] + d[1] + d[0]) / pf[win(0, 0)]
+    mark = tmp > eps_sf
+    fl = np.zeros(tuple(m + 2 for m in n), dtype=bool)
+    for o0 in range(3):
+        for o1 in range(3):
+            for o2 in range(3):
+                fl |= mark[o0:o0 + n[0] + 2, o1:o1 + n[1] + 2, o2:o2 + n[2] + 2]
+    return fl
 
 
 def _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, a3, wall_wrap):

@@ -283,3 +283,37 @@ def test_oracle_supersonic_all_mach_matches_numpy_restatement(oracle):
         assert o.g.dt == dt
         out.append(h.interior(h.prim).copy())
     assert not np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("riemann", ["lhlld", "hlld", "lhllc", "hllc"])
+def test_oracle_shock_flattening_in_the_stratified_box_matches_numpy_restatement(oracle, riemann):
+    """USE_SHOCK_FLATTENING in the stratified Helmholtz box at eps_sf 0.6, where the
+    background's vertical pressure jumps (0.42 ... 1.28 of p) flag part of the box: the
+    detector on the full pressure with the ghosts' equilibria, the HLL flux of the flagged
+    faces (hydro and MHD) and the x1 sweep's gamma_e branch, which leaves the equilibrium off
+    a flagged cell's side of the face and adds it to the other, agree with the restatement bit
+    for bit; the flattening changes the result."""
+    from phlegethon_b200 import helm_table
+    import numpy_restatement_eos as RE
+    tab, dpdr = helm_table.generate(nrho=271, nT=101)
+    cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=riemann.endswith("d"), mach=0.05,
+                                    table=helm_table.X1_TABLE, riemann=riemann, shock_flattening=True, eps_sf=0.6)
+    nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
+    helm = oracle.Helm.for_config(cfg, tab, dpdr)
+    hn, h0 = h.copy(), h.copy()
+    h0.cfg = cfg.replace(shock_flattening=False)
+    for g in (h, h0):
+        o = oracle.OracleGrid(g, helm, nthreads=2)
+        o.init_thermo()
+        o.compute_hyperbolic_dt()
+        o.time_loop(3)
+        if g is h:
+            dt_oracle = o.g.dt
+    W, eint, temp, _, b, dt = stratified_steps(hn, tab, dpdr, nd, 3)
+    for v in range(cfg.nvars):
+        np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
+    np.testing.assert_array_equal(h.interior(h.temp), temp)
+    for d in range(3 if cfg.mhd else 0):
+        np.testing.assert_array_equal(h.bface_interior(d), b[d])
+    assert dt_oracle == dt
+    assert not np.array_equal(h.interior(h.prim), h0.interior(h0.prim))
