@@ -666,7 +666,9 @@ def mhd_3d_steps(h, nsteps, low_mach):
     corner EMFs (S:11970-12200), the three face-B updates (S:12258-12432) and the 3D dt sum
     sx3 + sx1 + sx2, with the passive scalars the configuration carries (upwinded by the sign
     of the contact speed) and its reconstruction (LIM2ND, PPH or LIM5TH; the cell B edges by
-    the same formulas, S:8327-8469).  Returns (W, eint, temp, [b1, b2, b3], dt)."""
+    the same formulas, S:8327-8469), and USE_CONSTANT_ACCELERATION when the configuration sets
+    it (rho acc on the momenta and its work from the stage's input state, S:12806-12834).
+    Returns (W, eint, temp, [b1, b2, b3], dt)."""
     c = h.cfg
     G = c.ngc
     gm = c.gamma_ad
@@ -767,6 +769,11 @@ def mhd_3d_steps(h, nsteps, low_mach):
                 sgn[a] = mass_sign(F[0], qL[0], qR[0], smax)
                 div = [np.diff(f, axis=a) * idx[a] for f in F]
                 res = div if res is None else [rr + d for rr, d in zip(res, div)]
+            if c.constant_acceleration:
+                acc = c.acc
+                for d in range(3):
+                    res[1 + d] = res[1 + d] - U[0] * acc[d]
+                res[4] = res[4] - U[3] * acc[2] - U[1] * acc[0] - U[2] * acc[1]
             # cell EMFs at the padded cells, then the corners of each axis
             ec3 = -W[1] * B[1] + W[2] * B[0]
             ec1 = W[3] * B[1] - W[2] * B[2]

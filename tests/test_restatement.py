@@ -317,3 +317,23 @@ def test_oracle_shock_flattening_in_the_stratified_box_matches_numpy_restatement
         np.testing.assert_array_equal(h.bface_interior(d), b[d])
     assert dt_oracle == dt
     assert not np.array_equal(h.interior(h.prim), h0.interior(h0.prim))
+
+
+@pytest.mark.parametrize("riemann", ["hlld", "lhlld"])
+def test_oracle_constant_acceleration_matches_numpy_restatement(oracle, riemann):
+    """USE_CONSTANT_ACCELERATION (acc = (0.3, -0.2, 0.15)) on the smooth 3D MHD box: the
+    momentum source rho acc and its work, both from the stage's input state, bit for bit."""
+    h = smooth_box(3, riemann, "lim2nd", mhd=True)
+    h.cfg = h.cfg.replace(constant_acceleration=True, acc=(0.3, -0.2, 0.15))
+    hn = h.copy()
+    o = oracle.OracleGrid(h, nthreads=2)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(3)
+    W, eint, temp, b, dt = mhd_3d_steps(hn, 3, low_mach=riemann == "lhlld")
+    for v in range(h.cfg.nvars):
+        np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
+    np.testing.assert_array_equal(h.interior(h.eint), eint)
+    for d in range(3):
+        np.testing.assert_array_equal(h.bface_interior(d), b[d])
+    assert o.g.dt == dt
