@@ -1001,9 +1001,10 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
     (S:13640-13647), and the dt from helm_rhoT_given_full.  Without USE_FASTEOS each Riemann
     side solves helm_rhoP_given from the face guess (T(i-1) + T(i)) / 2 of the stage input's
     temperatures (S:8488-8495, S:14250-14256) with its own reconstructed Ye and 1/Abar, and the
-    gammas are neither reconstructed nor kept.  LIM2ND.  Returns (W, eint, temp, gammaf,
-    [b1, b2, b3], dt).  With USE_SHOCK_FLATTENING (3 ghost layers) the flagged faces take the
-    HLL flux and the x1 sweep's gamma_e follows the reference's flattened branch."""
+    gammas are neither reconstructed nor kept.  Returns (W, eint, temp, gammaf,
+    [b1, b2, b3], dt).  LIM2ND, PPH or LIM5TH.  With USE_SHOCK_FLATTENING (3 ghost layers) a
+    flagged cell's edges fall back to PLM, the flagged faces take the HLL flux and the x1
+    sweep's gamma_e follows the reference's flattened branch."""
     from numpy_restatement_eos import given_full, rhoe_given, rhoP_given
     c = h.cfg
     G = c.ngc
@@ -1103,29 +1104,40 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
                 trans = [t for t in range(3) if t != a]
                 nb = 2 if mhd else 0
                 arrs = Wd + ([B[t] for t in trans] if mhd else []) + [ged, gcd]
-                lo, hi = zip(*[_plm(w[along(a, G - 2, G + m)], w[along(a, G - 1, G + m + 1)],
-                                    w[along(a, G, G + m + 2)]) for w in arrs])
-                L = [np.take(x, range(0, m + 1), axis=a) for x in hi]
-                R = [np.take(x, range(1, m + 2), axis=a) for x in lo]
-                er, ep, eg, ph = eqf[a]
-                devL, devR = L[nv + nb], R[nv + nb]
-                for side in (L, R):
-                    side[0] = side[0] + er
-                    side[4] = side[4] + ep
-                    side[nv + nb] = side[nv + nb] + eg
+                # PPH limits the scalars only; LIM5TH everything
+                lim = [c.rec == "lim5th" or (c.rec == "pph" and 5 <= v < nv) for v in range(len(arrs))]
+
+                def edges(kind):
+                    lo, hi = zip(*[_rec([w[along(a, G - 3 + o, G + m - 1 + o)] if G - 3 + o >= 0 else None
+                                         for o in range(5)], kind, lv) for w, lv in zip(arrs, lim)])
+                    return ([np.take(x, range(0, m + 1), axis=a) for x in hi],
+                            [np.take(x, range(1, m + 2), axis=a) for x in lo])
+                L, R = edges(c.rec)
                 flat = None
                 if fl is not None:
                     ins = [slice(1, 1 + n[x]) for x in range(3)]
                     fleft = fl[tuple(slice(0, m + 1) if x == a else ins[x] for x in range(3))]
                     fright = fl[tuple(slice(1, m + 2) if x == a else ins[x] for x in range(3))]
                     flat = fleft | fright
-                    if a == 0 and fast:
-                        # the x1 sweep's flattened gamma_e (S:8834-8869): a flagged cell's PLM edge
-                        # replaces the face value without the equilibrium, which is added to the
-                        # other side of that face instead; LIM2ND edges are the PLM edges
-                        gl = np.where(fleft, devL, devL + eg)
-                        L[nv + nb] = np.where(fright, gl + eg, gl)
-                        R[nv + nb] = np.where(fright, devR, np.where(fleft, (devR + eg) + eg, devR + eg))
+                    # a flagged cell's edges fall back to LIM2ND PLM (S:8731-8878 and the x2 / x3
+                    # counterparts)
+                    pL, pR = edges("lim2nd")
+                    rawL, rawR = L[nv + nb], R[nv + nb]
+                    L = [np.where(fleft, u, v) for u, v in zip(pL, L)]
+                    R = [np.where(fright, u, v) for u, v in zip(pR, R)]
+                er, ep, eg, ph = eqf[a]
+                devL, devR = L[nv + nb], R[nv + nb]
+                for side in (L, R):
+                    side[0] = side[0] + er
+                    side[4] = side[4] + ep
+                    side[nv + nb] = side[nv + nb] + eg
+                if fl is not None and a == 0 and fast:
+                    # the x1 sweep's flattened gamma_e (S:8834-8869): a flagged cell's PLM edge
+                    # replaces the face value without the equilibrium, which is added to the
+                    # other side of that face instead
+                    gl = np.where(fleft, devL, rawL + eg)
+                    L[nv + nb] = np.where(fright, gl + eg, gl)
+                    R[nv + nb] = np.where(fright, devR, np.where(fleft, (rawR + eg) + eg, rawR + eg))
                 if a == 0:
                     qL, qR = L[:5], R[:5]
                 elif a == 1:

@@ -285,19 +285,22 @@ def test_oracle_supersonic_all_mach_matches_numpy_restatement(oracle):
     assert not np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("rec", ["lim2nd", "pph", "lim5th"])
 @pytest.mark.parametrize("riemann", ["lhlld", "hlld", "lhllc", "hllc"])
-def test_oracle_shock_flattening_in_the_stratified_box_matches_numpy_restatement(oracle, riemann):
+def test_oracle_shock_flattening_in_the_stratified_box_matches_numpy_restatement(oracle, riemann, rec):
     """USE_SHOCK_FLATTENING in the stratified Helmholtz box at eps_sf 0.6, where the
     background's vertical pressure jumps (0.42 ... 1.28 of p) flag part of the box: the
-    detector on the full pressure with the ghosts' equilibria, the HLL flux of the flagged
-    faces (hydro and MHD) and the x1 sweep's gamma_e branch, which leaves the equilibrium off
-    a flagged cell's side of the face and adds it to the other, agree with the restatement bit
-    for bit; the flattening changes the result."""
+    detector on the full pressure with the ghosts' equilibria, the PLM fallback of a flagged
+    cell's edges under PPH and LIM5TH, the HLL flux of the flagged faces (hydro and MHD) and
+    the x1 sweep's gamma_e branch, which leaves the equilibrium off a flagged cell's side of the
+    face and adds it to the other, agree with the restatement bit for bit; the flattening
+    changes the result."""
     from phlegethon_b200 import helm_table
     import numpy_restatement_eos as RE
     tab, dpdr = helm_table.generate(nrho=271, nT=101)
     cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=riemann.endswith("d"), mach=0.05,
-                                    table=helm_table.X1_TABLE, riemann=riemann, shock_flattening=True, eps_sf=0.6)
+                                    table=helm_table.X1_TABLE, riemann=riemann, rec=rec, shock_flattening=True,
+                                    eps_sf=0.6)
     nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
     helm = oracle.Helm.for_config(cfg, tab, dpdr)
     hn, h0 = h.copy(), h.copy()
@@ -335,5 +338,31 @@ def test_oracle_constant_acceleration_matches_numpy_restatement(oracle, riemann)
         np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
     np.testing.assert_array_equal(h.interior(h.eint), eint)
     for d in range(3):
+        np.testing.assert_array_equal(h.bface_interior(d), b[d])
+    assert o.g.dt == dt
+
+
+@pytest.mark.parametrize("rec", ["pph", "lim5th"])
+@pytest.mark.parametrize("riemann", ["lhlld", "lhllc"])
+def test_oracle_stratified_higher_order_matches_numpy_restatement(oracle, riemann, rec):
+    """The stratified Helmholtz box with PPH_REC (primitives, cell B and gammas unlimited, the
+    scalars limited) or LIM5TH_REC (all limited): bit for bit with the restatement."""
+    from phlegethon_b200 import helm_table
+    import numpy_restatement_eos as RE
+    tab, dpdr = helm_table.generate(nrho=271, nT=101)
+    cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=riemann.endswith("d"), mach=0.05,
+                                    table=helm_table.X1_TABLE, riemann=riemann, rec=rec)
+    nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
+    hn = h.copy()
+    o = oracle.OracleGrid(h, oracle.Helm.for_config(cfg, tab, dpdr), nthreads=2)
+    o.init_thermo()
+    o.compute_hyperbolic_dt()
+    o.time_loop(3)
+    W, eint, temp, (ge, gc), b, dt = stratified_steps(hn, tab, dpdr, nd, 3)
+    for v in range(cfg.nvars):
+        np.testing.assert_array_equal(h.interior(h.prim[v]), hn.interior(W[v]))
+    np.testing.assert_array_equal(h.interior(h.temp), temp)
+    np.testing.assert_array_equal(h.interior(h.gammaf[0]), hn.interior(ge))
+    for d in range(3 if cfg.mhd else 0):
         np.testing.assert_array_equal(h.bface_interior(d), b[d])
     assert o.g.dt == dt
