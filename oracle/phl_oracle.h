@@ -8,9 +8,11 @@
  * (source/source.F90, Fortran 2003 + MPI + HDF5) cannot be compiled in this container or
  * on the GPU box (no gfortran/mpifort), and its tests are compile-only
  * (.github/workflows/build.yml:22-37) with no golden vectors.  The restatement is pinned
- * instead by known-answer tests (uniform state, exact hydrostatic balance, L/R mirror
- * symmetry, div B, EoS round trips) and by an independent numpy restatement of the same
- * routines in tests/.
+ * instead by known-answer tests (exact solutions, conservation, symmetries of the step,
+ * thermodynamic identities, EoS round trips) and by an independent vectorised numpy
+ * restatement, read from the Fortran separately (tests/numpy_restatement.py,
+ * tests/numpy_restatement_eos.py), of every step option this library implements and of the
+ * Helmholtz evaluation and inversions, which equals it bit for bit.
  *
  * Every routine follows the reference's operation order (including the parenthesisation of
  * long sums) so that an FMA-free double build reproduces it bit for bit.  Arrays use the
