@@ -659,7 +659,29 @@ def _corner(eA, eB, ec, sA, sB):
     return 0.25 * (eS + eW + eN + eE + dS - dN + dW - dE)
 
 
-def mhd_3d_steps(h, nsteps, low_mach):
+class PeriodicHalo:
+    """The ghost exchange of one triply periodic domain: the three operations
+    `mhd_3d_steps` delegates, so that a decomposition can replace them."""
+
+    dx = None                    # cell sizes; None: the configuration's
+
+    @staticmethod
+    def fill(a, G):
+        """Ghost cells of a padded cell array."""
+        _fill_periodic3(a, G)
+
+    @staticmethod
+    def wrap3(e):
+        """One ghost layer along x3 of a face array whose x3 index is a cell index."""
+        return _wrap(e, 2)
+
+    @staticmethod
+    def max(x):
+        """The maximum over the whole domain of a local maximum (the dt reduction)."""
+        return x
+
+
+def mhd_3d_steps(h, nsteps, low_mach, halo=PeriodicHalo):
     """The 3D counterpart of `mhd_2d_steps` on a triply periodic box: the x2 and x3 frame
     rotations of states, fluxes and B (S:9715-9747, S:10101-10144, S:10845-10889,
     S:11241-11286), all three face-EMF components (S:8926-8951 and counterparts), the three
@@ -668,13 +690,14 @@ def mhd_3d_steps(h, nsteps, low_mach):
     of the contact speed) and its reconstruction (LIM2ND, PPH or LIM5TH; the cell B edges by
     the same formulas, S:8327-8469), and USE_CONSTANT_ACCELERATION when the configuration sets
     it (rho acc on the momenta and its work from the stage's input state, S:12806-12834).
-    Returns (W, eint, temp, [b1, b2, b3], dt)."""
+    `halo` supplies the ghost exchange along x3 and the dt reduction (a slab of a
+    decomposed domain).  Returns (W, eint, temp, [b1, b2, b3], dt)."""
     c = h.cfg
     G = c.ngc
     gm = c.gamma_ad
     igmm1 = 1.0 / (gm - 1.0)
     inv_mu = 1.0 / c.mu
-    idx = [1.0 / d for d in c.dx()]
+    idx = [1.0 / d for d in (halo.dx or c.dx())]
     n = [c.nx1, c.nx2, c.nx3]
     I = tuple(slice(G, G + m) for m in n)
     nv = c.nvars
@@ -687,7 +710,7 @@ def mhd_3d_steps(h, nsteps, low_mach):
         B[1][I] = 0.5 * (b[1][:, 1:] + b[1][:, :-1])
         B[2][I] = 0.5 * (b[2][:, :, 1:] + b[2][:, :, :-1])
         for a in B:
-            _fill_periodic3(a, G)
+            halo.fill(a, G)
 
     cell_b()
     eint = W[4][I] * igmm1
@@ -701,7 +724,7 @@ def mhd_3d_steps(h, nsteps, low_mach):
         sx1 = (np.abs(v1) + cs) * idx[0]
         sx2 = (np.abs(v2) + cs) * idx[1]
         sx3 = (np.abs(v3) + cs) * idx[2]
-        smax = (sx3 + sx1 + sx2).max()
+        smax = halo.max((sx3 + sx1 + sx2).max())
         return smax, c.cfl / smax
 
     def mass_sign(f, rl, rr, smax):
@@ -738,7 +761,7 @@ def mhd_3d_steps(h, nsteps, low_mach):
         b0 = [x.copy() for x in b]
         for a1, a2, c3 in rk:
             for w in W:
-                _fill_periodic3(w, G)
+                halo.fill(w, G)
             emf = [None, None, None]
             sgn = [None, None, None]
             res = None
@@ -786,14 +809,14 @@ def mhd_3d_steps(h, nsteps, low_mach):
                            (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
                             ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
                            (s[:, :-1], s[:, 1:]), (t[:-1], t[1:]))
-            e, s = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
+            e, s = halo.wrap3(emf[1][0]), halo.wrap3(sgn[1])
             f, t = _wrap(emf[2][0], 1), _wrap(sgn[2], 1)
             cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
                            (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
                             ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
                            (s[:, :, :-1], s[:, :, 1:]), (t[:, :-1], t[:, 1:]))
             e, s = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
-            f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
+            f, t = halo.wrap3(emf[0][1]), halo.wrap3(sgn[0])
             cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
                            (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
                             ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),
