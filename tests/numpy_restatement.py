@@ -1012,7 +1012,15 @@ def _fill_strat(a, G, flip):
         a[:, ny + G - 1 + g] = f * a[:, ny + G - g]
 
 
-def stratified_steps(h, tab, dpdr, nd, nsteps):
+class StratifiedHalo(PeriodicHalo):
+    """The ghost exchange of one whole stratified box (x1 / x3 periodic, x2 walls)."""
+
+    @staticmethod
+    def fill(a, G, flip=False):
+        _fill_strat(a, G, flip)
+
+
+def stratified_steps(h, tab, dpdr, nd, nsteps, halo=StratifiedHalo):
     """The stratified Helmholtz box (3D, x2 vertical between reflective walls, x1 / x3
     periodic), magnetised (HLLD / LHLLD with constrained transport) or not (HLLC / LHLLC, with
     FLUX_IS_ALL_MACH when the configuration sets it): USE_WB on rho, p and gamma_e (S:7151-7168, the equilibria added back at the
@@ -1025,14 +1033,15 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
     side solves helm_rhoP_given from the face guess (T(i-1) + T(i)) / 2 of the stage input's
     temperatures (S:8488-8495, S:14250-14256) with its own reconstructed Ye and 1/Abar, and the
     gammas are neither reconstructed nor kept.  Returns (W, eint, temp, gammaf,
-    [b1, b2, b3], dt).  LIM2ND, PPH or LIM5TH.  With USE_SHOCK_FLATTENING (3 ghost layers) a
+    [b1, b2, b3], dt).  `halo` supplies the ghost exchange along x3 and the dt reduction (a
+    slab of a decomposed box).  LIM2ND, PPH or LIM5TH.  With USE_SHOCK_FLATTENING (3 ghost layers) a
     flagged cell's edges fall back to PLM, the flagged faces take the HLL flux and the x1
     sweep's gamma_e follows the reference's flattened branch."""
     from numpy_restatement_eos import given_full, rhoe_given, rhoP_given
     c = h.cfg
     G = c.ngc
     tl, th = 10.0 ** c.helm_ltlo, 10.0 ** c.helm_lthi
-    idx = [1.0 / d for d in c.dx()]
+    idx = [1.0 / d for d in (halo.dx or c.dx())]
     n = [c.nx1, c.nx2, c.nx3]
     I = tuple(slice(G, G + m) for m in n)
     nv = c.nvars
@@ -1053,7 +1062,7 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
         B[1][I] = 0.5 * (b[1][:, 1:] + b[1][:, :-1])
         B[2][I] = 0.5 * (b[2][:, :, 1:] + b[2][:, :, :-1])
         for d, a in enumerate(B):
-            _fill_strat(a, G, d == 1)
+            halo.fill(a, G, d == 1)
 
     if mhd:
         cell_b()
@@ -1078,7 +1087,7 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
         sx1 = (np.abs(v1) + cs) * idx[0]
         sx2 = (np.abs(v2) + cs) * idx[1]
         sx3 = (np.abs(v3) + cs) * idx[2]
-        smax = (sx3 + sx1 + sx2).max()
+        smax = halo.max((sx3 + sx1 + sx2).max())
         return smax, c.cfl / smax
 
     def mass_sign(f, rl, rr, smax):
@@ -1112,12 +1121,12 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
             ged[I] = ge[I] - eq_ge
             gcd = gc.copy()
             for v, w in enumerate(Wd):
-                _fill_strat(w, G, v == 2)
-            _fill_strat(ged, G, False)
-            _fill_strat(gcd, G, False)
+                halo.fill(w, G, v == 2)
+            halo.fill(ged, G)
+            halo.fill(gcd, G)
             tpad = np.zeros_like(W[0])
             tpad[I] = temp
-            _fill_strat(tpad, G, False)
+            halo.fill(tpad, G)
             fl = _flatten_flags(Wd[4] + h.eq_prim_cc[1], G, n, c.eps_sf) if c.shock_flattening else None
             emf = [None, None, None]
             sgn = [None, None, None]
@@ -1205,7 +1214,7 @@ def stratified_steps(h, tab, dpdr, nd, nsteps):
             for d in range(3):
                 res[1 + d] = res[1 + d] - rdev * grav[d]
             if mhd:
-                b = _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, c3 * dt, wall_wrap)
+                b = _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, c3 * dt, wall_wrap, halo.wrap3)
                 cell_b()
             U = [a1 * u0 + a2 * u + c3 * dt * rr for u0, u, rr in zip(U0, U, res)]
             rho = U[0]
@@ -1250,7 +1259,7 @@ def _flatten_flags(pf, G, n, eps_sf):
     return fl
 
 
-def _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, a3, wall_wrap):
+def _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, a3, wall_wrap, wrap3):
     """Corner EMFs of the stratified box (reflective x2 walls, x1 / x3 periodic) and the RK
     update of the three face-B arrays."""
     I = tuple(slice(G, G + m) for m in n)
@@ -1265,14 +1274,14 @@ def _ct_walls(b, b0, emf, sgn, Wd, B, G, n, idx, a1, a2, a3, wall_wrap):
                    (ec3[G - 1:G + nx, G - 1:G + ny, Iz], ec3[G - 1:G + nx, G:G + ny + 1, Iz],
                     ec3[G:G + nx + 1, G:G + ny + 1, Iz], ec3[G:G + nx + 1, G - 1:G + ny, Iz]),
                    (s_[:, :-1], s_[:, 1:]), (t[:-1], t[1:]))
-    e, s_ = _wrap(emf[1][0], 2), _wrap(sgn[1], 2)
+    e, s_ = wrap3(emf[1][0]), wrap3(sgn[1])
     f, t = wall_wrap(emf[2][0], True), wall_wrap(sgn[2], False)
     cor1 = _corner((e[:, :, :-1], e[:, :, 1:]), (f[:, :-1], f[:, 1:]),
                    (ec1[Ix, G - 1:G + ny, G - 1:G + nz], ec1[Ix, G - 1:G + ny, G:G + nz + 1],
                     ec1[Ix, G:G + ny + 1, G:G + nz + 1], ec1[Ix, G:G + ny + 1, G - 1:G + nz]),
                    (s_[:, :, :-1], s_[:, :, 1:]), (t[:, :-1], t[:, 1:]))
     e, s_ = _wrap(emf[2][1], 0), _wrap(sgn[2], 0)
-    f, t = _wrap(emf[0][1], 2), _wrap(sgn[0], 2)
+    f, t = wrap3(emf[0][1]), wrap3(sgn[0])
     cor2 = _corner((e[:-1], e[1:]), (f[:, :, :-1], f[:, :, 1:]),
                    (ec2[G - 1:G + nx, Iy, G - 1:G + nz], ec2[G:G + nx + 1, Iy, G - 1:G + nz],
                     ec2[G:G + nx + 1, Iy, G:G + nz + 1], ec2[G - 1:G + nx, Iy, G:G + nz + 1]),

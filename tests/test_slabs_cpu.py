@@ -9,8 +9,8 @@ reference's MPI bricks (set up at source/source.F90:1160-1210) exchange at the s
 test runs the numpy restatement of the 3D MHD step on two slabs that exchange exactly that and
 nothing else, and requires the assembled result to equal the single-domain step bit for bit:
 the plan is complete, and the corners and faces on a slab boundary, computed by both
-neighbours, agree.  (The reference also exchanges temp and gammaf; the ideal-gas step here has
-neither.)
+neighbours, agree.  The stratified Helmholtz box, with its reflective x2 walls, adds the
+temperatures and the FASTEOS gammas to the exchanged cell arrays, as the reference does.
 """
 import os
 import socket
@@ -35,10 +35,11 @@ def _free_port():
 
 
 class SlabHalo:
-    """Ghost exchange of one x3 slab of a periodic domain over torch.distributed."""
+    """Ghost exchange of one x3 slab over torch.distributed: x1 periodic, x2 periodic or (walls)
+    mirrored at reflective walls, x3 periodic across the ranks."""
 
-    def __init__(self, rank, world, dx):
-        self.rank, self.world, self.dx = rank, world, dx
+    def __init__(self, rank, world, dx, walls=False):
+        self.rank, self.world, self.dx, self.walls = rank, world, dx, walls
         self.sent = 0          # bytes this rank has contributed to the exchanges
 
     def _neighbours(self, lo, hi):
@@ -52,10 +53,10 @@ class SlabHalo:
         above = got[(self.rank + 1) % self.world][0].numpy()
         return below, above
 
-    def fill(self, a, G):
-        # x1 and x2 are whole on every rank: periodic images locally, then the x3 ghost planes
+    def fill(self, a, G, flip=False):
+        # x1 and x2 are whole on every rank: their ghosts locally, then the x3 ghost planes
         # (whole padded planes, so the corner ghosts come along) from the neighbours
-        for ax in (0, 1):
+        for ax in ((0,) if self.walls else (0, 1)):
             m = a.shape[ax] - 2 * G
             lo = [slice(None)] * 3
             src = [slice(None)] * 3
@@ -63,6 +64,12 @@ class SlabHalo:
             a[tuple(lo)] = a[tuple(src)]
             lo[ax], src[ax] = slice(m + G, m + 2 * G), slice(G, 2 * G)
             a[tuple(lo)] = a[tuple(src)]
+        if self.walls:
+            ny = a.shape[1] - 2 * G
+            f = -1.0 if flip else 1.0
+            for g in range(1, G + 1):
+                a[:, G - g] = f * a[:, G + g - 1]
+                a[:, ny + G - 1 + g] = f * a[:, ny + G - g]
         nz = a.shape[2] - 2 * G
         below, above = self._neighbours(a[:, :, G:2 * G], a[:, :, nz:nz + G])
         a[:, :, :G] = below
@@ -139,3 +146,86 @@ def test_two_slabs_reproduce_the_single_domain_step(riemann):
     np.testing.assert_array_equal(b1[2][:, :, :nzl + 1], bf[2][:, :, nzl:])
     np.testing.assert_array_equal(b0[2][:, :, nzl], b1[2][:, :, 0])
     np.testing.assert_array_equal(b1[2][:, :, nzl], b0[2][:, :, 0])
+
+
+def _slab_of(full, rank, world):
+    """The x3 slab of host grid `full` that rank owns: every cell array with its ghost planes,
+    every face array of its planes (the x3 faces on both of its ends)."""
+    from phlegethon_b200.grid import HostGrid
+    c = full.cfg
+    G, nzl = c.ngc, c.nx3 // world
+    k0 = rank * nzl
+    loc = HostGrid(c.replace(nx3=nzl))
+    for name in ("prim", "temp", "eint", "gammaf", "grav", "phi_cc", "eq_prim_cc", "eq_gammae_cc", "b_cc"):
+        a = getattr(full, name)
+        if a is not None:
+            getattr(loc, name)[...] = a[..., k0:k0 + nzl + 2 * G]
+    for name in ("phi_x", "eq_prim_x", "eq_gammae_x"):
+        for d in range(3):
+            a = getattr(full, name)[d]
+            if a is not None:
+                getattr(loc, name)[d][...] = a[..., k0:k0 + nzl + (d == 2)]
+    if c.mhd:
+        for d in range(3):
+            bl = loc.bface_interior(d)
+            bl[...] = full.bface_interior(d)[:, :, k0:k0 + bl.shape[2]]
+    return loc
+
+
+def _strat_case(riemann, flattening):
+    from phlegethon_b200 import helm_table, problems
+    import numpy_restatement_eos as RE
+    tab, dpdr = helm_table.generate(nrho=271, nT=101)
+    cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=riemann.endswith("d"), mach=0.05,
+                                    table=helm_table.X1_TABLE, riemann=riemann,
+                                    shock_flattening=flattening, eps_sf=0.6)
+    nd = RE.nodes(cfg.helm_nT, cfg.helm_nrho, cfg.helm_ltlo, cfg.helm_lthi, cfg.helm_ldlo, cfg.helm_ldhi)
+    return h, tab, dpdr, nd
+
+
+def _strat_worker(rank, world, port, riemann, flattening, steps, out):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, HERE)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from numpy_restatement import stratified_steps
+        full, tab, dpdr, nd = _strat_case(riemann, flattening)
+        loc = _slab_of(full, rank, world)
+        halo = SlabHalo(rank, world, full.cfg.dx(), walls=True)
+        W, eint, temp, (ge, gc), b, dt = stratified_steps(loc, tab, dpdr, nd, steps, halo=halo)
+        G = full.cfg.ngc
+        out[rank] = ([w[G:-G, G:-G, G:-G] for w in W], temp, ge[G:-G, G:-G, G:-G], b, dt)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("riemann, flattening", [("lhlld", False), ("lhlld", True), ("lhllc", False)])
+def test_two_slabs_of_the_stratified_box_reproduce_the_single_domain_step(riemann, flattening):
+    """The stratified Helmholtz box (the benchmark's workloads, 8 x 12 x 6) split into two x3 slabs
+    of 3 planes: ghost planes of the primitives, scalars, cell B, the gammas and the
+    temperatures (the no-FASTEOS face guess and the Newton's warm start read the latter), the
+    EMF planes and the dt maximum reproduce the single-domain step bit for bit, with
+    shock flattening's detector reading the exchanged ghosts."""
+    sys.path.insert(0, HERE)
+    from numpy_restatement import stratified_steps
+    steps = 2
+    full, tab, dpdr, nd = _strat_case(riemann, flattening)
+    Wf, _, Tf, (gef, _), bf, dtf = stratified_steps(full.copy(), tab, dpdr, nd, steps)
+    G = full.cfg.ngc
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_strat_worker, args=(2, port, riemann, flattening, steps, out), nprocs=2,
+                       start_method="spawn")
+    (W0, T0, g0, b0, dt0), (W1, T1, g1, b1, dt1) = out[0], out[1]
+    assert dt0 == dt1 == dtf
+    for v in range(full.cfg.nvars):
+        np.testing.assert_array_equal(np.concatenate([W0[v], W1[v]], axis=2), Wf[v][G:-G, G:-G, G:-G])
+    np.testing.assert_array_equal(np.concatenate([T0, T1], axis=2), Tf)
+    np.testing.assert_array_equal(np.concatenate([g0, g1], axis=2), gef[G:-G, G:-G, G:-G])
+    if full.cfg.mhd:
+        for d in range(2):
+            np.testing.assert_array_equal(np.concatenate([b0[d], b1[d]], axis=2), bf[d])
+        np.testing.assert_array_equal(np.concatenate([b0[2][:, :, :-1], b1[2]], axis=2), bf[2])
