@@ -19,6 +19,9 @@ equations, independent of any restatement of the reference.
   slope, so on smooth data the scheme is first order (the error halves per doubling); PPH_REC
   and LIM5TH_REC converge faster than second order until their extremum limiters and the
   third-order Runge-Kutta stepper set the rate.
+* The Gresho vortex, a steady rotating flow in pressure balance, at Mach 0.1 and 0.01: LHLLC
+  keeps the same fraction of the kinetic energy at both Mach numbers, HLLC loses more at the
+  lower one (the low-Mach dissipation problem the LHLLC solver addresses).
 """
 import math
 
@@ -427,6 +430,54 @@ def test_periodic_box_conserves_mass_momentum_energy(oracle, case):
     for a, b in zip(p0, p1):
         assert abs(b - a) <= 1e-13 * scale, (p0, p1)
     assert abs(e1 - e0) <= 1e-13 * e0, (e0, e1)
+
+
+# ------------------------------------------------------------------------------ Gresho vortex
+def gresho(n, riemann, mach, gamma=5.0 / 3.0):
+    """The Gresho vortex, an exact steady solution of the Euler equations (Gresho & Chan 1990;
+    the low-Mach form of Miczek et al. 2015): v_phi = 5r (r < 0.2), 2 - 5r (r < 0.4), 0 beyond,
+    with the pressure that balances its centrifugal force, p = p0 + 12.5 r^2 (r < 0.2),
+    p0 + 12.5 r^2 + 4 (1 - 5r - ln 0.2 + ln r) (r < 0.4), p0 - 2 + 4 ln 2 beyond; rho = 1 and
+    p0 = 1 / (gamma M^2) - 1/2 sets the maximum Mach number M (the reference's tests/gresho
+    set-up: 40^2, gamma 5/3, LIM2ND, Mach_cutoff 1e-4)."""
+    cfg = Config(sdims=2, nx1=n, nx2=n, riemann=riemann, bc=[["periodic", "periodic"]] * 3,
+                 gamma_ad=gamma, mach_cutoff=1e-4, cfl=0.8)
+    h = HostGrid(cfg)
+    x, y, _ = h.coords()
+    dx, dy = x - 0.5, y - 0.5
+    r = np.sqrt(dx * dx + dy * dy)
+    rr = np.maximum(r, 1e-300)
+    vphi = np.where(r < 0.2, 5.0 * r, np.where(r < 0.4, 2.0 - 5.0 * r, 0.0))
+    p0 = 1.0 / gamma / mach ** 2 - 0.5
+    p = np.where(r < 0.2, p0 + 12.5 * r * r,
+                 np.where(r < 0.4, p0 + 12.5 * r * r + 4.0 * (1.0 - 5.0 * r - math.log(0.2) + np.log(rr)),
+                          p0 - 2.0 + 4.0 * math.log(2.0)))
+    h.prim[0] = 1.0
+    h.prim[1] = -vphi * dy / rr
+    h.prim[2] = vphi * dx / rr
+    h.prim[3] = p
+    return cfg, h
+
+
+def test_gresho_vortex_low_mach_dissipation(oracle):
+    """The low-dissipation solver's point (Minoshima & Miyoshi 2021): on the Gresho vortex the
+    kinetic energy LHLLC keeps after t = 0.2 does not depend on the Mach number (the star
+    pressure's dissipation scales with phi = chi (2 - chi)), while HLLC, whose dissipation does
+    not fall with the Mach number, loses more of it the lower the Mach number."""
+    kept = {}
+    for riemann in ("lhllc", "hllc"):
+        for mach in (0.1, 0.01):
+            cfg, h = gresho(40, riemann, mach)
+            ke0 = float((h.interior(h.prim)[1:3] ** 2).sum())
+            o = oracle.OracleGrid(h, None, nthreads=4)
+            o.init_thermo()
+            o.compute_hyperbolic_dt()
+            o.time_loop(100000, 0.2)
+            kept[riemann, mach] = float((h.interior(h.prim)[1:3] ** 2).sum()) / ke0
+    assert abs(kept["lhllc", 0.1] - kept["lhllc", 0.01]) < 2e-3
+    assert kept["lhllc", 0.01] > 0.85
+    assert kept["hllc", 0.01] < kept["hllc", 0.1] - 0.1
+    assert kept["lhllc", 0.01] > kept["hllc", 0.01] + 0.3
 
 
 # ------------------------------------------------------------------------------ the CUDA forms
