@@ -245,7 +245,8 @@ def hot_bubble_steps(h, nsteps, dt=None, eps_sf=None, rec="lim2nd"):
 
 
 # ------------------------------------------------------------------------------ ideal MHD
-def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None, side_eos=None, flat=None):
+def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None, side_eos=None, flat=None,
+          all_mach=False):
     """HLLD (low_mach False, HLLD_FLUX) or LHLLD (low_mach True, LHLLD_FLUX) flux of one face
     array in the face frame, ideal gas (S:13969-15024).  q = (rho, v1, v2, v3, p), b = (B
     normal, B transverse 2, B transverse 3); in 2D v3 and B3 are zero arrays, as the reference
@@ -254,15 +255,17 @@ def _hlld(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL=(), xR=(), fasteos=None,
     c^2 = gamma_c p / rho); side_eos = (e L, c^2 L, e R, c^2 R) takes each side's internal
     energy and sound speed squared as given (the Helmholtz solves without USE_FASTEOS); flat
     marks the faces of USE_SHOCK_FLATTENING, which take the two-wave HLL flux with
-    sL = min(0, sL), sR = max(0, sR) (S:14386-14493).  Returns the fluxes (rho, m1, m2, m3, E,
-    then one per scalar) and fluxb(2), fluxb(3)."""
-    (F, hF), (fb, hfb) = _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos)
+    sL = min(0, sL), sR = max(0, sR) (S:14386-14493); all_mach: FLUX_IS_ALL_MACH, LHLLD's
+    fan extended by the outer states L (sL > 0) and R (sR <= 0) (S:14576-14661).  Returns the
+    fluxes (rho, m1, m2, m3, E, then one per scalar) and fluxb(2), fluxb(3)."""
+    (F, hF), (fb, hfb) = _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos,
+                                   all_mach)
     if flat is None:
         return F, fb
     return [np.where(flat, a, b) for a, b in zip(hF, F)], [np.where(flat, a, b) for a, b in zip(hfb, fb)]
 
 
-def _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos):
+def _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_eos, all_mach=False):
     """`_hlld`'s arithmetic; returns ((F, HLL F), (fb, HLL fb))."""
     igmm1 = 1.0 / (gm - 1.0)
     rhoL, v1L, v2L, v3L, pL = qL
@@ -384,8 +387,17 @@ def _hlld_fan(qL, qR, bL, bR, gm, mach_cutoff, low_mach, xL, xR, fasteos, side_e
         re = pick(resL, re2L, re2R, resR)
         b2 = pick(b2sL, b22, b22, b2sR)
         b3 = pick(b3sL, b32, b32, b3sR)
-        F = [rho * u, rho * u * u + pst - bx1_2, rho * u * v2 - bx1 * b2, rho * u * v3 - bx1 * b3,
-             (re + pst) * u - bx1 * (bx1 * u + v2 * b2 + v3 * b3)]
+        pres = pst
+        if all_mach:
+            outL = sL > 0.0
+            outR = ~outL & ~sel[0] & ~sel[1] & ~sel[2] & ~(sR > 0.0)
+
+            def outer(a, l_, r_):
+                return np.where(outL, l_, np.where(outR, r_, a))
+            rho, u, v2, v3 = outer(rho, rhoL, rhoR), outer(u, v1L, v1R), outer(v2, v2L, v2R), outer(v3, v3L, v3R)
+            re, b2, b3, pres = outer(re, reL, reR), outer(b2, b2L, b2R), outer(b3, b3L, b3R), outer(pst, ptL, ptR)
+        F = [rho * u, rho * u * u + pres - bx1_2, rho * u * v2 - bx1 * b2, rho * u * v3 - bx1 * b3,
+             (re + pres) * u - bx1 * (bx1 * u + v2 * b2 + v3 * b3)]
         up = np.copysign(1.0, u)
         hp = 0.5 * (1.0 + up)
         hm = 0.5 * (1.0 - up)
@@ -780,7 +792,7 @@ def mhd_3d_steps(h, nsteps, low_mach, halo=PeriodicHalo):
                     qL = [L[0], L[3], L[1], L[2], L[4]]
                     qR = [R[0], R[3], R[1], R[2], R[4]]
                     bL, bR = [b[2], L[5], L[6]], [b[2], R[5], R[6]]
-                F, fb = _hlld(qL, qR, bL, bR, gm, c.mach_cutoff, low_mach, L[7:], R[7:])
+                F, fb = _hlld(qL, qR, bL, bR, gm, c.mach_cutoff, low_mach, L[7:], R[7:], all_mach=c.all_mach)
                 if a == 0:
                     emf[0] = (None, fb[1], -fb[0])
                 elif a == 1:
@@ -1195,6 +1207,7 @@ def stratified_steps(h, tab, dpdr, nd, nsteps, halo=StratifiedHalo):
                     eos = dict(side_eos=tuple(sides))
                 if mhd:
                     F, fb = _hlld(qL, qR, bL, bR, c.gamma_ad, c.mach_cutoff, low_mach, L[5:nv], R[5:nv], flat=flat,
+                                  all_mach=c.all_mach,
                                   **eos)
                     emf[a] = [(None, fb[1], -fb[0]), (-fb[1], None, -fb[0]), (fb[1], -fb[0], None)][a]
                 else:
