@@ -670,3 +670,24 @@ def test_helmholtz_sound_speed_from_finite_differences(oracle, table):
             gam1 = chi_t * (P / rho) * chi_t / (T * cv) + chi_r
             z = 1.0 + (E + clight * clight) * rho / P
             assert abs(clight * math.sqrt(gam1 / z) - sound) <= 1e-5 * sound, (lr, lt)
+
+
+# ------------------------------------------------------------------------------ determinism
+def test_oracle_is_independent_of_its_thread_count(oracle):
+    """The checker's OpenMP loops carry no order-dependent reduction (the dt reduction is a
+    maximum): the magnetised stratified Helmholtz box with shock flattening gives the same bits
+    on 1, 3 and 8 threads."""
+    res = []
+    for nt in (1, 3, 8):
+        cfg, h = problems.stratified_3d(8, ny=12, nz=6, mhd=True, mach=0.05, table=helm_table.X1_TABLE,
+                                        shock_flattening=True, eps_sf=0.6)
+        o = oracle.OracleGrid(h, oracle.Helm.for_config(cfg, *helm_table.generate(nrho=271, nT=101)),
+                              nthreads=nt)
+        o.init_thermo()
+        o.compute_hyperbolic_dt()
+        o.time_loop(3)
+        res.append((h.interior(h.prim).copy(), [h.bface_interior(d).copy() for d in range(3)], o.g.dt))
+    for r in res[1:]:
+        assert np.array_equal(r[0], res[0][0]) and r[2] == res[0][2]
+        for a, b in zip(r[1], res[0][1]):
+            assert np.array_equal(a, b)
