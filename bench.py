@@ -300,17 +300,50 @@ def cpu_rate(name, steps, nthreads=0, slab=None, fasteos=True, eos_table="fermi"
     return steps * cfg.n_cells / dt, cores, sample + ", %d steps" % steps
 
 
+def eos_reference_line(args):
+    """The EoS batch's reference arm: the oracle's bracket-guess inversion (helm_rhoe_given) of a
+    bounded slice of the same 2^24-sample batch, on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from phlegethon_b200 import helm_table, problems
+    n = args.n or (1 << 24)
+    k = min(n, 1 << 16)
+    rho, T, abar, zbar = problems.eos_samples(n, seed=99)
+    rho, T, abar, zbar = rho[:k], T[:k], abar[:k], zbar[:k]
+    cfg, _ = problems.stratified_3d(8)
+    helm = pyoracle.Helm.for_config(cfg, *helm_table.make(args.eos_table, workers=table_workers()))
+    e = np.array([helm.given2(*a, deriv=False)[0] for a in zip(rho, T, abar, zbar)])
+    cpu = eos_cpu_rate(rho, e, abar, zbar, seconds=max(5.0, 2.0 * max(1, args.steps)), eos_table=args.eos_table)
+    return {"impl": "reference", "metric": EOS_METRIC, "value": cpu["value"], "unit": "inversions/s",
+            "n_gpus": args.gpus, "steps": max(1, args.steps), "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "eos_batch", "n": n, "eos_table": args.eos_table},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "inversions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of the reference routines (oracle/), OpenMP over all host cores; "
+                    "the reference's Fortran build is unavailable (no gfortran/mpifort)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.config == "eos":
+        print(json.dumps(eos_reference_line(args)), flush=True)
+        return
     steps = max(1, args.steps)
     rate, cores, sample = cpu_rate(args.config, steps, fasteos=not args.no_fasteos, eos_table=args.eos_table)
     cfgname = args.config
+    n = args.n or default_size(cfgname)
+    # the same workload keys as the GPU arm's line (its name, size, cells and table); the
+    # oracle times a bounded slab of it, named in cpu_baseline.sample
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "zone-updates/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfgname, "n": args.n or default_size(cfgname), "eos_table": args.eos_table},
+            "config": {"workload": cfgname + ("_no_fasteos" if args.no_fasteos else ""), "n": n,
+                       "cells": n ** 3 if cfgname.startswith("stratified") else n ** 2,
+                       "eos_table": args.eos_table, "form": "fp64 (CPU oracle)",
+                       "parallelism": "single"},
             "cpu_baseline": {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
