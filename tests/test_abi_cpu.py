@@ -99,3 +99,22 @@ def test_python_binding_matches_header_arity(lib_path):
         params = protos[name].strip()
         n = 0 if params in ("", "void") else len(params.split(","))
         assert len(getattr(lib, name).argtypes) == n, name
+
+
+def test_bench_reference_arm_line():
+    """`bench.py --impl reference` (the oracle on the host's cores) prints one JSON line with the
+    contract's keys and the GPU arm's workload keys; the 256^2 hot bubble keeps it short."""
+    import json
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--config",
+                        "hot_bubble", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "zone-updates/s" and d["value"] > 0
+    assert d["config"]["workload"] == "hot_bubble" and d["config"]["n"] == 256
+    assert d["config"]["cells"] == 256 * 256
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
