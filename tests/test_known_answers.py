@@ -23,6 +23,7 @@ equations, independent of any restatement of the reference.
   keeps the same fraction of the kinetic energy at both Mach numbers, HLLC loses more at the
   lower one (the low-Mach dissipation problem the LHLLC solver addresses); threaded by a
   uniform axial field, LHLLD does the same while the Alfven speed stays below the flow speed.
+* The Runge-Kutta steppers are second (RK2) and third (RK3) order in time.
 """
 import math
 
@@ -522,6 +523,31 @@ def test_gresho_vortex_low_mach_dissipation_with_b(oracle):
     assert kept["hlld", 1e-3, 0.01] < kept["hlld", 1e-3, 0.1] - 0.03
     assert kept["lhlld", 0.3, 0.01] < kept["lhlld", 0.3, 0.1] - 0.1
     assert abs(kept["lhlld", 0.3, 0.01] - kept["hlld", 0.3, 0.01]) < 0.02
+
+
+# ------------------------------------------------------------------------------ time order
+def test_runge_kutta_order_in_time(oracle):
+    """The Shu-Osher coefficients of RK2_STEPPER and RK3_STEPPER (source.F90:7018-7038) give
+    second and third order in time: on one grid (64 cells, a density wave advected at unit
+    speed, PPH_REC whose unlimited edges make the semi-discrete system smooth) the difference
+    to a run at a 32 times smaller CFL number falls by 4x and 8x per halving of dt."""
+    def run(stages, cfl):
+        cfg = Config(sdims=2, nx1=64, nx2=4, x2u=4.0 / 64, riemann="hllc", rec="pph", rk_stages=stages,
+                     bc=[["periodic", "periodic"]] * 3, cfl=cfl, gamma_ad=1.4)
+        h = HostGrid(cfg)
+        x, _, _ = h.coords()
+        h.prim[0] = 1.0 + 0.2 * np.sin(2.0 * np.pi * x)
+        h.prim[1] = 1.0
+        h.prim[2] = 0.0
+        h.prim[3] = 1.0
+        run_oracle(oracle, cfg, h, 0.25)
+        return h.interior(h.prim)[0][:, 0, 0].copy()
+
+    for stages, order in ((2, 2.0), (3, 3.0)):
+        ref = run(stages, 0.4 / 64)
+        err = [float(np.abs(run(stages, c) - ref).max()) for c in (0.4, 0.2, 0.1, 0.05)]
+        rates = [math.log2(err[i] / err[i + 1]) for i in range(3)]
+        assert all(abs(r - order) < 0.1 for r in rates), (stages, rates)
 
 
 # ------------------------------------------------------------------------------ the CUDA forms
