@@ -550,6 +550,35 @@ def test_runge_kutta_order_in_time(oracle):
         assert all(abs(r - order) < 0.1 for r in rates), (stages, rates)
 
 
+def test_evolve_etot_conserves_total_energy_in_a_closed_box(oracle):
+    """The hot bubble between reflective walls under gravity: with EVOLVE_ETOT the scheme
+    evolves E + rho phi in conservation form (the potential flux F_rho phi_face,
+    source.F90:8961-8966), so the box's total energy including the potential, and its mass,
+    stay constant to rounding over 200 steps; with gravity as a momentum and work source
+    instead (S:12631-12638) the total drifts by O(1e-5)."""
+    from phlegethon_b200 import problems
+    drift = {}
+    for etot in (True, False):
+        cfg, h = problems.hot_bubble_2d(32)
+        h.cfg = cfg.replace(etot=etot)
+        phi = h.interior(h.phi_cc)
+
+        def totals():
+            w, e = h.interior(h.prim), h.interior(h.eint)
+            return float(w[0].sum()), float((e + 0.5 * w[0] * (w[1] ** 2 + w[2] ** 2) + w[0] * phi).sum())
+        o = oracle.OracleGrid(h, None, nthreads=4)
+        o.init_thermo()
+        o.compute_hyperbolic_dt()
+        m0, e0 = totals()
+        o.time_loop(200)
+        m1, e1 = totals()
+        assert abs(m1 / m0 - 1.0) < 1e-13
+        assert float(np.abs(h.interior(h.prim)[1:3]).max()) > 1e-2     # the bubble has risen
+        drift[etot] = abs(e1 / e0 - 1.0)
+    assert drift[True] < 1e-13
+    assert drift[False] > 1e-6
+
+
 # ------------------------------------------------------------------------------ the CUDA forms
 def run_gpu(cfg, h, tmax, precision):
     from phlegethon_b200.abi import Simulation
